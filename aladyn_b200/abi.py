@@ -1,0 +1,207 @@
+"""ctypes mirror of include/aladyn_gpu.h and the loader of the device library.
+
+The structures below must match the C header byte for byte; the
+``test_abi`` CPU test checks their sizes against the compiled library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libaladyn_gpu.so")
+
+AGPU_OK = 0
+AGPU_E_WINDOW = 2
+AGPU_E_COUNT = 99
+AGPU_E_ARG = 101
+AGPU_E_CUDA = 102
+AGPU_E_NOMEM = 103
+AGPU_E_CAPACITY = 104
+AGPU_E_INDEX = 105
+AGPU_E_IONZ_INDEX = 106
+AGPU_E_NONFINITE = 107
+AGPU_E_NODEVICE = 108
+AGPU_E_STATE = 109
+
+AGPU_FP64 = 0
+AGPU_FP32_SPLIT = 1
+
+AGPU_EBIT_INDEX = 1
+AGPU_EBIT_IONZ_INDEX = 2
+AGPU_EBIT_NONFINITE = 4
+AGPU_EBIT_CAPACITY = 8
+
+
+class AgpuParams(C.Structure):
+    _fields_ = [
+        ("ndim", C.c_int32),
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("nfield", C.c_int32),
+        ("curr_ndim", C.c_int32),
+        ("ibx", C.c_int32), ("iby", C.c_int32), ("ibz", C.c_int32),
+        ("iform", C.c_int32),
+        ("precision", C.c_int32),
+        ("nsp", C.c_int32),
+        ("nsp_run", C.c_int32),
+        ("w_sh", C.c_int32),
+        ("ionz_lev", C.c_int32),
+        ("n_mol_atoms", C.c_int32 * 4),
+        ("reserved_i", C.c_int32 * 4),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+        ("dx_inv", C.c_double), ("dy_inv", C.c_double), ("dz_inv", C.c_double),
+        ("dt", C.c_double),
+        ("xmn", C.c_double), ("ymn", C.c_double), ("zmn", C.c_double),
+        ("gxmin", C.c_double), ("gxmax", C.c_double),
+        ("gymin", C.c_double), ("gymax", C.c_double),
+        ("gzmin", C.c_double), ("gzmax", C.c_double),
+        ("xmax", C.c_double),
+        ("se_coeff", C.c_double * 2),
+        ("djc", C.c_double * 3),
+        ("ompe", C.c_double),
+        ("lorentz_fact", C.c_double * 4),
+        ("w_speed", C.c_double), ("wi_time", C.c_double), ("wf_time", C.c_double),
+        ("reserved_d", C.c_double * 4),
+        ("seed", C.c_uint64),
+        ("capacity", C.c_int64 * 4),
+    ]
+
+
+class AgpuPlasma(C.Structure):
+    _fields_ = [
+        ("ic", C.c_int32),
+        ("npx", C.c_int32), ("npy", C.c_int32), ("npz", C.c_int32),
+        ("charge", C.c_int32),
+        ("part_ind", C.c_int32),
+        ("wgh", C.c_float),
+        ("reserved_f", C.c_float),
+        ("x_start", C.c_double), ("x_end", C.c_double),
+        ("y_min", C.c_double), ("y_max", C.c_double),
+        ("z_min", C.c_double), ("z_max", C.c_double),
+        ("jitter", C.c_double),
+        ("seed", C.c_uint64),
+    ]
+
+
+class AgpuLaser(C.Structure):
+    _fields_ = [
+        ("a0", C.c_double), ("lam0", C.c_double), ("w0_y", C.c_double),
+        ("tau_fwhm", C.c_double), ("xc", C.c_double), ("xf", C.c_double),
+        ("y0", C.c_double), ("z0", C.c_double),
+    ]
+
+
+class AgpuStepOut(C.Structure):
+    _fields_ = [
+        ("np", C.c_int64 * 4),
+        ("removed", C.c_int64 * 4),
+        ("injected", C.c_int64 * 4),
+        ("new_electrons", C.c_int64),
+        ("ion_field_max", C.c_double),
+        ("xmn", C.c_double),
+        ("nshx", C.c_int32),
+        ("error_bits", C.c_uint32),
+    ]
+
+
+class AgpuDiagOut(C.Structure):
+    _fields_ = [
+        ("field_energy", C.c_double * 6),
+        ("max_abs_e", C.c_double),
+        ("kin_energy", C.c_double * 4),
+        ("charge", C.c_double * 4),
+        ("momentum", (C.c_double * 3) * 4),
+        ("np", C.c_int64 * 4),
+    ]
+
+
+class AgpuTimers(C.Structure):
+    _fields_ = [
+        ("ms_push_deposit", C.c_double),
+        ("ms_yee", C.c_double),
+        ("ms_sort", C.c_double),
+        ("ms_window", C.c_double),
+        ("ms_ionize", C.c_double),
+        ("ms_other", C.c_double),
+        ("launches_push_deposit", C.c_int64),
+        ("launches_yee", C.c_int64),
+        ("launches_total", C.c_int64),
+        ("pushes", C.c_int64),
+        ("yee_cells", C.c_int64),
+    ]
+
+
+# Every exported symbol of the C-ABI, with its ctypes signature.
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+SIGNATURES = {
+    "agpu_create": (C.c_int, [C.POINTER(AgpuParams), C.POINTER(_P)]),
+    "agpu_destroy": (C.c_int, [_P]),
+    "agpu_error_string": (C.c_char_p, [C.c_int]),
+    "agpu_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+    "agpu_set_fields": (C.c_int, [_P, _D, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "agpu_get_fields": (C.c_int, [_P, _D, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "agpu_get_currents": (C.c_int, [_P, _D, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "agpu_set_species": (C.c_int, [_P, C.c_int32, _D, C.c_int64, C.c_int64, C.c_int32]),
+    "agpu_get_species": (C.c_int, [_P, C.c_int32, _D, C.c_int64, C.POINTER(C.c_int64), C.c_int32]),
+    "agpu_get_count": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int64)]),
+    "agpu_set_plasma_source": (C.c_int, [_P, C.POINTER(AgpuPlasma)]),
+    "agpu_load_plasma": (C.c_int, [_P, C.c_int32]),
+    "agpu_init_laser": (C.c_int, [_P, C.POINTER(AgpuLaser)]),
+    "agpu_set_ionization_table": (C.c_int, [_P, C.c_int32, _D, C.c_int32, C.c_int32, C.c_double]),
+    "agpu_set_ionization_species": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                              C.c_int32, C.c_double]),
+    "agpu_step": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int32, C.POINTER(AgpuStepOut)]),
+    "agpu_window_inject": (C.c_int, [_P, C.c_int32, _D, C.c_int64, C.c_int64, C.c_int32]),
+    "agpu_diag": (C.c_int, [_P, C.POINTER(AgpuDiagOut)]),
+    "agpu_set_profiling": (C.c_int, [_P, C.c_int32]),
+    "agpu_get_timers": (C.c_int, [_P, C.POINTER(AgpuTimers)]),
+    "agpu_reset_timers": (C.c_int, [_P]),
+    "agpu_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "agpu_synchronize": (C.c_int, [_P]),
+    "agpu_set_sort_interval": (C.c_int, [_P, C.c_int32]),
+    "agpu_set_deterministic": (C.c_int, [_P, C.c_int32]),
+    "agpu_struct_sizes": (C.c_int, [C.POINTER(C.c_int64), C.c_int32]),
+}
+
+_lib = None
+
+
+class AgpuError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        msg = f"{where} failed with status {code}"
+        if _lib is not None:
+            try:
+                msg += ": " + _lib.agpu_error_string(code).decode()
+            except Exception:  # pragma: no cover - message only
+                pass
+        super().__init__(msg)
+        self.code = code
+
+
+def load_library(path: str | None = None):
+    """Load the in-tree device library; raise if it has not been built.
+
+    There is no CPU fallback: a missing library is an error.
+    """
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"device library {p} is missing; build it with "
+            "`python -m aladyn_b200.build` (nvcc, sm_100a)")
+    lib = C.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def check(code: int, where: str):
+    if code != AGPU_OK:
+        raise AgpuError(code, where)

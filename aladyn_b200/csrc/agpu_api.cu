@@ -1,0 +1,1031 @@
+// agpu_api.cu — the C-ABI of include/aladyn_gpu.h: handle lifetime, state
+// transfer, the step driver (lpf2_evolve + lp_run), window, ionization and
+// diagnostics.  Compiled with -fmad=false (host-side FP64 bookkeeping of the
+// window origin follows the reference's arithmetic).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/aladyn_gpu.h"
+#include "agpu_ionz.h"
+#include "agpu_kernels.h"
+#include "agpu_util.h"
+
+using namespace agpu;
+
+namespace {
+
+struct Species32 {
+  int* cell = nullptr;
+  float *ox = nullptr, *oy = nullptr, *oz = nullptr;
+  float *px = nullptr, *py = nullptr, *pz = nullptr;
+  uint64_t* slot = nullptr;
+  Part32View view() const { return Part32View{cell, ox, oy, oz, px, py, pz, slot}; }
+};
+
+enum Phase { PH_PUSH = 0, PH_YEE, PH_SORT, PH_WINDOW, PH_IONIZE, PH_OTHER, PH_N };
+
+struct Counters {
+  unsigned long long removed;
+  unsigned int err;
+  unsigned int pad;
+  double fmax;
+};
+
+}  // namespace
+
+struct agpu_handle {
+  agpu_params p;
+  Geo g;
+  int ndv = 0;
+  int device = 0;
+  int sms = 148;
+  cudaStream_t st = nullptr;
+  bool fp32 = false;
+  // FP64 form
+  double* ebf = nullptr;
+  double* jc = nullptr;
+  double* part[4] = {nullptr, nullptr, nullptr, nullptr};
+  double* tmp = nullptr;  // compaction target, cap_max * ndv
+  // FP32 split form
+  float* ebf32 = nullptr;
+  float* jhi = nullptr;
+  float* jlo = nullptr;
+  Species32 sp[4];
+  Species32 sptmp;
+  long long np[4] = {0, 0, 0, 0};
+  long long cap[4] = {0, 0, 0, 0};
+  long long capmax = 0;
+  // shared scratch
+  int* flag = nullptr;       // per particle (max capacity)
+  double* ef2 = nullptr;     // per ion |E|^2
+  Counters* d_cnt = nullptr;
+  Counters* h_cnt = nullptr;
+  Scratch scr{};
+  double* d_diag = nullptr;  // diagnostics accumulators
+  // window state (lp_window_xshift saved variables)
+  double xlapse = 0.0;
+  int wi1 = 0;
+  // plasma sources
+  agpu_plasma src[4];
+  bool has_src[4] = {false, false, false, false};
+  long long nptx[4] = {0, 0, 0, 0}, sptx_max[4] = {0, 0, 0, 0};
+  int npty[4] = {0, 0, 0, 0}, nptz[4] = {0, 0, 0, 0};
+  // ionization
+  double* d_wtab[4] = {nullptr, nullptr, nullptr, nullptr};
+  int zmax[4] = {0, 0, 0, 0};
+  double de_inv[4] = {0, 0, 0, 0};
+  double lp_max[4] = {0, 0, 0, 0};
+  int at_num[4] = {0, 0, 0, 0}, ion_min[4] = {0, 0, 0, 0}, model[4] = {0, 0, 0, 0};
+  bool auto_table[4] = {false, false, false, false};
+  int nsp_ionz = 1;
+  // flags
+  bool fields_set = false;
+  bool deterministic = false;
+  bool profiling = false;
+  int sort_interval = 0;
+  uint32_t error_bits = 0;
+  cudaEvent_t ev[2 * PH_N] = {};
+  agpu_timers timers{};
+};
+
+namespace {
+
+#define CK(call)                                                  \
+  do {                                                            \
+    cudaError_t e_ = (call);                                      \
+    if (e_ != cudaSuccess) {                                      \
+      std::fprintf(stderr, "aladyn_gpu: %s -> %s\n", #call, cudaGetErrorString(e_)); \
+      return AGPU_E_CUDA;                                         \
+    }                                                             \
+  } while (0)
+
+int dmalloc(void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return AGPU_E_NOMEM;
+  }
+  return 0;
+}
+
+YeeC yee_coef(const agpu_params& p) {
+  YeeC c;
+  c.dx_inv = p.dx_inv;
+  c.dy_inv = p.dy_inv;
+  c.dz_inv = p.dz_inv;
+  c.dt = p.dt;
+  c.se1 = p.se_coeff[0];
+  c.se2 = p.se_coeff[1];
+  c.ompe = p.ompe;
+  c.djc1 = p.djc[0];
+  c.djc2 = p.djc[1];
+  c.djc3 = p.djc[2];
+  return c;
+}
+
+void ph_begin(agpu_handle* h, int ph) {
+  if (h->profiling) cudaEventRecord(h->ev[2 * ph], h->st);
+}
+void ph_end(agpu_handle* h, int ph) {
+  if (!h->profiling) return;
+  cudaEventRecord(h->ev[2 * ph + 1], h->st);
+  cudaEventSynchronize(h->ev[2 * ph + 1]);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev[2 * ph], h->ev[2 * ph + 1]);
+  double* slots[PH_N] = {&h->timers.ms_push_deposit, &h->timers.ms_yee, &h->timers.ms_sort,
+                         &h->timers.ms_window, &h->timers.ms_ionize, &h->timers.ms_other};
+  *slots[ph] += ms;
+}
+
+int check_ptr(const void* p) { return p ? 0 : AGPU_E_ARG; }
+
+int free_all(agpu_handle* h) {
+  cudaFree(h->ebf);
+  cudaFree(h->jc);
+  for (int i = 0; i < 4; ++i) cudaFree(h->part[i]);
+  cudaFree(h->tmp);
+  cudaFree(h->ebf32);
+  cudaFree(h->jhi);
+  cudaFree(h->jlo);
+  auto freesp = [](Species32& s) {
+    cudaFree(s.cell);
+    cudaFree(s.ox);
+    cudaFree(s.oy);
+    cudaFree(s.oz);
+    cudaFree(s.px);
+    cudaFree(s.py);
+    cudaFree(s.pz);
+    cudaFree(s.slot);
+    s = Species32();
+  };
+  for (int i = 0; i < 4; ++i) freesp(h->sp[i]);
+  freesp(h->sptmp);
+  cudaFree(h->flag);
+  cudaFree(h->ef2);
+  cudaFree(h->d_cnt);
+  cudaFreeHost(h->h_cnt);
+  cudaFree(h->scr.blockcnt);
+  cudaFree(h->scr.total);
+  cudaFreeHost(h->scr.h_total);
+  cudaFree(h->d_diag);
+  for (int i = 0; i < 4; ++i) cudaFree(h->d_wtab[i]);
+  for (int i = 0; i < 2 * PH_N; ++i)
+    if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+  if (h->st) cudaStreamDestroy(h->st);
+  return 0;
+}
+
+int alloc_species32(Species32& s, long long cap, int ndim) {
+  int rc = 0;
+  rc |= dmalloc((void**)&s.cell, sizeof(int) * cap);
+  rc |= dmalloc((void**)&s.ox, sizeof(float) * cap);
+  rc |= dmalloc((void**)&s.oy, sizeof(float) * cap);
+  rc |= dmalloc((void**)&s.px, sizeof(float) * cap);
+  rc |= dmalloc((void**)&s.py, sizeof(float) * cap);
+  if (ndim == 3) {
+    rc |= dmalloc((void**)&s.oz, sizeof(float) * cap);
+    rc |= dmalloc((void**)&s.pz, sizeof(float) * cap);
+  }
+  rc |= dmalloc((void**)&s.slot, sizeof(uint64_t) * cap);
+  return rc ? AGPU_E_NOMEM : 0;
+}
+
+// Particle-count sync point: removed count and the sticky error word.
+int read_counters(agpu_handle* h) {
+  CK(cudaMemcpyAsync(h->h_cnt, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->error_bits |= h->h_cnt->err;
+  return 0;
+}
+
+long long lattice_columns_end(const agpu_handle* h, int ic, long long i1, double xmx, bool reference_quirk) {
+  // particles_inject (src/dynamics/window.f90:124-136): first column with
+  // xpt > xmx ends the block; when that column is sptx_max itself, the
+  // reference keeps it.
+  const agpu_plasma& s = h->src[ic];
+  double dxl = h->p.dx / (double)s.npx;
+  long long smax = h->sptx_max[ic];
+  long long ix;
+  if (i1 > smax) return i1 - 1;
+  for (ix = i1; ix <= smax; ++ix)
+    if (s.x_start + ((double)ix - 0.5) * dxl > xmx) break;
+  long long i2 = ix - 1;
+  if (reference_quirk && ix == smax) i2 = ix;
+  return i2;
+}
+
+int add_lattice_columns(agpu_handle* h, int ic, long long i1, long long i2) {
+  long long n = (i2 - i1 + 1) * (long long)h->npty[ic] * h->nptz[ic];
+  if (n <= 0) return 0;
+  if (h->np[ic] + n > h->cap[ic]) {
+    h->error_bits |= AGPU_EBIT_CAPACITY;
+    return AGPU_E_CAPACITY;
+  }
+  const agpu_plasma& s = h->src[ic];
+  LatticeArgs a;
+  a.ndim = h->p.ndim;
+  a.ic = ic;
+  a.npty = h->npty[ic];
+  a.nptz = h->nptz[ic];
+  a.i1 = i1;
+  a.i2 = i2;
+  a.charge = s.charge;
+  a.part_ind = s.part_ind;
+  a.wgh = s.wgh;
+  a.x_start = s.x_start;
+  a.y_min = s.y_min;
+  a.z_min = s.z_min;
+  a.dxl = h->p.dx / (double)s.npx;
+  a.dyl = h->p.dy / (double)s.npy;
+  a.dzl = h->p.dz / (double)s.npz;
+  a.jitter = s.jitter;
+  a.seed = s.seed;
+  if (h->fp32)
+    lattice32(a, h->sp[ic].view(), h->np[ic], h->g, h->p.xmn, h->p.ymn, h->p.zmn, h->p.dx_inv, h->p.dy_inv, h->p.dz_inv, h->st,
+              h->sms);
+  else
+    lattice64(a, h->part[ic], h->cap[ic], h->np[ic], h->st, h->sms);
+  CK(cudaGetLastError());
+  h->np[ic] += n;
+  return 0;
+}
+
+// Stable removal of the particles of species ic outside the box; x only when
+// window is set (cell_part_dist(.true.)), else x, y and z.
+int compact_species(agpu_handle* h, int ic, bool window) {
+  if (h->np[ic] <= 0) return 0;
+  long long kept;
+  if (h->fp32) {
+    int nx = h->p.nx, ny = h->p.ny, nz = h->p.nz;
+    kept = compact32(h->sp[ic].view(), h->sptmp.view(), h->np[ic], h->g.n1p, h->g.n2p, nx, ny, nz, window ? 0 : 1,
+                     (!window && h->p.ndim == 3) ? 1 : 0, h->scr, h->st);
+    std::swap(h->sp[ic], h->sptmp);
+  } else {
+    BoxBounds b{h->p.gxmin, h->p.gxmax, h->p.gymin, h->p.gymax, h->p.gzmin, h->p.gzmax, window ? 0 : 1,
+                (!window && h->p.ndim == 3) ? 1 : 0};
+    kept = compact64(h->part[ic], h->tmp, h->cap[ic], h->np[ic], h->ndv, b, h->scr, h->st);
+    // tmp has leading dimension cap[ic]; capacities are equal-size slots
+    std::swap(h->part[ic], h->tmp);
+  }
+  CK(cudaGetLastError());
+  h->np[ic] = kept;
+  return 0;
+}
+
+// Window shift of split positions: node index i -= nshx; a particle pushed
+// past node 1 is parked on node 1 with offset -0.5 (x_loc < 0), so the
+// compaction that follows removes it instead of wrapping into another row.
+__global__ void k_shift_cells(int* cell, float* ox, long long n, int nshx, int n1p) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int c = cell[q];
+    int i = c % n1p + 1;
+    int rest = c - (i - 1);
+    i -= nshx;
+    if (i < 1) {
+      i = 1;
+      ox[q] = -0.5f;
+    }
+    cell[q] = rest + (i - 1);
+  }
+}
+
+// lp_window_xshift (src/dynamics/window.f90:276-347).
+int window_xshift(agpu_handle* h, int witr, int init_iter, agpu_step_out* out) {
+  agpu_params& p = h->p;
+  if (init_iter == 0) {
+    h->xlapse = 0.0;
+    h->wi1 = 0;
+    return 0;
+  }
+  double dt_step = p.dt;
+  h->xlapse = h->xlapse + p.w_speed * dt_step * (double)witr;
+  int wi2 = (int)std::lround(p.dx_inv * h->xlapse);
+  int nshx = wi2 - h->wi1;
+  h->wi1 = wi2;
+  double sh = p.dx * (double)nshx;
+  p.xmax = p.xmax + sh;
+  p.gxmin = p.gxmin + sh;
+  p.gxmax = p.gxmax + sh;
+  p.xmn = p.xmn + sh;
+  out->nshx = nshx;
+  wi2 = h->g.ix2 - nshx;
+  if (wi2 <= 0) return AGPU_E_WINDOW;
+  if (nshx != 0) {
+    if (h->fp32)
+      xshift32(h->ebf32, h->g, h->g.nf, wi2, nshx, h->st, h->sms);
+    else
+      xshift64(h->ebf, h->g, h->g.nf, wi2, nshx, h->st, h->sms);
+    CK(cudaGetLastError());
+  }
+  for (int ic = 0; ic < p.nsp; ++ic) {
+    if (h->np[ic] <= 0) continue;
+    if (h->fp32 && nshx != 0) {
+      k_shift_cells<<<grid_for(h->np[ic], 256, h->sms, 16), 256, 0, h->st>>>(h->sp[ic].cell, h->sp[ic].ox, h->np[ic], nshx,
+                                                                               h->g.n1p);
+      CK(cudaGetLastError());
+    }
+    long long before = h->np[ic];
+    int rc = compact_species(h, ic, true);
+    if (rc) return rc;
+    out->removed[ic] += before - h->np[ic];
+  }
+  for (int ic = 0; ic < p.nsp; ++ic) {
+    if (!h->has_src[ic]) continue;
+    const agpu_plasma& s = h->src[ic];
+    if (s.x_start <= p.xmax && s.x_end > p.xmax) {
+      long long i1 = 1 + h->nptx[ic];
+      long long i2 = lattice_columns_end(h, ic, i1, p.xmax, true);
+      h->nptx[ic] = i2;
+      if (i2 > i1) {
+        long long before = h->np[ic];
+        int rc = add_lattice_columns(h, ic, i1, i2);
+        if (rc) return rc;
+        out->injected[ic] += h->np[ic] - before;
+      }
+    }
+  }
+  return 0;
+}
+
+int upload_table(agpu_handle* h, int ic, const double* tab, int zmax) {
+  size_t bytes = sizeof(double) * (size_t)(kNge + 2) * (zmax + 1);
+  if (!h->d_wtab[ic] || h->zmax[ic] != zmax) {
+    cudaFree(h->d_wtab[ic]);
+    h->d_wtab[ic] = nullptr;
+    if (dmalloc((void**)&h->d_wtab[ic], bytes)) return AGPU_E_NOMEM;
+  }
+  h->zmax[ic] = zmax;
+  CK(cudaMemcpy(h->d_wtab[ic], tab, bytes, cudaMemcpyHostToDevice));
+  if (ic + 1 > h->nsp_ionz) h->nsp_ionz = ic + 1;
+  return 0;
+}
+
+// Ionization of the FP64 form (pic_evolve_in_time.f90:44-68).
+int ionize64(agpu_handle* h, int iter, agpu_step_out* out) {
+  for (int ic = 1; ic < h->nsp_ionz && ic < h->p.nsp; ++ic) {
+    long long np = h->np[ic];
+    if (np <= 0 || !h->d_wtab[ic]) continue;
+    IonArgs64 a;
+    a.g = h->g;
+    a.ebf = h->ebf;
+    a.x = h->part[ic];
+    a.y = h->part[ic] + h->cap[ic];
+    a.z = h->part[ic] + 2 * h->cap[ic];
+    a.slot = h->part[ic] + (size_t)(h->ndv - 1) * h->cap[ic];
+    a.ef2 = h->ef2;
+    a.flag = h->flag;
+    a.np = np;
+    a.xmn = h->p.xmn;
+    a.ymn = h->p.ymn;
+    a.zmn = h->p.zmn;
+    a.dx_inv = h->p.dx_inv;
+    a.dy_inv = h->p.dy_inv;
+    a.dz_inv = h->p.dz_inv;
+    a.wtab = h->d_wtab[ic];
+    a.n_ge = kNge;
+    a.zmax = h->zmax[ic];
+    a.iter = iter;
+    a.ic = ic;
+    a.de_inv = h->de_inv[ic];
+    a.seed = h->p.seed;
+    a.err = &h->d_cnt->err;
+    int grid = grid_for(np, 256, h->sms, 8);
+    k64_ion_efield<<<grid, 256, 0, h->st>>>(a);
+    CK(cudaGetLastError());
+    if (iter % 100 == 0) {
+      max_nonneg(h->ef2, np, &h->d_cnt->fmax, h->st, h->sms);
+      CK(cudaGetLastError());
+      if (int rc_ = read_counters(h)) return rc_;
+      double m = std::sqrt(h->h_cnt->fmax);
+      out->ion_field_max = m;
+      if (h->auto_table[ic] && m > h->lp_max[ic]) {
+        h->lp_max[ic] = 1.1 * m;
+        std::vector<double> tab((size_t)(kNge + 2) * (h->at_num[ic] + 1));
+        double dinv = 0.0;
+        if (build_ionization_table(h->at_num[ic], h->ion_min[ic], h->model[ic], h->lp_max[ic], h->p.dt, tab.data(), &dinv))
+          return AGPU_E_ARG;
+        h->de_inv[ic] = dinv;
+        a.de_inv = dinv;
+        int rc = upload_table(h, ic, tab.data(), h->at_num[ic]);
+        if (rc) return rc;
+      }
+    }
+    k64_ionize<<<grid, 256, 0, h->st>>>(a);
+    CK(cudaGetLastError());
+    long long ne0 = h->np[0];
+    long long added = append_electrons64(h->flag, np, h->part[ic], h->cap[ic], h->part[0], h->cap[0], ne0, h->cap[0],
+                                         h->p.ndim, h->p.n_mol_atoms[ic], &h->d_cnt->err, h->scr, h->st);
+    CK(cudaGetLastError());
+    if (ne0 + added > h->cap[0]) {
+      h->error_bits |= AGPU_EBIT_CAPACITY;
+      added = h->cap[0] - ne0;
+    }
+    h->np[0] = ne0 + added;
+    out->new_electrons += added;
+  }
+  return 0;
+}
+
+}  // namespace
+
+// ============================================================================
+// C-ABI
+// ============================================================================
+extern "C" {
+
+const char* agpu_error_string(int code) {
+  switch (code) {
+    case AGPU_OK: return "ok";
+    case AGPU_E_WINDOW: return "window shift larger than the box (ier = 2)";
+    case AGPU_E_COUNT: return "particle count mismatch (ier = 99)";
+    case AGPU_E_ARG: return "invalid argument or unsupported configuration";
+    case AGPU_E_CUDA: return "CUDA runtime error";
+    case AGPU_E_NOMEM: return "device allocation failed";
+    case AGPU_E_CAPACITY: return "species capacity exceeded";
+    case AGPU_E_INDEX: return "particle stencil outside the field array";
+    case AGPU_E_IONZ_INDEX: return "ionization table index beyond n_ge+1";
+    case AGPU_E_NONFINITE: return "non-finite particle momentum";
+    case AGPU_E_NODEVICE: return "no usable CUDA device";
+    case AGPU_E_STATE: return "call out of order";
+    default: return "unknown status";
+  }
+}
+
+int agpu_device_count(int* n) {
+  if (!n) return AGPU_E_ARG;
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount(&c);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *n = 0;
+    return AGPU_E_NODEVICE;
+  }
+  *n = c;
+  return 0;
+}
+
+int agpu_struct_sizes(int64_t* sizes, int32_t n) {
+  if (!sizes) return AGPU_E_ARG;
+  int64_t s[6] = {(int64_t)sizeof(agpu_params), (int64_t)sizeof(agpu_plasma), (int64_t)sizeof(agpu_laser),
+                  (int64_t)sizeof(agpu_step_out), (int64_t)sizeof(agpu_diag_out), (int64_t)sizeof(agpu_timers)};
+  for (int i = 0; i < n && i < 6; ++i) sizes[i] = s[i];
+  return 0;
+}
+
+int agpu_create(const agpu_params* params, agpu_handle** out) {
+  if (!params || !out) return AGPU_E_ARG;
+  *out = nullptr;
+  const agpu_params& p = *params;
+  if (!(p.ndim == 2 || p.ndim == 3)) return AGPU_E_ARG;
+  if (p.nx < 4 || p.ny < 4 || (p.ndim == 3 && p.nz < 4)) return AGPU_E_ARG;
+  if (p.nfield != (p.ndim == 3 ? 6 : 3) || p.curr_ndim != (p.ndim == 3 ? 3 : 2)) return AGPU_E_ARG;
+  if (p.ibx != 0 || p.iby != 0 || p.ibz != 0 || p.iform < 0 || p.iform > 1) return AGPU_E_ARG;
+  if (p.nsp < 1 || p.nsp > 4 || p.nsp_run < 1 || p.nsp_run > p.nsp) return AGPU_E_ARG;
+  if (p.precision != AGPU_FP64 && p.precision != AGPU_FP32_SPLIT) return AGPU_E_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    cudaGetLastError();
+    return AGPU_E_NODEVICE;
+  }
+  agpu_handle* h = new (std::nothrow) agpu_handle();
+  if (!h) return AGPU_E_NOMEM;
+  h->p = p;
+  cudaGetDevice(&h->device);
+  cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
+  h->fp32 = (p.precision == AGPU_FP32_SPLIT);
+  Geo& g = h->g;
+  g.ndim = p.ndim;
+  g.n1p = p.nx + 5;
+  g.n2p = p.ny + 5;
+  g.n3p = (p.ndim == 3) ? p.nz + 5 : 1;
+  g.ix1 = 3;
+  g.ix2 = p.nx + 2;
+  g.jy1 = 3;
+  g.jy2 = p.ny + 2;
+  g.kz1 = (p.ndim == 3) ? 3 : 1;
+  g.kz2 = (p.ndim == 3) ? p.nz + 2 : 1;
+  g.nf = p.nfield;
+  g.nc = p.curr_ndim;
+  g.ncell = (long long)g.n1p * g.n2p * g.n3p;
+  if (h->fp32 && g.ncell >= (1ll << 31)) {
+    delete h;
+    return AGPU_E_ARG;
+  }
+  h->ndv = (p.ndim == 3) ? 7 : 5;
+  int rc = 0;
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) rc = AGPU_E_CUDA;
+  for (int i = 0; i < 2 * PH_N && !rc; ++i)
+    if (cudaEventCreate(&h->ev[i]) != cudaSuccess) rc = AGPU_E_CUDA;
+  long long capmax = 16;
+  for (int ic = 0; ic < 4; ++ic) {
+    h->cap[ic] = (ic < p.nsp) ? std::max<long long>(p.capacity[ic], 16) : 0;
+    capmax = std::max(capmax, h->cap[ic]);
+  }
+  // equal-size slots so that a compaction target can take any species
+  for (int ic = 0; ic < p.nsp; ++ic) h->cap[ic] = capmax;
+  h->capmax = capmax;
+  if (!rc) {
+    if (!h->fp32) {
+      rc |= dmalloc((void**)&h->ebf, sizeof(double) * g.ncell * g.nf);
+      rc |= dmalloc((void**)&h->jc, sizeof(double) * g.ncell * g.nc);
+      for (int ic = 0; ic < p.nsp && !rc; ++ic) rc |= dmalloc((void**)&h->part[ic], sizeof(double) * capmax * h->ndv);
+      if (!rc) rc |= dmalloc((void**)&h->tmp, sizeof(double) * capmax * h->ndv);
+    } else {
+      rc |= dmalloc((void**)&h->ebf32, sizeof(float) * g.ncell * g.nf);
+      rc |= dmalloc((void**)&h->jhi, sizeof(float) * g.ncell * g.nc);
+      rc |= dmalloc((void**)&h->jlo, sizeof(float) * g.ncell * g.nc);
+      for (int ic = 0; ic < p.nsp && !rc; ++ic) rc |= alloc_species32(h->sp[ic], capmax, p.ndim);
+      if (!rc) rc |= alloc_species32(h->sptmp, capmax, p.ndim);
+    }
+  }
+  if (!rc) {
+    rc |= dmalloc((void**)&h->flag, sizeof(int) * capmax);
+    if (p.ionz_lev > 0) rc |= dmalloc((void**)&h->ef2, sizeof(double) * capmax);
+    rc |= dmalloc((void**)&h->d_cnt, sizeof(Counters));
+    long long nb = (capmax + SEL_CHUNK - 1) / SEL_CHUNK + 1;
+    rc |= dmalloc((void**)&h->scr.blockcnt, sizeof(long long) * nb);
+    rc |= dmalloc((void**)&h->scr.total, sizeof(long long));
+    rc |= dmalloc((void**)&h->d_diag, sizeof(double) * 64);
+    if (cudaMallocHost((void**)&h->h_cnt, sizeof(Counters)) != cudaSuccess) rc |= AGPU_E_NOMEM;
+    if (cudaMallocHost((void**)&h->scr.h_total, sizeof(long long)) != cudaSuccess) rc |= AGPU_E_NOMEM;
+  }
+  if (!rc) {
+    if (h->ebf) cudaMemsetAsync(h->ebf, 0, sizeof(double) * g.ncell * g.nf, h->st);
+    if (h->jc) cudaMemsetAsync(h->jc, 0, sizeof(double) * g.ncell * g.nc, h->st);
+    if (h->ebf32) cudaMemsetAsync(h->ebf32, 0, sizeof(float) * g.ncell * g.nf, h->st);
+    if (h->jhi) cudaMemsetAsync(h->jhi, 0, sizeof(float) * g.ncell * g.nc, h->st);
+    if (h->jlo) cudaMemsetAsync(h->jlo, 0, sizeof(float) * g.ncell * g.nc, h->st);
+    cudaMemsetAsync(h->d_cnt, 0, sizeof(Counters), h->st);
+    if (cudaStreamSynchronize(h->st) != cudaSuccess) rc = AGPU_E_CUDA;
+  }
+  if (rc) {
+    free_all(h);
+    delete h;
+    return rc & AGPU_E_NOMEM ? AGPU_E_NOMEM : AGPU_E_CUDA;
+  }
+  *out = h;
+  return 0;
+}
+
+int agpu_destroy(agpu_handle* h) {
+  if (!h) return AGPU_E_ARG;
+  cudaStreamSynchronize(h->st);
+  free_all(h);
+  delete h;
+  return 0;
+}
+
+int agpu_set_fields(agpu_handle* h, const double* ebf, int32_t n1p, int32_t n2p, int32_t n3p, int32_t nc) {
+  if (!h || !ebf) return AGPU_E_ARG;
+  const Geo& g = h->g;
+  if (n1p != g.n1p || n2p != g.n2p || n3p != g.n3p || nc != g.nf) return AGPU_E_ARG;
+  size_t n = (size_t)g.ncell * g.nf;
+  if (!h->fp32) {
+    CK(cudaMemcpyAsync(h->ebf, ebf, sizeof(double) * n, cudaMemcpyHostToDevice, h->st));
+  } else {
+    double* stage = nullptr;
+    if (dmalloc((void**)&stage, sizeof(double) * n)) return AGPU_E_NOMEM;
+    cudaMemcpyAsync(stage, ebf, sizeof(double) * n, cudaMemcpyHostToDevice, h->st);
+    f64_to_f32(stage, h->ebf32, (long long)n, h->st, h->sms);
+    cudaStreamSynchronize(h->st);
+    cudaFree(stage);
+  }
+  CK(cudaStreamSynchronize(h->st));
+  h->fields_set = true;
+  return 0;
+}
+
+int agpu_get_fields(agpu_handle* h, double* ebf, int32_t n1p, int32_t n2p, int32_t n3p, int32_t nc) {
+  if (!h || !ebf) return AGPU_E_ARG;
+  const Geo& g = h->g;
+  if (n1p != g.n1p || n2p != g.n2p || n3p != g.n3p || nc != g.nf) return AGPU_E_ARG;
+  size_t n = (size_t)g.ncell * g.nf;
+  if (!h->fp32) {
+    CK(cudaMemcpyAsync(ebf, h->ebf, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
+  } else {
+    double* stage = nullptr;
+    if (dmalloc((void**)&stage, sizeof(double) * n)) return AGPU_E_NOMEM;
+    f32_to_f64(h->ebf32, stage, (long long)n, h->st, h->sms);
+    cudaMemcpyAsync(ebf, stage, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st);
+    cudaStreamSynchronize(h->st);
+    cudaFree(stage);
+  }
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+int agpu_get_currents(agpu_handle* h, double* jc, int32_t n1p, int32_t n2p, int32_t n3p, int32_t nc) {
+  if (!h || !jc) return AGPU_E_ARG;
+  const Geo& g = h->g;
+  if (n1p != g.n1p || n2p != g.n2p || n3p != g.n3p || nc != g.nc) return AGPU_E_ARG;
+  size_t n = (size_t)g.ncell * g.nc;
+  if (!h->fp32) {
+    CK(cudaMemcpyAsync(jc, h->jc, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
+  } else {
+    double* stage = nullptr;
+    if (dmalloc((void**)&stage, sizeof(double) * n)) return AGPU_E_NOMEM;
+    f32pair_to_f64(h->jhi, h->jlo, stage, (long long)n, h->st, h->sms);
+    cudaMemcpyAsync(jc, stage, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st);
+    cudaStreamSynchronize(h->st);
+    cudaFree(stage);
+  }
+  CK(cudaStreamSynchronize(h->st));
+  // curr = djc(i) * curr (curr_and_fields_util.f90:111-115), whole array
+  if (h->p.iform < 2)
+    for (int i = 0; i < h->p.ndim; ++i) {
+      double d = h->p.djc[i];
+      double* c = jc + (size_t)g.ncell * i;
+      for (size_t q = 0; q < (size_t)g.ncell; ++q) c[q] = d * c[q];
+    }
+  return 0;
+}
+
+int agpu_set_species(agpu_handle* h, int32_t ic, const double* part, int64_t ld, int64_t np, int32_t ndv) {
+  if (!h || ic < 0 || ic >= h->p.nsp || ndv != h->ndv || np < 0 || (np > 0 && (!part || ld < np))) return AGPU_E_ARG;
+  if (np > h->cap[ic]) return AGPU_E_CAPACITY;
+  if (!h->fp32) {
+    if (np > 0)
+      CK(cudaMemcpy2DAsync(h->part[ic], sizeof(double) * h->cap[ic], part, sizeof(double) * ld, sizeof(double) * np, ndv,
+                           cudaMemcpyHostToDevice, h->st));
+  } else if (np > 0) {
+    double* stage = nullptr;
+    if (dmalloc((void**)&stage, sizeof(double) * np * ndv)) return AGPU_E_NOMEM;
+    cudaMemcpy2DAsync(stage, sizeof(double) * np, part, sizeof(double) * ld, sizeof(double) * np, ndv, cudaMemcpyHostToDevice,
+                      h->st);
+    rec_to_split(stage, np, np, h->sp[ic].view(), 0, h->g, h->p.xmn, h->p.ymn, h->p.zmn, h->p.dx_inv, h->p.dy_inv, h->p.dz_inv,
+                 h->st, h->sms);
+    cudaStreamSynchronize(h->st);
+    cudaFree(stage);
+  }
+  CK(cudaStreamSynchronize(h->st));
+  h->np[ic] = np;
+  return 0;
+}
+
+int agpu_get_species(agpu_handle* h, int32_t ic, double* part, int64_t ld, int64_t* np, int32_t ndv) {
+  if (!h || ic < 0 || ic >= h->p.nsp || !np) return AGPU_E_ARG;
+  *np = h->np[ic];
+  if (!part) return 0;
+  if (ndv != h->ndv || ld < h->np[ic]) return AGPU_E_ARG;
+  long long n = h->np[ic];
+  if (n == 0) return 0;
+  if (!h->fp32) {
+    CK(cudaMemcpy2DAsync(part, sizeof(double) * ld, h->part[ic], sizeof(double) * h->cap[ic], sizeof(double) * n, ndv,
+                         cudaMemcpyDeviceToHost, h->st));
+  } else {
+    double* stage = nullptr;
+    if (dmalloc((void**)&stage, sizeof(double) * n * ndv)) return AGPU_E_NOMEM;
+    split_to_rec(h->sp[ic].view(), n, stage, n, h->g, h->p.xmn, h->p.ymn, h->p.zmn, h->p.dx, h->p.dy, h->p.dz, h->st, h->sms);
+    cudaMemcpy2DAsync(part, sizeof(double) * ld, stage, sizeof(double) * n, sizeof(double) * n, ndv, cudaMemcpyDeviceToHost,
+                      h->st);
+    cudaStreamSynchronize(h->st);
+    cudaFree(stage);
+  }
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+int agpu_get_count(agpu_handle* h, int32_t ic, int64_t* np) {
+  if (!h || !np || ic < 0 || ic >= h->p.nsp) return AGPU_E_ARG;
+  *np = h->np[ic];
+  return 0;
+}
+
+int agpu_set_plasma_source(agpu_handle* h, const agpu_plasma* src) {
+  if (!h || !src) return AGPU_E_ARG;
+  int ic = src->ic;
+  if (ic < 0 || ic >= h->p.nsp || src->npx < 1 || src->npy < 1 || src->npz < 1) return AGPU_E_ARG;
+  if (!(src->jitter >= 0.0 && src->jitter < 1.0)) return AGPU_E_ARG;
+  h->src[ic] = *src;
+  h->has_src[ic] = true;
+  h->nptx[ic] = 0;
+  double dxl = h->p.dx / (double)src->npx;
+  double dyl = h->p.dy / (double)src->npy;
+  double dzl = h->p.dz / (double)src->npz;
+  h->sptx_max[ic] = (long long)std::floor((src->x_end - src->x_start) / dxl + 1e-9);
+  h->npty[ic] = (int)std::floor((src->y_max - src->y_min) / dyl + 1e-9);
+  h->nptz[ic] = (h->p.ndim == 3) ? (int)std::floor((src->z_max - src->z_min) / dzl + 1e-9) : 1;
+  return 0;
+}
+
+int agpu_load_plasma(agpu_handle* h, int32_t ic) {
+  if (!h || ic < 0 || ic >= h->p.nsp) return AGPU_E_ARG;
+  if (!h->has_src[ic]) return AGPU_E_STATE;
+  h->nptx[ic] = 0;
+  long long i2 = lattice_columns_end(h, ic, 1, h->p.xmax, false);
+  h->nptx[ic] = i2;
+  int rc = 0;
+  if (i2 >= 1) rc = add_lattice_columns(h, ic, 1, i2);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+int agpu_init_laser(agpu_handle* h, const agpu_laser* l) {
+  if (!h || !l) return AGPU_E_ARG;
+  const double pi = 3.141592653589793;
+  LaserArgs a;
+  a.ndim = h->p.ndim;
+  double oml = 2.0 * pi / l->lam0;
+  a.amp = l->a0 * oml;
+  a.k0 = oml;
+  a.w0 = l->w0_y;
+  a.zr = pi * l->w0_y * l->w0_y / l->lam0;
+  a.w0x = l->tau_fwhm / std::sqrt(2.0 * std::log(2.0));
+  a.xc = l->xc;
+  a.xf = l->xf;
+  a.y0 = l->y0;
+  a.z0 = l->z0;
+  a.xmn = h->p.xmn;
+  a.ymn = h->p.ymn;
+  a.zmn = h->p.zmn;
+  a.dx = h->p.dx;
+  a.dy = h->p.dy;
+  a.dz = h->p.dz;
+  size_t n = (size_t)h->g.ncell * h->g.nf;
+  if (!h->fp32) {
+    laser64(a, h->ebf, h->g, h->st, h->sms);
+  } else {
+    double* stage = nullptr;
+    if (dmalloc((void**)&stage, sizeof(double) * n)) return AGPU_E_NOMEM;
+    f32_to_f64(h->ebf32, stage, (long long)n, h->st, h->sms);
+    laser64(a, stage, h->g, h->st, h->sms);
+    f64_to_f32(stage, h->ebf32, (long long)n, h->st, h->sms);
+    cudaStreamSynchronize(h->st);
+    cudaFree(stage);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->st));
+  h->fields_set = true;
+  return 0;
+}
+
+int agpu_set_ionization_table(agpu_handle* h, int32_t ic, const double* w_one_lev, int32_t n_ge, int32_t zmax, double de_inv) {
+  if (!h || !w_one_lev || ic < 1 || ic >= h->p.nsp || n_ge != kNge || zmax < 1 || zmax > 100) return AGPU_E_ARG;
+  if (h->fp32) return AGPU_E_ARG;  // ionization runs in the FP64 form
+  h->de_inv[ic] = de_inv;
+  h->auto_table[ic] = false;
+  return upload_table(h, ic, w_one_lev, zmax);
+}
+
+int agpu_set_ionization_species(agpu_handle* h, int32_t ic, int32_t atomic_number, int32_t ion_min, int32_t ion_max,
+                                int32_t ionz_model, double lp_max) {
+  if (!h || ic < 1 || ic >= h->p.nsp || ion_min < 0 || ion_max > atomic_number || ion_min >= ion_max) return AGPU_E_ARG;
+  if (h->fp32) return AGPU_E_ARG;
+  std::vector<double> tab((size_t)(kNge + 2) * (atomic_number + 1));
+  double dinv = 0.0;
+  if (build_ionization_table(atomic_number, ion_min, ionz_model, lp_max, h->p.dt, tab.data(), &dinv)) return AGPU_E_ARG;
+  h->at_num[ic] = atomic_number;
+  h->ion_min[ic] = ion_min;
+  h->model[ic] = ionz_model;
+  h->lp_max[ic] = lp_max;
+  h->de_inv[ic] = dinv;
+  h->auto_table[ic] = true;
+  return upload_table(h, ic, tab.data(), atomic_number);
+}
+
+int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu_step_out* out) {
+  if (!h) return AGPU_E_ARG;
+  agpu_step_out dummy;
+  if (!out) out = &dummy;
+  std::memset(out, 0, sizeof(*out));
+  out->ion_field_max = -1.0;
+  agpu_params& p = h->p;
+  int rc = 0;
+  CK(cudaMemsetAsync(h->d_cnt, 0, sizeof(Counters), h->st));
+  // pfields_prepare -> field_xyzbd
+  ph_begin(h, PH_YEE);
+  if (h->fp32) field_bd32(Dev32{h->g, h->ebf32, h->jhi, h->jlo}, h->st, h->sms);
+  else field_bd64(Dev64{h->g, h->ebf, h->jc}, h->st, h->sms);
+  CK(cudaGetLastError());
+  ph_end(h, PH_YEE);
+  // ionization
+  if (p.ionz_lev > 0 && !h->fp32) {
+    ph_begin(h, PH_IONIZE);
+    rc = ionize64(h, iter, out);
+    ph_end(h, PH_IONIZE);
+    if (rc) return rc;
+  }
+  // jc = 0, then each running species: gather/push/deposit
+  if (h->fp32) {
+    CK(cudaMemsetAsync(h->jhi, 0, sizeof(float) * h->g.ncell * h->g.nc, h->st));
+    CK(cudaMemsetAsync(h->jlo, 0, sizeof(float) * h->g.ncell * h->g.nc, h->st));
+  } else {
+    CK(cudaMemsetAsync(h->jc, 0, sizeof(double) * h->g.ncell * h->g.nc, h->st));
+  }
+  for (int ic = 0; ic < p.nsp_run; ++ic) {
+    long long np = h->np[ic];
+    if (np <= 0) continue;
+    CK(cudaMemsetAsync(&h->d_cnt->removed, 0, sizeof(unsigned long long), h->st));
+    ph_begin(h, PH_PUSH);
+    if (h->fp32) {
+      PushArgs32 a;
+      a.g = h->g;
+      a.ebf = h->ebf32;
+      a.jhi = h->jhi;
+      a.jlo = h->jlo;
+      const Species32& s = h->sp[ic];
+      a.p = Part32{s.cell, s.ox, s.oy, s.oz, s.px, s.py, s.pz, s.slot};
+      a.flag = h->flag;
+      a.np = np;
+      a.dt = (float)p.dt;
+      a.dth = (float)(0.5 * p.dt);
+      a.lfact = (float)p.lorentz_fact[ic];
+      a.dtx = (float)(p.dt * p.dx_inv);
+      a.dty = (float)(p.dt * p.dy_inv);
+      a.dtz = (float)(p.dt * p.dz_inv);
+      a.initial = initial_time ? 1 : 0;
+      a.removed = &h->d_cnt->removed;
+      a.err = &h->d_cnt->err;
+      push_deposit32(a, h->st, h->sms);
+    } else {
+      PushArgs64 a;
+      a.g = h->g;
+      a.ebf = h->ebf;
+      a.jc = h->jc;
+      double* b = h->part[ic];
+      long long cp = h->cap[ic];
+      a.x = b;
+      a.y = b + cp;
+      if (p.ndim == 3) {
+        a.z = b + 2 * cp;
+        a.px = b + 3 * cp;
+        a.py = b + 4 * cp;
+        a.pz = b + 5 * cp;
+        a.slot = b + 6 * cp;
+      } else {
+        a.z = nullptr;
+        a.px = b + 2 * cp;
+        a.py = b + 3 * cp;
+        a.pz = nullptr;
+        a.slot = b + 4 * cp;
+      }
+      a.flag = h->flag;
+      a.np = np;
+      a.xmn = p.xmn;
+      a.ymn = p.ymn;
+      a.zmn = p.zmn;
+      a.dx_inv = p.dx_inv;
+      a.dy_inv = p.dy_inv;
+      a.dz_inv = p.dz_inv;
+      a.dt = p.dt;
+      a.dth = 0.5 * p.dt;
+      a.lfact = p.lorentz_fact[ic];
+      a.gxmin = p.gxmin;
+      a.gxmax = p.gxmax;
+      a.gymin = p.gymin;
+      a.gymax = p.gymax;
+      a.gzmin = p.gzmin;
+      a.gzmax = p.gzmax;
+      a.initial = initial_time ? 1 : 0;
+      a.removed = &h->d_cnt->removed;
+      a.err = &h->d_cnt->err;
+      push_deposit64(a, h->st, h->sms, h->deterministic);
+    }
+    CK(cudaGetLastError());
+    ph_end(h, PH_PUSH);
+    h->timers.launches_push_deposit += 1;
+    h->timers.pushes += np;
+    if (int rc_ = read_counters(h)) return rc_;
+    if (h->h_cnt->removed > 0) {
+      ph_begin(h, PH_SORT);
+      long long before = h->np[ic];
+      rc = compact_species(h, ic, false);
+      ph_end(h, PH_SORT);
+      if (rc) return rc;
+      out->removed[ic] += before - h->np[ic];
+    }
+  }
+  // curr_mpi_collect -> jc_xyzbd (djc folded into the E update)
+  ph_begin(h, PH_YEE);
+  YeeC c = yee_coef(p);
+  if (h->fp32) {
+    Dev32 d{h->g, h->ebf32, h->jhi, h->jlo};
+    jfold32(d, h->st, h->sms);
+    yee32(d, c, h->st, h->sms);
+  } else {
+    Dev64 d{h->g, h->ebf, h->jc};
+    jfold64(d, h->st, h->sms);
+    yee64(d, c, h->st, h->sms);
+  }
+  CK(cudaGetLastError());
+  ph_end(h, PH_YEE);
+  h->timers.launches_yee += 1;
+  h->timers.yee_cells += (long long)p.nx * p.ny * (p.ndim == 3 ? p.nz : 1);
+  // lp_run: moving window
+  if (p.w_speed > 0.0 && p.w_sh > 0) {
+    if (t >= p.wi_time && t < p.wf_time) {
+      if (iter % p.w_sh == 0) {
+        ph_begin(h, PH_WINDOW);
+        rc = window_xshift(h, p.w_sh, iter, out);
+        ph_end(h, PH_WINDOW);
+        if (rc) return rc;
+      }
+    }
+  }
+  if (int rc_ = read_counters(h)) return rc_;
+  for (int ic = 0; ic < 4; ++ic) out->np[ic] = h->np[ic];
+  out->xmn = p.xmn;
+  out->error_bits = h->error_bits;
+  if (h->error_bits & AGPU_EBIT_CAPACITY) return AGPU_E_CAPACITY;
+  return 0;
+}
+
+int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t ld, int64_t n, int32_t ndv) {
+  if (!h || ic < 0 || ic >= h->p.nsp || ndv != h->ndv || n < 0 || (n > 0 && (!part || ld < n))) return AGPU_E_ARG;
+  if (h->np[ic] + n > h->cap[ic]) return AGPU_E_CAPACITY;
+  if (n == 0) return 0;
+  if (!h->fp32) {
+    CK(cudaMemcpy2DAsync(h->part[ic] + h->np[ic], sizeof(double) * h->cap[ic], part, sizeof(double) * ld, sizeof(double) * n,
+                         ndv, cudaMemcpyHostToDevice, h->st));
+  } else {
+    double* stage = nullptr;
+    if (dmalloc((void**)&stage, sizeof(double) * n * ndv)) return AGPU_E_NOMEM;
+    cudaMemcpy2DAsync(stage, sizeof(double) * n, part, sizeof(double) * ld, sizeof(double) * n, ndv, cudaMemcpyHostToDevice, h->st);
+    rec_to_split(stage, n, n, h->sp[ic].view(), h->np[ic], h->g, h->p.xmn, h->p.ymn, h->p.zmn, h->p.dx_inv, h->p.dy_inv,
+                 h->p.dz_inv, h->st, h->sms);
+    cudaStreamSynchronize(h->st);
+    cudaFree(stage);
+  }
+  CK(cudaStreamSynchronize(h->st));
+  h->np[ic] += n;
+  return 0;
+}
+
+int agpu_diag(agpu_handle* h, agpu_diag_out* out) {
+  if (!h || !out) return AGPU_E_ARG;
+  std::memset(out, 0, sizeof(*out));
+  CK(cudaMemsetAsync(h->d_diag, 0, sizeof(double) * 64, h->st));
+  double dvol = h->p.dx * h->p.dy * (h->p.ndim == 3 ? h->p.dz : 1.0);
+  if (h->fp32)
+    field_diag32(h->ebf32, h->g, dvol, h->d_diag, h->d_diag + 6, h->st, h->sms);
+  else
+    field_diag64(h->ebf, h->g, dvol, h->d_diag, h->d_diag + 6, h->st, h->sms);
+  for (int ic = 0; ic < h->p.nsp; ++ic) {
+    double* o = h->d_diag + 8 + 5 * ic;
+    if (h->fp32)
+      part_diag32(h->sp[ic].view(), h->np[ic], h->p.ndim, o, h->st, h->sms);
+    else
+      part_diag64(h->part[ic], h->cap[ic], h->np[ic], h->p.ndim, o, h->st, h->sms);
+  }
+  CK(cudaGetLastError());
+  double hd[64];
+  CK(cudaMemcpyAsync(hd, h->d_diag, sizeof(hd), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  for (int c = 0; c < 6; ++c) out->field_energy[c] = hd[c];
+  out->max_abs_e = hd[6];
+  for (int ic = 0; ic < 4; ++ic) {
+    const double* o = hd + 8 + 5 * ic;
+    out->kin_energy[ic] = o[0];
+    out->charge[ic] = o[1];
+    for (int c = 0; c < 3; ++c) out->momentum[ic][c] = o[2 + c];
+    out->np[ic] = h->np[ic];
+  }
+  return 0;
+}
+
+int agpu_set_profiling(agpu_handle* h, int32_t on) {
+  if (!h) return AGPU_E_ARG;
+  h->profiling = on != 0;
+  return 0;
+}
+int agpu_get_timers(agpu_handle* h, agpu_timers* out) {
+  if (!h || !out) return AGPU_E_ARG;
+  *out = h->timers;
+  return 0;
+}
+int agpu_reset_timers(agpu_handle* h) {
+  if (!h) return AGPU_E_ARG;
+  std::memset(&h->timers, 0, sizeof(h->timers));
+  return 0;
+}
+int agpu_get_stream(agpu_handle* h, void** stream) {
+  if (!h || !stream) return AGPU_E_ARG;
+  *stream = (void*)h->st;
+  return 0;
+}
+int agpu_synchronize(agpu_handle* h) {
+  if (!h) return AGPU_E_ARG;
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+int agpu_set_sort_interval(agpu_handle* h, int32_t steps) {
+  if (!h || steps < 0) return AGPU_E_ARG;
+  h->sort_interval = steps;
+  return 0;
+}
+int agpu_set_deterministic(agpu_handle* h, int32_t on) {
+  if (!h) return AGPU_E_ARG;
+  h->deterministic = on != 0;
+  return 0;
+}
+
+}  // extern "C"

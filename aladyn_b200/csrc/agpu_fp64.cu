@@ -1,0 +1,614 @@
+// agpu_fp64.cu — the plain FP64 form of the PIC step on sm_100a.
+//
+// Compiled with -fmad=false: every expression keeps the reference's
+// statement order and rounding (no fused multiply-add), so cell indices,
+// momenta and positions reproduce the Fortran arithmetic bit for bit given
+// the same fields; the currents differ only by the order of the atomic sums
+// unless the deterministic (serial) deposit is selected.
+#include "agpu_common.cuh"
+#include "agpu_kernels.h"
+#include "agpu_yee.cuh"
+
+namespace agpu {
+
+void field_bd64(const Dev64& d, cudaStream_t st, int sms) { field_bd_t<double>(d.ebf, d.g, st, sms); }
+
+// ============================================================================
+// Shapes (src/particles/grid_part_lib.f90)
+// ============================================================================
+// qlh per dimension (110-143, 212-259): quadratic on integer nodes, linear on
+// half nodes, index shifted by -1.
+__device__ __forceinline__ int qlh64(double xp, double ax[3], double axh[2]) {
+  double xx = 3.0 + xp;
+  int i = (int)(xx + 0.5);
+  double sx = xx - (double)i;
+  double sx2 = sx * sx;
+  ax[1] = 0.75 - sx2;
+  ax[2] = 0.5 * (0.25 + sx2 + sx);
+  ax[0] = 1. - ax[1] - ax[2];
+  axh[1] = sx + 0.5;
+  axh[0] = 1. - axh[1];
+  return i - 1;
+}
+// qden per dimension (337-358, 388-417): no shift.
+__device__ __forceinline__ int qden64(double xp, double ax[3]) {
+  double xx = 3.0 + xp;
+  int i = (int)(xx + 0.5);
+  double sx = xx - (double)i;
+  double sx2 = sx * sx;
+  ax[1] = 0.75 - sx2;
+  ax[2] = 0.5 * (0.25 + sx2 + sx);
+  ax[0] = 1. - ax[1] - ax[2];
+  return i;
+}
+// qqh per dimension (170-210, 261-320).
+__device__ __forceinline__ void qqh64(double xp, double ax[3], double axh[3], int* ix, int* ihx) {
+  double xx = 3.0 + xp;
+  int i = (int)(xx + 0.5);
+  double sx = xx - (double)i;
+  double sx2 = sx * sx;
+  ax[1] = 0.75 - sx2;
+  ax[2] = 0.5 * (0.25 + sx2 + sx);
+  ax[0] = 1. - ax[1] - ax[2];
+  int ih = (int)(xx);
+  sx = xx - (double)ih - 0.5;
+  sx2 = sx * sx;
+  axh[1] = 0.75 - sx2;
+  axh[2] = 0.5 * (0.25 + sx2 + sx);
+  axh[0] = 1. - axh[1] - axh[2];
+  *ix = i - 1;
+  *ihx = ih - 1;
+}
+
+// ============================================================================
+// Esirkepov deposit of one move (grid_part_connect.f90:956-1334) with FP64
+// atomics (or plain adds when the caller serialises the particles).
+// ============================================================================
+template <bool SERIAL>
+__device__ __forceinline__ void jadd(double* p, double v) {
+  if (SERIAL)
+    *p = *p + v;
+  else
+    atomicAdd(p, v);
+}
+
+// 1-D Esirkepov "DS" shape: axh[0..4] holds the new shape shifted by ih,
+// curr[0..4] the cumulative differences (grid_part_connect.f90:1020-1030).
+__device__ __forceinline__ void esirk_1d(const double a0[3], const double a1[3], int ih, double axh[5], double curr[5]) {
+#pragma unroll
+  for (int q = 0; q < 5; ++q) axh[q] = 0.;
+  // ih in {0,1,2}: branch-free placement into registers
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    int m = q - ih;
+    axh[q] = (m == 0) ? a1[0] : (m == 1) ? a1[1] : (m == 2) ? a1[2] : 0.;
+  }
+  curr[0] = -axh[0];
+  curr[1] = curr[0] + a0[0] - axh[1];
+  curr[2] = curr[1] + a0[1] - axh[2];
+  curr[3] = curr[2] + a0[2] - axh[3];
+  curr[4] = curr[3] - axh[4];
+}
+
+template <bool SERIAL>
+__device__ __forceinline__ bool esirkepov2d(const Geo& g, double* jc, double xn, double yn, double xo, double yo,
+                                            float wght) {
+  double ax0[3], ay0[3], ax1[3], ay1[3], axh[5], ayh[5], currx[5], curry[5];
+  int ii0 = qden64(xo, ax0);
+  int jj0 = qden64(yo, ay0);
+  int i = qden64(xn, ax1);
+  int j = qden64(yn, ay1);
+  int ih = i - ii0 + 1;
+  // a move of more than one cell (dt beyond the CFL limit) has no slot
+  if ((unsigned)ih > 2u || (unsigned)(j - jj0 + 1) > 2u) return false;
+  esirk_1d(ax0, ax1, ih, axh, currx);
+  axh[1] = axh[1] + ax0[0];
+  axh[2] = axh[2] + ax0[1];
+  axh[3] = axh[3] + ax0[2];
+  double w = (double)wght;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) currx[q] = w * currx[q];
+  int x0 = ih < 1 ? ih : 1;
+  int x1 = (ih + 2) > 3 ? ih + 2 : 3;
+  int jh = j - jj0 + 1;
+  esirk_1d(ay0, ay1, jh, ayh, curry);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) curry[q] = w * curry[q];
+  ayh[1] = ayh[1] + ay0[0];
+  ayh[2] = ayh[2] + ay0[1];
+  ayh[3] = ayh[3] + ay0[2];
+  int y0 = jh < 1 ? jh : 1;
+  int y1 = (jh + 2) > 3 ? jh + 2 : 3;
+  jj0 = jj0 - 1;
+  jh = jj0 - 1;
+  ii0 = ii0 - 1;
+  ih = ii0 - 1;
+  double* jx = jc;
+  double* jy = jc + g.ncell;
+  for (int j1 = y0; j1 <= y1; ++j1) {
+    int j2 = jh + j1;
+    for (int i1 = x0; i1 <= x1; ++i1) jadd<SERIAL>(&jx[goff(g, ih + i1, j2, 1)], ayh[j1] * currx[i1]);
+  }
+  for (int j1 = y0; j1 <= y1; ++j1) {
+    int j2 = jh + j1;
+    for (int i1 = x0; i1 <= x1; ++i1) jadd<SERIAL>(&jy[goff(g, ih + i1, j2, 1)], axh[i1] * curry[j1]);
+  }
+  return true;
+}
+
+template <bool SERIAL>
+__device__ __forceinline__ bool esirkepov3d(const Geo& g, double* jc, const double xn[3], const double xo[3],
+                                            float wght) {
+  double ax0[3], ay0[3], az0[3], ax1[3], ay1[3], az1[3];
+  double axh[5], ayh[5], azh[5], axh0[5], axh1[5], ayh0[5], ayh1[5];
+  double currx[5], curry[5], currz[5];
+  int ii0 = qden64(xo[0], ax0), jj0 = qden64(xo[1], ay0), kk0 = qden64(xo[2], az0);
+  int i = qden64(xn[0], ax1), j = qden64(xn[1], ay1), k = qden64(xn[2], az1);
+  if ((unsigned)(i - ii0 + 1) > 2u || (unsigned)(j - jj0 + 1) > 2u || (unsigned)(k - kk0 + 1) > 2u) return false;
+  double w = (double)wght;
+
+  int ih = i - ii0 + 1;
+  esirk_1d(ax0, ax1, ih, axh, currx);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) currx[q] = w * currx[q];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    axh0[q] = 0.5 * axh[q];
+    axh1[q] = axh[q];
+  }
+#pragma unroll
+  for (int i1 = 1; i1 <= 3; ++i1) {
+    axh0[i1] = axh0[i1] + ax0[i1 - 1];
+    axh1[i1] = axh1[i1] + 0.5 * ax0[i1 - 1];
+  }
+  int x0 = ih < 1 ? ih : 1;
+  int x1 = (ih + 2) > 3 ? ih + 2 : 3;
+  i = i - 1;
+  ii0 = ii0 - 1;
+
+  int jh = j - jj0 + 1;
+  esirk_1d(ay0, ay1, jh, ayh, curry);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) curry[q] = w * curry[q];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    ayh0[q] = 0.5 * ayh[q];
+    ayh1[q] = ayh[q];
+  }
+#pragma unroll
+  for (int i1 = 1; i1 <= 3; ++i1) {
+    ayh0[i1] = ayh0[i1] + ay0[i1 - 1];
+    ayh1[i1] = ayh1[i1] + 0.5 * ay0[i1 - 1];
+  }
+  int y0 = jh < 1 ? jh : 1;
+  int y1 = (jh + 2) > 3 ? jh + 2 : 3;
+  jj0 = jj0 - 1;
+  j = j - 1;
+
+  int kh = k - kk0 + 1;
+  esirk_1d(az0, az1, kh, azh, currz);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) currz[q] = w * currz[q];
+  kk0 = kk0 - 1;
+  k = k - 1;
+  int z0 = kh < 1 ? kh : 1;
+  int z1 = (kh + 2) > 3 ? kh + 2 : 3;
+
+  double* jx = jc;
+  double* jy = jc + g.ncell;
+  double* jz = jc + 2 * g.ncell;
+  jh = jj0 - 1;
+  ih = ii0 - 1;
+  for (int k1 = 0; k1 <= 2; ++k1)
+    for (int j1 = y0; j1 <= y1; ++j1) {
+      int j2 = jh + j1;
+      double dvol = ayh0[j1] * az0[k1];
+      double dvolh = ayh1[j1] * az1[k1];
+      for (int i1 = x0; i1 <= x1; ++i1) {
+        int i2 = ih + i1;
+        jadd<SERIAL>(&jx[goff(g, i2, j2, kk0 + k1)], dvol * currx[i1]);
+        jadd<SERIAL>(&jx[goff(g, i2, j2, k + k1)], dvolh * currx[i1]);
+      }
+    }
+  for (int k1 = 0; k1 <= 2; ++k1)
+    for (int j1 = y0; j1 <= y1; ++j1) {
+      int j2 = jh + j1;
+      double dvol = curry[j1] * az0[k1];
+      double dvolh = curry[j1] * az1[k1];
+      for (int i1 = x0; i1 <= x1; ++i1) {
+        int i2 = ih + i1;
+        jadd<SERIAL>(&jy[goff(g, i2, j2, kk0 + k1)], axh0[i1] * dvol);
+        jadd<SERIAL>(&jy[goff(g, i2, j2, k + k1)], axh1[i1] * dvolh);
+      }
+    }
+  kh = kk0 - 1;
+  for (int k1 = z0; k1 <= z1; ++k1) {
+    int k2 = kh + k1;
+    for (int j1 = 0; j1 <= 2; ++j1) {
+      double dvol = ay0[j1] * currz[k1];
+      double dvolh = ay1[j1] * currz[k1];
+      for (int i1 = x0; i1 <= x1; ++i1) {
+        int i2 = ih + i1;
+        jadd<SERIAL>(&jz[goff(g, i2, jj0 + j1, k2)], axh0[i1] * dvol);
+        jadd<SERIAL>(&jz[goff(g, i2, j + j1, k2)], axh1[i1] * dvolh);
+      }
+    }
+  }
+  return true;
+}
+
+// ============================================================================
+// A2-A12 fused: gather (set_part{2,3}d_hcell_acc, grid_part_connect.f90:
+// 89-285) -> charge multiply (curr_and_fields_util.f90:58-72) ->
+// [init_lpf_momenta (boris_push.f90:34-73)] -> exact-gamma Boris push
+// (boris_push.f90:75-168) -> box-edge test of cell_part_dist(.false.)
+// (mpi_part_interface.f90:467-523) -> Esirkepov deposit of the particles that
+// stay.  The reference runs these as separate sweeps with ebfp as scratch;
+// per particle the arithmetic is identical, and a particle that leaves the
+// box is exactly one that the reference removes before its deposit.
+// ============================================================================
+template <bool SERIAL>
+__global__ void __launch_bounds__(256) k64_push_dep_3d(PushArgs64 a) {
+  const Geo g = a.g;
+  const double* __restrict__ ex = a.ebf;
+  long long stride = SERIAL ? 1 : (long long)gridDim.x * blockDim.x;
+  long long first = SERIAL ? 0 : blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (SERIAL && (blockIdx.x != 0 || threadIdx.x != 0)) return;
+  for (long long n = first; n < a.np; n += stride) {
+    double x = a.x[n], y = a.y[n], z = a.z[n];
+    double pp[3] = {a.px[n], a.py[n], a.pz[n]};
+    uint64_t sl = dbits(a.slot[n]);
+    // set_local_3d_positions
+    double xo[3] = {a.dx_inv * (x - a.xmn), a.dy_inv * (y - a.ymn), a.dz_inv * (z - a.zmn)};
+    double ax1[3], axh[2], ay1[3], ayh[2], az1[3], azh[2];
+    int i = qlh64(xo[0], ax1, axh);
+    int j = qlh64(xo[1], ay1, ayh);
+    int k = qlh64(xo[2], az1, azh);
+    // gather needs i..i+2, the deposit i-1..i+3 (old node i+1 +- 2)
+    if (i < 2 || i > g.n1p - 3 || j < 2 || j > g.n2p - 3 || k < 2 || k > g.n3p - 3) {
+      raise_err(a.err, AGPU_EBIT_INDEX);
+      atomicAdd(a.removed, 1ull);  // outside the box: the compaction drops it
+      continue;
+    }
+    int ih = i, jh = j, kh = k;
+    double ap[6] = {0, 0, 0, 0, 0, 0};
+    const double* e1 = ex;
+    const double* e2 = ex + g.ncell;
+    const double* e3 = ex + 2 * g.ncell;
+    const double* b1 = ex + 3 * g.ncell;
+    const double* b2 = ex + 4 * g.ncell;
+    const double* b3 = ex + 5 * g.ncell;
+#pragma unroll
+    for (int k1 = 0; k1 <= 2; ++k1) {
+      int k2 = k + k1;
+#pragma unroll
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = j + j1;
+        double dvol = ay1[j1] * az1[k1];
+#pragma unroll
+        for (int i1 = 0; i1 <= 1; ++i1) ap[0] = ap[0] + axh[i1] * dvol * __ldg(&e1[goff(g, i1 + ih, j2, k2)]);
+      }
+#pragma unroll
+      for (int j1 = 0; j1 <= 1; ++j1) {
+        int j2 = jh + j1;
+        double dvol = ayh[j1] * az1[k1];
+#pragma unroll
+        for (int i1 = 0; i1 <= 2; ++i1) ap[1] = ap[1] + ax1[i1] * dvol * __ldg(&e2[goff(g, i + i1, j2, k2)]);
+#pragma unroll
+        for (int i1 = 0; i1 <= 1; ++i1) ap[5] = ap[5] + axh[i1] * dvol * __ldg(&b3[goff(g, i1 + ih, j2, k2)]);
+      }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 <= 1; ++k1) {
+      int k2 = kh + k1;
+#pragma unroll
+      for (int j1 = 0; j1 <= 1; ++j1) {
+        int j2 = jh + j1;
+        double dvol = ayh[j1] * azh[k1];
+#pragma unroll
+        for (int i1 = 0; i1 <= 2; ++i1) ap[3] = ap[3] + ax1[i1] * dvol * __ldg(&b1[goff(g, i1 + i, j2, k2)]);
+      }
+#pragma unroll
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = j + j1;
+        double dvol = ay1[j1] * azh[k1];
+#pragma unroll
+        for (int i1 = 0; i1 <= 1; ++i1) ap[4] = ap[4] + axh[i1] * dvol * __ldg(&b2[goff(g, ih + i1, j2, k2)]);
+#pragma unroll
+        for (int i1 = 0; i1 <= 2; ++i1) ap[2] = ap[2] + ax1[i1] * dvol * __ldg(&e3[goff(g, i1 + i, j2, k2)]);
+      }
+    }
+    // field_charge_multiply
+    double q = (double)slot_charge(sl);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) ap[c] = q * ap[c];
+    if (a.initial) {
+      double alp0 = a.dth * a.lfact;
+      double efp[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) efp[c] = -alp0 * ap[c];
+      double gam2 = 1. + (pp[0] * pp[0] + pp[1] * pp[1] + pp[2] * pp[2]);
+      double gam_inv = 1. / sqrt(gam2);
+      double vp[3] = {gam_inv * pp[0], gam_inv * pp[1], gam_inv * pp[2]};
+      pp[0] = pp[0] + efp[0] + vp[1] * efp[5] - vp[2] * efp[4];
+      pp[1] = pp[1] + efp[1] + vp[2] * efp[3] - vp[0] * efp[5];
+      pp[2] = pp[2] + efp[2] + vp[0] * efp[4] - vp[1] * efp[3];
+    }
+    // lpf_momenta_and_positions, 3D
+    double alp = a.dth * a.lfact;
+    double efp[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) efp[c] = alp * ap[c];
+    double vp[3] = {pp[0] + efp[0], pp[1] + efp[1], pp[2] + efp[2]};
+    double bb[3] = {efp[3], efp[4], efp[5]};
+    double gam02 = 1. + (vp[0] * vp[0] + vp[1] * vp[1] + vp[2] * vp[2]);
+    double b2v = bb[0] * bb[0] + bb[1] * bb[1] + bb[2] * bb[2];
+    double bv = bb[0] * vp[0] + bb[1] * vp[1] + bb[2] * vp[2];
+    gam02 = gam02 - b2v;
+    double gam2 = 0.5 * (gam02 + sqrt(gam02 * gam02 + 4. * (b2v + bv * bv)));
+    double gam = sqrt(gam2);
+    double vph[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) vph[c] = gam2 * vp[c] + bb[c] * bv;
+    vph[0] = vph[0] + gam * (vp[1] * bb[2] - vp[2] * bb[1]);
+    vph[1] = vph[1] + gam * (vp[2] * bb[0] - vp[0] * bb[2]);
+    vph[2] = vph[2] + gam * (vp[0] * bb[1] - vp[1] * bb[0]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) vph[c] = vph[c] / (b2v + gam2);
+    double pn[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) pn[c] = 2. * vph[c] - pp[c];
+    gam2 = 1. + (pn[0] * pn[0] + pn[1] * pn[1] + pn[2] * pn[2]);
+    double dtg = a.dt / sqrt(gam2);
+    double xnew = x + dtg * pn[0];
+    double ynew = y + dtg * pn[1];
+    double znew = z + dtg * pn[2];
+    a.px[n] = pn[0];
+    a.py[n] = pn[1];
+    a.pz[n] = pn[2];
+    a.x[n] = xnew;
+    a.y[n] = ynew;
+    a.z[n] = znew;
+    if (!(pn[0] == pn[0] && pn[1] == pn[1] && pn[2] == pn[2])) raise_err(a.err, AGPU_EBIT_NONFINITE);
+    // cell_part_dist(.false.): keep gmin < x <= gmax along x, y, z
+    bool keep = (xnew > a.gxmin && xnew <= a.gxmax) && (ynew > a.gymin && ynew <= a.gymax) &&
+                (znew > a.gzmin && znew <= a.gzmax);
+    if (!keep) {
+      a.flag[n] = 1;
+      atomicAdd(a.removed, 1ull);
+      continue;
+    }
+    double xn[3] = {a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn), a.dz_inv * (znew - a.zmn)};
+    float wght = (float)slot_charge(sl) * slot_wgh(sl);
+    if (!esirkepov3d<SERIAL>(g, a.jc, xn, xo, wght)) raise_err(a.err, AGPU_EBIT_INDEX);
+  }
+}
+
+template <bool SERIAL>
+__global__ void __launch_bounds__(256) k64_push_dep_2d(PushArgs64 a) {
+  const Geo g = a.g;
+  const double* __restrict__ ex = a.ebf;
+  long long stride = SERIAL ? 1 : (long long)gridDim.x * blockDim.x;
+  long long first = SERIAL ? 0 : blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (SERIAL && (blockIdx.x != 0 || threadIdx.x != 0)) return;
+  for (long long n = first; n < a.np; n += stride) {
+    double x = a.x[n], y = a.y[n];
+    double pp1 = a.px[n], pp2 = a.py[n];
+    uint64_t sl = dbits(a.slot[n]);
+    double xl = a.dx_inv * (x - a.xmn);
+    double yl = a.dy_inv * (y - a.ymn);
+    double ax1[3], axh[2], ay1[3], ayh[2];
+    int i = qlh64(xl, ax1, axh);
+    int j = qlh64(yl, ay1, ayh);
+    if (i < 2 || i > g.n1p - 3 || j < 2 || j > g.n2p - 3) {
+      raise_err(a.err, AGPU_EBIT_INDEX);
+      atomicAdd(a.removed, 1ull);  // outside the box: the compaction drops it
+      continue;
+    }
+    int ih = i, jh = j;
+    const double* e1 = ex;
+    const double* e2 = ex + g.ncell;
+    const double* b3 = ex + 2 * g.ncell;
+    double ap1 = 0., ap2 = 0., ap3 = 0.;
+#pragma unroll
+    for (int j1 = 0; j1 <= 2; ++j1) {
+      int j2 = j + j1;
+      double dvol = ay1[j1];
+#pragma unroll
+      for (int i1 = 0; i1 <= 1; ++i1) {
+        double dvol1 = axh[i1] * dvol;
+        ap1 = ap1 + dvol1 * __ldg(&e1[goff(g, i1 + ih, j2, 1)]);
+      }
+    }
+#pragma unroll
+    for (int j1 = 0; j1 <= 1; ++j1) {
+      int j2 = jh + j1;
+      double dvol = ayh[j1];
+#pragma unroll
+      for (int i1 = 0; i1 <= 2; ++i1) {
+        double dvol1 = ax1[i1] * dvol;
+        ap2 = ap2 + dvol1 * __ldg(&e2[goff(g, i + i1, j2, 1)]);
+      }
+#pragma unroll
+      for (int i1 = 0; i1 <= 1; ++i1) {
+        double dvol1 = axh[i1] * dvol;
+        ap3 = ap3 + dvol1 * __ldg(&b3[goff(g, i1 + ih, j2, 1)]);
+      }
+    }
+    double q = (double)slot_charge(sl);
+    ap1 = q * ap1;
+    ap2 = q * ap2;
+    ap3 = q * ap3;
+    if (a.initial) {
+      double alp0 = a.dth * a.lfact;
+      double efp1 = -alp0 * ap1, efp2 = -alp0 * ap2, efp3 = -alp0 * ap3;
+      double gam2 = 1. + (pp1 * pp1 + pp2 * pp2);
+      double gam_inv = 1. / sqrt(gam2);
+      double vp1 = pp1 * gam_inv, vp2 = pp2 * gam_inv;
+      pp1 = pp1 + efp1 + vp2 * efp3;
+      pp2 = pp2 + efp2 - vp1 * efp3;
+    }
+    double alp = a.dth * a.lfact;
+    double efp1 = alp * ap1, efp2 = alp * ap2, efp3 = alp * ap3;
+    double vp1 = pp1 + efp1, vp2 = pp2 + efp2, vp3 = efp3;
+    double gam02 = 1. + (vp1 * vp1 + vp2 * vp2);
+    double b2 = vp3 * vp3;
+    gam02 = gam02 - b2;
+    double gam2 = 0.5 * (gam02 + sqrt(gam02 * gam02 + 4. * b2));
+    double gam = sqrt(gam2);
+    double vph1 = gam2 * vp1 + gam * vp2 * vp3;
+    double vph2 = gam2 * vp2 - gam * vp1 * vp3;
+    vph1 = vph1 / (gam2 + b2);
+    vph2 = vph2 / (gam2 + b2);
+    double pn1 = 2. * vph1 - pp1;
+    double pn2 = 2. * vph2 - pp2;
+    gam2 = 1. + (pn1 * pn1 + pn2 * pn2);
+    double dtg = a.dt / sqrt(gam2);
+    double xnew = x + dtg * pn1;
+    double ynew = y + dtg * pn2;
+    a.px[n] = pn1;
+    a.py[n] = pn2;
+    a.x[n] = xnew;
+    a.y[n] = ynew;
+    if (!(pn1 == pn1 && pn2 == pn2)) raise_err(a.err, AGPU_EBIT_NONFINITE);
+    bool keep = (xnew > a.gxmin && xnew <= a.gxmax) && (ynew > a.gymin && ynew <= a.gymax);
+    if (!keep) {
+      a.flag[n] = 1;
+      atomicAdd(a.removed, 1ull);
+      continue;
+    }
+    float wght = (float)slot_charge(sl) * slot_wgh(sl);
+    if (!esirkepov2d<SERIAL>(g, a.jc, a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn), xl, yl, wght))
+      raise_err(a.err, AGPU_EBIT_INDEX);
+  }
+}
+
+void push_deposit64(const PushArgs64& a, cudaStream_t st, int sms, bool serial) {
+  if (a.np <= 0) return;
+  int block = 256;
+  int grid = serial ? 1 : grid_for(a.np, block, sms, 8);
+  if (a.g.ndim == 3) {
+    if (serial)
+      k64_push_dep_3d<true><<<1, 32, 0, st>>>(a);
+    else
+      k64_push_dep_3d<false><<<grid, block, 0, st>>>(a);
+  } else {
+    if (serial)
+      k64_push_dep_2d<true><<<1, 32, 0, st>>>(a);
+    else
+      k64_push_dep_2d<false><<<grid, block, 0, st>>>(a);
+  }
+}
+
+void jfold64(const Dev64& d, cudaStream_t st, int sms) { jfold_t<double>(d.jc, d.g, st, sms); }
+
+void yee64(const Dev64& d, const YeeC& c, cudaStream_t st, int sms) {
+  yee_t<double>(d.ebf, d.jc, (const double*)nullptr, d.g, c, st, sms);
+}
+
+// ============================================================================
+// A15: set_ion_efield (grid_part_connect.f90:288-410): |E|^2 on each ion with
+// the qqh shapes.
+// ============================================================================
+__global__ void k64_ion_efield(IonArgs64 a) {
+  const Geo g = a.g;
+  const double* E1 = a.ebf;
+  const double* E2 = a.ebf + g.ncell;
+  const double* E3 = a.ebf + 2 * g.ncell;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < a.np; n += (long long)gridDim.x * blockDim.x) {
+    double ef_sqr = 0.;
+    double xl = a.dx_inv * (a.x[n] - a.xmn);
+    double yl = a.dy_inv * (a.y[n] - a.ymn);
+    double ax1[3], axh[3], ay1[3], ayh[3], az1[3], azh[3];
+    int i, ih, j, jh, k = 1, kh = 1;
+    qqh64(xl, ax1, axh, &i, &ih);
+    qqh64(yl, ay1, ayh, &j, &jh);
+    int imin = min(i, ih), jmin = min(j, jh);
+    if (imin < 1 || max(i, ih) > g.n1p - 2 || jmin < 1 || max(j, jh) > g.n2p - 2) {
+      raise_err(a.err, AGPU_EBIT_INDEX);
+      a.ef2[n] = 0.0;
+      continue;
+    }
+    if (g.ndim == 2) {
+      for (int jp1 = 0; jp1 <= 2; ++jp1) {
+        double dvol = ay1[jp1];
+        for (int ip1 = 0; ip1 <= 2; ++ip1) {
+          double e = E1[goff(g, ih + ip1, j + jp1, 1)];
+          ef_sqr = ef_sqr + axh[ip1] * dvol * e * e;
+        }
+      }
+      for (int jp1 = 0; jp1 <= 2; ++jp1) {
+        double dvol = ayh[jp1];
+        for (int ip1 = 0; ip1 <= 2; ++ip1) {
+          double e = E2[goff(g, i + ip1, jh + jp1, 1)];
+          ef_sqr = ef_sqr + ax1[ip1] * dvol * e * e;
+        }
+      }
+    } else {
+      double zl = a.dz_inv * (a.z[n] - a.zmn);
+      qqh64(zl, az1, azh, &k, &kh);
+      if (min(k, kh) < 1 || max(k, kh) > g.n3p - 2) {
+        raise_err(a.err, AGPU_EBIT_INDEX);
+        a.ef2[n] = 0.0;
+        continue;
+      }
+      for (int kp1 = 0; kp1 <= 2; ++kp1) {
+        int kp2 = k + kp1;
+        for (int jp1 = 0; jp1 <= 2; ++jp1) {
+          double dvol = ay1[jp1] * az1[kp1];
+          for (int ip1 = 0; ip1 <= 2; ++ip1) {
+            double e = E1[goff(g, ip1 + ih, j + jp1, kp2)];
+            ef_sqr = ef_sqr + axh[ip1] * dvol * e * e;
+          }
+        }
+        for (int jp1 = 0; jp1 <= 2; ++jp1) {
+          double dvol = ayh[jp1] * az1[kp1];
+          for (int ip1 = 0; ip1 <= 2; ++ip1) {
+            double e = E2[goff(g, i + ip1, jh + jp1, kp2)];
+            ef_sqr = ef_sqr + ax1[ip1] * dvol * e * e;
+          }
+        }
+      }
+      for (int kp1 = 0; kp1 <= 2; ++kp1) {
+        int kp2 = kh + kp1;
+        for (int jp1 = 0; jp1 <= 2; ++jp1) {
+          double dvol = ay1[jp1] * azh[kp1];
+          for (int ip1 = 0; ip1 <= 2; ++ip1) {
+            double e = E3[goff(g, ip1 + i, j + jp1, kp2)];
+            ef_sqr = ef_sqr + ax1[ip1] * dvol * e * e;
+          }
+        }
+      }
+    }
+    a.ef2[n] = ef_sqr;
+  }
+}
+
+// A16: part_ionize, ionz_lev = 1 (ionize.f90:390-450) with the nk index of
+// ionization_cycle (ionize.f90:496-506): flag[n] = 1 when ion n ionizes.
+__global__ void k64_ionize(IonArgs64 a) {
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < a.np; n += (long long)gridDim.x * blockDim.x) {
+    double ef2 = a.ef2[n];
+    int nk = 0;
+    if (ef2 > 0.) {
+      double ef = sqrt(ef2);
+      nk = (int)llround(a.de_inv * ef);
+    }
+    if (nk > a.n_ge + 1) {
+      raise_err(a.err, AGPU_EBIT_IONZ_INDEX);
+      nk = a.n_ge + 1;
+    }
+    uint64_t sl = dbits(a.slot[n]);
+    int z0 = slot_charge(sl);
+    double pr = ionz_draw(a.seed, n, a.iter, a.ic);
+    double thr = (z0 >= 0 && z0 <= a.zmax) ? a.wtab[(long long)nk + (long long)(a.n_ge + 2) * z0] : 0.0;
+    int fl = 0;
+    if (pr < thr) {
+      a.slot[n] = bitsd(make_slot(z0 + 1, slot_part_ind(sl), slot_wgh(sl)));
+      fl = 1;
+    }
+    a.flag[n] = fl;
+  }
+}
+
+}  // namespace agpu

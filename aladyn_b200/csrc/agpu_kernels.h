@@ -1,0 +1,107 @@
+// agpu_kernels.h — internal interface between the C-ABI host code
+// (agpu_api.cu) and the kernel translation units (agpu_fp64.cu,
+// agpu_fp32.cu, agpu_util.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "agpu_common.cuh"
+
+namespace agpu {
+struct YeeC {
+  double dx_inv, dy_inv, dz_inv, dt, se1, se2, ompe, djc1, djc2, djc3;
+};
+}  // namespace agpu
+
+namespace agpu {
+
+// Device state of the FP64 form.
+struct Dev64 {
+  Geo g;
+  double* ebf;  // (n1p, n2p, n3p, nf)
+  double* jc;   // (n1p, n2p, n3p, nc), raw sums before djc
+};
+
+
+struct PushArgs64 {
+  Geo g;
+  const double* ebf;
+  double* jc;
+  double *x, *y, *z, *px, *py, *pz;
+  const double* slot;
+  int* flag;  // set to 1 for particles that leave the box
+  long long np;
+  double xmn, ymn, zmn, dx_inv, dy_inv, dz_inv;
+  double dt, dth, lfact;
+  double gxmin, gxmax, gymin, gymax, gzmin, gzmax;
+  int initial;
+  unsigned long long* removed;
+  unsigned int* err;
+};
+
+struct IonArgs64 {
+  Geo g;
+  const double* ebf;
+  const double *x, *y, *z;
+  double* slot;
+  double* ef2;
+  int* flag;
+  long long np;
+  double xmn, ymn, zmn, dx_inv, dy_inv, dz_inv;
+  const double* wtab;
+  int n_ge, zmax, iter, ic;
+  double de_inv;
+  uint64_t seed;
+  unsigned int* err;
+};
+
+void field_bd64(const Dev64& d, cudaStream_t st, int sms);
+void push_deposit64(const PushArgs64& a, cudaStream_t st, int sms, bool serial);
+void jfold64(const Dev64& d, cudaStream_t st, int sms);
+void yee64(const Dev64& d, const YeeC& c, cudaStream_t st, int sms);
+__global__ void k64_ion_efield(IonArgs64 a);
+__global__ void k64_ionize(IonArgs64 a);
+
+// ---------------------------------------------------------------------------
+// FP32 split form
+// ---------------------------------------------------------------------------
+// Particle record: int32 linear node index of the nearest integer node
+// (the reference's qden index int(3 + x_loc + 0.5), Fortran 1-based, linear
+// over (n1p, n2p, n3p)), FP32 offsets (3 + x_loc) - ix in [-0.5, 0.5),
+// FP32 momenta and the 8-byte packed charge/part_ind/wgh slot.
+struct Dev32 {
+  Geo g;
+  float* ebf;   // (n1p, n2p, n3p, nf)
+  float* jhi;   // (n1p, n2p, n3p, nc) compensated sum: value = jhi + jlo
+  float* jlo;
+};
+
+struct Part32 {
+  int* cell;
+  float *ox, *oy, *oz;
+  float *px, *py, *pz;
+  uint64_t* slot;
+};
+
+struct PushArgs32 {
+  Geo g;
+  const float* ebf;
+  float* jhi;
+  float* jlo;
+  Part32 p;
+  int* flag;
+  long long np;
+  float dt, dth, lfact;
+  float dtx, dty, dtz;  // dt * d{x,y,z}_inv
+  int initial;
+  unsigned long long* removed;
+  unsigned int* err;
+};
+
+
+void field_bd32(const Dev32& d, cudaStream_t st, int sms);
+void push_deposit32(const PushArgs32& a, cudaStream_t st, int sms);
+void jfold32(const Dev32& d, cudaStream_t st, int sms);
+void yee32(const Dev32& d, const YeeC& c, cudaStream_t st, int sms);
+
+}  // namespace agpu

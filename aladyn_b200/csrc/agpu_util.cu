@@ -1,0 +1,623 @@
+// agpu_util.cu — stable selection (compaction / append), the moving-window
+// field shift, lattice injection, laser initialisation and FP64 diagnostics.
+// Compiled with -fmad=false: positions generated here must match the
+// oracle's arithmetic bit for bit.
+#include "agpu_common.cuh"
+#include "agpu_util.h"
+
+namespace agpu {
+
+// ============================================================================
+// Stable selection.  Each block owns SEL_CHUNK consecutive elements; warp w
+// of the block owns the w-th run of 32*SEL_ITEMS of them and walks it in
+// 32-element groups with a ballot, so reads and writes stay coalesced and
+// the kept elements leave in their original order (the reference compacts
+// in order: mpi_part_interface.f90:496-519).
+// ============================================================================
+template <class Pred>
+__global__ void __launch_bounds__(SEL_BLOCK) k_sel_count(Pred pr, long long n, long long* blockcnt) {
+  __shared__ int wsum[SEL_BLOCK / 32];
+  long long base = (long long)blockIdx.x * SEL_CHUNK;
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long long wbase = base + (long long)warp * 32 * SEL_ITEMS;
+  int cnt = 0;
+  for (int it = 0; it < SEL_ITEMS; ++it) {
+    long long i = wbase + it * 32 + lane;
+    bool keep = (i < n) && pr(i);
+    cnt += __popc(__ballot_sync(0xffffffffu, keep));
+  }
+  if (lane == 0) wsum[warp] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long s = 0;
+    for (int w = 0; w < SEL_BLOCK / 32; ++w) s += wsum[w];
+    blockcnt[blockIdx.x] = s;
+  }
+}
+
+// Exclusive scan of the block counts in one block; total into *total.
+__global__ void k_scan_blocks(long long* cnt, long long nb, long long* total) {
+  __shared__ long long part[1024];
+  long long per = (nb + blockDim.x - 1) / blockDim.x;
+  long long lo = threadIdx.x * per, hi = min(lo + per, nb);
+  long long s = 0;
+  for (long long b = lo; b < hi; ++b) s += cnt[b];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long run = 0;
+    for (int t = 0; t < (int)blockDim.x; ++t) {
+      long long v = part[t];
+      part[t] = run;
+      run += v;
+    }
+    *total = run;
+  }
+  __syncthreads();
+  long long run = part[threadIdx.x];
+  for (long long b = lo; b < hi; ++b) {
+    long long v = cnt[b];
+    cnt[b] = run;
+    run += v;
+  }
+}
+
+template <class Pred, class Move>
+__global__ void __launch_bounds__(SEL_BLOCK) k_sel_scatter(Pred pr, Move mv, long long n, const long long* blockoff) {
+  __shared__ int wsum[SEL_BLOCK / 32];
+  __shared__ long long woff[SEL_BLOCK / 32];
+  long long base = (long long)blockIdx.x * SEL_CHUNK;
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long long wbase = base + (long long)warp * 32 * SEL_ITEMS;
+  int cnt = 0;
+  for (int it = 0; it < SEL_ITEMS; ++it) {
+    long long i = wbase + it * 32 + lane;
+    bool keep = (i < n) && pr(i);
+    cnt += __popc(__ballot_sync(0xffffffffu, keep));
+  }
+  if (lane == 0) wsum[warp] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long s = blockoff[blockIdx.x];
+    for (int w = 0; w < SEL_BLOCK / 32; ++w) {
+      woff[w] = s;
+      s += wsum[w];
+    }
+  }
+  __syncthreads();
+  long long o = woff[warp];
+  for (int it = 0; it < SEL_ITEMS; ++it) {
+    long long i = wbase + it * 32 + lane;
+    bool keep = (i < n) && pr(i);
+    unsigned int m = __ballot_sync(0xffffffffu, keep);
+    if (keep) mv(i, o + __popc(m & ((1u << lane) - 1u)));
+    o += __popc(m);
+  }
+}
+
+template <class Pred, class Move>
+long long select_run(Pred pr, Move mv, long long n, Scratch& s, cudaStream_t st) {
+  if (n <= 0) return 0;
+  long long nb = (n + SEL_CHUNK - 1) / SEL_CHUNK;
+  k_sel_count<Pred><<<(unsigned)nb, SEL_BLOCK, 0, st>>>(pr, n, s.blockcnt);
+  k_scan_blocks<<<1, 1024, 0, st>>>(s.blockcnt, nb, s.total);
+  k_sel_scatter<Pred, Move><<<(unsigned)nb, SEL_BLOCK, 0, st>>>(pr, mv, n, s.blockcnt);
+  long long tot = 0;
+  cudaMemcpyAsync(s.h_total, s.total, sizeof(long long), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  tot = *s.h_total;
+  return tot;
+}
+
+// ---- predicates / movers ---------------------------------------------------
+struct InBox64 {
+  const double *x, *y, *z;
+  double x0, x1, y0, y1, z0, z1;
+  int use_y, use_z;
+  __device__ bool operator()(long long i) const {
+    double a = x[i];
+    bool k = a > x0 && a <= x1;
+    if (use_y) {
+      double b = y[i];
+      k = k && b > y0 && b <= y1;
+    }
+    if (use_z) {
+      double c = z[i];
+      k = k && c > z0 && c <= z1;
+    }
+    return k;
+  }
+};
+struct MoveCols64 {
+  const double* src;
+  double* dst;
+  long long ld;
+  int ndv;
+  __device__ void operator()(long long i, long long o) const {
+    for (int c = 0; c < ndv; ++c) dst[(long long)c * ld + o] = src[(long long)c * ld + i];
+  }
+};
+
+long long compact64(double* part, double* tmp, long long cap, long long np, int ndv, const BoxBounds& b, Scratch& s,
+                    cudaStream_t st) {
+  InBox64 pr{part, part + cap, part + 2 * cap, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1, b.use_y, b.use_z};
+  MoveCols64 mv{part, tmp, cap, ndv};
+  long long kept = select_run(pr, mv, np, s, st);
+  return kept;
+}
+
+// Split form: x_loc = (ix - 3) + ox; keep 0 < x_loc <= nx along each axis,
+// evaluated exactly from the integer node and the offset in [-0.5, 0.5).
+struct InBox32 {
+  const int* cell;
+  const float *ox, *oy, *oz;
+  int n1p, n2p, nx, ny, nz;
+  int use_y, use_z;
+  __device__ static bool inside(int i, float o, int n) {
+    // 0 < (i-3) + o <= n
+    int m = i - 3;
+    bool gt0 = (m > 0) || (m == 0 && o > 0.f);
+    bool le = (m < n) || (m == n && o <= 0.f);
+    return gt0 && le;
+  }
+  __device__ bool operator()(long long q) const {
+    int c = cell[q];
+    int i = c % n1p + 1;
+    int r = c / n1p;
+    int j = r % n2p + 1;
+    int k = r / n2p + 1;
+    bool kp = inside(i, ox[q], nx);
+    if (use_y) kp = kp && inside(j, oy[q], ny);
+    if (use_z) kp = kp && inside(k, oz[q], nz);
+    return kp;
+  }
+};
+struct MoveSplit {
+  Part32View src, dst;
+  __device__ void operator()(long long i, long long o) const {
+    dst.cell[o] = src.cell[i];
+    dst.ox[o] = src.ox[i];
+    dst.oy[o] = src.oy[i];
+    dst.px[o] = src.px[i];
+    dst.py[o] = src.py[i];
+    dst.slot[o] = src.slot[i];
+    if (src.oz) {
+      dst.oz[o] = src.oz[i];
+      dst.pz[o] = src.pz[i];
+    }
+  }
+};
+
+long long compact32(const Part32View& src, const Part32View& dst, long long np, int n1p, int n2p, int nx, int ny, int nz,
+                    int use_y, int use_z, Scratch& s, cudaStream_t st) {
+  InBox32 pr{src.cell, src.ox, src.oy, src.oz, n1p, n2p, nx, ny, nz, use_y, use_z};
+  MoveSplit mv{src, dst};
+  return select_run(pr, mv, np, s, st);
+}
+
+// ---- ionization electron append (ionization_electrons_inject,
+// src/ionization/ionize.f90:258-322): for each ionized ion, in ion order, one
+// electron at the ion position with zero momentum and
+// wgh = ion wgh * n_mol_atoms, charge = part_ind = -1.
+struct FlagPred {
+  const int* flag;
+  __device__ bool operator()(long long i) const { return flag[i] != 0; }
+};
+struct AppendElectron64 {
+  const double* ion;
+  long long ion_ld;
+  double* el;
+  long long el_ld;
+  long long ne0, cap;
+  int ndim, n_mol;
+  unsigned int* err;
+  __device__ void operator()(long long i, long long o) const {
+    long long q = ne0 + o;
+    if (q >= cap) {
+      atomicOr(err, AGPU_EBIT_CAPACITY);
+      return;
+    }
+    int nd = ndim;  // positions 0..nd-1, momenta nd..2nd-1, slot 2nd
+    for (int c = 0; c < nd; ++c) el[(long long)c * el_ld + q] = ion[(long long)c * ion_ld + i];
+    for (int c = nd; c < 2 * nd; ++c) el[(long long)c * el_ld + q] = 0.0;
+    uint64_t sl = dbits(ion[(long long)(2 * nd) * ion_ld + i]);
+    float w = slot_wgh(sl) * (float)n_mol;
+    el[(long long)(2 * nd) * el_ld + q] = bitsd(make_slot(-1, -1, w));
+  }
+};
+long long append_electrons64(const int* flag, long long nion, const double* ion, long long ion_ld, double* el, long long el_ld,
+                             long long ne0, long long cap, int ndim, int n_mol, unsigned int* err, Scratch& s,
+                             cudaStream_t st) {
+  FlagPred pr{flag};
+  AppendElectron64 mv{ion, ion_ld, el, el_ld, ne0, cap, ndim, n_mol, err};
+  return select_run(pr, mv, nion, s, st);
+}
+
+struct AppendElectron32 {
+  Part32View ion, el;
+  long long ne0, cap;
+  int n_mol;
+  unsigned int* err;
+  __device__ void operator()(long long i, long long o) const {
+    long long q = ne0 + o;
+    if (q >= cap) {
+      atomicOr(err, AGPU_EBIT_CAPACITY);
+      return;
+    }
+    el.cell[q] = ion.cell[i];
+    el.ox[q] = ion.ox[i];
+    el.oy[q] = ion.oy[i];
+    el.px[q] = 0.f;
+    el.py[q] = 0.f;
+    if (el.oz) {
+      el.oz[q] = ion.oz[i];
+      el.pz[q] = 0.f;
+    }
+    uint64_t sl = ion.slot[i];
+    el.slot[q] = make_slot(-1, -1, slot_wgh(sl) * (float)n_mol);
+  }
+};
+long long append_electrons32(const int* flag, long long nion, const Part32View& ion, const Part32View& el, long long ne0,
+                             long long cap, int n_mol, unsigned int* err, Scratch& s, cudaStream_t st) {
+  FlagPred pr{flag};
+  AppendElectron32 mv{ion, el, ne0, cap, n_mol, err};
+  return select_run(pr, mv, nion, s, st);
+}
+
+// ============================================================================
+// fields_left_xshift (src/parallel/mpi_field_interface.f90:299-359): for each
+// (iy, iz, comp) row over the interior y/z range, f(ix) = f(ix + nshx) for
+// ix = ix1..wi2, then f(wi2+1 : wi2+nshx) = 0.  One block per row; chunks
+// move left in increasing order, every read of a chunk before its writes.
+// ============================================================================
+template <typename T>
+__global__ void k_xshift(T* f, Geo g, int nc, int wi2, int nshx) {
+  extern __shared__ unsigned char smem_raw[];
+  T* buf = reinterpret_cast<T*>(smem_raw);
+  int ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
+  long long rows = (long long)ny * nz * nc;
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    int iy = g.jy1 + (int)(r % ny);
+    int iz = g.kz1 + (int)((r / ny) % nz);
+    int ic = (int)(r / ((long long)ny * nz));
+    T* row = f + g.ncell * ic + goff(g, 1, iy, iz);  // row[ix-1] = f(ix)
+    for (int c0 = g.ix1; c0 <= wi2; c0 += blockDim.x) {
+      int ix = c0 + threadIdx.x;
+      if (ix <= wi2) buf[threadIdx.x] = row[ix + nshx - 1];
+      __syncthreads();
+      if (ix <= wi2) row[ix - 1] = buf[threadIdx.x];
+      __syncthreads();
+    }
+    for (int ix = wi2 + 1 + threadIdx.x; ix <= wi2 + nshx; ix += blockDim.x) row[ix - 1] = (T)0;
+  }
+}
+void xshift64(double* f, const Geo& g, int nc, int wi2, int nshx, cudaStream_t st, int sms) {
+  long long rows = (long long)(g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1) * nc;
+  int grid = (int)(rows < (long long)sms * 16 ? rows : (long long)sms * 16);
+  k_xshift<double><<<grid, 256, 256 * sizeof(double), st>>>(f, g, nc, wi2, nshx);
+}
+void xshift32(float* f, const Geo& g, int nc, int wi2, int nshx, cudaStream_t st, int sms) {
+  long long rows = (long long)(g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1) * nc;
+  int grid = (int)(rows < (long long)sms * 16 ? rows : (long long)sms * 16);
+  k_xshift<float><<<grid, 256, 256 * sizeof(float), st>>>(f, g, nc, wi2, nshx);
+}
+
+// ============================================================================
+// Lattice columns (add_particles, src/dynamics/window.f90:39-104): particle q
+// of the block of columns i1..i2 is column i1 + q % ncol, row
+// j = 1 + (q / ncol) % npty, k = 1 + q / (ncol*npty) (x fastest), with the
+// jittered lattice position of the oracle's ora_lattice_particle.
+// ============================================================================
+__device__ __forceinline__ void lattice_pos(const LatticeArgs& a, long long ixl, int j, int k, double* x, double* y,
+                                            double* z) {
+  uint32_t r[4];
+  philox4x32_10((uint32_t)ixl, (uint32_t)j, (uint32_t)k, (uint32_t)a.ic, (uint32_t)a.seed, (uint32_t)(a.seed >> 32), r);
+  double jx = a.jitter * (u32d(r[0]) - 0.5);
+  double jy = a.jitter * (u32d(r[1]) - 0.5);
+  double jz = a.jitter * (u32d(r[2]) - 0.5);
+  *x = a.x_start + ((double)ixl - 0.5 + jx) * a.dxl;
+  *y = a.y_min + ((double)j - 0.5 + jy) * a.dyl;
+  *z = (a.ndim == 3) ? a.z_min + ((double)k - 0.5 + jz) * a.dzl : 0.0;
+}
+
+__global__ void k_lattice64(LatticeArgs a, double* part, long long ld, long long n0) {
+  long long ncol = a.i2 - a.i1 + 1;
+  long long total = ncol * a.npty * a.nptz;
+  uint64_t sl = make_slot(a.charge, a.part_ind, a.wgh);
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+    long long ix = a.i1 + q % ncol;
+    int j = 1 + (int)((q / ncol) % a.npty);
+    int k = 1 + (int)(q / (ncol * a.npty));
+    double x, y, z;
+    lattice_pos(a, ix, j, k, &x, &y, &z);
+    long long n = n0 + q;
+    part[n] = x;
+    part[ld + n] = y;
+    if (a.ndim == 3) {
+      part[2 * ld + n] = z;
+      part[3 * ld + n] = 0.;
+      part[4 * ld + n] = 0.;
+      part[5 * ld + n] = 0.;
+      part[6 * ld + n] = bitsd(sl);
+    } else {
+      part[2 * ld + n] = 0.;
+      part[3 * ld + n] = 0.;
+      part[4 * ld + n] = bitsd(sl);
+    }
+  }
+}
+void lattice64(const LatticeArgs& a, double* part, long long ld, long long n0, cudaStream_t st, int sms) {
+  long long total = (a.i2 - a.i1 + 1) * (long long)a.npty * a.nptz;
+  if (total <= 0) return;
+  k_lattice64<<<grid_for(total, 256, sms, 16), 256, 0, st>>>(a, part, ld, n0);
+}
+
+// FP64 absolute position -> split (node, offset) with the qden index rule.
+__device__ __forceinline__ void to_split(double xabs, double mn, double dinv, int* node, float* off) {
+  double xx = 3.0 + dinv * (xabs - mn);
+  int i = (int)(xx + 0.5);
+  *node = i;
+  *off = (float)(xx - (double)i);
+}
+
+__global__ void k_lattice32(LatticeArgs a, Part32View p, long long n0, Geo g, double xmn, double ymn, double zmn,
+                            double dx_inv, double dy_inv, double dz_inv) {
+  long long ncol = a.i2 - a.i1 + 1;
+  long long total = ncol * a.npty * a.nptz;
+  uint64_t sl = make_slot(a.charge, a.part_ind, a.wgh);
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+    long long ix = a.i1 + q % ncol;
+    int j = 1 + (int)((q / ncol) % a.npty);
+    int k = 1 + (int)(q / (ncol * a.npty));
+    double x, y, z;
+    lattice_pos(a, ix, j, k, &x, &y, &z);
+    long long n = n0 + q;
+    int ni, nj, nk = 1;
+    float fx, fy, fz = 0.f;
+    to_split(x, xmn, dx_inv, &ni, &fx);
+    to_split(y, ymn, dy_inv, &nj, &fy);
+    if (a.ndim == 3) to_split(z, zmn, dz_inv, &nk, &fz);
+    p.cell[n] = (int)goff(g, ni, nj, nk);
+    p.ox[n] = fx;
+    p.oy[n] = fy;
+    p.px[n] = 0.f;
+    p.py[n] = 0.f;
+    if (p.oz) {
+      p.oz[n] = fz;
+      p.pz[n] = 0.f;
+    }
+    p.slot[n] = sl;
+  }
+}
+void lattice32(const LatticeArgs& a, const Part32View& p, long long n0, const Geo& g, double xmn, double ymn, double zmn,
+               double dx_inv, double dy_inv, double dz_inv, cudaStream_t st, int sms) {
+  long long total = (a.i2 - a.i1 + 1) * (long long)a.npty * a.nptz;
+  if (total <= 0) return;
+  k_lattice32<<<grid_for(total, 256, sms, 16), 256, 0, st>>>(a, p, n0, g, xmn, ymn, zmn, dx_inv, dy_inv, dz_inv);
+}
+
+// ---- conversions between the FP64 Fortran records and the split form -----
+__global__ void k_rec_to_split(const double* rec, long long ld, long long n, Part32View p, long long n0, Geo g, double xmn,
+                               double ymn, double zmn, double dx_inv, double dy_inv, double dz_inv) {
+  int nd = g.ndim;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int ni, nj, nk = 1;
+    float fx, fy, fz = 0.f;
+    to_split(rec[q], xmn, dx_inv, &ni, &fx);
+    to_split(rec[ld + q], ymn, dy_inv, &nj, &fy);
+    if (nd == 3) to_split(rec[2 * ld + q], zmn, dz_inv, &nk, &fz);
+    long long o = n0 + q;
+    p.cell[o] = (int)goff(g, ni, nj, nk);
+    p.ox[o] = fx;
+    p.oy[o] = fy;
+    p.px[o] = (float)rec[nd * ld + q];
+    p.py[o] = (float)rec[(nd + 1) * ld + q];
+    if (nd == 3) {
+      p.oz[o] = fz;
+      p.pz[o] = (float)rec[5 * ld + q];
+    }
+    p.slot[o] = dbits(rec[2 * nd * ld + q]);
+  }
+}
+void rec_to_split(const double* rec, long long ld, long long n, const Part32View& p, long long n0, const Geo& g, double xmn,
+                  double ymn, double zmn, double dx_inv, double dy_inv, double dz_inv, cudaStream_t st, int sms) {
+  if (n <= 0) return;
+  k_rec_to_split<<<grid_for(n, 256, sms, 16), 256, 0, st>>>(rec, ld, n, p, n0, g, xmn, ymn, zmn, dx_inv, dy_inv, dz_inv);
+}
+__global__ void k_split_to_rec(Part32View p, long long n, double* rec, long long ld, Geo g, double xmn, double ymn, double zmn,
+                               double dx, double dy, double dz) {
+  int nd = g.ndim;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int c = p.cell[q];
+    int i = c % g.n1p + 1;
+    int r = c / g.n1p;
+    int j = r % g.n2p + 1;
+    int k = r / g.n2p + 1;
+    rec[q] = xmn + ((double)(i - 3) + (double)p.ox[q]) * dx;
+    rec[ld + q] = ymn + ((double)(j - 3) + (double)p.oy[q]) * dy;
+    if (nd == 3) rec[2 * ld + q] = zmn + ((double)(k - 3) + (double)p.oz[q]) * dz;
+    rec[nd * ld + q] = (double)p.px[q];
+    rec[(nd + 1) * ld + q] = (double)p.py[q];
+    if (nd == 3) rec[5 * ld + q] = (double)p.pz[q];
+    rec[2 * nd * ld + q] = bitsd(p.slot[q]);
+  }
+}
+void split_to_rec(const Part32View& p, long long n, double* rec, long long ld, const Geo& g, double xmn, double ymn, double zmn,
+                  double dx, double dy, double dz, cudaStream_t st, int sms) {
+  if (n <= 0) return;
+  k_split_to_rec<<<grid_for(n, 256, sms, 16), 256, 0, st>>>(p, n, rec, ld, g, xmn, ymn, zmn, dx, dy, dz);
+}
+__global__ void k_f64_to_f32(const double* a, float* b, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    b[q] = (float)a[q];
+}
+__global__ void k_f32_to_f64(const float* a, double* b, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    b[q] = (double)a[q];
+}
+__global__ void k_f32pair_to_f64(const float* hi, const float* lo, double* b, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    b[q] = (double)hi[q] + (double)lo[q];
+}
+void f64_to_f32(const double* a, float* b, long long n, cudaStream_t st, int sms) {
+  k_f64_to_f32<<<grid_for(n, 256, sms, 16), 256, 0, st>>>(a, b, n);
+}
+void f32_to_f64(const float* a, double* b, long long n, cudaStream_t st, int sms) {
+  k_f32_to_f64<<<grid_for(n, 256, sms, 16), 256, 0, st>>>(a, b, n);
+}
+void f32pair_to_f64(const float* hi, const float* lo, double* b, long long n, cudaStream_t st, int sms) {
+  k_f32pair_to_f64<<<grid_for(n, 256, sms, 16), 256, 0, st>>>(hi, lo, b, n);
+}
+
+// ============================================================================
+// Laser: linearly polarised (y) paraxial Gaussian pulse moving along +x,
+// Ey on (i, j+1/2, k) and Bz = Ey(x + dx/2) on (i+1/2, j+1/2, k), both at
+// t = 0; Gaussian longitudinal envelope exp(-((x-xc)/w0_x)^2) with
+// w0_x = tau_fwhm / sqrt(2 ln 2) as the reference's g_prof pulse
+// (set_init_param.f90:318-330).  Interior nodes only.
+// ============================================================================
+__device__ double laser_ey(const LaserArgs& a, double x, double y, double z) {
+  double xi = x - a.xf;
+  double zr = a.zr;
+  double wr = a.w0 * sqrt(1.0 + (xi / zr) * (xi / zr));
+  double r2 = (y - a.y0) * (y - a.y0);
+  if (a.ndim == 3) r2 += (z - a.z0) * (z - a.z0);
+  double rinv = xi / (xi * xi + zr * zr);
+  double gouy = atan(xi / zr);
+  double amp = (a.ndim == 3) ? a.w0 / wr : sqrt(a.w0 / wr);
+  double ph = a.k0 * (x - a.xc) + 0.5 * a.k0 * r2 * rinv - ((a.ndim == 3) ? gouy : 0.5 * gouy);
+  double ex = (x - a.xc) / a.w0x;
+  return a.amp * amp * exp(-r2 / (wr * wr)) * exp(-ex * ex) * cos(ph);
+}
+__global__ void k_laser64(LaserArgs a, double* ebf, Geo g) {
+  int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
+  long long total = (long long)nx * ny * nz;
+  int cey = 1, cbz = g.nf - 1;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int i = g.ix1 + (int)(t % nx);
+    int j = g.jy1 + (int)((t / nx) % ny);
+    int k = g.kz1 + (int)(t / ((long long)nx * ny));
+    double x = a.xmn + (double)(i - 3) * a.dx;
+    double y = a.ymn + ((double)(j - 3) + 0.5) * a.dy;
+    double z = (g.ndim == 3) ? a.zmn + (double)(k - 3) * a.dz : 0.0;
+    long long o = goff(g, i, j, k);
+    ebf[g.ncell * cey + o] += laser_ey(a, x, y, z);
+    ebf[g.ncell * cbz + o] += laser_ey(a, x + 0.5 * a.dx, y, z);
+  }
+}
+void laser64(const LaserArgs& a, double* ebf, const Geo& g, cudaStream_t st, int sms) {
+  long long cells = (long long)(g.ix2 - g.ix1 + 1) * (g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1);
+  k_laser64<<<grid_for(cells, 256, sms, 16), 256, 0, st>>>(a, ebf, g);
+}
+
+// ============================================================================
+// Diagnostics (Envar / energy_momenta, diag_part_and_fields.f90:172-220,
+// 485-719), FP64 block reductions.
+// ============================================================================
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ void atomic_max_nonneg(double* a, double v) {
+  atomicMax(reinterpret_cast<unsigned long long*>(a), (unsigned long long)__double_as_longlong(v));
+}
+
+template <typename T>
+__global__ void k_field_diag(const T* ebf, Geo g, int nf, double dvol, double* out_e, double* out_max) {
+  int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
+  long long total = (long long)nx * ny * nz;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  double mx = 0.0;
+  int ne = (nf == 6) ? 3 : 2;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int i = g.ix1 + (int)(t % nx);
+    int j = g.jy1 + (int)((t / nx) % ny);
+    int k = g.kz1 + (int)(t / ((long long)nx * ny));
+    long long o = goff(g, i, j, k);
+    for (int c = 0; c < nf; ++c) {
+      double v = (double)ebf[g.ncell * c + o];
+      acc[c] += v * v;
+      if (c < ne) mx = fmax(mx, fabs(v));
+    }
+  }
+  for (int c = 0; c < nf; ++c) {
+    double v = warp_sum(acc[c]);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&out_e[c], v * dvol);
+  }
+  double m = warp_max(mx);
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out_max, m);
+}
+void field_diag64(const double* ebf, const Geo& g, double dvol, double* out_e, double* out_max, cudaStream_t st, int sms) {
+  long long cells = (long long)(g.ix2 - g.ix1 + 1) * (g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1);
+  k_field_diag<double><<<grid_for(cells, 256, sms, 8), 256, 0, st>>>(ebf, g, g.nf, dvol, out_e, out_max);
+}
+void field_diag32(const float* ebf, const Geo& g, double dvol, double* out_e, double* out_max, cudaStream_t st, int sms) {
+  long long cells = (long long)(g.ix2 - g.ix1 + 1) * (g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1);
+  k_field_diag<float><<<grid_for(cells, 256, sms, 8), 256, 0, st>>>(ebf, g, g.nf, dvol, out_e, out_max);
+}
+
+// out[0] = sum w (gamma-1), out[1] = sum charge*w, out[2..4] = sum w p
+__global__ void k_part_diag64(const double* part, long long ld, long long n, int nd, double* out) {
+  double a[5] = {0, 0, 0, 0, 0};
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    double p2 = 0.0, pv[3] = {0, 0, 0};
+    for (int c = 0; c < nd; ++c) {
+      pv[c] = part[(long long)(nd + c) * ld + q];
+      p2 += pv[c] * pv[c];
+    }
+    uint64_t sl = dbits(part[(long long)(2 * nd) * ld + q]);
+    double w = (double)slot_wgh(sl);
+    double gm = sqrt(1.0 + p2);
+    a[0] += w * (gm - 1.0);
+    a[1] += (double)slot_charge(sl) * w;
+    for (int c = 0; c < 3; ++c) a[2 + c] += w * pv[c];
+  }
+  for (int c = 0; c < 5; ++c) {
+    double v = warp_sum(a[c]);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&out[c], v);
+  }
+}
+void part_diag64(const double* part, long long ld, long long n, int nd, double* out, cudaStream_t st, int sms) {
+  if (n <= 0) return;
+  k_part_diag64<<<grid_for(n, 256, sms, 8), 256, 0, st>>>(part, ld, n, nd, out);
+}
+__global__ void k_part_diag32(Part32View p, long long n, int nd, double* out) {
+  double a[5] = {0, 0, 0, 0, 0};
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    double pv[3] = {(double)p.px[q], (double)p.py[q], nd == 3 ? (double)p.pz[q] : 0.0};
+    double p2 = pv[0] * pv[0] + pv[1] * pv[1] + pv[2] * pv[2];
+    uint64_t sl = p.slot[q];
+    double w = (double)slot_wgh(sl);
+    double gm = sqrt(1.0 + p2);
+    a[0] += w * (gm - 1.0);
+    a[1] += (double)slot_charge(sl) * w;
+    for (int c = 0; c < 3; ++c) a[2 + c] += w * pv[c];
+  }
+  for (int c = 0; c < 5; ++c) {
+    double v = warp_sum(a[c]);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&out[c], v);
+  }
+}
+void part_diag32(const Part32View& p, long long n, int nd, double* out, cudaStream_t st, int sms) {
+  if (n <= 0) return;
+  k_part_diag32<<<grid_for(n, 256, sms, 8), 256, 0, st>>>(p, n, nd, out);
+}
+
+// max of a non-negative FP64 array (ion |E|^2), for the lp_max refresh.
+__global__ void k_max_nonneg(const double* a, long long n, double* out) {
+  double m = 0.0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    m = fmax(m, a[q]);
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, m);
+}
+void max_nonneg(const double* a, long long n, double* out, cudaStream_t st, int sms) {
+  cudaMemsetAsync(out, 0, sizeof(double), st);
+  if (n > 0) k_max_nonneg<<<grid_for(n, 256, sms, 8), 256, 0, st>>>(a, n, out);
+}
+
+}  // namespace agpu

@@ -1,0 +1,77 @@
+// agpu_util.h — interface of agpu_util.cu (selection, window, injection,
+// laser, diagnostics, format conversions).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "agpu_common.cuh"
+
+namespace agpu {
+
+constexpr int SEL_BLOCK = 256;
+constexpr int SEL_ITEMS = 16;
+constexpr int SEL_CHUNK = SEL_BLOCK * SEL_ITEMS;
+
+struct Scratch {
+  long long* blockcnt;  // >= ceil(max particles / SEL_CHUNK)
+  long long* total;     // device scalar
+  long long* h_total;   // pinned host scalar
+};
+
+struct BoxBounds {
+  double x0, x1, y0, y1, z0, z1;
+  int use_y, use_z;
+};
+
+// Device pointers of one species in the split form (oz/pz null in 2D).
+struct Part32View {
+  int* cell;
+  float *ox, *oy, *oz;
+  float *px, *py, *pz;
+  uint64_t* slot;
+};
+
+struct LatticeArgs {
+  int ndim, ic, npty, nptz;
+  long long i1, i2;
+  int charge, part_ind;
+  float wgh;
+  double x_start, y_min, z_min, dxl, dyl, dzl, jitter;
+  uint64_t seed;
+};
+
+struct LaserArgs {
+  int ndim;
+  double amp, k0, w0, zr, w0x, xc, xf, y0, z0;
+  double xmn, ymn, zmn, dx, dy, dz;
+};
+
+long long compact64(double* part, double* tmp, long long cap, long long np, int ndv, const BoxBounds& b, Scratch& s,
+                    cudaStream_t st);
+long long compact32(const Part32View& src, const Part32View& dst, long long np, int n1p, int n2p, int nx, int ny, int nz,
+                    int use_y, int use_z, Scratch& s, cudaStream_t st);
+long long append_electrons64(const int* flag, long long nion, const double* ion, long long ion_ld, double* el, long long el_ld,
+                             long long ne0, long long cap, int ndim, int n_mol, unsigned int* err, Scratch& s,
+                             cudaStream_t st);
+long long append_electrons32(const int* flag, long long nion, const Part32View& ion, const Part32View& el, long long ne0,
+                             long long cap, int n_mol, unsigned int* err, Scratch& s, cudaStream_t st);
+void xshift64(double* f, const Geo& g, int nc, int wi2, int nshx, cudaStream_t st, int sms);
+void xshift32(float* f, const Geo& g, int nc, int wi2, int nshx, cudaStream_t st, int sms);
+void lattice64(const LatticeArgs& a, double* part, long long ld, long long n0, cudaStream_t st, int sms);
+void lattice32(const LatticeArgs& a, const Part32View& p, long long n0, const Geo& g, double xmn, double ymn, double zmn,
+               double dx_inv, double dy_inv, double dz_inv, cudaStream_t st, int sms);
+void rec_to_split(const double* rec, long long ld, long long n, const Part32View& p, long long n0, const Geo& g, double xmn,
+                  double ymn, double zmn, double dx_inv, double dy_inv, double dz_inv, cudaStream_t st, int sms);
+void split_to_rec(const Part32View& p, long long n, double* rec, long long ld, const Geo& g, double xmn, double ymn, double zmn,
+                  double dx, double dy, double dz, cudaStream_t st, int sms);
+void f64_to_f32(const double* a, float* b, long long n, cudaStream_t st, int sms);
+void f32_to_f64(const float* a, double* b, long long n, cudaStream_t st, int sms);
+void f32pair_to_f64(const float* hi, const float* lo, double* b, long long n, cudaStream_t st, int sms);
+void laser64(const LaserArgs& a, double* ebf, const Geo& g, cudaStream_t st, int sms);
+void field_diag64(const double* ebf, const Geo& g, double dvol, double* out_e, double* out_max, cudaStream_t st, int sms);
+void field_diag32(const float* ebf, const Geo& g, double dvol, double* out_e, double* out_max, cudaStream_t st, int sms);
+void part_diag64(const double* part, long long ld, long long n, int nd, double* out, cudaStream_t st, int sms);
+void part_diag32(const Part32View& p, long long n, int nd, double* out, cudaStream_t st, int sms);
+void max_nonneg(const double* a, long long n, double* out, cudaStream_t st, int sms);
+
+}  // namespace agpu

@@ -1,0 +1,309 @@
+// agpu_yee.cuh — field kernels templated on the storage type: boundary
+// extrapolation (A1), current fold (A13) and the leapfrog Yee update with
+// Mur-type open boundaries (A14).  Included by agpu_fp64.cu (T = double,
+// compiled without FMA contraction so the statement order of the reference
+// is kept bit for bit) and agpu_fp32.cu (T = float).
+#pragma once
+#include "agpu_common.cuh"
+#include "agpu_kernels.h"
+
+namespace agpu {
+
+#define GRID_STRIDE(t, total) \
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (total); t += (long long)gridDim.x * blockDim.x)
+
+// ---- A1: field_xyzbd (src/parallel/mpi_field_interface.f90:53-198) --------
+template <typename T>
+__global__ void k_field_bd_x(T* ebf, Geo g, int nc) {
+  int ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
+  long long total = (long long)ny * nz * nc;
+  GRID_STRIDE(t, total) {
+    int iy = g.jy1 + (int)(t % ny);
+    int iz = g.kz1 + (int)((t / ny) % nz);
+    int ik = (int)(t / ((long long)ny * nz));
+    T* f = ebf + g.ncell * ik;
+    f[goff(g, g.ix1 - 1, iy, iz)] = (T)2. * f[goff(g, g.ix1, iy, iz)] - f[goff(g, g.ix1 + 1, iy, iz)];
+    f[goff(g, g.ix2 + 1, iy, iz)] = (T)2. * f[goff(g, g.ix2, iy, iz)] - f[goff(g, g.ix2 - 1, iy, iz)];
+  }
+}
+template <typename T>
+__global__ void k_field_bd_y(T* ebf, Geo g, int nc) {
+  int nxe = g.ix2 - g.ix1 + 3, nz = g.kz2 - g.kz1 + 1;
+  long long total = (long long)nxe * nz * nc;
+  GRID_STRIDE(t, total) {
+    int ix = g.ix1 - 1 + (int)(t % nxe);
+    int iz = g.kz1 + (int)((t / nxe) % nz);
+    int ik = (int)(t / ((long long)nxe * nz));
+    T* f = ebf + g.ncell * ik;
+    f[goff(g, ix, g.jy1 - 1, iz)] = (T)2. * f[goff(g, ix, g.jy1, iz)] - f[goff(g, ix, g.jy1 + 1, iz)];
+    f[goff(g, ix, g.jy2 + 1, iz)] = (T)2. * f[goff(g, ix, g.jy2, iz)] - f[goff(g, ix, g.jy2 - 1, iz)];
+  }
+}
+template <typename T>
+__global__ void k_field_bd_z(T* ebf, Geo g, int nc) {
+  int nxe = g.ix2 - g.ix1 + 3, nye = g.jy2 - g.jy1 + 3;
+  long long total = (long long)nxe * nye * nc;
+  GRID_STRIDE(t, total) {
+    int ix = g.ix1 - 1 + (int)(t % nxe);
+    int iy = g.jy1 - 1 + (int)((t / nxe) % nye);
+    int ik = (int)(t / ((long long)nxe * nye));
+    T* f = ebf + g.ncell * ik;
+    f[goff(g, ix, iy, g.kz1 - 1)] = (T)2 * f[goff(g, ix, iy, g.kz1)] - f[goff(g, ix, iy, g.kz1 + 1)];
+    f[goff(g, ix, iy, g.kz2 + 1)] = (T)2 * f[goff(g, ix, iy, g.kz2)] - f[goff(g, ix, iy, g.kz2 - 1)];
+  }
+}
+template <typename T>
+void field_bd_t(T* ebf, const Geo& g, cudaStream_t st, int sms) {
+  int nc = g.nf;
+  k_field_bd_x<T><<<grid_for((long long)(g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1) * nc, 256, sms), 256, 0, st>>>(ebf, g, nc);
+  k_field_bd_y<T><<<grid_for((long long)(g.ix2 - g.ix1 + 3) * (g.kz2 - g.kz1 + 1) * nc, 256, sms), 256, 0, st>>>(ebf, g, nc);
+  if (g.ndim == 3)
+    k_field_bd_z<T><<<grid_for((long long)(g.ix2 - g.ix1 + 3) * (g.jy2 - g.jy1 + 3) * nc, 256, sms), 256, 0, st>>>(ebf, g, nc);
+}
+
+// ---- A13: jc_xyzbd (src/parallel/mpi_curr_interface.f90:551-643) ----------
+template <typename T>
+__global__ void k_jfold_x(T* jc, Geo g) {
+  int ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
+  long long total = (long long)ny * nz * g.nc;
+  GRID_STRIDE(t, total) {
+    int j = g.jy1 + (int)(t % ny);
+    int k = g.kz1 + (int)((t / ny) % nz);
+    int ik = (int)(t / ((long long)ny * nz));
+    T* c = jc + g.ncell * ik;
+    long long a = goff(g, g.ix1, j, k);
+    c[a] = c[a] + c[a - 1];
+    c[a - 1] = (T)0;
+    long long b = goff(g, g.ix2, j, k);
+    c[b] = c[b] + c[b + 1] + c[b + 2];
+    c[b + 1] = (T)0;
+    c[b + 2] = (T)0;
+  }
+}
+template <typename T>
+__global__ void k_jfold_y(T* jc, Geo g) {
+  int nx = g.ix2 - g.ix1 + 1, nz = g.kz2 - g.kz1 + 1;
+  long long total = (long long)nx * nz * g.nc;
+  long long sy = g.n1p;
+  GRID_STRIDE(t, total) {
+    int ix = g.ix1 + (int)(t % nx);
+    int iz = g.kz1 + (int)((t / nx) % nz);
+    int ik = (int)(t / ((long long)nx * nz));
+    T* c = jc + g.ncell * ik;
+    long long a = goff(g, ix, g.jy1, iz);
+    c[a] = c[a] + c[a - sy] + c[a - 2 * sy];
+    c[a - 2 * sy] = (T)0;
+    c[a - sy] = (T)0;
+    long long b = goff(g, ix, g.jy2, iz);
+    c[b] = c[b] + c[b + sy] + c[b + 2 * sy];
+    c[b + sy] = (T)0;
+    c[b + 2 * sy] = (T)0;
+  }
+}
+template <typename T>
+__global__ void k_jfold_z(T* jc, Geo g) {
+  int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1;
+  long long total = (long long)nx * ny * g.nc;
+  long long sz = (long long)g.n1p * g.n2p;
+  GRID_STRIDE(t, total) {
+    int ix = g.ix1 + (int)(t % nx);
+    int iy = g.jy1 + (int)((t / nx) % ny);
+    int ik = (int)(t / ((long long)nx * ny));
+    T* c = jc + g.ncell * ik;
+    long long a = goff(g, ix, iy, g.kz1);
+    c[a] = c[a] + c[a - sz];
+    c[a - sz] = (T)0;
+    long long b = goff(g, ix, iy, g.kz2);
+    c[b] = c[b] + c[b + sz] + c[b + 2 * sz];
+    c[b + sz] = (T)0;
+    c[b + 2 * sz] = (T)0;
+  }
+}
+template <typename T>
+void jfold_t(T* jc, const Geo& g, cudaStream_t st, int sms) {
+  k_jfold_x<T><<<grid_for((long long)(g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1) * g.nc, 256, sms), 256, 0, st>>>(jc, g);
+  k_jfold_y<T><<<grid_for((long long)(g.ix2 - g.ix1 + 1) * (g.kz2 - g.kz1 + 1) * g.nc, 256, sms), 256, 0, st>>>(jc, g);
+  if (g.ndim == 3)
+    k_jfold_z<T><<<grid_for((long long)(g.ix2 - g.ix1 + 1) * (g.jy2 - g.jy1 + 1) * g.nc, 256, sms), 256, 0, st>>>(jc, g);
+}
+
+// ---- A14: Yee (advance_lpf_fields, curr_and_fields_util.f90:176-260) ------
+
+// ef_bds (src/fields/grid_fields.f90:1204-1354): right-face Mur boundary of E.
+template <typename T>
+__global__ void k_ef_bds(T* ebf, Geo g, YeeC c, double dtl) {
+  int ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1, nx = g.ix2 - g.ix1 + 1;
+  long long nfx = (long long)ny * nz, nfy = (long long)nx * nz, nfz = (g.ndim == 3) ? (long long)nx * ny : 0;
+  int nf = g.nf;
+  T* E1 = ebf;
+  T* E2 = ebf + g.ncell;
+  T* E3 = ebf + 2 * g.ncell;
+  T* B1 = ebf + 3 * g.ncell;
+  T* B2 = ebf + 4 * g.ncell;
+  T* Bn = ebf + (nf - 1) * g.ncell;
+  const T one = (T)1., two = (T)2.;
+  GRID_STRIDE(t, nfx + nfy + nfz) {
+    if (t < nfx) {
+      int j = g.jy1 + (int)(t % ny), k = g.kz1 + (int)(t / ny);
+      T aphx = (T)(1.0 * c.dx_inv * dtl);
+      long long o = goff(g, g.ix2, j, k);
+      E2[o + 1] = (two * Bn[o] - (one - aphx) * E2[o]) / (one + aphx);
+      if (nf > 3) E3[o + 1] = -(two * B2[o] + (one - aphx) * E3[o]) / (one + aphx);
+    } else if (t < nfx + nfy) {
+      long long u = t - nfx;
+      int i = g.ix1 + (int)(u % nx), k = g.kz1 + (int)(u / nx);
+      T aphy = (T)(1.0 * c.dy_inv * dtl);
+      long long o = goff(g, i, g.jy2, k), o1 = o + g.n1p;
+      E1[o1] = -(two * Bn[o] + (one - aphy) * E1[o]) / (one + aphy);
+      if (nf > 3) E3[o1] = (two * B1[o] - (one - aphy) * E3[o]) / (one + aphy);
+    } else {
+      long long u = t - nfx - nfy;
+      int i = g.ix1 + (int)(u % nx), j = g.jy1 + (int)(u / nx);
+      T aphz = (T)(1.0 * c.dz_inv * dtl);
+      long long o = goff(g, i, j, g.kz2), o1 = o + (long long)g.n1p * g.n2p;
+      E1[o1] = (two * B2[o] - (one - aphz) * E1[o]) / (one + aphz);
+      E2[o1] = -(two * B1[o] + (one - aphz) * E2[o]) / (one + aphz);
+    }
+  }
+}
+// bf_bds (src/fields/grid_fields.f90:1069-1202): left-face Mur boundary of B.
+template <typename T>
+__global__ void k_bf_bds(T* ebf, Geo g, YeeC c, double dtl) {
+  int ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1, nx = g.ix2 - g.ix1 + 1;
+  long long nfx = (long long)ny * nz, nfy = (long long)nx * nz, nfz = (g.ndim == 3) ? (long long)nx * ny : 0;
+  int nf = g.nf;
+  T* E1 = ebf;
+  T* E2 = ebf + g.ncell;
+  T* E3 = ebf + 2 * g.ncell;
+  T* B1 = ebf + 3 * g.ncell;
+  T* B2 = ebf + 4 * g.ncell;
+  T* Bn = ebf + (nf - 1) * g.ncell;
+  const T one = (T)1., two = (T)2.;
+  GRID_STRIDE(t, nfx + nfy + nfz) {
+    if (t < nfx) {
+      int j = g.jy1 + (int)(t % ny), k = g.kz1 + (int)(t / ny);
+      T aphx = (T)(1.0 * c.dx_inv * dtl);
+      long long o = goff(g, g.ix1, j, k);
+      Bn[o - 1] = -(two * E2[o] + (one - aphx) * Bn[o]) / (one + aphx);
+      if (nf > 3) B2[o - 1] = (two * E3[o] - (one - aphx) * B2[o]) / (one + aphx);
+    } else if (t < nfx + nfy) {
+      long long u = t - nfx;
+      int i = g.ix1 + (int)(u % nx), k = g.kz1 + (int)(u / nx);
+      T aphy = (T)(1.0 * c.dy_inv * dtl);
+      long long o = goff(g, i, g.jy1, k), o1 = o - g.n1p;
+      T v = two * E1[o] - (one - aphy) * Bn[o];
+      Bn[o1] = v / (one + aphy);
+      if (nf > 3) {
+        T w = -two * E3[o] - (one - aphy) * B1[o];
+        B1[o1] = w / (one + aphy);
+      }
+    } else {
+      long long u = t - nfx - nfy;
+      int i = g.ix1 + (int)(u % nx), j = g.jy1 + (int)(u / nx);
+      T aphz = (T)(1.0 * c.dz_inv * dtl);
+      long long o = goff(g, i, j, g.kz1), o1 = o - (long long)g.n1p * g.n2p;
+      T v = two * E2[o] - (one - aphz) * B1[o];
+      B1[o1] = v / (one + aphz);
+      T w = -two * E1[o] - (one - aphz) * B2[o];
+      B2[o1] = w / (one + aphz);
+    }
+  }
+}
+
+// rote (grid_fields.f90:1405-1478): B -= dtf curl E, interior.
+template <typename T, int NDIM>
+__global__ void __launch_bounds__(256) k_rote(T* ebf, Geo g, YeeC c, double dtf) {
+  int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
+  long long total = (long long)nx * ny * nz;
+  double aphxd = dtf * c.dx_inv, aphyd = dtf * c.dy_inv, aphzd = dtf * c.dz_inv;
+  T aph1 = (T)(aphxd * c.se1), aph2 = (T)(aphxd * c.se2);
+  T sdhy = (T)(1.0 * aphyd), sdhz = (T)(1.0 * aphzd);
+  const T* E1 = ebf;
+  const T* E2 = ebf + g.ncell;
+  const T* E3 = ebf + 2 * g.ncell;
+  long long sy = g.n1p, sz = (long long)g.n1p * g.n2p;
+  GRID_STRIDE(t, total) {
+    int i = g.ix1 + (int)(t % nx);
+    int j = g.jy1 + (int)((t / nx) % ny);
+    int k = g.kz1 + (int)(t / ((long long)nx * ny));
+    long long o = goff(g, i, j, k);
+    if (NDIM == 2) {
+      T* Bz = ebf + 2 * g.ncell;
+      Bz[o] = Bz[o] - aph1 * (E2[o + 1] - E2[o]) + sdhy * (E1[o + sy] - E1[o]) - aph2 * (E2[o + 2] - E2[o - 1]);
+    } else {
+      T* Bx = ebf + 3 * g.ncell;
+      T* By = ebf + 4 * g.ncell;
+      T* Bz = ebf + 5 * g.ncell;
+      Bz[o] = Bz[o] - aph1 * (E2[o + 1] - E2[o]) + sdhy * (E1[o + sy] - E1[o]) - aph2 * (E2[o + 2] - E2[o - 1]);
+      Bx[o] = Bx[o] - sdhy * (E3[o + sy] - E3[o]) + sdhz * (E2[o + sz] - E2[o]);
+      By[o] = By[o] + aph1 * (E3[o + 1] - E3[o]) - sdhz * (E1[o + sz] - E1[o]) + aph2 * (E3[o + 2] - E3[o - 1]);
+    }
+  }
+}
+
+// rotb (grid_fields.f90:1480-1552) + E -= ompe * (djc * J)
+// (curr_and_fields_util.f90:111-115, 227-231).  jlo (optional) holds the
+// compensation term of a two-float current.
+template <typename T, int NDIM>
+__global__ void __launch_bounds__(256) k_rotb_j(T* ebf, const T* jc, const T* jlo, Geo g, YeeC c, double dtf) {
+  int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
+  long long total = (long long)nx * ny * nz;
+  double aphxd = dtf * c.dx_inv, aphyd = dtf * c.dy_inv, aphzd = dtf * c.dz_inv;
+  T aph1 = (T)(aphxd * c.se1), aph2 = (T)(aphxd * c.se2);
+  T sdy = (T)(1.0 * aphyd), sdz = (T)(aphzd * 1.0);
+  T ompe = (T)c.ompe, djc1 = (T)c.djc1, djc2 = (T)c.djc2, djc3 = (T)c.djc3;
+  T* E1 = ebf;
+  T* E2 = ebf + g.ncell;
+  long long sy = g.n1p, sz = (long long)g.n1p * g.n2p;
+  GRID_STRIDE(t, total) {
+    int i = g.ix1 + (int)(t % nx);
+    int j = g.jy1 + (int)((t / nx) % ny);
+    int k = g.kz1 + (int)(t / ((long long)nx * ny));
+    long long o = goff(g, i, j, k);
+    T j1 = jc[o], j2 = jc[o + g.ncell];
+    if (jlo) {
+      j1 = j1 + jlo[o];
+      j2 = j2 + jlo[o + g.ncell];
+    }
+    if (NDIM == 2) {
+      const T* Bz = ebf + 2 * g.ncell;
+      T ex = E1[o] + sdy * (Bz[o] - Bz[o - sy]);
+      T ey = E2[o] - aph1 * (Bz[o] - Bz[o - 1]) - aph2 * (Bz[o + 1] - Bz[o - 2]);
+      E1[o] = ex - ompe * (djc1 * j1);
+      E2[o] = ey - ompe * (djc2 * j2);
+    } else {
+      T* E3 = ebf + 2 * g.ncell;
+      const T* Bx = ebf + 3 * g.ncell;
+      const T* By = ebf + 4 * g.ncell;
+      const T* Bz = ebf + 5 * g.ncell;
+      T j3 = jc[o + 2 * g.ncell];
+      if (jlo) j3 = j3 + jlo[o + 2 * g.ncell];
+      T ex = E1[o] + sdy * (Bz[o] - Bz[o - sy]);
+      T ey = E2[o] - aph1 * (Bz[o] - Bz[o - 1]) - aph2 * (Bz[o + 1] - Bz[o - 2]);
+      ex = ex - sdz * (By[o] - By[o - sz]);
+      ey = ey + sdz * (Bx[o] - Bx[o - sz]);
+      T ez = E3[o] + aph1 * (By[o] - By[o - 1]) - sdy * (Bx[o] - Bx[o - sy]) + aph2 * (By[o + 1] - By[o - 2]);
+      E1[o] = ex - ompe * (djc1 * j1);
+      E2[o] = ey - ompe * (djc2 * j2);
+      E3[o] = ez - ompe * (djc3 * j3);
+    }
+  }
+}
+
+template <typename T>
+void yee_t(T* ebf, const T* jc, const T* jlo, const Geo& g, const YeeC& c, cudaStream_t st, int sms) {
+  long long cells = (long long)(g.ix2 - g.ix1 + 1) * (g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1);
+  long long faces = (long long)(g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1) + (long long)(g.ix2 - g.ix1 + 1) * (g.kz2 - g.kz1 + 1) +
+                    (g.ndim == 3 ? (long long)(g.ix2 - g.ix1 + 1) * (g.jy2 - g.jy1 + 1) : 0);
+  int gf = grid_for(faces, 256, sms);
+  int gc = grid_for(cells, 256, sms, 16);
+  double dt = c.dt, dth = 0.5 * dt;
+  k_ef_bds<T><<<gf, 256, 0, st>>>(ebf, g, c, 0.0);
+  if (g.ndim == 3) k_rote<T, 3><<<gc, 256, 0, st>>>(ebf, g, c, dth); else k_rote<T, 2><<<gc, 256, 0, st>>>(ebf, g, c, dth);
+  k_bf_bds<T><<<gf, 256, 0, st>>>(ebf, g, c, dt);
+  if (g.ndim == 3) k_rotb_j<T, 3><<<gc, 256, 0, st>>>(ebf, jc, jlo, g, c, dt); else k_rotb_j<T, 2><<<gc, 256, 0, st>>>(ebf, jc, jlo, g, c, dt);
+  k_ef_bds<T><<<gf, 256, 0, st>>>(ebf, g, c, dt);
+  if (g.ndim == 3) k_rote<T, 3><<<gc, 256, 0, st>>>(ebf, g, c, dth); else k_rote<T, 2><<<gc, 256, 0, st>>>(ebf, g, c, dth);
+}
+
+}  // namespace agpu

@@ -1,0 +1,261 @@
+/*
+ * aladyn_gpu.h — C-ABI of the B200 (sm_100a) laser-plasma PIC step library.
+ *
+ * The library runs ALaDyn's per-timestep particle-in-cell cycle on one GPU:
+ * field gather (staggered quadratic/linear shapes), the exact-gamma Boris
+ * push, Esirkepov charge-conserving current deposition, the leapfrog Yee
+ * update with first-order open boundaries, ADK field ionization and the
+ * moving window.  Particle and field arrays stay resident in device memory
+ * between calls; only the arrays the host asks for come back.
+ *
+ * Every entry point is plain C: pointers, sizes and POD structs.  Arrays use
+ * the reference's Fortran layouts so that a Fortran host can pass its own
+ * allocatables through ISO_C_BINDING without copies on its side:
+ *
+ *   ebf(n1p, n2p, n3p, nfield)  column-major FP64, n1p = nx+5, n2p = ny+5,
+ *                               n3p = nz+5 (3D) or 1 (2D); interior nodes are
+ *                               the Fortran indices 3..nx+2 (ix1..ix2) etc.
+ *                               (src/work/array_alloc.f90:56-83,
+ *                                src/grid/set_grid_param.f90:811-829)
+ *   part(ld, ndv)               column-major FP64 particle records,
+ *                               2D: x, y, px, py, wgh_cmp        (ndv = 5)
+ *                               3D: x, y, z, px, py, pz, wgh_cmp (ndv = 7)
+ *                               (src/work/pstruct_data.f90, array_alloc.f90)
+ *   wgh_cmp                     the FP64 slot that packs, little-endian,
+ *                               int16 charge | int16 part_ind | float32 wgh
+ *                               (src/work/precision_def.F90:33-40)
+ *
+ * Every call returns an int status: 0 = success, the reference's own `ier`
+ * codes where they apply (2 = window shift error, 99 = particle count
+ * mismatch) and the AGPU_E* codes below otherwise.  No call exits or aborts.
+ * One host thread drives one handle; each handle owns one CUDA stream.
+ */
+#ifndef ALADYN_GPU_H
+#define ALADYN_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define AGPU_OK 0
+#define AGPU_E_WINDOW 2          /* window shift larger than the box (window.f90:310-315) */
+#define AGPU_E_COUNT 99          /* particle count mismatch (mpi_part_interface.f90:572)  */
+#define AGPU_E_ARG 101           /* invalid argument / unsupported configuration           */
+#define AGPU_E_CUDA 102          /* a CUDA runtime call failed                             */
+#define AGPU_E_NOMEM 103         /* device allocation failed                               */
+#define AGPU_E_CAPACITY 104      /* a species outgrew its particle capacity                */
+#define AGPU_E_INDEX 105         /* a particle stencil left the field array                */
+#define AGPU_E_IONZ_INDEX 106    /* ionization table index beyond n_ge + 1 (clamped)       */
+#define AGPU_E_NONFINITE 107     /* non-finite momentum after the push                     */
+#define AGPU_E_NODEVICE 108      /* no CUDA device / extension not usable                  */
+#define AGPU_E_STATE 109         /* call out of order (e.g. step before fields are set)    */
+
+/* ---- precision forms --------------------------------------------------- */
+#define AGPU_FP64 0              /* plain FP64, the reference's arithmetic order          */
+#define AGPU_FP32_SPLIT 1        /* FP32 bulk, positions = int cell + FP32 offset,
+                                    compensated FP32 current accumulation                 */
+
+/* ---- device error word bits (agpu_step_out.error_bits) ----------------- */
+#define AGPU_EBIT_INDEX 1u
+#define AGPU_EBIT_IONZ_INDEX 2u
+#define AGPU_EBIT_NONFINITE 4u
+#define AGPU_EBIT_CAPACITY 8u
+
+/* Simulation parameters: the subset of the reference's common_param /
+ * grid_param module variables that the PIC step reads
+ * (src/work/common_param.f90, src/grid/grid_param.f90,
+ *  derived in src/start/set_init_param.f90:25-414 and
+ *  src/fields/grid_field_param.f90:36-99). Single-domain (one GPU) box. */
+typedef struct agpu_params {
+  int32_t ndim;            /* 2 or 3                                              */
+  int32_t nx, ny, nz;      /* interior cells (nx_loc, ny_loc, nz_loc); nz=1 in 2D */
+  int32_t nfield;          /* 3 in 2D (Ex,Ey,Bz), 6 in 3D (Ex,Ey,Ez,Bx,By,Bz)    */
+  int32_t curr_ndim;       /* 2 in 2D, 3 in 3D                                    */
+  int32_t ibx, iby, ibz;   /* boundary codes; 0 (open) is the supported value     */
+  int32_t iform;           /* 0 or 1: Esirkepov deposition                        */
+  int32_t precision;       /* AGPU_FP64 or AGPU_FP32_SPLIT                        */
+  int32_t nsp;             /* species count, 1..4; species 0 are electrons        */
+  int32_t nsp_run;         /* species that move (1 in the wake regime)            */
+  int32_t w_sh;            /* window shift period in steps (0 = no window)        */
+  int32_t ionz_lev;        /* 0 = no ionization, 1 = one-level ADK                */
+  int32_t n_mol_atoms[4];  /* atoms per molecule of each ion species (ionz_data) */
+  int32_t reserved_i[4];
+  double dx, dy, dz;       /* cell sizes (um)                                     */
+  double dx_inv, dy_inv, dz_inv;
+  double dt;               /* time step (um/c)                                    */
+  double xmn, ymn, zmn;    /* coordinate of interior node ix1 / jy1 / kz1         */
+  double gxmin, gxmax;     /* particle box in x: keep gxmin < x <= gxmax          */
+  double gymin, gymax;
+  double gzmin, gzmax;
+  double xmax;             /* grid x(nx): right end used by window injection      */
+  double se_coeff[2];      /* x-derivative coefficients (1,0) for der_ord = 2     */
+  double djc[3];           /* current normalisation (dx/2,dy/2) or (dx/3,..)      */
+  double ompe;             /* 4 pi r_c n0 1e-3                                    */
+  double lorentz_fact[4];  /* 1/mass per species                                  */
+  double w_speed, wi_time, wf_time;
+  double reserved_d[4];
+  uint64_t seed;           /* Philox key for ionization draws                     */
+  int64_t capacity[4];     /* device particle capacity per species                */
+} agpu_params;
+
+/* Lattice plasma source: a species loaded on a (jittered) lattice of
+ * npx*npy*npz particles per cell, as the reference's multi-layer gas target
+ * loader places particles at (i-1/2)/n inside each cell
+ * (src/IO/init_part_distrib.f90:152-203).  The same lattice feeds the
+ * moving-window injection of new columns (src/dynamics/window.f90:106-184). */
+typedef struct agpu_plasma {
+  int32_t ic;              /* species index (0 = electrons)                       */
+  int32_t npx, npy, npz;   /* particles per cell along x, y, z (npz=1 in 2D)      */
+  int32_t charge;          /* int16 charge stored in the packed slot              */
+  int32_t part_ind;        /* int16 tag stored in the packed slot                 */
+  float wgh;               /* float32 macro weight stored in the packed slot      */
+  float reserved_f;
+  double x_start, x_end;   /* plasma slab in x (um)                               */
+  double y_min, y_max;     /* transverse extent (um)                              */
+  double z_min, z_max;
+  double jitter;           /* jitter in units of the lattice spacing, in [0,1)    */
+  uint64_t seed;           /* Philox key of the jitter                            */
+} agpu_plasma;
+
+/* Linearly polarised (along y) Gaussian laser pulse focused at x = xf,
+ * sampled on the staggered grid (the build's synthetic stand-in for
+ * init_lp_inc0_fields, src/fields/init_grid_fields.f90:992-1386). */
+typedef struct agpu_laser {
+  double a0;               /* normalised amplitude                                */
+  double lam0;             /* wavelength (um)                                     */
+  double w0_y;             /* waist (um)                                          */
+  double tau_fwhm;         /* FWHM duration (um/c)                                */
+  double xc;               /* pulse centre at t = 0 (um)                          */
+  double xf;               /* focus position (um)                                 */
+  double y0, z0;           /* transverse centre                                   */
+} agpu_laser;
+
+typedef struct agpu_step_out {
+  int64_t np[4];           /* particles per species after the step                */
+  int64_t removed[4];      /* particles dropped at the box edges this step        */
+  int64_t injected[4];     /* particles added by the window this step             */
+  int64_t new_electrons;   /* electrons born from ionization this step            */
+  double ion_field_max;    /* max |E| on ions, when refreshed (else -1)           */
+  double xmn;              /* local x origin after the step                       */
+  int32_t nshx;            /* cells shifted by the window this step               */
+  uint32_t error_bits;     /* sticky device error word (AGPU_EBIT_*)              */
+} agpu_step_out;
+
+typedef struct agpu_diag_out {
+  double field_energy[6];  /* sum over interior cells of F^2 * dx*dy*dz           */
+  double max_abs_e;        /* max |E| component over interior cells               */
+  double kin_energy[4];    /* sum w*(gamma-1) per species                         */
+  double charge[4];        /* sum charge*w per species                            */
+  double momentum[4][3];   /* sum w*p per species                                 */
+  int64_t np[4];
+} agpu_diag_out;
+
+/* Per-phase device time, in milliseconds, accumulated by CUDA events on the
+ * handle's stream since the last agpu_reset_timers (enabled by
+ * agpu_set_profiling).  The byte counts are the algorithmic bytes that the
+ * library attributes to each phase (particle records read+written, cells). */
+typedef struct agpu_timers {
+  double ms_push_deposit;  /* fused gather + push + deposit                       */
+  double ms_yee;           /* Yee update incl. boundaries and current fold        */
+  double ms_sort;          /* particle tile sort / compaction                     */
+  double ms_window;        /* window shift + injection                            */
+  double ms_ionize;        /* ion field, ionization draws, electron append        */
+  double ms_other;
+  int64_t launches_push_deposit;
+  int64_t launches_yee;
+  int64_t launches_total;  /* every kernel launched by the library                */
+  int64_t pushes;          /* particle pushes performed                           */
+  int64_t yee_cells;       /* interior cells updated by the Yee kernels           */
+} agpu_timers;
+
+typedef struct agpu_handle agpu_handle;
+
+/* ---- lifecycle --------------------------------------------------------- */
+/* Replaces v_alloc (src/work/array_alloc.f90:56) + the module state that
+ * lpf2_evolve reads (src/dynamics/pic_evolve_in_time.f90:37-109). */
+int agpu_create(const agpu_params* params, agpu_handle** out);
+int agpu_destroy(agpu_handle* h);
+const char* agpu_error_string(int code);
+int agpu_device_count(int* n);
+
+/* ---- state transfer ---------------------------------------------------- */
+/* ebf(n1p,n2p,n3p,nc): the module array ebf (src/work/fstruct_data.f90:27). */
+int agpu_set_fields(agpu_handle* h, const double* ebf, int32_t n1p, int32_t n2p,
+                    int32_t n3p, int32_t nc);
+int agpu_get_fields(agpu_handle* h, double* ebf, int32_t n1p, int32_t n2p,
+                    int32_t n3p, int32_t nc);
+/* jc(n1p,n2p,n3p,curr_ndim) after the last step: the normalised currents
+ * that entered the E update (src/work/fstruct_data.f90:28). */
+int agpu_get_currents(agpu_handle* h, double* jc, int32_t n1p, int32_t n2p,
+                      int32_t n3p, int32_t nc);
+/* spec(ic)%part(1:np, 1:ndv) with leading dimension ld
+ * (src/work/pstruct_data.f90:31). */
+int agpu_set_species(agpu_handle* h, int32_t ic, const double* part, int64_t ld,
+                     int64_t np, int32_t ndv);
+int agpu_get_species(agpu_handle* h, int32_t ic, double* part, int64_t ld,
+                     int64_t* np, int32_t ndv);
+int agpu_get_count(agpu_handle* h, int32_t ic, int64_t* np);
+
+/* ---- initial state generated on the device ------------------------------ */
+/* Lattice loader (pspecies_distribute, src/IO/init_part_distrib.f90:152-203)
+ * and the window injection source (particles_inject, window.f90:106-184). */
+int agpu_set_plasma_source(agpu_handle* h, const agpu_plasma* src);
+int agpu_load_plasma(agpu_handle* h, int32_t ic);
+int agpu_init_laser(agpu_handle* h, const agpu_laser* laser);
+
+/* ---- ionization -------------------------------------------------------- */
+/* Upload w_one_lev(0:n_ge+1, 0:zmax) for ion species ic (>= 1), as built by
+ * set_field_ioniz_wfunction (src/ionization/ionize.f90:38-256), with
+ * de_inv = n_ge / lp_max.  Column-major: index (nk, z) -> nk + (n_ge+2)*z. */
+int agpu_set_ionization_table(agpu_handle* h, int32_t ic, const double* w_one_lev,
+                              int32_t n_ge, int32_t zmax, double de_inv);
+/* ADK parameters so the library can rebuild the table itself when the ion
+ * field exceeds lp_max (pic_evolve_in_time.f90:53-62). */
+int agpu_set_ionization_species(agpu_handle* h, int32_t ic, int32_t atomic_number,
+                                int32_t ion_min, int32_t ion_max, int32_t ionz_model,
+                                double lp_max);
+
+/* ---- the step ---------------------------------------------------------- */
+/* One call of lp_run (src/dynamics/pic_evolve_in_time.f90:113-144):
+ * lpf2_evolve (field boundary extrapolation, ionization, gather, push,
+ * box-edge removal, Esirkepov deposit, current fold, Yee update) and, when
+ * mod(iter, w_sh) == 0 inside [wi_time, wf_time), lp_window_xshift. */
+int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time,
+              agpu_step_out* out);
+/* Host-supplied window injection: append n records to species ic
+ * (add_particles semantics, src/dynamics/window.f90:39-104). */
+int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t ld,
+                       int64_t n, int32_t ndv);
+
+/* ---- diagnostics ------------------------------------------------------- */
+/* FP64 reductions of Envar / energy_momenta
+ * (src/diagnostics/diag_part_and_fields.f90:172-220, 485-719). */
+int agpu_diag(agpu_handle* h, agpu_diag_out* out);
+
+/* ---- profiling --------------------------------------------------------- */
+int agpu_set_profiling(agpu_handle* h, int32_t on);
+int agpu_get_timers(agpu_handle* h, agpu_timers* out);
+int agpu_reset_timers(agpu_handle* h);
+/* The handle's cudaStream_t, for callers that time on the launching stream. */
+int agpu_get_stream(agpu_handle* h, void** stream);
+int agpu_synchronize(agpu_handle* h);
+/* Deterministic mode: the deposit runs its particles in order in one
+ * thread, so every sum happens in the reference's order and the FP64 form
+ * reproduces the reference arithmetic bit for bit (slow; for verification,
+ * the race-free counterpart of the atomic deposit). */
+int agpu_set_deterministic(agpu_handle* h, int32_t on);
+/* Sort interval in steps for the tile sort (0 = never). */
+int agpu_set_sort_interval(agpu_handle* h, int32_t steps);
+/* sizeof of agpu_params, agpu_plasma, agpu_laser, agpu_step_out,
+ * agpu_diag_out, agpu_timers (in that order) into sizes[0..n-1], so that a
+ * binding can check its struct layouts against the library's. */
+int agpu_struct_sizes(int64_t* sizes, int32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ALADYN_GPU_H */

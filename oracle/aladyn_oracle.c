@@ -1,0 +1,1575 @@
+/*
+ * aladyn_oracle.c — CPU FP64 restatement of ALaDyn's per-timestep PIC cycle.
+ *
+ * TEST INFRASTRUCTURE ONLY.  The product (aladyn_b200/, the CUDA library)
+ * never links, loads or calls this file; tests/, the smoke check and
+ * bench.py's CPU baseline use it as the checker.
+ *
+ * parity unpinned: the reference is a Fortran 2003 + MPI + FFTW program that
+ * cannot be compiled in this image (no Fortran compiler, no MPI, no FFTW) and
+ * ships no tests, golden vectors or known-answer data.  This restatement is
+ * pinned instead to the reference's source text, line by line (each function
+ * cites the file:line it follows, paths relative to the ALaDyn project root),
+ * and to the method's own invariants checked in tests/: partition of unity of
+ * every shape set, discrete continuity of the Esirkepov current, vacuum Yee
+ * dispersion, |p| conservation in a pure magnetic field, and the closed-form
+ * one-level ionization probability.
+ *
+ * Arithmetic follows the Fortran statement order with no FMA contraction
+ * (compile with -ffp-contract=off), matching gfortran -O2 on generic x86-64
+ * with -fdefault-real-8; real(sp) roundings of the reference are kept.
+ * Indices are the Fortran 1-based ones, arrays use the Fortran layouts.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/aladyn_gpu.h"
+#include "philox.h"
+
+#define ORA_NGE 10000 /* n_ge, src/ionization/ionz_data.f90:55 */
+
+typedef struct ora_sim {
+  agpu_params p;
+  int n1p, n2p, n3p, ix1, ix2, jy1, jy2, kz1, kz2, ndv, nf, nc;
+  double* ebf;
+  double* jc;
+  double* part[4];
+  int64_t np[4], cap[4];
+  double* ebfp;
+  int64_t ebfp_cap;
+  /* window state (lp_window_xshift saved variables, window.f90:279-280) */
+  double xlapse;
+  int wi1;
+  /* plasma lattice sources (particles_inject, window.f90:106-184) */
+  agpu_plasma src[4];
+  int has_src[4];
+  int64_t nptx[4], sptx_max[4];
+  int npty[4], nptz[4];
+  /* ionization tables w_one_lev(0:n_ge+1, 0:zmax) per ion species */
+  double* wtab[4];
+  int zmax[4];
+  double de_inv[4];
+  double lp_max[4];
+  int at_num[4], ion_min[4], ionz_model[4];
+  int nsp_ionz; /* species index bound: ions 1..nsp_ionz-1 ionize */
+  uint32_t error_bits;
+  int nthreads; /* >1: threaded CPU baseline (per-thread current copies) */
+} ora_sim;
+
+/* ---- layout helpers (Fortran 1-based) ---------------------------------- */
+#define EBF(s, i, j, k, c)                                                            \
+  (s)->ebf[((size_t)(i)-1) +                                                          \
+           (size_t)(s)->n1p * (((size_t)(j)-1) +                                      \
+                               (size_t)(s)->n2p * (((size_t)(k)-1) + (size_t)(s)->n3p * ((size_t)(c)-1)))]
+#define JC(s, i, j, k, c)                                                             \
+  (s)->jc[((size_t)(i)-1) +                                                           \
+          (size_t)(s)->n1p * (((size_t)(j)-1) +                                       \
+                              (size_t)(s)->n2p * (((size_t)(k)-1) + (size_t)(s)->n3p * ((size_t)(c)-1)))]
+#define PART(s, ic, n, c) (s)->part[ic][(size_t)((c)-1) * (size_t)(s)->cap[ic] + (size_t)((n)-1)]
+#define PT(s, n, c) (s)->ebfp[(size_t)((c)-1) * (size_t)(s)->ebfp_cap + (size_t)((n)-1)]
+
+/* packed charge / part_ind / wgh slot (precision_def.F90:33-40) */
+typedef struct {
+  int16_t charge;
+  int16_t part_ind;
+  float wgh;
+} ora_pack;
+static inline ora_pack ora_unpack(double w) {
+  ora_pack r;
+  uint64_t b;
+  memcpy(&b, &w, 8);
+  r.charge = (int16_t)(uint16_t)(b & 0xffffu);
+  r.part_ind = (int16_t)(uint16_t)((b >> 16) & 0xffffu);
+  uint32_t fb = (uint32_t)(b >> 32);
+  memcpy(&r.wgh, &fb, 4);
+  return r;
+}
+static inline double ora_pack_slot(int16_t charge, int16_t part_ind, float wgh) {
+  uint32_t fb;
+  memcpy(&fb, &wgh, 4);
+  uint64_t b = (uint64_t)(uint16_t)charge | ((uint64_t)(uint16_t)part_ind << 16) | ((uint64_t)fb << 32);
+  double w;
+  memcpy(&w, &b, 8);
+  return w;
+}
+
+/* Fortran nint: round half away from zero. */
+static inline int ora_nint(double x) { return (int)lround(x); }
+
+static const double shx = 3.0; /* real(sp) shx = 3., grid_part_lib.f90:32 */
+
+/* ======================================================================== */
+/* lifecycle                                                                */
+/* ======================================================================== */
+ora_sim* ora_create(const agpu_params* p) {
+  ora_sim* s = (ora_sim*)calloc(1, sizeof(ora_sim));
+  if (!s) return NULL;
+  s->p = *p;
+  /* v_alloc: n1p = nxp + ihx with nxp = nx_loc + 2, ihx = 3
+     (src/work/array_alloc.f90:63-71, src/work/pstruct_data.f90:40) */
+  s->n1p = p->nx + 5;
+  s->n2p = p->ny + 5;
+  s->n3p = (p->ndim == 3) ? p->nz + 5 : 1;
+  /* p_ind(1) = min(sh_ix=3, n_loc), p_ind(2) = n_loc + p_ind(1) - 1
+     (set_grid_param.f90:604-609, 811-829) */
+  s->ix1 = 3;
+  s->ix2 = p->nx + 2;
+  s->jy1 = 3;
+  s->jy2 = p->ny + 2;
+  s->kz1 = (p->ndim == 3) ? 3 : 1;
+  s->kz2 = (p->ndim == 3) ? p->nz + 2 : 1;
+  s->ndv = (p->ndim == 3) ? 7 : 5;
+  s->nf = p->nfield;
+  s->nc = p->curr_ndim;
+  size_t ncell = (size_t)s->n1p * s->n2p * s->n3p;
+  s->ebf = (double*)calloc(ncell * s->nf, sizeof(double));
+  s->jc = (double*)calloc(ncell * s->nc, sizeof(double));
+  int64_t maxcap = 1;
+  for (int ic = 0; ic < 4; ++ic) {
+    s->cap[ic] = p->capacity[ic] > 0 ? p->capacity[ic] : 1;
+    if (ic < p->nsp) s->part[ic] = (double*)calloc((size_t)s->cap[ic] * s->ndv, sizeof(double));
+    if (s->cap[ic] > maxcap) maxcap = s->cap[ic];
+  }
+  s->ebfp_cap = maxcap;
+  s->ebfp = (double*)calloc((size_t)maxcap * s->ndv, sizeof(double));
+  s->nsp_ionz = 1;
+  s->nthreads = 1;
+  return s;
+}
+
+void ora_destroy(ora_sim* s) {
+  if (!s) return;
+  free(s->ebf);
+  free(s->jc);
+  for (int ic = 0; ic < 4; ++ic) {
+    free(s->part[ic]);
+    free(s->wtab[ic]);
+  }
+  free(s->ebfp);
+  free(s);
+}
+
+void ora_set_threads(ora_sim* s, int n) { s->nthreads = n > 0 ? n : 1; }
+
+int ora_dims(const ora_sim* s, int* out) {
+  out[0] = s->n1p; out[1] = s->n2p; out[2] = s->n3p;
+  out[3] = s->ix1; out[4] = s->ix2; out[5] = s->jy1; out[6] = s->jy2;
+  out[7] = s->kz1; out[8] = s->kz2; out[9] = s->ndv;
+  return 0;
+}
+
+int ora_set_fields(ora_sim* s, const double* ebf) {
+  memcpy(s->ebf, ebf, sizeof(double) * (size_t)s->n1p * s->n2p * s->n3p * s->nf);
+  return 0;
+}
+int ora_get_fields(const ora_sim* s, double* ebf) {
+  memcpy(ebf, s->ebf, sizeof(double) * (size_t)s->n1p * s->n2p * s->n3p * s->nf);
+  return 0;
+}
+int ora_get_currents(const ora_sim* s, double* jc) {
+  memcpy(jc, s->jc, sizeof(double) * (size_t)s->n1p * s->n2p * s->n3p * s->nc);
+  return 0;
+}
+int ora_set_species(ora_sim* s, int ic, const double* part, int64_t ld, int64_t np) {
+  if (ic < 0 || ic >= s->p.nsp || np > s->cap[ic]) return AGPU_E_ARG;
+  for (int c = 0; c < s->ndv; ++c)
+    memcpy(&s->part[ic][(size_t)c * s->cap[ic]], &part[(size_t)c * ld], sizeof(double) * (size_t)np);
+  s->np[ic] = np;
+  return 0;
+}
+int ora_get_species(const ora_sim* s, int ic, double* part, int64_t ld, int64_t* np) {
+  if (ic < 0 || ic >= s->p.nsp) return AGPU_E_ARG;
+  *np = s->np[ic];
+  if (part)
+    for (int c = 0; c < s->ndv; ++c)
+      memcpy(&part[(size_t)c * ld], &s->part[ic][(size_t)c * s->cap[ic]], sizeof(double) * (size_t)s->np[ic]);
+  return 0;
+}
+int64_t ora_count(const ora_sim* s, int ic) { return s->np[ic]; }
+uint32_t ora_error_bits(const ora_sim* s) { return s->error_bits; }
+double ora_xmn(const ora_sim* s) { return s->p.xmn; }
+
+/* ======================================================================== */
+/* A1: field_xyzbd (src/parallel/mpi_field_interface.f90:53-198), ib = 0     */
+/* ======================================================================== */
+void ora_field_xyzbd(ora_sim* s, int nc) {
+  int i1 = s->ix1, i2 = s->ix2, j1 = s->jy1, j2 = s->jy2, k1 = s->kz1, k2 = s->kz2;
+  /* pex0, ibx < 2 */
+  if (s->p.ibx < 2) {
+    for (int ik = 1; ik <= nc; ++ik)
+      for (int iz = k1; iz <= k2; ++iz)
+        for (int iy = j1; iy <= j2; ++iy)
+          EBF(s, s->ix1 - 1, iy, iz, ik) = 2. * EBF(s, s->ix1, iy, iz, ik) - EBF(s, s->ix1 + 1, iy, iz, ik);
+  }
+  i1 = i1 - 1;
+  if (s->p.ibx == 0) {
+    for (int ik = 1; ik <= nc; ++ik)
+      for (int iz = k1; iz <= k2; ++iz)
+        for (int iy = j1; iy <= j2; ++iy)
+          EBF(s, s->ix2 + 1, iy, iz, ik) = 2. * EBF(s, s->ix2, iy, iz, ik) - EBF(s, s->ix2 - 1, iy, iz, ik);
+  }
+  i2 = i2 + 1;
+  if (s->p.ndim < 2) return;
+  if (s->p.iby == 0) {
+    for (int ik = 1; ik <= nc; ++ik)
+      for (int iz = k1; iz <= k2; ++iz)
+        for (int ix = i1; ix <= i2; ++ix)
+          EBF(s, ix, s->jy1 - 1, iz, ik) = 2. * EBF(s, ix, s->jy1, iz, ik) - EBF(s, ix, s->jy1 + 1, iz, ik);
+  }
+  j1 = j1 - 1;
+  if (s->p.iby == 0) {
+    for (int ik = 1; ik <= nc; ++ik)
+      for (int iz = k1; iz <= k2; ++iz)
+        for (int ix = i1; ix <= i2; ++ix)
+          EBF(s, ix, s->jy2 + 1, iz, ik) = 2. * EBF(s, ix, s->jy2, iz, ik) - EBF(s, ix, s->jy2 - 1, iz, ik);
+  }
+  j2 = j2 + 1;
+  if (s->p.ndim < 3) return;
+  if (s->p.ibz == 0) {
+    for (int ik = 1; ik <= nc; ++ik)
+      for (int iy = j1; iy <= j2; ++iy)
+        for (int ix = i1; ix <= i2; ++ix)
+          EBF(s, ix, iy, s->kz1 - 1, ik) = 2 * EBF(s, ix, iy, s->kz1, ik) - EBF(s, ix, iy, s->kz1 + 1, ik);
+    for (int ik = 1; ik <= nc; ++ik)
+      for (int iy = j1; iy <= j2; ++iy)
+        for (int ix = i1; ix <= i2; ++ix)
+          EBF(s, ix, iy, s->kz2 + 1, ik) = 2 * EBF(s, ix, iy, s->kz2, ik) - EBF(s, ix, iy, s->kz2 - 1, ik);
+  }
+}
+
+/* ======================================================================== */
+/* A3 / A10 / qqh: spline shapes (src/particles/grid_part_lib.f90)          */
+/* ======================================================================== */
+/* qlh per dimension (qlh_2d_spline 110-143, qlh_3d_spline 212-259):
+   quadratic weights on integer nodes, linear on half nodes; ix-1. */
+static inline void ora_qlh_1d(double xp, double ax[3], double axh[2], int* ix) {
+  double xx = shx + xp;
+  int i = (int)(xx + 0.5);
+  double sx = xx - (double)i;
+  double sx2 = sx * sx;
+  ax[1] = 0.75 - sx2;
+  ax[2] = 0.5 * (0.25 + sx2 + sx);
+  ax[0] = 1. - ax[1] - ax[2];
+  axh[1] = sx + 0.5;
+  axh[0] = 1. - axh[1];
+  *ix = i - 1;
+}
+/* qqh per dimension (qqh_2d_spline 170-210, qqh_3d_spline 261-320). */
+static inline void ora_qqh_1d(double xp, double ax[3], double axh[3], int* ix, int* ihx) {
+  double xx = shx + xp;
+  int i = (int)(xx + 0.5);
+  double sx = xx - (double)i;
+  double sx2 = sx * sx;
+  ax[1] = 0.75 - sx2;
+  ax[2] = 0.5 * (0.25 + sx2 + sx);
+  ax[0] = 1. - ax[1] - ax[2];
+  int ih = (int)(xx);
+  sx = xx - (double)ih - 0.5;
+  sx2 = sx * sx;
+  axh[1] = 0.75 - sx2;
+  axh[2] = 0.5 * (0.25 + sx2 + sx);
+  axh[0] = 1. - axh[1] - axh[2];
+  *ix = i - 1;
+  *ihx = ih - 1;
+}
+/* qden per dimension (qden_2d_wgh 337-358, qden_3d_wgh 388-417): no ix-1. */
+static inline void ora_qden_1d(double xp, double ax[3], int* ix) {
+  double xx = shx + xp;
+  int i = (int)(xx + 0.5);
+  double sx = xx - (double)i;
+  double sx2 = sx * sx;
+  ax[1] = 0.75 - sx2;
+  ax[2] = 0.5 * (0.25 + sx2 + sx);
+  ax[0] = 1. - ax[1] - ax[2];
+  *ix = i;
+}
+
+/* Exported for the shape invariant tests. */
+void ora_shape_qlh(double xp, double* ax3, double* axh2, int* ix) { ora_qlh_1d(xp, ax3, axh2, ix); }
+void ora_shape_qqh(double xp, double* ax3, double* axh3, int* ix, int* ih) { ora_qqh_1d(xp, ax3, axh3, ix, ih); }
+void ora_shape_qden(double xp, double* ax3, int* ix) { ora_qden_1d(xp, ax3, ix); }
+
+/* ======================================================================== */
+/* A2 + A4/A5: gather (set_part2d_hcell_acc grid_part_connect.f90:89-185,    */
+/* set_part3d_hcell_acc 187-285) with set_local_*_positions (lib 458-519)   */
+/* ======================================================================== */
+static void ora_gather(ora_sim* s, int ic, int64_t np) {
+  const agpu_params* p = &s->p;
+  if (p->ndim == 2) {
+    for (int64_t n = 1; n <= np; ++n) {
+      double xl = p->dx_inv * (PART(s, ic, n, 1) - p->xmn);
+      double yl = p->dy_inv * (PART(s, ic, n, 2) - p->ymn);
+      double ax1[3], axh[2], ay1[3], ayh[2];
+      int i, j;
+      ora_qlh_1d(xl, ax1, axh, &i);
+      ora_qlh_1d(yl, ay1, ayh, &j);
+      int ih = i, jh = j;
+      double ap1 = 0., ap2 = 0., ap3 = 0.;
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = j + j1;
+        double dvol = ay1[j1];
+        for (int i1 = 0; i1 <= 1; ++i1) {
+          int i2 = i1 + ih;
+          double dvol1 = axh[i1] * dvol;
+          ap1 = ap1 + dvol1 * EBF(s, i2, j2, 1, 1);
+        }
+      }
+      for (int j1 = 0; j1 <= 1; ++j1) {
+        int j2 = jh + j1;
+        double dvol = ayh[j1];
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          int i2 = i + i1;
+          double dvol1 = ax1[i1] * dvol;
+          ap2 = ap2 + dvol1 * EBF(s, i2, j2, 1, 2);
+        }
+        for (int i1 = 0; i1 <= 1; ++i1) {
+          int i2 = i1 + ih;
+          double dvol1 = axh[i1] * dvol;
+          ap3 = ap3 + dvol1 * EBF(s, i2, j2, 1, 3);
+        }
+      }
+      PT(s, n, 1) = ap1;
+      PT(s, n, 2) = ap2;
+      PT(s, n, 3) = ap3;
+    }
+    return;
+  }
+  for (int64_t n = 1; n <= np; ++n) {
+    double xl = p->dx_inv * (PART(s, ic, n, 1) - p->xmn);
+    double yl = p->dy_inv * (PART(s, ic, n, 2) - p->ymn);
+    double zl = p->dz_inv * (PART(s, ic, n, 3) - p->zmn);
+    double ax1[3], axh[2], ay1[3], ayh[2], az1[3], azh[2];
+    int i, j, k;
+    ora_qlh_1d(xl, ax1, axh, &i);
+    ora_qlh_1d(yl, ay1, ayh, &j);
+    ora_qlh_1d(zl, az1, azh, &k);
+    int ih = i, jh = j, kh = k;
+    double ap[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int k1 = 0; k1 <= 2; ++k1) {
+      int k2 = k + k1;
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = j + j1;
+        double dvol = ay1[j1] * az1[k1];
+        for (int i1 = 0; i1 <= 1; ++i1) {
+          int i2 = i1 + ih;
+          ap[1] = ap[1] + axh[i1] * dvol * EBF(s, i2, j2, k2, 1);
+        }
+      }
+      for (int j1 = 0; j1 <= 1; ++j1) {
+        int j2 = jh + j1;
+        double dvol = ayh[j1] * az1[k1];
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          int i2 = i + i1;
+          ap[2] = ap[2] + ax1[i1] * dvol * EBF(s, i2, j2, k2, 2);
+        }
+        for (int i1 = 0; i1 <= 1; ++i1) {
+          int i2 = i1 + ih;
+          ap[6] = ap[6] + axh[i1] * dvol * EBF(s, i2, j2, k2, 6);
+        }
+      }
+    }
+    for (int k1 = 0; k1 <= 1; ++k1) {
+      int k2 = kh + k1;
+      for (int j1 = 0; j1 <= 1; ++j1) {
+        int j2 = jh + j1;
+        double dvol = ayh[j1] * azh[k1];
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          int i2 = i1 + i;
+          ap[4] = ap[4] + ax1[i1] * dvol * EBF(s, i2, j2, k2, 4);
+        }
+      }
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = j + j1;
+        double dvol = ay1[j1] * azh[k1];
+        for (int i1 = 0; i1 <= 1; ++i1) {
+          int i2 = ih + i1;
+          ap[5] = ap[5] + axh[i1] * dvol * EBF(s, i2, j2, k2, 5);
+        }
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          int i2 = i1 + i;
+          ap[3] = ap[3] + ax1[i1] * dvol * EBF(s, i2, j2, k2, 3);
+        }
+      }
+    }
+    for (int c = 1; c <= 6; ++c) PT(s, n, c) = ap[c];
+  }
+}
+
+/* A6: field_charge_multiply (src/dynamics/curr_and_fields_util.f90:58-72) */
+static void ora_field_charge_multiply(ora_sim* s, int ic, int64_t np) {
+  int ch = s->ndv;
+  for (int64_t n = 1; n <= np; ++n) {
+    ora_pack w = ora_unpack(PART(s, ic, n, ch));
+    double q = (double)w.charge;
+    for (int c = 1; c <= s->nf; ++c) PT(s, n, c) = q * PT(s, n, c);
+  }
+}
+
+/* A7: init_lpf_momenta (src/dynamics/boris_push.f90:34-73) */
+static void ora_init_lpf_momenta(ora_sim* s, int ic, int64_t np) {
+  double dth_lp = 0.5 * s->p.dt;
+  double alp = dth_lp * s->p.lorentz_fact[ic];
+  if (s->p.curr_ndim == 2) {
+    for (int64_t p = 1; p <= np; ++p) {
+      double efp[3];
+      for (int c = 0; c < 3; ++c) efp[c] = -alp * PT(s, p, c + 1);
+      double pp1 = PART(s, ic, p, 3), pp2 = PART(s, ic, p, 4);
+      double gam2 = 1. + (pp1 * pp1 + pp2 * pp2);
+      double gam_inv = 1. / sqrt(gam2);
+      double vp1 = pp1 * gam_inv, vp2 = pp2 * gam_inv;
+      PART(s, ic, p, 3) = PART(s, ic, p, 3) + efp[0] + vp2 * efp[2];
+      PART(s, ic, p, 4) = PART(s, ic, p, 4) + efp[1] - vp1 * efp[2];
+    }
+    return;
+  }
+  for (int64_t p = 1; p <= np; ++p) {
+    double pp[3] = {PART(s, ic, p, 4), PART(s, ic, p, 5), PART(s, ic, p, 6)};
+    double efp[6];
+    for (int c = 0; c < 6; ++c) efp[c] = -alp * PT(s, p, c + 1);
+    double gam2 = 1. + (pp[0] * pp[0] + pp[1] * pp[1] + pp[2] * pp[2]);
+    double gam_inv = 1. / sqrt(gam2);
+    double vp[3] = {gam_inv * pp[0], gam_inv * pp[1], gam_inv * pp[2]};
+    PART(s, ic, p, 4) = PART(s, ic, p, 4) + efp[0] + vp[1] * efp[5] - vp[2] * efp[4];
+    PART(s, ic, p, 5) = PART(s, ic, p, 5) + efp[1] + vp[2] * efp[3] - vp[0] * efp[5];
+    PART(s, ic, p, 6) = PART(s, ic, p, 6) + efp[2] + vp[0] * efp[4] - vp[1] * efp[3];
+  }
+}
+
+/* A8: lpf_momenta_and_positions (src/dynamics/boris_push.f90:75-168) */
+static void ora_push(ora_sim* s, int ic, int64_t np) {
+  double dt_lp = s->p.dt;
+  double dth_lp = 0.5 * dt_lp;
+  double alp = dth_lp * s->p.lorentz_fact[ic];
+  int ch;
+  if (s->p.curr_ndim == 2) {
+    ch = 5;
+    for (int64_t p = 1; p <= np; ++p) {
+      double pp1 = PART(s, ic, p, 3), pp2 = PART(s, ic, p, 4);
+      double efp1 = alp * PT(s, p, 1), efp2 = alp * PT(s, p, 2), efp3 = alp * PT(s, p, 3);
+      double vp1 = pp1 + efp1, vp2 = pp2 + efp2, vp3 = efp3;
+      double gam02 = 1. + (vp1 * vp1 + vp2 * vp2);
+      double b2 = vp3 * vp3;
+      gam02 = gam02 - b2;
+      double gam2 = 0.5 * (gam02 + sqrt(gam02 * gam02 + 4. * b2));
+      double gam = sqrt(gam2);
+      double vph1 = gam2 * vp1 + gam * vp2 * vp3;
+      double vph2 = gam2 * vp2 - gam * vp1 * vp3;
+      vph1 = vph1 / (gam2 + b2);
+      vph2 = vph2 / (gam2 + b2);
+      PART(s, ic, p, 3) = 2. * vph1 - pp1;
+      PART(s, ic, p, 4) = 2. * vph2 - pp2;
+      PT(s, p, 3) = PART(s, ic, p, 1);
+      PT(s, p, 4) = PART(s, ic, p, 2);
+      pp1 = PART(s, ic, p, 3);
+      pp2 = PART(s, ic, p, 4);
+      gam2 = 1. + (pp1 * pp1 + pp2 * pp2);
+      PT(s, p, 5) = dt_lp / sqrt(gam2);
+      vp1 = PT(s, p, 5) * pp1;
+      vp2 = PT(s, p, 5) * pp2;
+      PT(s, p, 1) = vp1;
+      PT(s, p, 2) = vp2;
+      PART(s, ic, p, 1) = PART(s, ic, p, 1) + vp1;
+      PART(s, ic, p, 2) = PART(s, ic, p, 2) + vp2;
+    }
+  } else {
+    ch = 7;
+    for (int64_t p = 1; p <= np; ++p) {
+      double pp[3] = {PART(s, ic, p, 4), PART(s, ic, p, 5), PART(s, ic, p, 6)};
+      double efp[6];
+      for (int c = 0; c < 6; ++c) efp[c] = alp * PT(s, p, c + 1);
+      double vp[3] = {pp[0] + efp[0], pp[1] + efp[1], pp[2] + efp[2]};
+      double bb[3] = {efp[3], efp[4], efp[5]};
+      double gam02 = 1. + (vp[0] * vp[0] + vp[1] * vp[1] + vp[2] * vp[2]);
+      double b2 = bb[0] * bb[0] + bb[1] * bb[1] + bb[2] * bb[2];
+      double bv = bb[0] * vp[0] + bb[1] * vp[1] + bb[2] * vp[2];
+      gam02 = gam02 - b2;
+      double gam2 = 0.5 * (gam02 + sqrt(gam02 * gam02 + 4. * (b2 + bv * bv)));
+      double gam = sqrt(gam2);
+      double vph[3];
+      for (int c = 0; c < 3; ++c) vph[c] = gam2 * vp[c] + bb[c] * bv;
+      vph[0] = vph[0] + gam * (vp[1] * bb[2] - vp[2] * bb[1]);
+      vph[1] = vph[1] + gam * (vp[2] * bb[0] - vp[0] * bb[2]);
+      vph[2] = vph[2] + gam * (vp[0] * bb[1] - vp[1] * bb[0]);
+      for (int c = 0; c < 3; ++c) vph[c] = vph[c] / (b2 + gam2);
+      for (int c = 0; c < 3; ++c) PART(s, ic, p, 4 + c) = 2. * vph[c] - pp[c];
+      for (int c = 0; c < 3; ++c) PT(s, p, 4 + c) = PART(s, ic, p, 1 + c);
+      for (int c = 0; c < 3; ++c) pp[c] = PART(s, ic, p, 4 + c);
+      gam2 = 1. + (pp[0] * pp[0] + pp[1] * pp[1] + pp[2] * pp[2]);
+      PT(s, p, 7) = dt_lp / sqrt(gam2);
+      for (int c = 0; c < 3; ++c) vp[c] = PT(s, p, 7) * pp[c];
+      for (int c = 0; c < 3; ++c) PT(s, p, 1 + c) = vp[c];
+      for (int c = 0; c < 3; ++c) PART(s, ic, p, 1 + c) = PART(s, ic, p, 1 + c) + vp[c];
+    }
+  }
+  if (s->p.iform < 2)
+    for (int64_t p = 1; p <= np; ++p) PT(s, p, ch) = PART(s, ic, p, ch);
+}
+
+/* A9: cell_part_dist(.false.) single domain -> reset_all_part_dist
+   (src/parallel/mpi_part_interface.f90:467-523, 525-753): stable removal of
+   particles outside (gmin, gmax] along x, then y, then z; spec and ebfp
+   compacted together. Returns the number removed. */
+static int64_t ora_reset_dist(ora_sim* s, int ic, int cin, double xl, double xr, int with_pt) {
+  int64_t np = s->np[ic], pout = 0;
+  for (int64_t n = 1; n <= np; ++n) {
+    double xp = PART(s, ic, n, cin);
+    if (xp <= xl) pout++;
+    if (xp > xr) pout++;
+  }
+  if (pout == 0) return 0;
+  int64_t q = 0;
+  for (int64_t n = 1; n <= np; ++n) {
+    double xp = PART(s, ic, n, cin);
+    if (xp > xl && xp <= xr) {
+      q++;
+      if (q != n) {
+        for (int c = 1; c <= s->ndv; ++c) PART(s, ic, q, c) = PART(s, ic, n, c);
+        if (with_pt)
+          for (int c = 1; c <= s->ndv; ++c) PT(s, q, c) = PT(s, n, c);
+      }
+    }
+  }
+  s->np[ic] = q;
+  return np - q;
+}
+
+static int64_t ora_cell_part_dist_step(ora_sim* s, int ic) {
+  int64_t r = 0;
+  r += ora_reset_dist(s, ic, 1, s->p.gxmin, s->p.gxmax, 1);
+  r += ora_reset_dist(s, ic, 2, s->p.gymin, s->p.gymax, 1);
+  if (s->p.ndim > 2) r += ora_reset_dist(s, ic, 3, s->p.gzmin, s->p.gzmax, 1);
+  return r;
+}
+
+/* ======================================================================== */
+/* A11/A12: Esirkepov deposit (grid_part_connect.f90:956-1334)              */
+/* ======================================================================== */
+static void ora_esirkepov_2d_one(ora_sim* s, double* jc, const double xp1[2], const double xp0[2],
+                                 float wght) {
+  double ax0[3], ay0[3], ax1[3], ay1[3];
+  double axh[5], ayh[5], currx[5], curry[5];
+  int i, j, ii0, jj0;
+  ora_qden_1d(xp0[0], ax0, &ii0);
+  ora_qden_1d(xp0[1], ay0, &jj0);
+  ora_qden_1d(xp1[0], ax1, &i);
+  ora_qden_1d(xp1[1], ay1, &j);
+  for (int q = 0; q < 5; ++q) axh[q] = 0.;
+  int ih = i - ii0 + 1;
+  for (int i1 = 0; i1 <= 2; ++i1) axh[ih + i1] = ax1[i1];
+  currx[0] = -axh[0];
+  for (int i1 = 1; i1 <= 3; ++i1) currx[i1] = currx[i1 - 1] + ax0[i1 - 1] - axh[i1];
+  currx[4] = currx[3] - axh[4];
+  for (int i1 = 1; i1 <= 3; ++i1) axh[i1] = axh[i1] + ax0[i1 - 1];
+  for (int q = 0; q < 5; ++q) currx[q] = (double)wght * currx[q];
+  int x0 = ih < 1 ? ih : 1;
+  int x1 = (ih + 2) > 3 ? ih + 2 : 3;
+  int jh = j - jj0 + 1;
+  for (int q = 0; q < 5; ++q) ayh[q] = 0.;
+  for (int i1 = 0; i1 <= 2; ++i1) ayh[jh + i1] = ay1[i1];
+  curry[0] = -ayh[0];
+  for (int i1 = 1; i1 <= 3; ++i1) curry[i1] = curry[i1 - 1] + ay0[i1 - 1] - ayh[i1];
+  curry[4] = curry[3] - ayh[4];
+  for (int q = 0; q < 5; ++q) curry[q] = (double)wght * curry[q];
+  for (int i1 = 1; i1 <= 3; ++i1) ayh[i1] = ayh[i1] + ay0[i1 - 1];
+  int y0 = jh < 1 ? jh : 1;
+  int y1 = (jh + 2) > 3 ? jh + 2 : 3;
+  jj0 = jj0 - 1;
+  j = j - 1;
+  jh = jj0 - 1;
+  i = i - 1;
+  ii0 = ii0 - 1;
+  ih = ii0 - 1;
+  size_t n1p = (size_t)s->n1p, n2p = (size_t)s->n2p;
+  size_t comp = n1p * n2p * (size_t)s->n3p;
+  for (int j1 = y0; j1 <= y1; ++j1) {
+    int j2 = jh + j1;
+    for (int i1 = x0; i1 <= x1; ++i1) {
+      int i2 = ih + i1;
+      size_t o = (size_t)(i2 - 1) + n1p * (size_t)(j2 - 1);
+      jc[o] = jc[o] + ayh[j1] * currx[i1];
+    }
+  }
+  for (int j1 = y0; j1 <= y1; ++j1) {
+    int j2 = jh + j1;
+    for (int i1 = x0; i1 <= x1; ++i1) {
+      int i2 = ih + i1;
+      size_t o = comp + (size_t)(i2 - 1) + n1p * (size_t)(j2 - 1);
+      jc[o] = jc[o] + axh[i1] * curry[j1];
+    }
+  }
+}
+
+static void ora_esirkepov_3d_one(ora_sim* s, double* jc, const double xp1[3], const double xp0[3],
+                                 float wght) {
+  double ax0[3], ay0[3], az0[3], ax1[3], ay1[3], az1[3];
+  double axh[5], ayh[5], azh[5], axh0[5], axh1[5], ayh0[5], ayh1[5];
+  double currx[5], curry[5], currz[5];
+  int i, j, k, ii0, jj0, kk0;
+  ora_qden_1d(xp0[0], ax0, &ii0);
+  ora_qden_1d(xp0[1], ay0, &jj0);
+  ora_qden_1d(xp0[2], az0, &kk0);
+  ora_qden_1d(xp1[0], ax1, &i);
+  ora_qden_1d(xp1[1], ay1, &j);
+  ora_qden_1d(xp1[2], az1, &k);
+
+  for (int q = 0; q < 5; ++q) axh[q] = 0.;
+  int ih = i - ii0 + 1;
+  for (int i1 = 0; i1 <= 2; ++i1) axh[ih + i1] = ax1[i1];
+  currx[0] = -axh[0];
+  for (int i1 = 1; i1 <= 3; ++i1) currx[i1] = currx[i1 - 1] + ax0[i1 - 1] - axh[i1];
+  currx[4] = currx[3] - axh[4];
+  for (int q = 0; q < 5; ++q) currx[q] = (double)wght * currx[q];
+  for (int q = 0; q < 5; ++q) {
+    axh0[q] = 0.5 * axh[q];
+    axh1[q] = axh[q];
+  }
+  for (int i1 = 1; i1 <= 3; ++i1) {
+    axh0[i1] = axh0[i1] + ax0[i1 - 1];
+    axh1[i1] = axh1[i1] + 0.5 * ax0[i1 - 1];
+  }
+  int x0 = ih < 1 ? ih : 1;
+  int x1 = (ih + 2) > 3 ? ih + 2 : 3;
+  i = i - 1;
+  ii0 = ii0 - 1;
+
+  int jh = j - jj0 + 1;
+  for (int q = 0; q < 5; ++q) ayh[q] = 0.;
+  for (int i1 = 0; i1 <= 2; ++i1) ayh[jh + i1] = ay1[i1];
+  curry[0] = -ayh[0];
+  for (int i1 = 1; i1 <= 3; ++i1) curry[i1] = curry[i1 - 1] + ay0[i1 - 1] - ayh[i1];
+  curry[4] = curry[3] - ayh[4];
+  for (int q = 0; q < 5; ++q) curry[q] = (double)wght * curry[q];
+  for (int q = 0; q < 5; ++q) {
+    ayh0[q] = 0.5 * ayh[q];
+    ayh1[q] = ayh[q];
+  }
+  for (int i1 = 1; i1 <= 3; ++i1) {
+    ayh0[i1] = ayh0[i1] + ay0[i1 - 1];
+    ayh1[i1] = ayh1[i1] + 0.5 * ay0[i1 - 1];
+  }
+  int y0 = jh < 1 ? jh : 1;
+  int y1 = (jh + 2) > 3 ? jh + 2 : 3;
+  jj0 = jj0 - 1;
+  j = j - 1;
+
+  int kh = k - kk0 + 1;
+  for (int q = 0; q < 5; ++q) azh[q] = 0.;
+  for (int i1 = 0; i1 <= 2; ++i1) azh[kh + i1] = az1[i1];
+  currz[0] = -azh[0];
+  for (int i1 = 1; i1 <= 3; ++i1) currz[i1] = currz[i1 - 1] + az0[i1 - 1] - azh[i1];
+  currz[4] = currz[3] - azh[4];
+  for (int q = 0; q < 5; ++q) currz[q] = (double)wght * currz[q];
+  kk0 = kk0 - 1;
+  k = k - 1;
+  int z0 = kh < 1 ? kh : 1;
+  int z1 = (kh + 2) > 3 ? kh + 2 : 3;
+
+  size_t n1p = (size_t)s->n1p, n2p = (size_t)s->n2p, n3p = (size_t)s->n3p;
+  size_t comp = n1p * n2p * n3p;
+#define JIX(i2, j2, k2, c) ((size_t)((i2)-1) + n1p * ((size_t)((j2)-1) + n2p * (size_t)((k2)-1)) + comp * (size_t)(c))
+  jh = jj0 - 1;
+  ih = ii0 - 1;
+  for (int k1 = 0; k1 <= 2; ++k1) {
+    for (int j1 = y0; j1 <= y1; ++j1) {
+      int j2 = jh + j1;
+      double dvol = ayh0[j1] * az0[k1];
+      double dvolh = ayh1[j1] * az1[k1];
+      for (int i1 = x0; i1 <= x1; ++i1) {
+        int i2 = ih + i1;
+        size_t o0 = JIX(i2, j2, kk0 + k1, 0), o1 = JIX(i2, j2, k + k1, 0);
+        jc[o0] = jc[o0] + dvol * currx[i1];
+        jc[o1] = jc[o1] + dvolh * currx[i1];
+      }
+    }
+  }
+  for (int k1 = 0; k1 <= 2; ++k1) {
+    for (int j1 = y0; j1 <= y1; ++j1) {
+      int j2 = jh + j1;
+      double dvol = curry[j1] * az0[k1];
+      double dvolh = curry[j1] * az1[k1];
+      for (int i1 = x0; i1 <= x1; ++i1) {
+        int i2 = ih + i1;
+        size_t o0 = JIX(i2, j2, kk0 + k1, 1), o1 = JIX(i2, j2, k + k1, 1);
+        jc[o0] = jc[o0] + axh0[i1] * dvol;
+        jc[o1] = jc[o1] + axh1[i1] * dvolh;
+      }
+    }
+  }
+  kh = kk0 - 1;
+  for (int k1 = z0; k1 <= z1; ++k1) {
+    int k2 = kh + k1;
+    for (int j1 = 0; j1 <= 2; ++j1) {
+      double dvol = ay0[j1] * currz[k1];
+      double dvolh = ay1[j1] * currz[k1];
+      for (int i1 = x0; i1 <= x1; ++i1) {
+        int i2 = ih + i1;
+        size_t o0 = JIX(i2, jj0 + j1, k2, 2), o1 = JIX(i2, j + j1, k2, 2);
+        jc[o0] = jc[o0] + axh0[i1] * dvol;
+        jc[o1] = jc[o1] + axh1[i1] * dvolh;
+      }
+    }
+  }
+#undef JIX
+}
+
+/* curr_accumulate -> esirkepov_{2,3}d_curr with the set_local_positions
+   preamble (curr_and_fields_util.f90:74-102; grid_part_connect.f90:979-987,
+   1201-1208): new positions from part, old positions from ebfp, weight
+   wght = real(charge*wgh, sp). */
+static void ora_curr_accumulate(ora_sim* s, int ic, int64_t np) {
+  const agpu_params* p = &s->p;
+  int nth = s->nthreads;
+  size_t jsz = (size_t)s->n1p * s->n2p * s->n3p * s->nc;
+  double** priv = NULL;
+  if (nth > 1) {
+    priv = (double**)calloc((size_t)nth, sizeof(double*));
+    for (int t = 1; t < nth; ++t) priv[t] = (double*)calloc(jsz, sizeof(double));
+    priv[0] = s->jc;
+  }
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nth) if (nth > 1)
+#endif
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    double* jc = (nth > 1) ? priv[tid] : s->jc;
+    int64_t lo = 1, hi = np;
+    if (nth > 1) {
+      int64_t chunk = (np + nth - 1) / nth;
+      lo = 1 + (int64_t)tid * chunk;
+      hi = lo + chunk - 1;
+      if (hi > np) hi = np;
+    }
+    for (int64_t n = lo; n <= hi; ++n) {
+      ora_pack w = ora_unpack(PART(s, ic, n, s->ndv));
+      float wght = (float)w.charge * w.wgh;
+      if (p->ndim == 2) {
+        double xp1[2] = {p->dx_inv * (PART(s, ic, n, 1) - p->xmn), p->dy_inv * (PART(s, ic, n, 2) - p->ymn)};
+        double xp0[2] = {p->dx_inv * (PT(s, n, 3) - p->xmn), p->dy_inv * (PT(s, n, 4) - p->ymn)};
+        ora_esirkepov_2d_one(s, jc, xp1, xp0, wght);
+      } else {
+        double xp1[3] = {p->dx_inv * (PART(s, ic, n, 1) - p->xmn), p->dy_inv * (PART(s, ic, n, 2) - p->ymn),
+                         p->dz_inv * (PART(s, ic, n, 3) - p->zmn)};
+        double xp0[3] = {p->dx_inv * (PT(s, n, 4) - p->xmn), p->dy_inv * (PT(s, n, 5) - p->ymn),
+                         p->dz_inv * (PT(s, n, 6) - p->zmn)};
+        ora_esirkepov_3d_one(s, jc, xp1, xp0, wght);
+      }
+    }
+  }
+  if (nth > 1) {
+    for (int t = 1; t < nth; ++t) {
+      for (size_t q = 0; q < jsz; ++q) s->jc[q] += priv[t][q];
+      free(priv[t]);
+    }
+    free(priv);
+  }
+}
+
+/* Deposit of one particle move for the continuity tests: positions in grid
+   units (local, as set_local_positions returns them). */
+void ora_deposit_move(ora_sim* s, const double* xnew, const double* xold, float wght) {
+  if (s->p.ndim == 2)
+    ora_esirkepov_2d_one(s, s->jc, xnew, xold, wght);
+  else
+    ora_esirkepov_3d_one(s, s->jc, xnew, xold, wght);
+}
+void ora_zero_currents(ora_sim* s) { memset(s->jc, 0, sizeof(double) * (size_t)s->n1p * s->n2p * s->n3p * s->nc); }
+
+/* Charge density of one particle with the qden shapes into rho(n1p,n2p,n3p)
+   (the density the Esirkepov scheme conserves; grid_part_lib.f90:337-417). */
+void ora_rho_one(const ora_sim* s, double* rho, const double* xl, double wght) {
+  double ax[3], ay[3], az[3] = {1, 0, 0};
+  int i, j, k = 1;
+  ora_qden_1d(xl[0], ax, &i);
+  ora_qden_1d(xl[1], ay, &j);
+  int nz = 1;
+  if (s->p.ndim == 3) {
+    ora_qden_1d(xl[2], az, &k);
+    nz = 3;
+  }
+  size_t n1p = (size_t)s->n1p, n2p = (size_t)s->n2p;
+  for (int k1 = 0; k1 < nz; ++k1)
+    for (int j1 = 0; j1 < 3; ++j1)
+      for (int i1 = 0; i1 < 3; ++i1) {
+        int i2 = i - 1 + i1, j2 = j - 1 + j1, k2 = (s->p.ndim == 3) ? k - 1 + k1 : 1;
+        rho[(size_t)(i2 - 1) + n1p * ((size_t)(j2 - 1) + n2p * (size_t)(k2 - 1))] += wght * ax[i1] * ay[j1] * az[k1];
+      }
+}
+
+/* ======================================================================== */
+/* A13: curr_mpi_collect -> jc_xyzbd + djc (curr_and_fields_util.f90:104-152,*/
+/* src/parallel/mpi_curr_interface.f90:551-643), ib = 0                      */
+/* ======================================================================== */
+static void ora_jc_xyzbd(ora_sim* s) {
+  int i1 = s->ix1, n1 = s->ix2, j1 = s->jy1, n2 = s->jy2, k1 = s->kz1, n3 = s->kz2;
+  int nc = s->nc;
+  if (s->p.ibx == 0) {
+    for (int ik = 1; ik <= nc; ++ik)
+      for (int k = k1; k <= n3; ++k)
+        for (int j = j1; j <= n2; ++j) {
+          JC(s, i1, j, k, ik) = JC(s, i1, j, k, ik) + JC(s, i1 - 1, j, k, ik);
+          JC(s, i1 - 1, j, k, ik) = 0.0;
+          JC(s, n1, j, k, ik) = JC(s, n1, j, k, ik) + JC(s, n1 + 1, j, k, ik) + JC(s, n1 + 2, j, k, ik);
+          JC(s, n1 + 1, j, k, ik) = 0.0;
+          JC(s, n1 + 2, j, k, ik) = 0.0;
+        }
+  }
+  if (s->p.ndim < 2) return;
+  if (s->p.iby == 0) {
+    for (int ik = 1; ik <= nc; ++ik)
+      for (int iz = k1; iz <= n3; ++iz)
+        for (int ix = i1; ix <= n1; ++ix) {
+          JC(s, ix, j1, iz, ik) = JC(s, ix, j1, iz, ik) + JC(s, ix, j1 - 1, iz, ik) + JC(s, ix, j1 - 2, iz, ik);
+          JC(s, ix, j1 - 2, iz, ik) = 0.0;
+          JC(s, ix, j1 - 1, iz, ik) = 0.0;
+        }
+    for (int ik = 1; ik <= nc; ++ik)
+      for (int iz = k1; iz <= n3; ++iz)
+        for (int ix = i1; ix <= n1; ++ix) {
+          JC(s, ix, n2, iz, ik) = JC(s, ix, n2, iz, ik) + JC(s, ix, n2 + 1, iz, ik) + JC(s, ix, n2 + 2, iz, ik);
+          JC(s, ix, n2 + 1, iz, ik) = 0.0;
+          JC(s, ix, n2 + 2, iz, ik) = 0.0;
+        }
+  }
+  if (s->p.ndim < 3) return;
+  if (s->p.ibz == 0) {
+    for (int ik = 1; ik <= nc; ++ik)
+      for (int iy = j1; iy <= n2; ++iy)
+        for (int ix = i1; ix <= n1; ++ix) {
+          JC(s, ix, iy, k1, ik) = JC(s, ix, iy, k1, ik) + JC(s, ix, iy, k1 - 1, ik);
+          JC(s, ix, iy, k1 - 1, ik) = 0.0;
+        }
+    for (int ik = 1; ik <= nc; ++ik)
+      for (int iy = j1; iy <= n2; ++iy)
+        for (int ix = i1; ix <= n1; ++ix) {
+          JC(s, ix, iy, n3, ik) = JC(s, ix, iy, n3, ik) + JC(s, ix, iy, n3 + 1, ik) + JC(s, ix, iy, n3 + 2, ik);
+          JC(s, ix, iy, n3 + 1, ik) = 0.0;
+          JC(s, ix, iy, n3 + 2, ik) = 0.0;
+        }
+  }
+}
+
+static void ora_curr_collect(ora_sim* s) {
+  ora_jc_xyzbd(s);
+  if (s->p.iform < 2) {
+    size_t comp = (size_t)s->n1p * s->n2p * s->n3p;
+    for (int i = 1; i <= s->p.ndim; ++i) {
+      double d = s->p.djc[i - 1];
+      double* c = s->jc + comp * (size_t)(i - 1);
+      for (size_t q = 0; q < comp; ++q) c[q] = d * c[q];
+    }
+  }
+}
+
+/* ======================================================================== */
+/* A14: advance_lpf_fields (curr_and_fields_util.f90:176-260) with ef_bds,   */
+/* bf_bds, rote, rotb (src/fields/grid_fields.f90:1069-1552); uniform grid   */
+/* so loc_xg/loc_yg/loc_zg stretch factors are 1.                            */
+/* ======================================================================== */
+static void ora_ef_bds(ora_sim* s, double dtl, int imbd) {
+  int nf = s->nf;
+  int ix2 = s->ix2, jy2 = s->jy2, kz2 = s->kz2;
+  double aphx, aphy, aphz;
+  if (s->p.ibx < 2 && s->p.ibx == 0) {
+    aphx = 1.0 * s->p.dx_inv * dtl;
+    for (int k = s->kz1; k <= kz2; ++k)
+      for (int j = s->jy1; j <= jy2; ++j)
+        EBF(s, ix2 + 1, j, k, 2) = (2. * EBF(s, ix2, j, k, nf) - (1. - aphx) * EBF(s, ix2, j, k, 2)) / (1. + aphx);
+    if (nf > 3)
+      for (int k = s->kz1; k <= kz2; ++k)
+        for (int j = s->jy1; j <= jy2; ++j)
+          EBF(s, ix2 + 1, j, k, 3) = -(2. * EBF(s, ix2, j, k, 5) + (1. - aphx) * EBF(s, ix2, j, k, 3)) / (1. + aphx);
+  }
+  if (s->p.ndim < 2) return;
+  if (s->p.iby < 2 && imbd == 0) {
+    aphy = 1.0 * s->p.dy_inv * dtl;
+    for (int k = s->kz1; k <= kz2; ++k)
+      for (int i = s->ix1; i <= ix2; ++i)
+        EBF(s, i, jy2 + 1, k, 1) = -(2. * EBF(s, i, jy2, k, nf) + (1. - aphy) * EBF(s, i, jy2, k, 1)) / (1. + aphy);
+    if (nf > 3)
+      for (int k = s->kz1; k <= kz2; ++k)
+        for (int i = s->ix1; i <= ix2; ++i)
+          EBF(s, i, jy2 + 1, k, 3) = (2. * EBF(s, i, jy2, k, 4) - (1. - aphy) * EBF(s, i, jy2, k, 3)) / (1. + aphy);
+  }
+  if (s->p.ndim < 3) return;
+  if (s->p.ibz < 2 && imbd == 0) {
+    aphz = 1.0 * s->p.dz_inv * dtl;
+    for (int j = s->jy1; j <= jy2; ++j)
+      for (int i = s->ix1; i <= ix2; ++i) {
+        EBF(s, i, j, kz2 + 1, 1) = (2. * EBF(s, i, j, kz2, 5) - (1. - aphz) * EBF(s, i, j, kz2, 1)) / (1. + aphz);
+        EBF(s, i, j, kz2 + 1, 2) = -(2. * EBF(s, i, j, kz2, 4) + (1. - aphz) * EBF(s, i, j, kz2, 2)) / (1. + aphz);
+      }
+  }
+}
+
+static void ora_bf_bds(ora_sim* s, double dtl, int imbd) {
+  int nf = s->nf;
+  int ix1 = s->ix1, jy1 = s->jy1, kz1 = s->kz1;
+  double aphx, aphy, aphz;
+  if (s->p.ibx < 2) {
+    aphx = 1.0 * s->p.dx_inv * dtl;
+    for (int k = s->kz1; k <= s->kz2; ++k)
+      for (int j = s->jy1; j <= s->jy2; ++j)
+        EBF(s, ix1 - 1, j, k, nf) = -(2. * EBF(s, ix1, j, k, 2) + (1. - aphx) * EBF(s, ix1, j, k, nf)) / (1. + aphx);
+    if (nf > 3)
+      for (int k = s->kz1; k <= s->kz2; ++k)
+        for (int j = s->jy1; j <= s->jy2; ++j)
+          EBF(s, ix1 - 1, j, k, 5) = (2. * EBF(s, ix1, j, k, 3) - (1. - aphx) * EBF(s, ix1, j, k, 5)) / (1. + aphx);
+  }
+  if (s->p.ndim < 2) return;
+  if (s->p.iby < 2 && imbd == 0) {
+    aphy = 1.0 * s->p.dy_inv * dtl;
+    for (int k = s->kz1; k <= s->kz2; ++k)
+      for (int i = s->ix1; i <= s->ix2; ++i) {
+        EBF(s, i, jy1 - 1, k, nf) = 2. * EBF(s, i, jy1, k, 1) - (1. - aphy) * EBF(s, i, jy1, k, nf);
+        EBF(s, i, jy1 - 1, k, nf) = EBF(s, i, jy1 - 1, k, nf) / (1. + aphy);
+      }
+    if (nf > 3)
+      for (int k = s->kz1; k <= s->kz2; ++k)
+        for (int i = s->ix1; i <= s->ix2; ++i) {
+          EBF(s, i, jy1 - 1, k, 4) = -2. * EBF(s, i, jy1, k, 3) - (1. - aphy) * EBF(s, i, jy1, k, 4);
+          EBF(s, i, jy1 - 1, k, 4) = EBF(s, i, jy1 - 1, k, 4) / (1. + aphy);
+        }
+  }
+  if (s->p.ndim < 3) return;
+  if (s->p.ibz < 2 && imbd == 0) {
+    aphz = 1.0 * s->p.dz_inv * dtl;
+    for (int j = s->jy1; j <= s->jy2; ++j)
+      for (int i = s->ix1; i <= s->ix2; ++i) {
+        EBF(s, i, j, kz1 - 1, 4) = 2. * EBF(s, i, j, kz1, 2) - (1. - aphz) * EBF(s, i, j, kz1, 4);
+        EBF(s, i, j, kz1 - 1, 4) = EBF(s, i, j, kz1 - 1, 4) / (1. + aphz);
+        EBF(s, i, j, kz1 - 1, 5) = -2. * EBF(s, i, j, kz1, 1) - (1. - aphz) * EBF(s, i, j, kz1, 5);
+        EBF(s, i, j, kz1 - 1, 5) = EBF(s, i, j, kz1 - 1, 5) / (1. + aphz);
+      }
+  }
+}
+
+static void ora_rote(ora_sim* s, double dtf) {
+  int nf = s->nf;
+  double aphx = dtf * s->p.dx_inv, aphy = dtf * s->p.dy_inv, aphz = dtf * s->p.dz_inv;
+  double aph1 = aphx * s->p.se_coeff[0], aph2 = aphx * s->p.se_coeff[1];
+  for (int k = s->kz1; k <= s->kz2; ++k)
+    for (int j = s->jy1; j <= s->jy2; ++j) {
+      double sdhy = 1.0 * aphy;
+      for (int i = s->ix1; i <= s->ix2; ++i)
+        EBF(s, i, j, k, nf) = EBF(s, i, j, k, nf) - aph1 * (EBF(s, i + 1, j, k, 2) - EBF(s, i, j, k, 2)) +
+                              sdhy * (EBF(s, i, j + 1, k, 1) - EBF(s, i, j, k, 1)) -
+                              aph2 * (EBF(s, i + 2, j, k, 2) - EBF(s, i - 1, j, k, 2));
+    }
+  if (nf < 6) return;
+  for (int k = s->kz1; k <= s->kz2; ++k) {
+    double sdhz = 1.0 * aphz;
+    for (int j = s->jy1; j <= s->jy2; ++j) {
+      double sdhy = 1.0 * aphy;
+      for (int i = s->ix1; i <= s->ix2; ++i) {
+        EBF(s, i, j, k, 4) = EBF(s, i, j, k, 4) - sdhy * (EBF(s, i, j + 1, k, 3) - EBF(s, i, j, k, 3)) +
+                             sdhz * (EBF(s, i, j, k + 1, 2) - EBF(s, i, j, k, 2));
+        EBF(s, i, j, k, 5) = EBF(s, i, j, k, 5) + aph1 * (EBF(s, i + 1, j, k, 3) - EBF(s, i, j, k, 3)) -
+                             sdhz * (EBF(s, i, j, k + 1, 1) - EBF(s, i, j, k, 1)) +
+                             aph2 * (EBF(s, i + 2, j, k, 3) - EBF(s, i - 1, j, k, 3));
+      }
+    }
+  }
+}
+
+static void ora_rotb(ora_sim* s, double dtf) {
+  int nf = s->nf;
+  double aphx = dtf * s->p.dx_inv, aphy = dtf * s->p.dy_inv, aphz = dtf * s->p.dz_inv;
+  double aph1 = aphx * s->p.se_coeff[0], aph2 = aphx * s->p.se_coeff[1];
+  for (int k = s->kz1; k <= s->kz2; ++k)
+    for (int j = s->jy1; j <= s->jy2; ++j) {
+      double sdy = 1.0 * aphy;
+      for (int i = s->ix1; i <= s->ix2; ++i) {
+        EBF(s, i, j, k, 1) = EBF(s, i, j, k, 1) + sdy * (EBF(s, i, j, k, nf) - EBF(s, i, j - 1, k, nf));
+        EBF(s, i, j, k, 2) = EBF(s, i, j, k, 2) - aph1 * (EBF(s, i, j, k, nf) - EBF(s, i - 1, j, k, nf)) -
+                             aph2 * (EBF(s, i + 1, j, k, nf) - EBF(s, i - 2, j, k, nf));
+      }
+    }
+  if (nf < 6) return;
+  for (int k = s->kz1; k <= s->kz2; ++k) {
+    double sdz = aphz * 1.0;
+    for (int j = s->jy1; j <= s->jy2; ++j) {
+      double sdy = aphy * 1.0;
+      for (int i = s->ix1; i <= s->ix2; ++i) {
+        EBF(s, i, j, k, 1) = EBF(s, i, j, k, 1) - sdz * (EBF(s, i, j, k, 5) - EBF(s, i, j, k - 1, 5));
+        EBF(s, i, j, k, 2) = EBF(s, i, j, k, 2) + sdz * (EBF(s, i, j, k, 4) - EBF(s, i, j, k - 1, 4));
+        EBF(s, i, j, k, 3) = EBF(s, i, j, k, 3) + aph1 * (EBF(s, i, j, k, 5) - EBF(s, i - 1, j, k, 5)) -
+                             sdy * (EBF(s, i, j, k, 4) - EBF(s, i, j - 1, k, 4)) +
+                             aph2 * (EBF(s, i + 1, j, k, 5) - EBF(s, i - 2, j, k, 5));
+      }
+    }
+  }
+}
+
+void ora_advance_fields(ora_sim* s) {
+  double dt_lp = s->p.dt;
+  double dth = 0.5 * dt_lp;
+  ora_ef_bds(s, 0.0, 0);
+  ora_rote(s, dth);
+  ora_bf_bds(s, dt_lp, 0);
+  ora_rotb(s, dt_lp);
+  for (int ik = 1; ik <= s->nc; ++ik)
+    for (int k = s->kz1; k <= s->kz2; ++k)
+      for (int j = s->jy1; j <= s->jy2; ++j)
+        for (int i = s->ix1; i <= s->ix2; ++i)
+          EBF(s, i, j, k, ik) = EBF(s, i, j, k, ik) - s->p.ompe * JC(s, i, j, k, ik);
+  ora_ef_bds(s, dt_lp, 0);
+  ora_rote(s, dth);
+}
+
+/* Exposed for tests: field-only pieces. */
+void ora_field_bd(ora_sim* s) { ora_field_xyzbd(s, s->nf); }
+void ora_set_currents(ora_sim* s, const double* jc) {
+  memcpy(s->jc, jc, sizeof(double) * (size_t)s->n1p * s->n2p * s->n3p * s->nc);
+}
+void ora_curr_fold(ora_sim* s) { ora_curr_collect(s); }
+
+/* ======================================================================== */
+/* A21 / window source: lattice plasma (the build's jittered stand-in for     */
+/* the reference's regular (i-1/2)/n lattice, init_part_distrib.f90:152-203) */
+/* ======================================================================== */
+static void ora_lattice_particle(const ora_sim* s, int ic, int64_t ixl, int j, int k, double* x, double* y,
+                                 double* z) {
+  const agpu_plasma* src = &s->src[ic];
+  double dxl = s->p.dx / (double)src->npx;
+  double dyl = s->p.dy / (double)src->npy;
+  double dzl = s->p.dz / (double)src->npz;
+  uint32_t ctr[4] = {(uint32_t)ixl, (uint32_t)j, (uint32_t)k, (uint32_t)ic};
+  uint32_t r[4];
+  ora_philox4x32_10(ctr, (uint32_t)src->seed, (uint32_t)(src->seed >> 32), r);
+  double jx = src->jitter * (ora_u32(r[0]) - 0.5);
+  double jy = src->jitter * (ora_u32(r[1]) - 0.5);
+  double jz = src->jitter * (ora_u32(r[2]) - 0.5);
+  *x = src->x_start + ((double)ixl - 0.5 + jx) * dxl;
+  *y = src->y_min + ((double)j - 0.5 + jy) * dyl;
+  *z = (s->p.ndim == 3) ? src->z_min + ((double)k - 0.5 + jz) * dzl : 0.0;
+}
+
+int ora_set_plasma_source(ora_sim* s, const agpu_plasma* src) {
+  int ic = src->ic;
+  if (ic < 0 || ic >= s->p.nsp) return AGPU_E_ARG;
+  s->src[ic] = *src;
+  s->has_src[ic] = 1;
+  s->nptx[ic] = 0;
+  double dxl = s->p.dx / (double)src->npx;
+  double dyl = s->p.dy / (double)src->npy;
+  double dzl = s->p.dz / (double)src->npz;
+  s->sptx_max[ic] = (int64_t)floor((src->x_end - src->x_start) / dxl + 1e-9);
+  s->npty[ic] = (int)floor((src->y_max - src->y_min) / dyl + 1e-9);
+  s->nptz[ic] = (s->p.ndim == 3) ? (int)floor((src->z_max - src->z_min) / dzl + 1e-9) : 1;
+  return 0;
+}
+
+/* add_particles (src/dynamics/window.f90:39-104): k, j, ix order with x
+   fastest; momenta zero; the packed slot carries charge, part_ind, wgh. */
+static int ora_add_columns(ora_sim* s, int ic, int64_t i1, int64_t i2) {
+  const agpu_plasma* src = &s->src[ic];
+  int64_t n = s->np[ic];
+  int64_t add = (i2 - i1 + 1) * (int64_t)s->npty[ic] * s->nptz[ic];
+  if (n + add > s->cap[ic]) {
+    s->error_bits |= AGPU_EBIT_CAPACITY;
+    return AGPU_E_CAPACITY;
+  }
+  double slot = ora_pack_slot((int16_t)src->charge, (int16_t)src->part_ind, src->wgh);
+  for (int k = 1; k <= s->nptz[ic]; ++k)
+    for (int j = 1; j <= s->npty[ic]; ++j)
+      for (int64_t ix = i1; ix <= i2; ++ix) {
+        double x, y, z;
+        ora_lattice_particle(s, ic, ix, j, k, &x, &y, &z);
+        n = n + 1;
+        PART(s, ic, n, 1) = x;
+        PART(s, ic, n, 2) = y;
+        if (s->p.ndim == 3) {
+          PART(s, ic, n, 3) = z;
+          PART(s, ic, n, 4) = 0.;
+          PART(s, ic, n, 5) = 0.;
+          PART(s, ic, n, 6) = 0.;
+          PART(s, ic, n, 7) = slot;
+        } else {
+          PART(s, ic, n, 3) = 0.;
+          PART(s, ic, n, 4) = 0.;
+          PART(s, ic, n, 5) = slot;
+        }
+      }
+  s->np[ic] = n;
+  return 0;
+}
+
+/* Lattice column x centre, xpt(ix) (init_part_distrib.f90 (i-1/2)/n rule). */
+static double ora_xpt(const ora_sim* s, int ic, int64_t ix) {
+  double dxl = s->p.dx / (double)s->src[ic].npx;
+  return s->src[ic].x_start + ((double)ix - 0.5) * dxl;
+}
+
+/* particles_inject (src/dynamics/window.f90:106-184) for one species. */
+static int64_t ora_inject_species(ora_sim* s, int ic, double xmx) {
+  int64_t i1 = 1 + s->nptx[ic], i2, ix;
+  int64_t smax = s->sptx_max[ic];
+  if (i1 <= smax) {
+    for (ix = i1; ix <= smax; ++ix)
+      if (ora_xpt(s, ic, ix) > xmx) break;
+    i2 = ix - 1;
+    if (ix == smax) i2 = ix;
+  } else {
+    i2 = i1 - 1;
+  }
+  s->nptx[ic] = i2;
+  if (i2 > i1) {
+    int64_t before = s->np[ic];
+    if (ora_add_columns(s, ic, i1, i2) != 0) return -1;
+    return s->np[ic] - before;
+  }
+  return 0;
+}
+
+/* Initial load: the same column rule from nptx = 0 against xmax. */
+int ora_load_plasma(ora_sim* s, int ic) {
+  if (!s->has_src[ic]) return AGPU_E_STATE;
+  s->nptx[ic] = 0;
+  int64_t i1 = 1, ix, i2;
+  for (ix = i1; ix <= s->sptx_max[ic]; ++ix)
+    if (ora_xpt(s, ic, ix) > s->p.xmax) break;
+  i2 = ix - 1;
+  s->nptx[ic] = i2;
+  if (i2 >= i1) return ora_add_columns(s, ic, i1, i2);
+  return 0;
+}
+
+/* ======================================================================== */
+/* A19: lp_window_xshift (src/dynamics/window.f90:276-347) with              */
+/* fields_left_xshift (mpi_field_interface.f90:299-359) and                  */
+/* cell_part_dist(.true.) (mpi_part_interface.f90:549-597, non-prlx branch)  */
+/* ======================================================================== */
+static int ora_window_xshift(ora_sim* s, int witr, int init_iter, agpu_step_out* out) {
+  agpu_params* p = &s->p;
+  if (init_iter == 0) {
+    s->xlapse = 0.0;
+    s->wi1 = 0;
+    return 0;
+  }
+  double dt_step = p->dt;
+  s->xlapse = s->xlapse + p->w_speed * dt_step * (double)witr;
+  int wi2 = ora_nint(p->dx_inv * s->xlapse);
+  int nshx = wi2 - s->wi1;
+  s->wi1 = wi2;
+  double sh = p->dx * (double)nshx;
+  p->xmax = p->xmax + sh;
+  p->gxmin = p->gxmin + sh;
+  p->gxmax = p->gxmax + sh;
+  p->xmn = p->xmn + sh;
+  if (out) out->nshx = nshx;
+  wi2 = s->ix2 - nshx;
+  if (wi2 <= 0) return AGPU_E_WINDOW;
+  if (nshx != 0) {
+    /* fields_left_xshift(ebf, i1 = ix1, wi2, 1, nfield, nshx) */
+    for (int ic = 1; ic <= s->nf; ++ic)
+      for (int iz = s->kz1; iz <= s->kz2; ++iz)
+        for (int iy = s->jy1; iy <= s->jy2; ++iy) {
+          for (int ix = s->ix1; ix <= wi2; ++ix) EBF(s, ix, iy, iz, ic) = EBF(s, ix + nshx, iy, iz, ic);
+          for (int ix = wi2 + 1; ix <= wi2 + nshx; ++ix) EBF(s, ix, iy, iz, ic) = 0.0;
+        }
+  }
+  /* cell_part_dist(.true.): x only, all species, spec compacted */
+  for (int ic = 0; ic < p->nsp; ++ic) {
+    if (s->np[ic] > 0) {
+      int64_t r = ora_reset_dist(s, ic, 1, p->gxmin, p->gxmax, 0);
+      if (out) out->removed[ic] += r;
+    }
+  }
+  /* pex1: inject when targ_in <= xmax < targ_end */
+  for (int ic = 0; ic < p->nsp; ++ic) {
+    if (!s->has_src[ic]) continue;
+    if (s->src[ic].x_start <= p->xmax && s->src[ic].x_end > p->xmax) {
+      int64_t a = ora_inject_species(s, ic, p->xmax);
+      if (a < 0) return AGPU_E_CAPACITY;
+      if (out) out->injected[ic] += a;
+    }
+  }
+  return 0;
+}
+
+/* ======================================================================== */
+/* A15-A18: ionization                                                       */
+/* ======================================================================== */
+/* set_ionization_coeff for one species (src/ionization/ionz_data.f90:131-245,
+   770-804): potentials V(i), l_fact and the ADK coefficients. Supported
+   atomic numbers: 1 (H), 2 (He), 3 (Li), 6 (C), 7 (N). */
+typedef struct {
+  double v[8], v_norm[8], e_c[8], nstar[8], vfact[8], e_b[8], c_nstar[8];
+  int l_fact[8];
+  int an;
+} ora_adk;
+
+static int ora_adk_coeff(int an, ora_adk* a) {
+  const double v_h = 13.5984, euler = 2.71828, pig = 3.141592653589793;
+  memset(a, 0, sizeof(*a));
+  for (int i = 0; i < 8; ++i) a->l_fact[i] = 1;
+  a->an = an;
+  switch (an) {
+    case 1:
+      a->v[1] = 13.5984;
+      break;
+    case 2:
+      a->v[1] = 24.5874;
+      a->v[2] = 54.41776;
+      break;
+    case 3:
+      a->v[1] = 5.3917;
+      a->v[2] = 75.6400;
+      a->v[3] = 122.4543;
+      break;
+    case 6:
+      a->v[1] = 11.2603;
+      a->v[2] = 24.3833;
+      a->l_fact[1] = a->l_fact[2] = 3;
+      a->v[3] = 47.8878;
+      a->v[4] = 64.4939;
+      a->v[5] = 392.087;
+      a->v[6] = 489.993;
+      break;
+    case 7:
+      a->v[1] = 14.53;
+      a->v[2] = 29.601;
+      a->v[3] = 47.449;
+      a->l_fact[1] = a->l_fact[2] = a->l_fact[3] = 3;
+      a->v[4] = 77.473;
+      a->v[5] = 97.89;
+      a->v[6] = 552.07;
+      a->v[7] = 667.046;
+      break;
+    default:
+      return AGPU_E_ARG;
+  }
+  for (int i = 1; i <= an; ++i) {
+    a->v_norm[i] = a->v[i] / v_h;
+    a->e_c[i] = a->v_norm[i] * a->v_norm[i] / (16. * (double)i);
+    a->nstar[i] = (double)i / sqrt(a->v_norm[i]);
+    a->vfact[i] = (a->v_norm[i]) * sqrt(a->v_norm[i]);
+    a->e_b[i] = 2. * a->vfact[i] / (3. * (2. * a->nstar[i] - 1.));
+  }
+  for (int i = 1; i <= an; ++i) {
+    a->c_nstar[i] = pow(2. * euler / a->nstar[i], 2 * a->nstar[i]);
+    a->c_nstar[i] = a->c_nstar[i] * (double)a->l_fact[i] / (2. * pig * a->nstar[i]);
+    a->c_nstar[i] = 0.5 * a->v_norm[i] * a->c_nstar[i];
+  }
+  return 0;
+}
+
+/* set_field_ioniz_wfunction, one-level branch (src/ionization/ionize.f90:
+   38-190): ADK rate tables for models 1-5 on n_ge bins of |E| in (0,e_max],
+   w_one_lev = 1 - exp(-dt_fs * omega_a * W). Output table column-major
+   (nk = 0..n_ge+1, z = 0..zm), rows never written by the reference are 0. */
+int ora_build_ionization_table(int an, int z0, int model, double e_max, double dt, double* tab,
+                               double* de_inv_out) {
+  const double omega_a = 41.3, pig = 3.141592653589793, tiny = 1.e-10;
+  const int n_ge = ORA_NGE;
+  ora_adk a;
+  if (ora_adk_coeff(an, &a) != 0) return AGPU_E_ARG;
+  int zm = an;
+  int nrow = n_ge + 2;
+  double* wi = (double*)calloc((size_t)(n_ge + 1) * (zm + 1), sizeof(double));
+  double dge = e_max / (double)n_ge;
+  double de_inv = 1. / dge;
+  for (int k = z0 + 1; k <= zm; ++k) {
+    int j = k - z0;
+    double ns = 2. * a.nstar[k] - 1.;
+    for (int i = 1; i <= n_ge; ++i) {
+      double ei = dge * (double)i;
+      double fact2 = (2. * a.vfact[k] / ei);
+      double fact1, w_adk, w_bsi, efact, avg_fact;
+      double w = 0.0;
+      switch (model) {
+        case 1:
+          fact1 = pow(fact2, ns);
+          w_adk = a.c_nstar[k] * fact1 * exp(-fact2 / 3.);
+          if (w_adk < tiny) w_adk = 0.0;
+          w = w_adk;
+          break;
+        case 2:
+          fact1 = pow(fact2, ns);
+          fact1 = fact1 * sqrt(3. * ei / (pig * a.vfact[k]));
+          w_adk = a.c_nstar[k] * fact1 * exp(-fact2 / 3.);
+          if (w_adk < tiny) w_adk = 0.0;
+          w = w_adk;
+          break;
+        case 3:
+        case 5:
+          if (model == 3) {
+            fact1 = pow(fact2, ns);
+            fact1 = fact1 * sqrt(3. * ei / (pig * a.vfact[k]));
+          } else {
+            fact1 = sqrt(3. * ei / (pig * a.vfact[k])) * pow(fact2, ns);
+          }
+          w_adk = a.c_nstar[k] * fact1 * exp(-fact2 / 3.);
+          if (w_adk < tiny) w_adk = 0.0;
+          w = w_adk;
+          if (ei > a.e_c[k]) {
+            fact2 = (2. * a.vfact[k] / a.e_c[k]);
+            if (model == 3) {
+              fact1 = pow(fact2, ns);
+              fact1 = fact1 * sqrt(3. * a.e_c[k] / (pig * a.vfact[k]));
+            } else {
+              fact1 = sqrt(3. * a.e_c[k] / (pig * a.vfact[k])) * pow(fact2, ns);
+            }
+            w_adk = a.c_nstar[k] * fact1 * exp(-fact2 / 3.);
+            w_bsi = a.vfact[k] * (1. - a.e_c[k] / ei) / (4. * pig * (double)k);
+            w = w_bsi + w_adk;
+          }
+          break;
+        case 4:
+          fact1 = pow(fact2, ns);
+          avg_fact = 1.0;
+          if (a.l_fact[k] > 1) {
+            for (int ll = 1; ll <= (a.l_fact[k] - 1) / 2; ++ll) avg_fact = avg_fact + 2. / pow(fact2, ll);
+            avg_fact = avg_fact / a.l_fact[k];
+            fact1 = fact1 * avg_fact;
+          }
+          fact1 = fact1 * sqrt(3. * ei / (pig * a.vfact[k]));
+          w_adk = a.c_nstar[k] * fact1 * exp(-fact2 / 3.);
+          if (w_adk < tiny) w_adk = 0.0;
+          w = w_adk;
+          efact = 1. - a.e_c[k] / ei;
+          w_bsi = a.vfact[k] * efact / (4. * pig * (double)k);
+          if (w_bsi < tiny) w_bsi = 0.;
+          if (ei > a.e_c[k]) w = (w_bsi < w_adk) ? w_bsi : w_adk;
+          if (ei > a.e_b[k]) w = w_bsi;
+          break;
+        default:
+          free(wi);
+          return AGPU_E_ARG;
+      }
+      wi[(size_t)i + (size_t)(n_ge + 1) * j] = w;
+    }
+  }
+  double dt_fs = 10. * dt / 3.;
+  for (size_t q = 0; q < (size_t)(n_ge + 1) * (zm + 1); ++q) wi[q] = omega_a * wi[q];
+  memset(tab, 0, sizeof(double) * (size_t)nrow * (zm + 1));
+  int zm_loc = zm - z0;
+  for (int z = 0; z <= zm_loc - 1; ++z) {
+    int zk = z + 1;
+    int k = z + z0;
+    for (int i = 1; i <= n_ge; ++i) tab[(size_t)i + (size_t)nrow * k] = 1. - exp(-dt_fs * wi[(size_t)i + (size_t)(n_ge + 1) * zk]);
+  }
+  free(wi);
+  *de_inv_out = de_inv;
+  return 0;
+}
+
+int ora_set_ionization_species(ora_sim* s, int ic, int an, int ion_min, int model, double lp_max) {
+  if (ic < 1 || ic >= s->p.nsp) return AGPU_E_ARG;
+  s->at_num[ic] = an;
+  s->ion_min[ic] = ion_min;
+  s->ionz_model[ic] = model;
+  s->zmax[ic] = an;
+  s->lp_max[ic] = lp_max;
+  free(s->wtab[ic]);
+  s->wtab[ic] = (double*)calloc((size_t)(ORA_NGE + 2) * (an + 1), sizeof(double));
+  if (ic + 1 > s->nsp_ionz) s->nsp_ionz = ic + 1;
+  return ora_build_ionization_table(an, ion_min, model, lp_max, s->p.dt, s->wtab[ic], &s->de_inv[ic]);
+}
+
+/* set_ion_efield (grid_part_connect.f90:288-410): |E|^2 on each ion with
+   the qqh shapes, into ebfp(:, id_ch). */
+static void ora_set_ion_efield(ora_sim* s, int ic, int64_t np) {
+  const agpu_params* p = &s->p;
+  int id_ch = s->ndv;
+  for (int64_t n = 1; n <= np; ++n) {
+    double ef_sqr = 0.;
+    double xl = p->dx_inv * (PART(s, ic, n, 1) - p->xmn);
+    double yl = p->dy_inv * (PART(s, ic, n, 2) - p->ymn);
+    double ax1[3], axh[3], ay1[3], ayh[3], az1[3], azh[3];
+    int i, ih, j, jh, k, kh;
+    ora_qqh_1d(xl, ax1, axh, &i, &ih);
+    ora_qqh_1d(yl, ay1, ayh, &j, &jh);
+    if (p->ndim == 2) {
+      for (int jp1 = 0; jp1 <= 2; ++jp1) {
+        int jp2 = j + jp1;
+        double dvol = ay1[jp1];
+        for (int ip1 = 0; ip1 <= 2; ++ip1) {
+          double ex = EBF(s, ih + ip1, jp2, 1, 1);
+          ef_sqr = ef_sqr + axh[ip1] * dvol * ex * ex;
+        }
+      }
+      for (int jp1 = 0; jp1 <= 2; ++jp1) {
+        int jp2 = jh + jp1;
+        double dvol = ayh[jp1];
+        for (int ip1 = 0; ip1 <= 2; ++ip1) {
+          double ey = EBF(s, i + ip1, jp2, 1, 2);
+          ef_sqr = ef_sqr + ax1[ip1] * dvol * ey * ey;
+        }
+      }
+    } else {
+      double zl = p->dz_inv * (PART(s, ic, n, 3) - p->zmn);
+      ora_qqh_1d(zl, az1, azh, &k, &kh);
+      for (int kp1 = 0; kp1 <= 2; ++kp1) {
+        int kp2 = k + kp1;
+        for (int jp1 = 0; jp1 <= 2; ++jp1) {
+          int jp2 = j + jp1;
+          double dvol = ay1[jp1] * az1[kp1];
+          for (int ip1 = 0; ip1 <= 2; ++ip1) {
+            double ex = EBF(s, ip1 + ih, jp2, kp2, 1);
+            ef_sqr = ef_sqr + axh[ip1] * dvol * ex * ex;
+          }
+        }
+        for (int jp1 = 0; jp1 <= 2; ++jp1) {
+          int jp2 = jh + jp1;
+          double dvol = ayh[jp1] * az1[kp1];
+          for (int ip1 = 0; ip1 <= 2; ++ip1) {
+            double ey = EBF(s, i + ip1, jp2, kp2, 2);
+            ef_sqr = ef_sqr + ax1[ip1] * dvol * ey * ey;
+          }
+        }
+      }
+      for (int kp1 = 0; kp1 <= 2; ++kp1) {
+        int kp2 = kh + kp1;
+        for (int jp1 = 0; jp1 <= 2; ++jp1) {
+          int jp2 = j + jp1;
+          double dvol = ay1[jp1] * azh[kp1];
+          for (int ip1 = 0; ip1 <= 2; ++ip1) {
+            double ez = EBF(s, ip1 + i, jp2, kp2, 3);
+            ef_sqr = ef_sqr + ax1[ip1] * dvol * ez * ez;
+          }
+        }
+      }
+    }
+    PT(s, n, id_ch) = ef_sqr;
+  }
+}
+
+/* Ionization draw for ion n (0-based) of species ic at step iter. */
+static inline double ora_ionz_draw(uint64_t seed, int64_t n, int iter, int ic) {
+  uint32_t ctr[4] = {(uint32_t)n, (uint32_t)((uint64_t)n >> 32), (uint32_t)iter, 0x494f0000u | (uint32_t)ic};
+  uint32_t r[4];
+  ora_philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32), r);
+  return ora_u53(r[0], r[1]);
+}
+
+/* ionization_cycle + part_ionize (ionz_lev = 1) + ionization_electrons_inject
+   (src/ionization/ionize.f90:452-558, 390-450, 258-322).  Returns the number
+   of new electrons. */
+static int64_t ora_ionization_cycle(ora_sim* s, int ic, int64_t np, int iter) {
+  int id_ch = s->ndv;
+  int n_ge = ORA_NGE, nrow = n_ge + 2;
+  double def_inv = s->de_inv[ic];
+  int64_t kk = 0;
+  int64_t ne = s->np[0];
+  /* count first (capacity), then apply in ion order */
+  for (int64_t n = 1; n <= np; ++n) {
+    double ef2 = PT(s, n, id_ch);
+    int nk = 0;
+    if (ef2 > 0.) {
+      double ef = sqrt(ef2);
+      nk = ora_nint(def_inv * ef);
+    }
+    if (nk > n_ge + 1) {
+      s->error_bits |= AGPU_EBIT_IONZ_INDEX;
+      nk = n_ge + 1;
+    }
+    ora_pack w = ora_unpack(PART(s, ic, n, id_ch));
+    int z0 = w.charge;
+    double pr = ora_ionz_draw(s->p.seed, n - 1, iter, ic);
+    double thr = (z0 >= 0 && z0 <= s->zmax[ic]) ? s->wtab[ic][(size_t)nk + (size_t)nrow * z0] : 0.0;
+    if (pr < thr) {
+      w.charge = (int16_t)(w.charge + 1);
+      PART(s, ic, n, id_ch) = ora_pack_slot(w.charge, w.part_ind, w.wgh);
+      kk++;
+      if (ne + 1 > s->cap[0]) {
+        s->error_bits |= AGPU_EBIT_CAPACITY;
+        continue;
+      }
+      ne = ne + 1;
+      float ewgh = w.wgh * (float)s->p.n_mol_atoms[ic];
+      double slot = ora_pack_slot(-1, -1, ewgh);
+      for (int c = 1; c <= s->p.curr_ndim; ++c) PART(s, 0, ne, c) = PART(s, ic, n, c);
+      for (int c = s->p.curr_ndim + 1; c <= 2 * s->p.curr_ndim; ++c) PART(s, 0, ne, c) = 0.0;
+      PART(s, 0, ne, id_ch) = slot;
+    }
+  }
+  s->np[0] = ne;
+  return kk;
+}
+
+/* ======================================================================== */
+/* lpf2_evolve + lp_run (src/dynamics/pic_evolve_in_time.f90:37-144)         */
+/* ======================================================================== */
+int ora_step(ora_sim* s, int iter, double t, int initial_time, agpu_step_out* out) {
+  agpu_params* p = &s->p;
+  agpu_step_out dummy;
+  if (!out) out = &dummy;
+  memset(out, 0, sizeof(*out));
+  out->ion_field_max = -1.0;
+  ora_field_xyzbd(s, s->nf);
+  if (p->ionz_lev > 0) {
+    for (int ic = 1; ic < s->nsp_ionz; ++ic) {
+      int64_t np = s->np[ic];
+      if (np > 0 && s->wtab[ic]) {
+        ora_set_ion_efield(s, ic, np);
+        if (iter % 100 == 0) {
+          double m = 0.0;
+          for (int64_t n = 1; n <= np; ++n)
+            if (PT(s, n, s->ndv) > m || n == 1) m = PT(s, n, s->ndv);
+          m = sqrt(m);
+          out->ion_field_max = m;
+          if (m > s->lp_max[ic]) {
+            s->lp_max[ic] = 1.1 * m;
+            ora_build_ionization_table(s->at_num[ic], s->ion_min[ic], s->ionz_model[ic], s->lp_max[ic], p->dt,
+                                       s->wtab[ic], &s->de_inv[ic]);
+          }
+        }
+        out->new_electrons += ora_ionization_cycle(s, ic, np, iter);
+      }
+    }
+  }
+  ora_zero_currents(s);
+  for (int ic = 0; ic < p->nsp_run; ++ic) {
+    int64_t np = s->np[ic];
+    ora_gather(s, ic, np);
+    ora_field_charge_multiply(s, ic, np);
+    if (initial_time) ora_init_lpf_momenta(s, ic, np);
+    ora_push(s, ic, np);
+    out->removed[ic] += ora_cell_part_dist_step(s, ic);
+    np = s->np[ic];
+    if (np > 0) ora_curr_accumulate(s, ic, np);
+  }
+  ora_curr_collect(s);
+  ora_advance_fields(s);
+  int rc = 0;
+  if (p->w_speed > 0.0 && p->w_sh > 0) {
+    if (t >= p->wi_time && t < p->wf_time) {
+      if (iter % p->w_sh == 0) rc = ora_window_xshift(s, p->w_sh, iter, out);
+    }
+  }
+  for (int ic = 0; ic < 4; ++ic) out->np[ic] = s->np[ic];
+  out->xmn = p->xmn;
+  out->error_bits = s->error_bits;
+  return rc;
+}
+
+/* Individual phases for tests. */
+void ora_phase_gather_push(ora_sim* s, int ic, int initial_time) {
+  int64_t np = s->np[ic];
+  ora_gather(s, ic, np);
+  ora_field_charge_multiply(s, ic, np);
+  if (initial_time) ora_init_lpf_momenta(s, ic, np);
+  ora_push(s, ic, np);
+}
+int ora_get_scratch(const ora_sim* s, int col, double* out, int64_t n) {
+  if (col < 1 || col > s->ndv || n > s->ebfp_cap) return AGPU_E_ARG;
+  memcpy(out, &s->ebfp[(size_t)(col - 1) * s->ebfp_cap], sizeof(double) * (size_t)n);
+  return 0;
+}
+int ora_get_ionization_table(const ora_sim* s, int ic, double* out) {
+  if (!s->wtab[ic]) return AGPU_E_STATE;
+  memcpy(out, s->wtab[ic], sizeof(double) * (size_t)(ORA_NGE + 2) * (s->zmax[ic] + 1));
+  return 0;
+}
+double ora_ionz_de_inv(const ora_sim* s, int ic) { return s->de_inv[ic]; }
+double ora_draw(uint64_t seed, int64_t n, int iter, int ic) { return ora_ionz_draw(seed, n, iter, ic); }
+void ora_philox(const uint32_t* ctr, uint32_t k0, uint32_t k1, uint32_t* out) { ora_philox4x32_10(ctr, k0, k1, out); }

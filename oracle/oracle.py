@@ -1,0 +1,184 @@
+"""ctypes wrapper of the CPU FP64 oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, the smoke check and bench.py's
+CPU-baseline leg, never by the product package.  See aladyn_oracle.c for the
+restated reference functions; parity unpinned (the Fortran reference cannot
+be compiled here and ships no golden vectors).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    src = [os.path.join(HERE, f) for f in ("aladyn_oracle.c", "philox.h", "Makefile")]
+    if force or not os.path.exists(LIB) or max(os.path.getmtime(s) for s in src) > os.path.getmtime(LIB):
+        subprocess.run(["make", "-s", "-C", HERE, "-B" if force else "liboracle.so"], check=True)
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    build()
+    lib = C.CDLL(LIB)
+    P, D, I64 = C.c_void_p, C.POINTER(C.c_double), C.c_int64
+    sig = {
+        "ora_create": (P, [P]),
+        "ora_destroy": (None, [P]),
+        "ora_set_threads": (None, [P, C.c_int]),
+        "ora_dims": (C.c_int, [P, C.POINTER(C.c_int)]),
+        "ora_set_fields": (C.c_int, [P, D]),
+        "ora_get_fields": (C.c_int, [P, D]),
+        "ora_get_currents": (C.c_int, [P, D]),
+        "ora_set_currents": (None, [P, D]),
+        "ora_set_species": (C.c_int, [P, C.c_int, D, I64, I64]),
+        "ora_get_species": (C.c_int, [P, C.c_int, D, I64, C.POINTER(I64)]),
+        "ora_count": (I64, [P, C.c_int]),
+        "ora_error_bits": (C.c_uint32, [P]),
+        "ora_xmn": (C.c_double, [P]),
+        "ora_step": (C.c_int, [P, C.c_int, C.c_double, C.c_int, P]),
+        "ora_field_bd": (None, [P]),
+        "ora_advance_fields": (None, [P]),
+        "ora_curr_fold": (None, [P]),
+        "ora_zero_currents": (None, [P]),
+        "ora_deposit_move": (None, [P, D, D, C.c_float]),
+        "ora_rho_one": (None, [P, D, D, C.c_double]),
+        "ora_phase_gather_push": (None, [P, C.c_int, C.c_int]),
+        "ora_get_scratch": (C.c_int, [P, C.c_int, D, I64]),
+        "ora_shape_qlh": (None, [C.c_double, D, D, C.POINTER(C.c_int)]),
+        "ora_shape_qqh": (None, [C.c_double, D, D, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "ora_shape_qden": (None, [C.c_double, D, C.POINTER(C.c_int)]),
+        "ora_set_plasma_source": (C.c_int, [P, P]),
+        "ora_load_plasma": (C.c_int, [P, C.c_int]),
+        "ora_build_ionization_table": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, D, D]),
+        "ora_set_ionization_species": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]),
+        "ora_get_ionization_table": (C.c_int, [P, C.c_int, D]),
+        "ora_ionz_de_inv": (C.c_double, [P, C.c_int]),
+        "ora_draw": (C.c_double, [C.c_uint64, I64, C.c_int, C.c_int]),
+        "ora_philox": (None, [C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+NGE = 10000
+
+
+class Oracle:
+    """The oracle's simulation state, same calls as aladyn_b200.sim.PicDevice."""
+
+    def __init__(self, params, threads: int = 1):
+        self.lib = load()
+        self.params = params
+        self._p = params  # keep alive
+        self.h = self.lib.ora_create(C.byref(params))
+        d = (C.c_int * 10)()
+        self.lib.ora_dims(self.h, d)
+        self.n1p, self.n2p, self.n3p = d[0], d[1], d[2]
+        self.ix1, self.ix2, self.jy1, self.jy2, self.kz1, self.kz2 = d[3], d[4], d[5], d[6], d[7], d[8]
+        self.ndv = d[9]
+        self.nf = params.nfield
+        self.nc = params.curr_ndim
+        if threads > 1:
+            self.lib.ora_set_threads(self.h, threads)
+
+    def close(self):
+        if self.h:
+            self.lib.ora_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def field_shape(self):
+        return (self.n1p, self.n2p, self.n3p, self.nf)
+
+    def set_fields(self, ebf):
+        a = np.asfortranarray(ebf, dtype=np.float64)
+        assert a.shape == self.field_shape()
+        self.lib.ora_set_fields(self.h, _dp(a))
+
+    def get_fields(self):
+        a = np.zeros(self.field_shape(), dtype=np.float64, order="F")
+        self.lib.ora_get_fields(self.h, _dp(a))
+        return a
+
+    def get_currents(self):
+        a = np.zeros((self.n1p, self.n2p, self.n3p, self.nc), dtype=np.float64, order="F")
+        self.lib.ora_get_currents(self.h, _dp(a))
+        return a
+
+    def set_currents(self, jc):
+        a = np.asfortranarray(jc, dtype=np.float64)
+        self.lib.ora_set_currents(self.h, _dp(a))
+
+    def set_species(self, ic, part):
+        a = np.asfortranarray(part, dtype=np.float64)
+        rc = self.lib.ora_set_species(self.h, ic, _dp(a), a.shape[0], a.shape[0])
+        assert rc == 0, rc
+
+    def count(self, ic):
+        return self.lib.ora_count(self.h, ic)
+
+    def get_species(self, ic):
+        n = self.count(ic)
+        a = np.zeros((max(n, 1), self.ndv), dtype=np.float64, order="F")
+        got = C.c_int64()
+        self.lib.ora_get_species(self.h, ic, _dp(a), a.shape[0], C.byref(got))
+        return a[:n]
+
+    def set_plasma_source(self, src):
+        assert self.lib.ora_set_plasma_source(self.h, C.byref(src)) == 0
+
+    def load_plasma(self, ic):
+        assert self.lib.ora_load_plasma(self.h, ic) == 0
+
+    def set_ionization_species(self, ic, an, ion_min, model, lp_max):
+        assert self.lib.ora_set_ionization_species(self.h, ic, an, ion_min, model, lp_max) == 0
+
+    def ionization_table(self, ic, zmax):
+        t = np.zeros((NGE + 2, zmax + 1), dtype=np.float64, order="F")
+        assert self.lib.ora_get_ionization_table(self.h, ic, _dp(t)) == 0
+        return t
+
+    def lp_run(self, t, iteration, initial_time=False):
+        from aladyn_b200.abi import AgpuStepOut
+        out = AgpuStepOut()
+        rc = self.lib.ora_step(self.h, iteration, t, 1 if initial_time else 0, C.byref(out))
+        return rc, out
+
+    def error_bits(self):
+        return self.lib.ora_error_bits(self.h)
+
+    def xmn(self):
+        return self.lib.ora_xmn(self.h)
+
+
+def build_ionization_table(an, z0, model, e_max, dt):
+    lib = load()
+    t = np.zeros((NGE + 2, an + 1), dtype=np.float64, order="F")
+    de = C.c_double()
+    rc = lib.ora_build_ionization_table(an, z0, model, e_max, dt, _dp(t), C.byref(de))
+    assert rc == 0, rc
+    return t, de.value
