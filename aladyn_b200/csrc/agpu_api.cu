@@ -254,6 +254,7 @@ int add_lattice_columns(agpu_handle* h, int ic, long long i1, long long i2) {
   else
     lattice64(a, h->part[ic], h->cap[ic], h->np[ic], h->st, h->sms);
   CK(cudaGetLastError());
+  h->timers.launches_total += 1;
   h->np[ic] += n;
   return 0;
 }
@@ -276,6 +277,7 @@ int compact_species(agpu_handle* h, int ic, bool window) {
     std::swap(h->part[ic], h->tmp);
   }
   CK(cudaGetLastError());
+  h->timers.launches_total += 3;  // count, scan, scatter
   h->np[ic] = kept;
   return 0;
 }
@@ -324,6 +326,7 @@ int window_xshift(agpu_handle* h, int witr, int init_iter, agpu_step_out* out) {
     else
       xshift64(h->ebf, h->g, h->g.nf, wi2, nshx, h->st, h->sms);
     CK(cudaGetLastError());
+    h->timers.launches_total += 1;
   }
   for (int ic = 0; ic < p.nsp; ++ic) {
     if (h->np[ic] <= 0) continue;
@@ -331,6 +334,7 @@ int window_xshift(agpu_handle* h, int witr, int init_iter, agpu_step_out* out) {
       k_shift_cells<<<grid_for(h->np[ic], 256, h->sms, 16), 256, 0, h->st>>>(h->sp[ic].cell, h->sp[ic].ox, h->np[ic], nshx,
                                                                                h->g.n1p);
       CK(cudaGetLastError());
+      h->timers.launches_total += 1;
     }
     long long before = h->np[ic];
     int rc = compact_species(h, ic, true);
@@ -420,6 +424,7 @@ int ionize64(agpu_handle* h, int iter, agpu_step_out* out) {
     }
     k64_ionize<<<grid, 256, 0, h->st>>>(a);
     CK(cudaGetLastError());
+    h->timers.launches_total += 2 + 3 + ((iter % 100 == 0) ? 1 : 0);  // efield, ionize, append, [max]
     long long ne0 = h->np[0];
     long long added = append_electrons64(h->flag, np, h->part[ic], h->cap[ic], h->part[0], h->cap[0], ne0, h->cap[0],
                                          h->p.ndim, h->p.n_mol_atoms[ic], &h->d_cnt->err, h->scr, h->st);
@@ -806,6 +811,7 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu
   if (h->fp32) field_bd32(Dev32{h->g, h->ebf32, h->jhi, h->jlo}, h->st, h->sms);
   else field_bd64(Dev64{h->g, h->ebf, h->jc}, h->st, h->sms);
   CK(cudaGetLastError());
+  h->timers.launches_total += (p.ndim == 3) ? 3 : 2;
   ph_end(h, PH_YEE);
   // ionization
   if (p.ionz_lev > 0 && !h->fp32) {
@@ -893,6 +899,7 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu
     CK(cudaGetLastError());
     ph_end(h, PH_PUSH);
     h->timers.launches_push_deposit += 1;
+    h->timers.launches_total += 1;
     h->timers.pushes += np;
     if (int rc_ = read_counters(h)) return rc_;
     if (h->h_cnt->removed > 0) {
@@ -919,6 +926,8 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu
   CK(cudaGetLastError());
   ph_end(h, PH_YEE);
   h->timers.launches_yee += 1;
+  // current fold (x, y[, z] faces; hi and lo in the split form) + 6 Yee kernels
+  h->timers.launches_total += ((p.ndim == 3) ? 3 : 2) * (h->fp32 ? 2 : 1) + 6;
   h->timers.yee_cells += (long long)p.nx * p.ny * (p.ndim == 3 ? p.nz : 1);
   // lp_run: moving window
   if (p.w_speed > 0.0 && p.w_sh > 0) {

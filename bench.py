@@ -1,0 +1,499 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 PIC step: particle-pushes/s of the 3D LWFA step
+(1024x256x256 cells, 8 particles/cell, ~5.4e8 electrons, moving window) in the
+FP32 split form and the plain FP64 form on one GPU, plus the Yee update GB/s.
+
+Contract (one JSON line from rank 0):
+  value      whole-job particle-pushes/s of the FP32 split form: particles x
+             steps / device time of the full step (gather, push, deposit,
+             box-edge removal, current fold, Yee update, window shift);
+  e2e        the same metric through the C-ABI with host buffers: every step
+             the host's window-injection records are copied from pinned host
+             memory (agpu_window_inject) and the step output plus the FP64
+             diagnostics come back (agpu_step, agpu_diag);
+  roofline   the fused gather+push+deposit kernel of the FP32 split form
+             against the measured HBM copy bandwidth;
+  cpu_baseline the oracle (CPU FP64 restatement of the reference) on all
+             host cores on a bounded sample of the same workload.
+
+--impl reference times the oracle alone (the reference's CPU arithmetic) on
+the host cores.  Under torchrun (N > 1) every rank runs one independent
+replica of the workload on its own GPU (replicas only: no collective on the
+data path) and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+LAM0 = 0.8  # um
+
+# Workloads (the reference's LWFA setups restated on synthetic seeded input)
+WORKLOADS = {
+    # 3D LWFA: 1024x256x256, dx = 0.05 lambda, dy = dz = 0.25 lambda, 8 ppc,
+    # n_e = 0.005 n_c, a0 = 3, waist 6 lambda, FWHM 10 lambda/c, window at c.
+    "lwfa3d_1024x256x256_ppc8": dict(ndim=3, nx=1024, ny=256, nz=256, k0=25.0, yx_rat=5.0, zx_rat=5.0,
+                                    cfl=0.8, ppc=(2, 2, 2), n_over_nc=0.005, a0=3.0, w0=6 * LAM0,
+                                    tau=10 * LAM0, x_plasma=0.0, xc_frac=0.7),
+    # 2D LWFA: 1024x256, dx = 0.05 lambda, dy = 0.2 lambda, 4 ppc, n_e = 0.01 n_c,
+    # plasma from x = 20 lambda, a0 = 2, waist 5 lambda.
+    "lwfa2d_1024x256_ppc4": dict(ndim=2, nx=1024, ny=256, nz=1, k0=25.0, yx_rat=4.0, zx_rat=1.0,
+                                 cfl=0.8, ppc=(2, 2, 1), n_over_nc=0.01, a0=2.0, w0=5 * LAM0,
+                                 tau=10 * LAM0, x_plasma=20 * LAM0, xc_frac=0.3),
+    # small 3D case for quick checks
+    "lwfa3d_256x128x128_ppc8": dict(ndim=3, nx=256, ny=128, nz=128, k0=25.0, yx_rat=5.0, zx_rat=5.0,
+                                   cfl=0.8, ppc=(2, 2, 2), n_over_nc=0.005, a0=3.0, w0=6 * LAM0,
+                                   tau=10 * LAM0, x_plasma=0.0, xc_frac=0.7),
+}
+DEFAULT_WORKLOAD = "lwfa3d_1024x256x256_ppc8"
+
+
+def bytes_per_push(ndim: int, ppc: int, fp32: bool) -> float:
+    """Algorithmic bytes of one particle push (gather+push+deposit):
+    particle record read + written once, fields read and currents written
+    once per cell, amortised over the particles of a cell.
+    FP64 3D: read x,p,w 56 B + write x,p 48 B + (6 field + 3 current words) x 8 B / ppc.
+    FP32 split 3D: read node 4 + offsets 12 + p 12 + slot 8 B, write node,
+    offsets, p 28 B, fields 24 B + currents (hi, lo) 24 B per cell / ppc."""
+    if ndim == 3:
+        return (36.0 + 28.0 + 48.0 / ppc) if fp32 else (104.0 + 72.0 / ppc)
+    return (24.0 + 20.0 + 28.0 / ppc) if fp32 else (72.0 + 40.0 / ppc)
+
+
+def yee_bytes_per_cell(ndim: int, fp32: bool) -> float:
+    """Read E, B, J and write E, B once: 15 words (3D) or 8 words (2D TE)."""
+    return (15 if ndim == 3 else 8) * (4 if fp32 else 8)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# workload set-up on the device
+# --------------------------------------------------------------------------
+def make_workload(name: str, precision: int, cap_factor: float = 1.04):
+    from aladyn_b200.config import Grid, laser, make_params, n_over_nc_to_n0, plasma
+    w = WORKLOADS[name]
+    g = Grid(w["ndim"], w["nx"], w["ny"], w["nz"], w["k0"], w["yx_rat"], w["zx_rat"], w["cfl"])
+    ppc = w["ppc"][0] * w["ppc"][1] * (w["ppc"][2] if w["ndim"] == 3 else 1)
+    ncell = w["nx"] * w["ny"] * (w["nz"] if w["ndim"] == 3 else 1)
+    cap = int(ncell * ppc * cap_factor) + 4096
+    p = make_params(g, precision=precision, capacity=(cap, 0, 0, 0), w_sh=10, w_speed=1.0)
+    lx = w["nx"] * p.dx
+    las = laser(w["a0"], LAM0, w["w0"], w["tau"], xc=w["xc_frac"] * lx, xf=w["xc_frac"] * lx)
+    n0 = n_over_nc_to_n0(w["n_over_nc"], LAM0)
+    src = plasma(0, w["ppc"][0], w["ppc"][1], w["ppc"][2] if w["ndim"] == 3 else 1, -1, n0 / ppc,
+                 x_start=p.gxmin + w["x_plasma"], x_end=1.0e7, y_min=p.gymin, y_max=p.gymax,
+                 z_min=p.gzmin, z_max=p.gzmax, jitter=0.5, seed=20241203)
+    return p, las, src, ppc
+
+
+def load_device(name, precision, host_injection=False):
+    from aladyn_b200.sim import PicDevice
+    p, las, src, ppc = make_workload(name, precision)
+    dev = PicDevice(p)
+    dev.init_laser(las)
+    if host_injection:
+        # the device loads the initial columns; later columns come from the host
+        from aladyn_b200.config import plasma
+        s2 = plasma(src.ic, src.npx, src.npy, src.npz, src.charge, src.wgh, x_start=src.x_start,
+                    x_end=p.xmax + 1e-9, y_min=src.y_min, y_max=src.y_max, z_min=src.z_min,
+                    z_max=src.z_max, jitter=src.jitter, seed=src.seed)
+        dev.set_plasma_source(s2)
+    else:
+        dev.set_plasma_source(src)
+    dev.load_plasma(0)
+    return dev, p, las, src, ppc
+
+
+def rel_l2_errors(fa, fb, p):
+    sl = (slice(2, p.nx + 2), slice(2, p.ny + 2), slice(2, p.nz + 2) if p.ndim == 3 else slice(0, 1))
+    out = []
+    for c in range(p.nfield):
+        a, b = fa[sl + (c,)], fb[sl + (c,)]
+        nb = float(np.linalg.norm(b))
+        out.append(float(np.linalg.norm(a - b)) / nb if nb > 0 else 0.0)
+    return out
+
+
+def timed_steps(dev, p, t, it, k, torch):
+    """Run k steps; device time by CUDA events on the library's stream."""
+    s = torch.cuda.ExternalStream(dev.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    dev.synchronize()
+    e0.record(s)
+    nsum = 0
+    for _ in range(k):
+        out = dev.lp_run(t, it, initial_time=(it == 0))
+        nsum += out.np[0] + out.removed[0] - out.injected[0]  # particles pushed this step
+        t += p.dt
+        it += 1
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1), nsum, t, it, out
+
+
+def run_form(name, precision, warmup, steps, torch, barrier, keep_fields=False):
+    """Warm-up, then the timed region with profiling timers on."""
+    dev, p, las, src, ppc = load_device(name, precision)
+    t, it = 0.0, 0
+    for _ in range(warmup):
+        dev.lp_run(t, it, initial_time=(it == 0))
+        t += p.dt
+        it += 1
+    dev.set_profiling(True)
+    dev.reset_timers()
+    barrier()
+    ms, pushes, t, it, out = timed_steps(dev, p, t, it, steps, torch)
+    tm = dev.timers()
+    fields = dev.get_fields() if keep_fields else None
+    res = dict(ms=ms, pushes=pushes, np=out.np[0], err=out.error_bits, timers=tm, p=p, ppc=ppc,
+               fields=fields, steps=steps)
+    dev.close()
+    return res
+
+
+def run_e2e(name, precision, warmup, steps, torch, barrier):
+    """Through the C-ABI with host buffers: the host supplies the window
+    injection records from pinned memory and reads the step output and the
+    FP64 diagnostics every step."""
+    from aladyn_b200.lattice import LatticeHost
+    dev, p, las, src, ppc = load_device(name, precision, host_injection=True)
+    host = LatticeHost(p, src)
+    host.nptx = host.columns_end(1, p.xmax, False)
+    # window schedule of lp_window_xshift (window.f90:276-347), replayed on
+    # the host to prepare every step's injection records before timing
+    total = warmup + steps
+    xlapse, wi1, xmax = 0.0, 0, p.xmax
+    inject = {}
+    for it in range(total):
+        tt = it * p.dt  # only the wi/wf window bounds use t; they are open here
+        if p.w_sh > 0 and it % p.w_sh == 0 and p.wi_time <= tt < p.wf_time:
+            if it == 0:
+                xlapse, wi1 = 0.0, 0
+                continue
+            xlapse = xlapse + p.w_speed * p.dt * float(p.w_sh)
+            wi2 = int(math.floor(abs(p.dx_inv * xlapse) + 0.5))
+            nshx = wi2 - wi1
+            wi1 = wi2
+            xmax = xmax + p.dx * float(nshx)
+            rec = host.inject_after_shift(xmax)
+            if rec.shape[0] > 0:
+                buf = torch.empty(rec.shape[::-1], dtype=torch.float64, pin_memory=True).numpy().T
+                buf[...] = rec
+                inject[it] = buf
+    t, it = 0.0, 0
+    h2d = 0
+    nsum = 0
+    for phase, k in (("warm", warmup), ("timed", steps)):
+        if phase == "timed":
+            barrier()
+            s = torch.cuda.ExternalStream(dev.stream())
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            dev.synchronize()
+            e0.record(s)
+        for _ in range(k):
+            out = dev.lp_run(t, it, initial_time=(it == 0))
+            if phase == "timed":
+                nsum += out.np[0] + out.removed[0] - out.injected[0]
+            if it in inject:
+                dev.window_inject(0, inject[it])
+                if phase == "timed":
+                    h2d += inject[it].nbytes
+            dev.diag()
+            t += p.dt
+            it += 1
+        if phase == "timed":
+            e1.record(s)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+    from aladyn_b200.abi import AgpuDiagOut, AgpuStepOut
+    d2h = steps * (C.sizeof(AgpuStepOut) + C.sizeof(AgpuDiagOut))
+    dev.close()
+    return dict(ms=ms, pushes=nsum, h2d=h2d / steps, d2h=d2h / steps)
+
+
+# --------------------------------------------------------------------------
+# CPU: the oracle (FP64 restatement of the reference's arithmetic)
+# --------------------------------------------------------------------------
+def cpu_sample(name, budget_s=15.0, threads=None, warmup=0, steps=None):
+    """The oracle on a bounded sample of the workload: the same cell size,
+    time step, plasma and laser on a sub-box with the same particles per cell
+    (the transverse and longitudinal extent reduced), stepped for about
+    budget_s seconds on all host cores."""
+    from aladyn_b200.abi import AGPU_FP64
+    from aladyn_b200.config import Grid, laser, make_params, n_over_nc_to_n0, plasma
+    from aladyn_b200.initial import laser_fields
+    from oracle.oracle import Oracle
+    w = dict(WORKLOADS[name])
+    if w["ndim"] == 3:
+        w.update(nx=256, ny=64, nz=64)
+    else:
+        w.update(nx=512, ny=128)
+    threads = threads or os.cpu_count() or 1
+    g = Grid(w["ndim"], w["nx"], w["ny"], w["nz"], w["k0"], w["yx_rat"], w["zx_rat"], w["cfl"])
+    ppc = w["ppc"][0] * w["ppc"][1] * (w["ppc"][2] if w["ndim"] == 3 else 1)
+    ncell = w["nx"] * w["ny"] * (w["nz"] if w["ndim"] == 3 else 1)
+    p = make_params(g, precision=AGPU_FP64, capacity=(int(ncell * ppc * 1.1) + 4096, 0, 0, 0), w_sh=10)
+    lx = w["nx"] * p.dx
+    las = laser(w["a0"], LAM0, min(w["w0"], 0.25 * w["ny"] * p.dy), w["tau"], xc=w["xc_frac"] * lx,
+                xf=w["xc_frac"] * lx)
+    n0 = n_over_nc_to_n0(w["n_over_nc"], LAM0)
+    src = plasma(0, w["ppc"][0], w["ppc"][1], w["ppc"][2] if w["ndim"] == 3 else 1, -1, n0 / ppc,
+                 x_start=p.gxmin + min(w["x_plasma"], 0.2 * lx), x_end=1.0e7, y_min=p.gymin, y_max=p.gymax,
+                 z_min=p.gzmin, z_max=p.gzmax, jitter=0.5, seed=20241203)
+    ora = Oracle(p, threads=threads)
+    ora.set_fields(laser_fields(p, las))
+    ora.set_plasma_source(src)
+    ora.load_plasma(0)
+    t, it, pushes = 0.0, 0, 0
+    for _ in range(warmup):
+        ora.lp_run(t, it, initial_time=(it == 0))
+        t += p.dt
+        it += 1
+    t0 = time.perf_counter()
+    done = 0
+    while True:
+        n = ora.count(0)
+        rc, out = ora.lp_run(t, it, initial_time=(it == 0))
+        pushes += n
+        t += p.dt
+        it += 1
+        done += 1
+        el = time.perf_counter() - t0
+        if steps is not None:
+            if done >= steps:
+                break
+        elif el >= budget_s or done >= 200:
+            break
+    sample = (f"{w['nx']}x{w['ny']}" + (f"x{w['nz']}" if w["ndim"] == 3 else "") +
+              f" cells, {ppc} ppc, {n} particles, {done} timed steps after {warmup} warm-up, "
+              f"FP64 oracle on {threads} threads")
+    return dict(value=pushes / el, cores=threads, sample=sample, steps=done, seconds=el)
+
+
+# --------------------------------------------------------------------------
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true", help="skip nvidia-smi sampling (profiler runs)")
+    a = ap.parse_args(argv)
+    a.warmup = max(a.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    w = WORKLOADS[a.workload]
+    ppc_w = w["ppc"][0] * w["ppc"][1] * (w["ppc"][2] if w["ndim"] == 3 else 1)
+    config = {"workload": a.workload, "grid": [w["nx"], w["ny"], w["nz"]], "ppc": ppc_w,
+              "shapes": "quadratic/linear staggered (reference qlh + Esirkepov)", "window": "moving, w_sh=10",
+              "l2": "inputs larger than L2 (particle arrays of tens of GB)", "replicas": world}
+    metric = "particle-pushes/s"
+
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        r = cpu_sample(a.workload, warmup=a.warmup, steps=a.steps)
+        line = {"metric": metric, "value": r["value"], "unit": "pushes/s", "n_gpus": a.gpus,
+                "steps": r["steps"], "warmup": a.warmup, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": config, "impl": "reference",
+                "cpu_baseline": {"value": r["value"], "unit": "pushes/s", "cores": r["cores"], "kind": "port",
+                                 "sample": r["sample"]},
+                "e2e": {"value": r["value"], "unit": "pushes/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+        def barrier():
+            dist.barrier()
+            torch.cuda.synchronize()
+
+        def maxred(x):
+            tt = torch.tensor([x], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            return float(tt.item())
+
+        def sumred(x):
+            tt = torch.tensor([x], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.SUM)
+            return float(tt.item())
+    else:
+        def barrier():
+            torch.cuda.synchronize()
+
+        def maxred(x):
+            return x
+
+        def sumred(x):
+            return x
+
+    from aladyn_b200.abi import AGPU_FP32_SPLIT, AGPU_FP64
+    clk = ClockSampler(torch.cuda.current_device() if world == 1 else local)
+    if not a.no_clocks:
+        clk.start()
+    r32 = run_form(a.workload, AGPU_FP32_SPLIT, a.warmup, a.steps, torch, barrier, keep_fields=(world == 1))
+    r64 = run_form(a.workload, AGPU_FP64, a.warmup, a.steps, torch, barrier, keep_fields=(world == 1))
+    clocks = clk.stop()
+    err = None
+    if r32["fields"] is not None and r64["fields"] is not None:
+        err = rel_l2_errors(r32["fields"], r64["fields"], r32["p"])
+        r32["fields"] = r64["fields"] = None
+    ms32 = maxred(r32["ms"])
+    ms64 = maxred(r64["ms"])
+    pushes32 = sumred(r32["pushes"])
+    pushes64 = sumred(r64["pushes"])
+    value = pushes32 / (ms32 * 1e-3)
+    value64 = pushes64 / (ms64 * 1e-3)
+
+    e2e = None
+    if not a.no_e2e:
+        r = run_e2e(a.workload, AGPU_FP32_SPLIT, a.warmup, a.steps, torch, barrier)
+        ms = maxred(r["ms"])
+        e2e = {"value": sumred(r["pushes"]) / (ms * 1e-3), "unit": "pushes/s",
+               "h2d_bytes_per_step": int(r["h2d"]), "d2h_bytes_per_step": int(r["d2h"]),
+               "path": "agpu_step + agpu_window_inject (pinned host records) + agpu_diag per step"}
+
+    peak, peak_kind = measured_peaks()
+    tm = r32["timers"]
+    bpp = bytes_per_push(w["ndim"], ppc_w, True)
+    ms_push = tm.ms_push_deposit
+    achieved = bpp * tm.pushes / (ms_push * 1e-3) / 1e9 if ms_push > 0 else None
+    p = r32["p"]
+    cells = p.nx * p.ny * (p.nz if p.ndim == 3 else 1)
+    yee32 = yee_bytes_per_cell(p.ndim, True) * cells * a.steps / (tm.ms_yee * 1e-3) / 1e9 if tm.ms_yee else None
+    tm64 = r64["timers"]
+    yee64 = yee_bytes_per_cell(p.ndim, False) * cells * a.steps / (tm64.ms_yee * 1e-3) / 1e9 if tm64.ms_yee else None
+    push64 = bytes_per_push(w["ndim"], ppc_w, False) * tm64.pushes / (tm64.ms_push_deposit * 1e-3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        c = cpu_sample(a.workload, budget_s=a.cpu_budget)
+        cpu = {"value": c["value"], "unit": "pushes/s", "cores": c["cores"], "kind": "port", "sample": c["sample"]}
+
+    if rank == 0:
+        line = {
+            "metric": metric, "value": value, "unit": "pushes/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms32 / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32-split (int node + f32 offset, f32 fields/momenta/currents)",
+            "data": "synthetic: seeded jittered lattice plasma + Gaussian laser", "config": config,
+            "fp64": {"value": value64, "unit": "pushes/s", "ms_per_step": ms64 / a.steps,
+                     "push_deposit_gbs": push64, "yee_gbs": yee64},
+            "fp32_over_fp64": value / value64,
+            "field_error_fp32_vs_fp64": {"rel_l2_per_component": err, "after_steps": a.warmup + a.steps},
+            "yee_gbs": {"fp32": yee32, "fp64": yee64,
+                        "note": "algorithmic 15 words/cell over the Yee phase (boundaries, current fold, 3 sweeps)"},
+            "roofline": {"bound": "hbm", "kernel": "k32_push_dep (gather+push+deposit, FP32 split)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+                         "bytes_per_push": bpp, "traffic": None},
+            "phase_ms_per_step": {"push_deposit": tm.ms_push_deposit / a.steps, "yee": tm.ms_yee / a.steps,
+                                  "sort_compact": tm.ms_sort / a.steps, "window": tm.ms_window / a.steps},
+            "gpu_launches": int(tm.launches_total),
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "error_bits": r32["err"] | r64["err"],
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -301,6 +301,7 @@ void ora_shape_qden(double xp, double* ax3, int* ix) { ora_qden_1d(xp, ax3, ix);
 static void ora_gather(ora_sim* s, int ic, int64_t np) {
   const agpu_params* p = &s->p;
   if (p->ndim == 2) {
+    #pragma omp parallel for schedule(static) num_threads(s->nthreads) if (s->nthreads > 1)
     for (int64_t n = 1; n <= np; ++n) {
       double xl = p->dx_inv * (PART(s, ic, n, 1) - p->xmn);
       double yl = p->dy_inv * (PART(s, ic, n, 2) - p->ymn);
@@ -339,6 +340,7 @@ static void ora_gather(ora_sim* s, int ic, int64_t np) {
     }
     return;
   }
+  #pragma omp parallel for schedule(static) num_threads(s->nthreads) if (s->nthreads > 1)
   for (int64_t n = 1; n <= np; ++n) {
     double xl = p->dx_inv * (PART(s, ic, n, 1) - p->xmn);
     double yl = p->dy_inv * (PART(s, ic, n, 2) - p->ymn);
@@ -403,6 +405,7 @@ static void ora_gather(ora_sim* s, int ic, int64_t np) {
 /* A6: field_charge_multiply (src/dynamics/curr_and_fields_util.f90:58-72) */
 static void ora_field_charge_multiply(ora_sim* s, int ic, int64_t np) {
   int ch = s->ndv;
+  #pragma omp parallel for schedule(static) num_threads(s->nthreads) if (s->nthreads > 1)
   for (int64_t n = 1; n <= np; ++n) {
     ora_pack w = ora_unpack(PART(s, ic, n, ch));
     double q = (double)w.charge;
@@ -415,6 +418,7 @@ static void ora_init_lpf_momenta(ora_sim* s, int ic, int64_t np) {
   double dth_lp = 0.5 * s->p.dt;
   double alp = dth_lp * s->p.lorentz_fact[ic];
   if (s->p.curr_ndim == 2) {
+    #pragma omp parallel for schedule(static) num_threads(s->nthreads) if (s->nthreads > 1)
     for (int64_t p = 1; p <= np; ++p) {
       double efp[3];
       for (int c = 0; c < 3; ++c) efp[c] = -alp * PT(s, p, c + 1);
@@ -427,6 +431,7 @@ static void ora_init_lpf_momenta(ora_sim* s, int ic, int64_t np) {
     }
     return;
   }
+  #pragma omp parallel for schedule(static) num_threads(s->nthreads) if (s->nthreads > 1)
   for (int64_t p = 1; p <= np; ++p) {
     double pp[3] = {PART(s, ic, p, 4), PART(s, ic, p, 5), PART(s, ic, p, 6)};
     double efp[6];
@@ -448,6 +453,7 @@ static void ora_push(ora_sim* s, int ic, int64_t np) {
   int ch;
   if (s->p.curr_ndim == 2) {
     ch = 5;
+    #pragma omp parallel for schedule(static) num_threads(s->nthreads) if (s->nthreads > 1)
     for (int64_t p = 1; p <= np; ++p) {
       double pp1 = PART(s, ic, p, 3), pp2 = PART(s, ic, p, 4);
       double efp1 = alp * PT(s, p, 1), efp2 = alp * PT(s, p, 2), efp3 = alp * PT(s, p, 3);
@@ -478,6 +484,7 @@ static void ora_push(ora_sim* s, int ic, int64_t np) {
     }
   } else {
     ch = 7;
+    #pragma omp parallel for schedule(static) num_threads(s->nthreads) if (s->nthreads > 1)
     for (int64_t p = 1; p <= np; ++p) {
       double pp[3] = {PART(s, ic, p, 4), PART(s, ic, p, 5), PART(s, ic, p, 6)};
       double efp[6];
@@ -1380,6 +1387,7 @@ int ora_set_ionization_species(ora_sim* s, int ic, int an, int ion_min, int mode
 static void ora_set_ion_efield(ora_sim* s, int ic, int64_t np) {
   const agpu_params* p = &s->p;
   int id_ch = s->ndv;
+  #pragma omp parallel for schedule(static) num_threads(s->nthreads) if (s->nthreads > 1)
   for (int64_t n = 1; n <= np; ++n) {
     double ef_sqr = 0.;
     double xl = p->dx_inv * (PART(s, ic, n, 1) - p->xmn);
