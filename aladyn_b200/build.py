@@ -31,9 +31,13 @@ UNITS = [
     ("agpu_util.cu", ["-fmad=false"]),
     ("agpu_api.cu", ["-fmad=false"]),
     ("agpu_fp32.cu", ["-fmad=true"]),
+    ("agpu_tile64.cu", ["-fmad=false"]),
+    ("agpu_tile32.cu", ["-fmad=true"]),
+    ("agpu_bin.cu", ["-fmad=false"]),
     ("agpu_ionz.cpp", []),
 ]
-HEADERS = ["agpu_common.cuh", "agpu_kernels.h", "agpu_util.h", "agpu_yee.cuh", "agpu_ionz.h"]
+HEADERS = ["agpu_common.cuh", "agpu_kernels.h", "agpu_util.h", "agpu_yee.cuh", "agpu_ionz.h", "agpu_bin.cuh",
+           "agpu_tile.h", "agpu_select.cuh"]
 
 
 def _mtime(p: str) -> float:

@@ -12,8 +12,10 @@
 #include <vector>
 
 #include "../../include/aladyn_gpu.h"
+#include "agpu_bin.cuh"
 #include "agpu_ionz.h"
 #include "agpu_kernels.h"
+#include "agpu_tile.h"
 #include "agpu_util.h"
 
 using namespace agpu;
@@ -33,7 +35,7 @@ enum Phase { PH_PUSH = 0, PH_YEE, PH_SORT, PH_WINDOW, PH_IONIZE, PH_OTHER, PH_N 
 struct Counters {
   unsigned long long removed;
   unsigned int err;
-  unsigned int pad;
+  int alive;  // particles in tiles after the last binning
   double fmax;
 };
 
@@ -84,6 +86,16 @@ struct agpu_handle {
   int at_num[4] = {0, 0, 0, 0}, ion_min[4] = {0, 0, 0, 0}, model[4] = {0, 0, 0, 0};
   bool auto_table[4] = {false, false, false, false};
   int nsp_ionz = 1;
+  // spatial tiles of the running species: key / perm per particle,
+  // histogram (ntiles+1), tile starts (ntiles+2), scatter cursors
+  TileGeo tg{};
+  int* key[4] = {nullptr, nullptr, nullptr, nullptr};
+  int* perm[4] = {nullptr, nullptr, nullptr, nullptr};
+  int* hist[4] = {nullptr, nullptr, nullptr, nullptr};
+  int* tstart[4] = {nullptr, nullptr, nullptr, nullptr};
+  int* cursor = nullptr;
+  bool binned[4] = {false, false, false, false};
+  long long nalive[4] = {0, 0, 0, 0};  // np minus removed records still stored
   // flags
   bool fields_set = false;
   bool deterministic = false;
@@ -145,8 +157,6 @@ void ph_end(agpu_handle* h, int ph) {
   *slots[ph] += ms;
 }
 
-int check_ptr(const void* p) { return p ? 0 : AGPU_E_ARG; }
-
 int free_all(agpu_handle* h) {
   cudaFree(h->ebf);
   cudaFree(h->jc);
@@ -177,6 +187,13 @@ int free_all(agpu_handle* h) {
   cudaFreeHost(h->scr.h_total);
   cudaFree(h->d_diag);
   for (int i = 0; i < 4; ++i) cudaFree(h->d_wtab[i]);
+  for (int i = 0; i < 4; ++i) {
+    cudaFree(h->key[i]);
+    cudaFree(h->perm[i]);
+    cudaFree(h->hist[i]);
+    cudaFree(h->tstart[i]);
+  }
+  cudaFree(h->cursor);
   for (int i = 0; i < 2 * PH_N; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
   if (h->st) cudaStreamDestroy(h->st);
@@ -222,9 +239,12 @@ long long lattice_columns_end(const agpu_handle* h, int ic, long long i1, double
   return i2;
 }
 
+int drop_removed(agpu_handle* h, int ic);
+
 int add_lattice_columns(agpu_handle* h, int ic, long long i1, long long i2) {
   long long n = (i2 - i1 + 1) * (long long)h->npty[ic] * h->nptz[ic];
   if (n <= 0) return 0;
+  if (int rc = drop_removed(h, ic)) return rc;
   if (h->np[ic] + n > h->cap[ic]) {
     h->error_bits |= AGPU_EBIT_CAPACITY;
     return AGPU_E_CAPACITY;
@@ -256,14 +276,38 @@ int add_lattice_columns(agpu_handle* h, int ic, long long i1, long long i2) {
   CK(cudaGetLastError());
   h->timers.launches_total += 1;
   h->np[ic] += n;
+  h->nalive[ic] += n;
+  h->binned[ic] = false;
   return 0;
 }
 
 // Stable removal of the particles of species ic outside the box; x only when
 // window is set (cell_part_dist(.true.)), else x, y and z.
+int drop_removed(agpu_handle* h, int ic);
+
 int compact_species(agpu_handle* h, int ic, bool window) {
   if (h->np[ic] <= 0) return 0;
   long long kept;
+  if (window && h->binned[ic]) {
+    // the window compaction copies the alive records along the tile
+    // permutation: the drop of x <= xmin and a physical sort by tile at once
+    if (h->fp32) {
+      kept = perm_compact32(h->perm[ic], h->nalive[ic], h->sp[ic].view(), h->sptmp.view(), true, h->g.n1p, h->p.nx, h->scr,
+                            h->st);
+      std::swap(h->sp[ic], h->sptmp);
+    } else {
+      kept = perm_compact64(h->perm[ic], h->nalive[ic], h->part[ic], h->tmp, h->cap[ic], h->ndv, true, h->p.gxmin,
+                            h->p.gxmax, h->scr, h->st);
+      std::swap(h->part[ic], h->tmp);
+    }
+    CK(cudaGetLastError());
+    h->timers.launches_total += 3;
+    h->np[ic] = kept;
+    h->nalive[ic] = kept;
+    h->binned[ic] = false;
+    return 0;
+  }
+  if (int rc = drop_removed(h, ic)) return rc;
   if (h->fp32) {
     int nx = h->p.nx, ny = h->p.ny, nz = h->p.nz;
     kept = compact32(h->sp[ic].view(), h->sptmp.view(), h->np[ic], h->g.n1p, h->g.n2p, nx, ny, nz, window ? 0 : 1,
@@ -279,6 +323,148 @@ int compact_species(agpu_handle* h, int ic, bool window) {
   CK(cudaGetLastError());
   h->timers.launches_total += 3;  // count, scan, scatter
   h->np[ic] = kept;
+  h->nalive[ic] = kept;
+  h->binned[ic] = false;
+  return 0;
+}
+
+// ---- binning of the running species ---------------------------------------
+bool tiled(const agpu_handle* h, int ic) { return !h->deterministic && ic < h->p.nsp_run && h->key[ic] != nullptr; }
+
+// Keys from the current positions, histogram, scan and permutation.
+int rebin(agpu_handle* h, int ic) {
+  const TileGeo& t = h->tg;
+  CK(cudaMemsetAsync(h->hist[ic], 0, sizeof(int) * (t.ntiles + 1), h->st));
+  if (h->fp32)
+    bin_keys_split(h->sp[ic].cell, h->np[ic], h->g, t, h->key[ic], h->hist[ic], &h->d_cnt->err, h->st, h->sms);
+  else
+    bin_keys_abs(h->part[ic], h->part[ic] + h->cap[ic], h->part[ic] + 2 * h->cap[ic], h->np[ic], h->g, t, h->p.xmn, h->p.ymn,
+                 h->p.zmn, h->p.dx_inv, h->p.dy_inv, h->p.dz_inv, h->key[ic], h->hist[ic], &h->d_cnt->err, h->st, h->sms);
+  bin_finish(h->key[ic], h->np[ic], t, h->hist[ic], h->tstart[ic], h->cursor, h->perm[ic], h->st, h->sms);
+  CK(cudaGetLastError());
+  h->timers.launches_total += 3;
+  CK(cudaMemcpyAsync(&h->d_cnt->alive, h->tstart[ic] + t.ntiles, sizeof(int), cudaMemcpyDeviceToDevice, h->st));
+  if (int rc = read_counters(h)) return rc;
+  h->nalive[ic] = h->h_cnt->alive;
+  h->binned[ic] = true;
+  return 0;
+}
+
+// Drop the removed records (key == ntiles) keeping the memory order, so the
+// stored arrays hold exactly the alive particles; the binning is then stale.
+int drop_removed(agpu_handle* h, int ic) {
+  if (!h->binned[ic] || h->nalive[ic] == h->np[ic]) return 0;
+  long long kept;
+  if (h->fp32) {
+    kept = compact_flag32(h->key[ic], h->tg.ntiles, h->sp[ic].view(), h->sptmp.view(), h->np[ic], h->scr, h->st);
+    std::swap(h->sp[ic], h->sptmp);
+  } else {
+    kept = compact_flag64(h->key[ic], h->tg.ntiles, h->part[ic], h->tmp, h->cap[ic], h->np[ic], h->ndv, h->scr, h->st);
+    std::swap(h->part[ic], h->tmp);
+  }
+  CK(cudaGetLastError());
+  h->timers.launches_total += 3;
+  h->np[ic] = kept;
+  h->nalive[ic] = kept;
+  h->binned[ic] = false;
+  return 0;
+}
+
+// Tiled gather + push + deposit of species ic, then the next binning from
+// the keys the kernel wrote.  Removed particles stay stored (key ntiles)
+// until the next compaction.
+int tiled_push(agpu_handle* h, int ic, int initial_time, agpu_step_out* out) {
+  const agpu_params& p = h->p;
+  if (!h->binned[ic]) {
+    ph_begin(h, PH_SORT);
+    int rc = rebin(h, ic);
+    ph_end(h, PH_SORT);
+    if (rc) return rc;
+  }
+  const long long alive0 = h->nalive[ic];
+  hist_reset(h->hist[ic], h->tstart[ic], h->tg, h->np[ic], false, h->st);
+  ph_begin(h, PH_PUSH);
+  if (h->fp32) {
+    TileArgs32 a;
+    a.g = h->g;
+    a.t = h->tg;
+    a.ebf = h->ebf32;
+    a.jhi = h->jhi;
+    a.jlo = h->jlo;
+    const Species32& s = h->sp[ic];
+    a.p = Part32{s.cell, s.ox, s.oy, s.oz, s.px, s.py, s.pz, s.slot};
+    a.perm = h->perm[ic];
+    a.tstart = h->tstart[ic];
+    a.key = h->key[ic];
+    a.hist = h->hist[ic];
+    a.dth = (float)(0.5 * p.dt);
+    a.lfact = (float)p.lorentz_fact[ic];
+    a.dtx = (float)(p.dt * p.dx_inv);
+    a.dty = (float)(p.dt * p.dy_inv);
+    a.dtz = (float)(p.dt * p.dz_inv);
+    a.initial = initial_time ? 1 : 0;
+    a.err = &h->d_cnt->err;
+    tile_push32(a, h->st);
+  } else {
+    TileArgs64 a;
+    a.g = h->g;
+    a.t = h->tg;
+    a.ebf = h->ebf;
+    a.jc = h->jc;
+    double* b = h->part[ic];
+    long long cp = h->cap[ic];
+    a.x = b;
+    a.y = b + cp;
+    if (p.ndim == 3) {
+      a.z = b + 2 * cp;
+      a.px = b + 3 * cp;
+      a.py = b + 4 * cp;
+      a.pz = b + 5 * cp;
+      a.slot = b + 6 * cp;
+    } else {
+      a.z = nullptr;
+      a.px = b + 2 * cp;
+      a.py = b + 3 * cp;
+      a.pz = nullptr;
+      a.slot = b + 4 * cp;
+    }
+    a.perm = h->perm[ic];
+    a.tstart = h->tstart[ic];
+    a.key = h->key[ic];
+    a.hist = h->hist[ic];
+    a.xmn = p.xmn;
+    a.ymn = p.ymn;
+    a.zmn = p.zmn;
+    a.dx_inv = p.dx_inv;
+    a.dy_inv = p.dy_inv;
+    a.dz_inv = p.dz_inv;
+    a.dt = p.dt;
+    a.dth = 0.5 * p.dt;
+    a.lfact = p.lorentz_fact[ic];
+    a.gxmin = p.gxmin;
+    a.gxmax = p.gxmax;
+    a.gymin = p.gymin;
+    a.gymax = p.gymax;
+    a.gzmin = p.gzmin;
+    a.gzmax = p.gzmax;
+    a.initial = initial_time ? 1 : 0;
+    a.err = &h->d_cnt->err;
+    tile_push64(a, h->st);
+  }
+  CK(cudaGetLastError());
+  ph_end(h, PH_PUSH);
+  h->timers.launches_push_deposit += 1;
+  h->timers.launches_total += 2;  // histogram reset + tile kernel
+  h->timers.pushes += alive0;
+  ph_begin(h, PH_SORT);
+  bin_finish(h->key[ic], h->np[ic], h->tg, h->hist[ic], h->tstart[ic], h->cursor, h->perm[ic], h->st, h->sms);
+  CK(cudaGetLastError());
+  h->timers.launches_total += 2;  // scan + scatter
+  CK(cudaMemcpyAsync(&h->d_cnt->alive, h->tstart[ic] + h->tg.ntiles, sizeof(int), cudaMemcpyDeviceToDevice, h->st));
+  if (int rc = read_counters(h)) return rc;
+  ph_end(h, PH_SORT);
+  h->nalive[ic] = h->h_cnt->alive;
+  out->removed[ic] += alive0 - h->nalive[ic];
   return 0;
 }
 
@@ -425,6 +611,7 @@ int ionize64(agpu_handle* h, int iter, agpu_step_out* out) {
     k64_ionize<<<grid, 256, 0, h->st>>>(a);
     CK(cudaGetLastError());
     h->timers.launches_total += 2 + 3 + ((iter % 100 == 0) ? 1 : 0);  // efield, ionize, append, [max]
+    if (int rc = drop_removed(h, 0)) return rc;
     long long ne0 = h->np[0];
     long long added = append_electrons64(h->flag, np, h->part[ic], h->cap[ic], h->part[0], h->cap[0], ne0, h->cap[0],
                                          h->p.ndim, h->p.n_mol_atoms[ic], &h->d_cnt->err, h->scr, h->st);
@@ -434,6 +621,8 @@ int ionize64(agpu_handle* h, int iter, agpu_step_out* out) {
       added = h->cap[0] - ne0;
     }
     h->np[0] = ne0 + added;
+    h->nalive[0] = h->np[0];
+    if (added > 0) h->binned[0] = false;
     out->new_electrons += added;
   }
   return 0;
@@ -550,6 +739,17 @@ int agpu_create(const agpu_params* params, agpu_handle** out) {
       for (int ic = 0; ic < p.nsp && !rc; ++ic) rc |= alloc_species32(h->sp[ic], capmax, p.ndim);
       if (!rc) rc |= alloc_species32(h->sptmp, capmax, p.ndim);
     }
+  }
+  if (!rc) {
+    h->tg = make_tiles(g, p.nx, p.ny, p.nz);
+    for (int ic = 0; ic < p.nsp_run && !rc; ++ic) {
+      rc |= dmalloc((void**)&h->key[ic], sizeof(int) * capmax);
+      rc |= dmalloc((void**)&h->perm[ic], sizeof(int) * capmax);
+      rc |= dmalloc((void**)&h->hist[ic], sizeof(int) * (h->tg.ntiles + 1));
+      rc |= dmalloc((void**)&h->tstart[ic], sizeof(int) * (h->tg.ntiles + 2));
+    }
+    if (!rc) rc |= dmalloc((void**)&h->cursor, sizeof(int) * (h->tg.ntiles + 1));
+    if (capmax >= (1ll << 31)) rc |= AGPU_E_NOMEM;  // int32 particle indices in the permutation
   }
   if (!rc) {
     rc |= dmalloc((void**)&h->flag, sizeof(int) * capmax);
@@ -672,11 +872,16 @@ int agpu_set_species(agpu_handle* h, int32_t ic, const double* part, int64_t ld,
   }
   CK(cudaStreamSynchronize(h->st));
   h->np[ic] = np;
+  h->nalive[ic] = np;
+  h->binned[ic] = false;
   return 0;
 }
 
 int agpu_get_species(agpu_handle* h, int32_t ic, double* part, int64_t ld, int64_t* np, int32_t ndv) {
   if (!h || ic < 0 || ic >= h->p.nsp || !np) return AGPU_E_ARG;
+  if (h->binned[ic] && h->nalive[ic] != h->np[ic]) {
+    if (int rc = drop_removed(h, ic)) return rc;
+  }
   *np = h->np[ic];
   if (!part) return 0;
   if (ndv != h->ndv || ld < h->np[ic]) return AGPU_E_ARG;
@@ -700,7 +905,7 @@ int agpu_get_species(agpu_handle* h, int32_t ic, double* part, int64_t ld, int64
 
 int agpu_get_count(agpu_handle* h, int32_t ic, int64_t* np) {
   if (!h || !np || ic < 0 || ic >= h->p.nsp) return AGPU_E_ARG;
-  *np = h->np[ic];
+  *np = h->binned[ic] ? h->nalive[ic] : h->np[ic];
   return 0;
 }
 
@@ -830,6 +1035,12 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu
   for (int ic = 0; ic < p.nsp_run; ++ic) {
     long long np = h->np[ic];
     if (np <= 0) continue;
+    if (tiled(h, ic)) {
+      if (int rc_ = tiled_push(h, ic, initial_time, out)) return rc_;
+      continue;
+    }
+    if (int rc_ = drop_removed(h, ic)) return rc_;
+    np = h->np[ic];
     CK(cudaMemsetAsync(&h->d_cnt->removed, 0, sizeof(unsigned long long), h->st));
     ph_begin(h, PH_PUSH);
     if (h->fp32) {
@@ -941,7 +1152,7 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu
     }
   }
   if (int rc_ = read_counters(h)) return rc_;
-  for (int ic = 0; ic < 4; ++ic) out->np[ic] = h->np[ic];
+  for (int ic = 0; ic < 4; ++ic) out->np[ic] = h->binned[ic] ? h->nalive[ic] : h->np[ic];
   out->xmn = p.xmn;
   out->error_bits = h->error_bits;
   if (h->error_bits & AGPU_EBIT_CAPACITY) return AGPU_E_CAPACITY;
@@ -950,6 +1161,7 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu
 
 int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t ld, int64_t n, int32_t ndv) {
   if (!h || ic < 0 || ic >= h->p.nsp || ndv != h->ndv || n < 0 || (n > 0 && (!part || ld < n))) return AGPU_E_ARG;
+  if (int rc = drop_removed(h, ic)) return rc;
   if (h->np[ic] + n > h->cap[ic]) return AGPU_E_CAPACITY;
   if (n == 0) return 0;
   if (!h->fp32) {
@@ -966,12 +1178,16 @@ int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t l
   }
   CK(cudaStreamSynchronize(h->st));
   h->np[ic] += n;
+  h->nalive[ic] = h->np[ic];
+  h->binned[ic] = false;
   return 0;
 }
 
 int agpu_diag(agpu_handle* h, agpu_diag_out* out) {
   if (!h || !out) return AGPU_E_ARG;
   std::memset(out, 0, sizeof(*out));
+  for (int ic = 0; ic < h->p.nsp; ++ic)
+    if (int rc = drop_removed(h, ic)) return rc;
   CK(cudaMemsetAsync(h->d_diag, 0, sizeof(double) * 64, h->st));
   double dvol = h->p.dx * h->p.dy * (h->p.ndim == 3 ? h->p.dz : 1.0);
   if (h->fp32)

@@ -1,0 +1,193 @@
+// agpu_bin.cu — per-step binning of particles by spatial tile: a key per
+// particle (its tile, or the removed bin), a histogram, an exclusive scan and
+// a scatter of particle indices into the permutation perm, so that tile t's
+// particles are perm[tstart[t] .. tstart[t+1]).  The particle records stay
+// where they are; the permutation is rebuilt every step from the keys that
+// the push kernel writes, and the records are physically reordered along it
+// whenever the window compaction copies them.
+#include "agpu_bin.cuh"
+#include "agpu_util.h"
+#include "agpu_select.cuh"
+
+namespace agpu {
+
+// keys from the split form's node index
+__global__ void k_keys_split(const int* cell, long long np, Geo g, TileGeo t, int* key, int* hist, unsigned int* err) {
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < np; n += (long long)gridDim.x * blockDim.x) {
+    int c = cell[n];
+    int i = c % g.n1p + 1;
+    int r = c / g.n1p;
+    int j = r % g.n2p + 1;
+    int k = (g.ndim == 3) ? r / g.n2p + 1 : 3;
+    int kk = tile_key(t, i, j, k);
+    key[n] = kk;
+    if (kk == t.ntiles) raise_err(err, AGPU_EBIT_INDEX);  // a record outside the node range
+    hist_add(hist, kk);
+  }
+}
+
+// keys from FP64 absolute positions: node = int(3 + x_loc + 0.5) (qden)
+__global__ void k_keys_abs(const double* x, const double* y, const double* z, long long np, Geo g, TileGeo t,
+                           double xmn, double ymn, double zmn, double dxi, double dyi, double dzi, int* key, int* hist,
+                           unsigned int* err) {
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < np; n += (long long)gridDim.x * blockDim.x) {
+    double xx = 3.0 + dxi * (x[n] - xmn);
+    double yy = 3.0 + dyi * (y[n] - ymn);
+    int i = (xx > -1e9 && xx < 2e9) ? (int)(xx + 0.5) : -1;
+    int j = (yy > -1e9 && yy < 2e9) ? (int)(yy + 0.5) : -1;
+    int k = 3;
+    if (g.ndim == 3) {
+      double zz = 3.0 + dzi * (z[n] - zmn);
+      k = (zz > -1e9 && zz < 2e9) ? (int)(zz + 0.5) : -1;
+    }
+    int kk = tile_key(t, i, j, k);
+    key[n] = kk;
+    if (kk == t.ntiles) raise_err(err, AGPU_EBIT_INDEX);  // a record outside the node range
+    hist_add(hist, kk);
+  }
+}
+
+// Exclusive scan of hist[0..nb) into start[0..nb], one block.
+__global__ void k_scan_int(const int* hist, int nb, int* start) {
+  __shared__ long long part[1024];
+  int per = (nb + blockDim.x - 1) / blockDim.x;
+  int lo = threadIdx.x * per, hi = min(lo + per, nb);
+  long long s = 0;
+  for (int b = lo; b < hi; ++b) s += hist[b];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long run = 0;
+    for (int q = 0; q < (int)blockDim.x; ++q) {
+      long long v = part[q];
+      part[q] = run;
+      run += v;
+    }
+    start[nb] = (int)run;
+  }
+  __syncthreads();
+  long long run = part[threadIdx.x];
+  for (int b = lo; b < hi; ++b) {
+    start[b] = (int)run;
+    run += hist[b];
+  }
+}
+
+// perm[start[key] + rank] = n, ranks from warp-aggregated cursors.
+__global__ void k_perm_scatter(const int* key, long long np, const int* start, int* cursor, int* perm) {
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < np; n += (long long)gridDim.x * blockDim.x) {
+    int kk = key[n];
+    unsigned int act = __activemask();
+    unsigned int peers = __match_any_sync(act, kk);
+    int leader = __ffs(peers) - 1;
+    int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&cursor[kk], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    int rank = __popc(peers & ((1u << lane) - 1u));
+    perm[start[kk] + base + rank] = (int)n;
+  }
+}
+
+void bin_keys_split(const int* cell, long long np, const Geo& g, const TileGeo& t, int* key, int* hist, unsigned int* err,
+                    cudaStream_t st, int sms) {
+  if (np <= 0) return;
+  k_keys_split<<<grid_for(np, 256, sms, 16), 256, 0, st>>>(cell, np, g, t, key, hist, err);
+}
+void bin_keys_abs(const double* x, const double* y, const double* z, long long np, const Geo& g, const TileGeo& t,
+                  double xmn, double ymn, double zmn, double dxi, double dyi, double dzi, int* key, int* hist,
+                  unsigned int* err, cudaStream_t st, int sms) {
+  if (np <= 0) return;
+  k_keys_abs<<<grid_for(np, 256, sms, 16), 256, 0, st>>>(x, y, z, np, g, t, xmn, ymn, zmn, dxi, dyi, dzi, key, hist, err);
+}
+// hist has ntiles+1 bins (the last one: removed particles)
+void bin_finish(const int* key, long long np, const TileGeo& t, const int* hist, int* start, int* cursor, int* perm,
+                cudaStream_t st, int sms) {
+  k_scan_int<<<1, 1024, 0, st>>>(hist, t.ntiles + 1, start);
+  cudaMemsetAsync(cursor, 0, sizeof(int) * (t.ntiles + 1), st);
+  if (np > 0) k_perm_scatter<<<grid_for(np, 256, sms, 16), 256, 0, st>>>(key, np, start, cursor, perm);
+}
+
+// ---- compaction along the permutation (physical reorder by tile) --------
+struct PermAlive {
+  const int* perm;
+  long long nalive;
+  __device__ bool operator()(long long q) const { return q < nalive; }
+};
+struct PermAliveInBox64 {
+  const int* perm;
+  long long nalive;
+  const double* x;
+  double x0, x1;
+  __device__ bool operator()(long long q) const {
+    if (q >= nalive) return false;
+    double a = x[perm[q]];
+    return a > x0 && a <= x1;
+  }
+};
+struct PermMove64 {
+  const int* perm;
+  const double* src;
+  double* dst;
+  long long ld;
+  int ndv;
+  __device__ void operator()(long long q, long long o) const {
+    long long p = perm[q];
+    for (int c = 0; c < ndv; ++c) dst[(long long)c * ld + o] = src[(long long)c * ld + p];
+  }
+};
+long long perm_compact64(const int* perm, long long nalive, double* part, double* tmp, long long cap, int ndv, bool xbox,
+                         double x0, double x1, Scratch& s, cudaStream_t st) {
+  PermMove64 mv{perm, part, tmp, cap, ndv};
+  if (xbox) {
+    PermAliveInBox64 pr{perm, nalive, part, x0, x1};
+    return select_run(pr, mv, nalive, s, st);
+  }
+  PermAlive pr{perm, nalive};
+  return select_run(pr, mv, nalive, s, st);
+}
+
+struct PermAliveInBox32 {
+  const int* perm;
+  long long nalive;
+  const int* cell;
+  const float* ox;
+  int n1p, nx;
+  __device__ bool operator()(long long q) const {
+    if (q >= nalive) return false;
+    int p = perm[q];
+    int i = cell[p] % n1p + 1;
+    int m = i - 3;
+    float o = ox[p];
+    return ((m > 0) || (m == 0 && o > 0.f)) && ((m < nx) || (m == nx && o <= 0.f));
+  }
+};
+struct PermMove32 {
+  const int* perm;
+  Part32View src, dst;
+  __device__ void operator()(long long q, long long o) const {
+    int p = perm[q];
+    dst.cell[o] = src.cell[p];
+    dst.ox[o] = src.ox[p];
+    dst.oy[o] = src.oy[p];
+    dst.px[o] = src.px[p];
+    dst.py[o] = src.py[p];
+    dst.slot[o] = src.slot[p];
+    if (src.oz) {
+      dst.oz[o] = src.oz[p];
+      dst.pz[o] = src.pz[p];
+    }
+  }
+};
+long long perm_compact32(const int* perm, long long nalive, const Part32View& src, const Part32View& dst, bool xbox, int n1p,
+                         int nx, Scratch& s, cudaStream_t st) {
+  PermMove32 mv{perm, src, dst};
+  if (xbox) {
+    PermAliveInBox32 pr{perm, nalive, src.cell, src.ox, n1p, nx};
+    return select_run(pr, mv, nalive, s, st);
+  }
+  PermAlive pr{perm, nalive};
+  return select_run(pr, mv, nalive, s, st);
+}
+
+}  // namespace agpu

@@ -1,0 +1,53 @@
+// agpu_tile.h — arguments of the tiled gather/push/deposit kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "agpu_bin.cuh"
+#include "agpu_kernels.h"
+
+namespace agpu {
+
+// Tile extents in nodes (3D and 2D).
+constexpr int TILE3_X = 8, TILE3_Y = 8, TILE3_Z = 8;
+constexpr int TILE2_X = 16, TILE2_Y = 16;
+
+struct TileArgs32 {
+  Geo g;
+  TileGeo t;
+  const float* ebf;
+  float* jhi;
+  float* jlo;
+  Part32 p;
+  const int* perm;
+  const int* tstart;
+  int* key;   // new tile key per particle (ntiles = removed)
+  int* hist;  // next histogram, ntiles + 1 bins
+  float dth, lfact, dtx, dty, dtz;
+  int initial;
+  unsigned int* err;
+};
+
+struct TileArgs64 {
+  Geo g;
+  TileGeo t;
+  const double* ebf;
+  double* jc;
+  double *x, *y, *z, *px, *py, *pz;
+  const double* slot;
+  const int* perm;
+  const int* tstart;
+  int* key;
+  int* hist;
+  double xmn, ymn, zmn, dx_inv, dy_inv, dz_inv;
+  double dt, dth, lfact;
+  double gxmin, gxmax, gymin, gymax, gzmin, gzmax;
+  int initial;
+  unsigned int* err;
+};
+
+TileGeo make_tiles(const Geo& g, int nx, int ny, int nz);
+void tile_push32(const TileArgs32& a, cudaStream_t st);
+void tile_push64(const TileArgs64& a, cudaStream_t st);
+void hist_reset(int* hist, const int* tstart, const TileGeo& t, long long np, bool first, cudaStream_t st);
+
+}  // namespace agpu

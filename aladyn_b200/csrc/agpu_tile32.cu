@@ -1,0 +1,346 @@
+// agpu_tile32.cu — tiled gather + push + deposit of the FP32 split form.
+//
+// One CTA per spatial tile of TX x TY x TZ nodes.  The tile's particles are
+// the permutation range perm[tstart[t] .. tstart[t+1]) built by the binning
+// pass, so every particle's node lies inside the tile.  The CTA
+//   1. stages the six field components of the tile plus a one-node guard
+//      (the qlh gather stencil) into shared memory,
+//   2. zeroes a shared current tile with a two-node guard (the Esirkepov
+//      window of a particle that moves at most one node),
+//   3. gathers, pushes (exact-gamma Boris) and deposits every particle, the
+//      deposit going into shared memory with native FP32 shared atomics,
+//   4. flushes the shared currents to the global (hi, lo) pair once, with
+//      the TwoSum error of each global add accumulated into lo,
+//   5. writes each particle's new tile key and the next histogram.
+#include "agpu_bin.cuh"
+#include "agpu_common.cuh"
+#include "agpu_tile.h"
+
+namespace agpu {
+
+namespace {
+
+__device__ __forceinline__ void kadd_g(float* hi, float* lo, float v) {
+  float old = atomicAdd(hi, v);
+  float s = __fadd_rn(old, v);
+  float bp = __fsub_rn(s, old);
+  float err = __fadd_rn(__fsub_rn(old, __fsub_rn(s, bp)), __fsub_rn(v, bp));
+  if (err != 0.f) atomicAdd(lo, err);
+}
+
+__device__ __forceinline__ void wq(float s, float a[3]) {
+  float s2 = s * s;
+  a[1] = 0.75f - s2;
+  a[2] = 0.5f * (0.25f + s2 + s);
+  a[0] = 1.f - a[1] - a[2];
+}
+
+__device__ __forceinline__ void esirk1(const float a0[3], const float a1[3], int ih, float axh[5], float cur[5]) {
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    int m = q - ih;
+    axh[q] = (m == 0) ? a1[0] : (m == 1) ? a1[1] : (m == 2) ? a1[2] : 0.f;
+  }
+  cur[0] = -axh[0];
+  cur[1] = cur[0] + a0[0] - axh[1];
+  cur[2] = cur[1] + a0[1] - axh[2];
+  cur[3] = cur[2] + a0[2] - axh[3];
+  cur[4] = cur[3] - axh[4];
+}
+
+__device__ __forceinline__ int renorm(float& s) {
+  int m = (s >= 0.5f) ? 1 : ((s < -0.5f) ? -1 : 0);
+  s = s - (float)m;
+  return m;
+}
+__device__ __forceinline__ bool inside(int node, float o, int n) {
+  int m = node - 3;
+  return ((m > 0) || (m == 0 && o > 0.f)) && ((m < n) || (m == n && o <= 0.f));
+}
+
+}  // namespace
+
+template <int NDIM, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(256) k32_tile(TileArgs32 a) {
+  constexpr int FX = TX + 2, FY = TY + 2, FZ = (NDIM == 3) ? TZ + 2 : 1;
+  constexpr int JX = TX + 4, JY = TY + 4, JZ = (NDIM == 3) ? TZ + 4 : 1;
+  constexpr int FV = FX * FY * FZ, JV = JX * JY * JZ;
+  constexpr int NF = (NDIM == 3) ? 6 : 3, NC = (NDIM == 3) ? 3 : 2;
+  extern __shared__ float smem[];
+  float* sF = smem;           // NF * FV
+  float* sJ = smem + NF * FV;  // NC * JV
+
+  const Geo g = a.g;
+  const int t = blockIdx.x;
+  const int beg = a.tstart[t], end = a.tstart[t + 1];
+  if (beg >= end) return;
+  const int tx = t % a.t.ntx, ty = (t / a.t.ntx) % a.t.nty, tz = t / (a.t.ntx * a.t.nty);
+  const int i0t = 3 + tx * TX, j0t = 3 + ty * TY, k0t = (NDIM == 3) ? 3 + tz * TZ : 1;
+
+  // 1-2: stage fields (nodes i0t-1 .. i0t+TX), zero currents
+  for (int e = threadIdx.x; e < NF * FV; e += blockDim.x) {
+    int c = e / FV, r = e - c * FV;
+    int lx = r % FX, ly = (r / FX) % FY, lz = r / (FX * FY);
+    int gi = i0t - 1 + lx, gj = j0t - 1 + ly, gk = (NDIM == 3) ? k0t - 1 + lz : 1;
+    float v = 0.f;
+    if (gi >= 1 && gi <= g.n1p && gj >= 1 && gj <= g.n2p && gk >= 1 && gk <= g.n3p)
+      v = __ldg(&a.ebf[g.ncell * c + goff(g, gi, gj, gk)]);
+    sF[e] = v;
+  }
+  for (int e = threadIdx.x; e < NC * JV; e += blockDim.x) sJ[e] = 0.f;
+  __syncthreads();
+
+  const int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
+  for (int q = beg + threadIdx.x; q < end; q += blockDim.x) {
+    const int p = a.perm[q];
+    const int c = a.p.cell[p];
+    const int i0 = c % g.n1p + 1;
+    const int r = c / g.n1p;
+    const int j0 = r % g.n2p + 1;
+    const int k0 = (NDIM == 3) ? r / g.n2p + 1 : 1;
+    float sx = a.p.ox[p], sy = a.p.oy[p], sz = (NDIM == 3) ? a.p.oz[p] : 0.f;
+    float pp[3] = {a.p.px[p], a.p.py[p], (NDIM == 3) ? a.p.pz[p] : 0.f};
+    const uint64_t sl = a.p.slot[p];
+    // local field coordinates of node i0-1 (the first stencil node)
+    const int fx = i0 - i0t, fy = j0 - j0t, fz = (NDIM == 3) ? k0 - k0t : 0;
+    if ((unsigned)fx >= (unsigned)TX || (unsigned)fy >= (unsigned)TY || (NDIM == 3 && (unsigned)fz >= (unsigned)TZ)) {
+      raise_err(a.err, AGPU_EBIT_INDEX);  // not binned in this tile: drop it
+      a.key[p] = a.t.ntiles;
+      hist_add(a.hist, a.t.ntiles);
+      continue;
+    }
+    float ax1[3], ay1[3], az1[3] = {0.f, 1.f, 0.f};
+    wq(sx, ax1);
+    wq(sy, ay1);
+    if (NDIM == 3) wq(sz, az1);
+    const float axh[2] = {0.5f - sx, sx + 0.5f};
+    const float ayh[2] = {0.5f - sy, sy + 0.5f};
+    const float azh[2] = {0.5f - sz, sz + 0.5f};
+    float ap[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (NDIM == 3) {
+      const float* e1 = sF;
+      const float* e2 = sF + FV;
+      const float* e3 = sF + 2 * FV;
+      const float* b1 = sF + 3 * FV;
+      const float* b2 = sF + 4 * FV;
+      const float* b3 = sF + 5 * FV;
+#pragma unroll
+      for (int k1 = 0; k1 < 3; ++k1) {
+#pragma unroll
+        for (int j1 = 0; j1 < 3; ++j1) {
+          int o = fx + FX * (fy + j1 + FY * (fz + k1));
+          ap[0] += ay1[j1] * az1[k1] * (axh[0] * e1[o] + axh[1] * e1[o + 1]);
+        }
+#pragma unroll
+        for (int j1 = 0; j1 < 2; ++j1) {
+          int o = fx + FX * (fy + j1 + FY * (fz + k1));
+          float dv = ayh[j1] * az1[k1];
+          ap[1] += dv * (ax1[0] * e2[o] + ax1[1] * e2[o + 1] + ax1[2] * e2[o + 2]);
+          ap[5] += dv * (axh[0] * b3[o] + axh[1] * b3[o + 1]);
+        }
+      }
+#pragma unroll
+      for (int k1 = 0; k1 < 2; ++k1) {
+#pragma unroll
+        for (int j1 = 0; j1 < 2; ++j1) {
+          int o = fx + FX * (fy + j1 + FY * (fz + k1));
+          ap[3] += ayh[j1] * azh[k1] * (ax1[0] * b1[o] + ax1[1] * b1[o + 1] + ax1[2] * b1[o + 2]);
+        }
+#pragma unroll
+        for (int j1 = 0; j1 < 3; ++j1) {
+          int o = fx + FX * (fy + j1 + FY * (fz + k1));
+          float dv = ay1[j1] * azh[k1];
+          ap[4] += dv * (axh[0] * b2[o] + axh[1] * b2[o + 1]);
+          ap[2] += dv * (ax1[0] * e3[o] + ax1[1] * e3[o + 1] + ax1[2] * e3[o + 2]);
+        }
+      }
+    } else {
+      const float* e1 = sF;
+      const float* e2 = sF + FV;
+      const float* b3 = sF + 2 * FV;
+#pragma unroll
+      for (int j1 = 0; j1 < 3; ++j1) {
+        int o = fx + FX * (fy + j1);
+        ap[0] += ay1[j1] * (axh[0] * e1[o] + axh[1] * e1[o + 1]);
+      }
+#pragma unroll
+      for (int j1 = 0; j1 < 2; ++j1) {
+        int o = fx + FX * (fy + j1);
+        ap[1] += ayh[j1] * (ax1[0] * e2[o] + ax1[1] * e2[o + 1] + ax1[2] * e2[o + 2]);
+        ap[5] += ayh[j1] * (axh[0] * b3[o] + axh[1] * b3[o + 1]);
+      }
+    }
+    const float qc = (float)slot_charge(sl);
+    if (a.initial) {
+      // init_lpf_momenta (boris_push.f90:34-73): p^0 -> p^{-1/2}
+      float alp0 = a.dth * a.lfact * qc;
+      float gi = rsqrtf(1.f + pp[0] * pp[0] + pp[1] * pp[1] + pp[2] * pp[2]);
+      float v0 = gi * pp[0], v1 = gi * pp[1], v2 = gi * pp[2];
+      float e[6];
+#pragma unroll
+      for (int cc = 0; cc < 6; ++cc) e[cc] = -alp0 * ap[cc];
+      pp[0] = pp[0] + e[0] + v1 * e[5] - v2 * e[4];
+      pp[1] = pp[1] + e[1] + v2 * e[3] - v0 * e[5];
+      pp[2] = pp[2] + e[2] + v0 * e[4] - v1 * e[3];
+    }
+    // exact-gamma Boris (boris_push.f90:75-168)
+    const float alp = a.dth * a.lfact * qc;
+    const float vp[3] = {pp[0] + alp * ap[0], pp[1] + alp * ap[1], pp[2] + alp * ap[2]};
+    const float bb[3] = {alp * ap[3], alp * ap[4], alp * ap[5]};
+    const float b2v = bb[0] * bb[0] + bb[1] * bb[1] + bb[2] * bb[2];
+    const float bv = bb[0] * vp[0] + bb[1] * vp[1] + bb[2] * vp[2];
+    const float gam02 = 1.f + vp[0] * vp[0] + vp[1] * vp[1] + vp[2] * vp[2] - b2v;
+    const float gam2 = 0.5f * (gam02 + sqrtf(gam02 * gam02 + 4.f * (b2v + bv * bv)));
+    const float gam = sqrtf(gam2);
+    const float inv = 1.f / (b2v + gam2);
+    float pn[3];
+    pn[0] = 2.f * (gam2 * vp[0] + bb[0] * bv + gam * (vp[1] * bb[2] - vp[2] * bb[1])) * inv - pp[0];
+    pn[1] = 2.f * (gam2 * vp[1] + bb[1] * bv + gam * (vp[2] * bb[0] - vp[0] * bb[2])) * inv - pp[1];
+    pn[2] = (NDIM == 3) ? 2.f * (gam2 * vp[2] + bb[2] * bv + gam * (vp[0] * bb[1] - vp[1] * bb[0])) * inv - pp[2] : 0.f;
+    const float dtg = rsqrtf(1.f + pn[0] * pn[0] + pn[1] * pn[1] + pn[2] * pn[2]);
+    float nsx = sx + a.dtx * dtg * pn[0];
+    float nsy = sy + a.dty * dtg * pn[1];
+    float nsz = (NDIM == 3) ? sz + a.dtz * dtg * pn[2] : 0.f;
+    const int mi = renorm(nsx), mj = renorm(nsy), mk = (NDIM == 3) ? renorm(nsz) : 0;
+    const int i1n = i0 + mi, j1n = j0 + mj, k1n = k0 + mk;
+    a.p.cell[p] = (int)goff(g, i1n, j1n, k1n);
+    a.p.ox[p] = nsx;
+    a.p.oy[p] = nsy;
+    a.p.px[p] = pn[0];
+    a.p.py[p] = pn[1];
+    if (NDIM == 3) {
+      a.p.oz[p] = nsz;
+      a.p.pz[p] = pn[2];
+    }
+    if (!(pn[0] == pn[0] && pn[1] == pn[1] && pn[2] == pn[2])) raise_err(a.err, AGPU_EBIT_NONFINITE);
+    bool keep = inside(i1n, nsx, nx) && inside(j1n, nsy, ny);
+    if (NDIM == 3) keep = keep && inside(k1n, nsz, nz);
+    int nkey = keep ? tile_key(a.t, i1n, j1n, (NDIM == 3) ? k1n : 3) : a.t.ntiles;
+    a.key[p] = nkey;
+    hist_add(a.hist, nkey);
+    if (!keep) continue;
+    // Esirkepov deposit into the shared tile (grid_part_connect.f90:956-1334).
+    // Old-plane and new-plane terms are regrouped onto the particle's 5-slot
+    // windows (slot 0 = old node - 2): each current component is one dense
+    // product over (x0..x1) x (y0..y1) [x (z0..z1)], 9-64 points.
+    const float wght = qc * slot_wgh(sl);
+    float ax0[3], ay0[3], axn[3], ayn[3];
+    wq(sx, ax0);
+    wq(sy, ay0);
+    wq(nsx, axn);
+    wq(nsy, ayn);
+    float sxh[5], cx[5], syh[5], cy[5];
+    const int ih = mi + 1, jh = mj + 1;
+    esirk1(ax0, axn, ih, sxh, cx);
+    esirk1(ay0, ayn, jh, syh, cy);
+    const int x0 = ih < 1 ? ih : 1, x1 = (ih + 2) > 3 ? ih + 2 : 3;
+    const int y0 = jh < 1 ? jh : 1, y1 = (jh + 2) > 3 ? jh + 2 : 3;
+#pragma unroll
+    for (int u = 0; u < 5; ++u) {
+      cx[u] *= wght;
+      cy[u] *= wght;
+    }
+    // local J coordinates of window slot 0 (node i0-2)
+    const int lx = i0 - i0t, ly = j0 - j0t;
+    float* sJx = sJ;
+    float* sJy = sJ + JV;
+    if (NDIM == 2) {
+      float wxs[5], wys[5];
+#pragma unroll
+      for (int u = 0; u < 5; ++u) {
+        wxs[u] = sxh[u] + ((u >= 1 && u <= 3) ? ax0[u - 1] : 0.f);
+        wys[u] = syh[u] + ((u >= 1 && u <= 3) ? ay0[u - 1] : 0.f);
+      }
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        if (v < y0 || v > y1) continue;
+#pragma unroll
+        for (int u = 0; u < 5; ++u) {
+          if (u < x0 || u > x1) continue;
+          int o = lx + u + JX * (ly + v);
+          atomicAdd(&sJx[o], wys[v] * cx[u]);
+          atomicAdd(&sJy[o], wxs[u] * cy[v]);
+        }
+      }
+    } else {
+      float az0[3], azn[3], szh[5], cz[5];
+      wq(sz, az0);
+      wq(nsz, azn);
+      const int kh = mk + 1;
+      esirk1(az0, azn, kh, szh, cz);
+      const int z0 = kh < 1 ? kh : 1, z1 = (kh + 2) > 3 ? kh + 2 : 3;
+      float wx0[5], wx1[5], wy0[5], wy1[5], b0[5], b1[5];
+#pragma unroll
+      for (int u = 0; u < 5; ++u) {
+        float a0x = (u >= 1 && u <= 3) ? ax0[u - 1] : 0.f;
+        float a0y = (u >= 1 && u <= 3) ? ay0[u - 1] : 0.f;
+        wx0[u] = 0.5f * sxh[u] + a0x;  // axh0
+        wx1[u] = sxh[u] + 0.5f * a0x;  // axh1
+        wy0[u] = 0.5f * syh[u] + a0y;  // ayh0
+        wy1[u] = syh[u] + 0.5f * a0y;  // ayh1
+        b0[u] = a0y;                   // old y shape on slots 1..3
+        int m = u - jh;
+        b1[u] = (m == 0) ? ayn[0] : (m == 1) ? ayn[1] : (m == 2) ? ayn[2] : 0.f;  // new y shape
+      }
+      float* sJz = sJ + 2 * JV;
+      for (int w = z0; w <= z1; ++w) {
+        const int m0 = w - 1, m1 = w - kh;
+        const float A0 = (m0 == 0) ? az0[0] : (m0 == 1) ? az0[1] : (m0 == 2) ? az0[2] : 0.f;
+        const float A1 = (m1 == 0) ? azn[0] : (m1 == 1) ? azn[1] : (m1 == 2) ? azn[2] : 0.f;
+        const float czw = wght * ((w == 0) ? cz[0] : (w == 1) ? cz[1] : (w == 2) ? cz[2] : (w == 3) ? cz[3] : cz[4]);
+        const int ow = lx + JX * (ly + JY * (k0 - k0t + w));
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          if (v < y0 || v > y1) continue;
+          const float wyv = wy0[v] * A0 + wy1[v] * A1;
+          const float cyv = cy[v];
+#pragma unroll
+          for (int u = 0; u < 5; ++u) {
+            if (u < x0 || u > x1) continue;
+            const int o = ow + u + JX * v;
+            atomicAdd(&sJx[o], cx[u] * wyv);
+            atomicAdd(&sJy[o], cyv * (wx0[u] * A0 + wx1[u] * A1));
+            atomicAdd(&sJz[o], czw * (wx0[u] * b0[v] + wx1[u] * b1[v]));
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // 4: one compensated flush of the tile's currents (nodes i0t-2 ..)
+  for (int e = threadIdx.x; e < NC * JV; e += blockDim.x) {
+    float v = sJ[e];
+    if (v == 0.f) continue;
+    int c = e / JV, rr = e - c * JV;
+    int lx = rr % JX, ly = (rr / JX) % JY, lz = rr / (JX * JY);
+    int gi = i0t - 2 + lx, gj = j0t - 2 + ly, gk = (NDIM == 3) ? k0t - 2 + lz : 1;
+    if (gi < 1 || gi > g.n1p || gj < 1 || gj > g.n2p || gk < 1 || gk > g.n3p) {
+      raise_err(a.err, AGPU_EBIT_INDEX);
+      continue;
+    }
+    long long o = g.ncell * c + goff(g, gi, gj, gk);
+    kadd_g(&a.jhi[o], &a.jlo[o], v);
+  }
+}
+
+size_t tile32_smem(int ndim, int tx, int ty, int tz) {
+  if (ndim == 3) return sizeof(float) * (6 * (tx + 2) * (ty + 2) * (tz + 2) + 3 * (tx + 4) * (ty + 4) * (tz + 4));
+  return sizeof(float) * (3 * (tx + 2) * (ty + 2) + 2 * (tx + 4) * (ty + 4));
+}
+
+void tile_push32(const TileArgs32& a, cudaStream_t st) {
+  if (a.t.ntiles <= 0) return;
+  if (a.g.ndim == 3) {
+    size_t sm = tile32_smem(3, TILE3_X, TILE3_Y, TILE3_Z);
+    auto k = k32_tile<3, TILE3_X, TILE3_Y, TILE3_Z>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k<<<a.t.ntiles, 256, sm, st>>>(a);
+  } else {
+    size_t sm = tile32_smem(2, TILE2_X, TILE2_Y, 1);
+    auto k = k32_tile<2, TILE2_X, TILE2_Y, 1>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k<<<a.t.ntiles, 256, sm, st>>>(a);
+  }
+}
+
+}  // namespace agpu

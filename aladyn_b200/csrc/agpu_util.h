@@ -50,6 +50,10 @@ long long compact64(double* part, double* tmp, long long cap, long long np, int 
                     cudaStream_t st);
 long long compact32(const Part32View& src, const Part32View& dst, long long np, int n1p, int n2p, int nx, int ny, int nz,
                     int use_y, int use_z, Scratch& s, cudaStream_t st);
+long long compact_flag64(const int* key, int dead, double* part, double* tmp, long long cap, long long np, int ndv, Scratch& s,
+                         cudaStream_t st);
+long long compact_flag32(const int* key, int dead, const Part32View& src, const Part32View& dst, long long np, Scratch& s,
+                         cudaStream_t st);
 long long append_electrons64(const int* flag, long long nion, const double* ion, long long ion_ld, double* el, long long el_ld,
                              long long ne0, long long cap, int ndim, int n_mol, unsigned int* err, Scratch& s,
                              cudaStream_t st);
