@@ -149,6 +149,8 @@ SIGNATURES = {
     "agpu_load_plasma": (C.c_int, [_P, C.c_int32]),
     "agpu_init_laser": (C.c_int, [_P, C.POINTER(AgpuLaser)]),
     "agpu_set_ionization_table": (C.c_int, [_P, C.c_int32, _D, C.c_int32, C.c_int32, C.c_double]),
+    "agpu_build_ionization_table": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, _D,
+                                              C.POINTER(C.c_double)]),
     "agpu_set_ionization_species": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                               C.c_int32, C.c_double]),
     "agpu_step": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int32, C.POINTER(AgpuStepOut)]),

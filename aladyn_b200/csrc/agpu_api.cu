@@ -986,6 +986,12 @@ int agpu_set_ionization_table(agpu_handle* h, int32_t ic, const double* w_one_le
   return upload_table(h, ic, w_one_lev, zmax);
 }
 
+int agpu_build_ionization_table(int32_t atomic_number, int32_t ion_min, int32_t ionz_model, double lp_max, double dt,
+                                double* w_one_lev, double* de_inv) {
+  if (!w_one_lev || !de_inv) return AGPU_E_ARG;
+  return build_ionization_table(atomic_number, ion_min, ionz_model, lp_max, dt, w_one_lev, de_inv) ? AGPU_E_ARG : 0;
+}
+
 int agpu_set_ionization_species(agpu_handle* h, int32_t ic, int32_t atomic_number, int32_t ion_min, int32_t ion_max,
                                 int32_t ionz_model, double lp_max) {
   if (!h || ic < 1 || ic >= h->p.nsp || ion_min < 0 || ion_max > atomic_number || ion_min >= ion_max) return AGPU_E_ARG;

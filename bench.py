@@ -351,6 +351,30 @@ def cpu_sample(name, budget_s=15.0, threads=None, warmup=0, steps=None):
     return dict(value=pushes / el, cores=threads, sample=sample, steps=done, seconds=el)
 
 
+def make_reducers(torch, world: int, device: str):
+    """Barrier and max/sum over ranks for the replicas-only multi-GPU run
+    (timing is the max over ranks, work the sum); identity at one rank."""
+    if world <= 1:
+        def barrier():
+            if device == "cuda":
+                torch.cuda.synchronize()
+
+        return barrier, (lambda x: x), (lambda x: x)
+    import torch.distributed as dist
+
+    def barrier():
+        dist.barrier()
+        if device == "cuda":
+            torch.cuda.synchronize()
+
+    def red(x, op):
+        t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    return barrier, (lambda x: red(x, dist.ReduceOp.MAX)), (lambda x: red(x, dist.ReduceOp.SUM))
+
+
 # --------------------------------------------------------------------------
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
@@ -397,29 +421,7 @@ def main(argv=None):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
-        def barrier():
-            dist.barrier()
-            torch.cuda.synchronize()
-
-        def maxred(x):
-            tt = torch.tensor([x], dtype=torch.float64, device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            return float(tt.item())
-
-        def sumred(x):
-            tt = torch.tensor([x], dtype=torch.float64, device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.SUM)
-            return float(tt.item())
-    else:
-        def barrier():
-            torch.cuda.synchronize()
-
-        def maxred(x):
-            return x
-
-        def sumred(x):
-            return x
+    barrier, maxred, sumred = make_reducers(torch, world, "cuda")
 
     from aladyn_b200.abi import AGPU_FP32_SPLIT, AGPU_FP64
     clk = ClockSampler(torch.cuda.current_device() if world == 1 else local)

@@ -212,6 +212,13 @@ int agpu_init_laser(agpu_handle* h, const agpu_laser* laser);
  * de_inv = n_ge / lp_max.  Column-major: index (nk, z) -> nk + (n_ge+2)*z. */
 int agpu_set_ionization_table(agpu_handle* h, int32_t ic, const double* w_one_lev,
                               int32_t n_ge, int32_t zmax, double de_inv);
+/* Host-only (no device needed): build w_one_lev(0:n_ge+1, 0:atomic_number)
+ * with n_ge = 10000 for the one-level model, as set_field_ioniz_wfunction
+ * (src/ionization/ionize.f90:38-190) with set_ionization_coeff
+ * (src/ionization/ionz_data.f90:131-245) does; de_inv = n_ge / lp_max.
+ * Supported atomic numbers 1, 2, 3, 6, 7; models 1-5. */
+int agpu_build_ionization_table(int32_t atomic_number, int32_t ion_min, int32_t ionz_model, double lp_max, double dt,
+                                double* w_one_lev, double* de_inv);
 /* ADK parameters so the library can rebuild the table itself when the ion
  * field exceeds lp_max (pic_evolve_in_time.f90:53-62). */
 int agpu_set_ionization_species(agpu_handle* h, int32_t ic, int32_t atomic_number,
