@@ -164,6 +164,8 @@ SIGNATURES = {
     "agpu_set_sort_interval": (C.c_int, [_P, C.c_int32]),
     "agpu_set_deterministic": (C.c_int, [_P, C.c_int32]),
     "agpu_struct_sizes": (C.c_int, [C.POINTER(C.c_int64), C.c_int32]),
+    "agpu_field_diag_noalloc": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                          C.c_double, _P, _P]),
 }
 
 _lib = None

@@ -34,6 +34,7 @@ UNITS = [
     ("agpu_tile64.cu", ["-fmad=false"]),
     ("agpu_tile32.cu", ["-fmad=true"]),
     ("agpu_bin.cu", ["-fmad=false"]),
+    ("agpu_noalloc.cu", ["-fmad=false"]),
     ("agpu_ionz.cpp", []),
 ]
 HEADERS = ["agpu_common.cuh", "agpu_kernels.h", "agpu_util.h", "agpu_yee.cuh", "agpu_ionz.h", "agpu_bin.cuh",

@@ -242,6 +242,23 @@ int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t l
  * (src/diagnostics/diag_part_and_fields.f90:172-220, 485-719). */
 int agpu_diag(agpu_handle* h, agpu_diag_out* out);
 
+/* Field diagnostics for callers that cannot allocate device memory (a host
+ * inside a CUDA stream capture, a host whose device memory comes from its
+ * own pool, a host that must not grow the device footprint).  No counterpart
+ * in the reference.  Computes, from a field array already on the device
+ * (d_ebf in the ebf(n1p,n2p,n3p,nf) layout, n1p = nx+5 ...), the values
+ * agpu_diag reports for the fields: d_out[c] = sum over interior cells of
+ * F_c^2 * dx*dy*dz (c < nf, 0 beyond), d_out[6] = max |E| (device array of
+ * 7 doubles, written on `stream`, a cudaStream_t or NULL).  Calls no
+ * cudaMalloc/cudaFree: its scratch is a file-scope device array of 65536 x 8
+ * doubles (4 MiB) that every GPU loading the library holds until exit, which
+ * limits the interior to 2^28 cells (larger grids return AGPU_E_CAPACITY).
+ * The first call on a device looks up the array's address there; make that
+ * call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+int agpu_field_diag_noalloc(const double* d_ebf, int32_t ndim, int32_t nx, int32_t ny, int32_t nz, double dx, double dy,
+                            double dz, double* d_out, void* stream);
+
 /* ---- profiling --------------------------------------------------------- */
 int agpu_set_profiling(agpu_handle* h, int32_t on);
 int agpu_get_timers(agpu_handle* h, agpu_timers* out);
