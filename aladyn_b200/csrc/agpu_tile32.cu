@@ -61,7 +61,7 @@ __device__ __forceinline__ bool inside(int node, float o, int n) {
 }  // namespace
 
 template <int NDIM, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(256) k32_tile(TileArgs32 a) {
+__global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
   constexpr int FX = TX + 2, FY = TY + 2, FZ = (NDIM == 3) ? TZ + 2 : 1;
   constexpr int JX = TX + 4, JY = TY + 4, JZ = (NDIM == 3) ? TZ + 4 : 1;
   constexpr int FV = FX * FY * FZ, JV = JX * JY * JZ;

@@ -54,7 +54,7 @@ __device__ __forceinline__ void esirk_d(const double a0[3], const double a1[3], 
 }  // namespace
 
 template <int NDIM, int TX, int TY, int TZ, bool SHJ>
-__global__ void __launch_bounds__(256) k64_tile(TileArgs64 a) {
+__global__ void __launch_bounds__(256, 2) k64_tile(TileArgs64 a) {
   constexpr int FX = TX + 2, FY = TY + 2, FZ = (NDIM == 3) ? TZ + 2 : 1;
   constexpr int JX = TX + 4, JY = TY + 4, JZ = (NDIM == 3) ? TZ + 4 : 1;
   constexpr int FV = FX * FY * FZ, JV = JX * JY * JZ;

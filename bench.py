@@ -53,7 +53,10 @@ WORKLOADS = {
     "lwfa2d_1024x256_ppc4": dict(ndim=2, nx=1024, ny=256, nz=1, k0=25.0, yx_rat=4.0, zx_rat=1.0,
                                  cfl=0.8, ppc=(2, 2, 1), n_over_nc=0.01, a0=2.0, w0=5 * LAM0,
                                  tau=10 * LAM0, x_plasma=20 * LAM0, xc_frac=0.3),
-    # small 3D case for quick checks
+    # small 3D cases for quick checks and profiler captures
+    "lwfa3d_128x64x64_ppc8": dict(ndim=3, nx=128, ny=64, nz=64, k0=25.0, yx_rat=5.0, zx_rat=5.0,
+                                 cfl=0.8, ppc=(2, 2, 2), n_over_nc=0.005, a0=3.0, w0=6 * LAM0,
+                                 tau=10 * LAM0, x_plasma=0.0, xc_frac=0.7),
     "lwfa3d_256x128x128_ppc8": dict(ndim=3, nx=256, ny=128, nz=128, k0=25.0, yx_rat=5.0, zx_rat=5.0,
                                    cfl=0.8, ppc=(2, 2, 2), n_over_nc=0.005, a0=3.0, w0=6 * LAM0,
                                    tau=10 * LAM0, x_plasma=0.0, xc_frac=0.7),
@@ -71,6 +74,12 @@ def bytes_per_push(ndim: int, ppc: int, fp32: bool) -> float:
     if ndim == 3:
         return (36.0 + 28.0 + 48.0 / ppc) if fp32 else (104.0 + 72.0 / ppc)
     return (24.0 + 20.0 + 28.0 / ppc) if fp32 else (72.0 + 40.0 / ppc)
+
+
+# DRAM bytes (read + write) per particle of one k32_tile launch, from an ncu
+# capture of the 128x64x64-cell, 8 ppc workload (295.0 MB for 4.19e6
+# particles); traffic grows in proportion to the particles of a launch.
+K32_DRAM_BYTES_PER_PUSH = 70.4
 
 
 def yee_bytes_per_cell(ndim: int, fp32: bool) -> float:
@@ -481,7 +490,10 @@ def main(argv=None):
             "roofline": {"bound": "hbm", "kernel": "k32_push_dep (gather+push+deposit, FP32 split)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
-                         "bytes_per_push": bpp, "traffic": None},
+                         "bytes_per_push": bpp,
+                         "traffic": (K32_DRAM_BYTES_PER_PUSH * tm.pushes / max(1, tm.launches_push_deposit)
+                                     if w["ndim"] == 3 and ppc_w == 8 else None),
+                         "traffic_note": "ncu dram bytes per particle of a small capture, scaled to the launch"},
             "phase_ms_per_step": {"push_deposit": tm.ms_push_deposit / a.steps, "yee": tm.ms_yee / a.steps,
                                   "sort_compact": tm.ms_sort / a.steps, "window": tm.ms_window / a.steps},
             "gpu_launches": int(tm.launches_total),
