@@ -628,6 +628,71 @@ int ionize64(agpu_handle* h, int iter, agpu_step_out* out) {
   return 0;
 }
 
+// Ionization of the FP32 split form: the same steps as ionize64 with the
+// ion |E|^2 gathered in FP32 from the split positions.
+int ionize32(agpu_handle* h, int iter, agpu_step_out* out) {
+  for (int ic = 1; ic < h->nsp_ionz && ic < h->p.nsp; ++ic) {
+    long long np = h->np[ic];
+    if (np <= 0 || !h->d_wtab[ic]) continue;
+    IonArgs32 a;
+    a.g = h->g;
+    a.ebf = h->ebf32;
+    a.cell = h->sp[ic].cell;
+    a.ox = h->sp[ic].ox;
+    a.oy = h->sp[ic].oy;
+    a.oz = h->sp[ic].oz;
+    a.slot = h->sp[ic].slot;
+    a.ef2 = h->ef2;
+    a.flag = h->flag;
+    a.np = np;
+    a.wtab = h->d_wtab[ic];
+    a.n_ge = kNge;
+    a.zmax = h->zmax[ic];
+    a.iter = iter;
+    a.ic = ic;
+    a.de_inv = h->de_inv[ic];
+    a.seed = h->p.seed;
+    a.err = &h->d_cnt->err;
+    int grid = grid_for(np, 256, h->sms, 8);
+    k32_ion_efield<<<grid, 256, 0, h->st>>>(a);
+    CK(cudaGetLastError());
+    if (iter % 100 == 0) {
+      max_nonneg(h->ef2, np, &h->d_cnt->fmax, h->st, h->sms);
+      CK(cudaGetLastError());
+      if (int rc = read_counters(h)) return rc;
+      double m = std::sqrt(h->h_cnt->fmax);
+      out->ion_field_max = m;
+      if (h->auto_table[ic] && m > h->lp_max[ic]) {
+        h->lp_max[ic] = 1.1 * m;
+        std::vector<double> tab((size_t)(kNge + 2) * (h->at_num[ic] + 1));
+        double dinv = 0.0;
+        if (build_ionization_table(h->at_num[ic], h->ion_min[ic], h->model[ic], h->lp_max[ic], h->p.dt, tab.data(), &dinv))
+          return AGPU_E_ARG;
+        h->de_inv[ic] = dinv;
+        a.de_inv = dinv;
+        if (int rc = upload_table(h, ic, tab.data(), h->at_num[ic])) return rc;
+      }
+    }
+    k32_ionize<<<grid, 256, 0, h->st>>>(a);
+    CK(cudaGetLastError());
+    h->timers.launches_total += 2 + 3 + ((iter % 100 == 0) ? 1 : 0);
+    if (int rc = drop_removed(h, 0)) return rc;
+    long long ne0 = h->np[0];
+    long long added = append_electrons32(h->flag, np, h->sp[ic].view(), h->sp[0].view(), ne0, h->cap[0],
+                                         h->p.n_mol_atoms[ic], &h->d_cnt->err, h->scr, h->st);
+    CK(cudaGetLastError());
+    if (ne0 + added > h->cap[0]) {
+      h->error_bits |= AGPU_EBIT_CAPACITY;
+      added = h->cap[0] - ne0;
+    }
+    h->np[0] = ne0 + added;
+    h->nalive[0] = h->np[0];
+    if (added > 0) h->binned[0] = false;
+    out->new_electrons += added;
+  }
+  return 0;
+}
+
 }  // namespace
 
 // ============================================================================
@@ -980,7 +1045,6 @@ int agpu_init_laser(agpu_handle* h, const agpu_laser* l) {
 
 int agpu_set_ionization_table(agpu_handle* h, int32_t ic, const double* w_one_lev, int32_t n_ge, int32_t zmax, double de_inv) {
   if (!h || !w_one_lev || ic < 1 || ic >= h->p.nsp || n_ge != kNge || zmax < 1 || zmax > 100) return AGPU_E_ARG;
-  if (h->fp32) return AGPU_E_ARG;  // ionization runs in the FP64 form
   h->de_inv[ic] = de_inv;
   h->auto_table[ic] = false;
   return upload_table(h, ic, w_one_lev, zmax);
@@ -995,7 +1059,6 @@ int agpu_build_ionization_table(int32_t atomic_number, int32_t ion_min, int32_t 
 int agpu_set_ionization_species(agpu_handle* h, int32_t ic, int32_t atomic_number, int32_t ion_min, int32_t ion_max,
                                 int32_t ionz_model, double lp_max) {
   if (!h || ic < 1 || ic >= h->p.nsp || ion_min < 0 || ion_max > atomic_number || ion_min >= ion_max) return AGPU_E_ARG;
-  if (h->fp32) return AGPU_E_ARG;
   std::vector<double> tab((size_t)(kNge + 2) * (atomic_number + 1));
   double dinv = 0.0;
   if (build_ionization_table(atomic_number, ion_min, ionz_model, lp_max, h->p.dt, tab.data(), &dinv)) return AGPU_E_ARG;
@@ -1025,9 +1088,9 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu
   h->timers.launches_total += (p.ndim == 3) ? 3 : 2;
   ph_end(h, PH_YEE);
   // ionization
-  if (p.ionz_lev > 0 && !h->fp32) {
+  if (p.ionz_lev > 0) {
     ph_begin(h, PH_IONIZE);
-    rc = ionize64(h, iter, out);
+    rc = h->fp32 ? ionize32(h, iter, out) : ionize64(h, iter, out);
     ph_end(h, PH_IONIZE);
     if (rc) return rc;
   }

@@ -322,3 +322,95 @@ void push_deposit32(const PushArgs32& a, cudaStream_t st, int sms) {
 }
 
 }  // namespace agpu
+
+namespace agpu {
+
+// ============================================================================
+// A15/A16 in the split form: |E|^2 on each ion with the qqh shapes
+// (set_ion_efield, grid_part_connect.f90:288-410) from the node + offset,
+// then the one-level draw of part_ionize (ionize.f90:390-450) against the
+// FP64 table.  Node index of the integer-node shape: i0 (offset s); of the
+// half-node shape: int(i0 + s) = i0 (s >= 0) or i0 - 1, offset s -/+ 0.5.
+// ============================================================================
+__global__ void k32_ion_efield(IonArgs32 a) {
+  const Geo g = a.g;
+  const float* E1 = a.ebf;
+  const float* E2 = a.ebf + g.ncell;
+  const float* E3 = a.ebf + 2 * g.ncell;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < a.np; n += (long long)gridDim.x * blockDim.x) {
+    int c = a.cell[n];
+    int i0 = c % g.n1p + 1, r = c / g.n1p, j0 = r % g.n2p + 1, k0 = (g.ndim == 3) ? r / g.n2p + 1 : 1;
+    float sv[3] = {a.ox[n], a.oy[n], (g.ndim == 3) ? a.oz[n] : 0.f};
+    int nd[3] = {i0, j0, k0};
+    float w1[3][3], wh[3][3];
+    int ib[3], ih[3];
+    for (int d = 0; d < 3; ++d) {
+      float s = sv[d], s2 = s * s;
+      w1[d][1] = 0.75f - s2;
+      w1[d][2] = 0.5f * (0.25f + s2 + s);
+      w1[d][0] = 1.f - w1[d][1] - w1[d][2];
+      ib[d] = nd[d] - 1;
+      int hn = (s >= 0.f) ? nd[d] : nd[d] - 1;
+      float sh = (s >= 0.f) ? s - 0.5f : s + 0.5f;
+      float h2 = sh * sh;
+      wh[d][1] = 0.75f - h2;
+      wh[d][2] = 0.5f * (0.25f + h2 + sh);
+      wh[d][0] = 1.f - wh[d][1] - wh[d][2];
+      ih[d] = hn - 1;
+    }
+    bool bad = ib[0] < 1 || ib[0] > g.n1p - 2 || ih[0] < 1 || ih[0] > g.n1p - 2 || ib[1] < 1 || ib[1] > g.n2p - 2 ||
+               ih[1] < 1 || ih[1] > g.n2p - 2;
+    if (g.ndim == 3) bad = bad || ib[2] < 1 || ib[2] > g.n3p - 2 || ih[2] < 1 || ih[2] > g.n3p - 2;
+    if (bad) {
+      raise_err(a.err, AGPU_EBIT_INDEX);
+      a.ef2[n] = 0.0;
+      continue;
+    }
+    float ef = 0.f;
+    if (g.ndim == 2) {
+      for (int jp = 0; jp < 3; ++jp)
+        for (int ip = 0; ip < 3; ++ip) {
+          float e = E1[goff(g, ih[0] + ip, ib[1] + jp, 1)];
+          ef += wh[0][ip] * w1[1][jp] * e * e;
+          float f = E2[goff(g, ib[0] + ip, ih[1] + jp, 1)];
+          ef += w1[0][ip] * wh[1][jp] * f * f;
+        }
+    } else {
+      for (int kp = 0; kp < 3; ++kp)
+        for (int jp = 0; jp < 3; ++jp)
+          for (int ip = 0; ip < 3; ++ip) {
+            float e = E1[goff(g, ih[0] + ip, ib[1] + jp, ib[2] + kp)];
+            ef += wh[0][ip] * w1[1][jp] * w1[2][kp] * e * e;
+            float f = E2[goff(g, ib[0] + ip, ih[1] + jp, ib[2] + kp)];
+            ef += w1[0][ip] * wh[1][jp] * w1[2][kp] * f * f;
+            float h = E3[goff(g, ib[0] + ip, ib[1] + jp, ih[2] + kp)];
+            ef += w1[0][ip] * w1[1][jp] * wh[2][kp] * h * h;
+          }
+    }
+    a.ef2[n] = (double)ef;
+  }
+}
+
+__global__ void k32_ionize(IonArgs32 a) {
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < a.np; n += (long long)gridDim.x * blockDim.x) {
+    double ef2 = a.ef2[n];
+    int nk = 0;
+    if (ef2 > 0.) nk = (int)llround(a.de_inv * sqrt(ef2));
+    if (nk > a.n_ge + 1) {
+      raise_err(a.err, AGPU_EBIT_IONZ_INDEX);
+      nk = a.n_ge + 1;
+    }
+    uint64_t sl = a.slot[n];
+    int z0 = slot_charge(sl);
+    double pr = ionz_draw(a.seed, n, a.iter, a.ic);
+    double thr = (z0 >= 0 && z0 <= a.zmax) ? a.wtab[(long long)nk + (long long)(a.n_ge + 2) * z0] : 0.0;
+    int fl = 0;
+    if (pr < thr) {
+      a.slot[n] = make_slot(z0 + 1, slot_part_ind(sl), slot_wgh(sl));
+      fl = 1;
+    }
+    a.flag[n] = fl;
+  }
+}
+
+}  // namespace agpu

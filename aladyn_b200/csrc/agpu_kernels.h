@@ -99,6 +99,24 @@ struct PushArgs32 {
 };
 
 
+struct IonArgs32 {
+  Geo g;
+  const float* ebf;
+  const int* cell;
+  const float *ox, *oy, *oz;
+  uint64_t* slot;
+  double* ef2;
+  int* flag;
+  long long np;
+  const double* wtab;
+  int n_ge, zmax, iter, ic;
+  double de_inv;
+  uint64_t seed;
+  unsigned int* err;
+};
+__global__ void k32_ion_efield(IonArgs32 a);
+__global__ void k32_ionize(IonArgs32 a);
+
 void field_bd32(const Dev32& d, cudaStream_t st, int sms);
 void push_deposit32(const PushArgs32& a, cudaStream_t st, int sms);
 void jfold32(const Dev32& d, cudaStream_t st, int sms);
