@@ -155,6 +155,8 @@ SIGNATURES = {
                                               C.c_int32, C.c_double]),
     "agpu_step": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int32, C.POINTER(AgpuStepOut)]),
     "agpu_window_inject": (C.c_int, [_P, C.c_int32, _D, C.c_int64, C.c_int64, C.c_int32]),
+    "agpu_beam_inject": (C.c_int, [_P, C.c_int32, _D, C.c_int64, C.c_int64, C.c_int32, C.c_double]),
+    "agpu_beam_potential": (C.c_int, [_P, _D, _D, C.c_double]),
     "agpu_diag": (C.c_int, [_P, C.POINTER(AgpuDiagOut)]),
     "agpu_set_profiling": (C.c_int, [_P, C.c_int32]),
     "agpu_get_timers": (C.c_int, [_P, C.POINTER(AgpuTimers)]),

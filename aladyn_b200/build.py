@@ -35,10 +35,11 @@ UNITS = [
     ("agpu_tile32.cu", ["-fmad=true"]),
     ("agpu_bin.cu", ["-fmad=false"]),
     ("agpu_noalloc.cu", ["-fmad=false"]),
+    ("agpu_beam.cu", ["-fmad=false"]),
     ("agpu_ionz.cpp", []),
 ]
 HEADERS = ["agpu_common.cuh", "agpu_kernels.h", "agpu_util.h", "agpu_yee.cuh", "agpu_ionz.h", "agpu_bin.cuh",
-           "agpu_tile.h", "agpu_select.cuh"]
+           "agpu_tile.h", "agpu_select.cuh", "agpu_beam.h"]
 
 
 def _mtime(p: str) -> float:
@@ -66,7 +67,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             subprocess.run(cmd, check=True)
             rebuilt = True
     if rebuilt or force or not os.path.exists(LIB):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lcufft",
+               "-Xlinker", "-rpath=/usr/local/cuda/lib64"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/aladyn_gpu.h"
+#include "agpu_beam.h"
 #include "agpu_bin.cuh"
 #include "agpu_ionz.h"
 #include "agpu_kernels.h"
@@ -1249,6 +1250,129 @@ int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t l
   h->np[ic] += n;
   h->nalive[ic] = h->np[ic];
   h->binned[ic] = false;
+  return 0;
+}
+
+// Geometry and constants of the bunch set-up; box lengths as set_grid
+// computes them (set_grid_param.f90:102-108, 168-170, 221-223).
+static BeamArgs beam_args(const agpu_handle* h, double gam2, double bet0) {
+  const agpu_params& p = h->p;
+  BeamArgs a;
+  a.g = h->g;
+  a.nx = p.nx;
+  a.ny = p.ny;
+  a.nz = p.ndim == 3 ? p.nz : 1;
+  a.dx = p.dx;
+  a.dy = p.dy;
+  a.dz = p.dz;
+  a.dx_inv = p.dx_inv;
+  a.dy_inv = p.dy_inv;
+  a.dz_inv = p.dz_inv;
+  a.xmn = p.xmn;
+  a.ymn = p.ymn;
+  a.zmn = p.zmn;
+  a.lx_box = p.xmax - p.xmn;
+  a.ly_box = p.gymax - p.gymin;
+  a.lz_box = p.gzmax - p.gzmin;
+  a.ompe = p.ompe;
+  a.gam2 = gam2;
+  a.bet0 = bet0;
+  return a;
+}
+
+int agpu_beam_potential(agpu_handle* h, const double* rho, double* pot, double gam2) {
+  if (!h || !rho || !pot || !(gam2 >= 1.0) || !std::isfinite(gam2)) return AGPU_E_ARG;
+  double* d = nullptr;
+  const size_t n = (size_t)h->g.ncell;
+  if (dmalloc((void**)&d, sizeof(double) * n)) return AGPU_E_NOMEM;
+  int rc = 0;
+  if (cudaMemcpyAsync(d, rho, sizeof(double) * n, cudaMemcpyHostToDevice, h->st) != cudaSuccess) rc = AGPU_E_CUDA;
+  int launches = 0;
+  if (!rc) rc = beam_potential(beam_args(h, gam2, 0.0), d, h->st, h->sms, &launches);
+  if (!rc && cudaMemcpyAsync(pot, d, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st) != cudaSuccess) rc = AGPU_E_CUDA;
+  if (cudaStreamSynchronize(h->st) != cudaSuccess && !rc) rc = AGPU_E_CUDA;
+  cudaFree(d);
+  h->timers.launches_total += launches;
+  return rc;
+}
+
+int agpu_beam_inject(agpu_handle* h, int32_t ic, const double* part, int64_t ld, int64_t nb_tot, int32_t ndv,
+                     double gam0) {
+  if (!h || ic < 0 || ic >= h->p.nsp || ndv != h->ndv || nb_tot < 0 || (nb_tot > 0 && (!part || ld < nb_tot)) ||
+      !(gam0 >= 1.0) || !std::isfinite(gam0))
+    return AGPU_E_ARG;
+  if (int rc = drop_removed(h, ic)) return rc;
+  const Geo& g = h->g;
+  const agpu_params& p = h->p;
+  const long long ldb = nb_tot > 0 ? nb_tot : 1;
+  double* stage = nullptr;  // the records as passed
+  double* sel = nullptr;    // the records inside the box, in order
+  double* pot = nullptr;    // split form: FP64 potential pair (the FP64 form uses jc(1:2))
+  int rc = 0;
+  if (dmalloc((void**)&stage, sizeof(double) * (size_t)ldb * ndv) ||
+      dmalloc((void**)&sel, sizeof(double) * (size_t)ldb * ndv) ||
+      (h->fp32 && dmalloc((void**)&pot, sizeof(double) * (size_t)g.ncell * 2)))
+    rc = AGPU_E_NOMEM;
+  int launches = 0;
+  long long nb = 0;
+  if (!rc && cudaMemsetAsync(h->d_cnt, 0, sizeof(Counters), h->st) != cudaSuccess) rc = AGPU_E_CUDA;
+  if (!rc && nb_tot > 0) {
+    if (cudaMemcpy2DAsync(stage, sizeof(double) * ldb, part, sizeof(double) * ld, sizeof(double) * nb_tot, ndv,
+                          cudaMemcpyHostToDevice, h->st) != cudaSuccess)
+      rc = AGPU_E_CUDA;
+    // mpi_beam_distribute (init_beam_part_distrib.f90:273-438): the records
+    // with x1 < x <= x2, y1 < y <= y2 (and z1 < z <= z2), in order
+    if (!rc) {
+      BoxBounds b{p.gxmin, p.gxmax, p.gymin, p.gymax, p.gzmin, p.gzmax, 1, p.ndim == 3 ? 1 : 0};
+      nb = compact64(stage, sel, ldb, nb_tot, ndv, b, h->scr, h->st);
+      launches += 3;
+      if (cudaGetLastError() != cudaSuccess) rc = AGPU_E_CUDA;
+    }
+  }
+  if (!rc && h->np[ic] + nb > h->cap[ic]) rc = AGPU_E_CAPACITY;
+  // spec(1)%part grows by the bunch records (beam_inject 508-535)
+  if (!rc && nb > 0) {
+    if (!h->fp32) {
+      if (cudaMemcpy2DAsync(h->part[ic] + h->np[ic], sizeof(double) * h->cap[ic], sel, sizeof(double) * ldb,
+                            sizeof(double) * nb, ndv, cudaMemcpyDeviceToDevice, h->st) != cudaSuccess)
+        rc = AGPU_E_CUDA;
+    } else {
+      rec_to_split(sel, ldb, nb, h->sp[ic].view(), h->np[ic], g, p.xmn, p.ymn, p.zmn, p.dx_inv, p.dy_inv, p.dz_inv, h->st,
+                   h->sms);
+      launches += 1;
+    }
+  }
+  // jc(:,:,:,1) = 0; set_grid_charge; fft_3d_psolv / fft_2d_psolv;
+  // jc(:,:,:,2) = bet0 jc(:,:,:,1); initial_beam_fields; ebf += ebf_bunch
+  const double gam2 = gam0 * gam0;
+  const double u0_b = std::sqrt(gam0 * gam0 - 1.);  // set_init_param.f90:353-354
+  const double bet0 = u0_b / gam0;
+  const BeamArgs a = beam_args(h, gam2, bet0);
+  double* p1 = h->fp32 ? pot : h->jc;
+  double* p2 = p1 ? p1 + g.ncell : nullptr;
+  if (!rc && cudaMemsetAsync(p1, 0, sizeof(double) * g.ncell, h->st) != cudaSuccess) rc = AGPU_E_CUDA;
+  if (!rc) {
+    beam_charge(a, sel, ldb, nb, p1, &h->d_cnt->err, h->st, h->sms);
+    launches += nb > 0 ? 1 : 0;
+    if (cudaGetLastError() != cudaSuccess) rc = AGPU_E_CUDA;
+  }
+  if (!rc) rc = beam_potential(a, p1, h->st, h->sms, &launches);
+  if (!rc) {
+    beam_fields(a, p1, p2, h->fp32 ? nullptr : h->ebf, h->fp32 ? h->ebf32 : nullptr, h->st, h->sms, &launches);
+    if (cudaGetLastError() != cudaSuccess) rc = AGPU_E_CUDA;
+  }
+  if (cudaStreamSynchronize(h->st) != cudaSuccess && !rc) rc = AGPU_E_CUDA;
+  cudaFree(stage);
+  cudaFree(sel);
+  cudaFree(pot);
+  h->timers.launches_total += launches;
+  if (rc) return rc;
+  if (int rc_ = read_counters(h)) return rc_;
+  h->np[ic] += nb;
+  h->nalive[ic] = h->np[ic];
+  h->binned[ic] = false;
+  h->fields_set = true;
+  if (h->h_cnt->err & AGPU_EBIT_INDEX) return AGPU_E_INDEX;
   return 0;
 }
 

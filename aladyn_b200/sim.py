@@ -20,7 +20,7 @@ import ctypes as C
 import numpy as np
 
 from . import abi
-from .abi import AgpuDiagOut, AgpuStepOut, AgpuTimers, check
+from .abi import AGPU_E_INDEX, AgpuDiagOut, AgpuStepOut, AgpuTimers, check
 from .config import dims, ndv
 
 
@@ -126,6 +126,25 @@ class PicDevice:
         a = np.asfortranarray(part, dtype=np.float64)
         check(self.lib.agpu_window_inject(self.h, ic, _dptr(a), a.shape[0], a.shape[0], self.ndv),
               "agpu_window_inject")
+
+    # -- PWFA bunch set-up (beam_inject) ---------------------------------------
+    def beam_inject(self, ic: int, part: np.ndarray, gam0: float) -> int:
+        """Append the bunch records inside the box to species ic and add the
+        bunch fields (Poisson solve of the bunch charge).  Returns the status:
+        0, or AGPU_E_INDEX when a record's stencil left the array."""
+        a = np.asfortranarray(part, dtype=np.float64)
+        rc = self.lib.agpu_beam_inject(self.h, ic, _dptr(a), a.shape[0], a.shape[0], self.ndv, gam0)
+        if rc not in (0, AGPU_E_INDEX):
+            check(rc, "agpu_beam_inject")
+        return rc
+
+    def beam_potential(self, rho: np.ndarray, gam2: float) -> np.ndarray:
+        """fft_3d_psolv / fft_2d_psolv of rho(n1p, n2p, n3p) on the device."""
+        a = np.asfortranarray(rho, dtype=np.float64)
+        assert a.shape == (self.n1p, self.n2p, self.n3p)
+        out = np.zeros_like(a, order="F")
+        check(self.lib.agpu_beam_potential(self.h, _dptr(a), _dptr(out), gam2), "agpu_beam_potential")
+        return out
 
     # -- initial state on the device ----------------------------------------
     def set_plasma_source(self, src):

@@ -237,6 +237,30 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time,
 int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t ld,
                        int64_t n, int32_t ndv);
 
+/* ---- PWFA bunch set-up ------------------------------------------------- */
+/* beam_inject (src/IO/init_beam_part_distrib.f90:474-630, uniform-grid
+ * branch), called once after the fields are set: of the nb bunch records
+ * part(ld, ndv) (host-built by the caller, as the reference's beam_data /
+ * bunch_gen build them on the host) those inside the box (gxmin < x <= gxmax,
+ * and y, z alike: mpi_beam_distribute, init_beam_part_distrib.f90:273-438)
+ * are appended, in order, to species ic; their charge density
+ * (set_grid_charge, src/particles/grid_part_util.f90:240-334) is solved for
+ * the potential with the FP64 sine-transform Poisson solver (fft_3d_psolv /
+ * fft_2d_psolv, src/IO/psolve.f90:117-238, kx/gam0 in 3D); ebf += the bunch
+ * fields of initial_beam_fields (src/fields/init_grid_fields.f90:32-134)
+ * with Bx = 0.  FP64 form: jc(1) holds the potential afterwards and jc(2)
+ * the reference's second component, as in the reference.  Allocates its
+ * scratch and cuFFT plans for the call.  Returns AGPU_E_INDEX (fields still
+ * added) when a record's stencil left the array; such records are skipped in
+ * the charge density. */
+int agpu_beam_inject(agpu_handle* h, int32_t ic, const double* part, int64_t ld,
+                     int64_t nb, int32_t ndv, double gam0);
+/* The Poisson solve alone (fft_3d_psolv / fft_2d_psolv with ft_mod = 2,
+ * sym = 1): rho and pot are host arrays in the field layout (n1p, n2p, n3p);
+ * pot = rho with the interior replaced by the potential of
+ * Laplacian(pot) = -ompe rho (x-derivative over gam2 in 3D). */
+int agpu_beam_potential(agpu_handle* h, const double* rho, double* pot, double gam2);
+
 /* ---- diagnostics ------------------------------------------------------- */
 /* FP64 reductions of Envar / energy_momenta
  * (src/diagnostics/diag_part_and_fields.f90:172-220, 485-719). */

@@ -1581,3 +1581,307 @@ int ora_get_ionization_table(const ora_sim* s, int ic, double* out) {
 double ora_ionz_de_inv(const ora_sim* s, int ic) { return s->de_inv[ic]; }
 double ora_draw(uint64_t seed, int64_t n, int iter, int ic) { return ora_ionz_draw(seed, n, iter, ic); }
 void ora_philox(const uint32_t* ctr, uint32_t k0, uint32_t k1, uint32_t* out) { ora_philox4x32_10(ctr, k0, k1, out); }
+
+/* ======================================================================== */
+/* A20: PWFA bunch set-up.  set_grid_charge (src/particles/grid_part_util.   */
+/* f90:240-334), the sine-transform Poisson solve fft_3d_psolv /            */
+/* fft_2d_psolv + beam_potential / beam_2d_potential (src/IO/psolve.f90:     */
+/* 39-238) with the wavenumbers of set_grid_param.f90:967-987 and the r2r    */
+/* transforms of src/fft/modern_fft_lib.F90:675-775, initial_beam_fields     */
+/* (src/fields/init_grid_fields.f90:32-134), the box selection of            */
+/* mpi_beam_distribute (src/IO/init_beam_part_distrib.f90:273-438) and       */
+/* beam_inject (init_beam_part_distrib.f90:474-630, uniform-grid branch).    */
+/* ======================================================================== */
+
+/* FFTW_RODFT00 of length n by its published definition (FFTW is not
+   vendored): Y_k = 2 sum_j x_j sin(pi (j+1)(k+1)/(n+1)), unnormalised.
+   sint[m] = sin(pi m/(n+1)), m in [0, 2(n+1)). */
+static void ora_rodft00(double* x, int n, double* work, const double* sint) {
+  for (int k = 0; k < n; ++k) {
+    double acc = 0.0;
+    for (int j = 0; j < n; ++j) acc += x[j] * sint[(size_t)((j + 1) * (k + 1)) % (size_t)(2 * (n + 1))];
+    work[k] = 2.0 * acc;
+  }
+  memcpy(x, work, sizeof(double) * (size_t)n);
+}
+
+static double* ora_sin_table(int n) {
+  double* t = (double*)malloc(sizeof(double) * (size_t)(2 * (n + 1)));
+  for (int m = 0; m < 2 * (n + 1); ++m) t[m] = sin(acos(-1.0) * (double)m / (double)(n + 1));
+  return t;
+}
+
+/* ftw1d_sc (modern_fft_lib.F90:675-775), sine kind, on the compact array
+   w(n1,n2,n3) along dir; is < 0 scales by 1/ndb with ndb = 2(n1+2) along x
+   (logical_dimension(kind, n1+1)) and 2(n+1) along y and z. */
+static void ora_ftw1d_sin(double* w, int n1, int n2, int n3, int is, int dir) {
+  int n = dir == 1 ? n1 : (dir == 2 ? n2 : n3);
+  double* line = (double*)malloc(sizeof(double) * (size_t)n);
+  double* work = (double*)malloc(sizeof(double) * (size_t)n);
+  double* sint = ora_sin_table(n);
+  int ndb = dir == 1 ? 2 * (n1 + 1 + 1) : 2 * (n + 1);
+  double sc = 1. / (double)ndb;
+  size_t s1 = 1, s2 = (size_t)n1, s3 = (size_t)n1 * n2;
+  size_t stride = dir == 1 ? s1 : (dir == 2 ? s2 : s3);
+  int na = dir == 1 ? n2 : n1, nb = dir == 3 ? n2 : n3;
+  size_t sa = dir == 1 ? s2 : s1, sb = dir == 3 ? s2 : s3;
+  for (int b = 0; b < nb; ++b)
+    for (int a = 0; a < na; ++a) {
+      double* base = w + (size_t)a * sa + (size_t)b * sb;
+      for (int i = 0; i < n; ++i) line[i] = base[(size_t)i * stride];
+      ora_rodft00(line, n, work, sint);
+      for (int i = 0; i < n; ++i) base[(size_t)i * stride] = is < 0 ? sc * line[i] : line[i];
+    }
+  free(line);
+  free(work);
+  free(sint);
+}
+
+/* Wavenumbers of the sine transform, case(2) of set_grid_param.f90:967-987:
+   sk(i) = 2 sin(0.5 d ak(i))/d with ak(i) = (pi/l_box) i. */
+static void ora_sine_k(double* sk, int n, double d, double l_box) {
+  double wk = acos(-1.0) / l_box;
+  for (int i = 1; i <= n; ++i) {
+    double ak = wk * (double)i;
+    sk[i - 1] = 2. * sin(0.5 * d * ak) / d;
+  }
+}
+
+/* fft_3d_psolv / fft_2d_psolv with ft_mod = 2, sym = 1, s_ind = 0 on the
+   field-layout array rho(n1p,n2p,n3p): the interior is replaced by the
+   potential of Laplacian(pot) = -omp0 rho, x-derivative over gam2 in 3D. */
+int ora_beam_potential(ora_sim* s, double* rho, double gam2) {
+  const agpu_params* p = &s->p;
+  int n1 = p->nx, n2 = p->ny, n3 = p->ndim == 3 ? p->nz : 1;
+  size_t n1p = (size_t)s->n1p, n2p = (size_t)s->n2p;
+  double* wb = (double*)malloc(sizeof(double) * (size_t)n1 * n2 * n3);
+  double *skx = (double*)calloc((size_t)n1 + 2, sizeof(double)), *sky = (double*)calloc((size_t)n2 + 2, sizeof(double)),
+         *skz = (double*)calloc((size_t)n3 + 2, sizeof(double));
+  if (!wb || !skx || !sky || !skz) return 103;
+  /* lx_box = x(n1) - x(1), ly_box = y(n2+1) - y(1), lz_box = z(n3+1) - z(1)
+     (set_grid_param.f90:102-108, 168-170, 221-223) */
+  ora_sine_k(skx, n1, p->dx, p->xmax - p->xmn);
+  if (n2 > 1) ora_sine_k(sky, n2, p->dy, p->gymax - p->gymin);
+  if (n3 > 1) ora_sine_k(skz, n3, p->dz, p->gzmax - p->gzmin);
+  for (int k = 0; k < n3; ++k)
+    for (int j = 0; j < n2; ++j)
+      for (int i = 0; i < n1; ++i)
+        wb[(size_t)i + (size_t)n1 * ((size_t)j + (size_t)n2 * k)] =
+            rho[(size_t)(s->ix1 - 1 + i) + n1p * ((size_t)(s->jy1 - 1 + j) + n2p * (size_t)(s->kz1 - 1 + k))];
+  double omp0 = p->ompe;
+  size_t ncell = (size_t)n1 * n2 * n3;
+  if (p->ndim == 3) {
+    /* pftw3d_sc(-1): x, then pftw2d_sc: y (n2 > 2), z (n3 > 2) */
+    ora_ftw1d_sin(wb, n1, n2, n3, -1, 1);
+    if (n2 > 2) ora_ftw1d_sin(wb, n1, n2, n3, -1, 2);
+    if (n2 > 2 && n3 > 2) ora_ftw1d_sin(wb, n1, n2, n3, -1, 3);
+    for (size_t q = 0; q < ncell; ++q) wb[q] = omp0 * wb[q];
+    /* beam_potential (psolve.f90:93-112) */
+    for (int iz = 0; iz < n3; ++iz)
+      for (int iy = 0; iy < n2; ++iy) {
+        double ak2p = skz[iz] * skz[iz] + sky[iy] * sky[iy];
+        double* row = wb + (size_t)n1 * ((size_t)iy + (size_t)n2 * iz);
+        if (ak2p > 0.0) {
+          for (int ix = 0; ix < n1; ++ix) {
+            double ak2 = ak2p + skx[ix] * skx[ix] / gam2;
+            row[ix] = row[ix] / ak2;
+          }
+        } else {
+          for (int ix = 1; ix < n1; ++ix) {
+            double ak2 = skx[ix] * skx[ix] / gam2;
+            row[ix] = row[ix] / ak2;
+          }
+        }
+      }
+    /* pftw3d_sc(+1): pftw2d_sc (z if n3 > 1, y if n2 > 1), then x */
+    if (n3 > 1) ora_ftw1d_sin(wb, n1, n2, n3, 1, 3);
+    if (n2 > 1) ora_ftw1d_sin(wb, n1, n2, n3, 1, 2);
+    ora_ftw1d_sin(wb, n1, n2, n3, 1, 1);
+  } else {
+    /* fft_2d_psolv: pftw2d_sc(-1) transforms y only (n3 = 1) */
+    if (n2 > 2) ora_ftw1d_sin(wb, n1, n2, n3, -1, 2);
+    for (size_t q = 0; q < ncell; ++q) wb[q] = omp0 * wb[q];
+    /* beam_2d_potential (psolve.f90:39-64) */
+    for (int iz = 0; iz < n3; ++iz)
+      for (int iy = 0; iy < n2; ++iy) {
+        double ak2p = skz[iz] * skz[iz] + sky[iy] * sky[iy];
+        double* row = wb + (size_t)n1 * ((size_t)iy + (size_t)n2 * iz);
+        if (ak2p > 0.0) {
+          for (int ix = 0; ix < n1; ++ix) row[ix] = row[ix] / ak2p;
+        } else {
+          for (int ix = 0; ix < n1; ++ix) row[ix] = 0.0;
+        }
+      }
+    if (n2 > 1) ora_ftw1d_sin(wb, n1, n2, n3, 1, 2);
+  }
+  for (int k = 0; k < n3; ++k)
+    for (int j = 0; j < n2; ++j)
+      for (int i = 0; i < n1; ++i)
+        rho[(size_t)(s->ix1 - 1 + i) + n1p * ((size_t)(s->jy1 - 1 + j) + n2p * (size_t)(s->kz1 - 1 + k))] =
+            wb[(size_t)i + (size_t)n1 * ((size_t)j + (size_t)n2 * k)];
+  free(wb);
+  free(skx);
+  free(sky);
+  free(skz);
+  return 0;
+}
+
+/* set_grid_charge (grid_part_util.f90:240-334) of np records part(ld, ndv)
+   into den(n1p,n2p,n3p): wght = real(charge*wgh, sp), qden shapes.  A record
+   whose stencil leaves the array is skipped (the reference has no check). */
+void ora_grid_charge(const ora_sim* s, const double* part, int64_t ld, int64_t np, double* den) {
+  const agpu_params* p = &s->p;
+  size_t n1p = (size_t)s->n1p, n2p = (size_t)s->n2p;
+  int ch = p->ndim == 3 ? 7 : 5;
+  for (int64_t n = 0; n < np; ++n) {
+    ora_pack pk = ora_unpack(part[(size_t)(ch - 1) * (size_t)ld + (size_t)n]);
+    float wght = (float)pk.charge * pk.wgh;
+    double ax0[3], ay0[3], az0[3];
+    int i, j, k;
+    double xl = p->dx_inv * (part[(size_t)n] - p->xmn);
+    double yl = p->dy_inv * (part[(size_t)ld + (size_t)n] - p->ymn);
+    if (!(fabs(xl) < 1e9) || !(fabs(yl) < 1e9)) continue;
+    ora_qden_1d(xl, ax0, &i);
+    ora_qden_1d(yl, ay0, &j);
+    for (int q = 0; q < 3; ++q) ax0[q] = (double)wght * ax0[q];
+    i -= 1;
+    j -= 1;
+    /* stencil nodes i..i+2 must lie in 1..n1p */
+    if (i < 1 || i > s->n1p - 2 || j < 1 || j > s->n2p - 2) continue;
+    if (p->ndim == 2) {
+      for (int j1 = 0; j1 <= 2; ++j1)
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol = ax0[i1] * ay0[j1];
+          den[(size_t)(i + i1 - 1) + n1p * (size_t)(j + j1 - 1)] += dvol;
+        }
+    } else {
+      double zl = p->dz_inv * (part[(size_t)2 * (size_t)ld + (size_t)n] - p->zmn);
+      if (!(fabs(zl) < 1e9)) continue;
+      ora_qden_1d(zl, az0, &k);
+      k -= 1;
+      if (k < 1 || k > s->n3p - 2) continue;
+      for (int k1 = 0; k1 <= 2; ++k1)
+        for (int j1 = 0; j1 <= 2; ++j1) {
+          double dvol = az0[k1] * ay0[j1];
+          for (int i1 = 0; i1 <= 2; ++i1)
+            den[(size_t)(i + i1 - 1) + n1p * ((size_t)(j + j1 - 1) + n2p * (size_t)(k + k1 - 1))] += ax0[i1] * dvol;
+        }
+    }
+  }
+}
+
+/* initial_beam_fields (init_grid_fields.f90:32-134) on poten = jc(:,:,:,1:2)
+   into efb(n1p,n2p,n3p,6) (zero on entry), single domain: pe1x, pe1y, pe1z. */
+static void ora_initial_beam_fields(ora_sim* s, double* efb, double g2, double bet) {
+  const agpu_params* p = &s->p;
+  int ix1 = s->ix1, ix2 = s->ix2, jy1 = s->jy1, jy2 = s->jy2, kz1 = s->kz1, kz2 = s->kz2;
+  size_t n1p = (size_t)s->n1p, n2p = (size_t)s->n2p, n3p = (size_t)s->n3p, nc3 = n1p * n2p * n3p;
+#define P1(i, j, k) s->jc[((size_t)(i)-1) + n1p * (((size_t)(j)-1) + n2p * ((size_t)(k)-1))]
+#define P2(i, j, k) s->jc[nc3 + ((size_t)(i)-1) + n1p * (((size_t)(j)-1) + n2p * ((size_t)(k)-1))]
+#define EF(i, j, k, c) efb[(size_t)((c)-1) * nc3 + ((size_t)(i)-1) + n1p * (((size_t)(j)-1) + n2p * ((size_t)(k)-1))]
+  {
+    int j = jy2;
+    for (int k = kz1; k <= kz2; ++k)
+      for (int i = ix1; i <= ix2; ++i) P1(i, j + 1, k) = 3. * (P1(i, j, k) - P1(i, j - 1, k)) + P1(i, j - 2, k);
+  }
+  for (int k = kz1; k <= kz2; ++k)
+    for (int j = jy1; j <= jy2; ++j) {
+      P1(ix2 + 1, j, k) = P1(ix2, j, k);
+      P2(ix2 + 1, j, k) = 2. * P2(ix2, j, k) - P2(ix2 - 1, j, k);
+    }
+  for (int k = kz1; k <= kz2; ++k)
+    for (int j = jy1; j <= jy2; ++j)
+      for (int i = ix1; i <= ix2; ++i) EF(i, j, k, 4) = 0.5 * (P2(i, j, k) + P2(i + 1, j, k));
+  for (int k = kz1; k <= kz2; ++k)
+    for (int j = jy1; j <= jy2; ++j) {
+      double sdhy = 1.0 * p->dy_inv; /* loc_yg(jj,3) = 1 on a uniform grid */
+      for (int i = ix1; i <= ix2 + 1; ++i) EF(i, j, k, 2) = -sdhy * (P1(i, j + 1, k) - P1(i, j, k));
+      for (int i = ix1; i <= ix2; ++i) EF(i, j, k, 1) = -p->dx_inv * (P1(i + 1, j, k) - P1(i, j, k)) / g2;
+    }
+  if (p->ndim == 2) {
+    for (int k = kz1; k <= kz2; ++k)
+      for (int j = jy1; j <= jy2; ++j)
+        for (int i = ix1; i <= ix2; ++i) EF(i, j, k, 3) = 0.5 * bet * (EF(i, j, k, 2) + EF(i + 1, j, k, 2));
+    return;
+  }
+  {
+    int k = kz2;
+    for (int j = jy1; j <= jy2; ++j)
+      for (int i = ix1; i <= ix2; ++i) P1(i, j, k + 1) = 2. * P1(i, j, k) - P1(i, j, k - 1);
+  }
+  for (int k = kz1; k <= kz2; ++k)
+    for (int j = jy1; j <= jy2; ++j)
+      for (int i = ix1; i <= ix2; ++i) EF(i, j, k, 6) = 0.5 * bet * (EF(i, j, k, 2) + EF(i + 1, j, k, 2));
+  for (int k = kz1; k <= kz2; ++k) {
+    double sdhz = 1.0 * p->dz_inv;
+    for (int j = jy1; j <= jy2; ++j)
+      for (int i = ix1; i <= ix2; ++i) EF(i, j, k, 3) = -sdhz * (P1(i, j, k + 1) - P1(i, j, k));
+  }
+  for (int k = kz1; k <= kz2; ++k)
+    for (int j = jy1; j <= jy2; ++j)
+      for (int i = ix1; i <= ix2; ++i) {
+        P2(i, j, k) = 0.5 * (EF(i, j, k, 3) + EF(i + 1, j, k, 3));
+        EF(i, j, k, 5) = -bet * P2(i, j, k);
+      }
+#undef P1
+#undef P2
+#undef EF
+}
+
+/* beam_inject (init_beam_part_distrib.f90:474-630), uniform grid: append the
+   bunch records inside the box to species ic, deposit their charge into
+   jc(1), solve for the potential, jc(2) = bet0 jc(1), then
+   ebf += initial_beam_fields with Bx = 0. */
+int ora_beam_inject(ora_sim* s, int ic, const double* part, int64_t ld, int64_t nb_tot, double gam0) {
+  if (ic < 0 || ic >= s->p.nsp || nb_tot < 0 || ld < nb_tot) return 101;
+  const agpu_params* p = &s->p;
+  /* mpi_beam_distribute (init_beam_part_distrib.f90:273-438): keep, in
+     order, the records with x1 < x <= x2, y1 < y <= y2 (and z1 < z <= z2) */
+  int64_t nb = 0;
+  int64_t* keep = (int64_t*)malloc(sizeof(int64_t) * (size_t)(nb_tot > 0 ? nb_tot : 1));
+  if (!keep) return 103;
+  for (int64_t n = 0; n < nb_tot; ++n) {
+    double x = part[(size_t)n], y = part[(size_t)ld + (size_t)n];
+    int in = y > p->gymin && y <= p->gymax && x > p->gxmin && x <= p->gxmax;
+    if (p->ndim == 3) {
+      double z = part[(size_t)2 * (size_t)ld + (size_t)n];
+      in = in && z > p->gzmin && z <= p->gzmax;
+    }
+    if (in) keep[nb++] = n;
+  }
+  if (s->np[ic] + nb > s->cap[ic]) {
+    free(keep);
+    return 104;
+  }
+  double* sel = (double*)malloc(sizeof(double) * (size_t)(nb > 0 ? nb : 1) * (size_t)s->ndv);
+  if (!sel) {
+    free(keep);
+    return 103;
+  }
+  for (int c = 1; c <= s->ndv; ++c)
+    for (int64_t n = 0; n < nb; ++n) {
+      double v = part[(size_t)(c - 1) * (size_t)ld + (size_t)keep[n]];
+      sel[(size_t)(c - 1) * (size_t)nb + (size_t)n] = v;
+      PART(s, ic, s->np[ic] + 1 + n, c) = v;
+    }
+  free(keep);
+  s->np[ic] += nb;
+  double gam2 = gam0 * gam0;
+  double u0_b = sqrt(gam0 * gam0 - 1.); /* set_init_param.f90:353-354 */
+  double bet0 = u0_b / gam0;
+  size_t nc3 = (size_t)s->n1p * s->n2p * s->n3p;
+  memset(s->jc, 0, sizeof(double) * nc3); /* jc(:,:,:,1) = 0.0 */
+  ora_grid_charge(s, sel, nb, nb, s->jc);
+  free(sel);
+  int rc = ora_beam_potential(s, s->jc, gam2);
+  if (rc) return rc;
+  for (size_t q = 0; q < nc3; ++q) s->jc[nc3 + q] = bet0 * s->jc[q];
+  double* efb = (double*)calloc(nc3 * 6, sizeof(double));
+  if (!efb) return 103;
+  ora_initial_beam_fields(s, efb, gam2, bet0);
+  memset(efb + 3 * nc3, 0, sizeof(double) * nc3); /* ebf_bunch(:,:,:,4) = 0 */
+  for (int c = 0; c < s->nf; ++c)
+    for (size_t q = 0; q < nc3; ++q) s->ebf[(size_t)c * nc3 + q] = s->ebf[(size_t)c * nc3 + q] + efb[(size_t)c * nc3 + q];
+  free(efb);
+  return 0;
+}

@@ -66,6 +66,9 @@ def load():
         "ora_ionz_de_inv": (C.c_double, [P, C.c_int]),
         "ora_draw": (C.c_double, [C.c_uint64, I64, C.c_int, C.c_int]),
         "ora_philox": (None, [C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32)]),
+        "ora_beam_inject": (C.c_int, [P, C.c_int, D, I64, I64, C.c_double]),
+        "ora_beam_potential": (C.c_int, [P, D, C.c_double]),
+        "ora_grid_charge": (None, [P, D, I64, I64, D]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -167,6 +170,27 @@ class Oracle:
         out = AgpuStepOut()
         rc = self.lib.ora_step(self.h, iteration, t, 1 if initial_time else 0, C.byref(out))
         return rc, out
+
+    def beam_inject(self, ic, part, gam0):
+        """beam_inject: append the bunch records inside the box, add the bunch
+        fields to ebf; jc(1) holds the potential afterwards."""
+        a = np.asfortranarray(part, dtype=np.float64)
+        return self.lib.ora_beam_inject(self.h, ic, _dp(a), a.shape[0], a.shape[0], gam0)
+
+    def beam_potential(self, rho, gam2):
+        """fft_3d_psolv / fft_2d_psolv on rho(n1p,n2p,n3p); returns a copy with
+        the interior replaced by the potential."""
+        a = np.array(rho, dtype=np.float64, order="F", copy=True)
+        assert a.shape == (self.n1p, self.n2p, self.n3p)
+        assert self.lib.ora_beam_potential(self.h, _dp(a), gam2) == 0
+        return a
+
+    def grid_charge(self, part):
+        """set_grid_charge of the records part(np, ndv) on a zero grid."""
+        a = np.asfortranarray(part, dtype=np.float64)
+        den = np.zeros((self.n1p, self.n2p, self.n3p), dtype=np.float64, order="F")
+        self.lib.ora_grid_charge(self.h, _dp(a), a.shape[0], a.shape[0], _dp(den))
+        return den
 
     def error_bits(self):
         return self.lib.ora_error_bits(self.h)

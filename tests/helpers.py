@@ -93,3 +93,51 @@ def sort_records(a: np.ndarray) -> np.ndarray:
         return a
     idx = np.lexsort(a.T[::-1])
     return a[idx]
+
+
+# ---- PWFA bunch (the 512x256x256 PWFA set-up on small grids) ----------------
+def grid_pwfa(ndim, nx=48, ny=32, nz=32):
+    """dx = 0.2 um, dy = dz = 0.5 um as the 512x256x256 PWFA case."""
+    if ndim == 2:
+        return Grid(2, nx, ny, 1, k0=5.0, yx_rat=2.5, zx_rat=1.0, cfl=0.8)
+    return Grid(3, nx, ny, nz, k0=5.0, yx_rat=2.5, zx_rat=2.5, cfl=0.8)
+
+
+def pwfa_bunch(p, nb=20000, sxb=2.0, syb=1.5, gam=1957.0, seed=77):
+    """A 200 pC bunch centred in the box (gam 1957, 1% spread, 1 um emittance)."""
+    from aladyn_b200.beam import Bunch
+    return Bunch(nb_tot=nb, charge_pc=200.0, sxb=sxb, syb=syb, gam=gam, epsy=1.0, epsz=1.0, dg=1.0,
+                 xc=p.xmn + 0.5 * p.nx * p.dx, yc=0.0, zc=0.0, seed=seed)
+
+
+def sine_mode(p, n1p, n2p, n3p, a, b, c):
+    """rho with a pure DST-I mode (a, b, c) (0-based) on the interior."""
+    n1, n2, n3 = p.nx, p.ny, (p.nz if p.ndim == 3 else 1)
+    sx = np.sin(np.pi * np.arange(1, n1 + 1) * (a + 1) / (n1 + 1))
+    sy = np.sin(np.pi * np.arange(1, n2 + 1) * (b + 1) / (n2 + 1))
+    sz = np.sin(np.pi * np.arange(1, n3 + 1) * (c + 1) / (n3 + 1)) if p.ndim == 3 else np.ones(1)
+    rho = np.zeros((n1p, n2p, n3p), order="F")
+    k0 = 2 if p.ndim == 3 else 0
+    rho[2:2 + n1, 2:2 + n2, k0:k0 + n3] = sx[:, None, None] * sy[None, :, None] * sz[None, None, :]
+    return rho
+
+
+def sine_mode_potential(p, rho, a, b, c, gam2):
+    """The reference solver's answer for a pure mode: omp0 rho / k^2 with
+    k_i = 2 sin(d_i ak_i / 2)/d_i, ak = pi i / l_box, and the x round-trip
+    factor (n1+1)/(n1+2) of its forward scale 1/(2(n1+2)) (3D only)."""
+    def sk(d, l, i):
+        return 2. * math.sin(0.5 * d * (math.acos(-1.0) / l * i)) / d
+    lx, ly, lz = p.xmax - p.xmn, p.gymax - p.gymin, p.gzmax - p.gzmin
+    if p.ndim == 3:
+        ak2 = sk(p.dz, lz, c + 1) ** 2 + sk(p.dy, ly, b + 1) ** 2 + sk(p.dx, lx, a + 1) ** 2 / gam2
+        return rho * (p.ompe / ak2) * (p.nx + 1) / (p.nx + 2)
+    return rho * (p.ompe / sk(p.dy, ly, b + 1) ** 2)
+
+
+def inside_box(p, rec):
+    """The records mpi_beam_distribute keeps: gxmin < x <= gxmax, y and z alike."""
+    m = (rec[:, 0] > p.gxmin) & (rec[:, 0] <= p.gxmax) & (rec[:, 1] > p.gymin) & (rec[:, 1] <= p.gymax)
+    if p.ndim == 3:
+        m &= (rec[:, 2] > p.gzmin) & (rec[:, 2] <= p.gzmax)
+    return rec[m]
