@@ -37,6 +37,7 @@ UNITS = [
     ("agpu_noalloc.cu", ["-fmad=false"]),
     ("agpu_beam.cu", ["-fmad=false"]),
     ("agpu_ionz.cpp", []),
+    ("agpu_batch.cpp", ["-Xcompiler", "-pthread"]),
 ]
 HEADERS = ["agpu_common.cuh", "agpu_kernels.h", "agpu_util.h", "agpu_yee.cuh", "agpu_ionz.h", "agpu_bin.cuh",
            "agpu_tile.h", "agpu_select.cuh", "agpu_beam.h"]
@@ -67,7 +68,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             subprocess.run(cmd, check=True)
             rebuilt = True
     if rebuilt or force or not os.path.exists(LIB):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lcufft",
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lcufft", "-Xcompiler", "-pthread",
                "-Xlinker", "-rpath=/usr/local/cuda/lib64"]
         if verbose:
             print(" ".join(cmd))

@@ -38,6 +38,8 @@ struct Counters {
   unsigned int err;
   int alive;  // particles in tiles after the last binning
   double fmax;
+  unsigned long long pushed;  // deferred mode: particles pushed since the last refresh
+  int alive4[4];              // deferred mode: alive count per species at the refresh
 };
 
 }  // namespace
@@ -97,6 +99,10 @@ struct agpu_handle {
   int* cursor = nullptr;
   bool binned[4] = {false, false, false, false};
   long long nalive[4] = {0, 0, 0, 0};  // np minus removed records still stored
+  // deferred counts: tiled steps leave the alive counts and the error word
+  // on the device; refresh_counts reads them at the next synchronisation
+  bool defer = false;
+  bool stale[4] = {false, false, false, false};
   // flags
   bool fields_set = false;
   bool deterministic = false;
@@ -224,6 +230,30 @@ int read_counters(agpu_handle* h) {
   return 0;
 }
 
+// Deferred mode: bring the alive counts of the species binned since the last
+// refresh, the pushed-particle count and the error word to the host, then
+// restart the device accumulators.
+int refresh_counts(agpu_handle* h) {
+  bool any = false;
+  for (int ic = 0; ic < 4; ++ic) any = any || h->stale[ic];
+  if (!any) return 0;
+  for (int ic = 0; ic < 4; ++ic)
+    if (h->stale[ic])
+      CK(cudaMemcpyAsync(&h->d_cnt->alive4[ic], h->tstart[ic] + h->tg.ntiles, sizeof(int), cudaMemcpyDeviceToDevice,
+                         h->st));
+  CK(cudaMemcpyAsync(h->h_cnt, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->error_bits |= h->h_cnt->err;
+  h->timers.pushes += (long long)h->h_cnt->pushed;
+  for (int ic = 0; ic < 4; ++ic)
+    if (h->stale[ic]) {
+      h->nalive[ic] = h->h_cnt->alive4[ic];
+      h->stale[ic] = false;
+    }
+  CK(cudaMemsetAsync(h->d_cnt, 0, sizeof(Counters), h->st));
+  return 0;
+}
+
 long long lattice_columns_end(const agpu_handle* h, int ic, long long i1, double xmx, bool reference_quirk) {
   // particles_inject (src/dynamics/window.f90:124-136): first column with
   // xpt > xmx ends the block; when that column is sptx_max itself, the
@@ -287,6 +317,7 @@ int add_lattice_columns(agpu_handle* h, int ic, long long i1, long long i2) {
 int drop_removed(agpu_handle* h, int ic);
 
 int compact_species(agpu_handle* h, int ic, bool window) {
+  if (int rc = refresh_counts(h)) return rc;
   if (h->np[ic] <= 0) return 0;
   long long kept;
   if (window && h->binned[ic]) {
@@ -344,16 +375,21 @@ int rebin(agpu_handle* h, int ic) {
   bin_finish(h->key[ic], h->np[ic], t, h->hist[ic], h->tstart[ic], h->cursor, h->perm[ic], h->st, h->sms);
   CK(cudaGetLastError());
   h->timers.launches_total += 3;
+  h->binned[ic] = true;
+  if (h->defer) {
+    h->stale[ic] = true;
+    return 0;
+  }
   CK(cudaMemcpyAsync(&h->d_cnt->alive, h->tstart[ic] + t.ntiles, sizeof(int), cudaMemcpyDeviceToDevice, h->st));
   if (int rc = read_counters(h)) return rc;
   h->nalive[ic] = h->h_cnt->alive;
-  h->binned[ic] = true;
   return 0;
 }
 
 // Drop the removed records (key == ntiles) keeping the memory order, so the
 // stored arrays hold exactly the alive particles; the binning is then stale.
 int drop_removed(agpu_handle* h, int ic) {
+  if (int rc = refresh_counts(h)) return rc;
   if (!h->binned[ic] || h->nalive[ic] == h->np[ic]) return 0;
   long long kept;
   if (h->fp32) {
@@ -383,7 +419,7 @@ int tiled_push(agpu_handle* h, int ic, int initial_time, agpu_step_out* out) {
     if (rc) return rc;
   }
   const long long alive0 = h->nalive[ic];
-  hist_reset(h->hist[ic], h->tstart[ic], h->tg, h->np[ic], false, h->st);
+  hist_reset(h->hist[ic], h->tstart[ic], h->tg, h->np[ic], false, h->defer ? &h->d_cnt->pushed : nullptr, h->st);
   ph_begin(h, PH_PUSH);
   if (h->fp32) {
     TileArgs32 a;
@@ -456,11 +492,16 @@ int tiled_push(agpu_handle* h, int ic, int initial_time, agpu_step_out* out) {
   ph_end(h, PH_PUSH);
   h->timers.launches_push_deposit += 1;
   h->timers.launches_total += 2;  // histogram reset + tile kernel
-  h->timers.pushes += alive0;
+  if (!h->defer) h->timers.pushes += alive0;
   ph_begin(h, PH_SORT);
   bin_finish(h->key[ic], h->np[ic], h->tg, h->hist[ic], h->tstart[ic], h->cursor, h->perm[ic], h->st, h->sms);
   CK(cudaGetLastError());
   h->timers.launches_total += 2;  // scan + scatter
+  if (h->defer) {
+    h->stale[ic] = true;
+    ph_end(h, PH_SORT);
+    return 0;
+  }
   CK(cudaMemcpyAsync(&h->d_cnt->alive, h->tstart[ic] + h->tg.ntiles, sizeof(int), cudaMemcpyDeviceToDevice, h->st));
   if (int rc = read_counters(h)) return rc;
   ph_end(h, PH_SORT);
@@ -940,11 +981,13 @@ int agpu_set_species(agpu_handle* h, int32_t ic, const double* part, int64_t ld,
   h->np[ic] = np;
   h->nalive[ic] = np;
   h->binned[ic] = false;
+  h->stale[ic] = false;
   return 0;
 }
 
 int agpu_get_species(agpu_handle* h, int32_t ic, double* part, int64_t ld, int64_t* np, int32_t ndv) {
   if (!h || ic < 0 || ic >= h->p.nsp || !np) return AGPU_E_ARG;
+  if (int rc = refresh_counts(h)) return rc;
   if (h->binned[ic] && h->nalive[ic] != h->np[ic]) {
     if (int rc = drop_removed(h, ic)) return rc;
   }
@@ -971,6 +1014,7 @@ int agpu_get_species(agpu_handle* h, int32_t ic, double* part, int64_t ld, int64
 
 int agpu_get_count(agpu_handle* h, int32_t ic, int64_t* np) {
   if (!h || !np || ic < 0 || ic >= h->p.nsp) return AGPU_E_ARG;
+  if (int rc = refresh_counts(h)) return rc;
   *np = h->binned[ic] ? h->nalive[ic] : h->np[ic];
   return 0;
 }
@@ -1080,7 +1124,15 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu
   out->ion_field_max = -1.0;
   agpu_params& p = h->p;
   int rc = 0;
-  CK(cudaMemsetAsync(h->d_cnt, 0, sizeof(Counters), h->st));
+  if (h->defer) {
+    // keep the error word and the push count accumulating on the device
+    CK(cudaMemsetAsync(&h->d_cnt->removed, 0, sizeof(unsigned long long), h->st));
+    CK(cudaMemsetAsync(&h->d_cnt->fmax, 0, sizeof(double), h->st));
+    if (p.ionz_lev > 0)
+      if (int rc_ = refresh_counts(h)) return rc_;
+  } else {
+    CK(cudaMemsetAsync(h->d_cnt, 0, sizeof(Counters), h->st));
+  }
   // pfields_prepare -> field_xyzbd
   ph_begin(h, PH_YEE);
   if (h->fp32) field_bd32(Dev32{h->g, h->ebf32, h->jhi, h->jlo}, h->st, h->sms);
@@ -1221,7 +1273,9 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu
       }
     }
   }
-  if (int rc_ = read_counters(h)) return rc_;
+  if (!h->defer)
+    if (int rc_ = read_counters(h)) return rc_;
+  // deferred mode: the counts of the last synchronisation point
   for (int ic = 0; ic < 4; ++ic) out->np[ic] = h->binned[ic] ? h->nalive[ic] : h->np[ic];
   out->xmn = p.xmn;
   out->error_bits = h->error_bits;
@@ -1432,7 +1486,15 @@ int agpu_get_stream(agpu_handle* h, void** stream) {
 }
 int agpu_synchronize(agpu_handle* h) {
   if (!h) return AGPU_E_ARG;
+  if (int rc = refresh_counts(h)) return rc;
   CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+int agpu_set_deferred_counts(agpu_handle* h, int32_t on) {
+  if (!h) return AGPU_E_ARG;
+  if (!on)
+    if (int rc = refresh_counts(h)) return rc;
+  h->defer = on != 0;
   return 0;
 }
 int agpu_set_sort_interval(agpu_handle* h, int32_t steps) {

@@ -402,12 +402,18 @@ void tile_push64(const TileArgs64& a, cudaStream_t st) {
 
 // Histogram of the next binning: tile bins zero, the removed bin keeps the
 // particles already removed (they are not revisited by any tile).
-__global__ void k_hist_reset(int* hist, const int* tstart, int ntiles, int np, int first) {
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= ntiles; b += gridDim.x * blockDim.x)
+// Next histogram zeroed, the dead bin seeded with the records already dead;
+// with `pushed` set, the alive count of this push (tstart[ntiles]) is added
+// to it (the deferred-count mode keeps the push count on the device).
+__global__ void k_hist_reset(int* hist, const int* tstart, int ntiles, int np, int first, unsigned long long* pushed) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= ntiles; b += gridDim.x * blockDim.x) {
     hist[b] = (b == ntiles && !first) ? (np - tstart[ntiles]) : 0;
+    if (b == ntiles && pushed) *pushed += (unsigned long long)tstart[ntiles];
+  }
 }
-void hist_reset(int* hist, const int* tstart, const TileGeo& t, long long np, bool first, cudaStream_t st) {
-  k_hist_reset<<<(t.ntiles + 256) / 256, 256, 0, st>>>(hist, tstart, t.ntiles, (int)np, first ? 1 : 0);
+void hist_reset(int* hist, const int* tstart, const TileGeo& t, long long np, bool first, unsigned long long* pushed,
+                cudaStream_t st) {
+  k_hist_reset<<<(t.ntiles + 256) / 256, 256, 0, st>>>(hist, tstart, t.ntiles, (int)np, first ? 1 : 0, pushed);
 }
 
 TileGeo make_tiles(const Geo& g, int nx, int ny, int nz) {

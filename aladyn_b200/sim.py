@@ -52,11 +52,15 @@ def unpack_slot(slot: np.ndarray):
 class PicDevice:
     """One simulation resident on one GPU."""
 
-    def __init__(self, params, lib_path: str | None = None):
+    def __init__(self, params, lib_path: str | None = None, handle=None):
         self.lib = abi.load_library(lib_path)
         self.params = params
-        self.h = C.c_void_p()
-        check(self.lib.agpu_create(C.byref(params), C.byref(self.h)), "agpu_create")
+        self.owned = handle is None
+        if handle is None:
+            self.h = C.c_void_p()
+            check(self.lib.agpu_create(C.byref(params), C.byref(self.h)), "agpu_create")
+        else:
+            self.h = handle  # an instance of a PicBatch, destroyed with the batch
         self.n1p, self.n2p, self.n3p = dims(params)
         self.ndv = ndv(params)
         self.nf = params.nfield
@@ -64,9 +68,9 @@ class PicDevice:
 
     # -- lifecycle ---------------------------------------------------------
     def close(self):
-        if self.h:
+        if self.h and self.owned:
             self.lib.agpu_destroy(self.h)
-            self.h = C.c_void_p()
+        self.h = C.c_void_p()
 
     def __enter__(self):
         return self
@@ -201,6 +205,55 @@ class PicDevice:
 
     def synchronize(self):
         check(self.lib.agpu_synchronize(self.h), "agpu_synchronize")
+
+
+    def set_deferred_counts(self, on: bool = True):
+        check(self.lib.agpu_set_deferred_counts(self.h, 1 if on else 0), "agpu_set_deferred_counts")
+
+
+class PicBatch:
+    """N independent simulations on one GPU (a parameter scan), advanced
+    together by agpu_batch_run.  ``instances[i]`` is a PicDevice view of
+    instance i for its set-up and read-back."""
+
+    def __init__(self, params_list, lib_path: str | None = None):
+        self.lib = abi.load_library(lib_path)
+        n = len(params_list)
+        self._params = (abi.AgpuParams * n)(*params_list)
+        self.b = C.c_void_p()
+        check(self.lib.agpu_batch_create(C.cast(self._params, C.c_void_p), n, C.byref(self.b)), "agpu_batch_create")
+        self.instances = []
+        for i in range(n):
+            h = C.c_void_p()
+            check(self.lib.agpu_batch_handle(self.b, i, C.byref(h)), "agpu_batch_handle")
+            self.instances.append(PicDevice(self._params[i], lib_path, handle=h))
+
+    def __len__(self):
+        return len(self.instances)
+
+    def run(self, nsteps: int, nthreads: int = 0):
+        """Advance every instance by nsteps; returns the per-instance status."""
+        st = (C.c_int32 * len(self))()
+        self.lib.agpu_batch_run(self.b, nsteps, nthreads, st)
+        return list(st)
+
+    def clock(self, i: int):
+        it, t = C.c_int32(), C.c_double()
+        check(self.lib.agpu_batch_clock(self.b, i, C.byref(it), C.byref(t)), "agpu_batch_clock")
+        return it.value, t.value
+
+    def close(self):
+        if self.b:
+            for d in self.instances:
+                d.h = C.c_void_p()
+            self.lib.agpu_batch_destroy(self.b)
+            self.b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def run_lp_cycle(dev: PicDevice, nsteps: int, t0: float = 0.0, iter0: int = 0):

@@ -261,6 +261,28 @@ int agpu_beam_inject(agpu_handle* h, int32_t ic, const double* part, int64_t ld,
  * Laplacian(pot) = -ompe rho (x-derivative over gam2 in 3D). */
 int agpu_beam_potential(agpu_handle* h, const double* rho, double* pot, double gam2);
 
+/* ---- batched instances (parameter scans) ------------------------------- */
+/* N independent simulations on one GPU, each with its own parameters,
+ * handle and stream (the reference runs a scan as N separate jobs).  No
+ * counterpart call in the reference: agpu_batch_run replaces running the N
+ * jobs' lp_run loops one after the other.  Set each instance up through its
+ * handle (agpu_batch_handle + the calls above), then agpu_batch_run advances
+ * every instance by nsteps steps from its own (iter, t), starting at
+ * (0, 0.0): worker threads (nthreads, 0 = one per host core, at most N) each
+ * drive a share of the instances in deferred-count mode and interleave their
+ * steps, so kernels of different instances overlap on the GPU.  status[i]
+ * (optional, N entries) receives each instance's first error; the return
+ * value is the first non-zero status.  All instances are synchronised and
+ * their counts refreshed when the call returns. */
+typedef struct agpu_batch agpu_batch;
+int agpu_batch_create(const agpu_params* params, int32_t n, agpu_batch** b);
+int agpu_batch_destroy(agpu_batch* b);
+int agpu_batch_size(const agpu_batch* b, int32_t* n);
+int agpu_batch_handle(agpu_batch* b, int32_t i, agpu_handle** h);
+int agpu_batch_run(agpu_batch* b, int32_t nsteps, int32_t nthreads, int32_t* status);
+/* The step counter and time of instance i after the steps run so far. */
+int agpu_batch_clock(const agpu_batch* b, int32_t i, int32_t* iter, double* t);
+
 /* ---- diagnostics ------------------------------------------------------- */
 /* FP64 reductions of Envar / energy_momenta
  * (src/diagnostics/diag_part_and_fields.f90:172-220, 485-719). */
@@ -295,6 +317,15 @@ int agpu_synchronize(agpu_handle* h);
  * reproduces the reference arithmetic bit for bit (slow; for verification,
  * the race-free counterpart of the atomic deposit). */
 int agpu_set_deterministic(agpu_handle* h, int32_t on);
+/* Deferred counts (on != 0): steps of the tiled species leave the particle
+ * counts, the push count and the error word on the device, so a step
+ * between window shifts makes no host synchronisation and a host can queue
+ * many steps ahead.  agpu_step_out.np and .error_bits then hold the values of
+ * the last synchronisation point (a window shift, agpu_get_count,
+ * agpu_get_species, agpu_diag, agpu_synchronize, or turning the mode off);
+ * .removed is not filled.  Off by default (the reference's lp_run reports
+ * the counts every step). */
+int agpu_set_deferred_counts(agpu_handle* h, int32_t on);
 /* Sort interval in steps for the tile sort (0 = never). */
 int agpu_set_sort_interval(agpu_handle* h, int32_t steps);
 /* sizeof of agpu_params, agpu_plasma, agpu_laser, agpu_step_out,

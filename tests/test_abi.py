@@ -53,6 +53,12 @@ def test_create_fails_loudly_without_device():
     h = C.c_void_p()
     assert lib.agpu_create(C.byref(p), C.byref(h)) == abi.AGPU_E_NODEVICE
     assert not h.value
+    # a batch of instances reports the same, and creates nothing
+    arr = (abi.AgpuParams * 3)(p, p, p)
+    b = C.c_void_p()
+    assert lib.agpu_batch_create(C.cast(arr, C.c_void_p), 3, C.byref(b)) == abi.AGPU_E_NODEVICE
+    assert not b.value
+    assert lib.agpu_batch_create(C.cast(arr, C.c_void_p), 0, C.byref(b)) == abi.AGPU_E_ARG
 
 
 @pytest.mark.parametrize("an,z0,model", [(7, 0, 1), (7, 0, 4), (7, 2, 2), (2, 0, 3), (6, 0, 5), (1, 0, 1)])
