@@ -63,6 +63,40 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = "lwfa3d_1024x256x256_ppc8"
 
+# Batched 2D scan: 256 LWFA instances, nx in {256..1024} x ny in {64, 128, 256}
+# (dx = 0.05 lambda, dy = 0.2 lambda, 4 ppc), a0 ~ U[1, 4], waist ~ U[3, 8]
+# lambda, n_e/n_c ~ logU[0.002, 0.02], drawn with Philox(seed, instance).
+SCAN_WORKLOAD = "scan2d_256"
+SCAN_NX = (256, 384, 512, 768, 1024)
+SCAN_NY = (64, 128, 256)
+
+
+def scan_instances(n: int, precision: int, seed: int = 20241205):
+    from aladyn_b200.config import Grid, laser, make_params, n_over_nc_to_n0, plasma
+    from aladyn_b200.lattice import philox4x32_10
+    idx = np.arange(n, dtype=np.uint32)
+    z = np.zeros(n, dtype=np.uint32)
+    r = philox4x32_10(idx, z, z, np.full(n, 0x5343414E, dtype=np.uint32), seed, 0)
+    r2 = philox4x32_10(idx, z, z + 1, np.full(n, 0x5343414E, dtype=np.uint32), seed, 0)
+    u = [(x.astype(np.float64) + 0.5) / 4294967296.0 for x in (*r, *r2)]
+    out = []
+    for i in range(n):
+        nx = SCAN_NX[int(u[0][i] * len(SCAN_NX))]
+        ny = SCAN_NY[int(u[1][i] * len(SCAN_NY))]
+        a0 = 1.0 + 3.0 * u[2][i]
+        w0 = (3.0 + 5.0 * u[3][i]) * LAM0
+        n_over_nc = 10.0 ** (math.log10(0.002) + u[4][i] * (math.log10(0.02) - math.log10(0.002)))
+        g = Grid(2, nx, ny, 1, 25.0, 4.0, 1.0, 0.8)
+        cap = int(nx * ny * 4 * 1.04) + 4096
+        p = make_params(g, precision=precision, capacity=(cap, 0, 0, 0), w_sh=10, w_speed=1.0)
+        lx = nx * p.dx
+        las = laser(a0, LAM0, w0, 10 * LAM0, xc=0.5 * lx, xf=0.5 * lx)
+        n0 = n_over_nc_to_n0(n_over_nc, LAM0)
+        src = plasma(0, 2, 2, 1, -1, n0 / 4, x_start=p.gxmin, x_end=1.0e7, y_min=p.gymin, y_max=p.gymax,
+                     jitter=0.5, seed=seed + i)
+        out.append((p, las, src))
+    return out
+
 
 def bytes_per_push(ndim: int, ppc: int, fp32: bool) -> float:
     """Algorithmic bytes of one particle push (gather+push+deposit):
@@ -384,6 +418,92 @@ def make_reducers(torch, world: int, device: str):
     return barrier, (lambda x: red(x, dist.ReduceOp.MAX)), (lambda x: red(x, dist.ReduceOp.SUM))
 
 
+def bench_scan(a, torch):
+    """Batched scan: the 256 instances advanced together (agpu_batch_run)
+    against the same instances run one after the other through agpu_step.
+    Both arms: fresh instances, W warm-up steps, then K timed steps; device
+    time by CUDA events bracketing the timed steps after a synchronisation."""
+    from aladyn_b200.abi import AGPU_FP32_SPLIT
+    from aladyn_b200.sim import PicBatch, PicDevice
+    n = 256
+    cases = scan_instances(n, AGPU_FP32_SPLIT)
+
+    def setup(d, las, src):
+        d.init_laser(las)
+        d.set_plasma_source(src)
+        d.load_plasma(0)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    clk = ClockSampler(torch.cuda.current_device())
+    if not a.no_clocks:
+        clk.start()
+    # batched arm
+    batch = PicBatch([c[0] for c in cases])
+    for d, (p, las, src) in zip(batch.instances, cases):
+        setup(d, las, src)
+    st = batch.run(a.warmup, a.scan_threads)
+    assert st == [0] * n, st
+    for d in batch.instances:
+        d.reset_timers()
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record()
+    st = batch.run(a.steps, a.scan_threads)
+    e1.record()
+    e1.synchronize()
+    ms_b = e0.elapsed_time(e1)
+    assert st == [0] * n, st
+    tms = [d.timers() for d in batch.instances]
+    pushes_b = sum(t.pushes for t in tms)
+    launches_b = sum(t.launches_total for t in tms)
+    batch.close()
+    # sequential arm: one instance at a time through the single-instance path
+    ms_s, pushes_s = 0.0, 0
+    for (p, las, src) in cases:
+        dev = PicDevice(p)
+        setup(dev, las, src)
+        t, it = 0.0, 0
+        for _ in range(a.warmup):
+            dev.lp_run(t, it, initial_time=(it == 0))
+            t += p.dt
+            it += 1
+        dev.reset_timers()
+        dev.synchronize()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record()
+        for _ in range(a.steps):
+            dev.lp_run(t, it, initial_time=(it == 0))
+            t += p.dt
+            it += 1
+        dev.synchronize()
+        e1.record()
+        e1.synchronize()
+        ms_s += e0.elapsed_time(e1)
+        pushes_s += dev.timers().pushes
+        dev.close()
+    clocks = clk.stop()
+    value = n * a.steps / (ms_b * 1e-3)
+    seq = n * a.steps / (ms_s * 1e-3)
+    cells = sum(c[0].nx * c[0].ny for c in cases)
+    line = {"metric": "instance-steps/s", "value": value, "unit": "instance-steps/s", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_b / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32-split",
+            "data": "synthetic: seeded instance draws, jittered lattice plasma, Gaussian lasers",
+            "config": {"workload": SCAN_WORKLOAD, "instances": n, "nx": list(SCAN_NX), "ny": list(SCAN_NY),
+                       "ppc": 4, "cells_total": cells, "window": "moving, w_sh=10",
+                       "threads": a.scan_threads or os.cpu_count()},
+            "sequential": {"value": seq, "unit": "instance-steps/s", "ms_per_step": ms_s / a.steps,
+                           "path": "agpu_step per instance, one instance after the other"},
+            "batched_over_sequential": value / seq,
+            "pushes_per_s": {"batched": pushes_b / (ms_b * 1e-3), "sequential": pushes_s / (ms_s * 1e-3)},
+            "gpu_launches": int(launches_b), "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # --------------------------------------------------------------------------
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
@@ -391,7 +511,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + [SCAN_WORKLOAD])
+    ap.add_argument("--scan-threads", type=int, default=0, help="batch worker threads (0 = host cores)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -402,6 +523,15 @@ def main(argv=None):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.workload == SCAN_WORKLOAD:
+        if a.impl == "reference" or world > 1:
+            if rank == 0:
+                print(json.dumps({"impl": a.impl, "workload": SCAN_WORKLOAD,
+                                  "unavailable": "the scan is measured as batched vs sequential on one GPU"}))
+            return 0
+        import torch
+        torch.cuda.set_device(local)
+        return bench_scan(a, torch)
     w = WORKLOADS[a.workload]
     ppc_w = w["ppc"][0] * w["ppc"][1] * (w["ppc"][2] if w["ndim"] == 3 else 1)
     config = {"workload": a.workload, "grid": [w["nx"], w["ny"], w["nz"]], "ppc": ppc_w,
