@@ -222,7 +222,10 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
     // Esirkepov deposit into the shared tile (grid_part_connect.f90:956-1334).
     // Old-plane and new-plane terms are regrouped onto the particle's 5-slot
     // windows (slot 0 = old node - 2): each current component is one dense
-    // product over (x0..x1) x (y0..y1) [x (z0..z1)], 9-64 points.
+    // product over (x0..x1) x (y0..y1) [x (z0..z1)].  Along its own axis a
+    // component's running sum ends at sum(S0) - sum(S1) = 0 in the last slot
+    // (x1 for Jx, y1 for Jy, z1 for Jz), so that slot is not deposited: 54
+    // instead of 81 shared atomics (3D) for a particle that stays in its cell.
     const float wght = qc * slot_wgh(sl);
     float ax0[3], ay0[3], axn[3], ayn[3];
     wq(sx, ax0);
@@ -258,8 +261,8 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
         for (int u = 0; u < 5; ++u) {
           if (u < x0 || u > x1) continue;
           int o = lx + u + JX * (ly + v);
-          atomicAdd(&sJx[o], wys[v] * cx[u]);
-          atomicAdd(&sJy[o], wxs[u] * cy[v]);
+          if (u < x1) atomicAdd(&sJx[o], wys[v] * cx[u]);
+          if (v < y1) atomicAdd(&sJy[o], wxs[u] * cy[v]);
         }
       }
     } else {
@@ -298,9 +301,9 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
           for (int u = 0; u < 5; ++u) {
             if (u < x0 || u > x1) continue;
             const int o = ow + u + JX * v;
-            atomicAdd(&sJx[o], cx[u] * wyv);
-            atomicAdd(&sJy[o], cyv * (wx0[u] * A0 + wx1[u] * A1));
-            atomicAdd(&sJz[o], czw * (wx0[u] * b0[v] + wx1[u] * b1[v]));
+            if (u < x1) atomicAdd(&sJx[o], cx[u] * wyv);
+            if (v < y1) atomicAdd(&sJy[o], cyv * (wx0[u] * A0 + wx1[u] * A1));
+            if (w < z1) atomicAdd(&sJz[o], czw * (wx0[u] * b0[v] + wx1[u] * b1[v]));
           }
         }
       }
