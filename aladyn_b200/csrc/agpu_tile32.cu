@@ -6,11 +6,18 @@
 //   1. stages the six field components of the tile plus a one-node guard
 //      (the qlh gather stencil) into shared memory,
 //   2. zeroes a shared current tile with a two-node guard (the Esirkepov
-//      window of a particle that moves at most one node),
+//      window of a particle that moves at most one node) and finds the
+//      tile's largest |charge * weight|,
 //   3. gathers, pushes (exact-gamma Boris) and deposits every particle, the
-//      deposit going into shared memory with native FP32 shared atomics,
-//   4. flushes the shared currents to the global (hi, lo) pair once, with
-//      the TwoSum error of each global add accumulated into lo,
+//      deposit going into shared memory as int32 fixed point with integer
+//      shared atomics (on sm_100a several times the throughput of FP32
+//      shared atomics, and unaffected by lanes that hit the same node); the
+//      tile's scale 2^30 / (max|q w| * particles) bounds every node's sum
+//      below 2^31 (one particle adds at most 1.69 |q w| to a node), and
+//      integer sums make the tile's currents independent of the order,
+//   4. flushes the shared currents to the global (hi, lo) pair once, each
+//      fixed-point sum converted exactly to FP64 and split into hi + lo,
+//      with the TwoSum error of each global add accumulated into lo,
 //   5. writes each particle's new tile key and the next histogram.
 #include "agpu_bin.cuh"
 #include "agpu_common.cuh"
@@ -27,6 +34,9 @@ __device__ __forceinline__ void kadd_g(float* hi, float* lo, float v) {
   float err = __fadd_rn(__fsub_rn(old, __fsub_rn(s, bp)), __fsub_rn(v, bp));
   if (err != 0.f) atomicAdd(lo, err);
 }
+
+// Fixed-point contribution of v at scale sc (|v sc| < 2^31 by construction).
+__device__ __forceinline__ void fx_add(int* a, float v, float sc) { atomicAdd(a, __float2int_rn(v * sc)); }
 
 __device__ __forceinline__ void wq(float s, float a[3]) {
   float s2 = s * s;
@@ -67,8 +77,9 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
   constexpr int FV = FX * FY * FZ, JV = JX * JY * JZ;
   constexpr int NF = (NDIM == 3) ? 6 : 3, NC = (NDIM == 3) ? 3 : 2;
   extern __shared__ float smem[];
-  float* sF = smem;           // NF * FV
-  float* sJ = smem + NF * FV;  // NC * JV
+  float* sF = smem;                                  // NF * FV
+  int* sJ = reinterpret_cast<int*>(smem + NF * FV);  // NC * JV, fixed point
+  __shared__ unsigned int s_wmax;
 
   const Geo g = a.g;
   const int t = blockIdx.x;
@@ -87,8 +98,25 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
       v = __ldg(&a.ebf[g.ncell * c + goff(g, gi, gj, gk)]);
     sF[e] = v;
   }
-  for (int e = threadIdx.x; e < NC * JV; e += blockDim.x) sJ[e] = 0.f;
+  for (int e = threadIdx.x; e < NC * JV; e += blockDim.x) sJ[e] = 0;
+  if (threadIdx.x == 0) s_wmax = 0u;
   __syncthreads();
+  {
+    // largest |charge * weight| of the tile (non-negative floats order as
+    // their bit patterns)
+    float wl = 0.f;
+    for (int q = beg + threadIdx.x; q < end; q += blockDim.x) {
+      const uint64_t sl = a.p.slot[a.perm[q]];
+      wl = fmaxf(wl, fabsf((float)slot_charge(sl) * slot_wgh(sl)));
+    }
+    if (!(wl <= 3.0e38f)) wl = 3.0e38f;  // NaN / inf weights: keep the scale finite
+    for (int o = 16; o > 0; o >>= 1) wl = fmaxf(wl, __shfl_xor_sync(0xffffffffu, wl, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&s_wmax, __float_as_uint(wl));
+  }
+  __syncthreads();
+  const float wtile = __uint_as_float(s_wmax) * (float)(end - beg);
+  float fsc = 1073741824.f / wtile;  // 2^30 / (max|q w| * particles)
+  if (!(fsc < 1.0e30f)) fsc = 1.0e30f;
 
   const int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
   for (int q = beg + threadIdx.x; q < end; q += blockDim.x) {
@@ -245,8 +273,8 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
     }
     // local J coordinates of window slot 0 (node i0-2)
     const int lx = i0 - i0t, ly = j0 - j0t;
-    float* sJx = sJ;
-    float* sJy = sJ + JV;
+    int* sJx = sJ;
+    int* sJy = sJ + JV;
     if (NDIM == 2) {
       float wxs[5], wys[5];
 #pragma unroll
@@ -261,8 +289,8 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
         for (int u = 0; u < 5; ++u) {
           if (u < x0 || u > x1) continue;
           int o = lx + u + JX * (ly + v);
-          if (u < x1) atomicAdd(&sJx[o], wys[v] * cx[u]);
-          if (v < y1) atomicAdd(&sJy[o], wxs[u] * cy[v]);
+          if (u < x1) fx_add(&sJx[o], wys[v] * cx[u], fsc);
+          if (v < y1) fx_add(&sJy[o], wxs[u] * cy[v], fsc);
         }
       }
     } else {
@@ -285,7 +313,7 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
         int m = u - jh;
         b1[u] = (m == 0) ? ayn[0] : (m == 1) ? ayn[1] : (m == 2) ? ayn[2] : 0.f;  // new y shape
       }
-      float* sJz = sJ + 2 * JV;
+      int* sJz = sJ + 2 * JV;
       for (int w = z0; w <= z1; ++w) {
         const int m0 = w - 1, m1 = w - kh;
         const float A0 = (m0 == 0) ? az0[0] : (m0 == 1) ? az0[1] : (m0 == 2) ? az0[2] : 0.f;
@@ -301,9 +329,9 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
           for (int u = 0; u < 5; ++u) {
             if (u < x0 || u > x1) continue;
             const int o = ow + u + JX * v;
-            if (u < x1) atomicAdd(&sJx[o], cx[u] * wyv);
-            if (v < y1) atomicAdd(&sJy[o], cyv * (wx0[u] * A0 + wx1[u] * A1));
-            if (w < z1) atomicAdd(&sJz[o], czw * (wx0[u] * b0[v] + wx1[u] * b1[v]));
+            if (u < x1) fx_add(&sJx[o], cx[u] * wyv, fsc);
+            if (v < y1) fx_add(&sJy[o], cyv * (wx0[u] * A0 + wx1[u] * A1), fsc);
+            if (w < z1) fx_add(&sJz[o], czw * (wx0[u] * b0[v] + wx1[u] * b1[v]), fsc);
           }
         }
       }
@@ -311,9 +339,10 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
   }
   __syncthreads();
   // 4: one compensated flush of the tile's currents (nodes i0t-2 ..)
+  const double inv_sc = 1.0 / (double)fsc;
   for (int e = threadIdx.x; e < NC * JV; e += blockDim.x) {
-    float v = sJ[e];
-    if (v == 0.f) continue;
+    const int iv = sJ[e];
+    if (iv == 0) continue;
     int c = e / JV, rr = e - c * JV;
     int lx = rr % JX, ly = (rr / JX) % JY, lz = rr / (JX * JY);
     int gi = i0t - 2 + lx, gj = j0t - 2 + ly, gk = (NDIM == 3) ? k0t - 2 + lz : 1;
@@ -322,7 +351,11 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
       continue;
     }
     long long o = g.ncell * c + goff(g, gi, gj, gk);
-    kadd_g(&a.jhi[o], &a.jlo[o], v);
+    const double dv = (double)iv * inv_sc;
+    const float vh = (float)dv;
+    const float vl = (float)(dv - (double)vh);
+    kadd_g(&a.jhi[o], &a.jlo[o], vh);
+    if (vl != 0.f) atomicAdd(&a.jlo[o], vl);
   }
 }
 
