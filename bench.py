@@ -208,9 +208,12 @@ def make_workload(name: str, precision: int, cap_factor: float = 1.04):
     return p, las, src, ppc
 
 
-def load_device(name, precision, host_injection=False):
+def load_device(name, precision, host_injection=False, cap_factor=1.04):
+    """The workload on a fresh device handle.  cap_factor sizes the particle
+    capacity over cells x ppc: long runs need headroom, the laser pushes
+    electrons forward while the window keeps injecting fresh columns."""
     from aladyn_b200.sim import PicDevice
-    p, las, src, ppc = make_workload(name, precision)
+    p, las, src, ppc = make_workload(name, precision, cap_factor)
     dev = PicDevice(p)
     dev.init_laser(las)
     if host_injection:
