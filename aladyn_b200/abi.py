@@ -158,11 +158,15 @@ SIGNATURES = {
     "agpu_beam_inject": (C.c_int, [_P, C.c_int32, _D, C.c_int64, C.c_int64, C.c_int32, C.c_double]),
     "agpu_beam_potential": (C.c_int, [_P, _D, _D, C.c_double]),
     "agpu_set_deferred_counts": (C.c_int, [_P, C.c_int32]),
+    "agpu_set_step_graphs": (C.c_int, [_P, C.c_int32]),
     "agpu_batch_create": (C.c_int, [_P, C.c_int32, C.POINTER(_P)]),
     "agpu_batch_destroy": (C.c_int, [_P]),
     "agpu_batch_size": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "agpu_batch_handle": (C.c_int, [_P, C.c_int32, C.POINTER(_P)]),
     "agpu_batch_run": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    "agpu_batch_set_graphs": (C.c_int, [_P, C.c_int32]),
+    "agpu_batch_set_multi": (C.c_int, [_P, C.c_int32]),
+    "agpu_batch_launches": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "agpu_batch_clock": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "agpu_diag": (C.c_int, [_P, C.POINTER(AgpuDiagOut)]),
     "agpu_set_profiling": (C.c_int, [_P, C.c_int32]),

@@ -16,6 +16,7 @@
 #include "agpu_bin.cuh"
 #include "agpu_ionz.h"
 #include "agpu_kernels.h"
+#include "agpu_multi.h"
 #include "agpu_tile.h"
 #include "agpu_util.h"
 
@@ -103,6 +104,12 @@ struct agpu_handle {
   // on the device; refresh_counts reads them at the next synchronisation
   bool defer = false;
   bool stale[4] = {false, false, false, false};
+  // step graph (deferred mode): the launches of a step between window
+  // shifts, captured once and replayed while the signature holds
+  bool use_graph = false;
+  cudaGraphExec_t gexec = nullptr;
+  unsigned char gsig[160] = {};
+  long long g_launches = 0, g_push = 0, g_yee = 0, g_cells = 0;
   // flags
   bool fields_set = false;
   bool deterministic = false;
@@ -203,6 +210,7 @@ int free_all(agpu_handle* h) {
   cudaFree(h->cursor);
   for (int i = 0; i < 2 * PH_N; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->st) cudaStreamDestroy(h->st);
   return 0;
 }
@@ -1116,7 +1124,248 @@ int agpu_set_ionization_species(agpu_handle* h, int32_t ic, int32_t atomic_numbe
   return upload_table(h, ic, tab.data(), atomic_number);
 }
 
+static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu_step_out* out);
+
+// What a captured step's launches depend on: particle counts and array
+// pointers (compactions swap buffers), binning state and the box.
+static void step_signature(const agpu_handle* h, unsigned char* sig) {
+  struct Sig {
+    long long np[4];
+    const void* ptr[4];
+    int binned[4];
+    double box[7];
+    int det, nsp_run;
+  } g;
+  std::memset(&g, 0, sizeof(g));
+  for (int ic = 0; ic < 4; ++ic) {
+    g.np[ic] = h->np[ic];
+    g.ptr[ic] = h->fp32 ? (const void*)h->sp[ic].cell : (const void*)h->part[ic];
+    g.binned[ic] = h->binned[ic] ? 1 : 0;
+  }
+  const agpu_params& p = h->p;
+  const double box[7] = {p.xmn, p.gxmin, p.gxmax, p.gymin, p.gymax, p.gzmin, p.gzmax};
+  std::memcpy(g.box, box, sizeof(box));
+  g.det = h->deterministic ? 1 : 0;
+  g.nsp_run = p.nsp_run;
+  static_assert(sizeof(Sig) <= sizeof(h->gsig), "signature buffer");
+  std::memset(sig, 0, sizeof(h->gsig));
+  std::memcpy(sig, &g, sizeof(g));
+}
+
 int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu_step_out* out) {
+  if (!h) return AGPU_E_ARG;
+  const agpu_params& p = h->p;
+  bool plain = h->use_graph && h->defer && !initial_time && p.ionz_lev == 0 && !h->profiling && !h->deterministic;
+  if (plain && p.w_speed > 0.0 && p.w_sh > 0 && t >= p.wi_time && t < p.wf_time && iter % p.w_sh == 0) plain = false;
+  for (int ic = 0; ic < p.nsp_run && plain; ++ic)
+    if (h->np[ic] > 0 && !(h->binned[ic] && h->key[ic])) plain = false;
+  if (!plain) return step_impl(h, iter, t, initial_time, out);
+  agpu_step_out dummy;
+  if (!out) out = &dummy;
+  unsigned char sig[sizeof(h->gsig)];
+  step_signature(h, sig);
+  if (!h->gexec || std::memcmp(sig, h->gsig, sizeof(sig)) != 0) {
+    // capture this step's launches into a graph (nothing runs yet)
+    const agpu_timers before = h->timers;
+    cudaGraph_t gr = nullptr;
+    CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    int rc = step_impl(h, iter, t, initial_time, out);
+    cudaError_t ec = cudaStreamEndCapture(h->st, &gr);
+    if (rc || ec != cudaSuccess || !gr) {
+      if (gr) cudaGraphDestroy(gr);
+      cudaGetLastError();
+      h->timers = before;
+      if (rc) return rc;
+      h->use_graph = false;  // capture refused: plain launches from here on
+      return step_impl(h, iter, t, initial_time, out);
+    }
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    h->gexec = nullptr;
+    cudaError_t ei = cudaGraphInstantiate(&h->gexec, gr, 0);
+    cudaGraphDestroy(gr);
+    if (ei != cudaSuccess) {
+      cudaGetLastError();
+      h->gexec = nullptr;
+      h->timers = before;
+      h->use_graph = false;
+      return step_impl(h, iter, t, initial_time, out);
+    }
+    std::memcpy(h->gsig, sig, sizeof(sig));
+    h->g_launches = h->timers.launches_total - before.launches_total;
+    h->g_push = h->timers.launches_push_deposit - before.launches_push_deposit;
+    h->g_yee = h->timers.launches_yee - before.launches_yee;
+    h->g_cells = h->timers.yee_cells - before.yee_cells;
+    h->timers = before;
+  } else {
+    std::memset(out, 0, sizeof(*out));
+    out->ion_field_max = -1.0;
+    for (int ic = 0; ic < 4; ++ic) out->np[ic] = h->binned[ic] ? h->nalive[ic] : h->np[ic];
+    out->xmn = p.xmn;
+    out->error_bits = h->error_bits;
+  }
+  CK(cudaGraphLaunch(h->gexec, h->st));
+  h->timers.launches_total += h->g_launches;
+  h->timers.launches_push_deposit += h->g_push;
+  h->timers.launches_yee += h->g_yee;
+  h->timers.yee_cells += h->g_cells;
+  return 0;
+}
+
+// ---- multi-instance steps (used by the batch runner) -----------------------
+// A step is "plain" when it is a deferred-count step between window shifts
+// of the split form with one running species, binned, no ionization and no
+// profiling: exactly the launches that one multi-instance step performs.
+int agpu_x_plain(agpu_handle* h, int32_t iter, double t, int32_t initial_time) {
+  if (!h) return 0;
+  const agpu_params& p = h->p;
+  if (!h->fp32 || !h->defer || initial_time || p.ionz_lev > 0 || h->profiling || h->deterministic || p.nsp_run != 1)
+    return 0;
+  if (p.w_speed > 0.0 && p.w_sh > 0 && t >= p.wi_time && t < p.wf_time && iter % p.w_sh == 0) return 0;
+  if (h->np[0] <= 0 || !h->binned[0] || !h->key[0]) return 0;
+  return 1;
+}
+
+struct agpu_x_ws {
+  int maxn = 0;
+  cudaStream_t st = nullptr;
+  MultiInst* d_desc = nullptr;
+  MultiInst* h_desc = nullptr;
+  int* d_off = nullptr;
+  int* h_off = nullptr;
+  long long launches = 0;
+};
+
+int agpu_x_ws_create(int32_t maxn, agpu_x_ws** out) {
+  if (!out || maxn < 1) return AGPU_E_ARG;
+  agpu_x_ws* w = new (std::nothrow) agpu_x_ws();
+  if (!w) return AGPU_E_NOMEM;
+  w->maxn = maxn;
+  int rc = 0;
+  if (cudaStreamCreateWithFlags(&w->st, cudaStreamNonBlocking) != cudaSuccess) rc = AGPU_E_CUDA;
+  if (!rc) rc |= dmalloc((void**)&w->d_desc, sizeof(MultiInst) * maxn);
+  if (!rc) rc |= dmalloc((void**)&w->d_off, sizeof(int) * (maxn + 1));
+  if (!rc && cudaMallocHost((void**)&w->h_desc, sizeof(MultiInst) * maxn) != cudaSuccess) rc = AGPU_E_NOMEM;
+  if (!rc && cudaMallocHost((void**)&w->h_off, sizeof(int) * (maxn + 1)) != cudaSuccess) rc = AGPU_E_NOMEM;
+  if (rc) {
+    cudaGetLastError();
+    cudaFree(w->d_desc);
+    cudaFree(w->d_off);
+    cudaFreeHost(w->h_desc);
+    cudaFreeHost(w->h_off);
+    if (w->st) cudaStreamDestroy(w->st);
+    delete w;
+    return rc;
+  }
+  *out = w;
+  return 0;
+}
+
+int agpu_x_ws_destroy(agpu_x_ws* w) {
+  if (!w) return AGPU_E_ARG;
+  cudaStreamSynchronize(w->st);
+  cudaFree(w->d_desc);
+  cudaFree(w->d_off);
+  cudaFreeHost(w->h_desc);
+  cudaFreeHost(w->h_off);
+  cudaStreamDestroy(w->st);
+  delete w;
+  return 0;
+}
+
+long long agpu_x_ws_launches(const agpu_x_ws* w) { return w ? w->launches : 0; }
+
+// One plain step of n handles (all agpu_x_plain, same ndim, their streams
+// idle) as one launch per phase on the workspace's stream; returns after the
+// step has finished on the GPU.
+int agpu_x_step_many(agpu_handle** hs, int32_t n, agpu_x_ws* w) {
+  if (!hs || !w || n < 1 || n > w->maxn) return AGPU_E_ARG;
+  const int ndim = hs[0]->p.ndim;
+  long long max_cells = 1, max_faces = 1, max_np = 1;
+  int total = 0;
+  for (int i = 0; i < n; ++i) {
+    agpu_handle* h = hs[i];
+    if (h->p.ndim != ndim) return AGPU_E_ARG;
+    const Geo& g = h->g;
+    const agpu_params& p = h->p;
+    MultiInst& m = w->h_desc[i];
+    TileArgs32& a = m.ta;
+    a.g = g;
+    a.t = h->tg;
+    a.ebf = h->ebf32;
+    a.jhi = h->jhi;
+    a.jlo = h->jlo;
+    const Species32& sp = h->sp[0];
+    a.p = Part32{sp.cell, sp.ox, sp.oy, sp.oz, sp.px, sp.py, sp.pz, sp.slot};
+    a.perm = h->perm[0];
+    a.tstart = h->tstart[0];
+    a.key = h->key[0];
+    a.hist = h->hist[0];
+    a.dth = (float)(0.5 * p.dt);
+    a.lfact = (float)p.lorentz_fact[0];
+    a.dtx = (float)(p.dt * p.dx_inv);
+    a.dty = (float)(p.dt * p.dy_inv);
+    a.dtz = (float)(p.dt * p.dz_inv);
+    a.initial = 0;
+    a.err = &h->d_cnt->err;
+    m.ebf = h->ebf32;
+    m.yc = yee_coef(p);
+    m.cursor = h->cursor;
+    m.pushed = &h->d_cnt->pushed;
+    m.removed = &h->d_cnt->removed;
+    m.fmax = &h->d_cnt->fmax;
+    m.np = h->np[0];
+    w->h_off[i] = total;
+    total += h->tg.ntiles;
+    long long cells = (long long)p.nx * p.ny * (ndim == 3 ? p.nz : 1);
+    long long faces = (long long)(p.ny + 3) * (ndim == 3 ? p.nz + 3 : 1) + (long long)(p.nx + 3) * (ndim == 3 ? p.nz + 3 : 1) +
+                      (ndim == 3 ? (long long)(p.nx + 3) * (p.ny + 3) : 0);
+    max_cells = std::max(max_cells, std::max(cells, g.ncell * g.nc));
+    max_faces = std::max(max_faces, faces * g.nf);
+    max_np = std::max(max_np, h->np[0]);
+  }
+  w->h_off[n] = total;
+  auto blocks = [](long long work, int cap) { return (int)std::max(1LL, std::min<long long>((work + 255) / 256, cap)); };
+  MultiPlan pl;
+  pl.n = n;
+  pl.ndim = ndim;
+  pl.total_tiles = total;
+  pl.gx_cells = blocks(max_cells, 64);
+  pl.gx_faces = blocks(max_faces, 16);
+  pl.gx_parts = blocks(max_np, 128);
+  cudaStream_t st = w->st;
+  CK(cudaMemcpyAsync(w->d_desc, w->h_desc, sizeof(MultiInst) * n, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(w->d_off, w->h_off, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
+  int launches = 0;
+  multi_pre32(w->d_desc, pl, st, &launches);
+  multi_field_bd32(w->d_desc, pl, st, &launches);
+  multi_tile32(w->d_desc, w->d_off, pl, st, &launches);
+  multi_bin32(w->d_desc, pl, st, &launches);
+  multi_fields32(w->d_desc, pl, st, &launches);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  w->launches += launches;
+  for (int i = 0; i < n; ++i) {
+    agpu_handle* h = hs[i];
+    h->stale[0] = true;
+    h->timers.launches_push_deposit += 1;
+    h->timers.launches_yee += 1;
+    h->timers.yee_cells += (long long)h->p.nx * h->p.ny * (ndim == 3 ? h->p.nz : 1);
+  }
+  return 0;
+}
+
+int agpu_set_step_graphs(agpu_handle* h, int32_t on) {
+  if (!h) return AGPU_E_ARG;
+  h->use_graph = on != 0;
+  if (!h->use_graph && h->gexec) {
+    cudaStreamSynchronize(h->st);
+    cudaGraphExecDestroy(h->gexec);
+    h->gexec = nullptr;
+  }
+  return 0;
+}
+
+static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu_step_out* out) {
   if (!h) return AGPU_E_ARG;
   agpu_step_out dummy;
   if (!out) out = &dummy;

@@ -6,6 +6,7 @@
 // the push kernel writes, and the records are physically reordered along it
 // whenever the window compaction copies them.
 #include "agpu_bin.cuh"
+#include "agpu_multi.h"
 #include "agpu_util.h"
 #include "agpu_select.cuh"
 
@@ -48,7 +49,7 @@ __global__ void k_keys_abs(const double* x, const double* y, const double* z, lo
 }
 
 // Exclusive scan of hist[0..nb) into start[0..nb], one block.
-__global__ void k_scan_int(const int* hist, int nb, int* start) {
+__device__ void d_scan_int(const int* hist, int nb, int* start) {
   __shared__ long long part[1024];
   int per = (nb + blockDim.x - 1) / blockDim.x;
   int lo = threadIdx.x * per, hi = min(lo + per, nb);
@@ -72,10 +73,12 @@ __global__ void k_scan_int(const int* hist, int nb, int* start) {
     run += hist[b];
   }
 }
+__global__ void k_scan_int(const int* hist, int nb, int* start) { d_scan_int(hist, nb, start); }
 
 // perm[start[key] + rank] = n, ranks from warp-aggregated cursors.
-__global__ void k_perm_scatter(const int* key, long long np, const int* start, int* cursor, int* perm) {
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < np; n += (long long)gridDim.x * blockDim.x) {
+__device__ void d_perm_scatter(const int* key, long long np, const int* start, int* cursor, int* perm, long long bid_,
+                               long long nb_) {
+  for (long long n = bid_ * (long long)blockDim.x + threadIdx.x; n < np; n += nb_ * (long long)blockDim.x) {
     int kk = key[n];
     unsigned int act = __activemask();
     unsigned int peers = __match_any_sync(act, kk);
@@ -87,6 +90,9 @@ __global__ void k_perm_scatter(const int* key, long long np, const int* start, i
     int rank = __popc(peers & ((1u << lane) - 1u));
     perm[start[kk] + base + rank] = (int)n;
   }
+}
+__global__ void k_perm_scatter(const int* key, long long np, const int* start, int* cursor, int* perm) {
+  d_perm_scatter(key, np, start, cursor, perm, blockIdx.x, gridDim.x);
 }
 
 void bin_keys_split(const int* cell, long long np, const Geo& g, const TileGeo& t, int* key, int* hist, unsigned int* err,
@@ -188,6 +194,25 @@ long long perm_compact32(const int* perm, long long nalive, const Part32View& sr
   }
   PermAlive pr{perm, nalive};
   return select_run(pr, mv, nalive, s, st);
+}
+
+
+// ---- multi-instance binning: scan (one block per instance), scatter ------
+namespace {
+__global__ void km_scan(const MultiInst* __restrict__ d) {
+  const MultiInst& m = d[blockIdx.x];
+  d_scan_int(m.ta.hist, m.ta.t.ntiles + 1, const_cast<int*>(m.ta.tstart));
+}
+__global__ void km_scatter(const MultiInst* __restrict__ d) {
+  const MultiInst& m = d[blockIdx.y];
+  d_perm_scatter(m.ta.key, m.np, m.ta.tstart, m.cursor, const_cast<int*>(m.ta.perm), blockIdx.x, gridDim.x);
+}
+}  // namespace
+
+void multi_bin32(const MultiInst* d, const MultiPlan& pl, cudaStream_t st, int* launches) {
+  km_scan<<<pl.n, 1024, 0, st>>>(d);
+  km_scatter<<<dim3(pl.gx_parts, pl.n), 256, 0, st>>>(d);
+  *launches += 2;
 }
 
 }  // namespace agpu

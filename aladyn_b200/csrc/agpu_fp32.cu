@@ -8,6 +8,7 @@
 // old value, the TwoSum rounding error of that add is accumulated into lo.
 #include "agpu_common.cuh"
 #include "agpu_kernels.h"
+#include "agpu_multi.h"
 #include "agpu_yee.cuh"
 
 namespace agpu {
@@ -411,6 +412,110 @@ __global__ void k32_ionize(IonArgs32 a) {
     }
     a.flag[n] = fl;
   }
+}
+
+
+// ---- multi-instance field phases (one row of blocks per instance) ---------
+namespace {
+
+__global__ void km_pre(const MultiInst* __restrict__ d) {
+  const MultiInst& m = d[blockIdx.y];
+  const Geo g = m.ta.g;
+  const long long bid_ = blockIdx.x, nb_ = gridDim.x;
+  const long long nj = g.ncell * g.nc;
+  GRID_STRIDE(q, nj) {
+    m.ta.jhi[q] = 0.f;
+    m.ta.jlo[q] = 0.f;
+  }
+  const int nt = m.ta.t.ntiles;
+  GRID_STRIDE(b, (long long)nt + 1) {
+    m.cursor[b] = 0;
+    if (b == nt) {
+      const int alive = m.ta.tstart[nt];
+      m.ta.hist[b] = (int)(m.np - alive);  // the records already dead
+      *m.pushed += (unsigned long long)alive;
+      *m.removed = 0ull;
+      *m.fmax = 0.0;
+    } else {
+      m.ta.hist[b] = 0;
+    }
+  }
+  d_field_bd_x<float>(m.ebf, g, g.nf, bid_, nb_);
+}
+__global__ void km_bd_y(const MultiInst* __restrict__ d) {
+  const MultiInst& m = d[blockIdx.y];
+  d_field_bd_y<float>(m.ebf, m.ta.g, m.ta.g.nf, blockIdx.x, gridDim.x);
+}
+__global__ void km_bd_z(const MultiInst* __restrict__ d) {
+  const MultiInst& m = d[blockIdx.y];
+  d_field_bd_z<float>(m.ebf, m.ta.g, m.ta.g.nf, blockIdx.x, gridDim.x);
+}
+__global__ void km_fold_x(const MultiInst* __restrict__ d) {
+  const MultiInst& m = d[blockIdx.y];
+  d_jfold_x<float>(m.ta.jhi, m.ta.g, blockIdx.x, gridDim.x);
+  d_jfold_x<float>(m.ta.jlo, m.ta.g, blockIdx.x, gridDim.x);
+}
+__global__ void km_fold_y(const MultiInst* __restrict__ d) {
+  const MultiInst& m = d[blockIdx.y];
+  d_jfold_y<float>(m.ta.jhi, m.ta.g, blockIdx.x, gridDim.x);
+  d_jfold_y<float>(m.ta.jlo, m.ta.g, blockIdx.x, gridDim.x);
+}
+__global__ void km_fold_z(const MultiInst* __restrict__ d) {
+  const MultiInst& m = d[blockIdx.y];
+  d_jfold_z<float>(m.ta.jhi, m.ta.g, blockIdx.x, gridDim.x);
+  d_jfold_z<float>(m.ta.jlo, m.ta.g, blockIdx.x, gridDim.x);
+}
+__global__ void km_ef_bds(const MultiInst* __restrict__ d, int full_dt) {
+  const MultiInst& m = d[blockIdx.y];
+  d_ef_bds<float>(m.ebf, m.ta.g, m.yc, full_dt ? m.yc.dt : 0.0, blockIdx.x, gridDim.x);
+}
+__global__ void km_bf_bds(const MultiInst* __restrict__ d) {
+  const MultiInst& m = d[blockIdx.y];
+  d_bf_bds<float>(m.ebf, m.ta.g, m.yc, m.yc.dt, blockIdx.x, gridDim.x);
+}
+template <int NDIM>
+__global__ void __launch_bounds__(256) km_rote(const MultiInst* __restrict__ d) {
+  const MultiInst& m = d[blockIdx.y];
+  d_rote<float, NDIM>(m.ebf, m.ta.g, m.yc, 0.5 * m.yc.dt, blockIdx.x, gridDim.x);
+}
+template <int NDIM>
+__global__ void __launch_bounds__(256) km_rotb_j(const MultiInst* __restrict__ d) {
+  const MultiInst& m = d[blockIdx.y];
+  d_rotb_j<float, NDIM>(m.ebf, m.ta.jhi, m.ta.jlo, m.ta.g, m.yc, m.yc.dt, blockIdx.x, gridDim.x);
+}
+
+}  // namespace
+
+void multi_pre32(const MultiInst* d, const MultiPlan& pl, cudaStream_t st, int* launches) {
+  km_pre<<<dim3(pl.gx_cells, pl.n), 256, 0, st>>>(d);
+  *launches += 1;
+}
+void multi_field_bd32(const MultiInst* d, const MultiPlan& pl, cudaStream_t st, int* launches) {
+  km_bd_y<<<dim3(pl.gx_faces, pl.n), 256, 0, st>>>(d);
+  *launches += 1;
+  if (pl.ndim == 3) {
+    km_bd_z<<<dim3(pl.gx_faces, pl.n), 256, 0, st>>>(d);
+    *launches += 1;
+  }
+}
+// the order of yee_t (curr_and_fields_util.f90:176-260): ef_bds(0), rote(dt/2),
+// bf_bds(dt), rotb + current(dt), ef_bds(dt), rote(dt/2)
+void multi_fields32(const MultiInst* d, const MultiPlan& pl, cudaStream_t st, int* launches) {
+  km_fold_x<<<dim3(pl.gx_faces, pl.n), 256, 0, st>>>(d);
+  km_fold_y<<<dim3(pl.gx_faces, pl.n), 256, 0, st>>>(d);
+  *launches += 2;
+  if (pl.ndim == 3) {
+    km_fold_z<<<dim3(pl.gx_faces, pl.n), 256, 0, st>>>(d);
+    *launches += 1;
+  }
+  const dim3 gf(pl.gx_faces, pl.n), gc(pl.gx_cells, pl.n);
+  km_ef_bds<<<gf, 256, 0, st>>>(d, 0);
+  if (pl.ndim == 3) km_rote<3><<<gc, 256, 0, st>>>(d); else km_rote<2><<<gc, 256, 0, st>>>(d);
+  km_bf_bds<<<gf, 256, 0, st>>>(d);
+  if (pl.ndim == 3) km_rotb_j<3><<<gc, 256, 0, st>>>(d); else km_rotb_j<2><<<gc, 256, 0, st>>>(d);
+  km_ef_bds<<<gf, 256, 0, st>>>(d, 1);
+  if (pl.ndim == 3) km_rote<3><<<gc, 256, 0, st>>>(d); else km_rote<2><<<gc, 256, 0, st>>>(d);
+  *launches += 6;
 }
 
 }  // namespace agpu

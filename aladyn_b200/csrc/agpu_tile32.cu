@@ -21,6 +21,7 @@
 //   5. writes each particle's new tile key and the next histogram.
 #include "agpu_bin.cuh"
 #include "agpu_common.cuh"
+#include "agpu_multi.h"
 #include "agpu_tile.h"
 
 namespace agpu {
@@ -71,7 +72,7 @@ __device__ __forceinline__ bool inside(int node, float o, int n) {
 }  // namespace
 
 template <int NDIM, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
+__device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
   constexpr int FX = TX + 2, FY = TY + 2, FZ = (NDIM == 3) ? TZ + 2 : 1;
   constexpr int JX = TX + 4, JY = TY + 4, JZ = (NDIM == 3) ? TZ + 4 : 1;
   constexpr int FV = FX * FY * FZ, JV = JX * JY * JZ;
@@ -82,7 +83,6 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
   __shared__ unsigned int s_wmax;
 
   const Geo g = a.g;
-  const int t = blockIdx.x;
   const int beg = a.tstart[t], end = a.tstart[t + 1];
   if (beg >= end) return;
   const int tx = t % a.t.ntx, ty = (t / a.t.ntx) % a.t.nty, tz = t / (a.t.ntx * a.t.nty);
@@ -359,6 +359,25 @@ __global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
   }
 }
 
+template <int NDIM, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(256, 4) k32_tile(TileArgs32 a) {
+  d32_tile<NDIM, TX, TY, TZ>(a, blockIdx.x);
+}
+
+// One block per tile of any instance: instance i owns the global tiles
+// [tile_off[i], tile_off[i+1]).
+template <int NDIM, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(256, 4) km32_tile(const MultiInst* __restrict__ d, const int* __restrict__ tile_off,
+                                                    int n) {
+  const int b = blockIdx.x;
+  int lo = 0, hi = n;  // tile_off[lo] <= b < tile_off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(&tile_off[mid]) <= b) lo = mid; else hi = mid;
+  }
+  d32_tile<NDIM, TX, TY, TZ>(d[lo].ta, b - __ldg(&tile_off[lo]));
+}
+
 size_t tile32_smem(int ndim, int tx, int ty, int tz) {
   if (ndim == 3) return sizeof(float) * (6 * (tx + 2) * (ty + 2) * (tz + 2) + 3 * (tx + 4) * (ty + 4) * (tz + 4));
   return sizeof(float) * (3 * (tx + 2) * (ty + 2) + 2 * (tx + 4) * (ty + 4));
@@ -377,6 +396,22 @@ void tile_push32(const TileArgs32& a, cudaStream_t st) {
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k<<<a.t.ntiles, 256, sm, st>>>(a);
   }
+}
+
+void multi_tile32(const MultiInst* d, const int* tile_off, const MultiPlan& pl, cudaStream_t st, int* launches) {
+  if (pl.total_tiles <= 0) return;
+  if (pl.ndim == 3) {
+    size_t sm = tile32_smem(3, TILE3_X, TILE3_Y, TILE3_Z);
+    auto k = km32_tile<3, TILE3_X, TILE3_Y, TILE3_Z>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k<<<pl.total_tiles, 256, sm, st>>>(d, tile_off, pl.n);
+  } else {
+    size_t sm = tile32_smem(2, TILE2_X, TILE2_Y, 1);
+    auto k = km32_tile<2, TILE2_X, TILE2_Y, 1>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k<<<pl.total_tiles, 256, sm, st>>>(d, tile_off, pl.n);
+  }
+  *launches += 1;
 }
 
 }  // namespace agpu

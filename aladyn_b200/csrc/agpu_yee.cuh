@@ -9,12 +9,16 @@
 
 namespace agpu {
 
+// Every kernel body is a device function over "its" blocks bid_ of nb_, so
+// that the same body runs as a single-instance kernel (bid_ = blockIdx.x) or
+// inside a kernel that serves many instances at once (one row of blocks per
+// instance).
 #define GRID_STRIDE(t, total) \
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (total); t += (long long)gridDim.x * blockDim.x)
+  for (long long t = bid_ * (long long)blockDim.x + threadIdx.x; t < (total); t += nb_ * (long long)blockDim.x)
 
 // ---- A1: field_xyzbd (src/parallel/mpi_field_interface.f90:53-198) --------
 template <typename T>
-__global__ void k_field_bd_x(T* ebf, Geo g, int nc) {
+__device__ __forceinline__ void d_field_bd_x(T* ebf, Geo g, int nc, long long bid_, long long nb_) {
   int ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
   long long total = (long long)ny * nz * nc;
   GRID_STRIDE(t, total) {
@@ -27,7 +31,11 @@ __global__ void k_field_bd_x(T* ebf, Geo g, int nc) {
   }
 }
 template <typename T>
-__global__ void k_field_bd_y(T* ebf, Geo g, int nc) {
+__global__ void k_field_bd_x(T* ebf, Geo g, int nc) {
+  d_field_bd_x<T>(ebf, g, nc, blockIdx.x, gridDim.x);
+}
+template <typename T>
+__device__ __forceinline__ void d_field_bd_y(T* ebf, Geo g, int nc, long long bid_, long long nb_) {
   int nxe = g.ix2 - g.ix1 + 3, nz = g.kz2 - g.kz1 + 1;
   long long total = (long long)nxe * nz * nc;
   GRID_STRIDE(t, total) {
@@ -40,7 +48,11 @@ __global__ void k_field_bd_y(T* ebf, Geo g, int nc) {
   }
 }
 template <typename T>
-__global__ void k_field_bd_z(T* ebf, Geo g, int nc) {
+__global__ void k_field_bd_y(T* ebf, Geo g, int nc) {
+  d_field_bd_y<T>(ebf, g, nc, blockIdx.x, gridDim.x);
+}
+template <typename T>
+__device__ __forceinline__ void d_field_bd_z(T* ebf, Geo g, int nc, long long bid_, long long nb_) {
   int nxe = g.ix2 - g.ix1 + 3, nye = g.jy2 - g.jy1 + 3;
   long long total = (long long)nxe * nye * nc;
   GRID_STRIDE(t, total) {
@@ -53,6 +65,10 @@ __global__ void k_field_bd_z(T* ebf, Geo g, int nc) {
   }
 }
 template <typename T>
+__global__ void k_field_bd_z(T* ebf, Geo g, int nc) {
+  d_field_bd_z<T>(ebf, g, nc, blockIdx.x, gridDim.x);
+}
+template <typename T>
 void field_bd_t(T* ebf, const Geo& g, cudaStream_t st, int sms) {
   int nc = g.nf;
   k_field_bd_x<T><<<grid_for((long long)(g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1) * nc, 256, sms), 256, 0, st>>>(ebf, g, nc);
@@ -63,7 +79,7 @@ void field_bd_t(T* ebf, const Geo& g, cudaStream_t st, int sms) {
 
 // ---- A13: jc_xyzbd (src/parallel/mpi_curr_interface.f90:551-643) ----------
 template <typename T>
-__global__ void k_jfold_x(T* jc, Geo g) {
+__device__ __forceinline__ void d_jfold_x(T* jc, Geo g, long long bid_, long long nb_) {
   int ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
   long long total = (long long)ny * nz * g.nc;
   GRID_STRIDE(t, total) {
@@ -81,7 +97,11 @@ __global__ void k_jfold_x(T* jc, Geo g) {
   }
 }
 template <typename T>
-__global__ void k_jfold_y(T* jc, Geo g) {
+__global__ void k_jfold_x(T* jc, Geo g) {
+  d_jfold_x<T>(jc, g, blockIdx.x, gridDim.x);
+}
+template <typename T>
+__device__ __forceinline__ void d_jfold_y(T* jc, Geo g, long long bid_, long long nb_) {
   int nx = g.ix2 - g.ix1 + 1, nz = g.kz2 - g.kz1 + 1;
   long long total = (long long)nx * nz * g.nc;
   long long sy = g.n1p;
@@ -101,7 +121,11 @@ __global__ void k_jfold_y(T* jc, Geo g) {
   }
 }
 template <typename T>
-__global__ void k_jfold_z(T* jc, Geo g) {
+__global__ void k_jfold_y(T* jc, Geo g) {
+  d_jfold_y<T>(jc, g, blockIdx.x, gridDim.x);
+}
+template <typename T>
+__device__ __forceinline__ void d_jfold_z(T* jc, Geo g, long long bid_, long long nb_) {
   int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1;
   long long total = (long long)nx * ny * g.nc;
   long long sz = (long long)g.n1p * g.n2p;
@@ -120,6 +144,10 @@ __global__ void k_jfold_z(T* jc, Geo g) {
   }
 }
 template <typename T>
+__global__ void k_jfold_z(T* jc, Geo g) {
+  d_jfold_z<T>(jc, g, blockIdx.x, gridDim.x);
+}
+template <typename T>
 void jfold_t(T* jc, const Geo& g, cudaStream_t st, int sms) {
   k_jfold_x<T><<<grid_for((long long)(g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1) * g.nc, 256, sms), 256, 0, st>>>(jc, g);
   k_jfold_y<T><<<grid_for((long long)(g.ix2 - g.ix1 + 1) * (g.kz2 - g.kz1 + 1) * g.nc, 256, sms), 256, 0, st>>>(jc, g);
@@ -131,7 +159,7 @@ void jfold_t(T* jc, const Geo& g, cudaStream_t st, int sms) {
 
 // ef_bds (src/fields/grid_fields.f90:1204-1354): right-face Mur boundary of E.
 template <typename T>
-__global__ void k_ef_bds(T* ebf, Geo g, YeeC c, double dtl) {
+__device__ __forceinline__ void d_ef_bds(T* ebf, Geo g, YeeC c, double dtl, long long bid_, long long nb_) {
   int ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1, nx = g.ix2 - g.ix1 + 1;
   long long nfx = (long long)ny * nz, nfy = (long long)nx * nz, nfz = (g.ndim == 3) ? (long long)nx * ny : 0;
   int nf = g.nf;
@@ -166,9 +194,13 @@ __global__ void k_ef_bds(T* ebf, Geo g, YeeC c, double dtl) {
     }
   }
 }
+template <typename T>
+__global__ void k_ef_bds(T* ebf, Geo g, YeeC c, double dtl) {
+  d_ef_bds<T>(ebf, g, c, dtl, blockIdx.x, gridDim.x);
+}
 // bf_bds (src/fields/grid_fields.f90:1069-1202): left-face Mur boundary of B.
 template <typename T>
-__global__ void k_bf_bds(T* ebf, Geo g, YeeC c, double dtl) {
+__device__ __forceinline__ void d_bf_bds(T* ebf, Geo g, YeeC c, double dtl, long long bid_, long long nb_) {
   int ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1, nx = g.ix2 - g.ix1 + 1;
   long long nfx = (long long)ny * nz, nfy = (long long)nx * nz, nfz = (g.ndim == 3) ? (long long)nx * ny : 0;
   int nf = g.nf;
@@ -209,10 +241,14 @@ __global__ void k_bf_bds(T* ebf, Geo g, YeeC c, double dtl) {
     }
   }
 }
+template <typename T>
+__global__ void k_bf_bds(T* ebf, Geo g, YeeC c, double dtl) {
+  d_bf_bds<T>(ebf, g, c, dtl, blockIdx.x, gridDim.x);
+}
 
 // rote (grid_fields.f90:1405-1478): B -= dtf curl E, interior.
 template <typename T, int NDIM>
-__global__ void __launch_bounds__(256) k_rote(T* ebf, Geo g, YeeC c, double dtf) {
+__device__ __forceinline__ void d_rote(T* ebf, Geo g, YeeC c, double dtf, long long bid_, long long nb_) {
   int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
   long long total = (long long)nx * ny * nz;
   double aphxd = dtf * c.dx_inv, aphyd = dtf * c.dy_inv, aphzd = dtf * c.dz_inv;
@@ -240,12 +276,16 @@ __global__ void __launch_bounds__(256) k_rote(T* ebf, Geo g, YeeC c, double dtf)
     }
   }
 }
+template <typename T, int NDIM>
+__global__ void __launch_bounds__(256) k_rote(T* ebf, Geo g, YeeC c, double dtf) {
+  d_rote<T, NDIM>(ebf, g, c, dtf, blockIdx.x, gridDim.x);
+}
 
 // rotb (grid_fields.f90:1480-1552) + E -= ompe * (djc * J)
 // (curr_and_fields_util.f90:111-115, 227-231).  jlo (optional) holds the
 // compensation term of a two-float current.
 template <typename T, int NDIM>
-__global__ void __launch_bounds__(256) k_rotb_j(T* ebf, const T* jc, const T* jlo, Geo g, YeeC c, double dtf) {
+__device__ __forceinline__ void d_rotb_j(T* ebf, const T* jc, const T* jlo, Geo g, YeeC c, double dtf, long long bid_, long long nb_) {
   int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
   long long total = (long long)nx * ny * nz;
   double aphxd = dtf * c.dx_inv, aphyd = dtf * c.dy_inv, aphzd = dtf * c.dz_inv;
@@ -288,6 +328,10 @@ __global__ void __launch_bounds__(256) k_rotb_j(T* ebf, const T* jc, const T* jl
       E3[o] = ez - ompe * (djc3 * j3);
     }
   }
+}
+template <typename T, int NDIM>
+__global__ void __launch_bounds__(256) k_rotb_j(T* ebf, const T* jc, const T* jlo, Geo g, YeeC c, double dtf) {
+  d_rotb_j<T, NDIM>(ebf, jc, jlo, g, c, dtf, blockIdx.x, gridDim.x);
 }
 
 template <typename T>

@@ -210,6 +210,9 @@ class PicDevice:
     def set_deferred_counts(self, on: bool = True):
         check(self.lib.agpu_set_deferred_counts(self.h, 1 if on else 0), "agpu_set_deferred_counts")
 
+    def set_step_graphs(self, on: bool = True):
+        check(self.lib.agpu_set_step_graphs(self.h, 1 if on else 0), "agpu_set_step_graphs")
+
 
 class PicBatch:
     """N independent simulations on one GPU (a parameter scan), advanced
@@ -236,6 +239,17 @@ class PicBatch:
         st = (C.c_int32 * len(self))()
         self.lib.agpu_batch_run(self.b, nsteps, nthreads, st)
         return list(st)
+
+    def set_graphs(self, on: bool = True):
+        check(self.lib.agpu_batch_set_graphs(self.b, 1 if on else 0), "agpu_batch_set_graphs")
+
+    def set_multi(self, on: bool = True):
+        check(self.lib.agpu_batch_set_multi(self.b, 1 if on else 0), "agpu_batch_set_multi")
+
+    def launches(self) -> int:
+        n = C.c_int64()
+        check(self.lib.agpu_batch_launches(self.b, C.byref(n)), "agpu_batch_launches")
+        return n.value
 
     def clock(self, i: int):
         it, t = C.c_int32(), C.c_double()

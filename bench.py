@@ -430,6 +430,8 @@ def bench_scan(a, torch):
     from aladyn_b200.sim import PicBatch, PicDevice
     n = 256
     cases = scan_instances(n, AGPU_FP32_SPLIT)
+    for p, _, _ in cases:  # headroom: the lasers push electrons forward as the window injects
+        p.capacity[0] = int(p.capacity[0] * 1.5)
 
     def setup(d, las, src):
         d.init_laser(las)
@@ -450,6 +452,7 @@ def bench_scan(a, torch):
     assert st == [0] * n, st
     for d in batch.instances:
         d.reset_timers()
+    launches0 = batch.launches()
     torch.cuda.synchronize()
     e0, e1 = ev(), ev()
     e0.record()
@@ -460,7 +463,7 @@ def bench_scan(a, torch):
     assert st == [0] * n, st
     tms = [d.timers() for d in batch.instances]
     pushes_b = sum(t.pushes for t in tms)
-    launches_b = sum(t.launches_total for t in tms)
+    launches_b = sum(t.launches_total for t in tms) + batch.launches() - launches0
     batch.close()
     # sequential arm: one instance at a time through the single-instance path
     ms_s, pushes_s = 0.0, 0

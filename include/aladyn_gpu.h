@@ -280,6 +280,18 @@ int agpu_batch_destroy(agpu_batch* b);
 int agpu_batch_size(const agpu_batch* b, int32_t* n);
 int agpu_batch_handle(agpu_batch* b, int32_t i, agpu_handle** h);
 int agpu_batch_run(agpu_batch* b, int32_t nsteps, int32_t nthreads, int32_t* status);
+/* Multi-instance steps (on by default): the steps between window shifts of
+ * all instances of the split form with one running species run as one
+ * kernel per phase over every instance together (about 15 launches per batch
+ * step whatever N); first steps, window shifts and other instances step one
+ * by one on worker threads.  With it off, each worker steps its instances on
+ * their own streams, from per-instance step graphs when
+ * agpu_batch_set_graphs is on (the default). */
+int agpu_batch_set_multi(agpu_batch* b, int32_t on);
+int agpu_batch_set_graphs(agpu_batch* b, int32_t on);
+/* Kernel launches issued by the multi-instance steps so far (the per-instance
+ * launches are in each instance's agpu_timers). */
+int agpu_batch_launches(const agpu_batch* b, int64_t* n);
 /* The step counter and time of instance i after the steps run so far. */
 int agpu_batch_clock(const agpu_batch* b, int32_t i, int32_t* iter, double* t);
 
@@ -326,6 +338,14 @@ int agpu_set_deterministic(agpu_handle* h, int32_t on);
  * .removed is not filled.  Off by default (the reference's lp_run reports
  * the counts every step). */
 int agpu_set_deferred_counts(agpu_handle* h, int32_t on);
+/* Step graphs (on != 0, effective in deferred-count mode): a step between
+ * window shifts (not the first step, no ionization, profiling off, every
+ * running species binned) is captured once as a CUDA graph and replayed as
+ * one graph launch while the particle counts, buffers and box stay the same;
+ * the next window shift or any change of the species makes the following
+ * plain step capture again.  Saves the per-kernel launch cost of small
+ * grids; the work done is the same. */
+int agpu_set_step_graphs(agpu_handle* h, int32_t on);
 /* Sort interval in steps for the tile sort (0 = never). */
 int agpu_set_sort_interval(agpu_handle* h, int32_t steps);
 /* sizeof of agpu_params, agpu_plasma, agpu_laser, agpu_step_out,

@@ -1,13 +1,16 @@
 """Batched instances (agpu_batch_*) and the deferred-count mode.
 
-* Deferred counts: one instance stepped with the per-step host
+* Deferred counts (with and without CUDA-graph replay of the steps between
+  window shifts): one instance stepped with the per-step host
   synchronisation and a copy stepped in deferred mode agree (FP64 form,
   25 steps across two window shifts): particle counts equal, fields within
   1e-9 (only the atomic summation order of the deposit differs).
 * A batch of 2D instances of different sizes, lasers and densities advanced
-  by agpu_batch_run against the same instances run one after the other
-  through agpu_step: counts and pushes equal, fields within 1e-9 (FP64) or
-  1e-4 relative L2 (FP32 split, where atomic order changes the roundings).
+  by agpu_batch_run (multi-instance steps between window shifts, or every
+  instance on its own stream) against the same instances run one after the
+  other through agpu_step: counts and pushes equal, fields within 1e-9
+  (FP64) or 1e-4 relative L2 (FP32 split, where atomic order changes the
+  roundings).
 """
 import math
 
@@ -45,11 +48,12 @@ def _setup(dev, las, src):
     dev.load_plasma(0)
 
 
-def _run_sync(p, las, src, steps, deferred=False):
+def _run_sync(p, las, src, steps, deferred=False, graphs=False):
     dev = PicDevice(p)
     _setup(dev, las, src)
     if deferred:
         dev.set_deferred_counts(True)
+        dev.set_step_graphs(graphs)
     t = 0.0
     for it in range(steps):
         dev.lp_run(t, it, initial_time=(it == 0))
@@ -62,24 +66,32 @@ def _rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-def test_deferred_counts_match_synchronous_steps():
+@pytest.mark.parametrize("graphs", [False, True])
+def test_deferred_counts_match_synchronous_steps(graphs):
+    """Deferred counts, with or without the step graphs replaying the steps
+    between window shifts, against per-step synchronous steps."""
     p, las, src = scan_instance(2, AGPU_FP64)
     a = _run_sync(p, las, src, 25)
-    b = _run_sync(p, las, src, 25, deferred=True)
+    b = _run_sync(p, las, src, 25, deferred=True, graphs=graphs)
     assert a.count(0) == b.count(0) > 0
     assert a.timers().pushes == b.timers().pushes
     assert _rel(b.get_fields(), a.get_fields()) < 1e-9
 
 
-@pytest.mark.parametrize("precision", [AGPU_FP64, AGPU_FP32_SPLIT])
-def test_batch_matches_sequential_instances(precision):
+@pytest.mark.parametrize("precision,multi", [(AGPU_FP64, True), (AGPU_FP32_SPLIT, True), (AGPU_FP32_SPLIT, False)])
+def test_batch_matches_sequential_instances(precision, multi):
+    """multi: the steps between window shifts run as one multi-instance step
+    (split form; FP64 instances step one by one either way)."""
     n, steps = 6, 25
     cases = [scan_instance(i, precision) for i in range(n)]
     batch = PicBatch([c[0] for c in cases])
+    batch.set_multi(multi)
     for d, (p, las, src) in zip(batch.instances, cases):
         _setup(d, las, src)
     status = batch.run(steps, nthreads=3)
     assert status == [0] * n
+    if multi and precision == AGPU_FP32_SPLIT:
+        assert batch.launches() > 0  # the multi-instance path ran
     for i, (p, las, src) in enumerate(cases):
         it, t = batch.clock(i)
         assert it == steps and abs(t - steps * p.dt) < 1e-9
