@@ -27,6 +27,9 @@ AGPU_E_STATE = 109
 AGPU_FP64 = 0
 AGPU_FP32_SPLIT = 1
 
+AGPU_SHAPE_QUADRATIC = 0
+AGPU_SHAPE_CUBIC = 1
+
 AGPU_EBIT_INDEX = 1
 AGPU_EBIT_IONZ_INDEX = 2
 AGPU_EBIT_NONFINITE = 4
@@ -47,7 +50,8 @@ class AgpuParams(C.Structure):
         ("w_sh", C.c_int32),
         ("ionz_lev", C.c_int32),
         ("n_mol_atoms", C.c_int32 * 4),
-        ("reserved_i", C.c_int32 * 4),
+        ("shape", C.c_int32),
+        ("reserved_i", C.c_int32 * 3),
         ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
         ("dx_inv", C.c_double), ("dy_inv", C.c_double), ("dz_inv", C.c_double),
         ("dt", C.c_double),

@@ -33,6 +33,7 @@ UNITS = [
     ("agpu_fp32.cu", ["-fmad=true"]),
     ("agpu_tile64.cu", ["-fmad=false"]),
     ("agpu_tile32.cu", ["-fmad=true"]),
+    ("agpu_tile32c.cu", ["-fmad=true"]),
     ("agpu_bin.cu", ["-fmad=false"]),
     ("agpu_noalloc.cu", ["-fmad=false"]),
     ("agpu_beam.cu", ["-fmad=false"]),

@@ -50,7 +50,7 @@ def make_params(grid: Grid, *, precision: int = AGPU_FP64, nsp: int = 1, nsp_run
                 w_sh: int = 10, w_speed: float = 1.0, wi_time: float = 0.0,
                 wf_time: float = 1.0e9, capacity=(0, 0, 0, 0), der_ord: int = 2,
                 mass_number=(1.0, 1.0, 1.0), ionz_lev: int = 0, n_mol_atoms=(1, 1, 1, 1),
-                seed: int = 12345) -> AgpuParams:
+                seed: int = 12345, shape: int = 0) -> AgpuParams:
     p = AgpuParams()
     ndim = grid.ndim
     p.ndim = ndim
@@ -65,6 +65,7 @@ def make_params(grid: Grid, *, precision: int = AGPU_FP64, nsp: int = 1, nsp_run
     p.nsp_run = nsp_run
     p.w_sh = w_sh
     p.ionz_lev = ionz_lev
+    p.shape = shape  # 0: the reference's quadratic/linear shapes, 1: cubic extension
     for i in range(4):
         p.n_mol_atoms[i] = n_mol_atoms[i]
     # set_grid (set_grid_param.f90:52-226), uniform axes

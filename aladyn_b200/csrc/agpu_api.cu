@@ -369,7 +369,12 @@ int compact_species(agpu_handle* h, int ic, bool window) {
 }
 
 // ---- binning of the running species ---------------------------------------
-bool tiled(const agpu_handle* h, int ic) { return !h->deterministic && ic < h->p.nsp_run && h->key[ic] != nullptr; }
+// The FP64 tile kernel has the reference's quadratic shapes only; the cubic
+// FP64 form runs the per-particle kernels.
+bool tiled(const agpu_handle* h, int ic) {
+  return !h->deterministic && ic < h->p.nsp_run && h->key[ic] != nullptr &&
+         (h->fp32 || h->p.shape == AGPU_SHAPE_QUADRATIC);
+}
 
 // Keys from the current positions, histogram, scan and permutation.
 int rebin(agpu_handle* h, int ic) {
@@ -449,7 +454,10 @@ int tiled_push(agpu_handle* h, int ic, int initial_time, agpu_step_out* out) {
     a.dtz = (float)(p.dt * p.dz_inv);
     a.initial = initial_time ? 1 : 0;
     a.err = &h->d_cnt->err;
-    tile_push32(a, h->st);
+    if (p.shape == AGPU_SHAPE_CUBIC)
+      tile_push32_cubic(a, h->st);
+    else
+      tile_push32(a, h->st);
   } else {
     TileArgs64 a;
     a.g = h->g;
@@ -799,6 +807,7 @@ int agpu_create(const agpu_params* params, agpu_handle** out) {
   if (p.ibx != 0 || p.iby != 0 || p.ibz != 0 || p.iform < 0 || p.iform > 1) return AGPU_E_ARG;
   if (p.nsp < 1 || p.nsp > 4 || p.nsp_run < 1 || p.nsp_run > p.nsp) return AGPU_E_ARG;
   if (p.precision != AGPU_FP64 && p.precision != AGPU_FP32_SPLIT) return AGPU_E_ARG;
+  if (p.shape != AGPU_SHAPE_QUADRATIC && p.shape != AGPU_SHAPE_CUBIC) return AGPU_E_ARG;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
     cudaGetLastError();
@@ -1218,7 +1227,8 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu
 int agpu_x_plain(agpu_handle* h, int32_t iter, double t, int32_t initial_time) {
   if (!h) return 0;
   const agpu_params& p = h->p;
-  if (!h->fp32 || !h->defer || initial_time || p.ionz_lev > 0 || h->profiling || h->deterministic || p.nsp_run != 1)
+  if (!h->fp32 || !h->defer || initial_time || p.ionz_lev > 0 || h->profiling || h->deterministic || p.nsp_run != 1 ||
+      p.shape != AGPU_SHAPE_QUADRATIC)
     return 0;
   if (p.w_speed > 0.0 && p.w_sh > 0 && t >= p.wi_time && t < p.wf_time && iter % p.w_sh == 0) return 0;
   if (h->np[0] <= 0 || !h->binned[0] || !h->key[0]) return 0;
@@ -1474,6 +1484,7 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
       a.gzmin = p.gzmin;
       a.gzmax = p.gzmax;
       a.initial = initial_time ? 1 : 0;
+      a.shape = p.shape;
       a.removed = &h->d_cnt->removed;
       a.err = &h->d_cnt->err;
       push_deposit64(a, h->st, h->sms, h->deterministic);
@@ -1753,6 +1764,8 @@ int agpu_set_sort_interval(agpu_handle* h, int32_t steps) {
 }
 int agpu_set_deterministic(agpu_handle* h, int32_t on) {
   if (!h) return AGPU_E_ARG;
+  // the per-particle FP32 kernel has the quadratic shapes only
+  if (on && h->fp32 && h->p.shape == AGPU_SHAPE_CUBIC) return AGPU_E_ARG;
   h->deterministic = on != 0;
   return 0;
 }

@@ -237,6 +237,177 @@ __device__ __forceinline__ bool esirkepov3d(const Geo& g, double* jc, const doub
   return true;
 }
 
+
+// ============================================================================
+// Cubic shape extension (AGPU_SHAPE_CUBIC; no counterpart in the reference):
+// cubic B-spline weights on integer nodes (the weights of cden_3d_wgh,
+// grid_part_lib.f90:419-454), quadratic on half nodes (qqh), and Esirkepov's
+// deposit with 4-point shapes on 6-slot windows.  Same arithmetic, in the
+// same order, as the oracle's restatement.
+// ============================================================================
+__device__ __forceinline__ int cden64(double xp, double a[4]) {
+  const double one_sixth = 1.0 / 6.0, two_third = 2.0 / 3.0;
+  double xx = 3.0 + xp;
+  int i = (int)xx;
+  double sx = xx - (double)i;
+  double sx2 = sx * sx;
+  double sx3 = sx2 * sx;
+  a[1] = two_third - sx2 + 0.5 * sx3;
+  a[2] = one_sixth + 0.5 * (sx + sx2 - sx3);
+  a[3] = one_sixth * sx3;
+  a[0] = 1. - a[1] - a[2] - a[3];
+  return i;
+}
+__device__ __forceinline__ int qhalf64(double xp, double a[3]) {
+  double xx = 3.0 + xp;
+  int h = (int)xx;
+  double sx = xx - (double)h - 0.5;
+  double sx2 = sx * sx;
+  a[1] = 0.75 - sx2;
+  a[2] = 0.5 * (0.25 + sx2 + sx);
+  a[0] = 1. - a[1] - a[2];
+  return h;
+}
+
+// Gather of the 2 (2D: Ex, Ey, Bz) or 6 field components; false when the
+// stencil leaves the array.  Per point (w_x * (w_y * w_z)) * F.
+__device__ __forceinline__ bool gather_cubic64(const Geo& g, const double* __restrict__ ebf, const double* xl, int ndim,
+                                               double ap[6]) {
+  double ax[4], ay[4], az[4] = {0., 1., 0., 0.}, axh[3], ayh[3], azh[3] = {0., 1., 0.};
+  const int fx = cden64(xl[0], ax), hx = qhalf64(xl[0], axh);
+  const int fy = cden64(xl[1], ay), hy = qhalf64(xl[1], ayh);
+  int kz0 = 1, kh0 = 1, nzi = 1;
+  if (ndim == 3) {
+    const int fz = cden64(xl[2], az), hz = qhalf64(xl[2], azh);
+    kz0 = fz - 1;
+    kh0 = hz - 1;
+    nzi = 4;
+    if (kz0 < 1 || fz + 2 > g.n3p) return false;
+  }
+  if (fx - 1 < 1 || fx + 2 > g.n1p || fy - 1 < 1 || fy + 2 > g.n2p) return false;
+  const int ix0 = fx - 1, iy0 = fy - 1, hx0 = hx - 1, hy0 = hy - 1;
+  const double* wzi = (ndim == 3) ? az : az + 1;
+  const double* E1 = ebf;
+  const double* E2 = ebf + g.ncell;
+  for (int c = 0; c < 6; ++c) ap[c] = 0.;
+  for (int k1 = 0; k1 < nzi; ++k1)
+    for (int j1 = 0; j1 < 4; ++j1) {
+      double dvol = ay[j1] * wzi[k1];
+      for (int i1 = 0; i1 < 3; ++i1) ap[0] += (axh[i1] * dvol) * __ldg(&E1[goff(g, hx0 + i1, iy0 + j1, kz0 + k1)]);
+    }
+  for (int k1 = 0; k1 < nzi; ++k1)
+    for (int j1 = 0; j1 < 3; ++j1) {
+      double dvol = ayh[j1] * wzi[k1];
+      for (int i1 = 0; i1 < 4; ++i1) ap[1] += (ax[i1] * dvol) * __ldg(&E2[goff(g, ix0 + i1, hy0 + j1, kz0 + k1)]);
+    }
+  if (ndim == 2) {
+    const double* B3 = ebf + 2 * g.ncell;
+    for (int j1 = 0; j1 < 3; ++j1) {
+      double dvol = ayh[j1];
+      for (int i1 = 0; i1 < 3; ++i1) ap[2] += (axh[i1] * dvol) * __ldg(&B3[goff(g, hx0 + i1, hy0 + j1, 1)]);
+    }
+    return true;
+  }
+  const double* E3 = ebf + 2 * g.ncell;
+  const double* B1 = ebf + 3 * g.ncell;
+  const double* B2 = ebf + 4 * g.ncell;
+  const double* B3 = ebf + 5 * g.ncell;
+  for (int k1 = 0; k1 < 3; ++k1)
+    for (int j1 = 0; j1 < 4; ++j1) {
+      double dvol = ay[j1] * azh[k1];
+      for (int i1 = 0; i1 < 4; ++i1) ap[2] += (ax[i1] * dvol) * __ldg(&E3[goff(g, ix0 + i1, iy0 + j1, kh0 + k1)]);
+    }
+  for (int k1 = 0; k1 < 3; ++k1)
+    for (int j1 = 0; j1 < 3; ++j1) {
+      double dvol = ayh[j1] * azh[k1];
+      for (int i1 = 0; i1 < 4; ++i1) ap[3] += (ax[i1] * dvol) * __ldg(&B1[goff(g, ix0 + i1, hy0 + j1, kh0 + k1)]);
+    }
+  for (int k1 = 0; k1 < 3; ++k1)
+    for (int j1 = 0; j1 < 4; ++j1) {
+      double dvol = ay[j1] * azh[k1];
+      for (int i1 = 0; i1 < 3; ++i1) ap[4] += (axh[i1] * dvol) * __ldg(&B2[goff(g, hx0 + i1, iy0 + j1, kh0 + k1)]);
+    }
+  for (int k1 = 0; k1 < 4; ++k1)
+    for (int j1 = 0; j1 < 3; ++j1) {
+      double dvol = ayh[j1] * az[k1];
+      for (int i1 = 0; i1 < 3; ++i1) ap[5] += (axh[i1] * dvol) * __ldg(&B3[goff(g, hx0 + i1, hy0 + j1, kz0 + k1)]);
+    }
+  return true;
+}
+
+// 1-D window: old shape on slots 1..4 (slot 0 = old floor node - 2), new on
+// sh..sh+3, running current; returns the node of slot 0.
+__device__ __forceinline__ int cubic_window64(double x0l, double x1l, double s0[6], double s1[6], double cur[6], int* lo,
+                                              int* hi) {
+  double a0[4], a1[4];
+  const int f0 = cden64(x0l, a0);
+  const int f1 = cden64(x1l, a1);
+  const int sh = f1 - f0 + 1;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    s0[q] = (q >= 1 && q <= 4) ? a0[q - 1] : 0.;
+    const int m = q - sh;
+    s1[q] = (sh >= 0 && sh <= 2 && m >= 0 && m <= 3) ? a1[m] : 0.;
+  }
+  cur[0] = s0[0] - s1[0];
+#pragma unroll
+  for (int q = 1; q < 6; ++q) cur[q] = cur[q - 1] + s0[q] - s1[q];
+  *lo = sh < 1 ? sh : 1;
+  *hi = (sh + 3) > 4 ? sh + 3 : 4;
+  return f0 - 2;
+}
+
+template <bool SERIAL>
+__device__ bool esirkepov_cubic64(const Geo& g, double* jc, const double* xn, const double* xo, float wght, int ndim) {
+  double sx0[6], sx1[6], cx[6], sy0[6], sy1[6], cy[6], sz0[6], sz1[6], cz[6];
+  int x0, x1, y0, y1, z0 = 0, z1 = 0;
+  const int bx = cubic_window64(xo[0], xn[0], sx0, sx1, cx, &x0, &x1);
+  const int by = cubic_window64(xo[1], xn[1], sy0, sy1, cy, &y0, &y1);
+  int bz = 1;
+  if (ndim == 3) bz = cubic_window64(xo[2], xn[2], sz0, sz1, cz, &z0, &z1);
+  const double w = (double)wght;
+  bool ok = true;
+  double* jx = jc;
+  double* jy = jc + g.ncell;
+  if (ndim == 2) {
+    for (int v = y0; v <= y1; ++v)
+      for (int u = x0; u <= x1; ++u) {
+        const int i = bx + u, j = by + v;
+        if (i < 1 || i > g.n1p || j < 1 || j > g.n2p) {
+          ok = false;
+          continue;
+        }
+        const long long o = goff(g, i, j, 1);
+        jadd<SERIAL>(&jx[o], (w * cx[u]) * (sy0[v] + sy1[v]));
+        jadd<SERIAL>(&jy[o], (sx0[u] + sx1[u]) * (w * cy[v]));
+      }
+    return ok;
+  }
+  double wx0[6], wx1[6], wy0[6], wy1[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    wx0[q] = 0.5 * sx1[q] + sx0[q];
+    wx1[q] = sx1[q] + 0.5 * sx0[q];
+    wy0[q] = 0.5 * sy1[q] + sy0[q];
+    wy1[q] = sy1[q] + 0.5 * sy0[q];
+  }
+  double* jz = jc + 2 * g.ncell;
+  for (int ww = z0; ww <= z1; ++ww)
+    for (int v = y0; v <= y1; ++v)
+      for (int u = x0; u <= x1; ++u) {
+        const int i = bx + u, j = by + v, k = bz + ww;
+        if (i < 1 || i > g.n1p || j < 1 || j > g.n2p || k < 1 || k > g.n3p) {
+          ok = false;
+          continue;
+        }
+        const long long o = goff(g, i, j, k);
+        jadd<SERIAL>(&jx[o], (w * cx[u]) * (wy0[v] * sz0[ww] + wy1[v] * sz1[ww]));
+        jadd<SERIAL>(&jy[o], (w * cy[v]) * (wx0[u] * sz0[ww] + wx1[u] * sz1[ww]));
+        jadd<SERIAL>(&jz[o], (w * cz[ww]) * (wx0[u] * sy0[v] + wx1[u] * sy1[v]));
+      }
+  return ok;
+}
+
 // ============================================================================
 // A2-A12 fused: gather (set_part{2,3}d_hcell_acc, grid_part_connect.f90:
 // 89-285) -> charge multiply (curr_and_fields_util.f90:58-72) ->
@@ -247,7 +418,7 @@ __device__ __forceinline__ bool esirkepov3d(const Geo& g, double* jc, const doub
 // per particle the arithmetic is identical, and a particle that leaves the
 // box is exactly one that the reference removes before its deposit.
 // ============================================================================
-template <bool SERIAL>
+template <bool SERIAL, int SHAPE>
 __global__ void __launch_bounds__(256) k64_push_dep_3d(PushArgs64 a) {
   const Geo g = a.g;
   const double* __restrict__ ex = a.ebf;
@@ -260,62 +431,70 @@ __global__ void __launch_bounds__(256) k64_push_dep_3d(PushArgs64 a) {
     uint64_t sl = dbits(a.slot[n]);
     // set_local_3d_positions
     double xo[3] = {a.dx_inv * (x - a.xmn), a.dy_inv * (y - a.ymn), a.dz_inv * (z - a.zmn)};
-    double ax1[3], axh[2], ay1[3], ayh[2], az1[3], azh[2];
-    int i = qlh64(xo[0], ax1, axh);
-    int j = qlh64(xo[1], ay1, ayh);
-    int k = qlh64(xo[2], az1, azh);
-    // gather needs i..i+2, the deposit i-1..i+3 (old node i+1 +- 2)
-    if (i < 2 || i > g.n1p - 3 || j < 2 || j > g.n2p - 3 || k < 2 || k > g.n3p - 3) {
-      raise_err(a.err, AGPU_EBIT_INDEX);
-      atomicAdd(a.removed, 1ull);  // outside the box: the compaction drops it
-      continue;
-    }
-    int ih = i, jh = j, kh = k;
     double ap[6] = {0, 0, 0, 0, 0, 0};
-    const double* e1 = ex;
-    const double* e2 = ex + g.ncell;
-    const double* e3 = ex + 2 * g.ncell;
-    const double* b1 = ex + 3 * g.ncell;
-    const double* b2 = ex + 4 * g.ncell;
-    const double* b3 = ex + 5 * g.ncell;
-#pragma unroll
-    for (int k1 = 0; k1 <= 2; ++k1) {
-      int k2 = k + k1;
-#pragma unroll
-      for (int j1 = 0; j1 <= 2; ++j1) {
-        int j2 = j + j1;
-        double dvol = ay1[j1] * az1[k1];
-#pragma unroll
-        for (int i1 = 0; i1 <= 1; ++i1) ap[0] = ap[0] + axh[i1] * dvol * __ldg(&e1[goff(g, i1 + ih, j2, k2)]);
+    if (SHAPE == AGPU_SHAPE_CUBIC) {
+      if (!gather_cubic64(g, ex, xo, 3, ap)) {
+        raise_err(a.err, AGPU_EBIT_INDEX);
+        atomicAdd(a.removed, 1ull);  // outside the box: the compaction drops it
+        continue;
       }
-#pragma unroll
-      for (int j1 = 0; j1 <= 1; ++j1) {
-        int j2 = jh + j1;
-        double dvol = ayh[j1] * az1[k1];
-#pragma unroll
-        for (int i1 = 0; i1 <= 2; ++i1) ap[1] = ap[1] + ax1[i1] * dvol * __ldg(&e2[goff(g, i + i1, j2, k2)]);
-#pragma unroll
-        for (int i1 = 0; i1 <= 1; ++i1) ap[5] = ap[5] + axh[i1] * dvol * __ldg(&b3[goff(g, i1 + ih, j2, k2)]);
+    } else {
+      double ax1[3], axh[2], ay1[3], ayh[2], az1[3], azh[2];
+      int i = qlh64(xo[0], ax1, axh);
+      int j = qlh64(xo[1], ay1, ayh);
+      int k = qlh64(xo[2], az1, azh);
+      // gather needs i..i+2, the deposit i-1..i+3 (old node i+1 +- 2)
+      if (i < 2 || i > g.n1p - 3 || j < 2 || j > g.n2p - 3 || k < 2 || k > g.n3p - 3) {
+        raise_err(a.err, AGPU_EBIT_INDEX);
+        atomicAdd(a.removed, 1ull);  // outside the box: the compaction drops it
+        continue;
       }
-    }
-#pragma unroll
-    for (int k1 = 0; k1 <= 1; ++k1) {
-      int k2 = kh + k1;
-#pragma unroll
-      for (int j1 = 0; j1 <= 1; ++j1) {
-        int j2 = jh + j1;
-        double dvol = ayh[j1] * azh[k1];
-#pragma unroll
-        for (int i1 = 0; i1 <= 2; ++i1) ap[3] = ap[3] + ax1[i1] * dvol * __ldg(&b1[goff(g, i1 + i, j2, k2)]);
+      int ih = i, jh = j, kh = k;
+      const double* e1 = ex;
+      const double* e2 = ex + g.ncell;
+      const double* e3 = ex + 2 * g.ncell;
+      const double* b1 = ex + 3 * g.ncell;
+      const double* b2 = ex + 4 * g.ncell;
+      const double* b3 = ex + 5 * g.ncell;
+  #pragma unroll
+      for (int k1 = 0; k1 <= 2; ++k1) {
+        int k2 = k + k1;
+  #pragma unroll
+        for (int j1 = 0; j1 <= 2; ++j1) {
+          int j2 = j + j1;
+          double dvol = ay1[j1] * az1[k1];
+  #pragma unroll
+          for (int i1 = 0; i1 <= 1; ++i1) ap[0] = ap[0] + axh[i1] * dvol * __ldg(&e1[goff(g, i1 + ih, j2, k2)]);
+        }
+  #pragma unroll
+        for (int j1 = 0; j1 <= 1; ++j1) {
+          int j2 = jh + j1;
+          double dvol = ayh[j1] * az1[k1];
+  #pragma unroll
+          for (int i1 = 0; i1 <= 2; ++i1) ap[1] = ap[1] + ax1[i1] * dvol * __ldg(&e2[goff(g, i + i1, j2, k2)]);
+  #pragma unroll
+          for (int i1 = 0; i1 <= 1; ++i1) ap[5] = ap[5] + axh[i1] * dvol * __ldg(&b3[goff(g, i1 + ih, j2, k2)]);
+        }
       }
-#pragma unroll
-      for (int j1 = 0; j1 <= 2; ++j1) {
-        int j2 = j + j1;
-        double dvol = ay1[j1] * azh[k1];
-#pragma unroll
-        for (int i1 = 0; i1 <= 1; ++i1) ap[4] = ap[4] + axh[i1] * dvol * __ldg(&b2[goff(g, ih + i1, j2, k2)]);
-#pragma unroll
-        for (int i1 = 0; i1 <= 2; ++i1) ap[2] = ap[2] + ax1[i1] * dvol * __ldg(&e3[goff(g, i1 + i, j2, k2)]);
+  #pragma unroll
+      for (int k1 = 0; k1 <= 1; ++k1) {
+        int k2 = kh + k1;
+  #pragma unroll
+        for (int j1 = 0; j1 <= 1; ++j1) {
+          int j2 = jh + j1;
+          double dvol = ayh[j1] * azh[k1];
+  #pragma unroll
+          for (int i1 = 0; i1 <= 2; ++i1) ap[3] = ap[3] + ax1[i1] * dvol * __ldg(&b1[goff(g, i1 + i, j2, k2)]);
+        }
+  #pragma unroll
+        for (int j1 = 0; j1 <= 2; ++j1) {
+          int j2 = j + j1;
+          double dvol = ay1[j1] * azh[k1];
+  #pragma unroll
+          for (int i1 = 0; i1 <= 1; ++i1) ap[4] = ap[4] + axh[i1] * dvol * __ldg(&b2[goff(g, ih + i1, j2, k2)]);
+  #pragma unroll
+          for (int i1 = 0; i1 <= 2; ++i1) ap[2] = ap[2] + ax1[i1] * dvol * __ldg(&e3[goff(g, i1 + i, j2, k2)]);
+        }
       }
     }
     // field_charge_multiply
@@ -380,11 +559,13 @@ __global__ void __launch_bounds__(256) k64_push_dep_3d(PushArgs64 a) {
     }
     double xn[3] = {a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn), a.dz_inv * (znew - a.zmn)};
     float wght = (float)slot_charge(sl) * slot_wgh(sl);
-    if (!esirkepov3d<SERIAL>(g, a.jc, xn, xo, wght)) raise_err(a.err, AGPU_EBIT_INDEX);
+    const bool dep_ok = (SHAPE == AGPU_SHAPE_CUBIC) ? esirkepov_cubic64<SERIAL>(g, a.jc, xn, xo, wght, 3)
+                                                   : esirkepov3d<SERIAL>(g, a.jc, xn, xo, wght);
+    if (!dep_ok) raise_err(a.err, AGPU_EBIT_INDEX);
   }
 }
 
-template <bool SERIAL>
+template <bool SERIAL, int SHAPE>
 __global__ void __launch_bounds__(256) k64_push_dep_2d(PushArgs64 a) {
   const Geo g = a.g;
   const double* __restrict__ ex = a.ebf;
@@ -397,42 +578,55 @@ __global__ void __launch_bounds__(256) k64_push_dep_2d(PushArgs64 a) {
     uint64_t sl = dbits(a.slot[n]);
     double xl = a.dx_inv * (x - a.xmn);
     double yl = a.dy_inv * (y - a.ymn);
-    double ax1[3], axh[2], ay1[3], ayh[2];
-    int i = qlh64(xl, ax1, axh);
-    int j = qlh64(yl, ay1, ayh);
-    if (i < 2 || i > g.n1p - 3 || j < 2 || j > g.n2p - 3) {
-      raise_err(a.err, AGPU_EBIT_INDEX);
-      atomicAdd(a.removed, 1ull);  // outside the box: the compaction drops it
-      continue;
-    }
-    int ih = i, jh = j;
-    const double* e1 = ex;
-    const double* e2 = ex + g.ncell;
-    const double* b3 = ex + 2 * g.ncell;
     double ap1 = 0., ap2 = 0., ap3 = 0.;
-#pragma unroll
-    for (int j1 = 0; j1 <= 2; ++j1) {
-      int j2 = j + j1;
-      double dvol = ay1[j1];
-#pragma unroll
-      for (int i1 = 0; i1 <= 1; ++i1) {
-        double dvol1 = axh[i1] * dvol;
-        ap1 = ap1 + dvol1 * __ldg(&e1[goff(g, i1 + ih, j2, 1)]);
+    if (SHAPE == AGPU_SHAPE_CUBIC) {
+      double apc[6];
+      const double xl2[2] = {xl, yl};
+      if (!gather_cubic64(g, ex, xl2, 2, apc)) {
+        raise_err(a.err, AGPU_EBIT_INDEX);
+        atomicAdd(a.removed, 1ull);  // outside the box: the compaction drops it
+        continue;
       }
-    }
-#pragma unroll
-    for (int j1 = 0; j1 <= 1; ++j1) {
-      int j2 = jh + j1;
-      double dvol = ayh[j1];
-#pragma unroll
-      for (int i1 = 0; i1 <= 2; ++i1) {
-        double dvol1 = ax1[i1] * dvol;
-        ap2 = ap2 + dvol1 * __ldg(&e2[goff(g, i + i1, j2, 1)]);
+      ap1 = apc[0];
+      ap2 = apc[1];
+      ap3 = apc[2];
+    } else {
+      double ax1[3], axh[2], ay1[3], ayh[2];
+      int i = qlh64(xl, ax1, axh);
+      int j = qlh64(yl, ay1, ayh);
+      if (i < 2 || i > g.n1p - 3 || j < 2 || j > g.n2p - 3) {
+        raise_err(a.err, AGPU_EBIT_INDEX);
+        atomicAdd(a.removed, 1ull);  // outside the box: the compaction drops it
+        continue;
       }
-#pragma unroll
-      for (int i1 = 0; i1 <= 1; ++i1) {
-        double dvol1 = axh[i1] * dvol;
-        ap3 = ap3 + dvol1 * __ldg(&b3[goff(g, i1 + ih, j2, 1)]);
+      int ih = i, jh = j;
+      const double* e1 = ex;
+      const double* e2 = ex + g.ncell;
+      const double* b3 = ex + 2 * g.ncell;
+  #pragma unroll
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = j + j1;
+        double dvol = ay1[j1];
+  #pragma unroll
+        for (int i1 = 0; i1 <= 1; ++i1) {
+          double dvol1 = axh[i1] * dvol;
+          ap1 = ap1 + dvol1 * __ldg(&e1[goff(g, i1 + ih, j2, 1)]);
+        }
+      }
+  #pragma unroll
+      for (int j1 = 0; j1 <= 1; ++j1) {
+        int j2 = jh + j1;
+        double dvol = ayh[j1];
+  #pragma unroll
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = ax1[i1] * dvol;
+          ap2 = ap2 + dvol1 * __ldg(&e2[goff(g, i + i1, j2, 1)]);
+        }
+  #pragma unroll
+        for (int i1 = 0; i1 <= 1; ++i1) {
+          double dvol1 = axh[i1] * dvol;
+          ap3 = ap3 + dvol1 * __ldg(&b3[goff(g, i1 + ih, j2, 1)]);
+        }
       }
     }
     double q = (double)slot_charge(sl);
@@ -478,8 +672,14 @@ __global__ void __launch_bounds__(256) k64_push_dep_2d(PushArgs64 a) {
       continue;
     }
     float wght = (float)slot_charge(sl) * slot_wgh(sl);
-    if (!esirkepov2d<SERIAL>(g, a.jc, a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn), xl, yl, wght))
-      raise_err(a.err, AGPU_EBIT_INDEX);
+    bool dep_ok;
+    if (SHAPE == AGPU_SHAPE_CUBIC) {
+      const double xn2[2] = {a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn)}, xo2[2] = {xl, yl};
+      dep_ok = esirkepov_cubic64<SERIAL>(g, a.jc, xn2, xo2, wght, 2);
+    } else {
+      dep_ok = esirkepov2d<SERIAL>(g, a.jc, a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn), xl, yl, wght);
+    }
+    if (!dep_ok) raise_err(a.err, AGPU_EBIT_INDEX);
   }
 }
 
@@ -487,16 +687,17 @@ void push_deposit64(const PushArgs64& a, cudaStream_t st, int sms, bool serial) 
   if (a.np <= 0) return;
   int block = 256;
   int grid = serial ? 1 : grid_for(a.np, block, sms, 8);
+  const bool cubic = a.shape == AGPU_SHAPE_CUBIC;
   if (a.g.ndim == 3) {
     if (serial)
-      k64_push_dep_3d<true><<<1, 32, 0, st>>>(a);
+      cubic ? k64_push_dep_3d<true, 1><<<1, 32, 0, st>>>(a) : k64_push_dep_3d<true, 0><<<1, 32, 0, st>>>(a);
     else
-      k64_push_dep_3d<false><<<grid, block, 0, st>>>(a);
+      cubic ? k64_push_dep_3d<false, 1><<<grid, block, 0, st>>>(a) : k64_push_dep_3d<false, 0><<<grid, block, 0, st>>>(a);
   } else {
     if (serial)
-      k64_push_dep_2d<true><<<1, 32, 0, st>>>(a);
+      cubic ? k64_push_dep_2d<true, 1><<<1, 32, 0, st>>>(a) : k64_push_dep_2d<true, 0><<<1, 32, 0, st>>>(a);
     else
-      k64_push_dep_2d<false><<<grid, block, 0, st>>>(a);
+      cubic ? k64_push_dep_2d<false, 1><<<grid, block, 0, st>>>(a) : k64_push_dep_2d<false, 0><<<grid, block, 0, st>>>(a);
   }
 }
 

@@ -35,6 +35,7 @@ struct PushArgs64 {
   double dt, dth, lfact;
   double gxmin, gxmax, gymin, gymax, gzmin, gzmax;
   int initial;
+  int shape;  // AGPU_SHAPE_QUADRATIC or AGPU_SHAPE_CUBIC
   unsigned long long* removed;
   unsigned int* err;
 };

@@ -47,6 +47,8 @@ struct TileArgs64 {
 
 TileGeo make_tiles(const Geo& g, int nx, int ny, int nz);
 void tile_push32(const TileArgs32& a, cudaStream_t st);
+// the cubic shape extension (agpu_tile32c.cu)
+void tile_push32_cubic(const TileArgs32& a, cudaStream_t st);
 void tile_push64(const TileArgs64& a, cudaStream_t st);
 void hist_reset(int* hist, const int* tstart, const TileGeo& t, long long np, bool first, unsigned long long* pushed,
                 cudaStream_t st);

@@ -58,6 +58,15 @@ extern "C" {
 #define AGPU_FP32_SPLIT 1        /* FP32 bulk, positions = int cell + FP32 offset,
                                     compensated FP32 current accumulation                 */
 
+/* ---- particle shapes --------------------------------------------------- */
+#define AGPU_SHAPE_QUADRATIC 0   /* quadratic on integer nodes, linear on half nodes
+                                    (qlh, grid_part_lib.f90:110-143, 212-259) and the
+                                    quadratic Esirkepov deposit: the reference        */
+#define AGPU_SHAPE_CUBIC 1       /* extension with no counterpart in the reference:
+                                    cubic B-spline on integer nodes (the weights of
+                                    cden_3d_wgh, grid_part_lib.f90:419-454), quadratic
+                                    on half nodes, cubic Esirkepov deposit            */
+
 /* ---- device error word bits (agpu_step_out.error_bits) ----------------- */
 #define AGPU_EBIT_INDEX 1u
 #define AGPU_EBIT_IONZ_INDEX 2u
@@ -82,7 +91,9 @@ typedef struct agpu_params {
   int32_t w_sh;            /* window shift period in steps (0 = no window)        */
   int32_t ionz_lev;        /* 0 = no ionization, 1 = one-level ADK                */
   int32_t n_mol_atoms[4];  /* atoms per molecule of each ion species (ionz_data) */
-  int32_t reserved_i[4];
+  int32_t shape;           /* AGPU_SHAPE_QUADRATIC (the reference's qlh gather and
+                              quadratic Esirkepov) or AGPU_SHAPE_CUBIC           */
+  int32_t reserved_i[3];
   double dx, dy, dz;       /* cell sizes (um)                                     */
   double dx_inv, dy_inv, dz_inv;
   double dt;               /* time step (um/c)                                    */

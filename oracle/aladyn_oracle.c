@@ -728,6 +728,202 @@ static void ora_esirkepov_3d_one(ora_sim* s, double* jc, const double xp1[3], co
    preamble (curr_and_fields_util.f90:74-102; grid_part_connect.f90:979-987,
    1201-1208): new positions from part, old positions from ebfp, weight
    wght = real(charge*wgh, sp). */
+/* ======================================================================== */
+/* Cubic shape extension (AGPU_SHAPE_CUBIC).  No counterpart in the         */
+/* reference, which gathers and deposits with quadratic shapes only; the     */
+/* cubic B-spline weights are those of its charge-density helper            */
+/* cden_3d_wgh (grid_part_lib.f90:419-454), the half-node weights those of   */
+/* qqh (170-210), and the deposit is Esirkepov's scheme with 4-point shapes  */
+/* on 6-slot windows, written in the same regrouped form as the quadratic   */
+/* one: J = curr(u) * (S0-plane term + S1-plane term).                      */
+/* ======================================================================== */
+static const double ora_one_sixth = 1.0 / 6.0, ora_two_third = 2.0 / 3.0;
+/* cubic weights on integer nodes i-1..i+2, i = int(3 + x) */
+static inline void ora_cden_1d(double xp, double a[4], int* ix) {
+  double xx = shx + xp;
+  int i = (int)xx;
+  double sx = xx - (double)i;
+  double sx2 = sx * sx;
+  double sx3 = sx2 * sx;
+  a[1] = ora_two_third - sx2 + 0.5 * sx3;
+  a[2] = ora_one_sixth + 0.5 * (sx + sx2 - sx3);
+  a[3] = ora_one_sixth * sx3;
+  a[0] = 1. - a[1] - a[2] - a[3];
+  *ix = i;
+}
+/* quadratic weights on half nodes h-1..h+1 (index m stands for m + 1/2) */
+static inline void ora_qhalf_1d(double xp, double a[3], int* ih) {
+  double xx = shx + xp;
+  int h = (int)xx;
+  double sx = xx - (double)h - 0.5;
+  double sx2 = sx * sx;
+  a[1] = 0.75 - sx2;
+  a[2] = 0.5 * (0.25 + sx2 + sx);
+  a[0] = 1. - a[1] - a[2];
+  *ih = h;
+}
+void ora_shape_cubic(double xp, double* a4, double* ah3, int* ix, int* ih) {
+  ora_cden_1d(xp, a4, ix);
+  ora_qhalf_1d(xp, ah3, ih);
+}
+
+/* Gather with cubic (integer) x quadratic (half) weights; the staggering of
+   set_part3d_hcell_acc / set_part2d_hcell_acc.  Product order per point:
+   (w_x * (w_y * w_z)) * F. */
+static void ora_gather_cubic(ora_sim* s, int ic, int64_t np) {
+  const agpu_params* p = &s->p;
+  #pragma omp parallel for schedule(static) num_threads(s->nthreads) if (s->nthreads > 1)
+  for (int64_t n = 1; n <= np; ++n) {
+    double xl = p->dx_inv * (PART(s, ic, n, 1) - p->xmn);
+    double yl = p->dy_inv * (PART(s, ic, n, 2) - p->ymn);
+    double ax[4], ay[4], az[4] = {0., 1., 0., 0.}, axh[3], ayh[3], azh[3] = {0., 1., 0.};
+    int fx, fy, fz = 2, hx, hy, hz = 1;
+    ora_cden_1d(xl, ax, &fx);
+    ora_qhalf_1d(xl, axh, &hx);
+    ora_cden_1d(yl, ay, &fy);
+    ora_qhalf_1d(yl, ayh, &hy);
+    int nzi = 1, nzh = 1, kz0 = 1, kh0 = 1;
+    if (p->ndim == 3) {
+      double zl = p->dz_inv * (PART(s, ic, n, 3) - p->zmn);
+      ora_cden_1d(zl, az, &fz);
+      ora_qhalf_1d(zl, azh, &hz);
+      nzi = 4;
+      nzh = 3;
+      kz0 = fz - 1;
+      kh0 = hz - 1;
+    }
+    const int ix0 = fx - 1, iy0 = fy - 1, hx0 = hx - 1, hy0 = hy - 1;
+    const double* wzi = (p->ndim == 3) ? az : az + 1;
+    const double* wzh = (p->ndim == 3) ? azh : azh + 1;
+    double ap[6] = {0., 0., 0., 0., 0., 0.};
+    /* Ex(i+1/2, j, k) */
+    for (int k1 = 0; k1 < nzi; ++k1)
+      for (int j1 = 0; j1 < 4; ++j1) {
+        double dvol = ay[j1] * wzi[k1];
+        for (int i1 = 0; i1 < 3; ++i1) ap[0] += (axh[i1] * dvol) * EBF(s, hx0 + i1, iy0 + j1, kz0 + k1, 1);
+      }
+    /* Ey(i, j+1/2, k) */
+    for (int k1 = 0; k1 < nzi; ++k1)
+      for (int j1 = 0; j1 < 3; ++j1) {
+        double dvol = ayh[j1] * wzi[k1];
+        for (int i1 = 0; i1 < 4; ++i1) ap[1] += (ax[i1] * dvol) * EBF(s, ix0 + i1, hy0 + j1, kz0 + k1, 2);
+      }
+    if (p->ndim == 2) {
+      /* Bz(i+1/2, j+1/2) */
+      for (int j1 = 0; j1 < 3; ++j1) {
+        double dvol = ayh[j1];
+        for (int i1 = 0; i1 < 3; ++i1) ap[2] += (axh[i1] * dvol) * EBF(s, hx0 + i1, hy0 + j1, 1, 3);
+      }
+      PT(s, n, 1) = ap[0];
+      PT(s, n, 2) = ap[1];
+      PT(s, n, 3) = ap[2];
+      continue;
+    }
+    /* Ez(i, j, k+1/2) */
+    for (int k1 = 0; k1 < 3; ++k1)
+      for (int j1 = 0; j1 < 4; ++j1) {
+        double dvol = ay[j1] * azh[k1];
+        for (int i1 = 0; i1 < 4; ++i1) ap[2] += (ax[i1] * dvol) * EBF(s, ix0 + i1, iy0 + j1, kh0 + k1, 3);
+      }
+    /* Bx(i, j+1/2, k+1/2) */
+    for (int k1 = 0; k1 < 3; ++k1)
+      for (int j1 = 0; j1 < 3; ++j1) {
+        double dvol = ayh[j1] * azh[k1];
+        for (int i1 = 0; i1 < 4; ++i1) ap[3] += (ax[i1] * dvol) * EBF(s, ix0 + i1, hy0 + j1, kh0 + k1, 4);
+      }
+    /* By(i+1/2, j, k+1/2) */
+    for (int k1 = 0; k1 < 3; ++k1)
+      for (int j1 = 0; j1 < 4; ++j1) {
+        double dvol = ay[j1] * azh[k1];
+        for (int i1 = 0; i1 < 3; ++i1) ap[4] += (axh[i1] * dvol) * EBF(s, hx0 + i1, iy0 + j1, kh0 + k1, 5);
+      }
+    /* Bz(i+1/2, j+1/2, k) */
+    for (int k1 = 0; k1 < 4; ++k1)
+      for (int j1 = 0; j1 < 3; ++j1) {
+        double dvol = ayh[j1] * az[k1];
+        for (int i1 = 0; i1 < 3; ++i1) ap[5] += (axh[i1] * dvol) * EBF(s, hx0 + i1, hy0 + j1, kz0 + k1, 6);
+      }
+    for (int c = 0; c < 6; ++c) PT(s, n, 1 + c) = ap[c];
+  }
+}
+
+/* 1-D part of the cubic Esirkepov deposit: old shape on slots 1..4 (slot 0
+   = old floor node - 2), new shape on slots sh..sh+3 (sh = new floor - old
+   floor + 1, in 0..2), the running current on the 6 slots, and the slot
+   range lo..hi the particle touches. */
+static void ora_cubic_window(double x0l, double x1l, double s0[6], double s1[6], double cur[6], int* base, int* lo,
+                             int* hi) {
+  double a0[4], a1[4];
+  int f0, f1;
+  ora_cden_1d(x0l, a0, &f0);
+  ora_cden_1d(x1l, a1, &f1);
+  int sh = f1 - f0 + 1;
+  for (int q = 0; q < 6; ++q) {
+    s0[q] = 0.;
+    s1[q] = 0.;
+  }
+  for (int q = 0; q < 4; ++q) s0[q + 1] = a0[q];
+  if (sh >= 0 && sh <= 2)
+    for (int q = 0; q < 4; ++q) s1[q + sh] = a1[q];
+  cur[0] = s0[0] - s1[0];
+  for (int q = 1; q < 6; ++q) cur[q] = cur[q - 1] + s0[q] - s1[q];
+  *base = f0 - 2;
+  *lo = sh < 1 ? sh : 1;
+  *hi = (sh + 3) > 4 ? sh + 3 : 4;
+}
+
+static inline int ora_in_box(const ora_sim* s, int i, int j, int k) {
+  return i >= 1 && i <= s->n1p && j >= 1 && j <= s->n2p && k >= 1 && k <= s->n3p;
+}
+
+static void ora_esirkepov_cubic_2d_one(ora_sim* s, double* jc, const double xp1[2], const double xp0[2], float wght) {
+  double sx0[6], sx1[6], cx[6], sy0[6], sy1[6], cy[6];
+  int bx, x0, x1, by, y0, y1;
+  ora_cubic_window(xp0[0], xp1[0], sx0, sx1, cx, &bx, &x0, &x1);
+  ora_cubic_window(xp0[1], xp1[1], sy0, sy1, cy, &by, &y0, &y1);
+  size_t n1p = (size_t)s->n1p, comp = n1p * (size_t)s->n2p * (size_t)s->n3p;
+  for (int v = y0; v <= y1; ++v)
+    for (int u = x0; u <= x1; ++u) {
+      int i = bx + u, j = by + v;
+      if (!ora_in_box(s, i, j, 1)) {
+        s->error_bits |= AGPU_EBIT_INDEX;
+        continue;
+      }
+      size_t o = (size_t)(i - 1) + n1p * (size_t)(j - 1);
+      jc[o] = jc[o] + ((double)wght * cx[u]) * (sy0[v] + sy1[v]);
+      jc[comp + o] = jc[comp + o] + (sx0[u] + sx1[u]) * ((double)wght * cy[v]);
+    }
+}
+
+static void ora_esirkepov_cubic_3d_one(ora_sim* s, double* jc, const double xp1[3], const double xp0[3], float wght) {
+  double sx0[6], sx1[6], cx[6], sy0[6], sy1[6], cy[6], sz0[6], sz1[6], cz[6];
+  int bx, x0, x1, by, y0, y1, bz, z0, z1;
+  ora_cubic_window(xp0[0], xp1[0], sx0, sx1, cx, &bx, &x0, &x1);
+  ora_cubic_window(xp0[1], xp1[1], sy0, sy1, cy, &by, &y0, &y1);
+  ora_cubic_window(xp0[2], xp1[2], sz0, sz1, cz, &bz, &z0, &z1);
+  double wx0[6], wx1[6], wy0[6], wy1[6];
+  for (int q = 0; q < 6; ++q) {
+    wx0[q] = 0.5 * sx1[q] + sx0[q];
+    wx1[q] = sx1[q] + 0.5 * sx0[q];
+    wy0[q] = 0.5 * sy1[q] + sy0[q];
+    wy1[q] = sy1[q] + 0.5 * sy0[q];
+  }
+  size_t n1p = (size_t)s->n1p, n2p = (size_t)s->n2p, comp = n1p * n2p * (size_t)s->n3p;
+  for (int w = z0; w <= z1; ++w)
+    for (int v = y0; v <= y1; ++v)
+      for (int u = x0; u <= x1; ++u) {
+        int i = bx + u, j = by + v, k = bz + w;
+        if (!ora_in_box(s, i, j, k)) {
+          s->error_bits |= AGPU_EBIT_INDEX;
+          continue;
+        }
+        size_t o = (size_t)(i - 1) + n1p * ((size_t)(j - 1) + n2p * (size_t)(k - 1));
+        jc[o] = jc[o] + ((double)wght * cx[u]) * (wy0[v] * sz0[w] + wy1[v] * sz1[w]);
+        jc[comp + o] = jc[comp + o] + ((double)wght * cy[v]) * (wx0[u] * sz0[w] + wx1[u] * sz1[w]);
+        jc[2 * comp + o] = jc[2 * comp + o] + ((double)wght * cz[w]) * (wx0[u] * sy0[v] + wx1[u] * sy1[v]);
+      }
+}
+
 static void ora_curr_accumulate(ora_sim* s, int ic, int64_t np) {
   const agpu_params* p = &s->p;
   int nth = s->nthreads;
@@ -760,13 +956,19 @@ static void ora_curr_accumulate(ora_sim* s, int ic, int64_t np) {
       if (p->ndim == 2) {
         double xp1[2] = {p->dx_inv * (PART(s, ic, n, 1) - p->xmn), p->dy_inv * (PART(s, ic, n, 2) - p->ymn)};
         double xp0[2] = {p->dx_inv * (PT(s, n, 3) - p->xmn), p->dy_inv * (PT(s, n, 4) - p->ymn)};
-        ora_esirkepov_2d_one(s, jc, xp1, xp0, wght);
+        if (p->shape == AGPU_SHAPE_CUBIC)
+          ora_esirkepov_cubic_2d_one(s, jc, xp1, xp0, wght);
+        else
+          ora_esirkepov_2d_one(s, jc, xp1, xp0, wght);
       } else {
         double xp1[3] = {p->dx_inv * (PART(s, ic, n, 1) - p->xmn), p->dy_inv * (PART(s, ic, n, 2) - p->ymn),
                          p->dz_inv * (PART(s, ic, n, 3) - p->zmn)};
         double xp0[3] = {p->dx_inv * (PT(s, n, 4) - p->xmn), p->dy_inv * (PT(s, n, 5) - p->ymn),
                          p->dz_inv * (PT(s, n, 6) - p->zmn)};
-        ora_esirkepov_3d_one(s, jc, xp1, xp0, wght);
+        if (p->shape == AGPU_SHAPE_CUBIC)
+          ora_esirkepov_cubic_3d_one(s, jc, xp1, xp0, wght);
+        else
+          ora_esirkepov_3d_one(s, jc, xp1, xp0, wght);
       }
     }
   }
@@ -782,16 +984,39 @@ static void ora_curr_accumulate(ora_sim* s, int ic, int64_t np) {
 /* Deposit of one particle move for the continuity tests: positions in grid
    units (local, as set_local_positions returns them). */
 void ora_deposit_move(ora_sim* s, const double* xnew, const double* xold, float wght) {
-  if (s->p.ndim == 2)
-    ora_esirkepov_2d_one(s, s->jc, xnew, xold, wght);
-  else
-    ora_esirkepov_3d_one(s, s->jc, xnew, xold, wght);
+  const int cubic = s->p.shape == AGPU_SHAPE_CUBIC;
+  if (s->p.ndim == 2) {
+    if (cubic) ora_esirkepov_cubic_2d_one(s, s->jc, xnew, xold, wght);
+    else ora_esirkepov_2d_one(s, s->jc, xnew, xold, wght);
+  } else {
+    if (cubic) ora_esirkepov_cubic_3d_one(s, s->jc, xnew, xold, wght);
+    else ora_esirkepov_3d_one(s, s->jc, xnew, xold, wght);
+  }
 }
 void ora_zero_currents(ora_sim* s) { memset(s->jc, 0, sizeof(double) * (size_t)s->n1p * s->n2p * s->n3p * s->nc); }
 
 /* Charge density of one particle with the qden shapes into rho(n1p,n2p,n3p)
    (the density the Esirkepov scheme conserves; grid_part_lib.f90:337-417). */
 void ora_rho_one(const ora_sim* s, double* rho, const double* xl, double wght) {
+  if (s->p.shape == AGPU_SHAPE_CUBIC) {
+    /* cubic density: nodes i-1..i+2 of the floor node i (cden_*_wgh) */
+    double cx[4], cy[4], cz[4] = {1, 0, 0, 0};
+    int i, j, k = 2, nzc = 1;
+    ora_cden_1d(xl[0], cx, &i);
+    ora_cden_1d(xl[1], cy, &j);
+    if (s->p.ndim == 3) {
+      ora_cden_1d(xl[2], cz, &k);
+      nzc = 4;
+    }
+    size_t n1p = (size_t)s->n1p, n2p = (size_t)s->n2p;
+    for (int k1 = 0; k1 < nzc; ++k1)
+      for (int j1 = 0; j1 < 4; ++j1)
+        for (int i1 = 0; i1 < 4; ++i1) {
+          int i2 = i - 1 + i1, j2 = j - 1 + j1, k2 = (s->p.ndim == 3) ? k - 1 + k1 : 1;
+          rho[(size_t)(i2 - 1) + n1p * ((size_t)(j2 - 1) + n2p * (size_t)(k2 - 1))] += wght * cx[i1] * cy[j1] * cz[k1];
+        }
+    return;
+  }
   double ax[3], ay[3], az[3] = {1, 0, 0};
   int i, j, k = 1;
   ora_qden_1d(xl[0], ax, &i);
@@ -1538,7 +1763,7 @@ int ora_step(ora_sim* s, int iter, double t, int initial_time, agpu_step_out* ou
   ora_zero_currents(s);
   for (int ic = 0; ic < p->nsp_run; ++ic) {
     int64_t np = s->np[ic];
-    ora_gather(s, ic, np);
+    if (s->p.shape == AGPU_SHAPE_CUBIC) ora_gather_cubic(s, ic, np); else ora_gather(s, ic, np);
     ora_field_charge_multiply(s, ic, np);
     if (initial_time) ora_init_lpf_momenta(s, ic, np);
     ora_push(s, ic, np);
@@ -1563,7 +1788,7 @@ int ora_step(ora_sim* s, int iter, double t, int initial_time, agpu_step_out* ou
 /* Individual phases for tests. */
 void ora_phase_gather_push(ora_sim* s, int ic, int initial_time) {
   int64_t np = s->np[ic];
-  ora_gather(s, ic, np);
+  if (s->p.shape == AGPU_SHAPE_CUBIC) ora_gather_cubic(s, ic, np); else ora_gather(s, ic, np);
   ora_field_charge_multiply(s, ic, np);
   if (initial_time) ora_init_lpf_momenta(s, ic, np);
   ora_push(s, ic, np);

@@ -58,6 +58,7 @@ def load():
         "ora_shape_qlh": (None, [C.c_double, D, D, C.POINTER(C.c_int)]),
         "ora_shape_qqh": (None, [C.c_double, D, D, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "ora_shape_qden": (None, [C.c_double, D, C.POINTER(C.c_int)]),
+        "ora_shape_cubic": (None, [C.c_double, D, D, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "ora_set_plasma_source": (C.c_int, [P, P]),
         "ora_load_plasma": (C.c_int, [P, C.c_int]),
         "ora_build_ionization_table": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, D, D]),

@@ -47,12 +47,14 @@ def test_shapes_partition_of_unity():
         assert abs(sum(ax) - 1.0) < 1e-15
 
 
-@pytest.mark.parametrize("ndim", [2, 3])
-def test_esirkepov_discrete_continuity(ndim):
+@pytest.mark.parametrize("ndim,shape", [(2, 0), (3, 0), (2, 1), (3, 1)])
+def test_esirkepov_discrete_continuity(ndim, shape):
     """rho^1 - rho^0 + c * (J(i) - J(i-1)) summed over axes = 0 at round-off,
     c = 1/2 in 2D and 1/3 in 3D (the djc normalisation,
-    src/start/set_init_param.f90:92-103)."""
+    src/start/set_init_param.f90:92-103); quadratic (the reference) and the
+    cubic extension, each with its own density."""
     p = small_case(ndim, nx=16, ny=16, nz=16, cap=10)
+    p.shape = shape
     o = Oracle(p)
     rng = np.random.default_rng(7 + ndim)
     shape = (o.n1p, o.n2p, o.n3p)
@@ -71,6 +73,23 @@ def test_esirkepov_discrete_continuity(ndim):
         div = sum(jc[..., a] - np.roll(jc[..., a], 1, axis=a) for a in range(ndim))
         res = (r1 - r0) + cfac * div
         assert np.abs(res).max() < 1e-14 * max(1.0, abs(float(w)))
+
+
+def test_cubic_shapes_partition_of_unity_and_symmetry():
+    """Cubic B-spline weights (the cden weights) and the quadratic half-node
+    weights sum to one; the cubic weights are the B-spline of the distance
+    to each node, so mirroring the offset mirrors the weights."""
+    lib = load()
+    a4 = (C.c_double * 4)()
+    ah = (C.c_double * 3)()
+    ix, ih = C.c_int(), C.c_int()
+    for x in np.linspace(0.0, 9.999, 401):
+        lib.ora_shape_cubic(float(x), a4, ah, C.byref(ix), C.byref(ih))
+        assert abs(sum(a4) - 1.0) < 1e-15 and abs(sum(ah) - 1.0) < 1e-15
+        s = 3.0 + x - ix.value
+        bs = lambda d: (2 - abs(d)) ** 3 / 6 if abs(d) >= 1 else 2 / 3 - d * d + abs(d) ** 3 / 2
+        for q in range(4):
+            assert abs(a4[q] - bs(s + 1 - q)) < 1e-14
 
 
 def test_boris_pure_magnetic_field_conserves_momentum():
