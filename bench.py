@@ -53,6 +53,11 @@ WORKLOADS = {
     "lwfa2d_1024x256_ppc4": dict(ndim=2, nx=1024, ny=256, nz=1, k0=25.0, yx_rat=4.0, zx_rat=1.0,
                                  cfl=0.8, ppc=(2, 2, 1), n_over_nc=0.01, a0=2.0, w0=5 * LAM0,
                                  tau=10 * LAM0, x_plasma=20 * LAM0, xc_frac=0.3),
+    # the same 3D workload with the cubic shape extension (the reference
+    # gathers and deposits with quadratic shapes only)
+    "lwfa3d_1024x256x256_ppc8_cubic": dict(ndim=3, nx=1024, ny=256, nz=256, k0=25.0, yx_rat=5.0, zx_rat=5.0,
+                                          cfl=0.8, ppc=(2, 2, 2), n_over_nc=0.005, a0=3.0, w0=6 * LAM0,
+                                          tau=10 * LAM0, x_plasma=0.0, xc_frac=0.7, shape=1),
     # small 3D cases for quick checks and profiler captures
     "lwfa3d_128x64x64_ppc8": dict(ndim=3, nx=128, ny=64, nz=64, k0=25.0, yx_rat=5.0, zx_rat=5.0,
                                  cfl=0.8, ppc=(2, 2, 2), n_over_nc=0.005, a0=3.0, w0=6 * LAM0,
@@ -198,7 +203,7 @@ def make_workload(name: str, precision: int, cap_factor: float = 1.04):
     ppc = w["ppc"][0] * w["ppc"][1] * (w["ppc"][2] if w["ndim"] == 3 else 1)
     ncell = w["nx"] * w["ny"] * (w["nz"] if w["ndim"] == 3 else 1)
     cap = int(ncell * ppc * cap_factor) + 4096
-    p = make_params(g, precision=precision, capacity=(cap, 0, 0, 0), w_sh=10, w_speed=1.0)
+    p = make_params(g, precision=precision, capacity=(cap, 0, 0, 0), w_sh=10, w_speed=1.0, shape=w.get("shape", 0))
     lx = w["nx"] * p.dx
     las = laser(w["a0"], LAM0, w["w0"], w["tau"], xc=w["xc_frac"] * lx, xf=w["xc_frac"] * lx)
     n0 = n_over_nc_to_n0(w["n_over_nc"], LAM0)
@@ -540,8 +545,10 @@ def main(argv=None):
         return bench_scan(a, torch)
     w = WORKLOADS[a.workload]
     ppc_w = w["ppc"][0] * w["ppc"][1] * (w["ppc"][2] if w["ndim"] == 3 else 1)
+    shapes = ("cubic on integer nodes, quadratic on half nodes, cubic Esirkepov (extension)" if w.get("shape", 0)
+              else "quadratic/linear staggered (reference qlh + Esirkepov)")
     config = {"workload": a.workload, "grid": [w["nx"], w["ny"], w["nz"]], "ppc": ppc_w,
-              "shapes": "quadratic/linear staggered (reference qlh + Esirkepov)", "window": "moving, w_sh=10",
+              "shapes": shapes, "window": "moving, w_sh=10",
               "l2": "inputs larger than L2 (particle arrays of tens of GB)", "replicas": world}
     metric = "particle-pushes/s"
 
@@ -628,7 +635,7 @@ def main(argv=None):
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
                          "bytes_per_push": bpp,
                          "traffic": (K32_DRAM_BYTES_PER_PUSH * tm.pushes / max(1, tm.launches_push_deposit)
-                                     if w["ndim"] == 3 and ppc_w == 8 else None),
+                                     if w["ndim"] == 3 and ppc_w == 8 and not w.get("shape", 0) else None),
                          "traffic_note": "ncu dram bytes per particle of a small capture, scaled to the launch"},
             "phase_ms_per_step": {"push_deposit": tm.ms_push_deposit / a.steps, "yee": tm.ms_yee / a.steps,
                                   "sort_compact": tm.ms_sort / a.steps, "window": tm.ms_window / a.steps},
