@@ -163,6 +163,7 @@ SIGNATURES = {
     "agpu_beam_potential": (C.c_int, [_P, _D, _D, C.c_double]),
     "agpu_set_deferred_counts": (C.c_int, [_P, C.c_int32]),
     "agpu_set_step_graphs": (C.c_int, [_P, C.c_int32]),
+    "agpu_set_fused_yee": (C.c_int, [_P, C.c_int32]),
     "agpu_batch_create": (C.c_int, [_P, C.c_int32, C.POINTER(_P)]),
     "agpu_batch_destroy": (C.c_int, [_P]),
     "agpu_batch_size": (C.c_int, [_P, C.POINTER(C.c_int32)]),

@@ -41,7 +41,7 @@ UNITS = [
     ("agpu_batch.cpp", ["-Xcompiler", "-pthread"]),
 ]
 HEADERS = ["agpu_common.cuh", "agpu_kernels.h", "agpu_util.h", "agpu_yee.cuh", "agpu_ionz.h", "agpu_bin.cuh",
-           "agpu_tile.h", "agpu_select.cuh", "agpu_beam.h", "agpu_multi.h"]
+           "agpu_tile.h", "agpu_select.cuh", "agpu_beam.h", "agpu_multi.h", "agpu_yee_fused.cuh"]
 
 
 def _mtime(p: str) -> float:

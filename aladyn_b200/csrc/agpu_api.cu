@@ -55,6 +55,9 @@ struct agpu_handle {
   bool fp32 = false;
   // FP64 form
   double* ebf = nullptr;
+  double* ebf_alt = nullptr;  // the fused Yee step's output, swapped with ebf
+  float* ebf32_alt = nullptr;
+  bool fused_yee = true;
   double* jc = nullptr;
   double* part[4] = {nullptr, nullptr, nullptr, nullptr};
   double* tmp = nullptr;  // compaction target, cap_max * ndv
@@ -177,6 +180,8 @@ int free_all(agpu_handle* h) {
   for (int i = 0; i < 4; ++i) cudaFree(h->part[i]);
   cudaFree(h->tmp);
   cudaFree(h->ebf32);
+  cudaFree(h->ebf_alt);
+  cudaFree(h->ebf32_alt);
   cudaFree(h->jhi);
   cudaFree(h->jlo);
   auto freesp = [](Species32& s) {
@@ -853,11 +858,13 @@ int agpu_create(const agpu_params* params, agpu_handle** out) {
   if (!rc) {
     if (!h->fp32) {
       rc |= dmalloc((void**)&h->ebf, sizeof(double) * g.ncell * g.nf);
+      rc |= dmalloc((void**)&h->ebf_alt, sizeof(double) * g.ncell * g.nf);
       rc |= dmalloc((void**)&h->jc, sizeof(double) * g.ncell * g.nc);
       for (int ic = 0; ic < p.nsp && !rc; ++ic) rc |= dmalloc((void**)&h->part[ic], sizeof(double) * capmax * h->ndv);
       if (!rc) rc |= dmalloc((void**)&h->tmp, sizeof(double) * capmax * h->ndv);
     } else {
       rc |= dmalloc((void**)&h->ebf32, sizeof(float) * g.ncell * g.nf);
+      rc |= dmalloc((void**)&h->ebf32_alt, sizeof(float) * g.ncell * g.nf);
       rc |= dmalloc((void**)&h->jhi, sizeof(float) * g.ncell * g.nc);
       rc |= dmalloc((void**)&h->jlo, sizeof(float) * g.ncell * g.nc);
       for (int ic = 0; ic < p.nsp && !rc; ++ic) rc |= alloc_species32(h->sp[ic], capmax, p.ndim);
@@ -1507,20 +1514,33 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
   // curr_mpi_collect -> jc_xyzbd (djc folded into the E update)
   ph_begin(h, PH_YEE);
   YeeC c = yee_coef(p);
+  // the fused step writes a second field array (its tiles read halos of the
+  // input); not inside step graphs, whose launches keep their pointers
+  const bool fused = h->fused_yee && !h->use_graph;
   if (h->fp32) {
     Dev32 d{h->g, h->ebf32, h->jhi, h->jlo};
     jfold32(d, h->st, h->sms);
-    yee32(d, c, h->st, h->sms);
+    if (fused) {
+      yee32_fused(h->ebf32, h->ebf32_alt, h->jhi, h->jlo, h->g, c, h->st);
+      std::swap(h->ebf32, h->ebf32_alt);
+    } else {
+      yee32(d, c, h->st, h->sms);
+    }
   } else {
     Dev64 d{h->g, h->ebf, h->jc};
     jfold64(d, h->st, h->sms);
-    yee64(d, c, h->st, h->sms);
+    if (fused) {
+      yee64_fused(h->ebf, h->ebf_alt, h->jc, h->g, c, h->st);
+      std::swap(h->ebf, h->ebf_alt);
+    } else {
+      yee64(d, c, h->st, h->sms);
+    }
   }
   CK(cudaGetLastError());
   ph_end(h, PH_YEE);
   h->timers.launches_yee += 1;
-  // current fold (x, y[, z] faces; hi and lo in the split form) + 6 Yee kernels
-  h->timers.launches_total += ((p.ndim == 3) ? 3 : 2) * (h->fp32 ? 2 : 1) + 6;
+  // current fold (x, y[, z] faces; hi and lo in the split form) + the Yee kernels
+  h->timers.launches_total += ((p.ndim == 3) ? 3 : 2) * (h->fp32 ? 2 : 1) + (fused ? 1 : 6);
   h->timers.yee_cells += (long long)p.nx * p.ny * (p.ndim == 3 ? p.nz : 1);
   // lp_run: moving window
   if (p.w_speed > 0.0 && p.w_sh > 0) {
@@ -1762,6 +1782,12 @@ int agpu_set_sort_interval(agpu_handle* h, int32_t steps) {
   h->sort_interval = steps;
   return 0;
 }
+int agpu_set_fused_yee(agpu_handle* h, int32_t on) {
+  if (!h) return AGPU_E_ARG;
+  h->fused_yee = on != 0;
+  return 0;
+}
+
 int agpu_set_deterministic(agpu_handle* h, int32_t on) {
   if (!h) return AGPU_E_ARG;
   // the per-particle FP32 kernel has the quadratic shapes only

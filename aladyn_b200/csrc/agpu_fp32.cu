@@ -10,6 +10,7 @@
 #include "agpu_kernels.h"
 #include "agpu_multi.h"
 #include "agpu_yee.cuh"
+#include "agpu_yee_fused.cuh"
 
 namespace agpu {
 
@@ -19,6 +20,10 @@ void jfold32(const Dev32& d, cudaStream_t st, int sms) {
   jfold_t<float>(d.jlo, d.g, st, sms);
 }
 void yee32(const Dev32& d, const YeeC& c, cudaStream_t st, int sms) { yee_t<float>(d.ebf, d.jhi, d.jlo, d.g, c, st, sms); }
+void yee32_fused(const float* fin, float* fout, const float* jhi, const float* jlo, const Geo& g, const YeeC& c,
+                 cudaStream_t st) {
+  yee_fused_t<float>(fin, fout, jhi, jlo, g, c, st);
+}
 
 // Compensated accumulation: hi += v with the rounding error of that add
 // (Knuth TwoSum on the value the atomic saw) added into lo.

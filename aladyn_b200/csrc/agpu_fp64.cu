@@ -8,6 +8,7 @@
 #include "agpu_common.cuh"
 #include "agpu_kernels.h"
 #include "agpu_yee.cuh"
+#include "agpu_yee_fused.cuh"
 
 namespace agpu {
 
@@ -705,6 +706,9 @@ void jfold64(const Dev64& d, cudaStream_t st, int sms) { jfold_t<double>(d.jc, d
 
 void yee64(const Dev64& d, const YeeC& c, cudaStream_t st, int sms) {
   yee_t<double>(d.ebf, d.jc, (const double*)nullptr, d.g, c, st, sms);
+}
+void yee64_fused(const double* fin, double* fout, const double* jc, const Geo& g, const YeeC& c, cudaStream_t st) {
+  yee_fused_t<double>(fin, fout, jc, (const double*)nullptr, g, c, st);
 }
 
 // ============================================================================

@@ -60,6 +60,8 @@ void field_bd64(const Dev64& d, cudaStream_t st, int sms);
 void push_deposit64(const PushArgs64& a, cudaStream_t st, int sms, bool serial);
 void jfold64(const Dev64& d, cudaStream_t st, int sms);
 void yee64(const Dev64& d, const YeeC& c, cudaStream_t st, int sms);
+// the whole leapfrog step in one z-streaming kernel, fin -> fout (fout != fin)
+void yee64_fused(const double* fin, double* fout, const double* jc, const Geo& g, const YeeC& c, cudaStream_t st);
 __global__ void k64_ion_efield(IonArgs64 a);
 __global__ void k64_ionize(IonArgs64 a);
 
@@ -122,5 +124,7 @@ void field_bd32(const Dev32& d, cudaStream_t st, int sms);
 void push_deposit32(const PushArgs32& a, cudaStream_t st, int sms);
 void jfold32(const Dev32& d, cudaStream_t st, int sms);
 void yee32(const Dev32& d, const YeeC& c, cudaStream_t st, int sms);
+void yee32_fused(const float* fin, float* fout, const float* jhi, const float* jlo, const Geo& g, const YeeC& c,
+                 cudaStream_t st);
 
 }  // namespace agpu

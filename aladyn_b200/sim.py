@@ -210,6 +210,9 @@ class PicDevice:
     def set_deferred_counts(self, on: bool = True):
         check(self.lib.agpu_set_deferred_counts(self.h, 1 if on else 0), "agpu_set_deferred_counts")
 
+    def set_fused_yee(self, on: bool = True):
+        check(self.lib.agpu_set_fused_yee(self.h, 1 if on else 0), "agpu_set_fused_yee")
+
     def set_step_graphs(self, on: bool = True):
         check(self.lib.agpu_set_step_graphs(self.h, 1 if on else 0), "agpu_set_step_graphs")
 

@@ -357,6 +357,12 @@ int agpu_set_deferred_counts(agpu_handle* h, int32_t on);
  * plain step capture again.  Saves the per-kernel launch cost of small
  * grids; the work done is the same. */
 int agpu_set_step_graphs(agpu_handle* h, int32_t on);
+/* The leapfrog Yee update (with its Mur boundaries) as one z-streaming
+ * kernel writing a second field array (on, the default), or as the six
+ * separate sweeps and face kernels (off).  Same results; the fused kernel
+ * reads and writes each field word once.  Step graphs use the separate
+ * kernels. */
+int agpu_set_fused_yee(agpu_handle* h, int32_t on);
 /* Sort interval in steps for the tile sort (0 = never). */
 int agpu_set_sort_interval(agpu_handle* h, int32_t steps);
 /* sizeof of agpu_params, agpu_plasma, agpu_laser, agpu_step_out,
