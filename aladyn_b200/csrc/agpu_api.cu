@@ -57,7 +57,7 @@ struct agpu_handle {
   double* ebf = nullptr;
   double* ebf_alt = nullptr;  // the fused Yee step's output, swapped with ebf
   float* ebf32_alt = nullptr;
-  bool fused_yee = true;
+  bool fused_yee = false;  // measured: the separate sweeps are faster in 3D
   double* jc = nullptr;
   double* part[4] = {nullptr, nullptr, nullptr, nullptr};
   double* tmp = nullptr;  // compaction target, cap_max * ndv

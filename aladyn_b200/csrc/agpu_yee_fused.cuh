@@ -1,7 +1,7 @@
 // agpu_yee_fused.cuh — the whole leapfrog Yee step (A14: ef_bds(0), rote(dt/2),
 // bf_bds(dt), rotb + current(dt), ef_bds(dt), rote(dt/2), the order of
 // advance_lpf_fields, src/fields/curr_and_fields_util.f90:176-260) in one
-// kernel that streams along z.
+// kernel that streams along z (in chunks of YF_KC planes per CTA).
 //
 // Each CTA owns a column tile (TX x TY nodes of the full (n1p, n2p) plane) and
 // writes every node of its columns, k = 1..n3p, into a second field array:
@@ -28,9 +28,10 @@ namespace agpu {
 constexpr int YF_TX = 32, YF_TY = 8;
 constexpr int YF_RW = YF_TX + 9, YF_RH = YF_TY + 3;  // region x: X0-4 .. X0+TX+4, y: Y0-1 .. Y0+TY+1
 constexpr int YF_RP = YF_RW * YF_RH;
+constexpr int YF_KC = 4;  // output planes per CTA along z (blockIdx.z = chunk)
 
 template <typename T, int NDIM>
-__global__ void __launch_bounds__(256) k_yee_fused(const T* __restrict__ fin, T* __restrict__ fout,
+__global__ void __launch_bounds__(256, 6) k_yee_fused(const T* __restrict__ fin, T* __restrict__ fout,
                                                    const T* __restrict__ jc, const T* __restrict__ jlo, Geo g,
                                                    YeeC c) {
   extern __shared__ unsigned char yf_smem[];
@@ -70,8 +71,15 @@ __global__ void __launch_bounds__(256) k_yee_fused(const T* __restrict__ fin, T*
       for (int cc = 0; cc < nf; ++cc) fout[cc * nc3 + o] = fin[cc * nc3 + o];
     }
   };
-  for (int k = 1; k < kz1 - 1; ++k) copy_plane(k);
-  for (int k = kz2 + 2; k <= g.n3p; ++k) copy_plane(k);
+  // this CTA's interior output planes c0..c1 (3D)
+  const int c0 = kz1 + blockIdx.z * YF_KC;
+  const int c1 = min(kz2, c0 + YF_KC - 1);
+  if (NDIM == 3 || blockIdx.z == 0) {
+    if (c0 == kz1)
+      for (int k = 1; k < kz1 - 1; ++k) copy_plane(k);
+    if (c1 == kz2)
+      for (int k = kz2 + 2; k <= g.n3p; ++k) copy_plane(k);
+  }
 
   // ---- load plane k into E slot se / B slot sb, then its first ef_bds faces --
   auto load_plane = [&](int k, int se, int sb) {
@@ -256,18 +264,30 @@ __global__ void __launch_bounds__(256) k_yee_fused(const T* __restrict__ fin, T*
     finish_plane(1, 0, 0, 0);
     return;
   }
-  // planes kz1-1 (its E and B are outputs, B gets bf_bds's z-face), kz1, kz1+1
-  load_plane(kz1 - 1, slot(kz1 - 1), slot(kz1 - 1));
-  load_plane(kz1, slot(kz1), slot(kz1));
-  load_plane(kz1 + 1, slot(kz1 + 1), slot(kz1 + 1));
+  // planes c0-1, c0, c0+1.  Plane kz1-1 is an output of the first chunk (B
+  // gets bf_bds's z-face); for a later chunk, plane c0-1 belongs to the chunk
+  // below and its B1/2 (with its faces) is recomputed here.
+  load_plane(c0 - 1, slot(c0 - 1), slot(c0 - 1));
+  load_plane(c0, slot(c0), slot(c0));
+  load_plane(c0 + 1, slot(c0 + 1), slot(c0 + 1));
   __syncthreads();
-  ef_faces(kz1, slot(kz1), slot(kz1), slot(kz1), aphx0, aphy0);
-  if (kz1 + 1 <= kz2)
-    ef_faces(kz1 + 1, slot(kz1 + 1), slot(kz1 + 1), slot(kz1 + 1), aphx0, aphy0);
+  if (c0 - 1 >= kz1) ef_faces(c0 - 1, slot(c0 - 1), slot(c0 - 1), slot(c0 - 1), aphx0, aphy0);
+  ef_faces(c0, slot(c0), slot(c0), slot(c0), aphx0, aphy0);
+  if (c0 + 1 <= kz2)
+    ef_faces(c0 + 1, slot(c0 + 1), slot(c0 + 1), slot(c0 + 1), aphx0, aphy0);
   else
-    ef_zface(slot(kz1 + 1), slot(kz1), slot(kz1), aphz0);
+    ef_zface(slot(c0 + 1), slot(c0), slot(c0), aphz0);
   __syncthreads();
-  for (int m = kz1; m <= kz2; ++m) {
+  if (c0 - 1 >= kz1) {
+    const int sp = slot(c0 - 1);
+    rote(c0 - 1, sp, slot(c0), sp, r_aph1, r_aph2, r_sdhy, r_sdhz, 1, YF_RW - 3, 0, YF_RH - 2);
+    __syncthreads();
+    bf_faces(c0 - 1, sp, sp);
+    __syncthreads();
+  }
+  // the last plane whose En this CTA needs: c1 + 1 (or the top face plane)
+  const int mlast = (c1 == kz2) ? kz2 : c1 + 1;
+  for (int m = c0; m <= mlast; ++m) {
     const int sm = slot(m), su = slot(m + 1), sd = slot(m - 1);
     rote(m, sm, su, sm, r_aph1, r_aph2, r_sdhy, r_sdhz, 1, YF_RW - 3, 0, YF_RH - 2);  // B1/2(m)
     __syncthreads();
@@ -278,9 +298,11 @@ __global__ void __launch_bounds__(256) k_yee_fused(const T* __restrict__ fin, T*
     __syncthreads();
     ef_faces(m, sm, sm, sm, aphx1, aphy1);
     __syncthreads();
-    finish_plane(m - 1, sd, sm, sd);  // B_new(m-1) and the outputs of plane m-1
-    __syncthreads();
-    if (m + 2 <= kz2 + 1) {  // plane m+2 into the slot of m-1
+    if ((m - 1 >= c0 || m - 1 == kz1 - 1) && m - 1 <= c1) {
+      finish_plane(m - 1, sd, sm, sd);  // B_new(m-1) and the outputs of plane m-1
+      __syncthreads();
+    }
+    if (m + 2 <= mlast + 1) {  // plane m+2 into the slot of m-1
       load_plane(m + 2, sd, sd);
       __syncthreads();
       if (m + 2 <= kz2)
@@ -290,17 +312,20 @@ __global__ void __launch_bounds__(256) k_yee_fused(const T* __restrict__ fin, T*
       __syncthreads();
     }
   }
-  const int s2 = slot(kz2), s3 = slot(kz2 + 1);
-  ef_zface(s3, s2, s2, aphz1);  // the second ef_bds z-face, from En(kz2) and B1/2(kz2)
-  __syncthreads();
-  finish_plane(kz2, s2, s3, s2);
-  finish_plane(kz2 + 1, s3, s3, s3);
+  if (c1 == kz2) {
+    const int s2 = slot(kz2), s3 = slot(kz2 + 1);
+    ef_zface(s3, s2, s2, aphz1);  // the second ef_bds z-face, from En(kz2) and B1/2(kz2)
+    __syncthreads();
+    finish_plane(kz2, s2, s3, s2);
+    finish_plane(kz2 + 1, s3, s3, s3);
+  }
 }
 
 // fout = the fields after one leapfrog step of fin (fout != fin)
 template <typename T>
 void yee_fused_t(const T* fin, T* fout, const T* jc, const T* jlo, const Geo& g, const YeeC& c, cudaStream_t st) {
-  dim3 grid((g.n1p + YF_TX - 1) / YF_TX, (g.n2p + YF_TY - 1) / YF_TY);
+  const int nchunk = (g.ndim == 3) ? (g.kz2 - g.kz1 + 1 + YF_KC - 1) / YF_KC : 1;
+  dim3 grid((g.n1p + YF_TX - 1) / YF_TX, (g.n2p + YF_TY - 1) / YF_TY, nchunk);
   const size_t sm = sizeof(T) * 18 * YF_RP;
   if (g.ndim == 3) {
     cudaFuncSetAttribute(k_yee_fused<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

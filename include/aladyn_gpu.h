@@ -358,9 +358,11 @@ int agpu_set_deferred_counts(agpu_handle* h, int32_t on);
  * grids; the work done is the same. */
 int agpu_set_step_graphs(agpu_handle* h, int32_t on);
 /* The leapfrog Yee update (with its Mur boundaries) as one z-streaming
- * kernel writing a second field array (on, the default), or as the six
- * separate sweeps and face kernels (off).  Same results; the fused kernel
- * reads and writes each field word once.  Step graphs use the separate
+ * kernel writing a second field array (on), or as the six separate sweeps
+ * and face kernels (off, the default).  Same results (bit for bit in FP64);
+ * the fused kernel moves each field word once, but with one column tile and
+ * a few planes per CTA it is latency bound and on a B200 it is slower than
+ * the separate kernels in 3D (faster in 2D).  Step graphs use the separate
  * kernels. */
 int agpu_set_fused_yee(agpu_handle* h, int32_t on);
 /* Sort interval in steps for the tile sort (0 = never). */
