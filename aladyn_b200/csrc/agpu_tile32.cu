@@ -260,78 +260,170 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
     wq(sy, ay0);
     wq(nsx, axn);
     wq(nsy, ayn);
-    float sxh[5], cx[5], syh[5], cy[5];
-    const int ih = mi + 1, jh = mj + 1;
-    esirk1(ax0, axn, ih, sxh, cx);
-    esirk1(ay0, ayn, jh, syh, cy);
-    const int x0 = ih < 1 ? ih : 1, x1 = (ih + 2) > 3 ? ih + 2 : 3;
-    const int y0 = jh < 1 ? jh : 1, y1 = (jh + 2) > 3 ? jh + 2 : 3;
-#pragma unroll
-    for (int u = 0; u < 5; ++u) {
-      cx[u] *= wght;
-      cy[u] *= wght;
-    }
     // local J coordinates of window slot 0 (node i0-2)
     const int lx = i0 - i0t, ly = j0 - j0t;
     int* sJx = sJ;
     int* sJy = sJ + JV;
+    // When no lane of the warp changes cell, every window is slots 1..3 and
+    // the deposit is a fixed 3 x 3 [x 3] loop without predicates; otherwise
+    // each window is compacted to the four slots x0 .. x0+3 that can be
+    // non-zero.  Both forms evaluate the same expressions per node.
+    const bool stay = (mi == 0) && (mj == 0) && (NDIM == 2 || mk == 0);
+    const bool warp_stays = __all_sync(__activemask(), stay);
     if (NDIM == 2) {
-      float wxs[5], wys[5];
+      if (warp_stays) {
+        float cx[3], cy[3], wxs[3], wys[3];  // index s = window slot s+1
+        cx[0] = (-0.f + ax0[0]) - axn[0];
+        cy[0] = (-0.f + ay0[0]) - ayn[0];
+        cx[1] = (cx[0] + ax0[1]) - axn[1];
+        cy[1] = (cy[0] + ay0[1]) - ayn[1];
 #pragma unroll
-      for (int u = 0; u < 5; ++u) {
-        wxs[u] = sxh[u] + ((u >= 1 && u <= 3) ? ax0[u - 1] : 0.f);
-        wys[u] = syh[u] + ((u >= 1 && u <= 3) ? ay0[u - 1] : 0.f);
-      }
+        for (int s = 0; s < 3; ++s) {
+          cx[s] *= wght;
+          cy[s] *= wght;
+          wxs[s] = axn[s] + ax0[s];
+          wys[s] = ayn[s] + ay0[s];
+        }
 #pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        if (v < y0 || v > y1) continue;
+        for (int t = 0; t < 3; ++t) {
+#pragma unroll
+          for (int s = 0; s < 3; ++s) {
+            const int o = lx + 1 + s + JX * (ly + 1 + t);
+            if (s < 2) fx_add(&sJx[o], wys[t] * cx[s], fsc);
+            if (t < 2) fx_add(&sJy[o], wxs[s] * cy[t], fsc);
+          }
+        }
+      } else {
+        float sxh[5], cx[5], syh[5], cy[5];
+        const int ih = mi + 1, jh = mj + 1;
+        esirk1(ax0, axn, ih, sxh, cx);
+        esirk1(ay0, ayn, jh, syh, cy);
+        const int x0 = ih < 1 ? ih : 1, x1 = (ih + 2) > 3 ? ih + 2 : 3;
+        const int y0 = jh < 1 ? jh : 1, y1 = (jh + 2) > 3 ? jh + 2 : 3;
+        float wxs[5], wys[5];
 #pragma unroll
         for (int u = 0; u < 5; ++u) {
-          if (u < x0 || u > x1) continue;
-          int o = lx + u + JX * (ly + v);
-          if (u < x1) fx_add(&sJx[o], wys[v] * cx[u], fsc);
-          if (v < y1) fx_add(&sJy[o], wxs[u] * cy[v], fsc);
+          cx[u] *= wght;
+          cy[u] *= wght;
+          wxs[u] = sxh[u] + ((u >= 1 && u <= 3) ? ax0[u - 1] : 0.f);
+          wys[u] = syh[u] + ((u >= 1 && u <= 3) ? ay0[u - 1] : 0.f);
+        }
+        float cxc[4], cyc[4], wxc[4], wyc[4];  // index s = window slot x0+s (y0+s)
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          cxc[s] = x0 ? cx[s + 1] : cx[s];
+          wxc[s] = x0 ? wxs[s + 1] : wxs[s];
+          cyc[s] = y0 ? cy[s + 1] : cy[s];
+          wyc[s] = y0 ? wys[s + 1] : wys[s];
+        }
+        const int nxw = x1 - x0, nyw = y1 - y0;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          if (t > nyw) continue;
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            if (s > nxw) continue;
+            const int o = lx + x0 + s + JX * (ly + y0 + t);
+            if (s < nxw) fx_add(&sJx[o], wyc[t] * cxc[s], fsc);
+            if (t < nyw) fx_add(&sJy[o], wxc[s] * cyc[t], fsc);
+          }
         }
       }
     } else {
-      float az0[3], azn[3], szh[5], cz[5];
+      float az0[3], azn[3];
       wq(sz, az0);
       wq(nsz, azn);
-      const int kh = mk + 1;
-      esirk1(az0, azn, kh, szh, cz);
-      const int z0 = kh < 1 ? kh : 1, z1 = (kh + 2) > 3 ? kh + 2 : 3;
-      float wx0[5], wx1[5], wy0[5], wy1[5], b0[5], b1[5];
-#pragma unroll
-      for (int u = 0; u < 5; ++u) {
-        float a0x = (u >= 1 && u <= 3) ? ax0[u - 1] : 0.f;
-        float a0y = (u >= 1 && u <= 3) ? ay0[u - 1] : 0.f;
-        wx0[u] = 0.5f * sxh[u] + a0x;  // axh0
-        wx1[u] = sxh[u] + 0.5f * a0x;  // axh1
-        wy0[u] = 0.5f * syh[u] + a0y;  // ayh0
-        wy1[u] = syh[u] + 0.5f * a0y;  // ayh1
-        b0[u] = a0y;                   // old y shape on slots 1..3
-        int m = u - jh;
-        b1[u] = (m == 0) ? ayn[0] : (m == 1) ? ayn[1] : (m == 2) ? ayn[2] : 0.f;  // new y shape
-      }
       int* sJz = sJ + 2 * JV;
-      for (int w = z0; w <= z1; ++w) {
-        const int m0 = w - 1, m1 = w - kh;
-        const float A0 = (m0 == 0) ? az0[0] : (m0 == 1) ? az0[1] : (m0 == 2) ? az0[2] : 0.f;
-        const float A1 = (m1 == 0) ? azn[0] : (m1 == 1) ? azn[1] : (m1 == 2) ? azn[2] : 0.f;
-        const float czw = wght * ((w == 0) ? cz[0] : (w == 1) ? cz[1] : (w == 2) ? cz[2] : (w == 3) ? cz[3] : cz[4]);
-        const int ow = lx + JX * (ly + JY * (k0 - k0t + w));
+      if (warp_stays) {
+        float cx[3], cy[3], cz[3], wx0[3], wx1[3], wy0[3], wy1[3];  // index s = window slot s+1
+        cx[0] = (-0.f + ax0[0]) - axn[0];
+        cy[0] = (-0.f + ay0[0]) - ayn[0];
+        cz[0] = (-0.f + az0[0]) - azn[0];
+        cx[1] = (cx[0] + ax0[1]) - axn[1];
+        cy[1] = (cy[0] + ay0[1]) - ayn[1];
+        cz[1] = (cz[0] + az0[1]) - azn[1];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          if (v < y0 || v > y1) continue;
-          const float wyv = wy0[v] * A0 + wy1[v] * A1;
-          const float cyv = cy[v];
+        for (int s = 0; s < 3; ++s) {
+          cx[s] *= wght;
+          cy[s] *= wght;
+          wx0[s] = 0.5f * axn[s] + ax0[s];
+          wx1[s] = axn[s] + 0.5f * ax0[s];
+          wy0[s] = 0.5f * ayn[s] + ay0[s];
+          wy1[s] = ayn[s] + 0.5f * ay0[s];
+        }
 #pragma unroll
-          for (int u = 0; u < 5; ++u) {
-            if (u < x0 || u > x1) continue;
-            const int o = ow + u + JX * v;
-            if (u < x1) fx_add(&sJx[o], cx[u] * wyv, fsc);
-            if (v < y1) fx_add(&sJy[o], cyv * (wx0[u] * A0 + wx1[u] * A1), fsc);
-            if (w < z1) fx_add(&sJz[o], czw * (wx0[u] * b0[v] + wx1[u] * b1[v]), fsc);
+        for (int r = 0; r < 3; ++r) {
+          const float A0 = az0[r], A1 = azn[r];
+          const float czw = wght * cz[r];
+          const int ow = lx + 1 + JX * (ly + 1 + JY * (k0 - k0t + 1 + r));
+#pragma unroll
+          for (int t = 0; t < 3; ++t) {
+            const float wyv = wy0[t] * A0 + wy1[t] * A1;
+#pragma unroll
+            for (int s = 0; s < 3; ++s) {
+              const int o = ow + s + JX * t;
+              if (s < 2) fx_add(&sJx[o], cx[s] * wyv, fsc);
+              if (t < 2) fx_add(&sJy[o], cy[t] * (wx0[s] * A0 + wx1[s] * A1), fsc);
+              if (r < 2) fx_add(&sJz[o], czw * (wx0[s] * ay0[t] + wx1[s] * ayn[t]), fsc);
+            }
+          }
+        }
+      } else {
+        float sxh[5], cx[5], syh[5], cy[5], szh[5], cz[5];
+        const int ih = mi + 1, jh = mj + 1, kh = mk + 1;
+        esirk1(ax0, axn, ih, sxh, cx);
+        esirk1(ay0, ayn, jh, syh, cy);
+        esirk1(az0, azn, kh, szh, cz);
+        const int x0 = ih < 1 ? ih : 1, x1 = (ih + 2) > 3 ? ih + 2 : 3;
+        const int y0 = jh < 1 ? jh : 1, y1 = (jh + 2) > 3 ? jh + 2 : 3;
+        const int z0 = kh < 1 ? kh : 1, z1 = (kh + 2) > 3 ? kh + 2 : 3;
+        float wx0[5], wx1[5], wy0[5], wy1[5], b0[5], b1[5];
+#pragma unroll
+        for (int u = 0; u < 5; ++u) {
+          cx[u] *= wght;
+          cy[u] *= wght;
+          const float a0x = (u >= 1 && u <= 3) ? ax0[u - 1] : 0.f;
+          const float a0y = (u >= 1 && u <= 3) ? ay0[u - 1] : 0.f;
+          wx0[u] = 0.5f * sxh[u] + a0x;  // axh0
+          wx1[u] = sxh[u] + 0.5f * a0x;  // axh1
+          wy0[u] = 0.5f * syh[u] + a0y;  // ayh0
+          wy1[u] = syh[u] + 0.5f * a0y;  // ayh1
+          b0[u] = a0y;                   // old y shape on slots 1..3
+          b1[u] = syh[u];                // new y shape
+        }
+        // index s = window slot x0+s (y0+s)
+        float cxc[4], wx0c[4], wx1c[4], cyc[4], wy0c[4], wy1c[4], b0c[4], b1c[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          cxc[s] = x0 ? cx[s + 1] : cx[s];
+          wx0c[s] = x0 ? wx0[s + 1] : wx0[s];
+          wx1c[s] = x0 ? wx1[s + 1] : wx1[s];
+          cyc[s] = y0 ? cy[s + 1] : cy[s];
+          wy0c[s] = y0 ? wy0[s + 1] : wy0[s];
+          wy1c[s] = y0 ? wy1[s + 1] : wy1[s];
+          b0c[s] = y0 ? b0[s + 1] : b0[s];
+          b1c[s] = y0 ? b1[s + 1] : b1[s];
+        }
+        const int nxw = x1 - x0, nyw = y1 - y0;
+        for (int w = z0; w <= z1; ++w) {
+          const int m0 = w - 1;
+          const float A0 = (m0 == 0) ? az0[0] : (m0 == 1) ? az0[1] : (m0 == 2) ? az0[2] : 0.f;
+          const float A1 = (w == 0) ? szh[0] : (w == 1) ? szh[1] : (w == 2) ? szh[2] : (w == 3) ? szh[3] : szh[4];
+          const float czw = wght * ((w == 0) ? cz[0] : (w == 1) ? cz[1] : (w == 2) ? cz[2] : (w == 3) ? cz[3] : cz[4]);
+          const int ow = lx + x0 + JX * (ly + y0 + JY * (k0 - k0t + w));
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            if (t > nyw) continue;
+            const float wyv = wy0c[t] * A0 + wy1c[t] * A1;
+            const float cyv = cyc[t];
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+              if (s > nxw) continue;
+              const int o = ow + s + JX * t;
+              if (s < nxw) fx_add(&sJx[o], cxc[s] * wyv, fsc);
+              if (t < nyw) fx_add(&sJy[o], cyv * (wx0c[s] * A0 + wx1c[s] * A1), fsc);
+              if (w < z1) fx_add(&sJz[o], czw * (wx0c[s] * b0c[t] + wx1c[s] * b1c[t]), fsc);
+            }
           }
         }
       }
