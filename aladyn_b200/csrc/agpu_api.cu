@@ -838,6 +838,7 @@ int agpu_create(const agpu_params* params, agpu_handle** out) {
   g.nf = p.nfield;
   g.nc = p.curr_ndim;
   g.ncell = (long long)g.n1p * g.n2p * g.n3p;
+  geo_divisors(g);
   if (h->fp32 && g.ncell >= (1ll << 31)) {
     delete h;
     return AGPU_E_ARG;

@@ -16,10 +16,9 @@ namespace agpu {
 __global__ void k_keys_split(const int* cell, long long np, Geo g, TileGeo t, int* key, int* hist, unsigned int* err) {
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < np; n += (long long)gridDim.x * blockDim.x) {
     int c = cell[n];
-    int i = c % g.n1p + 1;
-    int r = c / g.n1p;
-    int j = r % g.n2p + 1;
-    int k = (g.ndim == 3) ? r / g.n2p + 1 : 3;
+    int i, j, k;
+    cell_split(g, c, i, j, k);
+    if (g.ndim != 3) k = 3;
     int kk = tile_key(t, i, j, k);
     key[n] = kk;
     if (kk == t.ntiles) raise_err(err, AGPU_EBIT_INDEX);  // a record outside the node range

@@ -23,6 +23,17 @@ AGPU_HD int tile_key(const TileGeo& t, int i, int j, int k) {
   return a + t.ntx * (b + t.nty * c);
 }
 
+// tile_key for a kernel compiled for the tile extent (TX, TY, TZ) == (t.tx, t.ty, t.tz).
+template <int TX, int TY, int TZ>
+AGPU_HD int tile_key_c(const TileGeo& t, int i, int j, int k) {
+  unsigned a = (unsigned)(i - 3), b = (unsigned)(j - 3), c = (unsigned)(k - 3);
+  a /= TX;
+  b /= TY;
+  c /= TZ;
+  if (a >= (unsigned)t.ntx || b >= (unsigned)t.nty || c >= (unsigned)t.ntz) return t.ntiles;
+  return (int)a + t.ntx * ((int)b + t.nty * (int)c);
+}
+
 // Warp-aggregated histogram increment of key (all active lanes call it).
 __device__ __forceinline__ void hist_add(int* hist, int key) {
   unsigned int act = __activemask();

@@ -14,7 +14,43 @@
 struct Geo {
   int ndim, n1p, n2p, n3p, ix1, ix2, jy1, jy2, kz1, kz2, nf, nc;
   long long ncell;  // n1p*n2p*n3p
+  uint32_t dm1, dm2;  // div31 multipliers of n1p and n2p (geo_divisors)
+  int ds1, ds2;       // and their shifts
 };
+
+// floor(n / d) for 0 <= n < 2^31 and d >= 2 with one multiply-high
+// (Granlund and Montgomery, PLDI 1994, Theorem 4.2, N = 31): with
+// l = ceil(log2 d) and m = ceil(2^(31+l) / d), m d - 2^(31+l) < d <= 2^l, so
+// floor(n / d) = floor(n m / 2^(31+l)); m < 2^32 for every d >= 2.
+AGPU_HD uint32_t div31(uint32_t n, uint32_t m, int sh) {
+#ifdef __CUDA_ARCH__
+  return __umulhi(n, m) >> sh;
+#else
+  return (uint32_t)(((uint64_t)n * m) >> 32) >> sh;
+#endif
+}
+
+inline void div31_constants(uint32_t d, uint32_t& m, int& sh) {
+  int l = 0;
+  while ((1ull << l) < d) ++l;
+  m = (uint32_t)(((1ull << (31 + l)) + d - 1) / d);
+  sh = l - 1;  // the shift after the high word: 31 + l - 32
+}
+
+// Fills the divisor constants of a Geo whose n1p, n2p are set (both >= 2).
+inline void geo_divisors(Geo& g) {
+  div31_constants((uint32_t)g.n1p, g.dm1, g.ds1);
+  div31_constants((uint32_t)g.n2p, g.dm2, g.ds2);
+}
+
+// Fortran node (i, j, k) of a linear cell index 0 <= c < 2^31 (goff's inverse).
+AGPU_HD void cell_split(const Geo& g, int c, int& i, int& j, int& k) {
+  const uint32_t r = div31((uint32_t)c, g.dm1, g.ds1);
+  const uint32_t q = div31(r, g.dm2, g.ds2);
+  i = c - (int)r * g.n1p + 1;
+  j = (int)r - (int)q * g.n2p + 1;
+  k = (int)q + 1;
+}
 
 // Linear offset of Fortran node (i, j, k) (1-based) in one component.
 AGPU_HD long long goff(const Geo& g, int i, int j, int k) {

@@ -75,10 +75,8 @@ __global__ void __launch_bounds__(256) k32_push_dep(PushArgs32 a) {
   const int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < a.np; n += (long long)gridDim.x * blockDim.x) {
     int c = a.p.cell[n];
-    int i0 = c % g.n1p + 1;
-    int r = c / g.n1p;
-    int j0 = r % g.n2p + 1;
-    int k0 = r / g.n2p + 1;
+    int i0, j0, k0;
+    cell_split(g, c, i0, j0, k0);
     float sx = a.p.ox[n], sy = a.p.oy[n], sz = (NDIM == 3) ? a.p.oz[n] : 0.f;
     float pp[3] = {a.p.px[n], a.p.py[n], (NDIM == 3) ? a.p.pz[n] : 0.f};
     uint64_t sl = a.p.slot[n];
@@ -345,7 +343,8 @@ __global__ void k32_ion_efield(IonArgs32 a) {
   const float* E3 = a.ebf + 2 * g.ncell;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < a.np; n += (long long)gridDim.x * blockDim.x) {
     int c = a.cell[n];
-    int i0 = c % g.n1p + 1, r = c / g.n1p, j0 = r % g.n2p + 1, k0 = (g.ndim == 3) ? r / g.n2p + 1 : 1;
+    int i0, j0, k0;
+    cell_split(g, c, i0, j0, k0);
     float sv[3] = {a.ox[n], a.oy[n], (g.ndim == 3) ? a.oz[n] : 0.f};
     int nd[3] = {i0, j0, k0};
     float w1[3][3], wh[3][3];

@@ -140,6 +140,7 @@ extern "C" int agpu_field_diag_noalloc(const double* d_ebf, int32_t ndim, int32_
   g.nf = (ndim == 3) ? 6 : 3;
   g.nc = (ndim == 3) ? 3 : 2;
   g.ncell = (long long)g.n1p * g.n2p * g.n3p;
+  geo_divisors(g);
   const long long ncells = (long long)nx * ny * (ndim == 3 ? nz : 1);
   const long long nb = (ncells + NA_CELLS_PER_BLOCK - 1) / NA_CELLS_PER_BLOCK;
   if (nb > NA_MAX_BLOCKS) return AGPU_E_CAPACITY;  // more than 2^28 interior cells

@@ -12,9 +12,12 @@
 //      deposit going into shared memory as int32 fixed point with integer
 //      shared atomics (on sm_100a several times the throughput of FP32
 //      shared atomics, and unaffected by lanes that hit the same node); the
-//      tile's scale 2^30 / (max|q w| * particles) bounds every node's sum
-//      below 2^31 (one particle adds at most 1.69 |q w| to a node), and
-//      integer sums make the tile's currents independent of the order,
+//      tile's scale 2^30 / (max|q w| * max(particles, 512)) bounds every
+//      node's sum below 2^31 and every single contribution below 2^22 (one
+//      particle adds at most 1.69 |q w| to a node), so each contribution is
+//      rounded to an integer by one FMA with 1.5 * 2^23 (no conversion
+//      instruction), and integer sums make the tile's currents independent
+//      of the order,
 //   4. flushes the shared currents to the global (hi, lo) pair once, each
 //      fixed-point sum converted exactly to FP64 and split into hi + lo,
 //      with the TwoSum error of each global add accumulated into lo,
@@ -36,8 +39,13 @@ __device__ __forceinline__ void kadd_g(float* hi, float* lo, float v) {
   if (err != 0.f) atomicAdd(lo, err);
 }
 
-// Fixed-point contribution of v at scale sc (|v sc| < 2^31 by construction).
-__device__ __forceinline__ void fx_add(int* a, float v, float sc) { atomicAdd(a, __float2int_rn(v * sc)); }
+// Fixed-point contribution x * y, already in units of the tile's scale and
+// below 2^22 in magnitude by construction: x * y + 1.5 * 2^23, rounded once,
+// lies in [2^23, 2^24) where the float spacing is 1, so its bit pattern minus
+// that of 1.5 * 2^23 is x * y rounded to the nearest integer (ties to even).
+__device__ __forceinline__ void fx_add(int* a, float x, float y) {
+  atomicAdd(a, __float_as_int(__fmaf_rn(x, y, 12582912.f)) - 0x4B400000);
+}
 
 __device__ __forceinline__ void wq(float s, float a[3]) {
   float s2 = s * s;
@@ -114,18 +122,16 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
     if ((threadIdx.x & 31) == 0) atomicMax(&s_wmax, __float_as_uint(wl));
   }
   __syncthreads();
-  const float wtile = __uint_as_float(s_wmax) * (float)(end - beg);
-  float fsc = 1073741824.f / wtile;  // 2^30 / (max|q w| * particles)
+  const float wtile = __uint_as_float(s_wmax) * (float)max(end - beg, 512);
+  float fsc = 1073741824.f / wtile;  // 2^30 / (max|q w| * max(particles, 512))
   if (!(fsc < 1.0e30f)) fsc = 1.0e30f;
 
   const int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
   for (int q = beg + threadIdx.x; q < end; q += blockDim.x) {
     const int p = a.perm[q];
     const int c = a.p.cell[p];
-    const int i0 = c % g.n1p + 1;
-    const int r = c / g.n1p;
-    const int j0 = r % g.n2p + 1;
-    const int k0 = (NDIM == 3) ? r / g.n2p + 1 : 1;
+    int i0, j0, k0;
+    cell_split(g, c, i0, j0, k0);
     float sx = a.p.ox[p], sy = a.p.oy[p], sz = (NDIM == 3) ? a.p.oz[p] : 0.f;
     float pp[3] = {a.p.px[p], a.p.py[p], (NDIM == 3) ? a.p.pz[p] : 0.f};
     const uint64_t sl = a.p.slot[p];
@@ -243,7 +249,7 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
     if (!(pn[0] == pn[0] && pn[1] == pn[1] && pn[2] == pn[2])) raise_err(a.err, AGPU_EBIT_NONFINITE);
     bool keep = inside(i1n, nsx, nx) && inside(j1n, nsy, ny);
     if (NDIM == 3) keep = keep && inside(k1n, nsz, nz);
-    int nkey = keep ? tile_key(a.t, i1n, j1n, (NDIM == 3) ? k1n : 3) : a.t.ntiles;
+    int nkey = keep ? tile_key_c<TX, TY, TZ>(a.t, i1n, j1n, (NDIM == 3) ? k1n : 3) : a.t.ntiles;
     a.key[p] = nkey;
     hist_add(a.hist, nkey);
     if (!keep) continue;
@@ -255,6 +261,7 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
     // (x1 for Jx, y1 for Jy, z1 for Jz), so that slot is not deposited: 54
     // instead of 81 shared atomics (3D) for a particle that stays in its cell.
     const float wght = qc * slot_wgh(sl);
+    const float wsc = wght * fsc;  // charge x weight in fixed-point units
     float ax0[3], ay0[3], axn[3], ayn[3];
     wq(sx, ax0);
     wq(sy, ay0);
@@ -279,8 +286,8 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
         cy[1] = (cy[0] + ay0[1]) - ayn[1];
 #pragma unroll
         for (int s = 0; s < 3; ++s) {
-          cx[s] *= wght;
-          cy[s] *= wght;
+          cx[s] *= wsc;
+          cy[s] *= wsc;
           wxs[s] = axn[s] + ax0[s];
           wys[s] = ayn[s] + ay0[s];
         }
@@ -289,8 +296,8 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
 #pragma unroll
           for (int s = 0; s < 3; ++s) {
             const int o = lx + 1 + s + JX * (ly + 1 + t);
-            if (s < 2) fx_add(&sJx[o], wys[t] * cx[s], fsc);
-            if (t < 2) fx_add(&sJy[o], wxs[s] * cy[t], fsc);
+            if (s < 2) fx_add(&sJx[o], wys[t], cx[s]);
+            if (t < 2) fx_add(&sJy[o], wxs[s], cy[t]);
           }
         }
       } else {
@@ -303,8 +310,8 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
         float wxs[5], wys[5];
 #pragma unroll
         for (int u = 0; u < 5; ++u) {
-          cx[u] *= wght;
-          cy[u] *= wght;
+          cx[u] *= wsc;
+          cy[u] *= wsc;
           wxs[u] = sxh[u] + ((u >= 1 && u <= 3) ? ax0[u - 1] : 0.f);
           wys[u] = syh[u] + ((u >= 1 && u <= 3) ? ay0[u - 1] : 0.f);
         }
@@ -324,8 +331,8 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
           for (int s = 0; s < 4; ++s) {
             if (s > nxw) continue;
             const int o = lx + x0 + s + JX * (ly + y0 + t);
-            if (s < nxw) fx_add(&sJx[o], wyc[t] * cxc[s], fsc);
-            if (t < nyw) fx_add(&sJy[o], wxc[s] * cyc[t], fsc);
+            if (s < nxw) fx_add(&sJx[o], wyc[t], cxc[s]);
+            if (t < nyw) fx_add(&sJy[o], wxc[s], cyc[t]);
           }
         }
       }
@@ -344,8 +351,8 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
         cz[1] = (cz[0] + az0[1]) - azn[1];
 #pragma unroll
         for (int s = 0; s < 3; ++s) {
-          cx[s] *= wght;
-          cy[s] *= wght;
+          cx[s] *= wsc;
+          cy[s] *= wsc;
           wx0[s] = 0.5f * axn[s] + ax0[s];
           wx1[s] = axn[s] + 0.5f * ax0[s];
           wy0[s] = 0.5f * ayn[s] + ay0[s];
@@ -354,7 +361,7 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
           const float A0 = az0[r], A1 = azn[r];
-          const float czw = wght * cz[r];
+          const float czw = wsc * cz[r];
           const int ow = lx + 1 + JX * (ly + 1 + JY * (k0 - k0t + 1 + r));
 #pragma unroll
           for (int t = 0; t < 3; ++t) {
@@ -362,9 +369,9 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
 #pragma unroll
             for (int s = 0; s < 3; ++s) {
               const int o = ow + s + JX * t;
-              if (s < 2) fx_add(&sJx[o], cx[s] * wyv, fsc);
-              if (t < 2) fx_add(&sJy[o], cy[t] * (wx0[s] * A0 + wx1[s] * A1), fsc);
-              if (r < 2) fx_add(&sJz[o], czw * (wx0[s] * ay0[t] + wx1[s] * ayn[t]), fsc);
+              if (s < 2) fx_add(&sJx[o], cx[s], wyv);
+              if (t < 2) fx_add(&sJy[o], cy[t], wx0[s] * A0 + wx1[s] * A1);
+              if (r < 2) fx_add(&sJz[o], czw, wx0[s] * ay0[t] + wx1[s] * ayn[t]);
             }
           }
         }
@@ -380,8 +387,8 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
         float wx0[5], wx1[5], wy0[5], wy1[5], b0[5], b1[5];
 #pragma unroll
         for (int u = 0; u < 5; ++u) {
-          cx[u] *= wght;
-          cy[u] *= wght;
+          cx[u] *= wsc;
+          cy[u] *= wsc;
           const float a0x = (u >= 1 && u <= 3) ? ax0[u - 1] : 0.f;
           const float a0y = (u >= 1 && u <= 3) ? ay0[u - 1] : 0.f;
           wx0[u] = 0.5f * sxh[u] + a0x;  // axh0
@@ -409,7 +416,7 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
           const int m0 = w - 1;
           const float A0 = (m0 == 0) ? az0[0] : (m0 == 1) ? az0[1] : (m0 == 2) ? az0[2] : 0.f;
           const float A1 = (w == 0) ? szh[0] : (w == 1) ? szh[1] : (w == 2) ? szh[2] : (w == 3) ? szh[3] : szh[4];
-          const float czw = wght * ((w == 0) ? cz[0] : (w == 1) ? cz[1] : (w == 2) ? cz[2] : (w == 3) ? cz[3] : cz[4]);
+          const float czw = wsc * ((w == 0) ? cz[0] : (w == 1) ? cz[1] : (w == 2) ? cz[2] : (w == 3) ? cz[3] : cz[4]);
           const int ow = lx + x0 + JX * (ly + y0 + JY * (k0 - k0t + w));
 #pragma unroll
           for (int t = 0; t < 4; ++t) {
@@ -420,9 +427,9 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
             for (int s = 0; s < 4; ++s) {
               if (s > nxw) continue;
               const int o = ow + s + JX * t;
-              if (s < nxw) fx_add(&sJx[o], cxc[s] * wyv, fsc);
-              if (t < nyw) fx_add(&sJy[o], cyv * (wx0c[s] * A0 + wx1c[s] * A1), fsc);
-              if (w < z1) fx_add(&sJz[o], czw * (wx0c[s] * b0c[t] + wx1c[s] * b1c[t]), fsc);
+              if (s < nxw) fx_add(&sJx[o], cxc[s], wyv);
+              if (t < nyw) fx_add(&sJy[o], cyv, wx0c[s] * A0 + wx1c[s] * A1);
+              if (w < z1) fx_add(&sJz[o], czw, wx0c[s] * b0c[t] + wx1c[s] * b1c[t]);
             }
           }
         }

@@ -25,7 +25,12 @@ __device__ __forceinline__ void kadd_gc(float* hi, float* lo, float v) {
   float err = __fadd_rn(__fsub_rn(old, __fsub_rn(s, bp)), __fsub_rn(v, bp));
   if (err != 0.f) atomicAdd(lo, err);
 }
-__device__ __forceinline__ void fx_addc(int* a, float v, float sc) { atomicAdd(a, __float2int_rn(v * sc)); }
+// Fixed-point contribution x * y in units of the tile's scale, below 2^22 in
+// magnitude by construction: rounded to the nearest integer by one FMA with
+// 1.5 * 2^23 (the sum lies in [2^23, 2^24), where the float spacing is 1).
+__device__ __forceinline__ void fx_addc(int* a, float x, float y) {
+  atomicAdd(a, __float_as_int(__fmaf_rn(x, y, 12582912.f)) - 0x4B400000);
+}
 
 // cubic B-spline weights at nodes f-1..f+2, s in [0, 1) from the floor node f
 __device__ __forceinline__ void wcub(float s, float a[4]) {
@@ -126,17 +131,17 @@ __global__ void __launch_bounds__(256, 3) k32c_tile(TileArgs32 a) {
   __syncthreads();
   // one particle adds at most (4/3)|q w| to a node: the scale keeps every
   // node's sum below 2^31
-  float fsc = 1073741824.f / (__uint_as_float(s_wmax) * (float)(end - beg));
+  // 2^30 / (max|q w| * max(particles, 512)): node sums below 2^31 (one
+  // particle adds at most 4/3 |q w| to a node), single contributions below 2^22
+  float fsc = 1073741824.f / (__uint_as_float(s_wmax) * (float)max(end - beg, 512));
   if (!(fsc < 1.0e30f)) fsc = 1.0e30f;
 
   const int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
   for (int q = beg + threadIdx.x; q < end; q += blockDim.x) {
     const int p = a.perm[q];
     const int c = a.p.cell[p];
-    const int i0 = c % g.n1p + 1;
-    const int r = c / g.n1p;
-    const int j0 = r % g.n2p + 1;
-    const int k0 = (NDIM == 3) ? r / g.n2p + 1 : 1;
+    int i0, j0, k0;
+    cell_split(g, c, i0, j0, k0);
     float ox = a.p.ox[p], oy = a.p.oy[p], oz = (NDIM == 3) ? a.p.oz[p] : 0.f;
     float pp[3] = {a.p.px[p], a.p.py[p], (NDIM == 3) ? a.p.pz[p] : 0.f};
     const uint64_t sl = a.p.slot[p];
@@ -262,12 +267,12 @@ __global__ void __launch_bounds__(256, 3) k32c_tile(TileArgs32 a) {
     if (!(pn[0] == pn[0] && pn[1] == pn[1] && pn[2] == pn[2])) raise_err(a.err, AGPU_EBIT_NONFINITE);
     bool keep = inside_c(i1n, nox, nx) && inside_c(j1n, noy, ny);
     if (NDIM == 3) keep = keep && inside_c(k1n, noz, nz);
-    int nkey = keep ? tile_key(a.t, i1n, j1n, (NDIM == 3) ? k1n : 3) : a.t.ntiles;
+    int nkey = keep ? tile_key_c<TX, TY, TZ>(a.t, i1n, j1n, (NDIM == 3) ? k1n : 3) : a.t.ntiles;
     a.key[p] = nkey;
     hist_add(a.hist, nkey);
     if (!keep) continue;
     // cubic Esirkepov deposit: slot 0 of each window is the old floor node - 2
-    const float wght = qc * slot_wgh(sl);
+    const float wsc = qc * slot_wgh(sl) * fsc;  // charge x weight in fixed-point units
     float s1x, s1y, s1z = 0.f;
     const int gx = floor_of(i1n, nox, &s1x), gy = floor_of(j1n, noy, &s1y);
     const int gz = (NDIM == 3) ? floor_of(k1n, noz, &s1z) : 1;
@@ -283,18 +288,35 @@ __global__ void __launch_bounds__(256, 3) k32c_tile(TileArgs32 a) {
     const int y0 = shy < 1 ? shy : 1, y1 = (shy + 3) > 4 ? shy + 3 : 4;
     int* sJx = sJ;
     int* sJy = sJ + JV;
-    if (NDIM == 2) {
+    // When no lane of the warp changes floor node, every window is slots
+    // 1..4 and the deposit is a fixed 4 x 4 [x 4] loop without predicates
+    // (the same expressions as the general loop).
+    const bool stay = shx == 1 && shy == 1 && (NDIM == 2 || shz == 1);
+    const bool warp_stays = __all_sync(__activemask(), stay);
+    if (NDIM == 2 && warp_stays) {
+#pragma unroll
+      for (int v = 1; v <= 4; ++v) {
+        const float wyv = sy0[v] + sy1[v];
+        const float cyv = wsc * cy[v];
+#pragma unroll
+        for (int u = 1; u <= 4; ++u) {
+          const int o = lx + u + JX * (ly + v);
+          if (u < 4) fx_addc(&sJx[o], wsc * cx[u], wyv);
+          if (v < 4) fx_addc(&sJy[o], sx0[u] + sx1[u], cyv);
+        }
+      }
+    } else if (NDIM == 2) {
 #pragma unroll
       for (int v = 0; v < 6; ++v) {
         if (v < y0 || v > y1) continue;
         const float wyv = sy0[v] + sy1[v];
-        const float cyv = wght * cy[v];
+        const float cyv = wsc * cy[v];
 #pragma unroll
         for (int u = 0; u < 6; ++u) {
           if (u < x0 || u > x1) continue;
           const int o = lx + u + JX * (ly + v);
-          if (u < x1) fx_addc(&sJx[o], (wght * cx[u]) * wyv, fsc);
-          if (v < y1) fx_addc(&sJy[o], (sx0[u] + sx1[u]) * cyv, fsc);
+          if (u < x1) fx_addc(&sJx[o], wsc * cx[u], wyv);
+          if (v < y1) fx_addc(&sJy[o], sx0[u] + sx1[u], cyv);
         }
       }
     } else {
@@ -308,28 +330,48 @@ __global__ void __launch_bounds__(256, 3) k32c_tile(TileArgs32 a) {
         wx1[q2] = sx1[q2] + 0.5f * sx0[q2];
         wy0[q2] = 0.5f * sy1[q2] + sy0[q2];
         wy1[q2] = sy1[q2] + 0.5f * sy0[q2];
-        cx[q2] *= wght;
-        cy[q2] *= wght;
-        cz[q2] *= wght;
+        cx[q2] *= wsc;
+        cy[q2] *= wsc;
+        cz[q2] *= wsc;
       }
       int* sJz = sJ + 2 * JV;
-      for (int w = z0; w <= z1; ++w) {
-        const float A0 = (w == 0) ? sz0[0] : (w == 1) ? sz0[1] : (w == 2) ? sz0[2] : (w == 3) ? sz0[3] : (w == 4) ? sz0[4] : sz0[5];
-        const float A1 = (w == 0) ? sz1[0] : (w == 1) ? sz1[1] : (w == 2) ? sz1[2] : (w == 3) ? sz1[3] : (w == 4) ? sz1[4] : sz1[5];
-        const float czw = (w == 0) ? cz[0] : (w == 1) ? cz[1] : (w == 2) ? cz[2] : (w == 3) ? cz[3] : (w == 4) ? cz[4] : cz[5];
-        const int ow = lx + JX * (ly + JY * (lz + w));
+      if (warp_stays) {
 #pragma unroll
-        for (int v = 0; v < 6; ++v) {
-          if (v < y0 || v > y1) continue;
-          const float wyv = wy0[v] * A0 + wy1[v] * A1;
-          const float cyv = cy[v];
+        for (int w = 1; w <= 4; ++w) {
+          const float A0 = sz0[w], A1 = sz1[w], czw = cz[w];
+          const int ow = lx + JX * (ly + JY * (lz + w));
 #pragma unroll
-          for (int u = 0; u < 6; ++u) {
-            if (u < x0 || u > x1) continue;
-            const int o = ow + u + JX * v;
-            if (u < x1) fx_addc(&sJx[o], cx[u] * wyv, fsc);
-            if (v < y1) fx_addc(&sJy[o], cyv * (wx0[u] * A0 + wx1[u] * A1), fsc);
-            if (w < z1) fx_addc(&sJz[o], czw * (wx0[u] * sy0[v] + wx1[u] * sy1[v]), fsc);
+          for (int v = 1; v <= 4; ++v) {
+            const float wyv = wy0[v] * A0 + wy1[v] * A1;
+            const float cyv = cy[v];
+#pragma unroll
+            for (int u = 1; u <= 4; ++u) {
+              const int o = ow + u + JX * v;
+              if (u < 4) fx_addc(&sJx[o], cx[u], wyv);
+              if (v < 4) fx_addc(&sJy[o], cyv, wx0[u] * A0 + wx1[u] * A1);
+              if (w < 4) fx_addc(&sJz[o], czw, wx0[u] * sy0[v] + wx1[u] * sy1[v]);
+            }
+          }
+        }
+      } else {
+        for (int w = z0; w <= z1; ++w) {
+          const float A0 = (w == 0) ? sz0[0] : (w == 1) ? sz0[1] : (w == 2) ? sz0[2] : (w == 3) ? sz0[3] : (w == 4) ? sz0[4] : sz0[5];
+          const float A1 = (w == 0) ? sz1[0] : (w == 1) ? sz1[1] : (w == 2) ? sz1[2] : (w == 3) ? sz1[3] : (w == 4) ? sz1[4] : sz1[5];
+          const float czw = (w == 0) ? cz[0] : (w == 1) ? cz[1] : (w == 2) ? cz[2] : (w == 3) ? cz[3] : (w == 4) ? cz[4] : cz[5];
+          const int ow = lx + JX * (ly + JY * (lz + w));
+#pragma unroll
+          for (int v = 0; v < 6; ++v) {
+            if (v < y0 || v > y1) continue;
+            const float wyv = wy0[v] * A0 + wy1[v] * A1;
+            const float cyv = cy[v];
+#pragma unroll
+            for (int u = 0; u < 6; ++u) {
+              if (u < x0 || u > x1) continue;
+              const int o = ow + u + JX * v;
+              if (u < x1) fx_addc(&sJx[o], cx[u], wyv);
+              if (v < y1) fx_addc(&sJy[o], cyv, wx0[u] * A0 + wx1[u] * A1);
+              if (w < z1) fx_addc(&sJz[o], czw, wx0[u] * sy0[v] + wx1[u] * sy1[v]);
+            }
           }
         }
       }
