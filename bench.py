@@ -65,6 +65,12 @@ WORKLOADS = {
     "lwfa3d_256x128x128_ppc8": dict(ndim=3, nx=256, ny=128, nz=128, k0=25.0, yx_rat=5.0, zx_rat=5.0,
                                    cfl=0.8, ppc=(2, 2, 2), n_over_nc=0.005, a0=3.0, w0=6 * LAM0,
                                    tau=10 * LAM0, x_plasma=0.0, xc_frac=0.7),
+    # the physical box of lwfa3d_1024x256x256_ppc8 at 3/8 of its resolution:
+    # the same laser-to-box volume fraction with 28e6 particles (profiler
+    # captures of the kernel mix the full-size step sees)
+    "lwfa3d_384x96x96_ppc8": dict(ndim=3, nx=384, ny=96, nz=96, k0=9.375, yx_rat=5.0, zx_rat=5.0,
+                                 cfl=0.8, ppc=(2, 2, 2), n_over_nc=0.005, a0=3.0, w0=6 * LAM0,
+                                 tau=10 * LAM0, x_plasma=0.0, xc_frac=0.7),
 }
 DEFAULT_WORKLOAD = "lwfa3d_1024x256x256_ppc8"
 
@@ -116,9 +122,9 @@ def bytes_per_push(ndim: int, ppc: int, fp32: bool) -> float:
 
 
 # DRAM bytes (read + write) per particle of one k32_tile launch, from an ncu
-# capture of the 128x64x64-cell, 8 ppc workload (295.0 MB for 4.19e6
+# capture of the 384x96x96-cell, 8 ppc workload (2135.7 MB for 2.83e7
 # particles); traffic grows in proportion to the particles of a launch.
-K32_DRAM_BYTES_PER_PUSH = 70.4
+K32_DRAM_BYTES_PER_PUSH = 75.4
 
 
 def yee_bytes_per_cell(ndim: int, fp32: bool) -> float:
