@@ -1714,20 +1714,27 @@ int agpu_beam_inject(agpu_handle* h, int32_t ic, const double* part, int64_t ld,
 int agpu_diag(agpu_handle* h, agpu_diag_out* out) {
   if (!h || !out) return AGPU_E_ARG;
   std::memset(out, 0, sizeof(*out));
-  for (int ic = 0; ic < h->p.nsp; ++ic)
-    if (int rc = drop_removed(h, ic)) return rc;
+  // removed records of a binned species stay stored until the next
+  // compaction: the particle sums run over the alive ones along the tile
+  // permutation instead of compacting (a full copy and a rebinning)
+  if (int rc = refresh_counts(h)) return rc;
   CK(cudaMemsetAsync(h->d_diag, 0, sizeof(double) * 64, h->st));
   double dvol = h->p.dx * h->p.dy * (h->p.ndim == 3 ? h->p.dz : 1.0);
   if (h->fp32)
     field_diag32(h->ebf32, h->g, dvol, h->d_diag, h->d_diag + 6, h->st, h->sms);
   else
     field_diag64(h->ebf, h->g, dvol, h->d_diag, h->d_diag + 6, h->st, h->sms);
+  long long nd_alive[4] = {0, 0, 0, 0};
   for (int ic = 0; ic < h->p.nsp; ++ic) {
     double* o = h->d_diag + 8 + 5 * ic;
+    const bool along = h->binned[ic] && h->nalive[ic] < h->np[ic];
+    const int* perm = along ? h->perm[ic] : nullptr;
+    const long long n = along ? h->nalive[ic] : h->np[ic];
+    nd_alive[ic] = n;
     if (h->fp32)
-      part_diag32(h->sp[ic].view(), h->np[ic], h->p.ndim, o, h->st, h->sms);
+      part_diag32(h->sp[ic].view(), n, h->p.ndim, perm, o, h->st, h->sms);
     else
-      part_diag64(h->part[ic], h->cap[ic], h->np[ic], h->p.ndim, o, h->st, h->sms);
+      part_diag64(h->part[ic], h->cap[ic], n, h->p.ndim, perm, o, h->st, h->sms);
   }
   CK(cudaGetLastError());
   double hd[64];
@@ -1740,7 +1747,7 @@ int agpu_diag(agpu_handle* h, agpu_diag_out* out) {
     out->kin_energy[ic] = o[0];
     out->charge[ic] = o[1];
     for (int c = 0; c < 3; ++c) out->momentum[ic][c] = o[2 + c];
-    out->np[ic] = h->np[ic];
+    out->np[ic] = nd_alive[ic];
   }
   return 0;
 }

@@ -478,10 +478,13 @@ void field_diag32(const float* ebf, const Geo& g, double dvol, double* out_e, do
   k_field_diag<float><<<grid_for(cells, 256, sms, 8), 256, 0, st>>>(ebf, g, g.nf, dvol, out_e, out_max);
 }
 
-// out[0] = sum w (gamma-1), out[1] = sum charge*w, out[2..4] = sum w p
-__global__ void k_part_diag64(const double* part, long long ld, long long n, int nd, double* out) {
+// out[0] = sum w (gamma-1), out[1] = sum charge*w, out[2..4] = sum w p over
+// the records q < n, or over records perm[q], q < n, when perm is given (the
+// alive records of a binned species, removed ones still stored)
+__global__ void k_part_diag64(const double* part, long long ld, long long n, int nd, const int* perm, double* out) {
   double a[5] = {0, 0, 0, 0, 0};
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+  for (long long qq = blockIdx.x * (long long)blockDim.x + threadIdx.x; qq < n; qq += (long long)gridDim.x * blockDim.x) {
+    const long long q = perm ? (long long)perm[qq] : qq;
     double p2 = 0.0, pv[3] = {0, 0, 0};
     for (int c = 0; c < nd; ++c) {
       pv[c] = part[(long long)(nd + c) * ld + q];
@@ -499,13 +502,15 @@ __global__ void k_part_diag64(const double* part, long long ld, long long n, int
     if ((threadIdx.x & 31) == 0) atomicAdd(&out[c], v);
   }
 }
-void part_diag64(const double* part, long long ld, long long n, int nd, double* out, cudaStream_t st, int sms) {
+void part_diag64(const double* part, long long ld, long long n, int nd, const int* perm, double* out, cudaStream_t st,
+                 int sms) {
   if (n <= 0) return;
-  k_part_diag64<<<grid_for(n, 256, sms, 8), 256, 0, st>>>(part, ld, n, nd, out);
+  k_part_diag64<<<grid_for(n, 256, sms, 8), 256, 0, st>>>(part, ld, n, nd, perm, out);
 }
-__global__ void k_part_diag32(Part32View p, long long n, int nd, double* out) {
+__global__ void k_part_diag32(Part32View p, long long n, int nd, const int* perm, double* out) {
   double a[5] = {0, 0, 0, 0, 0};
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+  for (long long qq = blockIdx.x * (long long)blockDim.x + threadIdx.x; qq < n; qq += (long long)gridDim.x * blockDim.x) {
+    const long long q = perm ? (long long)perm[qq] : qq;
     double pv[3] = {(double)p.px[q], (double)p.py[q], nd == 3 ? (double)p.pz[q] : 0.0};
     double p2 = pv[0] * pv[0] + pv[1] * pv[1] + pv[2] * pv[2];
     uint64_t sl = p.slot[q];
@@ -520,9 +525,9 @@ __global__ void k_part_diag32(Part32View p, long long n, int nd, double* out) {
     if ((threadIdx.x & 31) == 0) atomicAdd(&out[c], v);
   }
 }
-void part_diag32(const Part32View& p, long long n, int nd, double* out, cudaStream_t st, int sms) {
+void part_diag32(const Part32View& p, long long n, int nd, const int* perm, double* out, cudaStream_t st, int sms) {
   if (n <= 0) return;
-  k_part_diag32<<<grid_for(n, 256, sms, 8), 256, 0, st>>>(p, n, nd, out);
+  k_part_diag32<<<grid_for(n, 256, sms, 8), 256, 0, st>>>(p, n, nd, perm, out);
 }
 
 // max of a non-negative FP64 array (ion |E|^2), for the lp_max refresh.

@@ -74,8 +74,10 @@ void f32pair_to_f64(const float* hi, const float* lo, double* b, long long n, cu
 void laser64(const LaserArgs& a, double* ebf, const Geo& g, cudaStream_t st, int sms);
 void field_diag64(const double* ebf, const Geo& g, double dvol, double* out_e, double* out_max, cudaStream_t st, int sms);
 void field_diag32(const float* ebf, const Geo& g, double dvol, double* out_e, double* out_max, cudaStream_t st, int sms);
-void part_diag64(const double* part, long long ld, long long n, int nd, double* out, cudaStream_t st, int sms);
-void part_diag32(const Part32View& p, long long n, int nd, double* out, cudaStream_t st, int sms);
+// perm: null (records 0..n-1) or the alive records perm[0..n-1]
+void part_diag64(const double* part, long long ld, long long n, int nd, const int* perm, double* out, cudaStream_t st,
+                 int sms);
+void part_diag32(const Part32View& p, long long n, int nd, const int* perm, double* out, cudaStream_t st, int sms);
 void max_nonneg(const double* a, long long n, double* out, cudaStream_t st, int sms);
 
 }  // namespace agpu
