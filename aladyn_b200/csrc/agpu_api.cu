@@ -94,13 +94,15 @@ struct agpu_handle {
   bool auto_table[4] = {false, false, false, false};
   int nsp_ionz = 1;
   // spatial tiles of the running species: key / perm per particle,
-  // histogram (ntiles+1), tile starts (ntiles+2), scatter cursors
+  // histogram (nkeys+1), key starts (nkeys+2), scatter cursors (nkeys+1) and
+  // the scan's block sums
   TileGeo tg{};
   int* key[4] = {nullptr, nullptr, nullptr, nullptr};
   int* perm[4] = {nullptr, nullptr, nullptr, nullptr};
   int* hist[4] = {nullptr, nullptr, nullptr, nullptr};
   int* tstart[4] = {nullptr, nullptr, nullptr, nullptr};
   int* cursor = nullptr;
+  int* scan_tmp = nullptr;
   bool binned[4] = {false, false, false, false};
   long long nalive[4] = {0, 0, 0, 0};  // np minus removed records still stored
   // deferred counts: tiled steps leave the alive counts and the error word
@@ -213,6 +215,7 @@ int free_all(agpu_handle* h) {
     cudaFree(h->tstart[i]);
   }
   cudaFree(h->cursor);
+  cudaFree(h->scan_tmp);
   for (int i = 0; i < 2 * PH_N; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
@@ -252,7 +255,7 @@ int refresh_counts(agpu_handle* h) {
   if (!any) return 0;
   for (int ic = 0; ic < 4; ++ic)
     if (h->stale[ic])
-      CK(cudaMemcpyAsync(&h->d_cnt->alive4[ic], h->tstart[ic] + h->tg.ntiles, sizeof(int), cudaMemcpyDeviceToDevice,
+      CK(cudaMemcpyAsync(&h->d_cnt->alive4[ic], h->tstart[ic] + h->tg.nkeys, sizeof(int), cudaMemcpyDeviceToDevice,
                          h->st));
   CK(cudaMemcpyAsync(h->h_cnt, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
@@ -384,37 +387,39 @@ bool tiled(const agpu_handle* h, int ic) {
 // Keys from the current positions, histogram, scan and permutation.
 int rebin(agpu_handle* h, int ic) {
   const TileGeo& t = h->tg;
-  CK(cudaMemsetAsync(h->hist[ic], 0, sizeof(int) * (t.ntiles + 1), h->st));
+  CK(cudaMemsetAsync(h->hist[ic], 0, sizeof(int) * (t.nkeys + 1), h->st));
   if (h->fp32)
-    bin_keys_split(h->sp[ic].cell, h->np[ic], h->g, t, h->key[ic], h->hist[ic], &h->d_cnt->err, h->st, h->sms);
+    bin_keys_split(h->sp[ic].cell, h->sp[ic].ox, h->sp[ic].oy, h->sp[ic].oz, h->np[ic], h->g, t, h->key[ic], h->hist[ic],
+                   &h->d_cnt->err, h->st, h->sms);
   else
     bin_keys_abs(h->part[ic], h->part[ic] + h->cap[ic], h->part[ic] + 2 * h->cap[ic], h->np[ic], h->g, t, h->p.xmn, h->p.ymn,
                  h->p.zmn, h->p.dx_inv, h->p.dy_inv, h->p.dz_inv, h->key[ic], h->hist[ic], &h->d_cnt->err, h->st, h->sms);
-  bin_finish(h->key[ic], h->np[ic], t, h->hist[ic], h->tstart[ic], h->cursor, h->perm[ic], h->st, h->sms);
+  const int nl = bin_finish(h->key[ic], h->np[ic], t, h->hist[ic], h->tstart[ic], h->cursor, h->perm[ic], h->scan_tmp,
+                            h->st, h->sms);
   CK(cudaGetLastError());
-  h->timers.launches_total += 3;
+  h->timers.launches_total += (h->np[ic] > 0 ? 1 : 0) + nl;  // keys, scan, scatter
   h->binned[ic] = true;
   if (h->defer) {
     h->stale[ic] = true;
     return 0;
   }
-  CK(cudaMemcpyAsync(&h->d_cnt->alive, h->tstart[ic] + t.ntiles, sizeof(int), cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync(&h->d_cnt->alive, h->tstart[ic] + t.nkeys, sizeof(int), cudaMemcpyDeviceToDevice, h->st));
   if (int rc = read_counters(h)) return rc;
   h->nalive[ic] = h->h_cnt->alive;
   return 0;
 }
 
-// Drop the removed records (key == ntiles) keeping the memory order, so the
+// Drop the removed records (key == nkeys) keeping the memory order, so the
 // stored arrays hold exactly the alive particles; the binning is then stale.
 int drop_removed(agpu_handle* h, int ic) {
   if (int rc = refresh_counts(h)) return rc;
   if (!h->binned[ic] || h->nalive[ic] == h->np[ic]) return 0;
   long long kept;
   if (h->fp32) {
-    kept = compact_flag32(h->key[ic], h->tg.ntiles, h->sp[ic].view(), h->sptmp.view(), h->np[ic], h->scr, h->st);
+    kept = compact_flag32(h->key[ic], h->tg.nkeys, h->sp[ic].view(), h->sptmp.view(), h->np[ic], h->scr, h->st);
     std::swap(h->sp[ic], h->sptmp);
   } else {
-    kept = compact_flag64(h->key[ic], h->tg.ntiles, h->part[ic], h->tmp, h->cap[ic], h->np[ic], h->ndv, h->scr, h->st);
+    kept = compact_flag64(h->key[ic], h->tg.nkeys, h->part[ic], h->tmp, h->cap[ic], h->np[ic], h->ndv, h->scr, h->st);
     std::swap(h->part[ic], h->tmp);
   }
   CK(cudaGetLastError());
@@ -426,7 +431,7 @@ int drop_removed(agpu_handle* h, int ic) {
 }
 
 // Tiled gather + push + deposit of species ic, then the next binning from
-// the keys the kernel wrote.  Removed particles stay stored (key ntiles)
+// the keys the kernel wrote.  Removed particles stay stored (key nkeys)
 // until the next compaction.
 int tiled_push(agpu_handle* h, int ic, int initial_time, agpu_step_out* out) {
   const agpu_params& p = h->p;
@@ -515,15 +520,16 @@ int tiled_push(agpu_handle* h, int ic, int initial_time, agpu_step_out* out) {
   h->timers.launches_total += 2;  // histogram reset + tile kernel
   if (!h->defer) h->timers.pushes += alive0;
   ph_begin(h, PH_SORT);
-  bin_finish(h->key[ic], h->np[ic], h->tg, h->hist[ic], h->tstart[ic], h->cursor, h->perm[ic], h->st, h->sms);
+  const int nl = bin_finish(h->key[ic], h->np[ic], h->tg, h->hist[ic], h->tstart[ic], h->cursor, h->perm[ic], h->scan_tmp,
+                            h->st, h->sms);
   CK(cudaGetLastError());
-  h->timers.launches_total += 2;  // scan + scatter
+  h->timers.launches_total += nl;  // scan + scatter
   if (h->defer) {
     h->stale[ic] = true;
     ph_end(h, PH_SORT);
     return 0;
   }
-  CK(cudaMemcpyAsync(&h->d_cnt->alive, h->tstart[ic] + h->tg.ntiles, sizeof(int), cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync(&h->d_cnt->alive, h->tstart[ic] + h->tg.nkeys, sizeof(int), cudaMemcpyDeviceToDevice, h->st));
   if (int rc = read_counters(h)) return rc;
   ph_end(h, PH_SORT);
   h->nalive[ic] = h->h_cnt->alive;
@@ -877,10 +883,11 @@ int agpu_create(const agpu_params* params, agpu_handle** out) {
     for (int ic = 0; ic < p.nsp_run && !rc; ++ic) {
       rc |= dmalloc((void**)&h->key[ic], sizeof(int) * capmax);
       rc |= dmalloc((void**)&h->perm[ic], sizeof(int) * capmax);
-      rc |= dmalloc((void**)&h->hist[ic], sizeof(int) * (h->tg.ntiles + 1));
-      rc |= dmalloc((void**)&h->tstart[ic], sizeof(int) * (h->tg.ntiles + 2));
+      rc |= dmalloc((void**)&h->hist[ic], sizeof(int) * (h->tg.nkeys + 1));
+      rc |= dmalloc((void**)&h->tstart[ic], sizeof(int) * (h->tg.nkeys + 2));
     }
-    if (!rc) rc |= dmalloc((void**)&h->cursor, sizeof(int) * (h->tg.ntiles + 1));
+    if (!rc) rc |= dmalloc((void**)&h->cursor, sizeof(int) * (h->tg.nkeys + 1));
+    if (!rc) rc |= dmalloc((void**)&h->scan_tmp, sizeof(int) * bin_scan_tmp_ints(h->tg));
     if (capmax >= (1ll << 31)) rc |= AGPU_E_NOMEM;  // int32 particle indices in the permutation
   }
   if (!rc) {

@@ -1,7 +1,8 @@
 // agpu_bin.cu — per-step binning of particles by spatial tile: a key per
-// particle (its tile, or the removed bin), a histogram, an exclusive scan and
-// a scatter of particle indices into the permutation perm, so that tile t's
-// particles are perm[tstart[t] .. tstart[t+1]).  The particle records stay
+// particle (its tile and row inside the tile, or the removed bin), a
+// histogram, an exclusive scan and a scatter of particle indices into the
+// permutation perm, so that tile t's particles are
+// perm[tstart[t * nsub] .. tstart[(t + 1) * nsub]), row by row.  The particle records stay
 // where they are; the permutation is rebuilt every step from the keys that
 // the push kernel writes, and the records are physically reordered along it
 // whenever the window compaction copies them.
@@ -12,16 +13,17 @@
 
 namespace agpu {
 
-// keys from the split form's node index
-__global__ void k_keys_split(const int* cell, long long np, Geo g, TileGeo t, int* key, int* hist, unsigned int* err) {
+// keys from the split form's node index and offsets
+__global__ void k_keys_split(const int* cell, const float* ox, const float* oy, const float* oz, long long np, Geo g,
+                             TileGeo t, int* key, int* hist, unsigned int* err) {
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < np; n += (long long)gridDim.x * blockDim.x) {
     int c = cell[n];
     int i, j, k;
     cell_split(g, c, i, j, k);
     if (g.ndim != 3) k = 3;
-    int kk = tile_key(t, i, j, k);
+    int kk = tile_key(t, i, j, k, offset_octant(ox[n], oy[n], (g.ndim == 3) ? oz[n] : 0.f, g.ndim));
     key[n] = kk;
-    if (kk == t.ntiles) raise_err(err, AGPU_EBIT_INDEX);  // a record outside the node range
+    if (kk == t.nkeys) raise_err(err, AGPU_EBIT_INDEX);  // a record outside the node range
     hist_add(hist, kk);
   }
 }
@@ -36,13 +38,15 @@ __global__ void k_keys_abs(const double* x, const double* y, const double* z, lo
     int i = (xx > -1e9 && xx < 2e9) ? (int)(xx + 0.5) : -1;
     int j = (yy > -1e9 && yy < 2e9) ? (int)(yy + 0.5) : -1;
     int k = 3;
+    float sz = 0.f;
     if (g.ndim == 3) {
       double zz = 3.0 + dzi * (z[n] - zmn);
       k = (zz > -1e9 && zz < 2e9) ? (int)(zz + 0.5) : -1;
+      sz = (float)(zz - (double)k);
     }
-    int kk = tile_key(t, i, j, k);
+    int kk = tile_key(t, i, j, k, offset_octant((float)(xx - (double)i), (float)(yy - (double)j), sz, g.ndim));
     key[n] = kk;
-    if (kk == t.ntiles) raise_err(err, AGPU_EBIT_INDEX);  // a record outside the node range
+    if (kk == t.nkeys) raise_err(err, AGPU_EBIT_INDEX);  // a record outside the node range
     hist_add(hist, kk);
   }
 }
@@ -94,10 +98,10 @@ __global__ void k_perm_scatter(const int* key, long long np, const int* start, i
   d_perm_scatter(key, np, start, cursor, perm, blockIdx.x, gridDim.x);
 }
 
-void bin_keys_split(const int* cell, long long np, const Geo& g, const TileGeo& t, int* key, int* hist, unsigned int* err,
-                    cudaStream_t st, int sms) {
+void bin_keys_split(const int* cell, const float* ox, const float* oy, const float* oz, long long np, const Geo& g,
+                    const TileGeo& t, int* key, int* hist, unsigned int* err, cudaStream_t st, int sms) {
   if (np <= 0) return;
-  k_keys_split<<<grid_for(np, 256, sms, 16), 256, 0, st>>>(cell, np, g, t, key, hist, err);
+  k_keys_split<<<grid_for(np, 256, sms, 16), 256, 0, st>>>(cell, ox, oy, oz, np, g, t, key, hist, err);
 }
 void bin_keys_abs(const double* x, const double* y, const double* z, long long np, const Geo& g, const TileGeo& t,
                   double xmn, double ymn, double zmn, double dxi, double dyi, double dzi, int* key, int* hist,
@@ -105,13 +109,84 @@ void bin_keys_abs(const double* x, const double* y, const double* z, long long n
   if (np <= 0) return;
   k_keys_abs<<<grid_for(np, 256, sms, 16), 256, 0, st>>>(x, y, z, np, g, t, xmn, ymn, zmn, dxi, dyi, dzi, key, hist, err);
 }
-// hist has ntiles+1 bins (the last one: removed particles)
-void bin_finish(const int* key, long long np, const TileGeo& t, const int* hist, int* start, int* cursor, int* perm,
-                cudaStream_t st, int sms) {
-  k_scan_int<<<1, 1024, 0, st>>>(hist, t.ntiles + 1, start);
-  cudaMemsetAsync(cursor, 0, sizeof(int) * (t.ntiles + 1), st);
-  if (np > 0) k_perm_scatter<<<grid_for(np, 256, sms, 16), 256, 0, st>>>(key, np, start, cursor, perm);
+// ---- exclusive scan of many bins: block sums, a scan of the block sums,
+// then each block's scan offset by its block's start -------------------------
+constexpr int SCAN_ITEMS = 16, SCAN_THREADS = 256, SCAN_BLOCK = SCAN_ITEMS * SCAN_THREADS;
+
+__device__ __forceinline__ int block_exclusive_sum(int v, int* s_warp, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int inc = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += u;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      const int x = s_warp[w];
+      s_warp[w] = run;
+      run += x;
+    }
+    *total = run;
+  }
+  __syncthreads();
+  return s_warp[warp] + inc - v;
 }
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(const int* hist, int n, int* bsum) {
+  __shared__ int s_warp[SCAN_THREADS / 32];
+  __shared__ int s_total;
+  const int base = blockIdx.x * SCAN_BLOCK;
+  int v = 0;
+  for (int e = threadIdx.x; e < SCAN_BLOCK; e += blockDim.x)
+    if (base + e < n) v += hist[base + e];
+  block_exclusive_sum(v, s_warp, &s_total);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = s_total;
+}
+
+// start[i] = boff[block] + exclusive sum inside the block; start[n] = total
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int* hist, int n, const int* boff, int* start) {
+  __shared__ int s_warp[SCAN_THREADS / 32];
+  __shared__ int s_total;
+  const int base = blockIdx.x * SCAN_BLOCK + threadIdx.x * SCAN_ITEMS;
+  int v[SCAN_ITEMS];
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    v[k] = (base + k < n) ? hist[base + k] : 0;
+    sum += v[k];
+  }
+  int run = boff[blockIdx.x] + block_exclusive_sum(sum, s_warp, &s_total);
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    if (base + k < n) start[base + k] = run;
+    run += v[k];
+    if (base + k == n - 1) start[n] = run;
+  }
+}
+
+// hist has nkeys+1 bins (the last one: removed particles).  scan_tmp holds
+// bin_scan_tmp_ints(t) ints.  Returns the kernels launched.
+int bin_finish(const int* key, long long np, const TileGeo& t, const int* hist, int* start, int* cursor, int* perm,
+               int* scan_tmp, cudaStream_t st, int sms) {
+  const int n = t.nkeys + 1;
+  const int nb = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  if (nb <= 1) {
+    k_scan_int<<<1, 1024, 0, st>>>(hist, n, start);
+  } else {
+    int* bsum = scan_tmp;
+    int* boff = scan_tmp + nb + 1;
+    k_scan_sums<<<nb, SCAN_THREADS, 0, st>>>(hist, n, bsum);
+    k_scan_int<<<1, 1024, 0, st>>>(bsum, nb, boff);
+    k_scan_apply<<<nb, SCAN_THREADS, 0, st>>>(hist, n, boff, start);
+  }
+  cudaMemsetAsync(cursor, 0, sizeof(int) * n, st);
+  if (np > 0) k_perm_scatter<<<grid_for(np, 256, sms, 16), 256, 0, st>>>(key, np, start, cursor, perm);
+  return (nb <= 1 ? 1 : 3) + (np > 0 ? 1 : 0);
+}
+int bin_scan_tmp_ints(const TileGeo& t) { return 2 * ((t.nkeys + 1) / SCAN_BLOCK + 3); }
 
 // ---- compaction along the permutation (physical reorder by tile) --------
 struct PermAlive {
@@ -200,7 +275,7 @@ long long perm_compact32(const int* perm, long long nalive, const Part32View& sr
 namespace {
 __global__ void km_scan(const MultiInst* __restrict__ d) {
   const MultiInst& m = d[blockIdx.x];
-  d_scan_int(m.ta.hist, m.ta.t.ntiles + 1, const_cast<int*>(m.ta.tstart));
+  d_scan_int(m.ta.hist, m.ta.t.nkeys + 1, const_cast<int*>(m.ta.tstart));
 }
 __global__ void km_scatter(const MultiInst* __restrict__ d) {
   const MultiInst& m = d[blockIdx.y];

@@ -431,7 +431,7 @@ __global__ void km_pre(const MultiInst* __restrict__ d) {
     m.ta.jhi[q] = 0.f;
     m.ta.jlo[q] = 0.f;
   }
-  const int nt = m.ta.t.ntiles;
+  const int nt = m.ta.t.nkeys;
   GRID_STRIDE(b, (long long)nt + 1) {
     m.cursor[b] = 0;
     if (b == nt) {

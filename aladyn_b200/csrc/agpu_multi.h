@@ -17,7 +17,7 @@ struct MultiInst {
   TileArgs32 ta;               // geometry, fields (read), currents, particles, binning arrays
   float* ebf;                  // fields (written by the field phases)
   YeeC yc;
-  int* cursor;                 // scatter cursors (ntiles + 1)
+  int* cursor;                 // scatter cursors (nkeys + 1)
   unsigned long long* pushed;  // the instance's device push counter
   unsigned long long* removed;
   double* fmax;

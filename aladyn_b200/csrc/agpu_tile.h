@@ -22,8 +22,8 @@ struct TileArgs32 {
   Part32 p;
   const int* perm;
   const int* tstart;
-  int* key;   // new tile key per particle (ntiles = removed)
-  int* hist;  // next histogram, ntiles + 1 bins
+  int* key;   // new key per particle (tile and row; nkeys = removed)
+  int* hist;  // next histogram, nkeys + 1 bins
   float dth, lfact, dtx, dty, dtz;
   int initial;
   unsigned int* err;

@@ -91,7 +91,7 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
   __shared__ unsigned int s_wmax;
 
   const Geo g = a.g;
-  const int beg = a.tstart[t], end = a.tstart[t + 1];
+  const int beg = a.tstart[t * a.t.nsub], end = a.tstart[(t + 1) * a.t.nsub];
   if (beg >= end) return;
   const int tx = t % a.t.ntx, ty = (t / a.t.ntx) % a.t.nty, tz = t / (a.t.ntx * a.t.nty);
   const int i0t = 3 + tx * TX, j0t = 3 + ty * TY, k0t = (NDIM == 3) ? 3 + tz * TZ : 1;
@@ -139,8 +139,8 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
     const int fx = i0 - i0t, fy = j0 - j0t, fz = (NDIM == 3) ? k0 - k0t : 0;
     if ((unsigned)fx >= (unsigned)TX || (unsigned)fy >= (unsigned)TY || (NDIM == 3 && (unsigned)fz >= (unsigned)TZ)) {
       raise_err(a.err, AGPU_EBIT_INDEX);  // not binned in this tile: drop it
-      a.key[p] = a.t.ntiles;
-      hist_add(a.hist, a.t.ntiles);
+      a.key[p] = a.t.nkeys;
+      hist_add(a.hist, a.t.nkeys);
       continue;
     }
     float ax1[3], ay1[3], az1[3] = {0.f, 1.f, 0.f};
@@ -249,7 +249,9 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
     if (!(pn[0] == pn[0] && pn[1] == pn[1] && pn[2] == pn[2])) raise_err(a.err, AGPU_EBIT_NONFINITE);
     bool keep = inside(i1n, nsx, nx) && inside(j1n, nsy, ny);
     if (NDIM == 3) keep = keep && inside(k1n, nsz, nz);
-    int nkey = keep ? tile_key_c<TX, TY, TZ>(a.t, i1n, j1n, (NDIM == 3) ? k1n : 3) : a.t.ntiles;
+    int nkey = keep ? tile_key_c<TX, TY, TZ, (NDIM == 3) ? 8 : 4>(a.t, i1n, j1n, (NDIM == 3) ? k1n : 3,
+                                                                   offset_octant(nsx, nsy, nsz, NDIM))
+                    : a.t.nkeys;
     a.key[p] = nkey;
     hist_add(a.hist, nkey);
     if (!keep) continue;

@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256, 3) k32c_tile(TileArgs32 a) {
 
   const Geo g = a.g;
   const int t = blockIdx.x;
-  const int beg = a.tstart[t], end = a.tstart[t + 1];
+  const int beg = a.tstart[t * a.t.nsub], end = a.tstart[(t + 1) * a.t.nsub];
   if (beg >= end) return;
   const int tx = t % a.t.ntx, ty = (t / a.t.ntx) % a.t.nty, tz = t / (a.t.ntx * a.t.nty);
   const int i0t = 3 + tx * TX, j0t = 3 + ty * TY, k0t = (NDIM == 3) ? 3 + tz * TZ : 1;
@@ -148,8 +148,8 @@ __global__ void __launch_bounds__(256, 3) k32c_tile(TileArgs32 a) {
     if ((unsigned)(i0 - i0t) >= (unsigned)TX || (unsigned)(j0 - j0t) >= (unsigned)TY ||
         (NDIM == 3 && (unsigned)(k0 - k0t) >= (unsigned)TZ)) {
       raise_err(a.err, AGPU_EBIT_INDEX);
-      a.key[p] = a.t.ntiles;
-      hist_add(a.hist, a.t.ntiles);
+      a.key[p] = a.t.nkeys;
+      hist_add(a.hist, a.t.nkeys);
       continue;
     }
     float sx, sy, sz = 0.f;
@@ -267,7 +267,9 @@ __global__ void __launch_bounds__(256, 3) k32c_tile(TileArgs32 a) {
     if (!(pn[0] == pn[0] && pn[1] == pn[1] && pn[2] == pn[2])) raise_err(a.err, AGPU_EBIT_NONFINITE);
     bool keep = inside_c(i1n, nox, nx) && inside_c(j1n, noy, ny);
     if (NDIM == 3) keep = keep && inside_c(k1n, noz, nz);
-    int nkey = keep ? tile_key_c<TX, TY, TZ>(a.t, i1n, j1n, (NDIM == 3) ? k1n : 3) : a.t.ntiles;
+    int nkey = keep ? tile_key_c<TX, TY, TZ, (NDIM == 3) ? 8 : 4>(a.t, i1n, j1n, (NDIM == 3) ? k1n : 3,
+                                                                   offset_octant(nox, noy, noz, NDIM))
+                    : a.t.nkeys;
     a.key[p] = nkey;
     hist_add(a.hist, nkey);
     if (!keep) continue;

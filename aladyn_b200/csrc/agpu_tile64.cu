@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(256, 2) k64_tile(TileArgs64 a) {
 
   const Geo g = a.g;
   const int t = blockIdx.x;
-  const int beg = a.tstart[t], end = a.tstart[t + 1];
+  const int beg = a.tstart[t * a.t.nsub], end = a.tstart[(t + 1) * a.t.nsub];
   if (beg >= end) return;
   const int tx = t % a.t.ntx, ty = (t / a.t.ntx) % a.t.nty, tz = t / (a.t.ntx * a.t.nty);
   const int i0t = 3 + tx * TX, j0t = 3 + ty * TY, k0t = (NDIM == 3) ? 3 + tz * TZ : 1;
@@ -102,8 +102,8 @@ __global__ void __launch_bounds__(256, 2) k64_tile(TileArgs64 a) {
     const int fx = i - (i0t - 1), fy = j - (j0t - 1), fz = (NDIM == 3) ? k - (k0t - 1) : 0;
     if ((unsigned)fx >= (unsigned)TX || (unsigned)fy >= (unsigned)TY || (NDIM == 3 && (unsigned)fz >= (unsigned)TZ)) {
       raise_err(a.err, AGPU_EBIT_INDEX);
-      a.key[p] = a.t.ntiles;
-      hist_add(a.hist, a.t.ntiles);
+      a.key[p] = a.t.nkeys;
+      hist_add(a.hist, a.t.nkeys);
       continue;
     }
     double ap[6] = {0, 0, 0, 0, 0, 0};
@@ -283,7 +283,9 @@ __global__ void __launch_bounds__(256, 2) k64_tile(TileArgs64 a) {
       raise_err(a.err, AGPU_EBIT_INDEX);  // moved more than one cell: no window slot
       keep = false;
     }
-    int nkey = keep ? tile_key(a.t, in, jn, (NDIM == 3) ? kn : 3) : a.t.ntiles;
+    const int oct = offset_octant((float)(3.0 + xn[0] - (double)in), (float)(3.0 + xn[1] - (double)jn),
+                                  (NDIM == 3) ? (float)(3.0 + xn[2] - (double)kn) : 0.f, NDIM);
+    int nkey = keep ? tile_key(a.t, in, jn, (NDIM == 3) ? kn : 3, oct) : a.t.nkeys;
     a.key[p] = nkey;
     hist_add(a.hist, nkey);
     if (!keep) continue;
@@ -403,17 +405,17 @@ void tile_push64(const TileArgs64& a, cudaStream_t st) {
 // Histogram of the next binning: tile bins zero, the removed bin keeps the
 // particles already removed (they are not revisited by any tile).
 // Next histogram zeroed, the dead bin seeded with the records already dead;
-// with `pushed` set, the alive count of this push (tstart[ntiles]) is added
+// with `pushed` set, the alive count of this push (tstart[nkeys]) is added
 // to it (the deferred-count mode keeps the push count on the device).
-__global__ void k_hist_reset(int* hist, const int* tstart, int ntiles, int np, int first, unsigned long long* pushed) {
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= ntiles; b += gridDim.x * blockDim.x) {
-    hist[b] = (b == ntiles && !first) ? (np - tstart[ntiles]) : 0;
-    if (b == ntiles && pushed) *pushed += (unsigned long long)tstart[ntiles];
+__global__ void k_hist_reset(int* hist, const int* tstart, int nkeys, int np, int first, unsigned long long* pushed) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nkeys; b += gridDim.x * blockDim.x) {
+    hist[b] = (b == nkeys && !first) ? (np - tstart[nkeys]) : 0;
+    if (b == nkeys && pushed) *pushed += (unsigned long long)tstart[nkeys];
   }
 }
 void hist_reset(int* hist, const int* tstart, const TileGeo& t, long long np, bool first, unsigned long long* pushed,
                 cudaStream_t st) {
-  k_hist_reset<<<(t.ntiles + 256) / 256, 256, 0, st>>>(hist, tstart, t.ntiles, (int)np, first ? 1 : 0, pushed);
+  k_hist_reset<<<(t.nkeys + 256) / 256, 256, 0, st>>>(hist, tstart, t.nkeys, (int)np, first ? 1 : 0, pushed);
 }
 
 TileGeo make_tiles(const Geo& g, int nx, int ny, int nz) {
@@ -432,6 +434,9 @@ TileGeo make_tiles(const Geo& g, int nx, int ny, int nz) {
   t.nty = (ny + 1 + t.ty - 1) / t.ty;
   t.ntz = (g.ndim == 3) ? (nz + 1 + t.tz - 1) / t.tz : 1;
   t.ntiles = t.ntx * t.nty * t.ntz;
+  t.nq = (g.ndim == 3) ? 8 : 4;
+  t.nsub = t.ty * t.tz * t.nq;
+  t.nkeys = t.ntiles * t.nsub;
   return t;
 }
 

@@ -82,9 +82,11 @@ def test_fp64_deterministic_multistep_bitexact(ndim):
     assert np.array_equal(dev.get_currents().view(np.uint64), ora.get_currents().view(np.uint64))
 
 
-@pytest.mark.parametrize("ndim", [2, 3])
-def test_fp64_atomic_multistep_close(ndim):
-    p, dev, ora = _pair(ndim)
+@pytest.mark.parametrize("ndim,kw", [(2, {}), (3, {}),
+                                     # more than 4096 binning keys: the multi-block key scan
+                                     (2, dict(nx=1024, ny=64, cap=400_000)), (3, dict(nx=96, cap=400_000))])
+def test_fp64_atomic_multistep_close(ndim, kw):
+    p, dev, ora = _pair(ndim, **kw)
     t = 0.0
     for it in range(24):
         out = dev.lp_run(t, it, initial_time=(it == 0))
