@@ -78,20 +78,37 @@ __device__ void d_scan_int(const int* hist, int nb, int* start) {
 }
 __global__ void k_scan_int(const int* hist, int nb, int* start) { d_scan_int(hist, nb, start); }
 
-// perm[start[key] + rank] = n, ranks from warp-aggregated cursors.
+// perm[start[key] + rank] = n, ranks from warp-aggregated cursors.  Each warp
+// takes SC_U consecutive runs of 32 records per pass, so that SC_U cursor
+// atomics (one round trip to L2 each) are in flight together; the lanes of
+// a run with one key get consecutive slots in lane order.  Warp-uniform loop
+// (blockDim a multiple of 32).
+constexpr int SC_U = 4;
 __device__ void d_perm_scatter(const int* key, long long np, const int* start, int* cursor, int* perm, long long bid_,
                                long long nb_) {
-  for (long long n = bid_ * (long long)blockDim.x + threadIdx.x; n < np; n += nb_ * (long long)blockDim.x) {
-    int kk = key[n];
-    unsigned int act = __activemask();
-    unsigned int peers = __match_any_sync(act, kk);
-    int leader = __ffs(peers) - 1;
-    int lane = threadIdx.x & 31;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(&cursor[kk], __popc(peers));
-    base = __shfl_sync(peers, base, leader);
-    int rank = __popc(peers & ((1u << lane) - 1u));
-    perm[start[kk] + base + rank] = (int)n;
+  const int lane = threadIdx.x & 31;
+  const long long warp = (bid_ * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = (nb_ * (long long)blockDim.x) >> 5;
+  for (long long base = warp * 32 * SC_U; base < np; base += nwarps * 32 * SC_U) {
+    int kk[SC_U], b[SC_U], rank[SC_U], lead[SC_U];
+#pragma unroll
+    for (int u = 0; u < SC_U; ++u) {
+      const long long n = base + u * 32 + lane;
+      kk[u] = (n < np) ? key[n] : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < SC_U; ++u) {
+      const unsigned peers = __match_any_sync(0xffffffffu, kk[u]);
+      lead[u] = __ffs(peers) - 1;
+      rank[u] = __popc(peers & ((1u << lane) - 1u));
+      b[u] = 0;
+      if (lane == lead[u] && kk[u] >= 0) b[u] = atomicAdd(&cursor[kk[u]], __popc(peers));
+    }
+#pragma unroll
+    for (int u = 0; u < SC_U; ++u) {
+      const int bb = __shfl_sync(0xffffffffu, b[u], lead[u]);
+      if (kk[u] >= 0) perm[start[kk[u]] + bb + rank[u]] = (int)(base + u * 32 + lane);
+    }
   }
 }
 __global__ void k_perm_scatter(const int* key, long long np, const int* start, int* cursor, int* perm) {
