@@ -103,6 +103,11 @@ struct agpu_handle {
   int* tstart[4] = {nullptr, nullptr, nullptr, nullptr};
   int* cursor = nullptr;
   int* scan_tmp = nullptr;
+  // staging of window-injection records for the split form (kept between
+  // calls: a per-call device allocation of hundreds of MB can take longer
+  // than the step)
+  double* inj_stage = nullptr;
+  long long inj_stage_recs = 0;
   bool binned[4] = {false, false, false, false};
   long long nalive[4] = {0, 0, 0, 0};  // np minus removed records still stored
   // deferred counts: tiled steps leave the alive counts and the error word
@@ -216,6 +221,7 @@ int free_all(agpu_handle* h) {
   }
   cudaFree(h->cursor);
   cudaFree(h->scan_tmp);
+  cudaFree(h->inj_stage);
   for (int i = 0; i < 2 * PH_N; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
@@ -1580,13 +1586,26 @@ int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t l
     CK(cudaMemcpy2DAsync(h->part[ic] + h->np[ic], sizeof(double) * h->cap[ic], part, sizeof(double) * ld, sizeof(double) * n,
                          ndv, cudaMemcpyHostToDevice, h->st));
   } else {
-    double* stage = nullptr;
-    if (dmalloc((void**)&stage, sizeof(double) * n * ndv)) return AGPU_E_NOMEM;
-    cudaMemcpy2DAsync(stage, sizeof(double) * n, part, sizeof(double) * ld, sizeof(double) * n, ndv, cudaMemcpyHostToDevice, h->st);
-    rec_to_split(stage, n, n, h->sp[ic].view(), h->np[ic], h->g, h->p.xmn, h->p.ymn, h->p.zmn, h->p.dx_inv, h->p.dy_inv,
-                 h->p.dz_inv, h->st, h->sms);
-    cudaStreamSynchronize(h->st);
-    cudaFree(stage);
+    // chunks of at most 2^20 records through a staging buffer kept in the
+    // handle (allocated on the first call, grown up to the chunk size)
+    const long long chunk_max = 1ll << 20;
+    const long long chunk = n < chunk_max ? n : chunk_max;
+    if (h->inj_stage_recs < chunk) {
+      CK(cudaStreamSynchronize(h->st));
+      cudaFree(h->inj_stage);
+      h->inj_stage = nullptr;
+      h->inj_stage_recs = 0;
+      if (dmalloc((void**)&h->inj_stage, sizeof(double) * chunk * ndv)) return AGPU_E_NOMEM;
+      h->inj_stage_recs = chunk;
+    }
+    for (long long q0 = 0; q0 < n; q0 += chunk) {
+      const long long m = (n - q0) < chunk ? (n - q0) : chunk;
+      CK(cudaMemcpy2DAsync(h->inj_stage, sizeof(double) * m, part + q0, sizeof(double) * ld, sizeof(double) * m, ndv,
+                           cudaMemcpyHostToDevice, h->st));
+      rec_to_split(h->inj_stage, m, m, h->sp[ic].view(), h->np[ic] + q0, h->g, h->p.xmn, h->p.ymn, h->p.zmn, h->p.dx_inv,
+                   h->p.dy_inv, h->p.dz_inv, h->st, h->sms);
+      CK(cudaGetLastError());
+    }
   }
   CK(cudaStreamSynchronize(h->st));
   h->np[ic] += n;

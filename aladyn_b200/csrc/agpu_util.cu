@@ -444,22 +444,45 @@ __device__ __forceinline__ void atomic_max_nonneg(double* a, double v) {
   atomicMax(reinterpret_cast<unsigned long long*>(a), (unsigned long long)__double_as_longlong(v));
 }
 
+// One warp per interior x-row (j, k), the lanes along x: coalesced reads and
+// no per-cell index division.
 template <typename T>
 __global__ void k_field_diag(const T* ebf, Geo g, int nf, double dvol, double* out_e, double* out_max) {
-  int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
-  long long total = (long long)nx * ny * nz;
+  const int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
+  const long long nrows = (long long)ny * nz;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   double mx = 0.0;
-  int ne = (nf == 6) ? 3 : 2;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int i = g.ix1 + (int)(t % nx);
-    int j = g.jy1 + (int)((t / nx) % ny);
-    int k = g.kz1 + (int)(t / ((long long)nx * ny));
-    long long o = goff(g, i, j, k);
-    for (int c = 0; c < nf; ++c) {
-      double v = (double)ebf[g.ncell * c + o];
-      acc[c] += v * v;
-      if (c < ne) mx = fmax(mx, fabs(v));
+  const int ne = (nf == 6) ? 3 : 2;
+  const int lane = threadIdx.x & 31;
+  const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long r = warp; r < nrows; r += nwarps) {
+    const int j = g.jy1 + (int)(r % ny), k = g.kz1 + (int)(r / ny);
+    const long long o0 = goff(g, g.ix1, j, k);
+    if (sizeof(T) == 8) {
+      for (int i = lane; i < nx; i += 32) {
+        const long long o = o0 + i;
+        for (int c = 0; c < nf; ++c) {
+          double v = (double)ebf[g.ncell * c + o];
+          acc[c] += v * v;
+          if (c < ne) mx = fmax(mx, fabs(v));
+        }
+      }
+    } else {
+      // split form: a lane's squares of one row summed in FP32 (the field
+      // words are FP32), the row partial added in FP64
+      float rs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      float rm = 0.f;
+      for (int i = lane; i < nx; i += 32) {
+        const long long o = o0 + i;
+        for (int c = 0; c < nf; ++c) {
+          const float v = (float)ebf[g.ncell * c + o];
+          rs[c] = fmaf(v, v, rs[c]);
+          if (c < ne) rm = fmaxf(rm, fabsf(v));
+        }
+      }
+      for (int c = 0; c < nf; ++c) acc[c] += (double)rs[c];
+      mx = fmax(mx, (double)rm);
     }
   }
   for (int c = 0; c < nf; ++c) {
@@ -471,11 +494,11 @@ __global__ void k_field_diag(const T* ebf, Geo g, int nf, double dvol, double* o
 }
 void field_diag64(const double* ebf, const Geo& g, double dvol, double* out_e, double* out_max, cudaStream_t st, int sms) {
   long long cells = (long long)(g.ix2 - g.ix1 + 1) * (g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1);
-  k_field_diag<double><<<grid_for(cells, 256, sms, 8), 256, 0, st>>>(ebf, g, g.nf, dvol, out_e, out_max);
+  k_field_diag<double><<<grid_for(cells / 8, 256, sms, 16), 256, 0, st>>>(ebf, g, g.nf, dvol, out_e, out_max);
 }
 void field_diag32(const float* ebf, const Geo& g, double dvol, double* out_e, double* out_max, cudaStream_t st, int sms) {
   long long cells = (long long)(g.ix2 - g.ix1 + 1) * (g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1);
-  k_field_diag<float><<<grid_for(cells, 256, sms, 8), 256, 0, st>>>(ebf, g, g.nf, dvol, out_e, out_max);
+  k_field_diag<float><<<grid_for(cells / 8, 256, sms, 16), 256, 0, st>>>(ebf, g, g.nf, dvol, out_e, out_max);
 }
 
 // out[0] = sum w (gamma-1), out[1] = sum charge*w, out[2..4] = sum w p over
@@ -505,20 +528,25 @@ __global__ void k_part_diag64(const double* part, long long ld, long long n, int
 void part_diag64(const double* part, long long ld, long long n, int nd, const int* perm, double* out, cudaStream_t st,
                  int sms) {
   if (n <= 0) return;
-  k_part_diag64<<<grid_for(n, 256, sms, 8), 256, 0, st>>>(part, ld, n, nd, perm, out);
+  k_part_diag64<<<grid_for(n, 256, sms, 16), 256, 0, st>>>(part, ld, n, nd, perm, out);
 }
+// Split form: each record's terms in FP32 (its momenta are FP32; gamma - 1 as
+// p^2 / (1 + gamma), free of cancellation), summed in FP64; the charge term
+// is exact.
 __global__ void k_part_diag32(Part32View p, long long n, int nd, const int* perm, double* out) {
   double a[5] = {0, 0, 0, 0, 0};
   for (long long qq = blockIdx.x * (long long)blockDim.x + threadIdx.x; qq < n; qq += (long long)gridDim.x * blockDim.x) {
     const long long q = perm ? (long long)perm[qq] : qq;
-    double pv[3] = {(double)p.px[q], (double)p.py[q], nd == 3 ? (double)p.pz[q] : 0.0};
-    double p2 = pv[0] * pv[0] + pv[1] * pv[1] + pv[2] * pv[2];
-    uint64_t sl = p.slot[q];
-    double w = (double)slot_wgh(sl);
-    double gm = sqrt(1.0 + p2);
-    a[0] += w * (gm - 1.0);
-    a[1] += (double)slot_charge(sl) * w;
-    for (int c = 0; c < 3; ++c) a[2 + c] += w * pv[c];
+    const float px = p.px[q], py = p.py[q], pz = (nd == 3) ? p.pz[q] : 0.f;
+    const float p2 = fmaf(px, px, fmaf(py, py, pz * pz));
+    const float g1 = p2 / (1.f + sqrtf(1.f + p2));
+    const uint64_t sl = p.slot[q];
+    const float w = slot_wgh(sl);
+    a[0] += (double)(w * g1);
+    a[1] += (double)slot_charge(sl) * (double)w;
+    a[2] += (double)(w * px);
+    a[3] += (double)(w * py);
+    a[4] += (double)(w * pz);
   }
   for (int c = 0; c < 5; ++c) {
     double v = warp_sum(a[c]);
@@ -527,7 +555,7 @@ __global__ void k_part_diag32(Part32View p, long long n, int nd, const int* perm
 }
 void part_diag32(const Part32View& p, long long n, int nd, const int* perm, double* out, cudaStream_t st, int sms) {
   if (n <= 0) return;
-  k_part_diag32<<<grid_for(n, 256, sms, 8), 256, 0, st>>>(p, n, nd, perm, out);
+  k_part_diag32<<<grid_for(n, 256, sms, 16), 256, 0, st>>>(p, n, nd, perm, out);
 }
 
 // max of a non-negative FP64 array (ion |E|^2), for the lp_max refresh.
