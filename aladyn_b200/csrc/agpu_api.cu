@@ -436,6 +436,38 @@ int drop_removed(agpu_handle* h, int ic) {
   return 0;
 }
 
+// agpu_set_sort_interval: every sort_interval steps (not on window steps,
+// whose compaction reorders the records anyway) the records of a tiled
+// species are moved along the step's tile permutation, so that memory order
+// follows the tiles again where the particles have drifted (runs without a
+// moving window never compact otherwise).  Removed records are dropped.
+bool sort_step(const agpu_handle* h, int iter) {
+  const agpu_params& p = h->p;
+  if (h->sort_interval <= 0 || iter <= 0 || iter % h->sort_interval != 0) return false;
+  return !(p.w_speed > 0.0 && p.w_sh > 0 && iter % p.w_sh == 0);
+}
+
+int reorder_records(agpu_handle* h, int ic) {
+  if (!h->binned[ic]) return 0;
+  if (int rc = refresh_counts(h)) return rc;
+  long long kept;
+  if (h->fp32) {
+    kept = perm_compact32(h->perm[ic], h->nalive[ic], h->sp[ic].view(), h->sptmp.view(), false, h->g.n1p, h->p.nx, h->scr,
+                          h->st);
+    std::swap(h->sp[ic], h->sptmp);
+  } else {
+    kept = perm_compact64(h->perm[ic], h->nalive[ic], h->part[ic], h->tmp, h->cap[ic], h->ndv, false, h->p.gxmin,
+                          h->p.gxmax, h->scr, h->st);
+    std::swap(h->part[ic], h->tmp);
+  }
+  CK(cudaGetLastError());
+  h->timers.launches_total += 3;
+  h->np[ic] = kept;
+  h->nalive[ic] = kept;
+  h->binned[ic] = false;
+  return 0;
+}
+
 // Tiled gather + push + deposit of species ic, then the next binning from
 // the keys the kernel wrote.  Removed particles stay stored (key nkeys)
 // until the next compaction.
@@ -1187,6 +1219,7 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu
   const agpu_params& p = h->p;
   bool plain = h->use_graph && h->defer && !initial_time && p.ionz_lev == 0 && !h->profiling && !h->deterministic;
   if (plain && p.w_speed > 0.0 && p.w_sh > 0 && t >= p.wi_time && t < p.wf_time && iter % p.w_sh == 0) plain = false;
+  if (plain && sort_step(h, iter)) plain = false;
   for (int ic = 0; ic < p.nsp_run && plain; ++ic)
     if (h->np[ic] > 0 && !(h->binned[ic] && h->key[ic])) plain = false;
   if (!plain) return step_impl(h, iter, t, initial_time, out);
@@ -1439,6 +1472,8 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
     if (np <= 0) continue;
     if (tiled(h, ic)) {
       if (int rc_ = tiled_push(h, ic, initial_time, out)) return rc_;
+      if (sort_step(h, iter))
+        if (int rc_ = reorder_records(h, ic)) return rc_;
       continue;
     }
     if (int rc_ = drop_removed(h, ic)) return rc_;

@@ -213,6 +213,10 @@ class PicDevice:
     def set_fused_yee(self, on: bool = True):
         check(self.lib.agpu_set_fused_yee(self.h, 1 if on else 0), "agpu_set_fused_yee")
 
+    def set_sort_interval(self, steps: int):
+        """Move the records along the tile permutation every `steps` steps (0: never)."""
+        check(self.lib.agpu_set_sort_interval(self.h, int(steps)), "agpu_set_sort_interval")
+
     def set_step_graphs(self, on: bool = True):
         check(self.lib.agpu_set_step_graphs(self.h, 1 if on else 0), "agpu_set_step_graphs")
 

@@ -365,7 +365,12 @@ int agpu_set_step_graphs(agpu_handle* h, int32_t on);
  * the separate kernels in 3D (faster in 2D).  Step graphs use the separate
  * kernels. */
 int agpu_set_fused_yee(agpu_handle* h, int32_t on);
-/* Sort interval in steps for the tile sort (0 = never). */
+/* Sort interval (steps > 0): every `steps` steps the records of each tiled
+ * species are moved in memory along the step's tile permutation (removed
+ * records dropped), so that memory order follows the tiles again; window
+ * steps are skipped (their compaction reorders anyway).  0 (the default):
+ * records move only at window compactions.  No counterpart in the reference
+ * (its particles are never sorted); the physics is unchanged. */
 int agpu_set_sort_interval(agpu_handle* h, int32_t steps);
 /* sizeof of agpu_params, agpu_plasma, agpu_laser, agpu_step_out,
  * agpu_diag_out, agpu_timers (in that order) into sizes[0..n-1], so that a
