@@ -533,20 +533,42 @@ void part_diag64(const double* part, long long ld, long long n, int nd, const in
 // Split form: each record's terms in FP32 (its momenta are FP32; gamma - 1 as
 // p^2 / (1 + gamma), free of cancellation), summed in FP64; the charge term
 // is exact.
+__device__ __forceinline__ void diag_terms32(float px, float py, float pz, uint64_t sl, double a[5]) {
+  const float p2 = fmaf(px, px, fmaf(py, py, pz * pz));
+  const float g1 = p2 / (1.f + sqrtf(1.f + p2));
+  const float w = slot_wgh(sl);
+  a[0] += (double)(w * g1);
+  a[1] += (double)slot_charge(sl) * (double)w;
+  a[2] += (double)(w * px);
+  a[3] += (double)(w * py);
+  a[4] += (double)(w * pz);
+}
 __global__ void k_part_diag32(Part32View p, long long n, int nd, const int* perm, double* out) {
   double a[5] = {0, 0, 0, 0, 0};
-  for (long long qq = blockIdx.x * (long long)blockDim.x + threadIdx.x; qq < n; qq += (long long)gridDim.x * blockDim.x) {
-    const long long q = perm ? (long long)perm[qq] : qq;
-    const float px = p.px[q], py = p.py[q], pz = (nd == 3) ? p.pz[q] : 0.f;
-    const float p2 = fmaf(px, px, fmaf(py, py, pz * pz));
-    const float g1 = p2 / (1.f + sqrtf(1.f + p2));
-    const uint64_t sl = p.slot[q];
-    const float w = slot_wgh(sl);
-    a[0] += (double)(w * g1);
-    a[1] += (double)slot_charge(sl) * (double)w;
-    a[2] += (double)(w * px);
-    a[3] += (double)(w * py);
-    a[4] += (double)(w * pz);
+  if (perm) {
+    for (long long qq = blockIdx.x * (long long)blockDim.x + threadIdx.x; qq < n; qq += (long long)gridDim.x * blockDim.x) {
+      const long long q = perm[qq];
+      diag_terms32(p.px[q], p.py[q], (nd == 3) ? p.pz[q] : 0.f, p.slot[q], a);
+    }
+  } else {
+    // records 0..n-1 four at a time with 16-byte loads (the arrays are
+    // allocation-aligned), the last n % 4 one by one
+    const long long n4 = n >> 2;
+    const float4* px4 = reinterpret_cast<const float4*>(p.px);
+    const float4* py4 = reinterpret_cast<const float4*>(p.py);
+    const float4* pz4 = reinterpret_cast<const float4*>(p.pz);
+    const ulonglong2* sl2 = reinterpret_cast<const ulonglong2*>(p.slot);
+    for (long long g4 = blockIdx.x * (long long)blockDim.x + threadIdx.x; g4 < n4; g4 += (long long)gridDim.x * blockDim.x) {
+      const float4 x = px4[g4], y = py4[g4];
+      const float4 z = (nd == 3) ? pz4[g4] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const ulonglong2 s0 = sl2[2 * g4], s1 = sl2[2 * g4 + 1];
+      diag_terms32(x.x, y.x, z.x, s0.x, a);
+      diag_terms32(x.y, y.y, z.y, s0.y, a);
+      diag_terms32(x.z, y.z, z.z, s1.x, a);
+      diag_terms32(x.w, y.w, z.w, s1.y, a);
+    }
+    const long long q = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q < n) diag_terms32(p.px[q], p.py[q], (nd == 3) ? p.pz[q] : 0.f, p.slot[q], a);
   }
   for (int c = 0; c < 5; ++c) {
     double v = warp_sum(a[c]);
@@ -555,7 +577,7 @@ __global__ void k_part_diag32(Part32View p, long long n, int nd, const int* perm
 }
 void part_diag32(const Part32View& p, long long n, int nd, const int* perm, double* out, cudaStream_t st, int sms) {
   if (n <= 0) return;
-  k_part_diag32<<<grid_for(n, 256, sms, 16), 256, 0, st>>>(p, n, nd, perm, out);
+  k_part_diag32<<<grid_for(perm ? n : (n + 3) / 4, 256, sms, 16), 256, 0, st>>>(p, n, nd, perm, out);
 }
 
 // max of a non-negative FP64 array (ion |E|^2), for the lp_max refresh.

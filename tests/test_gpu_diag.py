@@ -58,3 +58,36 @@ def test_diag_sums(ndim, precision, tol):
     ne = 3 if ndim == 3 else 2
     emax = max(np.abs(f[sl + (c,)]).max() for c in range(ne))
     assert abs(d.max_abs_e - emax) <= 1e-12 * emax
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+@pytest.mark.parametrize("precision,tol", [(AGPU_FP64, 1e-12), (AGPU_FP32_SPLIT, 1e-6)])
+def test_diag_sums_fresh_records(ndim, precision, tol):
+    """Records set from the host (a count that is not a multiple of four,
+    random momenta, no removed records): the straight pass over the arrays."""
+    from aladyn_b200.sim import pack_slot
+    p = small_case(ndim, precision=precision)
+    dev = PicDevice(p)
+    rng = np.random.default_rng(5)
+    n = 40_003
+    nd = 2 * ndim + 1
+    rec = np.zeros((n, nd))
+    lo = (p.xmn + 3 * p.dx, p.ymn + 3 * p.dy, p.zmn + 3 * p.dz)
+    hi = (p.xmn + (p.nx - 3) * p.dx, p.ymn + (p.ny - 3) * p.dy, p.zmn + (p.nz - 3) * p.dz)
+    for d in range(ndim):
+        rec[:, d] = rng.uniform(lo[d], hi[d], n)
+    rec[:, ndim:2 * ndim] = rng.normal(0.0, 0.5, (n, ndim))
+    rec[:, -1] = pack_slot(rng.integers(-1, 3, n), 0, rng.uniform(0.1, 2.0, n))
+    dev.set_species(0, rec)
+    d = dev.diag()
+    s = dev.get_species(0)
+    q, _, w = unpack_slot(s[:, -1])
+    w = w.astype(np.float64)
+    pm = s[:, ndim:2 * ndim]
+    kin = np.sum(w * (np.sqrt(1.0 + np.sum(pm * pm, axis=1)) - 1.0))
+    assert d.np[0] == n
+    assert abs(d.kin_energy[0] - kin) <= tol * kin
+    assert abs(d.charge[0] - np.sum(q * w)) <= 1e-12 * np.sum(np.abs(q) * w)
+    scale = np.sum(w * np.sqrt(np.sum(pm * pm, axis=1)))
+    for c in range(ndim):
+        assert abs(d.momentum[0][c] - np.sum(w * pm[:, c])) <= tol * scale, c
