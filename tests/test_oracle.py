@@ -201,3 +201,48 @@ def test_threaded_oracle_matches_serial():
         outs.append(o.get_fields())
     a, b = outs
     assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_oracle_empty_species_with_window(ndim):
+    """No particles at all: the step, the window shift (no injection source)
+    and the field update run, nothing is counted and no error bit is set."""
+    p = small_case(ndim, nx=40, ny=20, nz=12, cap=1000)
+    o = Oracle(p)
+    o.set_fields(laser_fields(p))
+    e0 = float(np.sum(o.get_fields() ** 2))
+    t = 0.0
+    for it in range(12):
+        rc, out = o.lp_run(t, it, initial_time=(it == 0))
+        assert rc == 0 and out.error_bits == 0
+        assert out.np[0] == 0 and out.injected[0] == 0 and out.removed[0] == 0
+        t += p.dt
+    e1 = float(np.sum(o.get_fields() ** 2))
+    assert np.isfinite(e1) and e1 <= 1.5 * e0
+    assert o.count(0) == 0
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_oracle_box_edge_removal(ndim):
+    """reset_all_part_dist keeps xl < x <= xr per axis (mpi_part_interface.f90:
+    467-523): at rest in zero fields, a record exactly on the right box edge
+    stays, one just beyond it and one exactly on the left edge leave."""
+    from aladyn_b200.sim import pack_slot
+    p = small_case(ndim, nx=40, ny=20, nz=12, cap=1000)
+    o = Oracle(p)
+    o.set_fields(np.zeros(o.field_shape(), order="F"))
+    yc = 0.5 * (p.gymin + p.gymax)
+    zc = 0.5 * (p.gzmin + p.gzmax)
+    xs = [p.gxmax, p.gxmax + 1e-9 * p.dx, p.gxmin, 0.5 * (p.gxmin + p.gxmax)]
+    rec = np.zeros((len(xs), 2 * ndim + 1))
+    rec[:, 0] = xs
+    rec[:, 1] = yc
+    if ndim == 3:
+        rec[:, 2] = zc
+    rec[:, -1] = pack_slot(-1, 0, 1.0)
+    o.set_species(0, rec)
+    rc, out = o.lp_run(0.0, 1)  # no window shift on iteration 1
+    assert rc == 0 and out.error_bits == 0
+    kept = o.get_species(0)
+    assert kept.shape[0] == 2
+    assert sorted(kept[:, 0].tolist()) == sorted([p.gxmax, xs[3]])
