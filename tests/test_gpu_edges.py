@@ -61,3 +61,36 @@ def test_box_edge_removal(ndim, precision):
     want = sorted([p.gxmax, xs[3]])
     got = sorted(kept[:, 0].tolist())
     assert np.allclose(got, want, rtol=0, atol=1e-6 * p.dx)
+
+
+@pytest.mark.parametrize("precision", [AGPU_FP64, AGPU_FP32_SPLIT])
+def test_capacity_limits(precision):
+    """A species that would outgrow its capacity is refused with
+    AGPU_E_CAPACITY (records, plasma load, window injection) before anything
+    is written past the arrays; the records already set stay intact."""
+    from aladyn_b200.abi import AGPU_E_CAPACITY, AgpuError
+    from tests.helpers import plasma_source
+    ndim = 3
+    p = small_case(ndim, precision=precision, nx=40, ny=20, nz=12, cap=1000)
+    dev = PicDevice(p)
+    dev.set_fields(laser_fields(p))
+    yc = 0.5 * (p.gymin + p.gymax)
+    rec = np.zeros((1001, 2 * ndim + 1))
+    rec[:, 0] = np.linspace(p.gxmin + p.dx, p.gxmax - p.dx, 1001)
+    rec[:, 1] = yc
+    rec[:, 2] = 0.5 * (p.gzmin + p.gzmax)
+    rec[:, -1] = pack_slot(-1, 0, 1.0)
+    with pytest.raises(AgpuError) as e:
+        dev.set_species(0, rec)
+    assert e.value.code == AGPU_E_CAPACITY
+    dev.set_species(0, rec[:1000])
+    with pytest.raises(AgpuError) as e:
+        dev.window_inject(0, rec[:1])
+    assert e.value.code == AGPU_E_CAPACITY
+    dev.set_plasma_source(plasma_source(p))
+    with pytest.raises(AgpuError) as e:
+        dev.load_plasma(0)
+    assert e.value.code == AGPU_E_CAPACITY
+    back = dev.get_species(0)
+    assert back.shape[0] == 1000
+    assert np.abs(back[:, 0] - rec[:1000, 0]).max() <= 1e-6 * p.dx
