@@ -240,7 +240,11 @@ int agpu_set_ionization_species(agpu_handle* h, int32_t ic, int32_t atomic_numbe
 /* One call of lp_run (src/dynamics/pic_evolve_in_time.f90:113-144):
  * lpf2_evolve (field boundary extrapolation, ionization, gather, push,
  * box-edge removal, Esirkepov deposit, current fold, Yee update) and, when
- * mod(iter, w_sh) == 0 inside [wi_time, wf_time), lp_window_xshift. */
+ * mod(iter, w_sh) == 0 inside [wi_time, wf_time), lp_window_xshift.
+ * out->error_bits is the sticky device error word; once a species has
+ * outgrown its capacity (AGPU_EBIT_CAPACITY, set by any call that refused
+ * records for that reason) every later step returns AGPU_E_CAPACITY, as
+ * the reference stops on an allocation failure. */
 int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time,
               agpu_step_out* out);
 /* Host-supplied window injection: append n records to species ic
