@@ -243,8 +243,9 @@ int agpu_set_ionization_species(agpu_handle* h, int32_t ic, int32_t atomic_numbe
  * mod(iter, w_sh) == 0 inside [wi_time, wf_time), lp_window_xshift.
  * out->error_bits is the sticky device error word; once a species has
  * outgrown its capacity (AGPU_EBIT_CAPACITY, set by any call that refused
- * records for that reason) every later step returns AGPU_E_CAPACITY, as
- * the reference stops on an allocation failure. */
+ * records for that reason) every later step returns AGPU_E_CAPACITY (the
+ * reference reallocates its particle arrays instead; the device arrays are
+ * sized once, by agpu_params.capacity). */
 int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time,
               agpu_step_out* out);
 /* Host-supplied window injection: append n records to species ic
