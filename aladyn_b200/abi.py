@@ -180,6 +180,9 @@ SIGNATURES = {
     "agpu_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "agpu_synchronize": (C.c_int, [_P]),
     "agpu_set_sort_interval": (C.c_int, [_P, C.c_int32]),
+    "agpu_get_window_state": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                        C.POINTER(C.c_double)]),
+    "agpu_set_window_state": (C.c_int, [_P, C.c_double, C.POINTER(C.c_int64)]),
     "agpu_set_deterministic": (C.c_int, [_P, C.c_int32]),
     "agpu_struct_sizes": (C.c_int, [C.POINTER(C.c_int64), C.c_int32]),
     "agpu_field_diag_noalloc": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,

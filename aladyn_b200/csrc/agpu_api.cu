@@ -1089,6 +1089,26 @@ int agpu_get_count(agpu_handle* h, int32_t ic, int64_t* np) {
   return 0;
 }
 
+int agpu_get_window_state(agpu_handle* h, double* xlapse, int64_t* nptx, int64_t* sptx_max, double* xmn) {
+  if (!h || !xlapse || !nptx || !sptx_max || !xmn) return AGPU_E_ARG;
+  *xlapse = h->xlapse;
+  for (int ic = 0; ic < 4; ++ic) {
+    nptx[ic] = h->nptx[ic];
+    sptx_max[ic] = h->sptx_max[ic];
+  }
+  *xmn = h->p.xmn;
+  return 0;
+}
+int agpu_set_window_state(agpu_handle* h, double xlapse, const int64_t* nptx) {
+  if (!h || !nptx || !(xlapse >= 0.0)) return AGPU_E_ARG;
+  for (int ic = 0; ic < 4; ++ic)
+    if (nptx[ic] < 0) return AGPU_E_ARG;
+  h->xlapse = xlapse;
+  h->wi1 = (int)std::lround(h->p.dx_inv * xlapse);
+  for (int ic = 0; ic < 4; ++ic) h->nptx[ic] = nptx[ic];
+  return 0;
+}
+
 int agpu_set_plasma_source(agpu_handle* h, const agpu_plasma* src) {
   if (!h || !src) return AGPU_E_ARG;
   int ic = src->ic;

@@ -213,6 +213,20 @@ class PicDevice:
     def set_fused_yee(self, on: bool = True):
         check(self.lib.agpu_set_fused_yee(self.h, 1 if on else 0), "agpu_set_fused_yee")
 
+    def window_state(self):
+        """(xlapse, nptx[4], sptx_max[4], xmn): what a dump carries besides
+        fields and particles."""
+        x = C.c_double()
+        n = (C.c_int64 * 4)()
+        m = (C.c_int64 * 4)()
+        xmn = C.c_double()
+        check(self.lib.agpu_get_window_state(self.h, C.byref(x), n, m, C.byref(xmn)), "agpu_get_window_state")
+        return x.value, list(n), list(m), xmn.value
+
+    def set_window_state(self, xlapse: float, nptx):
+        n = (C.c_int64 * 4)(*[int(v) for v in (list(nptx) + [0, 0, 0, 0])[:4]])
+        check(self.lib.agpu_set_window_state(self.h, float(xlapse), n), "agpu_set_window_state")
+
     def set_sort_interval(self, steps: int):
         """Move the records along the tile permutation every `steps` steps (0: never)."""
         check(self.lib.agpu_set_sort_interval(self.h, int(steps)), "agpu_set_sort_interval")

@@ -210,6 +210,20 @@ int agpu_get_species(agpu_handle* h, int32_t ic, double* part, int64_t ld,
                      int64_t* np, int32_t ndv);
 int agpu_get_count(agpu_handle* h, int32_t ic, int64_t* np);
 
+/* ---- dump / restart state (dump_data / restart, src/start/pic_dump.f90) -- */
+/* The state a dump carries besides fields and particles: the window counter
+ * xlapse of lp_window_xshift (window.f90:279-280; wi1 = nint(dx_inv*xlapse)
+ * follows from it), the lattice columns already injected nptx[4] and the
+ * last target column sptx_max[4] (records 3-4 of Comm-data.bin), and the
+ * current box origin xmn.  A restart creates the handle with agpu_params
+ * whose xmn, gxmin, gxmax and xmax are shifted by the dumped origin shift
+ * (restart, pic_dump.f90:515-526), sets the plasma source, fields and
+ * particles, then xlapse and nptx here.  xlapse 0 (the reference's dumps
+ * do not hold it) restarts the window counters as the reference's restart
+ * does.  No device work. */
+int agpu_get_window_state(agpu_handle* h, double* xlapse, int64_t* nptx, int64_t* sptx_max, double* xmn);
+int agpu_set_window_state(agpu_handle* h, double xlapse, const int64_t* nptx);
+
 /* ---- initial state generated on the device ------------------------------ */
 /* Lattice loader (pspecies_distribute, src/IO/init_part_distrib.f90:152-203)
  * and the window injection source (particles_inject, window.f90:106-184). */

@@ -194,6 +194,24 @@ int64_t ora_count(const ora_sim* s, int ic) { return s->np[ic]; }
 uint32_t ora_error_bits(const ora_sim* s) { return s->error_bits; }
 double ora_xmn(const ora_sim* s) { return s->p.xmn; }
 
+/* Window and injection state carried by a dump (dump_data / restart,
+ * src/start/pic_dump.f90:35-380, 382-795): the window counter xlapse of
+ * lp_window_xshift (window.f90:279-280; wi1 = nint(dx_inv*xlapse) follows
+ * from it), the columns already injected nptx and the last target column
+ * sptx_max (records 3-4 of Comm-data.bin), and the box origin (x(1), rdata(9)). */
+void ora_get_window_state(const ora_sim* s, double* xlapse, int64_t* nptx, int64_t* sptx_max) {
+  *xlapse = s->xlapse;
+  for (int ic = 0; ic < 4; ++ic) {
+    nptx[ic] = s->nptx[ic];
+    sptx_max[ic] = s->sptx_max[ic];
+  }
+}
+void ora_set_window_state(ora_sim* s, double xlapse, const int64_t* nptx) {
+  s->xlapse = xlapse;
+  s->wi1 = ora_nint(s->p.dx_inv * xlapse);
+  for (int ic = 0; ic < 4; ++ic) s->nptx[ic] = nptx[ic];
+}
+
 /* ======================================================================== */
 /* A1: field_xyzbd (src/parallel/mpi_field_interface.f90:53-198), ib = 0     */
 /* ======================================================================== */

@@ -46,6 +46,8 @@ def load():
         "ora_count": (I64, [P, C.c_int]),
         "ora_error_bits": (C.c_uint32, [P]),
         "ora_xmn": (C.c_double, [P]),
+        "ora_get_window_state": (None, [P, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "ora_set_window_state": (None, [P, C.c_double, C.POINTER(C.c_int64)]),
         "ora_step": (C.c_int, [P, C.c_int, C.c_double, C.c_int, P]),
         "ora_field_bd": (None, [P]),
         "ora_advance_fields": (None, [P]),
@@ -198,6 +200,19 @@ class Oracle:
 
     def xmn(self):
         return self.lib.ora_xmn(self.h)
+
+    def window_state(self):
+        """(xlapse, nptx[4], sptx_max[4], xmn) of the window and the
+        injection, as aladyn_b200.sim.PicDevice.window_state."""
+        x = C.c_double()
+        n = (C.c_int64 * 4)()
+        m = (C.c_int64 * 4)()
+        self.lib.ora_get_window_state(self.h, C.byref(x), n, m)
+        return x.value, list(n), list(m), self.xmn()
+
+    def set_window_state(self, xlapse, nptx):
+        n = (C.c_int64 * 4)(*[int(v) for v in (list(nptx) + [0, 0, 0, 0])[:4]])
+        self.lib.ora_set_window_state(self.h, float(xlapse), n)
 
 
 def build_ionization_table(an, z0, model, e_max, dt):
