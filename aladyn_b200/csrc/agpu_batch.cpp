@@ -149,6 +149,15 @@ int agpu_batch_run(agpu_batch* b, int32_t nsteps, int32_t nthreads, int32_t* sta
     if (!b->status[i]) b->status[i] = agpu_set_step_graphs(b->h[i], (b->graphs && !b->multi) ? 1 : 0);
   }
   if (b->multi && !b->ws && agpu_x_ws_create(n, &b->ws) != 0) b->multi = false;
+  if (b->multi) {
+    // the multi-instance steps run on the workspace's stream and read every
+    // instance's buffers: let work the host queued on the instances' own
+    // streams before this call (set-up, injection, diagnostics) finish first
+    for (int i = 0; i < n; ++i) {
+      int rc = agpu_synchronize(b->h[i]);
+      if (rc && !b->status[i]) b->status[i] = rc;
+    }
+  }
   auto step_one = [b](int i) {
     int rc = agpu_step(b->h[i], b->iter[i], b->t[i], b->iter[i] == 0 ? 1 : 0, nullptr);
     if (rc) {

@@ -16,6 +16,7 @@
 // streams, two host threads) race on it; serialise them.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 
 #include "../../include/aladyn_gpu.h"
@@ -32,30 +33,82 @@ constexpr int NA_SLOTS = 8;                           // 6 energies, max |E|, pa
 // 65536 blocks x 8 doubles = 4 MiB, held by every GPU that loads the library
 static __device__ __align__(256) double g_na_partials[NA_MAX_BLOCKS * NA_SLOTS];
 
-constexpr int NA_MAX_DEVICES = 64;
+// The array's device address belongs to the module instance loaded into one
+// CUDA context: a device reset, or a host that drives the device through a
+// context of its own, loads the module again at another address.  The cache
+// is therefore keyed on (device, context), and every call made outside a
+// stream capture looks the address up again (cheap), so a stale entry can
+// only be used by a capture that starts before any plain call in a new
+// context.  The driver's cuCtxGetCurrent is reached through the runtime's
+// entry-point query, so the library does not link libcuda itself.
+constexpr int NA_CACHE = 64;
+struct NaEntry {
+  int dev;
+  void* ctx;
+  double* ptr;
+};
 std::mutex g_na_mu;
-double* g_na_ptr[NA_MAX_DEVICES] = {};
+NaEntry g_na_cache[NA_CACHE] = {};
+int g_na_used = 0;
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn g_ctx_get = nullptr;
+bool g_ctx_tried = false;
 
-// Device address of the scratch array on the current device, looked up once
-// per device (cudaGetSymbolAddress) and cached.
-int na_scratch(double** out) {
+void* na_current_context() {
+  if (!g_ctx_tried) {
+    g_ctx_tried = true;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get = reinterpret_cast<CtxGetCurrentFn>(fn);
+    else
+      cudaGetLastError();
+  }
+  void* ctx = nullptr;
+  if (!g_ctx_get || g_ctx_get(&ctx) != 0) return nullptr;
+  return ctx;
+}
+
+// Device address of the scratch array in the current context.
+int na_scratch(cudaStream_t st, double** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
     return AGPU_E_NODEVICE;
   }
-  if (dev < 0 || dev >= NA_MAX_DEVICES) return AGPU_E_ARG;
-  std::lock_guard<std::mutex> lk(g_na_mu);
-  if (!g_na_ptr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_na_partials);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      return AGPU_E_CUDA;
-    }
-    g_na_ptr[dev] = static_cast<double*>(p);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    return AGPU_E_CUDA;
   }
-  *out = g_na_ptr[dev];
+  std::lock_guard<std::mutex> lk(g_na_mu);
+  void* ctx = na_current_context();
+  int slot = -1;
+  for (int i = 0; i < g_na_used; ++i)
+    if (g_na_cache[i].dev == dev && g_na_cache[i].ctx == ctx) slot = i;
+  if (slot >= 0 && cap != cudaStreamCaptureStatusNone) {
+    *out = g_na_cache[slot].ptr;
+    return 0;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_na_partials);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    return AGPU_E_CUDA;
+  }
+  if (!ctx) ctx = na_current_context();  // the lookup made the primary context current
+  if (slot < 0) {
+    for (int i = 0; i < g_na_used; ++i)
+      if (g_na_cache[i].dev == dev && g_na_cache[i].ctx == ctx) slot = i;
+  }
+  if (slot < 0) {
+    slot = (g_na_used < NA_CACHE) ? g_na_used++ : (int)(((uintptr_t)ctx >> 4) % NA_CACHE);
+    g_na_cache[slot].dev = dev;
+    g_na_cache[slot].ctx = ctx;
+  }
+  g_na_cache[slot].ptr = static_cast<double*>(p);
+  *out = g_na_cache[slot].ptr;
   return 0;
 }
 
@@ -144,9 +197,9 @@ extern "C" int agpu_field_diag_noalloc(const double* d_ebf, int32_t ndim, int32_
   const long long ncells = (long long)nx * ny * (ndim == 3 ? nz : 1);
   const long long nb = (ncells + NA_CELLS_PER_BLOCK - 1) / NA_CELLS_PER_BLOCK;
   if (nb > NA_MAX_BLOCKS) return AGPU_E_CAPACITY;  // more than 2^28 interior cells
-  double* partials = nullptr;
-  if (int rc = na_scratch(&partials)) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double* partials = nullptr;
+  if (int rc = na_scratch(st, &partials)) return rc;
   const double dvol = dx * dy * (ndim == 3 ? dz : 1.0);
   k_na_partial<<<(unsigned)nb, NA_BLOCK, 0, st>>>(d_ebf, g, ncells, partials);
   k_na_final<<<1, NA_BLOCK, 0, st>>>(partials, (int)nb, g.nf, dvol, d_out);

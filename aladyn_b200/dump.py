@@ -28,8 +28,9 @@ Files of a dump directory:
     FP64 column by column (written only when some species holds particles).
 ``Dist-wgyz.bin``
     ``loc_ypt(1:npty, ic)`` per species, ``loc_zpt(1:nptz, ic)`` per species,
-    ``loc_wghyz(1:npty, 1:nptz, ic)`` per species, raw FP64 (written only
-    when some species holds particles).
+    ``loc_wghyz(1:npty, 1:nptz, ic)`` per species, raw FP64 (written
+    whenever the run has particle species, even before any particle is in
+    the box, and read whenever present).
 
 The (iter, t) of a dump are those of the next step, as the reference's main
 loop writes them after ``timing`` (src/ALaDyn.F90:92-106).  A restart builds
@@ -160,6 +161,11 @@ def write_dump(dirpath: str, st: DumpState, xmax: float) -> None:
             for s in st.species:
                 if s.shape[0] > 0:
                     np.asarray(s, dtype=np.float64).ravel(order="F").tofile(f)
+    # dump_data writes the transverse lattice whenever particles are part of
+    # the run, even with no particle in the box yet (a dump taken before the
+    # target enters the window), and restart reads it unconditionally
+    # (pic_dump.f90:336-377, 733-760)
+    if nsp > 0:
         with open(os.path.join(dirpath, DISTYZ), "wb") as f:
             for ic in range(nsp):
                 if npty[ic] > 0:
@@ -240,7 +246,7 @@ def read_dump(dirpath: str) -> DumpState:
     else:
         species = [np.zeros((0, ndv), order="F") for _ in range(nsp)]
     ypt = zpt = wghyz = None
-    if sum(npt) > 0 and os.path.exists(os.path.join(dirpath, DISTYZ)):
+    if os.path.exists(os.path.join(dirpath, DISTYZ)):
         d = np.fromfile(os.path.join(dirpath, DISTYZ), dtype=np.float64)
         off = 0
         ypt, zpt, wghyz = [], [], []

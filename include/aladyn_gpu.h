@@ -341,9 +341,13 @@ int agpu_diag(agpu_handle* h, agpu_diag_out* out);
  * cudaMalloc/cudaFree: its scratch is a file-scope device array of 65536 x 8
  * doubles (4 MiB) that every GPU loading the library holds until exit, which
  * limits the interior to 2^28 cells (larger grids return AGPU_E_CAPACITY).
- * The first call on a device looks up the array's address there; make that
- * call before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race and must be serialised by the caller. */
+ * The array's address is looked up in the calling thread's current context
+ * by every call made outside a stream capture (a device reset, or a host
+ * driving the device through a context of its own, loads the library's
+ * device code again at another address); a call inside a capture uses the
+ * address that the last plain call found in the same context, so make one
+ * plain call in each context before capturing.  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
 int agpu_field_diag_noalloc(const double* d_ebf, int32_t ndim, int32_t nx, int32_t ny, int32_t nz, double dx, double dy,
                             double dz, double* d_out, void* stream);
 

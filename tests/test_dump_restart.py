@@ -117,3 +117,38 @@ def test_reference_dump_restarts_window_counters(tmp_path):
         t += p.dt
     # lp_window_xshift from xlapse = 0, wi1 = 0 at the first shift after the restart
     assert out.nshx == int(math.floor(p.dx_inv * p.w_speed * p.dt * p.w_sh + 0.5))
+
+
+def test_dump_before_target_enters_window(tmp_path):
+    """A dump taken while the box holds no particle yet (the target starts
+    beyond the right edge) still carries the transverse lattice in
+    Dist-wgyz.bin, as dump_data writes it whenever particles are part of the
+    run (pic_dump.f90:336-377); the restart reads it and continues bit for
+    bit through the window shift that brings the target in."""
+    p = small_case(3, nx=40, ny=20, nz=12, cap=120_000)
+    src = plasma_source(p)
+    src.x_start = p.xmax + 3 * p.dx
+    src.x_end = p.xmax + 40 * p.dx
+    a = Oracle(p)
+    a.set_fields(laser_fields(p))
+    a.set_plasma_source(src)
+    a.load_plasma(0)
+    assert a.get_species(0).shape[0] == 0
+    t = _run(p, src, 5, holder=a)
+    st = dump.capture(a, p, 5, t, [src])
+    dump.write_dump(str(tmp_path), st, a.xmn() + (p.xmax - p.xmn))
+    assert not os.path.exists(tmp_path / dump.PARTICLES)
+    assert os.path.getsize(tmp_path / dump.DISTYZ) == 8 * (len(st.ypt[0]) + len(st.zpt[0]) + st.wghyz[0].size) > 0
+    back = dump.read_dump(str(tmp_path))
+    assert back.ypt is not None and np.array_equal(back.ypt[0], st.ypt[0])
+    assert np.array_equal(back.zpt[0], st.zpt[0]) and np.array_equal(back.wghyz[0], st.wghyz[0])
+    b = Oracle(dump.shifted_params(p, back.x0))
+    b.set_plasma_source(src)
+    dump.restore(b, back)
+    ta = _run(p, src, 19, t=t, it0=5, holder=a)  # through the shift at 10 (injection) and 20
+    tb = _run(p, src, 19, t=back.t, it0=back.it, holder=b)
+    assert ta == tb
+    n = a.get_species(0).shape[0]
+    assert n > 0 and b.get_species(0).shape[0] == n
+    assert np.array_equal(a.get_species(0).view(np.uint64), b.get_species(0).view(np.uint64))
+    assert np.array_equal(a.get_fields().view(np.uint64), b.get_fields().view(np.uint64))
