@@ -1,0 +1,61 @@
+"""Discrete continuity of a whole step on the oracle, through the host-side
+residual of aladyn_b200.conservation (the same check the GPU tests and the
+benchmark apply to the device's currents): after a few laser-driven steps,
+one more step's currents satisfy rho1 - rho0 + c div J_raw = 0 to FP64
+round-off, c = 1/2 (2D) or 1/3 (3D) (grid_part_connect.f90:956-1334 with
+the djc normalisation of set_init_param.f90:92-103)."""
+import numpy as np
+import pytest
+
+from aladyn_b200.conservation import charge_density, step_residual
+from oracle.oracle import Oracle
+from tests.helpers import laser_fields, plasma_source, small_case
+
+
+def conservation_case(ndim, precision=0, nx=48, ny=24, nz=24):
+    """A laser in a plasma slab kept 6 cells away from every edge (no
+    removal, no folded ghost current), no moving window."""
+    p = small_case(ndim, precision=precision, nx=nx, ny=ny, nz=nz, cap=200_000, w_sh=0)
+    src = plasma_source(p, x_start_frac=0.15)
+    src.x_end = p.xmax - 6 * p.dx
+    src.y_min, src.y_max = p.gymin + 6 * p.dy, p.gymax - 6 * p.dy
+    if ndim == 3:
+        src.z_min, src.z_max = p.gzmin + 6 * p.dz, p.gzmax - 6 * p.dz
+    return p, src, laser_fields(p, a0=3.0)
+
+
+def residual_after(holder, p, steps):
+    t = 0.0
+    for it in range(steps):
+        holder.lp_run(t, it, initial_time=(it == 0))
+        t += p.dt
+    part0 = holder.get_species(0)
+    holder.lp_run(t, steps)
+    part1 = holder.get_species(0)
+    assert part1.shape[0] == part0.shape[0] > 0
+    return step_residual(p, part0, part1, holder.get_currents(), margin=4)
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_oracle_step_conserves_charge(ndim):
+    p, src, ebf = conservation_case(ndim)
+    o = Oracle(p)
+    o.set_fields(ebf)
+    o.set_plasma_source(src)
+    o.load_plasma(0)
+    res, rho, divj = residual_after(o, p, 4)
+    assert divj > 1e-4 * rho  # the step moved charge
+    assert res <= 1e-14 * rho, (res, rho, divj)
+
+
+def test_charge_density_partition_of_unity():
+    p, src, _ = conservation_case(3)
+    o = Oracle(p)
+    o.set_plasma_source(src)
+    o.load_plasma(0)
+    part = o.get_species(0)
+    rho = charge_density(p, part, (o.n1p, o.n2p, o.n3p))
+    from aladyn_b200.sim import unpack_slot
+    q, _, w = unpack_slot(part[:, -1])
+    total = float(np.sum(q.astype(np.float32) * w.astype(np.float32), dtype=np.float64))
+    assert abs(rho.sum() - total) <= 1e-12 * abs(total)
