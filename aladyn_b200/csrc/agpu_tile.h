@@ -7,11 +7,11 @@
 
 namespace agpu {
 
-// Tile extents in nodes (3D and 2D).
-// 3D: 16 x 8 x 4 nodes, the fastest of 8x8x8, 16x8x4, 32x4x4 and 32x4x2 on
-// the 3D LWFA step (2% ahead of 8x8x8).
-constexpr int TILE3_X = 16, TILE3_Y = 8, TILE3_Z = 4;
-constexpr int TILE2_X = 16, TILE2_Y = 16;
+// Tile extents in nodes (3D and 2D).  32 nodes along x: the FP32 split
+// kernel gives each warp one x-row of a tile, one node per lane, so that its
+// shared-memory stencil reads are 32 consecutive words.
+constexpr int TILE3_X = 32, TILE3_Y = 4, TILE3_Z = 4;
+constexpr int TILE2_X = 32, TILE2_Y = 8;
 
 struct TileArgs32 {
   Geo g;
