@@ -95,6 +95,28 @@ class AgpuLaser(C.Structure):
     ]
 
 
+class AgpuLpPulse(C.Structure):
+    _fields_ = [
+        ("ee0", C.c_double), ("t_loc", C.c_double), ("tf", C.c_double), ("wx", C.c_double),
+        ("wy", C.c_double), ("xf0", C.c_double), ("om0", C.c_double), ("ycent", C.c_double),
+        ("zcent", C.c_double), ("g_prof", C.c_int32), ("reserved", C.c_int32),
+    ]
+
+
+AGPU_NE = 100
+
+
+class AgpuEnvarOut(C.Structure):
+    _fields_ = [
+        ("np", C.c_int64), ("ek", C.c_double * 7), ("ekmax", C.c_double), ("psig", C.c_double * 3),
+        ("nde", C.c_double * AGPU_NE),
+    ]
+
+
+class AgpuEnvarFieldsOut(C.Structure):
+    _fields_ = [("energy", C.c_double * 6), ("fmax", C.c_double * 6), ("e2max", C.c_double)]
+
+
 class AgpuStepOut(C.Structure):
     _fields_ = [
         ("np", C.c_int64 * 4),
@@ -152,6 +174,9 @@ SIGNATURES = {
     "agpu_set_plasma_source": (C.c_int, [_P, C.POINTER(AgpuPlasma)]),
     "agpu_load_plasma": (C.c_int, [_P, C.c_int32]),
     "agpu_init_laser": (C.c_int, [_P, C.POINTER(AgpuLaser)]),
+    "agpu_init_lp_fields": (C.c_int, [_P, C.POINTER(AgpuLpPulse)]),
+    "agpu_envar_species": (C.c_int, [_P, C.c_int32, C.c_double, C.POINTER(AgpuEnvarOut)]),
+    "agpu_envar_fields": (C.c_int, [_P, C.POINTER(AgpuEnvarFieldsOut)]),
     "agpu_set_ionization_table": (C.c_int, [_P, C.c_int32, _D, C.c_int32, C.c_int32, C.c_double]),
     "agpu_build_ionization_table": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, _D,
                                               C.POINTER(C.c_double)]),

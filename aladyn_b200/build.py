@@ -36,6 +36,7 @@ UNITS = [
     ("agpu_tile32c.cu", ["-fmad=true"]),
     ("agpu_bin.cu", ["-fmad=false"]),
     ("agpu_noalloc.cu", ["-fmad=false"]),
+    ("agpu_envar.cu", ["-fmad=false"]),
     ("agpu_beam.cu", ["-fmad=false"]),
     ("agpu_ionz.cpp", []),
     ("agpu_batch.cpp", ["-Xcompiler", "-pthread"]),

@@ -77,6 +77,10 @@ struct agpu_handle {
   Counters* h_cnt = nullptr;
   Scratch scr{};
   double* d_diag = nullptr;  // diagnostics accumulators
+  double* d_envar = nullptr;  // Envar reductions (16 + AGPU_NE doubles)
+  int* tile_work = nullptr;         // (tile, chunk) pairs of dense tiles, split form
+  unsigned int* tile_work_n = nullptr;
+  int tile_work_cap = 0;
   // window state (lp_window_xshift saved variables)
   double xlapse = 0.0;
   int wi1 = 0;
@@ -212,6 +216,9 @@ int free_all(agpu_handle* h) {
   cudaFree(h->scr.total);
   cudaFreeHost(h->scr.h_total);
   cudaFree(h->d_diag);
+  cudaFree(h->d_envar);
+  cudaFree(h->tile_work);
+  cudaFree(h->tile_work_n);
   for (int i = 0; i < 4; ++i) cudaFree(h->d_wtab[i]);
   for (int i = 0; i < 4; ++i) {
     cudaFree(h->key[i]);
@@ -502,10 +509,13 @@ int tiled_push(agpu_handle* h, int ic, int initial_time, agpu_step_out* out) {
     a.dtz = (float)(p.dt * p.dz_inv);
     a.initial = initial_time ? 1 : 0;
     a.err = &h->d_cnt->err;
+    a.work = h->tile_work;
+    a.work_n = h->tile_work_n;
+    a.work_cap = h->tile_work_cap;
     if (p.shape == AGPU_SHAPE_CUBIC)
       tile_push32_cubic(a, h->st);
     else
-      tile_push32(a, h->st);
+      h->timers.launches_total += tile_push32(a, h->st, h->sms) - 1;
   } else {
     TileArgs64 a;
     a.g = h->g;
@@ -936,6 +946,13 @@ int agpu_create(const agpu_params* params, agpu_handle** out) {
     rc |= dmalloc((void**)&h->scr.blockcnt, sizeof(long long) * nb);
     rc |= dmalloc((void**)&h->scr.total, sizeof(long long));
     rc |= dmalloc((void**)&h->d_diag, sizeof(double) * 64);
+    rc |= dmalloc((void**)&h->d_envar, sizeof(double) * (16 + AGPU_NE));
+    if (h->fp32) {
+      // every chunk beyond a tile's first holds LIST_CAP particles
+      h->tile_work_cap = (int)(capmax / tile32_list_cap(p.ndim)) + 16;
+      rc |= dmalloc((void**)&h->tile_work, sizeof(int) * 2 * (size_t)h->tile_work_cap);
+      rc |= dmalloc((void**)&h->tile_work_n, 2 * sizeof(unsigned int));
+    }
     if (cudaMallocHost((void**)&h->h_cnt, sizeof(Counters)) != cudaSuccess) rc |= AGPU_E_NOMEM;
     if (cudaMallocHost((void**)&h->scr.h_total, sizeof(long long)) != cudaSuccess) rc |= AGPU_E_NOMEM;
   }
@@ -1139,21 +1156,21 @@ int agpu_load_plasma(agpu_handle* h, int32_t ic) {
   return 0;
 }
 
-int agpu_init_laser(agpu_handle* h, const agpu_laser* l) {
-  if (!h || !l) return AGPU_E_ARG;
-  const double pi = 3.141592653589793;
+int agpu_init_lp_fields(agpu_handle* h, const agpu_lp_pulse* l) {
+  if (!h || !l || !(l->wx > 0.0) || !(l->wy > 0.0) || !(l->om0 > 0.0)) return AGPU_E_ARG;
   LaserArgs a;
   a.ndim = h->p.ndim;
-  double oml = 2.0 * pi / l->lam0;
-  a.amp = l->a0 * oml;
-  a.k0 = oml;
-  a.w0 = l->w0_y;
-  a.zr = pi * l->w0_y * l->w0_y / l->lam0;
-  a.w0x = l->tau_fwhm / std::sqrt(2.0 * std::log(2.0));
-  a.xc = l->xc;
-  a.xf = l->xf;
-  a.y0 = l->y0;
-  a.z0 = l->z0;
+  a.g_prof = l->g_prof ? 1 : 0;
+  a.ee0 = l->ee0;
+  a.t1 = l->t_loc - l->tf;  // coords(4)
+  a.xf0 = l->xf0;
+  a.om0 = l->om0;
+  a.wx = l->wx;
+  a.wy = l->wy;
+  a.zra = 0.5 * l->om0 * l->wy * l->wy;  // par_lp(5)
+  a.eps = 1. / (l->om0 * l->wy);         // par_lp(6)
+  a.ycent = l->ycent;
+  a.zcent = l->zcent;
   a.xmn = h->p.xmn;
   a.ymn = h->p.ymn;
   a.zmn = h->p.zmn;
@@ -1176,6 +1193,27 @@ int agpu_init_laser(agpu_handle* h, const agpu_laser* l) {
   CK(cudaStreamSynchronize(h->st));
   h->fields_set = true;
   return 0;
+}
+
+int agpu_init_laser(agpu_handle* h, const agpu_laser* l) {
+  if (!h || !l || !(l->lam0 > 0.0) || !(l->tau_fwhm > 0.0)) return AGPU_E_ARG;
+  // lp_pulse (src/IO/init_laser_field.f90:33-100) with the set_initial_param
+  // quantities (set_init_param.f90:291-330): Gaussian profile, aph_fwhm =
+  // sqrt(2 ln 2), lx_fwhm = tau_fwhm (a length, um/c)
+  const double pi2 = 2.0 * 3.141592653589793;
+  agpu_lp_pulse a;
+  a.om0 = pi2 / l->lam0;
+  a.ee0 = l->a0 * a.om0;
+  a.wx = l->tau_fwhm / std::sqrt(2. * std::log(2.));
+  a.wy = l->w0_y;
+  a.xf0 = l->xf;
+  a.tf = l->xf - l->xc;
+  a.t_loc = 0.0;
+  a.ycent = l->y0;
+  a.zcent = l->z0;
+  a.g_prof = 1;
+  a.reserved = 0;
+  return agpu_init_lp_fields(h, &a);
 }
 
 int agpu_set_ionization_table(agpu_handle* h, int32_t ic, const double* w_one_lev, int32_t n_ge, int32_t zmax, double de_inv) {
@@ -1391,6 +1429,9 @@ int agpu_x_step_many(agpu_handle** hs, int32_t n, agpu_x_ws* w) {
     a.dtz = (float)(p.dt * p.dz_inv);
     a.initial = 0;
     a.err = &h->d_cnt->err;
+    a.work = nullptr;  // the multi-instance tile kernel runs every chunk in the tile's CTA
+    a.work_n = nullptr;
+    a.work_cap = 0;
     m.ebf = h->ebf32;
     m.yc = yee_coef(p);
     m.cursor = h->cursor;
@@ -1830,6 +1871,55 @@ int agpu_diag(agpu_handle* h, agpu_diag_out* out) {
     for (int c = 0; c < 3; ++c) out->momentum[ic][c] = o[2 + c];
     out->np[ic] = nd_alive[ic];
   }
+  return 0;
+}
+
+int agpu_envar_species(agpu_handle* h, int32_t ic, double pmass, agpu_envar_out* out) {
+  if (!h || !out || ic < 0 || ic >= h->p.nsp) return AGPU_E_ARG;
+  std::memset(out, 0, sizeof(*out));
+  if (int rc = refresh_counts(h)) return rc;
+  CK(cudaMemsetAsync(h->d_envar, 0, sizeof(double) * (16 + AGPU_NE), h->st));
+  const bool along = h->binned[ic] && h->nalive[ic] < h->np[ic];
+  const int* perm = along ? h->perm[ic] : nullptr;
+  const long long n = along ? h->nalive[ic] : h->np[ic];
+  if (h->fp32) {
+    const Part32View v = h->sp[ic].view();
+    envar_species(nullptr, 0, &v, perm, n, h->g, h->p.ymn, h->p.zmn, h->p.dy, h->p.dz, pmass, h->d_envar, h->st, h->sms);
+  } else {
+    envar_species(h->part[ic], h->cap[ic], nullptr, perm, n, h->g, h->p.ymn, h->p.zmn, h->p.dy, h->p.dz, pmass,
+                  h->d_envar, h->st, h->sms);
+  }
+  CK(cudaGetLastError());
+  double hd[16 + AGPU_NE];
+  CK(cudaMemcpyAsync(hd, h->d_envar, sizeof(hd), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  out->np = n;
+  for (int c = 0; c < 7; ++c) out->ek[c] = hd[c];
+  out->ekmax = hd[7];
+  for (int c = 0; c < 3; ++c) out->psig[c] = hd[8 + c];
+  for (int b = 0; b < AGPU_NE; ++b) out->nde[b] = hd[16 + b];
+  return 0;
+}
+
+int agpu_envar_fields(agpu_handle* h, agpu_envar_fields_out* out) {
+  if (!h || !out) return AGPU_E_ARG;
+  std::memset(out, 0, sizeof(*out));
+  CK(cudaMemsetAsync(h->d_envar, 0, sizeof(double) * 16, h->st));
+  if (h->fp32)
+    envar_fields32(h->ebf32, h->g, h->d_envar, h->st, h->sms);
+  else
+    envar_fields64(h->ebf, h->g, h->d_envar, h->st, h->sms);
+  CK(cudaGetLastError());
+  double hd[16];
+  CK(cudaMemcpyAsync(hd, h->d_envar, sizeof(hd), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  // Envar: ekt(1:nfield) = dgvol * sum, dgvol = dx dy dz (2D dx dy dy)
+  const double dgvol = (h->p.ndim == 2) ? h->p.dx * h->p.dy * h->p.dy : h->p.dx * h->p.dy * h->p.dz;
+  for (int c = 0; c < h->g.nf; ++c) {
+    out->energy[c] = dgvol * hd[c];
+    out->fmax[c] = hd[6 + c];
+  }
+  out->e2max = hd[12];
   return 0;
 }
 

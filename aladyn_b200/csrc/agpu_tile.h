@@ -27,6 +27,11 @@ struct TileArgs32 {
   float dth, lfact, dtx, dty, dtz;
   int initial;
   unsigned int* err;
+  // further chunks of dense tiles: (tile, chunk) pairs and the counters
+  // (count, next); null: every tile's CTA runs all its chunks
+  int* work;
+  unsigned int* work_n;
+  int work_cap;
 };
 
 struct TileArgs64 {
@@ -48,7 +53,8 @@ struct TileArgs64 {
 };
 
 TileGeo make_tiles(const Geo& g, int nx, int ny, int nz);
-void tile_push32(const TileArgs32& a, cudaStream_t st);
+int tile_push32(const TileArgs32& a, cudaStream_t st, int sms);
+int tile32_list_cap(int ndim);
 // the cubic shape extension (agpu_tile32c.cu)
 void tile_push32_cubic(const TileArgs32& a, cudaStream_t st);
 void tile_push64(const TileArgs64& a, cudaStream_t st);

@@ -577,8 +577,9 @@ __device__ __forceinline__ void queue_deposit(float* sJ, const float* q, int e) 
 
 }  // namespace
 
+// Particles [beg, end) of tile t (at most LIST_CAP of them).
 template <int NDIM>
-__device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
+__device__ __forceinline__ void d32_chunk(const TileArgs32& a, const int t, const int beg, const int end) {
   using C = CT<NDIM>;
   constexpr int TX = C::TX, TY = C::TY, TZ = C::TZ, NCELL = C::NCELL;
   constexpr int FX = C::FX, FY = C::FY, JX = C::JX, JY = C::JY, JV = C::JV;
@@ -593,8 +594,6 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
   __shared__ int sHist[C::NSUB];
 
   const Geo g = a.g;
-  const int beg = a.tstart[t * a.t.nsub], end = a.tstart[(t + 1) * a.t.nsub];
-  if (beg >= end) return;
   const int tx = t % a.t.ntx, ty = (t / a.t.ntx) % a.t.nty, tz = t / (a.t.ntx * a.t.nty);
   const int i0t = 3 + tx * TX, j0t = 3 + ty * TY, k0t = (NDIM == 3) ? 3 + tz * TZ : 1;
   const int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
@@ -603,11 +602,12 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
   // 1: stage fields (nodes i0t-1 .. i0t+TX), one x-row of FX nodes per
   // warp and pass (lane = node, the first FX - 32 lanes take the rest),
   // zero currents and node counts
+  __syncthreads();  // a previous chunk of this CTA has finished with shared memory
   {
     constexpr int NROW = NF * FY * C::FZ;
     const int gi0 = i0t - 1 + lane, gi1 = gi0 + 32;
     const bool in0 = gi0 >= 1 && gi0 <= g.n1p, in1 = (lane < FX - 32) && gi1 <= g.n1p;
-#pragma unroll 2
+#pragma unroll 4
     for (int row = warp; row < NROW; row += NT / 32) {
       const int c = row / (FY * C::FZ), r = row - c * (FY * C::FZ);
       const int gj = j0t - 1 + r % FY, gk = (NDIM == 3) ? k0t - 1 + r / FY : 1;
@@ -625,8 +625,7 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
   const int kbase = t * C::NSUB;
   __syncthreads();
 
-  const int n = end - beg;
-  if (n <= C::LIST_CAP) {
+  {
     // 2: counting sort of the tile's particles by node; each thread holds
     // its (at most LIST_CAP / NT) record indices and nodes in registers, all
     // loads of a thread in flight together
@@ -774,69 +773,112 @@ __device__ __forceinline__ void d32_tile(const TileArgs32& a, const int t) {
     }
     __syncwarp();
     if (lane < qn) queue_deposit<NDIM>(sJ, qw, lane);
-  } else {
-    // a dense tile: one particle per thread, every deposit on the full window
-    for (int q = beg + threadIdx.x; q < end; q += NT) {
-      const int p = a.perm[q];
-      int i0, j0, k0;
-      cell_split(g, a.p.cell[p], i0, j0, k0);
-      const int lx = i0 - i0t, ly = j0 - j0t, lz = (NDIM == 3) ? k0 - k0t : 0;
-      if ((unsigned)lx >= (unsigned)TX || (unsigned)ly >= (unsigned)TY || (NDIM == 3 && (unsigned)lz >= (unsigned)TZ)) {
-        raise_err(a.err, AGPU_EBIT_INDEX);
-        a.key[p] = a.t.nkeys;
-        hist_add(a.hist, a.t.nkeys);
-        continue;
-      }
-      const Moved m =
-          push_one<NDIM>(a, sF, sHist, kbase, p, load_rec<NDIM>(a, p), i0, j0, k0, lx, ly, lz, nx, ny, nz, false, 0);
-      if (m.keep) deposit_window<NDIM>(sJ, lx, ly, lz, m);
-    }
   }
   __syncthreads();
   // 4: the tile's histogram counts, then one compensated flush of its
-  // currents (nodes i0t-2 ..): four global adds in flight per thread, then
-  // the TwoSum errors of the four into lo
+  // currents (nodes i0t-2 ..)
   for (int e = threadIdx.x; e < C::NSUB; e += NT)
     if (sHist[e]) atomicAdd(&a.hist[kbase + e], sHist[e]);
-  // x-rows of JX nodes, one per warp and pass (lane = node, the first
-  // JX - 32 lanes take the rest): the row's two global adds per lane in
-  // flight together, then their TwoSum errors into lo
+  // x-rows of JX nodes, R per warp and pass (lane = node, the first
+  // JX - 32 lanes take the rest): the rows' global adds in flight together,
+  // then their TwoSum errors into lo
   {
     constexpr int NROW = NC * JY * C::JZ;
     const int gi0 = i0t - 2 + lane;
     const bool xin0 = gi0 >= 1 && gi0 <= g.n1p, xin1 = (lane < JX - 32) && gi0 + 32 <= g.n1p;
-#pragma unroll 2
-    for (int row = warp; row < NROW; row += NT / 32) {
-      const int c = row / (JY * C::JZ), r = row - c * (JY * C::JZ);
-      const int gj = j0t - 2 + r % JY, gk = (NDIM == 3) ? k0t - 2 + r / JY : 1;
-      const bool rin = gj >= 1 && gj <= g.n2p && gk >= 1 && gk <= g.n3p;
-      float v[2] = {sJ[row * JX + lane], (lane < JX - 32) ? sJ[row * JX + 32 + lane] : 0.f};
-      const bool in[2] = {rin && xin0, rin && xin1};
-      const long long o0 = g.ncell * c + goff(g, gi0, gj, gk);
-      float old[2];
+    constexpr int R = 4;  // rows of a warp in flight
+    for (int row0 = warp; row0 < NROW; row0 += R * (NT / 32)) {
+      float v[2 * R], old[2 * R];
+      long long o[R];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        if (v[u] != 0.f && !in[u]) {
-          raise_err(a.err, AGPU_EBIT_INDEX);
-          v[u] = 0.f;
+      for (int u = 0; u < R; ++u) {
+        const int row = row0 + u * (NT / 32);
+        v[2 * u] = v[2 * u + 1] = 0.f;
+        o[u] = 0;
+        if (row < NROW) {
+          const int c = row / (JY * C::JZ), r = row - c * (JY * C::JZ);
+          const int gj = j0t - 2 + r % JY, gk = (NDIM == 3) ? k0t - 2 + r / JY : 1;
+          const bool rin = gj >= 1 && gj <= g.n2p && gk >= 1 && gk <= g.n3p;
+          v[2 * u] = sJ[row * JX + lane];
+          v[2 * u + 1] = (lane < JX - 32) ? sJ[row * JX + 32 + lane] : 0.f;
+          const bool in0 = rin && xin0, in1 = rin && xin1;
+          if ((v[2 * u] != 0.f && !in0) || (v[2 * u + 1] != 0.f && !in1)) {
+            raise_err(a.err, AGPU_EBIT_INDEX);
+            if (!in0) v[2 * u] = 0.f;
+            if (!in1) v[2 * u + 1] = 0.f;
+          }
+          o[u] = g.ncell * c + goff(g, gi0, gj, gk);
         }
-        old[u] = (v[u] != 0.f) ? atomicAdd(&a.jhi[o0 + 32 * u], v[u]) : 0.f;
       }
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        if (v[u] == 0.f) continue;
-        const float sm = __fadd_rn(old[u], v[u]);
-        const float bp = __fsub_rn(sm, old[u]);
-        const float err = __fadd_rn(__fsub_rn(old[u], __fsub_rn(sm, bp)), __fsub_rn(v[u], bp));
-        if (err != 0.f) atomicAdd(&a.jlo[o0 + 32 * u], err);
+      for (int e = 0; e < 2 * R; ++e)
+        old[e] = (v[e] != 0.f) ? atomicAdd(&a.jhi[o[e >> 1] + 32 * (e & 1)], v[e]) : 0.f;
+#pragma unroll
+      for (int e = 0; e < 2 * R; ++e) {
+        if (v[e] == 0.f) continue;
+        const float sm = __fadd_rn(old[e], v[e]);
+        const float bp = __fsub_rn(sm, old[e]);
+        const float err = __fadd_rn(__fsub_rn(old[e], __fsub_rn(sm, bp)), __fsub_rn(v[e], bp));
+        if (err != 0.f) atomicAdd(&a.jlo[o[e >> 1] + 32 * (e & 1)], err);
       }
     }
   }
 }
 
+// Tile t, first chunk of at most LIST_CAP particles; the CTA lists the
+// tile's further chunks (a dense tile) as (tile, chunk) pairs for
+// k32_tile_more.
+template <int NDIM>
+__device__ __forceinline__ void d32_tile_first(const TileArgs32& a, const int t) {
+  constexpr int CAP = CT<NDIM>::LIST_CAP;
+  const int beg = a.tstart[t * a.t.nsub], end = a.tstart[(t + 1) * a.t.nsub];
+  if (beg >= end) return;
+  const int nch = (end - beg + CAP - 1) / CAP;
+  if (nch > 1 && threadIdx.x == 0) {
+    const unsigned base = atomicAdd(&a.work_n[0], (unsigned)(nch - 1));
+    for (int c = 1; c < nch; ++c) {
+      const unsigned e = base + (unsigned)(c - 1);
+      if (e < (unsigned)a.work_cap) {
+        a.work[2 * e] = t;
+        a.work[2 * e + 1] = c;
+      } else {
+        raise_err(a.err, AGPU_EBIT_CAPACITY);  // cannot happen: the list holds capacity / LIST_CAP chunks
+      }
+    }
+  }
+  d32_chunk<NDIM>(a, t, beg, min(end, beg + CAP));
+}
+
+// Tile t, all its chunks in turn (the multi-instance kernel, no work list).
+template <int NDIM>
+__device__ __forceinline__ void d32_tile_all(const TileArgs32& a, const int t) {
+  constexpr int CAP = CT<NDIM>::LIST_CAP;
+  const int beg = a.tstart[t * a.t.nsub], end = a.tstart[(t + 1) * a.t.nsub];
+  for (int c = beg; c < end; c += CAP) d32_chunk<NDIM>(a, t, c, min(end, c + CAP));
+}
+
 template <int NDIM>
 __global__ void __launch_bounds__(NT, (NDIM == 3) ? 2 : 3) k32_tile(TileArgs32 a) {
-  d32_tile<NDIM>(a, blockIdx.x);
+  d32_tile_first<NDIM>(a, blockIdx.x);
+}
+
+// The listed further chunks of dense tiles, pulled by a fixed grid of CTAs
+// from a shared counter (the list is complete: k32_tile has finished).
+template <int NDIM>
+__global__ void __launch_bounds__(NT, (NDIM == 3) ? 2 : 3) k32_tile_more(TileArgs32 a) {
+  constexpr int CAP = CT<NDIM>::LIST_CAP;
+  __shared__ unsigned s_item;
+  const unsigned total = min(a.work_n[0], (unsigned)a.work_cap);
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(&a.work_n[1], 1u);
+    __syncthreads();
+    const unsigned item = s_item;
+    if (item >= total) return;
+    const int t = a.work[2 * item], c = a.work[2 * item + 1];
+    const int beg = a.tstart[t * a.t.nsub], end = a.tstart[(t + 1) * a.t.nsub];
+    d32_chunk<NDIM>(a, t, beg + c * CAP, min(end, beg + (c + 1) * CAP));
+  }
 }
 
 // One block per tile of any instance: instance i owns the global tiles
@@ -850,23 +892,34 @@ __global__ void __launch_bounds__(NT, (NDIM == 3) ? 2 : 3) km32_tile(const Multi
     const int mid = (lo + hi) >> 1;
     if (__ldg(&tile_off[mid]) <= b) lo = mid; else hi = mid;
   }
-  d32_tile<NDIM>(d[lo].ta, b - __ldg(&tile_off[lo]));
+  d32_tile_all<NDIM>(d[lo].ta, b - __ldg(&tile_off[lo]));
 }
 
 size_t tile32_smem(int ndim) { return sizeof(float) * (size_t)((ndim == 3) ? CT<3>::WORDS : CT<2>::WORDS); }
 
-void tile_push32(const TileArgs32& a, cudaStream_t st) {
-  if (a.t.ntiles <= 0) return;
+int tile32_list_cap(int ndim) { return (ndim == 3) ? CT<3>::LIST_CAP : CT<2>::LIST_CAP; }
+
+// Returns the kernels launched (the work-list counters are reset here).
+int tile_push32(const TileArgs32& a, cudaStream_t st, int sms) {
+  if (a.t.ntiles <= 0) return 0;
   const size_t sm = tile32_smem(a.g.ndim);
+  if (a.work) cudaMemsetAsync(a.work_n, 0, 2 * sizeof(unsigned int), st);
   if (a.g.ndim == 3) {
     auto k = k32_tile<3>;
+    auto k2 = k32_tile_more<3>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k<<<a.t.ntiles, NT, sm, st>>>(a);
+    if (a.work) k2<<<2 * sms, NT, sm, st>>>(a);
   } else {
     auto k = k32_tile<2>;
+    auto k2 = k32_tile_more<2>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k<<<a.t.ntiles, NT, sm, st>>>(a);
+    if (a.work) k2<<<3 * sms, NT, sm, st>>>(a);
   }
+  return a.work ? 2 : 1;
 }
 
 void multi_tile32(const MultiInst* d, const int* tile_off, const MultiPlan& pl, cudaStream_t st, int* launches) {

@@ -388,39 +388,81 @@ void f32pair_to_f64(const float* hi, const float* lo, double* b, long long n, cu
 }
 
 // ============================================================================
-// Laser: linearly polarised (y) paraxial Gaussian pulse moving along +x,
-// Ey on (i, j+1/2, k) and Bz = Ey(x + dx/2) on (i+1/2, j+1/2, k), both at
-// t = 0; Gaussian longitudinal envelope exp(-((x-xc)/w0_x)^2) with
-// w0_x = tau_fwhm / sqrt(2 ln 2) as the reference's g_prof pulse
-// (set_init_param.f90:318-330).  Interior nodes only.
+// Laser: init_lp_inc0_fields (src/fields/init_grid_fields.f90:992-1386),
+// lp = 1 (linear polarisation, normal incidence): every interior node gets
+// ee0 times the pulse field of its component at the component's staggered
+// position.  lp_fields is get_laser_gprof_fields_lp / get_laser_fields_lp
+// (init_grid_fields.f90:487-578) in 3D and their 2D forms (406-485), in the
+// reference's order of operations; (cx, cy, cz) = position - (xf0, yc, zc),
+// a.t1 = t_loc - tf.  FP64 throughout (this file is built without FMA
+// contraction).
 // ============================================================================
-__device__ double laser_ey(const LaserArgs& a, double x, double y, double z) {
-  double xi = x - a.xf;
-  double zr = a.zr;
-  double wr = a.w0 * sqrt(1.0 + (xi / zr) * (xi / zr));
-  double r2 = (y - a.y0) * (y - a.y0);
-  if (a.ndim == 3) r2 += (z - a.z0) * (z - a.z0);
-  double rinv = xi / (xi * xi + zr * zr);
-  double gouy = atan(xi / zr);
-  double amp = (a.ndim == 3) ? a.w0 / wr : sqrt(a.w0 / wr);
-  double ph = a.k0 * (x - a.xc) + 0.5 * a.k0 * r2 * rinv - ((a.ndim == 3) ? gouy : 0.5 * gouy);
-  double ex = (x - a.xc) / a.w0x;
-  return a.amp * amp * exp(-r2 / (wr * wr)) * exp(-ex * ex) * cos(ph);
+__device__ void lp_fields(const LaserArgs& a, double cx, double cy, double cz, double f[6]) {
+  const double pi = 3.141592653589793;
+  double x1 = cx;
+  const double y1 = cy / a.wy;
+  const double z1 = (a.ndim == 3) ? cz / a.wy : 0.0;
+  const double t1 = a.t1;
+  const double r2 = (a.ndim == 3) ? y1 * y1 + z1 * z1 : y1 * y1;
+  const double phi0 = a.om0 * (t1 - x1);
+  double phi1;
+  if (a.g_prof) {
+    phi1 = (t1 - x1) / a.wx;
+  } else {
+    phi1 = pi * (t1 - x1) / a.wx;
+    if (fabs(phi1) > 0.5 * pi) phi1 = 0.5 * pi;
+  }
+  x1 = x1 / a.zra;
+  const double w2 = 1. / (1. + x1 * x1);
+  const double phx = (a.ndim == 3) ? atan(x1) : 0.5 * atan(x1);
+  const double phig00 = phi0 + phx - x1 * r2 * w2;
+  const double phig10 = phig00 + phx;
+  const double tshape = a.g_prof ? exp(-phi1 * phi1) : cos(phi1) * cos(phi1);
+  const double wshape = ((a.ndim == 3) ? sqrt(w2) : sqrt(sqrt(w2))) * exp(-w2 * r2);
+  const double ampl = tshape * sin(phig00);
+  f[1] = wshape * ampl;
+  // the 3D Gaussian form multiplies in another order (init_grid_fields.f90:570)
+  const double ampl_1 = (a.g_prof && a.ndim == 3) ? 2. * a.eps * tshape * w2 * exp(-w2 * r2)
+                                                  : tshape * 2. * a.eps * w2 * exp(-w2 * r2);
+  f[0] = y1 * ampl_1 * cos(phig10);
+  f[3] = (a.ndim == 3) ? z1 * ampl_1 * cos(phig10) : 0.0;
+  f[5] = f[1];
+  f[2] = 0.0;
+  f[4] = 0.0;
 }
 __global__ void k_laser64(LaserArgs a, double* ebf, Geo g) {
-  int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
-  long long total = (long long)nx * ny * nz;
-  int cey = 1, cbz = g.nf - 1;
+  const int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
+  const long long total = (long long)nx * ny * nz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int i = g.ix1 + (int)(t % nx);
-    int j = g.jy1 + (int)((t / nx) % ny);
-    int k = g.kz1 + (int)(t / ((long long)nx * ny));
-    double x = a.xmn + (double)(i - 3) * a.dx;
-    double y = a.ymn + ((double)(j - 3) + 0.5) * a.dy;
-    double z = (g.ndim == 3) ? a.zmn + (double)(k - 3) * a.dz : 0.0;
-    long long o = goff(g, i, j, k);
-    ebf[g.ncell * cey + o] += laser_ey(a, x, y, z);
-    ebf[g.ncell * cbz + o] += laser_ey(a, x + 0.5 * a.dx, y, z);
+    const int i = g.ix1 + (int)(t % nx);
+    const int j = g.jy1 + (int)((t / nx) % ny);
+    const int k = g.kz1 + (int)(t / ((long long)nx * ny));
+    const double xx = a.xmn + a.dx * (double)(i - 3), xxh = xx + 0.5 * a.dx;
+    const double yy = a.ymn + a.dy * (double)(j - 3), yyh = yy + 0.5 * a.dy;
+    const double zz = (g.ndim == 3) ? a.zmn + a.dz * (double)(k - 3) : 0.0, zzh = zz + 0.5 * a.dz;
+    const long long o = goff(g, i, j, k);
+    double f[6];
+    if (g.ndim == 3) {
+      lp_fields(a, xxh - a.xf0, yy - a.ycent, zz - a.zcent, f);  // Ex(xxh, yy, zz)
+      ebf[o] += a.ee0 * f[0];
+      lp_fields(a, xx - a.xf0, yyh - a.ycent, zz - a.zcent, f);  // Ey(xx, yyh, zz)
+      ebf[g.ncell + o] += a.ee0 * f[1];
+      lp_fields(a, xx - a.xf0, yy - a.ycent, zzh - a.zcent, f);  // Ez(xx, yy, zzh)
+      ebf[2 * g.ncell + o] += a.ee0 * f[2];
+      lp_fields(a, xx - a.xf0, yyh - a.ycent, zzh - a.zcent, f);  // Bx(xx, yyh, zzh)
+      ebf[3 * g.ncell + o] += a.ee0 * f[3];
+      lp_fields(a, xxh - a.xf0, yy - a.ycent, zzh - a.zcent, f);  // By(xxh, yy, zzh)
+      ebf[4 * g.ncell + o] += a.ee0 * f[4];
+      lp_fields(a, xxh - a.xf0, yyh - a.ycent, zz - a.zcent, f);  // Bz(xxh, yyh, zz)
+      ebf[5 * g.ncell + o] += a.ee0 * f[5];
+    } else {
+      lp_fields(a, xxh - a.xf0, yy - a.ycent, 0.0, f);  // Ex(xxh, yy)
+      ebf[o] += a.ee0 * f[0];
+      lp_fields(a, xx - a.xf0, yyh - a.ycent, 0.0, f);  // Ey(xx, yyh)
+      ebf[g.ncell + o] += a.ee0 * f[1];
+      lp_fields(a, xxh - a.xf0, yyh - a.ycent, 0.0, f);  // Bz(xxh, yyh)
+      ebf[2 * g.ncell + o] += a.ee0 * f[5];
+    }
   }
 }
 void laser64(const LaserArgs& a, double* ebf, const Geo& g, cudaStream_t st, int sms) {

@@ -40,9 +40,11 @@ struct LatticeArgs {
   uint64_t seed;
 };
 
+// init_lp_inc0_fields for one pulse (lp = 1): par_lp of the reference and
+// the grid of the set-up
 struct LaserArgs {
-  int ndim;
-  double amp, k0, w0, zr, w0x, xc, xf, y0, z0;
+  int ndim, g_prof;
+  double ee0, t1, xf0, om0, wx, wy, zra, eps, ycent, zcent;
   double xmn, ymn, zmn, dx, dy, dz;
 };
 
@@ -78,6 +80,12 @@ void field_diag32(const float* ebf, const Geo& g, double dvol, double* out_e, do
 void part_diag64(const double* part, long long ld, long long n, int nd, const int* perm, double* out, cudaStream_t st,
                  int sms);
 void part_diag32(const Part32View& p, long long n, int nd, const int* perm, double* out, cudaStream_t st, int sms);
+// Envar reductions (agpu_envar.cu): per species into d_out[0..16+AGPU_NE)
+// (ek(1:7), ekmax, psig(1:3), nde(1:ne) at 16..), fields into d_out[0..13)
+void envar_species(const double* part, long long ld, const Part32View* sp, const int* perm, long long n, const Geo& g,
+                   double ymn, double zmn, double dy, double dz, double pmass, double* d_out, cudaStream_t st, int sms);
+void envar_fields64(const double* ebf, const Geo& g, double* d_out, cudaStream_t st, int sms);
+void envar_fields32(const float* ebf, const Geo& g, double* d_out, cudaStream_t st, int sms);
 void max_nonneg(const double* a, long long n, double* out, cudaStream_t st, int sms);
 
 }  // namespace agpu

@@ -160,6 +160,9 @@ class PicDevice:
     def init_laser(self, laser):
         check(self.lib.agpu_init_laser(self.h, C.byref(laser)), "agpu_init_laser")
 
+    def init_lp_fields(self, pulse):
+        check(self.lib.agpu_init_lp_fields(self.h, C.byref(pulse)), "agpu_init_lp_fields")
+
     def set_ionization_species(self, ic, atomic_number, ion_min, ion_max, model, lp_max):
         check(self.lib.agpu_set_ionization_species(self.h, ic, atomic_number, ion_min, ion_max,
                                                    model, lp_max), "agpu_set_ionization_species")
@@ -184,6 +187,16 @@ class PicDevice:
         return out
 
     # -- control / profiling --------------------------------------------------
+    def envar_species(self, ic: int, pmass: float) -> "abi.AgpuEnvarOut":
+        o = abi.AgpuEnvarOut()
+        check(self.lib.agpu_envar_species(self.h, ic, pmass, C.byref(o)), "agpu_envar_species")
+        return o
+
+    def envar_fields(self) -> "abi.AgpuEnvarFieldsOut":
+        o = abi.AgpuEnvarFieldsOut()
+        check(self.lib.agpu_envar_fields(self.h, C.byref(o)), "agpu_envar_fields")
+        return o
+
     def set_deterministic(self, on: bool = True):
         check(self.lib.agpu_set_deterministic(self.h, 1 if on else 0), "agpu_set_deterministic")
 

@@ -269,9 +269,15 @@ def timed_steps(dev, p, t, it, k, torch):
     return e0.elapsed_time(e1), nsum, t, it, out
 
 
-def run_form(name, precision, warmup, steps, torch, barrier, keep_fields=False):
-    """Warm-up, then the timed region with profiling timers on."""
+def run_form(name, precision, warmup, steps, torch, barrier, keep_fields=False, graphs=False):
+    """Warm-up, then the timed region with profiling timers on.  graphs:
+    deferred counts and step graphs (the library's fastest form of a step
+    on small grids, where launches dominate); the pushes then come from the
+    library's own counters."""
     dev, p, las, src, ppc = load_device(name, precision)
+    if graphs:
+        dev.set_deferred_counts(True)
+        dev.set_step_graphs(True)
     t, it = 0.0, 0
     for _ in range(warmup):
         dev.lp_run(t, it, initial_time=(it == 0))
@@ -281,6 +287,9 @@ def run_form(name, precision, warmup, steps, torch, barrier, keep_fields=False):
     dev.reset_timers()
     barrier()
     ms, pushes, t, it, out = timed_steps(dev, p, t, it, steps, torch)
+    if graphs:
+        dev.set_deferred_counts(False)  # synchronises and refreshes the counters
+        pushes = dev.timers().pushes
     tm = dev.timers()
     fields = dev.get_fields() if keep_fields else None
     res = dict(ms=ms, pushes=pushes, np=out.np[0], err=out.error_bits, timers=tm, p=p, ppc=ppc,
@@ -433,14 +442,16 @@ def make_reducers(torch, world: int, device: str):
     return barrier, (lambda x: red(x, dist.ReduceOp.MAX)), (lambda x: red(x, dist.ReduceOp.SUM))
 
 
-def bench_scan(a, torch):
-    """Batched scan: the 256 instances advanced together (agpu_batch_run)
-    against the same instances run one after the other through agpu_step.
-    Both arms: fresh instances, W warm-up steps, then K timed steps; device
-    time by CUDA events bracketing the timed steps after a synchronisation."""
+def scan_measure(torch, warmup, steps, threads=0, n=256):
+    """Batched scan: the n instances advanced together (agpu_batch_run)
+    against the same instances run one after the other through the
+    single-instance path in its fastest form (deferred counts, each step
+    replayed from its captured CUDA graph), so that the ratio measures the
+    batching, not removed host synchronisations.  Both arms: fresh
+    instances, W warm-up steps, then K timed steps; device time by CUDA
+    events bracketing the timed steps after a synchronisation."""
     from aladyn_b200.abi import AGPU_FP32_SPLIT
     from aladyn_b200.sim import PicBatch, PicDevice
-    n = 256
     cases = scan_instances(n, AGPU_FP32_SPLIT)
     for p, _, _ in cases:  # headroom: the lasers push electrons forward as the window injects
         p.capacity[0] = int(p.capacity[0] * 1.5)
@@ -453,46 +464,47 @@ def bench_scan(a, torch):
     def ev():
         return torch.cuda.Event(enable_timing=True)
 
-    clk = ClockSampler(torch.cuda.current_device())
-    if not a.no_clocks:
-        clk.start()
     # batched arm
     batch = PicBatch([c[0] for c in cases])
     for d, (p, las, src) in zip(batch.instances, cases):
         setup(d, las, src)
-    st = batch.run(a.warmup, a.scan_threads)
-    assert st == [0] * n, st
+    st = batch.run(warmup, threads)
+    if st != [0] * n:
+        raise RuntimeError(f"batched warm-up failed: {st}")
     for d in batch.instances:
         d.reset_timers()
     launches0 = batch.launches()
     torch.cuda.synchronize()
     e0, e1 = ev(), ev()
     e0.record()
-    st = batch.run(a.steps, a.scan_threads)
+    st = batch.run(steps, threads)
     e1.record()
     e1.synchronize()
     ms_b = e0.elapsed_time(e1)
-    assert st == [0] * n, st
+    if st != [0] * n:
+        raise RuntimeError(f"batched steps failed: {st}")
     tms = [d.timers() for d in batch.instances]
     pushes_b = sum(t.pushes for t in tms)
     launches_b = sum(t.launches_total for t in tms) + batch.launches() - launches0
     batch.close()
-    # sequential arm: one instance at a time through the single-instance path
+    # sequential arm: one instance at a time, deferred counts + step graphs
     ms_s, pushes_s = 0.0, 0
     for (p, las, src) in cases:
         dev = PicDevice(p)
         setup(dev, las, src)
+        dev.set_deferred_counts(True)
+        dev.set_step_graphs(True)
         t, it = 0.0, 0
-        for _ in range(a.warmup):
+        for _ in range(warmup):
             dev.lp_run(t, it, initial_time=(it == 0))
             t += p.dt
             it += 1
-        dev.reset_timers()
         dev.synchronize()
+        dev.reset_timers()
         torch.cuda.synchronize()
         e0, e1 = ev(), ev()
         e0.record()
-        for _ in range(a.steps):
+        for _ in range(steps):
             dev.lp_run(t, it, initial_time=(it == 0))
             t += p.dt
             it += 1
@@ -500,24 +512,268 @@ def bench_scan(a, torch):
         e1.record()
         e1.synchronize()
         ms_s += e0.elapsed_time(e1)
+        dev.set_deferred_counts(False)  # refreshes the push count on the host
         pushes_s += dev.timers().pushes
         dev.close()
-    clocks = clk.stop()
-    value = n * a.steps / (ms_b * 1e-3)
-    seq = n * a.steps / (ms_s * 1e-3)
     cells = sum(c[0].nx * c[0].ny for c in cases)
-    line = {"metric": "instance-steps/s", "value": value, "unit": "instance-steps/s", "n_gpus": 1,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_b / a.steps, "higher_is_better": True,
+    return dict(ms_b=ms_b, ms_s=ms_s, pushes_b=pushes_b, pushes_s=pushes_s, launches_b=launches_b, cells=cells,
+                value=n * steps / (ms_b * 1e-3), sequential=n * steps / (ms_s * 1e-3), n=n)
+
+
+# --------------------------------------------------------------------------
+# the other configurations, measured beside the headline workload
+# --------------------------------------------------------------------------
+def _guard(fn, *args):
+    """One extra measurement; a failure is reported in its key instead of
+    losing the line."""
+    try:
+        return fn(*args)
+    except Exception as e:  # noqa: BLE001
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
+def extra_forms(name, torch, warmup, steps, graphs=False):
+    """Both precision forms of a workload: pushes/s of the full step, the
+    push/deposit kernel's algorithmic GB/s and the Yee phase GB/s."""
+    from aladyn_b200.abi import AGPU_FP32_SPLIT, AGPU_FP64
+    w = WORKLOADS[name]
+    ppc = w["ppc"][0] * w["ppc"][1] * (w["ppc"][2] if w["ndim"] == 3 else 1)
+    out = {"workload": name, "warmup": warmup, "steps": steps,
+           "path": "deferred counts + step graphs" if graphs else "agpu_step, counts every step"}
+    for key, prec in (("fp32_split", AGPU_FP32_SPLIT), ("fp64", AGPU_FP64)):
+        r = run_form(name, prec, warmup, steps, torch, lambda: torch.cuda.synchronize(), graphs=graphs)
+        tm, p = r["timers"], r["p"]
+        cells = p.nx * p.ny * (p.nz if p.ndim == 3 else 1)
+        fp32 = prec == AGPU_FP32_SPLIT
+        out[key] = {"pushes_per_s": r["pushes"] / (r["ms"] * 1e-3), "ms_per_step": r["ms"] / steps,
+                    "push_deposit_gbs": bytes_per_push(w["ndim"], ppc, fp32) * tm.pushes /
+                    (tm.ms_push_deposit * 1e-3) / 1e9 if tm.ms_push_deposit else None,
+                    "yee_gbs": yee_bytes_per_cell(p.ndim, fp32) * cells * steps / (tm.ms_yee * 1e-3) / 1e9
+                    if tm.ms_yee else None,
+                    "error_bits": r["err"]}
+    out["fp32_over_fp64"] = out["fp32_split"]["pushes_per_s"] / out["fp64"]["pushes_per_s"]
+    return out
+
+
+def extra_ionization(torch, warmup, steps):
+    """3D ionization-injection LWFA (768x192x192, dx = 0.05 lambda, dy = dz =
+    0.25 lambda): pre-ionised electrons at n_e = 0.005 n_c plus a 1%
+    nitrogen dopant of neutral atoms (7 levels, one-level ADK model 1,
+    Philox draws), 4 particles per cell each, laser a0 = 1.8, waist 6
+    lambda, FWHM 10 lambda/c focused in the plasma.  Both forms: pushes/s
+    (electrons) and the electrons born during the timed steps."""
+    from aladyn_b200.abi import AGPU_FP32_SPLIT, AGPU_FP64
+    from aladyn_b200.config import Grid, laser, make_params, n_over_nc_to_n0, plasma
+    from aladyn_b200.sim import PicDevice
+    nx, ny, nz, a0 = 768, 192, 192, 1.8
+    g = Grid(3, nx, ny, nz, 25.0, 5.0, 5.0, 0.8)
+    ncell = nx * ny * nz
+    n0 = n_over_nc_to_n0(0.005, LAM0)
+    lp_max = 1.5 * a0 * 2.0 * math.pi / LAM0
+    out = {"grid": [nx, ny, nz], "ppc_each": 4, "dopant": "N, 1% of n_e, 7 levels, ADK model 1",
+           "warmup": warmup, "steps": steps}
+    for key, prec in (("fp32_split", AGPU_FP32_SPLIT), ("fp64", AGPU_FP64)):
+        p = make_params(g, precision=prec, nsp=2, nsp_run=1, capacity=(int(ncell * 4 * 1.5), int(ncell * 4 * 1.04), 0, 0),
+                        w_sh=10, ionz_lev=1, n_mol_atoms=(1, 1, 1, 1), mass_number=(14.0, 1.0, 1.0))
+        lx = nx * p.dx
+        dev = PicDevice(p)
+        dev.init_laser(laser(a0, LAM0, 6 * LAM0, 10 * LAM0, xc=0.6 * lx, xf=0.6 * lx))
+        x0 = p.gxmin + 0.3 * lx
+        dev.set_plasma_source(plasma(0, 2, 2, 1, -1, n0 / 4, x_start=x0, x_end=1.0e7, y_min=p.gymin,
+                                     y_max=p.gymax, z_min=p.gzmin, z_max=p.gzmax, jitter=0.5, seed=20241204))
+        dev.set_plasma_source(plasma(1, 2, 2, 1, 0, 0.01 * n0 / 4, x_start=x0, x_end=1.0e7, y_min=p.gymin,
+                                     y_max=p.gymax, z_min=p.gzmin, z_max=p.gzmax, jitter=0.5, seed=20241205))
+        dev.load_plasma(0)
+        dev.load_plasma(1)
+        dev.set_ionization_species(1, 7, 0, 7, 1, lp_max)
+        t, it = 0.0, 0
+        for _ in range(warmup):
+            dev.lp_run(t, it, initial_time=(it == 0))
+            t += p.dt
+            it += 1
+        dev.set_profiling(True)
+        dev.reset_timers()
+        s = torch.cuda.ExternalStream(dev.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        dev.synchronize()
+        e0.record(s)
+        born, pushed, err = 0, 0, 0
+        for _ in range(steps):
+            o = dev.lp_run(t, it)
+            born += o.new_electrons
+            pushed += o.np[0] + o.removed[0] - o.injected[0] - o.new_electrons
+            err |= o.error_bits
+            t += p.dt
+            it += 1
+        e1.record(s)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        tm = dev.timers()
+        out[key] = {"electron_pushes_per_s": pushed / (ms * 1e-3), "ms_per_step": ms / steps,
+                    "ionize_ms_per_step": tm.ms_ionize / steps, "electrons_born": int(born),
+                    "electrons": int(dev.count(0)), "ions": int(dev.count(1)), "error_bits": int(err)}
+        dev.close()
+    b32, b64 = out["fp32_split"]["electrons_born"], out["fp64"]["electrons_born"]
+    out["born_fp32_over_fp64"] = b32 / b64 if b64 else None
+    out["fp32_over_fp64"] = out["fp32_split"]["electron_pushes_per_s"] / out["fp64"]["electron_pushes_per_s"]
+    return out
+
+
+def extra_pwfa(torch, warmup, steps):
+    """3D beam-driven PWFA, FP32 split form: 512x256x256 cells, dx = 0.2 um,
+    dy = dz = 0.5 um, plasma n_e = 1e17 cm^-3 at 4 particles per cell, a
+    bi-Gaussian driver of 2e7 macroparticles (200 pC, gamma 1957, 1% rms
+    energy spread, sigma_z = 5 um, sigma_r = 3 um, 1 mm mrad); the bunch
+    set-up (charge deposit and the FP64 sine-transform Poisson solve of its
+    self-fields, agpu_beam_inject) timed once, then the standard cycle."""
+    from aladyn_b200.abi import AGPU_FP32_SPLIT
+    from aladyn_b200.beam import Bunch, bunch_records
+    from aladyn_b200.config import Grid, make_params, plasma
+    from aladyn_b200.sim import PicDevice
+    nx, ny, nz, nb = 512, 256, 256, 20_000_000
+    g = Grid(3, nx, ny, nz, 5.0, 2.5, 2.5, 0.8)
+    ncell = nx * ny * nz
+    p = make_params(g, precision=AGPU_FP32_SPLIT, capacity=(int(ncell * 4 * 1.04) + nb + 4096, 0, 0, 0), w_sh=10)
+    lx = nx * p.dx
+    b = Bunch(nb_tot=nb, charge_pc=200.0, sxb=5.0, syb=3.0, gam=1957.0, epsy=1.0, epsz=1.0, dg=1.0,
+              xc=p.xmn + 0.6 * lx, seed=77)
+    t0 = time.perf_counter()
+    rec = bunch_records(p, b, n0_ref=0.1)
+    gen_s = time.perf_counter() - t0
+    dev = PicDevice(p)
+    dev.set_plasma_source(plasma(0, 2, 2, 1, -1, 0.25, x_start=p.gxmin, x_end=1.0e7, y_min=p.gymin, y_max=p.gymax,
+                                 z_min=p.gzmin, z_max=p.gzmax, jitter=0.5, seed=20241206))
+    dev.load_plasma(0)
+    dev.synchronize()
+    t0 = time.perf_counter()
+    rc = dev.beam_inject(0, rec, b.gam)
+    dev.synchronize()
+    setup_s = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError(f"agpu_beam_inject returned {rc}")
+    n = dev.count(0)
+    t, it = 0.0, 0
+    for _ in range(warmup):
+        dev.lp_run(t, it, initial_time=(it == 0))
+        t += p.dt
+        it += 1
+    dev.set_profiling(True)
+    dev.reset_timers()
+    ms, pushes, t, it, o = timed_steps(dev, p, t, it, steps, torch)
+    tm = dev.timers()
+    dev.close()
+    return {"grid": [nx, ny, nz], "bunch_macroparticles": nb, "particles": int(n), "form": "fp32_split",
+            "bunch_setup_s": setup_s, "bunch_records_host_s": gen_s,
+            "setup_note": "agpu_beam_inject wall time: record upload, charge deposit, FP64 DST-I Poisson "
+                          "solve (cuFFT), bunch fields",
+            "pushes_per_s": pushes / (ms * 1e-3), "ms_per_step": ms / steps,
+            "push_deposit_ms_per_step": tm.ms_push_deposit / steps, "warmup": warmup, "steps": steps,
+            "error_bits": int(o.error_bits)}
+
+
+def extra_scan(torch, warmup, steps):
+    r = scan_measure(torch, warmup, steps, 0)
+    return {"instances": r["n"], "warmup": warmup, "steps": steps,
+            "batched_instance_steps_per_s": r["value"], "sequential_instance_steps_per_s": r["sequential"],
+            "batched_over_sequential": r["value"] / r["sequential"],
+            "sequential_path": "agpu_step per instance, one after the other, deferred counts and step graphs",
+            "batched_gpu_launches": int(r["launches_b"])}
+
+
+def extra_continuity(torch):
+    """Discrete continuity residual of one step (rho1 - rho0 + c div J_raw,
+    FP64 on the host from the records before and after the step and the
+    step's currents) relative to max |rho|, both forms, on the 3D
+    128x64x64 and the 2D 1024x256 workloads, step 8 (the laser is in the
+    plasma, no window shift yet); nodes within 5 of the array edges (folded
+    ghost currents, box-edge removal) are left out."""
+    from aladyn_b200.abi import AGPU_FP32_SPLIT, AGPU_FP64
+    from aladyn_b200.conservation import step_residual
+    out = {"definition": "max|rho1 - rho0 + c div J_raw| / max|rho0|, c = 1/3 (3D), 1/2 (2D), one step"}
+    for name in ("lwfa3d_128x64x64_ppc8", "lwfa2d_1024x256_ppc4"):
+        res = {}
+        for key, prec in (("fp32_split", AGPU_FP32_SPLIT), ("fp64", AGPU_FP64)):
+            dev, p, las, src, ppc = load_device(name, prec)
+            t = 0.0
+            for it in range(8):  # the first window shift comes at step 10
+                dev.lp_run(t, it, initial_time=(it == 0))
+                t += p.dt
+            part0 = dev.get_species(0)
+            dev.lp_run(t, 8)
+            part1 = dev.get_species(0)
+            q = type(p).from_buffer_copy(p)
+            q.xmn = dev.window_state()[3]
+            r, rho, divj = step_residual(q, part0, part1, dev.get_currents(), margin=5)
+            res[key] = {"residual_rel": r / rho, "max_c_div_j_rel": divj / rho}
+            dev.close()
+        out[name] = res
+    return out
+
+
+def extra_accuracy(torch, steps=1000):
+    """FP32 split vs FP64 field error after a long run on the physical box of
+    the 1024x256x256 workload at 3/8 of its resolution (384x96x96 cells, 8
+    ppc, 2.8e7 electrons, moving window): relative L2 per component."""
+    from aladyn_b200.abi import AGPU_FP32_SPLIT, AGPU_FP64
+    name = "lwfa3d_384x96x96_ppc8"
+    f = {}
+    for key, prec in (("fp64", AGPU_FP64), ("fp32_split", AGPU_FP32_SPLIT), ("fp64_rerun", AGPU_FP64)):
+        dev, p, las, src, ppc = load_device(name, prec, cap_factor=1.6)
+        t = 0.0
+        for it in range(steps):
+            dev.lp_run(t, it, initial_time=(it == 0))
+            t += p.dt
+        f[key] = (dev.get_fields(), dev.count(0))
+        dev.close()
+
+    def total(fa, fb):
+        sl = (slice(2, p.nx + 2), slice(2, p.ny + 2), slice(2, p.nz + 2), slice(None))
+        return float(np.linalg.norm(fa[sl] - fb[sl]) / np.linalg.norm(fb[sl]))
+
+    err = rel_l2_errors(f["fp32_split"][0], f["fp64"][0], p)
+    ctl = rel_l2_errors(f["fp64_rerun"][0], f["fp64"][0], p)
+    return {"workload": name, "steps": steps, "rel_l2_per_component": err, "max": max(err),
+            "rel_l2_all_components": total(f["fp32_split"][0], f["fp64"][0]),
+            "fp64_rerun_rel_l2_per_component": ctl,
+            "fp64_rerun_rel_l2_all_components": total(f["fp64_rerun"][0], f["fp64"][0]),
+            "control_note": "a second FP64 run differs from the first only by the order of its atomic sums",
+            "electrons": {k: int(v[1]) for k, v in f.items()}}
+
+
+def extras(torch, warmup):
+    k = 5
+    return {
+        "c1_2d": _guard(extra_forms, "lwfa2d_1024x256_ppc4", torch, warmup, 20, True),
+        "c2_cubic": _guard(extra_forms, "lwfa3d_1024x256x256_ppc8_cubic", torch, warmup, k),
+        "c3_pwfa": _guard(extra_pwfa, torch, warmup, k),
+        "c4_ionization": _guard(extra_ionization, torch, warmup, k),
+        "scan": _guard(extra_scan, torch, warmup, 10),
+        "continuity_residual": _guard(extra_continuity, torch),
+        "accuracy_1000_steps": _guard(extra_accuracy, torch),
+    }
+
+
+def bench_scan(a, torch):
+    clk = ClockSampler(torch.cuda.current_device())
+    if not a.no_clocks:
+        clk.start()
+    r = scan_measure(torch, a.warmup, a.steps, a.scan_threads)
+    clocks = clk.stop()
+    n = r["n"]
+    line = {"metric": "instance-steps/s", "value": r["value"], "unit": "instance-steps/s", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": r["ms_b"] / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32-split",
             "data": "synthetic: seeded instance draws, jittered lattice plasma, Gaussian lasers",
             "config": {"workload": SCAN_WORKLOAD, "instances": n, "nx": list(SCAN_NX), "ny": list(SCAN_NY),
-                       "ppc": 4, "cells_total": cells, "window": "moving, w_sh=10",
+                       "ppc": 4, "cells_total": r["cells"], "window": "moving, w_sh=10",
                        "threads": a.scan_threads or os.cpu_count()},
-            "sequential": {"value": seq, "unit": "instance-steps/s", "ms_per_step": ms_s / a.steps,
-                           "path": "agpu_step per instance, one instance after the other"},
-            "batched_over_sequential": value / seq,
-            "pushes_per_s": {"batched": pushes_b / (ms_b * 1e-3), "sequential": pushes_s / (ms_s * 1e-3)},
-            "gpu_launches": int(launches_b), "clocks": clocks}
+            "sequential": {"value": r["sequential"], "unit": "instance-steps/s", "ms_per_step": r["ms_s"] / a.steps,
+                           "path": "agpu_step per instance, one instance after the other, deferred counts and "
+                                   "step graphs"},
+            "batched_over_sequential": r["value"] / r["sequential"],
+            "pushes_per_s": {"batched": r["pushes_b"] / (r["ms_b"] * 1e-3),
+                             "sequential": r["pushes_s"] / (r["ms_s"] * 1e-3)},
+            "gpu_launches": int(r["launches_b"]), "clocks": clocks}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -535,6 +791,7 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-clocks", action="store_true", help="skip nvidia-smi sampling (profiler runs)")
+    ap.add_argument("--no-extras", action="store_true", help="only the headline workload")
     a = ap.parse_args(argv)
     a.warmup = max(a.warmup, 3)
 
@@ -620,6 +877,10 @@ def main(argv=None):
     yee64 = yee_bytes_per_cell(p.ndim, False) * cells * a.steps / (tm64.ms_yee * 1e-3) / 1e9 if tm64.ms_yee else None
     push64 = bytes_per_push(w["ndim"], ppc_w, False) * tm64.pushes / (tm64.ms_push_deposit * 1e-3) / 1e9
 
+    more = {}
+    if world == 1 and not a.no_extras and a.workload == DEFAULT_WORKLOAD:
+        more = extras(torch, a.warmup)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         c = cpu_sample(a.workload, budget_s=a.cpu_budget)
@@ -637,7 +898,7 @@ def main(argv=None):
             "field_error_fp32_vs_fp64": {"rel_l2_per_component": err, "after_steps": a.warmup + a.steps},
             "yee_gbs": {"fp32": yee32, "fp64": yee64,
                         "note": "algorithmic 15 words/cell over the Yee phase (boundaries, current fold, 3 sweeps)"},
-            "roofline": {"bound": "hbm", "kernel": "k32_push_dep (gather+push+deposit, FP32 split)",
+            "roofline": {"bound": "hbm", "kernel": "k32_tile (gather+push+deposit, FP32 split)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
                          "bytes_per_push": bpp,
@@ -652,6 +913,7 @@ def main(argv=None):
             "cpu_baseline": cpu,
             "error_bits": r32["err"] | r64["err"],
         }
+        line.update(more)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -131,9 +131,13 @@ typedef struct agpu_plasma {
   uint64_t seed;           /* Philox key of the jitter                            */
 } agpu_plasma;
 
-/* Linearly polarised (along y) Gaussian laser pulse focused at x = xf,
- * sampled on the staggered grid (the build's synthetic stand-in for
- * init_lp_inc0_fields, src/fields/init_grid_fields.f90:992-1386). */
+/* Linearly polarised (along y) laser pulse with a Gaussian longitudinal
+ * profile (g_prof), focused at x = xf: the namelist quantities from which
+ * lp_pulse (src/IO/init_laser_field.f90:33-100) and set_initial_param
+ * (src/start/set_init_param.f90:291-330) derive the arguments of
+ * init_lp_inc0_fields; agpu_init_laser passes them on as an agpu_lp_pulse
+ * with ee0 = a0 * 2 pi / lam0, om0 = 2 pi / lam0, wx = tau_fwhm / sqrt(2 ln 2),
+ * wy = w0_y, xf0 = xf, tf = xf - xc, t_loc = 0, g_prof = 1. */
 typedef struct agpu_laser {
   double a0;               /* normalised amplitude                                */
   double lam0;             /* wavelength (um)                                     */
@@ -143,6 +147,24 @@ typedef struct agpu_laser {
   double xf;               /* focus position (um)                                 */
   double y0, z0;           /* transverse centre                                   */
 } agpu_laser;
+
+/* The arguments of init_lp_inc0_fields (src/fields/init_grid_fields.f90:
+ * 992-1386) for one linearly polarised pulse at normal incidence (lp = 1,
+ * P mode), whose fields come from get_laser_gprof_fields_lp (g_prof = 1)
+ * or get_laser_fields_lp (g_prof = 0) in 3D (init_grid_fields.f90:487-578)
+ * and their 2D forms (406-485). */
+typedef struct agpu_lp_pulse {
+  double ee0;              /* field amplitude lp_amp = a0 * oml                     */
+  double t_loc;            /* time of the set-up (0)                                */
+  double tf;               /* t0_lp: focus time, xf0 - pulse centre                 */
+  double wx;               /* w0_x: longitudinal profile length                     */
+  double wy;               /* w0_y: waist                                           */
+  double xf0;              /* focus position xf                                     */
+  double om0;              /* oml = 2 pi / lam0                                     */
+  double ycent, zcent;     /* transverse centre                                     */
+  int32_t g_prof;          /* 1: exp(-((t-x)/wx)^2); 0: cos^2(pi (t-x)/wx), |.| <= pi/2 */
+  int32_t reserved;
+} agpu_lp_pulse;
 
 typedef struct agpu_step_out {
   int64_t np[4];           /* particles per species after the step                */
@@ -230,6 +252,12 @@ int agpu_set_window_state(agpu_handle* h, double xlapse, const int64_t* nptx);
 int agpu_set_plasma_source(agpu_handle* h, const agpu_plasma* src);
 int agpu_load_plasma(agpu_handle* h, int32_t ic);
 int agpu_init_laser(agpu_handle* h, const agpu_laser* laser);
+/* init_lp_inc0_fields (src/fields/init_grid_fields.f90:992-1386), lp = 1:
+ * adds the pulse to the fields on the interior nodes, each component
+ * sampled at its staggered position (3D: Ex(xh,y,z), Ey(x,yh,z), Ez(x,y,zh),
+ * Bx(x,yh,zh), By(xh,y,zh), Bz(xh,yh,z); 2D: Ex(xh,y), Ey(x,yh), Bz(xh,yh))
+ * with x = xmn + (i-3) dx, xh = x + dx/2 and y, z alike, in FP64. */
+int agpu_init_lp_fields(agpu_handle* h, const agpu_lp_pulse* pulse);
 
 /* ---- ionization -------------------------------------------------------- */
 /* Upload w_one_lev(0:n_ge+1, 0:zmax) for ion species ic (>= 1), as built by
@@ -329,6 +357,33 @@ int agpu_batch_clock(const agpu_batch* b, int32_t i, int32_t* iter, double* t);
 /* FP64 reductions of Envar / energy_momenta
  * (src/diagnostics/diag_part_and_fields.f90:172-220, 485-719). */
 int agpu_diag(agpu_handle* h, agpu_diag_out* out);
+
+/* The reductions of Envar (src/diagnostics/diag_part_and_fields.f90:485-719)
+ * with energy_momenta (172-220) and energy_spect (126-142), in the
+ * reference's definitions; the host applies pmass, np_per_cell and the unit
+ * constants (mev_to_joule, field_energy, e0) as Envar does. */
+#define AGPU_NE 100              /* energy spectrum bins (ne, diag_part_and_fields.f90:37) */
+typedef struct agpu_envar_out {
+  int64_t np;              /* alive particles of the species                       */
+  double ek[7];            /* energy_momenta's ek(1:7): 3D ek(1:3) = sum p_k
+                              (unweighted), 2D ek(1:2) = sum wgh p_k; ek(4) = sum
+                              wgh (y pz - z py) (3D); ek(5) = 0; ek(6) = sum
+                              real(charge wgh, sp); ek(7) = sum wgh (gamma - 1)  */
+  double ekmax;            /* max (gamma - 1)                                      */
+  double psig[3];          /* sum (p_k - ek(k)/np)^2, k <= curr_ndim (Envar 594-604) */
+  double nde[AGPU_NE];     /* energy_spect: weights wgh in bins min(nint(pmass
+                              (gamma-1) / de) + 1, ne), de = pmass ekmax / ne;
+                              zero when pmass ekmax < 1e-6                        */
+} agpu_envar_out;
+typedef struct agpu_envar_fields_out {
+  double energy[6];        /* dgvol * sum over interior nodes of F_c^2, dgvol =
+                              dx dy dz (2D: dx dy dy), components past nfield 0  */
+  double fmax[6];          /* max |F_c| over the interior nodes                     */
+  double e2max;            /* max over nodes of sum_{c <= curr_ndim} E_c^2          */
+} agpu_envar_fields_out;
+/* Species ic with its pmass = electron_mass * mass(ic) (MeV). */
+int agpu_envar_species(agpu_handle* h, int32_t ic, double pmass, agpu_envar_out* out);
+int agpu_envar_fields(agpu_handle* h, agpu_envar_fields_out* out);
 
 /* Field diagnostics for callers that cannot allocate device memory (a host
  * inside a CUDA stream capture, a host whose device memory comes from its

@@ -2128,3 +2128,212 @@ int ora_beam_inject(ora_sim* s, int ic, const double* part, int64_t ld, int64_t 
   free(efb);
   return 0;
 }
+
+/* ======================================================================== */
+/* A21: init_lp_inc0_fields (src/fields/init_grid_fields.f90:992-1386),     */
+/* lp = 1 (P polarisation, normal incidence), with get_laser_gprof_fields_lp */
+/* / get_laser_fields_lp (487-578) and the 2D forms (406-485).  Grid        */
+/* coordinates of the interior nodes: x = xmn + (i-3) dx, xh = x + dx/2,    */
+/* y and z alike (x(i) = dx*(i-1), xh = x + 0.5 dx, set_grid_param.f90:77-78,*/
+/* 129-130, 187-188, with the box origin of the parameters).                */
+/* ======================================================================== */
+static void ora_lp_fields(int ndim, int g_prof, const double par_lp[7], const double coords[4], double fields[6]) {
+  const double pi = acos(-1.0);
+  double x1, y1, z1 = 0.0, t1, pih, r2, phi0, phi1, w2, phx, phig00, phig10, tshape, wshape, ampl, ampl_1;
+  x1 = coords[0];
+  y1 = coords[1] / par_lp[3];
+  if (ndim == 3) z1 = coords[2] / par_lp[3];
+  t1 = coords[3];
+  pih = 0.5 * pi;
+  r2 = (ndim == 3) ? y1 * y1 + z1 * z1 : y1 * y1;
+  phi0 = par_lp[0] * (t1 - x1);
+  if (g_prof) {
+    phi1 = (t1 - x1) / par_lp[2];
+  } else {
+    phi1 = pi * (t1 - x1) / par_lp[2];
+    if (fabs(phi1) > pih) phi1 = pih;
+  }
+  x1 = x1 / par_lp[4];
+  w2 = 1. / (1. + x1 * x1);
+  phx = (ndim == 3) ? atan(x1) : 0.5 * atan(x1);
+  phig00 = phi0 + phx - x1 * r2 * w2;
+  phig10 = phig00 + phx;
+  tshape = g_prof ? exp(-phi1 * phi1) : cos(phi1) * cos(phi1);
+  wshape = ((ndim == 3) ? sqrt(w2) : sqrt(sqrt(w2))) * exp(-w2 * r2);
+  ampl = tshape * sin(phig00);
+  fields[1] = wshape * ampl;
+  if (g_prof && ndim == 3)
+    ampl_1 = 2. * par_lp[5] * tshape * w2 * exp(-w2 * r2);
+  else
+    ampl_1 = tshape * 2. * par_lp[5] * w2 * exp(-w2 * r2);
+  fields[0] = y1 * ampl_1 * cos(phig10);
+  fields[3] = (ndim == 3) ? z1 * ampl_1 * cos(phig10) : 0.0;
+  fields[5] = fields[1];
+  fields[2] = 0.0;
+  fields[4] = 0.0;
+}
+
+void ora_init_lp_fields(ora_sim* s, const agpu_lp_pulse* a) {
+  const int ndim = s->p.ndim;
+  double par_lp[7], coords[4], f[6];
+  const double sigma = 1. / (a->om0 * a->wx);
+  const double eps = 1. / (a->om0 * a->wy);
+  const double zra = 0.5 * a->om0 * a->wy * a->wy;
+  par_lp[0] = a->om0;
+  par_lp[1] = a->xf0 - a->tf;
+  par_lp[2] = a->wx;
+  par_lp[3] = a->wy;
+  par_lp[4] = zra;
+  par_lp[5] = eps;
+  par_lp[6] = sigma;
+  coords[3] = a->t_loc - a->tf;
+  const int k1 = (ndim == 3) ? s->kz1 : 1, k2 = (ndim == 3) ? s->kz2 : 1;
+  for (int k = k1; k <= k2; ++k) {
+    const double zz = (ndim == 3) ? s->p.zmn + s->p.dz * (double)(k - 3) : 0.0;
+    const double zzh = zz + 0.5 * s->p.dz;
+    for (int j = s->jy1; j <= s->jy2; ++j) {
+      const double yy = s->p.ymn + s->p.dy * (double)(j - 3), yyh = yy + 0.5 * s->p.dy;
+      for (int i = s->ix1; i <= s->ix2; ++i) {
+        const double xx = s->p.xmn + s->p.dx * (double)(i - 3), xxh = xx + 0.5 * s->p.dx;
+        if (ndim == 3) {
+          coords[0] = xxh - a->xf0; coords[1] = yy - a->ycent; coords[2] = zz - a->zcent;
+          ora_lp_fields(3, a->g_prof, par_lp, coords, f);
+          EBF(s, i, j, k, 1) = EBF(s, i, j, k, 1) + a->ee0 * f[0];
+          coords[0] = xx - a->xf0; coords[1] = yyh - a->ycent;
+          ora_lp_fields(3, a->g_prof, par_lp, coords, f);
+          EBF(s, i, j, k, 2) = EBF(s, i, j, k, 2) + a->ee0 * f[1];
+          coords[0] = xx - a->xf0; coords[1] = yy - a->ycent; coords[2] = zzh - a->zcent;
+          ora_lp_fields(3, a->g_prof, par_lp, coords, f);
+          EBF(s, i, j, k, 3) = EBF(s, i, j, k, 3) + a->ee0 * f[2];
+          coords[0] = xx - a->xf0; coords[1] = yyh - a->ycent; coords[2] = zzh - a->zcent;
+          ora_lp_fields(3, a->g_prof, par_lp, coords, f);
+          EBF(s, i, j, k, 4) = EBF(s, i, j, k, 4) + a->ee0 * f[3];
+          coords[0] = xxh - a->xf0; coords[1] = yy - a->ycent; coords[2] = zzh - a->zcent;
+          ora_lp_fields(3, a->g_prof, par_lp, coords, f);
+          EBF(s, i, j, k, 5) = EBF(s, i, j, k, 5) + a->ee0 * f[4];
+          coords[0] = xxh - a->xf0; coords[1] = yyh - a->ycent; coords[2] = zz - a->zcent;
+          ora_lp_fields(3, a->g_prof, par_lp, coords, f);
+          EBF(s, i, j, k, 6) = EBF(s, i, j, k, 6) + a->ee0 * f[5];
+        } else {
+          coords[2] = 0.0;
+          coords[0] = xxh - a->xf0; coords[1] = yy - a->ycent;
+          ora_lp_fields(2, a->g_prof, par_lp, coords, f);
+          EBF(s, i, j, k, 1) = EBF(s, i, j, k, 1) + a->ee0 * f[0];
+          coords[0] = xx - a->xf0; coords[1] = yyh - a->ycent;
+          ora_lp_fields(2, a->g_prof, par_lp, coords, f);
+          EBF(s, i, j, k, 2) = EBF(s, i, j, k, 2) + a->ee0 * f[1];
+          coords[0] = xxh - a->xf0; coords[1] = yyh - a->ycent;
+          ora_lp_fields(2, a->g_prof, par_lp, coords, f);
+          EBF(s, i, j, k, 3) = EBF(s, i, j, k, 3) + a->ee0 * f[5];
+        }
+      }
+    }
+  }
+}
+
+/* ======================================================================== */
+/* A22: Envar's reductions (src/diagnostics/diag_part_and_fields.f90:485-719)*/
+/* with energy_momenta (172-220) and energy_spect (126-142), one rank.       */
+/* out[0..6] = ek(1:7), out[7] = ekmax, out[8..10] = psig(1:3) (the sums    */
+/* of (p - <p>)^2 of 594-604), out[16..16+ne) = nde(1:ne).                  */
+/* ======================================================================== */
+void ora_envar_species(const ora_sim* s, int ic, double pmass, double* out) {
+  const int ne = AGPU_NE, nd = s->p.ndim, cnd = s->nc;
+  const int64_t np = s->np[ic];
+  memset(out, 0, sizeof(double) * (16 + ne));
+  double ek[7] = {0, 0, 0, 0, 0, 0, 0}, ekmax = 0.0;
+  for (int64_t ip = 1; ip <= np; ++ip) {
+    double xp[3] = {0, 0, 0}, vp[3] = {0, 0, 0}, gamm, gam1;
+    if (nd < 3) {
+      vp[0] = PART(s, ic, ip, 3);
+      vp[1] = PART(s, ic, ip, 4);
+      gamm = sqrt(1. + vp[0] * vp[0] + vp[1] * vp[1]);
+    } else {
+      for (int c = 0; c < 3; ++c) {
+        xp[c] = PART(s, ic, ip, 1 + c);
+        vp[c] = PART(s, ic, ip, 4 + c);
+      }
+      gamm = sqrt(1. + vp[0] * vp[0] + vp[1] * vp[1] + vp[2] * vp[2]);
+    }
+    uint64_t b;
+    double slot = PART(s, ic, ip, 2 * nd + 1);
+    memcpy(&b, &slot, 8);
+    const int16_t charge = (int16_t)(uint16_t)(b & 0xffffu);
+    uint32_t wb = (uint32_t)(b >> 32);
+    float wgh;
+    memcpy(&wgh, &wb, 4);
+    gam1 = gamm - 1.;
+    if (nd < 3) {
+      for (int ik = 0; ik < cnd; ++ik) ek[ik] = ek[ik] + (double)wgh * vp[ik];
+    } else {
+      for (int ik = 0; ik < cnd; ++ik) ek[ik] = ek[ik] + vp[ik];
+      ek[3] = ek[3] + (double)wgh * (xp[1] * vp[2] - xp[2] * vp[1]);
+    }
+    ek[5] = ek[5] + (double)((float)charge * wgh);
+    ek[6] = ek[6] + (double)wgh * gam1;
+    ekmax = fmax(ekmax, gam1);
+  }
+  for (int c = 0; c < 7; ++c) out[c] = ek[c];
+  out[7] = ekmax;
+  /* <[p - <p>]^2> sums, <p> = ek(ik) * np_norm */
+  const double np_norm = (np > 0) ? 1.0 / (double)np : 1.0;
+  for (int ik = 0; ik < cnd; ++ik) {
+    const double m = ek[ik] * np_norm;
+    double acc = 0.0;
+    for (int64_t ix = 1; ix <= np; ++ix) {
+      const double sg = PART(s, ic, ix, ik + cnd + 1) - m;
+      acc = acc + sg * sg;
+    }
+    out[8 + ik] = acc;
+  }
+  /* energy_spect(np, ek_max, gfield) with ek_max = pmass * ekmax */
+  const double ekem = pmass * ekmax;
+  const double de = ekem / (double)ne;
+  if (ekem < 1.e-06) return;
+  for (int64_t ip = 1; ip <= np; ++ip) {
+    double gamm;
+    if (nd < 3)
+      gamm = sqrt(1. + PART(s, ic, ip, 3) * PART(s, ic, ip, 3) + PART(s, ic, ip, 4) * PART(s, ic, ip, 4));
+    else
+      gamm = sqrt(1. + PART(s, ic, ip, 4) * PART(s, ic, ip, 4) + PART(s, ic, ip, 5) * PART(s, ic, ip, 5) +
+                  PART(s, ic, ip, 6) * PART(s, ic, ip, 6));
+    uint64_t b;
+    double slot = PART(s, ic, ip, 2 * nd + 1);
+    memcpy(&b, &slot, 8);
+    uint32_t wb = (uint32_t)(b >> 32);
+    float wgh;
+    memcpy(&wgh, &wb, 4);
+    const double xx = pmass * (gamm - 1.) / de;
+    int ix = (int)round(xx);
+    ix = (ix + 1 < ne) ? ix + 1 : ne;
+    out[16 + ix - 1] = out[16 + ix - 1] + (double)wgh;
+  }
+}
+
+/* Envar's field section (uniform grid): out[0..5] = dgvol * sum F^2,
+   out[6..11] = max |F_c|, out[12] = max over nodes of sum_{c<=curr_ndim} E_c^2. */
+void ora_envar_fields(const ora_sim* s, double* out) {
+  memset(out, 0, sizeof(double) * 16);
+  const double dgvol = (s->p.ndim == 2) ? s->p.dx * s->p.dy * s->p.dy : s->p.dx * s->p.dy * s->p.dz;
+  for (int ik = 1; ik <= s->nf; ++ik) {
+    double ekt = 0.0, mx = 0.0;
+    for (int iz = s->kz1; iz <= s->kz2; ++iz)
+      for (int iy = s->jy1; iy <= s->jy2; ++iy)
+        for (int ix = s->ix1; ix <= s->ix2; ++ix) {
+          const double v = EBF(s, ix, iy, iz, ik);
+          ekt = ekt + v * v;
+          mx = fmax(mx, fabs(v));
+        }
+    out[ik - 1] = dgvol * ekt;
+    out[6 + ik - 1] = (ekt > 0.0) ? mx : 0.0;
+  }
+  double e2 = 0.0;
+  for (int iz = s->kz1; iz <= s->kz2; ++iz)
+    for (int iy = s->jy1; iy <= s->jy2; ++iy)
+      for (int ix = s->ix1; ix <= s->ix2; ++ix) {
+        double ef2 = 0.0;
+        for (int c = 1; c <= s->nc; ++c) ef2 = ef2 + EBF(s, ix, iy, iz, c) * EBF(s, ix, iy, iz, c);
+        e2 = fmax(e2, ef2);
+      }
+  out[12] = e2;
+}

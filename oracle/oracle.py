@@ -72,6 +72,9 @@ def load():
         "ora_beam_inject": (C.c_int, [P, C.c_int, D, I64, I64, C.c_double]),
         "ora_beam_potential": (C.c_int, [P, D, C.c_double]),
         "ora_grid_charge": (None, [P, D, I64, I64, D]),
+        "ora_init_lp_fields": (None, [P, P]),
+        "ora_envar_species": (None, [P, C.c_int, C.c_double, D]),
+        "ora_envar_fields": (None, [P, D]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -124,6 +127,22 @@ class Oracle:
         a = np.asfortranarray(ebf, dtype=np.float64)
         assert a.shape == self.field_shape()
         self.lib.ora_set_fields(self.h, _dp(a))
+
+    def envar_species(self, ic, pmass):
+        """Envar's per-species reductions: (np, ek(1:7), ekmax, psig(1:3), nde(1:100))."""
+        out = np.zeros(116)
+        self.lib.ora_envar_species(self.h, ic, pmass, _dp(out))
+        return self.count(ic), out[:7].copy(), float(out[7]), out[8:11].copy(), out[16:116].copy()
+
+    def envar_fields(self):
+        """Envar's field reductions: (energy[6], fmax[6], e2max)."""
+        out = np.zeros(16)
+        self.lib.ora_envar_fields(self.h, _dp(out))
+        return out[:6].copy(), out[6:12].copy(), float(out[12])
+
+    def init_lp_fields(self, pulse):
+        """init_lp_inc0_fields: pulse is an aladyn_b200.abi.AgpuLpPulse."""
+        self.lib.ora_init_lp_fields(self.h, C.cast(C.pointer(pulse), C.c_void_p))
 
     def get_fields(self):
         a = np.zeros(self.field_shape(), dtype=np.float64, order="F")
