@@ -629,17 +629,30 @@ __device__ __forceinline__ void d32_chunk(const TileArgs32& a, const int t, cons
     // 2: counting sort of the tile's particles by node; each thread holds
     // its (at most LIST_CAP / NT) record indices and nodes in registers, all
     // loads of a thread in flight together
+    // (the slots past the chunk's particles are skipped: nu is the same
+    // for the whole CTA)
     constexpr int U = (C::LIST_CAP + NT - 1) / NT;
+    const int nu = (end - beg + NT - 1) / NT;
     int pv[U], lv[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
+      pv[u] = -1;
+      lv[u] = 0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (u >= nu) break;
       const int q = beg + threadIdx.x + u * NT;
       pv[u] = (q < end) ? __ldg(&a.perm[q]) : -1;
     }
 #pragma unroll
-    for (int u = 0; u < U; ++u) lv[u] = (pv[u] >= 0) ? a.p.cell[pv[u]] : 0;
+    for (int u = 0; u < U; ++u) {
+      if (u >= nu) break;
+      lv[u] = (pv[u] >= 0) ? a.p.cell[pv[u]] : 0;
+    }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
+      if (u >= nu) break;
       if (pv[u] < 0) continue;
       int i0, j0, k0;
       cell_split(g, lv[u], i0, j0, k0);
@@ -685,8 +698,10 @@ __device__ __forceinline__ void d32_chunk(const TileArgs32& a, const int t, cons
     }
     __syncthreads();
 #pragma unroll
-    for (int u = 0; u < U; ++u)
+    for (int u = 0; u < U; ++u) {
+      if (u >= nu) break;
       if (pv[u] >= 0) sList[atomicAdd(&sCur[lv[u]], 1)] = pv[u];
+    }
     __syncthreads();
 
     // 3: one node per thread, pass by pass (a warp = one x-row of 32 nodes);
@@ -892,7 +907,13 @@ __global__ void __launch_bounds__(NT, (NDIM == 3) ? 2 : 3) km32_tile(const Multi
     const int mid = (lo + hi) >> 1;
     if (__ldg(&tile_off[mid]) <= b) lo = mid; else hi = mid;
   }
-  d32_tile_all<NDIM>(d[lo].ta, b - __ldg(&tile_off[lo]));
+  // the instance's arguments in shared memory: read from the global
+  // descriptor they would be reloaded after every global store (which the
+  // compiler cannot prove does not alias them)
+  __shared__ TileArgs32 sa;
+  if (threadIdx.x == 0) sa = d[lo].ta;
+  __syncthreads();
+  d32_tile_all<NDIM>(sa, b - __ldg(&tile_off[lo]));
 }
 
 size_t tile32_smem(int ndim) { return sizeof(float) * (size_t)((ndim == 3) ? CT<3>::WORDS : CT<2>::WORDS); }
