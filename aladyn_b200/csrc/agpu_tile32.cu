@@ -123,6 +123,12 @@ __device__ __forceinline__ void cpa8(void* sdst, const void* gsrc) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
 }
+// 4-byte copy, or a zero fill (no read) when !valid
+__device__ __forceinline__ void cpa4z(void* sdst, const void* gsrc, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  const int n = valid ? 4 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(gsrc), "r"(n) : "memory");
+}
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -600,24 +606,23 @@ __device__ __forceinline__ void d32_chunk(const TileArgs32& a, const int t, cons
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
   // 1: stage fields (nodes i0t-1 .. i0t+TX), one x-row of FX nodes per
-  // warp and pass (lane = node, the first FX - 32 lanes take the rest),
-  // zero currents and node counts
+  // warp and pass (lane = node, the first FX - 32 lanes take the rest), as
+  // asynchronous copies that complete while the CTA zeroes its currents and
+  // sorts its particles (nodes outside the array are zero-filled)
   __syncthreads();  // a previous chunk of this CTA has finished with shared memory
   {
     constexpr int NROW = NF * FY * C::FZ;
     const int gi0 = i0t - 1 + lane, gi1 = gi0 + 32;
     const bool in0 = gi0 >= 1 && gi0 <= g.n1p, in1 = (lane < FX - 32) && gi1 <= g.n1p;
-#pragma unroll 4
     for (int row = warp; row < NROW; row += NT / 32) {
       const int c = row / (FY * C::FZ), r = row - c * (FY * C::FZ);
       const int gj = j0t - 1 + r % FY, gk = (NDIM == 3) ? k0t - 1 + r / FY : 1;
       const bool rin = gj >= 1 && gj <= g.n2p && gk >= 1 && gk <= g.n3p;
       const float* src = a.ebf + g.ncell * c + goff(g, gi0, gj, gk);
-      const float v0 = (rin && in0) ? __ldg(src) : 0.f;
-      const float v1 = (rin && in1) ? __ldg(src + 32) : 0.f;
-      sF[row * FX + lane] = v0;
-      if (lane < FX - 32) sF[row * FX + 32 + lane] = v1;
+      cpa4z(&sF[row * FX + lane], (rin && in0) ? src : a.ebf, rin && in0);
+      if (lane < FX - 32) cpa4z(&sF[row * FX + 32 + lane], (rin && in1) ? src + 32 : a.ebf, rin && in1);
     }
+    cpa_commit();
   }
   for (int e = threadIdx.x; e < NC * JV; e += NT) sJ[e] = 0.f;
   for (int e = threadIdx.x; e < NCELL; e += NT) sCur[e] = 0;
@@ -702,6 +707,7 @@ __device__ __forceinline__ void d32_chunk(const TileArgs32& a, const int t, cons
       if (u >= nu) break;
       if (pv[u] >= 0) sList[atomicAdd(&sCur[lv[u]], 1)] = pv[u];
     }
+    cpa_wait_all();  // this thread's field copies; the barrier makes all of them visible
     __syncthreads();
 
     // 3: one node per thread, pass by pass (a warp = one x-row of 32 nodes);
@@ -801,7 +807,7 @@ __device__ __forceinline__ void d32_chunk(const TileArgs32& a, const int t, cons
     constexpr int NROW = NC * JY * C::JZ;
     const int gi0 = i0t - 2 + lane;
     const bool xin0 = gi0 >= 1 && gi0 <= g.n1p, xin1 = (lane < JX - 32) && gi0 + 32 <= g.n1p;
-    constexpr int R = 4;  // rows of a warp in flight
+    constexpr int R = 8;  // rows of a warp in flight
     for (int row0 = warp; row0 < NROW; row0 += R * (NT / 32)) {
       float v[2 * R], old[2 * R];
       long long o[R];
