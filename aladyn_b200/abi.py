@@ -103,6 +103,13 @@ class AgpuLpPulse(C.Structure):
     ]
 
 
+class AgpuEnvParams(C.Structure):
+    _fields_ = [
+        ("om0", C.c_double), ("opt_der1", C.c_double), ("hord_der2", C.c_double),
+        ("der_ord", C.c_int32), ("reserved", C.c_int32),
+    ]
+
+
 AGPU_NE = 100
 
 
@@ -184,6 +191,12 @@ SIGNATURES = {
                                               C.c_int32, C.c_double]),
     "agpu_step": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int32, C.POINTER(AgpuStepOut)]),
     "agpu_window_inject": (C.c_int, [_P, C.c_int32, _D, C.c_int64, C.c_int64, C.c_int32]),
+    "agpu_env_enable": (C.c_int, [_P, C.POINTER(AgpuEnvParams)]),
+    "agpu_set_envelope": (C.c_int, [_P, _D, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "agpu_get_envelope": (C.c_int, [_P, _D, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "agpu_get_env_source": (C.c_int, [_P, _D, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "agpu_init_envelope": (C.c_int, [_P, C.POINTER(AgpuLpPulse), C.c_int32]),
+    "agpu_env_run": (C.c_int, [_P, C.c_int32, C.c_double, C.POINTER(AgpuStepOut)]),
     "agpu_beam_inject": (C.c_int, [_P, C.c_int32, _D, C.c_int64, C.c_int64, C.c_int32, C.c_double]),
     "agpu_beam_potential": (C.c_int, [_P, _D, _D, C.c_double]),
     "agpu_set_deferred_counts": (C.c_int, [_P, C.c_int32]),

@@ -37,12 +37,14 @@ UNITS = [
     ("agpu_bin.cu", ["-fmad=false"]),
     ("agpu_noalloc.cu", ["-fmad=false"]),
     ("agpu_envar.cu", ["-fmad=false"]),
+    ("agpu_env.cu", ["-fmad=false"]),
     ("agpu_beam.cu", ["-fmad=false"]),
     ("agpu_ionz.cpp", []),
     ("agpu_batch.cpp", ["-Xcompiler", "-pthread"]),
 ]
 HEADERS = ["agpu_common.cuh", "agpu_kernels.h", "agpu_util.h", "agpu_yee.cuh", "agpu_ionz.h", "agpu_bin.cuh",
-           "agpu_tile.h", "agpu_select.cuh", "agpu_beam.h", "agpu_multi.h", "agpu_yee_fused.cuh"]
+           "agpu_tile.h", "agpu_select.cuh", "agpu_beam.h", "agpu_multi.h", "agpu_yee_fused.cuh", "agpu_env.h",
+           "agpu_fp64_dep.cuh"]
 
 
 def _mtime(p: str) -> float:

@@ -121,6 +121,26 @@ def make_params(grid: Grid, *, precision: int = AGPU_FP64, nsp: int = 1, nsp_run
     return p
 
 
+def env_params(grid: Grid, lam0: float, der_ord: int = 2):
+    """The envelope solver's constants: oml = 2 pi / lam0 and, for der_ord 3,
+    opt_der1 = (4 - nu^2)/3 and hord_der2 = -(1 - nu^2)/12 with the
+    multi-D optimised nu of set_field_param (grid_field_param.f90:36-72)."""
+    from .abi import AgpuEnvParams
+    e = AgpuEnvParams()
+    e.om0 = 2.0 * PI / lam0
+    e.der_ord = der_ord
+    e.opt_der1, e.hord_der2 = 1.0, 0.0
+    if der_ord == 3:
+        nu = grid.cfl
+        if grid.ndim > 1:
+            nu = grid.cfl * grid.yx_rat / math.sqrt(grid.yx_rat * grid.yx_rat + float(grid.ndim) - 1.)
+        e.hord_der2 = -(1. - nu * nu) / 12.
+        e.opt_der1 = (4. - nu * nu) / 3.
+    elif der_ord != 2:
+        raise ValueError("der_ord must be 2 or 3")
+    return e
+
+
 def n_over_nc_to_n0(n_over_nc: float, lam0: float) -> float:
     """n0_ref (1e18 cm^-3) giving electron density n/nc (set_init_param.f90:272-279)."""
     ncrit = PI / (RC0 * lam0 * lam0)
@@ -156,5 +176,5 @@ def ndv(p: AgpuParams) -> int:
     return 7 if p.ndim == 3 else 5
 
 
-__all__ = ["Grid", "make_params", "plasma", "laser", "dims", "ndv", "nint", "ompe_value",
+__all__ = ["Grid", "make_params", "plasma", "laser", "dims", "ndv", "nint", "ompe_value", "env_params",
            "n_over_nc_to_n0", "AGPU_FP64", "AGPU_FP32_SPLIT"]

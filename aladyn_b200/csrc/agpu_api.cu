@@ -14,6 +14,7 @@
 #include "../../include/aladyn_gpu.h"
 #include "agpu_beam.h"
 #include "agpu_bin.cuh"
+#include "agpu_env.h"
 #include "agpu_ionz.h"
 #include "agpu_kernels.h"
 #include "agpu_multi.h"
@@ -81,6 +82,12 @@ struct agpu_handle {
   int* tile_work = nullptr;         // (tile, chunk) pairs of dense tiles, split form
   unsigned int* tile_work_n = nullptr;
   int tile_work_cap = 0;
+  // envelope model (agpu_env_enable): env(n1p,n2p,n3p,4), the step's source
+  // scratch (ndim+1 components) and the density before its copy
+  double* env = nullptr;
+  double* env_av = nullptr;
+  double* env_den = nullptr;
+  agpu_env_params ep{};
   // window state (lp_window_xshift saved variables)
   double xlapse = 0.0;
   int wi1 = 0;
@@ -229,6 +236,9 @@ int free_all(agpu_handle* h) {
   cudaFree(h->cursor);
   cudaFree(h->scan_tmp);
   cudaFree(h->inj_stage);
+  cudaFree(h->env);
+  cudaFree(h->env_av);
+  cudaFree(h->env_den);
   for (int i = 0; i < 2 * PH_N; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
@@ -628,8 +638,10 @@ int window_xshift(agpu_handle* h, int witr, int init_iter, agpu_step_out* out) {
       xshift32(h->ebf32, h->g, h->g.nf, wi2, nshx, h->st, h->sms);
     else
       xshift64(h->ebf, h->g, h->g.nf, wi2, nshx, h->st, h->sms);
+    // envelope: fields_left_xshift(env, i1, wi2, 1, nc_env = 4, nshx) (window.f90:326-330)
+    if (h->env) xshift64(h->env, h->g, 4, wi2, nshx, h->st, h->sms);
     CK(cudaGetLastError());
-    h->timers.launches_total += 1;
+    h->timers.launches_total += h->env ? 2 : 1;
   }
   for (int ic = 0; ic < p.nsp; ++ic) {
     if (h->np[ic] <= 0) continue;
@@ -1707,6 +1719,203 @@ int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t l
   h->np[ic] += n;
   h->nalive[ic] = h->np[ic];
   h->binned[ic] = false;
+  return 0;
+}
+
+// ---- envelope cycle (Env_cycle, src/ALaDyn.F90:111-130) -------------------
+int agpu_env_enable(agpu_handle* h, const agpu_env_params* ep) {
+  if (!h || !ep || h->fp32 || (ep->der_ord != 2 && ep->der_ord != 3) || !(ep->om0 > 0.0)) return AGPU_E_ARG;
+  const Geo& g = h->g;
+  if (g.ix2 - g.ix1 < 3 || g.jy2 - g.jy1 < 2 || (g.ndim == 3 && g.kz2 - g.kz1 < 2)) return AGPU_E_ARG;
+  CK(cudaStreamSynchronize(h->st));
+  cudaFree(h->env);
+  cudaFree(h->env_av);
+  cudaFree(h->env_den);
+  h->env = h->env_av = h->env_den = nullptr;
+  const size_t c3 = (size_t)g.ncell;
+  int rc = dmalloc((void**)&h->env, sizeof(double) * c3 * 4);
+  rc |= dmalloc((void**)&h->env_av, sizeof(double) * c3 * (g.ndim + 1));
+  rc |= dmalloc((void**)&h->env_den, sizeof(double) * c3);
+  if (rc) return AGPU_E_NOMEM;
+  CK(cudaMemsetAsync(h->env, 0, sizeof(double) * c3 * 4, h->st));
+  CK(cudaMemsetAsync(h->env_av, 0, sizeof(double) * c3 * (g.ndim + 1), h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->ep = *ep;
+  return 0;
+}
+
+static int env_copy(agpu_handle* h, double* dev, const double* src_h, double* dst_h, int32_t n1p, int32_t n2p,
+                    int32_t n3p, int32_t nc, int32_t want) {
+  if (!h || !dev) return h ? AGPU_E_STATE : AGPU_E_ARG;
+  const Geo& g = h->g;
+  if (n1p != g.n1p || n2p != g.n2p || n3p != g.n3p || nc != want) return AGPU_E_ARG;
+  const size_t bytes = sizeof(double) * (size_t)g.ncell * nc;
+  if (src_h) CK(cudaMemcpyAsync(dev, src_h, bytes, cudaMemcpyHostToDevice, h->st));
+  if (dst_h) CK(cudaMemcpyAsync(dst_h, dev, bytes, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+int agpu_set_envelope(agpu_handle* h, const double* env, int32_t n1p, int32_t n2p, int32_t n3p, int32_t nc) {
+  if (!env) return AGPU_E_ARG;
+  return env_copy(h, h ? h->env : nullptr, env, nullptr, n1p, n2p, n3p, nc, 4);
+}
+int agpu_get_envelope(agpu_handle* h, double* env, int32_t n1p, int32_t n2p, int32_t n3p, int32_t nc) {
+  if (!env) return AGPU_E_ARG;
+  return env_copy(h, h ? h->env : nullptr, nullptr, env, n1p, n2p, n3p, nc, 4);
+}
+int agpu_get_env_source(agpu_handle* h, double* av, int32_t n1p, int32_t n2p, int32_t n3p, int32_t nc) {
+  if (!av) return AGPU_E_ARG;
+  return env_copy(h, h ? h->env_av : nullptr, nullptr, av, n1p, n2p, n3p, nc, h ? h->p.ndim + 1 : 0);
+}
+
+int agpu_init_envelope(agpu_handle* h, const agpu_lp_pulse* l, int32_t plane_wave) {
+  if (!h || !l || !(l->wx > 0.0) || !(l->wy > 0.0) || !(l->om0 > 0.0)) return AGPU_E_ARG;
+  if (!h->env) return AGPU_E_STATE;
+  EnvPulseArgs a;
+  a.ndim = h->p.ndim;
+  a.g_prof = l->g_prof ? 1 : 0;
+  a.plane_wave = plane_wave ? 1 : 0;
+  a.ee0 = l->ee0;
+  a.t = l->t_loc - l->tf;
+  a.tm = a.t - h->p.dt;
+  a.xf0 = l->xf0;
+  a.wx = l->wx;
+  a.wy = l->wy;
+  a.zra = 0.5 * l->om0 * l->wy * l->wy;
+  a.ycent = l->ycent;
+  a.zcent = l->zcent;
+  a.xmn = h->p.xmn;
+  a.ymn = h->p.ymn;
+  a.zmn = h->p.zmn;
+  a.dx = h->p.dx;
+  a.dy = h->p.dy;
+  a.dz = h->p.dz;
+  env_init_pulse(a, h->env, h->g, h->st, h->sms);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+// env_run (src/dynamics/env_evolve_in_time.f90:363-391): env_lpf2_evolve
+// (196-361) for species 0, then the moving window.
+int agpu_env_run(agpu_handle* h, int32_t iter, double t, agpu_step_out* out) {
+  if (!h) return AGPU_E_ARG;
+  agpu_step_out dummy;
+  if (!out) out = &dummy;
+  std::memset(out, 0, sizeof(*out));
+  out->ion_field_max = -1.0;
+  if (!h->env) return AGPU_E_STATE;
+  agpu_params& p = h->p;
+  const Geo& g = h->g;
+  const int ic = 0;
+  if (int rc = drop_removed(h, ic)) return rc;
+  CK(cudaMemsetAsync(h->d_cnt, 0, sizeof(Counters), h->st));
+  EnvArgs a;
+  a.g = g;
+  a.ebf = h->ebf;
+  a.env = h->env;
+  a.av = h->env_av;
+  a.den = h->env_den;
+  a.jc = h->jc;
+  double* b = h->part[ic];
+  const long long cp = h->cap[ic];
+  a.x = b;
+  a.y = b + cp;
+  if (p.ndim == 3) {
+    a.z = b + 2 * cp;
+    a.px = b + 3 * cp;
+    a.py = b + 4 * cp;
+    a.pz = b + 5 * cp;
+    a.slot = b + 6 * cp;
+  } else {
+    a.z = nullptr;
+    a.px = b + 2 * cp;
+    a.py = b + 3 * cp;
+    a.pz = nullptr;
+    a.slot = b + 4 * cp;
+  }
+  a.flag = h->flag;
+  a.np = h->np[ic];
+  a.xmn = p.xmn;
+  a.ymn = p.ymn;
+  a.zmn = p.zmn;
+  a.dx_inv = p.dx_inv;
+  a.dy_inv = p.dy_inv;
+  a.dz_inv = p.dz_inv;
+  a.dt = p.dt;
+  a.lfact = p.lorentz_fact[ic];
+  a.ompe = p.ompe;
+  a.gxmin = p.gxmin;
+  a.gxmax = p.gxmax;
+  a.gymin = p.gymin;
+  a.gymax = p.gymax;
+  a.gzmin = p.gzmin;
+  a.gzmax = p.gzmax;
+  a.om0 = h->ep.om0;
+  a.opt_der1 = h->ep.opt_der1;
+  a.hord_der2 = h->ep.hord_der2;
+  a.der_ord = h->ep.der_ord;
+  a.ibx = p.ibx;
+  a.iby = p.iby;
+  a.ibz = p.ibz;
+  a.iform = p.iform;
+  a.removed = &h->d_cnt->removed;
+  a.err = &h->d_cnt->err;
+  const size_t c3 = (size_t)g.ncell;
+  ph_begin(h, PH_PUSH);
+  // jc(:,:,:,:) = 0; env_amp_prepare
+  CK(cudaMemsetAsync(h->env_av, 0, sizeof(double) * c3 * (g.ndim + 1), h->st));
+  env_amp_grad(a, h->st, h->sms);
+  // set_env_acc, lpf_env_momenta, set_env_density (jc(:,:,:,1) = 0 first)
+  CK(cudaMemsetAsync(h->env_den, 0, sizeof(double) * c3, h->st));
+  env_acc_momenta(a, h->st, h->sms, h->deterministic);
+  // env_den_collect; jc(3) = jc(1)
+  env_den_collect(a, h->st, h->sms);
+  // advance_lpf_envelope, env_fields_average
+  env_advance(a, h->st, h->sms);
+  // set_env_grad_interp, lpf_env_positions, cell_part_dist, curr_accumulate
+  CK(cudaMemsetAsync(h->jc, 0, sizeof(double) * c3 * g.nc, h->st));
+  env_positions_deposit(a, h->st, h->sms, h->deterministic);
+  CK(cudaGetLastError());
+  ph_end(h, PH_PUSH);
+  h->timers.launches_push_deposit += 2;
+  h->timers.launches_total += 12 + (g.ndim == 3 ? 2 : 0);
+  h->timers.pushes += a.np;
+  if (int rc = read_counters(h)) return rc;
+  int rc = 0;
+  if (h->h_cnt->removed > 0) {
+    ph_begin(h, PH_SORT);
+    const long long before = h->np[ic];
+    rc = compact_species(h, ic, false);
+    ph_end(h, PH_SORT);
+    if (rc) return rc;
+    out->removed[ic] += before - h->np[ic];
+  }
+  // curr_mpi_collect (djc folded into the E update), advance_lpf_fields
+  ph_begin(h, PH_YEE);
+  Dev64 d{g, h->ebf, h->jc};
+  jfold64(d, h->st, h->sms);
+  yee64(d, yee_coef(p), h->st, h->sms);
+  CK(cudaGetLastError());
+  ph_end(h, PH_YEE);
+  h->timers.launches_yee += 1;
+  h->timers.launches_total += ((p.ndim == 3) ? 3 : 2) + 6;
+  h->timers.yee_cells += (long long)p.nx * p.ny * (p.ndim == 3 ? p.nz : 1);
+  if (p.w_speed > 0.0 && p.w_sh > 0) {
+    if (t >= p.wi_time && t < p.wf_time) {
+      if (iter % p.w_sh == 0) {
+        ph_begin(h, PH_WINDOW);
+        rc = window_xshift(h, p.w_sh, iter, out);
+        ph_end(h, PH_WINDOW);
+        if (rc) return rc;
+      }
+    }
+  }
+  if (int rc_ = read_counters(h)) return rc_;
+  for (int q = 0; q < 4; ++q) out->np[q] = h->binned[q] ? h->nalive[q] : h->np[q];
+  out->xmn = p.xmn;
+  out->error_bits = h->error_bits;
+  if (h->error_bits & AGPU_EBIT_CAPACITY) return AGPU_E_CAPACITY;
   return 0;
 }
 

@@ -181,6 +181,35 @@ class PicDevice:
 
     step = lp_run
 
+    # -- envelope cycle (Env_cycle, src/ALaDyn.F90:111-130) -------------------
+    def env_enable(self, ep: "abi.AgpuEnvParams"):
+        check(self.lib.agpu_env_enable(self.h, C.byref(ep)), "agpu_env_enable")
+
+    def init_envelope(self, pulse, plane_wave: bool = False):
+        check(self.lib.agpu_init_envelope(self.h, C.byref(pulse), 1 if plane_wave else 0), "agpu_init_envelope")
+
+    def set_envelope(self, env: np.ndarray):
+        a = np.asfortranarray(env, dtype=np.float64)
+        assert a.shape == (self.n1p, self.n2p, self.n3p, 4), a.shape
+        check(self.lib.agpu_set_envelope(self.h, _dptr(a), self.n1p, self.n2p, self.n3p, 4), "agpu_set_envelope")
+
+    def get_envelope(self) -> np.ndarray:
+        a = np.zeros((self.n1p, self.n2p, self.n3p, 4), dtype=np.float64, order="F")
+        check(self.lib.agpu_get_envelope(self.h, _dptr(a), self.n1p, self.n2p, self.n3p, 4), "agpu_get_envelope")
+        return a
+
+    def get_env_source(self) -> np.ndarray:
+        nav = 4 if self.n3p > 1 else 3
+        a = np.zeros((self.n1p, self.n2p, self.n3p, nav), dtype=np.float64, order="F")
+        check(self.lib.agpu_get_env_source(self.h, _dptr(a), self.n1p, self.n2p, self.n3p, nav),
+              "agpu_get_env_source")
+        return a
+
+    def env_run(self, t: float, iteration: int) -> AgpuStepOut:
+        out = AgpuStepOut()
+        check(self.lib.agpu_env_run(self.h, iteration, t, C.byref(out)), "agpu_env_run")
+        return out
+
     def diag(self) -> AgpuDiagOut:
         out = AgpuDiagOut()
         check(self.lib.agpu_diag(self.h, C.byref(out)), "agpu_diag")

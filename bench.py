@@ -123,9 +123,9 @@ def bytes_per_push(ndim: int, ppc: int, fp32: bool) -> float:
 
 # DRAM bytes (read + write) per particle of one k32_tile launch, from an ncu
 # capture of the 384x96x96-cell, 8 ppc workload two steps after a window
-# shift (2172.0 MB for 2.83e7 particles); traffic grows in proportion to the
+# shift (2045.8 MB for 2.83e7 particles); traffic grows in proportion to the
 # particles of a launch.
-K32_DRAM_BYTES_PER_PUSH = 76.7
+K32_DRAM_BYTES_PER_PUSH = 72.3
 
 
 def yee_bytes_per_cell(ndim: int, fp32: bool) -> float:

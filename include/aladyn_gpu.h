@@ -295,6 +295,45 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time,
 int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t ld,
                        int64_t n, int32_t ndv);
 
+/* ---- envelope cycle ---------------------------------------------------- */
+/* The reference's Env_cycle (src/ALaDyn.F90:111-130): the laser enters as
+ * the complex envelope A of its vector potential (env(:,:,:,1:2) = Re, Im of
+ * A^n, env(:,:,:,3:4) = A^{n-1}) advanced by the explicit Maxwell envelope
+ * solver, and species 0 feels the wake fields plus the ponderomotive force
+ * of |A|^2/2.  FP64 form, one running species, fixed (non-comoving) frame,
+ * der_ord 2 or 3, no ionization or second colour. */
+typedef struct agpu_env_params {
+  double om0;              /* oml = 2 pi / lam0, the envelope's carrier frequency   */
+  double opt_der1;         /* der_ord 3: (4 - nu^2)/3, else 1
+                              (set_field_param, src/fields/grid_field_param.f90:54-72) */
+  double hord_der2;        /* der_ord 3: -(1 - nu^2)/12, else 0                       */
+  int32_t der_ord;         /* 2 or 3                                                   */
+  int32_t reserved;
+} agpu_env_params;
+/* Allocates env(n1p,n2p,n3p,4) (zeroed) and the step's source scratch: the
+ * reference's jc(:,:,:,1:ndim+1) during env_lpf2_evolve. */
+int agpu_env_enable(agpu_handle* h, const agpu_env_params* ep);
+/* env(n1p, n2p, n3p, 4), column-major FP64 with ghosts, as the reference's
+ * module array env (src/work/fstruct_data.f90:32, src/work/array_alloc.f90:
+ * 107-112). */
+int agpu_set_envelope(agpu_handle* h, const double* env, int32_t n1p, int32_t n2p, int32_t n3p, int32_t nc);
+int agpu_get_envelope(agpu_handle* h, double* env, int32_t n1p, int32_t n2p, int32_t n3p, int32_t nc);
+/* The source scratch after the last env step (nc = ndim + 1): component 1
+ * holds |A|^2/2 at t^{n+1/2} on the interior, components 2..ndim+1 its
+ * staggered gradient (env_fields_average + env_grad). */
+int agpu_get_env_source(agpu_handle* h, double* av, int32_t n1p, int32_t n2p, int32_t n3p, int32_t nc);
+/* init_gprof_envelope_field (g_prof = 1) or init_envelope_field (g_prof =
+ * 0) (src/fields/init_grid_fields.f90:140-399), called from init_envelope
+ * (src/IO/init_laser_field.f90:150-200) with ee0 = a0, tf = t0_lp,
+ * wx = w0_x, wy = w0_y, xf0 = xf, om0 = oml: ADDS the pulse's A^n and
+ * A^{n-1} = A(t - dt) on the interior nodes; plane_wave != 0 is the pw = 0
+ * branch.  Coordinates x = xmn + (i-3) dx, y and z alike. */
+int agpu_init_envelope(agpu_handle* h, const agpu_lp_pulse* pulse, int32_t plane_wave);
+/* One call of env_run (src/dynamics/env_evolve_in_time.f90:363-391):
+ * env_lpf2_evolve (196-361) for species 0 and, when mod(iter, w_sh) == 0
+ * inside [wi_time, wf_time), lp_window_xshift, which shifts env as well. */
+int agpu_env_run(agpu_handle* h, int32_t iter, double t, agpu_step_out* out);
+
 /* ---- PWFA bunch set-up ------------------------------------------------- */
 /* beam_inject (src/IO/init_beam_part_distrib.f90:474-630, uniform-grid
  * branch), called once after the fields are set: of the nb bunch records

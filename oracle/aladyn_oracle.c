@@ -59,6 +59,11 @@ typedef struct ora_sim {
   int nsp_ionz; /* species index bound: ions 1..nsp_ionz-1 ionize */
   uint32_t error_bits;
   int nthreads; /* >1: threaded CPU baseline (per-thread current copies) */
+  /* envelope model: env(n1p,n2p,n3p,4) and the step's jc(:,:,:,1:ndim+1) */
+  double* env;
+  double* av;
+  int nav;
+  agpu_env_params ep;
 } ora_sim;
 
 /* ---- layout helpers (Fortran 1-based) ---------------------------------- */
@@ -151,6 +156,8 @@ void ora_destroy(ora_sim* s) {
     free(s->wtab[ic]);
   }
   free(s->ebfp);
+  free(s->env);
+  free(s->av);
   free(s);
 }
 
@@ -1425,6 +1432,17 @@ static int ora_window_xshift(ora_sim* s, int witr, int init_iter, agpu_step_out*
           for (int ix = s->ix1; ix <= wi2; ++ix) EBF(s, ix, iy, iz, ic) = EBF(s, ix + nshx, iy, iz, ic);
           for (int ix = wi2 + 1; ix <= wi2 + nshx; ++ix) EBF(s, ix, iy, iz, ic) = 0.0;
         }
+    /* envelope: fields_left_xshift(env, i1, wi2, 1, nc_env = 4, nshx) (window.f90:326-330) */
+    if (s->env) {
+      const size_t c3 = (size_t)s->n1p * s->n2p * s->n3p;
+      for (int ic = 0; ic < 4; ++ic)
+        for (int iz = s->kz1; iz <= s->kz2; ++iz)
+          for (int iy = s->jy1; iy <= s->jy2; ++iy) {
+            double* row = s->env + c3 * ic + (size_t)s->n1p * ((size_t)(iy - 1) + (size_t)s->n2p * (size_t)(iz - 1)) - 1;
+            for (int ix = s->ix1; ix <= wi2; ++ix) row[ix] = row[ix + nshx];
+            for (int ix = wi2 + 1; ix <= wi2 + nshx; ++ix) row[ix] = 0.0;
+          }
+    }
   }
   /* cell_part_dist(.true.): x only, all species, spec compacted */
   for (int ic = 0; ic < p->nsp; ++ic) {
@@ -2336,4 +2354,737 @@ void ora_envar_fields(const ora_sim* s, double* out) {
         e2 = fmax(e2, ef2);
       }
   out[12] = e2;
+}
+
+/* ======================================================================== */
+/* Envelope cycle: env_run -> env_lpf2_evolve (src/dynamics/                */
+/* env_evolve_in_time.f90:196-361, 363-391) for species 0, one rank, fixed  */
+/* frame (ib = 2: env_maxw_solve), der_ord 2 or 3, no ionization, no       */
+/* second colour, no fluid.  env(:,:,:,1:2) = A^n (Re, Im), 3:4 = A^{n-1};  */
+/* av(:,:,:,1:ndim+1) is the reference's jc during the envelope part of the */
+/* step.  Uniform grid: the stretch factors loc_yg/loc_zg(:,3:4) are 1, so  */
+/* the factors they multiply in are left out (x * 1 == x exactly).          */
+/* ======================================================================== */
+#define ORA_I4(s, i, j, k, c) \
+  (((size_t)(i)-1) + (size_t)(s)->n1p * (((size_t)(j)-1) + (size_t)(s)->n2p * (((size_t)(k)-1) + (size_t)(s)->n3p * ((size_t)(c)-1))))
+#define ENV(s, i, j, k, c) (s)->env[ORA_I4(s, i, j, k, c)]
+#define AV(s, i, j, k, c) (s)->av[ORA_I4(s, i, j, k, c)]
+
+int ora_env_enable(ora_sim* s, const agpu_env_params* ep) {
+  if (!ep || (ep->der_ord != 2 && ep->der_ord != 3)) return AGPU_E_ARG;
+  const size_t c3 = (size_t)s->n1p * s->n2p * s->n3p;
+  free(s->env);
+  free(s->av);
+  s->nav = s->p.ndim + 1;
+  s->env = (double*)calloc(c3 * 4, sizeof(double));
+  s->av = (double*)calloc(c3 * (size_t)s->nav, sizeof(double));
+  if (!s->env || !s->av) return AGPU_E_NOMEM;
+  s->ep = *ep;
+  return 0;
+}
+int ora_set_envelope(ora_sim* s, const double* env) {
+  if (!s->env) return AGPU_E_STATE;
+  memcpy(s->env, env, sizeof(double) * (size_t)s->n1p * s->n2p * s->n3p * 4);
+  return 0;
+}
+int ora_get_envelope(const ora_sim* s, double* env) {
+  if (!s->env) return AGPU_E_STATE;
+  memcpy(env, s->env, sizeof(double) * (size_t)s->n1p * s->n2p * s->n3p * 4);
+  return 0;
+}
+int ora_get_env_source(const ora_sim* s, double* av) {
+  if (!s->av) return AGPU_E_STATE;
+  memcpy(av, s->av, sizeof(double) * (size_t)s->n1p * s->n2p * s->n3p * (size_t)s->nav);
+  return 0;
+}
+
+/* init_gprof_envelope_field (g_prof) / init_envelope_field
+   (src/fields/init_grid_fields.f90:274-399 / 140-272) with the arguments of
+   init_envelope (src/IO/init_laser_field.f90:150-200): adds A^n (t_loc) and
+   A^{n-1} (t_loc - dt) on i = ix1..nxp, j = jy1..jy2, k = kz1..kz2. */
+void ora_init_envelope(ora_sim* s, const agpu_lp_pulse* a, int plane_wave) {
+  const double pi = acos(-1.0);
+  const int ndim = s->p.ndim;
+  const double t = a->t_loc - a->tf;
+  const double tm = t - s->p.dt;
+  const double zra = 0.5 * a->om0 * a->wy * a->wy;
+  const double pih = 0.5 * acos(-1.0);
+  const double ee0 = a->ee0, wx = a->wx, wy = a->wy;
+  for (int k = s->kz1; k <= s->kz2; ++k) {
+    const double zz = (ndim == 3) ? (s->p.zmn + s->p.dz * (double)(k - 3) - a->zcent) / wy : 0.0;
+    for (int j = s->jy1; j <= s->jy2; ++j) {
+      const double yy = (s->p.ymn + s->p.dy * (double)(j - 3) - a->ycent) / wy;
+      const double r2 = (ndim == 3) ? (yy * yy + zz * zz) : yy * yy;
+      for (int i = s->ix1; i <= s->ix2; ++i) {
+        double xx = s->p.xmn + s->p.dx * (double)(i - 3);
+        xx = xx - a->xf0;
+        double phi0, phi1, phi, ar, ai, ampl1, ampl0;
+        if (a->g_prof) {
+          phi1 = (xx - t) / wx;
+          phi0 = (xx - tm) / wx;
+          if (plane_wave) {
+            phi = atan(xx);
+            ar = ee0 * cos(phi);
+            ai = -ee0 * sin(phi);
+          } else {
+            xx = xx / zra;
+            const double w2 = 1. / (1. + xx * xx);
+            const double phx = atan(xx);
+            phi = phx - xx * r2 * w2;
+            const double ws = (ndim == 3) ? sqrt(w2) : sqrt(sqrt(w2));
+            ar = ee0 * cos(phi) * ws * exp(-w2 * r2);
+            ai = -ee0 * sin(phi) * ws * exp(-w2 * r2);
+          }
+          ampl1 = exp(-phi1 * phi1);
+          ampl0 = exp(-phi0 * phi0);
+        } else {
+          if (plane_wave || ndim < 3) {
+            phi1 = pi * (xx - t) / wx;
+            phi0 = pi * (xx - tm) / wx;
+          } else {
+            phi1 = pi * (t - xx) / wx;
+            phi0 = pi * (tm - xx) / wx;
+          }
+          if (fabs(phi1) > pih) phi1 = pih;
+          if (fabs(phi0) > pih) phi0 = pih;
+          if (plane_wave) {
+            phi = 0.0;
+            ar = ee0 * cos(phi);
+            ai = -ee0 * sin(phi);
+          } else {
+            xx = xx / zra;
+            const double w2 = 1. / (1. + xx * xx);
+            const double phx = atan(xx);
+            phi = phx - xx * r2 * w2;
+            const double ws = (ndim == 3) ? sqrt(w2) : sqrt(sqrt(w2));
+            ar = ee0 * cos(phi) * ws * exp(-w2 * r2);
+            ai = -ee0 * sin(phi) * ws * exp(-w2 * r2);
+          }
+          ampl1 = cos(phi1) * cos(phi1);
+          ampl0 = cos(phi0) * cos(phi0);
+        }
+        ENV(s, i, j, k, 1) = ENV(s, i, j, k, 1) + ampl1 * ar;
+        ENV(s, i, j, k, 2) = ENV(s, i, j, k, 2) + ampl1 * ai;
+        ENV(s, i, j, k, 3) = ENV(s, i, j, k, 3) + ampl0 * ar;
+        ENV(s, i, j, k, 4) = ENV(s, i, j, k, 4) + ampl0 * ai;
+      }
+    }
+  }
+}
+
+/* env_grad (src/fields/grid_fields.f90:426-586), der_ord < 4, one rank (all
+   boundaries are domain edges): av(2) = D_x av(1) at i+1/2, av(3) = D_y at
+   j+1/2, av(4) = D_z at k+1/2 (3D), one-sided at the edges; the 3D edge
+   branches also write the ghost planes kz1-1 and kz2+1 of av(1). */
+static void ora_env_grad(ora_sim* s) {
+  const double dxi = s->p.dx_inv, dyi = s->p.dy_inv, dzi = s->p.dz_inv;
+  const int ix1 = s->ix1, ix2 = s->ix2, jy1 = s->jy1, jy2 = s->jy2, kz1 = s->kz1, kz2 = s->kz2;
+  for (int k = kz1; k <= kz2; ++k)
+    for (int j = jy1; j <= jy2; ++j) {
+      AV(s, ix1, j, k, 2) = dxi * (AV(s, ix1 + 1, j, k, 1) - AV(s, ix1, j, k, 1));
+      int i = ix2 - 1;
+      AV(s, i, j, k, 2) = dxi * (AV(s, i + 1, j, k, 1) - AV(s, i, j, k, 1));
+      AV(s, i + 1, j, k, 2) = dxi * (2. * AV(s, i, j, k, 1) - 3. * AV(s, i - 1, j, k, 1) + AV(s, i - 2, j, k, 1));
+      for (i = ix1 + 1; i <= ix2 - 2; ++i) AV(s, i, j, k, 2) = dxi * (AV(s, i + 1, j, k, 1) - AV(s, i, j, k, 1));
+    }
+  for (int k = kz1; k <= kz2; ++k) {
+    for (int i = ix1; i <= ix2; ++i)
+      AV(s, i, jy2, k, 3) = dyi * (2. * AV(s, i, jy2, k, 1) - 3. * AV(s, i, jy2 - 1, k, 1) + AV(s, i, jy2 - 2, k, 1));
+    for (int i = ix1; i <= ix2; ++i) AV(s, i, jy2 - 1, k, 3) = dyi * (AV(s, i, jy2, k, 1) - AV(s, i, jy2 - 1, k, 1));
+  }
+  for (int k = kz1; k <= kz2; ++k)
+    for (int i = ix1; i <= ix2; ++i) AV(s, i, jy1, k, 3) = dyi * (AV(s, i, jy1 + 1, k, 1) - AV(s, i, jy1, k, 1));
+  for (int k = kz1; k <= kz2; ++k)
+    for (int j = jy1 + 1; j <= jy2 - 2; ++j)
+      for (int i = ix1; i <= ix2; ++i) AV(s, i, j, k, 3) = dyi * (AV(s, i, j + 1, k, 1) - AV(s, i, j, k, 1));
+  if (s->p.ndim == 2) return;
+  for (int j = jy1; j <= jy2; ++j)
+    for (int i = ix1; i <= ix2; ++i) {
+      AV(s, i, j, kz2 + 1, 1) = 2. * AV(s, i, j, kz2, 1) - AV(s, i, j, kz2 - 1, 1);
+      AV(s, i, j, kz2, 4) = dzi * (AV(s, i, j, kz2 + 1, 1) - AV(s, i, j, kz2, 1));
+    }
+  for (int j = jy1; j <= jy2; ++j)
+    for (int i = ix1; i <= ix2; ++i) {
+      AV(s, i, j, kz1 - 1, 1) = 2. * AV(s, i, j, kz1, 1) - AV(s, i, j, kz1 + 1, 1);
+      AV(s, i, j, kz1, 4) = dzi * (AV(s, i, j, kz1 + 1, 1) - AV(s, i, j, kz1, 1));
+    }
+  for (int k = kz1 + 1; k <= kz2 - 1; ++k)
+    for (int j = jy1; j <= jy2; ++j)
+      for (int i = ix1; i <= ix2; ++i) AV(s, i, j, k, 4) = dzi * (AV(s, i, j, k + 1, 1) - AV(s, i, j, k, 1));
+}
+
+/* env_amp_prepare (env_evolve_in_time.f90:129-158): av(1) = |A^n|^2/2 on the
+   interior, then env_grad. */
+static void ora_env_amp_prepare(ora_sim* s) {
+  for (int k = s->kz1; k <= s->kz2; ++k)
+    for (int j = s->jy1; j <= s->jy2; ++j)
+      for (int i = s->ix1; i <= s->ix2; ++i)
+        AV(s, i, j, k, 1) = 0.5 * (ENV(s, i, j, k, 1) * ENV(s, i, j, k, 1) + ENV(s, i, j, k, 2) * ENV(s, i, j, k, 2));
+  ora_env_grad(s);
+}
+
+/* set_env_acc (src/particles/grid_part_connect.f90:414-615): qqh gather at
+   x^n of (E, B), F = |A|^2/2 and grad F; the approximate gamma
+   gam_new = (gam - (dth q E.p gam - dth q^2 gradF.p / 2) / gam^2) / gam^2;
+   exit pt(1:3) = q E - q^2 gradF / (2 gam_new), pt(4:6) = q B / gam_new,
+   pt(7) = wgh / gam_new (2D: pt(1:2), pt(3) = q Bz / gam_new, pt(5)). */
+static void ora_env_acc(ora_sim* s, int64_t np) {
+  const agpu_params* p = &s->p;
+  const double dth = 0.5 * p->dt;
+  for (int64_t n = 1; n <= np; ++n) {
+    ora_pack w = ora_unpack(PART(s, 0, n, s->ndv));
+    const double charge = (double)w.charge;
+    double ax1[3], axh1[3], ay1[3], ayh1[3], az1[3], azh1[3];
+    int i, ih, j, jh, k, kh;
+    if (p->ndim == 2) {
+      double ap[7] = {0, 0, 0, 0, 0, 0, 0};
+      const double xp0 = p->dx_inv * (PART(s, 0, n, 1) - p->xmn);
+      const double xp1 = p->dy_inv * (PART(s, 0, n, 2) - p->ymn);
+      const double u1 = PART(s, 0, n, 3), u2 = PART(s, 0, n, 4);
+      ora_qqh_1d(xp0, ax1, axh1, &i, &ih);
+      ora_qqh_1d(xp1, ay1, ayh1, &j, &jh);
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = j + j1;
+        double dvol = ay1[j1];
+        for (int i1 = 0; i1 <= 2; ++i1) ap[6] = ap[6] + ax1[i1] * dvol * AV(s, i + i1, j2, 1, 1);
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = dvol * axh1[i1];
+          ap[1] = ap[1] + dvol1 * EBF(s, ih + i1, j2, 1, 1);
+          ap[4] = ap[4] + dvol1 * AV(s, ih + i1, j2, 1, 2);
+        }
+      }
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = jh + j1;
+        double dvol = ayh1[j1];
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = dvol * ax1[i1];
+          ap[2] = ap[2] + dvol1 * EBF(s, i + i1, j2, 1, 2);
+          ap[5] = ap[5] + dvol1 * AV(s, i + i1, j2, 1, 3);
+        }
+        for (int i1 = 0; i1 <= 2; ++i1) ap[3] = ap[3] + axh1[i1] * dvol * EBF(s, ih + i1, j2, 1, 3);
+      }
+      const double gam2 = 1. + u1 * u1 + u2 * u2 + ap[6];
+      for (int c = 1; c <= 3; ++c) ap[c] = charge * ap[c];
+      for (int c = 4; c <= 5; ++c) ap[c] = 0.5 * charge * charge * ap[c];
+      const double aa1 = dth * (ap[1] * u1 + ap[2] * u2);
+      const double b1 = dth * (ap[4] * u1 + ap[5] * u2);
+      const double gam = sqrt(gam2);
+      const double dgam = (aa1 * gam - b1) / gam2;
+      const double gam_inv = (gam - dgam) / gam2;
+      for (int c = 3; c <= 5; ++c) ap[c] = ap[c] * gam_inv;
+      PT(s, n, 1) = ap[1] - ap[4];
+      PT(s, n, 2) = ap[2] - ap[5];
+      PT(s, n, 3) = ap[3];
+      PT(s, n, 5) = (double)w.wgh * gam_inv;
+      continue;
+    }
+    double ap[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const double xp0 = p->dx_inv * (PART(s, 0, n, 1) - p->xmn);
+    const double xp1 = p->dy_inv * (PART(s, 0, n, 2) - p->ymn);
+    const double xp2 = p->dz_inv * (PART(s, 0, n, 3) - p->zmn);
+    const double u1 = PART(s, 0, n, 4), u2 = PART(s, 0, n, 5), u3 = PART(s, 0, n, 6);
+    ora_qqh_1d(xp0, ax1, axh1, &i, &ih);
+    ora_qqh_1d(xp1, ay1, ayh1, &j, &jh);
+    ora_qqh_1d(xp2, az1, azh1, &k, &kh);
+    for (int k1 = 0; k1 <= 2; ++k1) {
+      int k2 = k + k1;
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = j + j1;
+        double dvol = ay1[j1] * az1[k1];
+        for (int i1 = 0; i1 <= 2; ++i1) ap[10] = ap[10] + ax1[i1] * dvol * AV(s, i1 + i, j2, k2, 1);
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = dvol * axh1[i1];
+          ap[1] = ap[1] + dvol1 * EBF(s, i1 + ih, j2, k2, 1);
+          ap[7] = ap[7] + dvol1 * AV(s, i1 + ih, j2, k2, 2);
+        }
+      }
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = jh + j1;
+        double dvol = ayh1[j1] * az1[k1];
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = dvol * ax1[i1];
+          ap[2] = ap[2] + dvol1 * EBF(s, i + i1, j2, k2, 2);
+          ap[8] = ap[8] + dvol1 * AV(s, i + i1, j2, k2, 3);
+        }
+        for (int i1 = 0; i1 <= 2; ++i1) ap[6] = ap[6] + axh1[i1] * dvol * EBF(s, i1 + ih, j2, k2, 6);
+      }
+    }
+    for (int k1 = 0; k1 <= 2; ++k1) {
+      int k2 = kh + k1;
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = jh + j1;
+        double dvol = ayh1[j1] * azh1[k1];
+        for (int i1 = 0; i1 <= 2; ++i1) ap[4] = ap[4] + ax1[i1] * dvol * EBF(s, i1 + i, j2, k2, 4);
+      }
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = j + j1;
+        double dvol = ay1[j1] * azh1[k1];
+        for (int i1 = 0; i1 <= 2; ++i1) ap[5] = ap[5] + axh1[i1] * dvol * EBF(s, ih + i1, j2, k2, 5);
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = dvol * ax1[i1];
+          ap[3] = ap[3] + dvol1 * EBF(s, i1 + i, j2, k2, 3);
+          ap[9] = ap[9] + dvol1 * AV(s, i1 + i, j2, k2, 4);
+        }
+      }
+    }
+    const double gam2 = 1. + u1 * u1 + u2 * u2 + u3 * u3 + ap[10];
+    for (int c = 1; c <= 6; ++c) ap[c] = charge * ap[c];
+    for (int c = 7; c <= 9; ++c) ap[c] = 0.5 * charge * charge * ap[c];
+    const double aa1 = dth * (ap[1] * u1 + ap[2] * u2 + ap[3] * u3);
+    const double b1 = dth * (ap[7] * u1 + ap[8] * u2 + ap[9] * u3);
+    const double gam = sqrt(gam2);
+    const double dgam = (aa1 * gam - b1) / gam2;
+    const double gam_inv = (gam - dgam) / gam2;
+    for (int c = 4; c <= 9; ++c) ap[c] = ap[c] * gam_inv;
+    for (int c = 1; c <= 3; ++c) PT(s, n, c) = ap[c] - ap[c + 6];
+    for (int c = 4; c <= 6; ++c) PT(s, n, c) = ap[c];
+    PT(s, n, 7) = (double)w.wgh * gam_inv;
+  }
+}
+
+/* lpf_env_momenta (src/dynamics/boris_push.f90:170-223): Boris rotation
+   with the force pt(1:3) and pt(4:6) = q B / gam (2D: pt(1:2), pt(3));
+   p^{n-1/2} -> p^{n+1/2}; exit pt(1:3) = x^n. */
+static void ora_env_momenta(ora_sim* s, int64_t np) {
+  const double alp = 0.5 * s->p.dt * s->p.lorentz_fact[0];
+  for (int64_t n = 1; n <= np; ++n) {
+    if (s->p.curr_ndim == 2) {
+      const double pp1 = PART(s, 0, n, 3), pp2 = PART(s, 0, n, 4);
+      const double efp1 = alp * PT(s, n, 1), efp2 = alp * PT(s, n, 2), efp3 = alp * PT(s, n, 3);
+      const double vp1 = pp1 + efp1, vp2 = pp2 + efp2;
+      const double bb1 = efp3;
+      const double b2 = 1. + bb1 * bb1;
+      double vph1 = vp1 + vp2 * bb1;
+      double vph2 = vp2 - vp1 * bb1;
+      vph1 = vph1 / b2;
+      vph2 = vph2 / b2;
+      PART(s, 0, n, 3) = 2. * vph1 - pp1;
+      PART(s, 0, n, 4) = 2. * vph2 - pp2;
+      PT(s, n, 1) = PART(s, 0, n, 1);
+      PT(s, n, 2) = PART(s, 0, n, 2);
+      continue;
+    }
+    double pp[3], efp[6], vp[3], bb[3], vph[3];
+    for (int c = 0; c < 3; ++c) pp[c] = PART(s, 0, n, 4 + c);
+    for (int c = 0; c < 6; ++c) efp[c] = alp * PT(s, n, 1 + c);
+    for (int c = 0; c < 3; ++c) vp[c] = efp[c] + pp[c];
+    for (int c = 0; c < 3; ++c) bb[c] = efp[3 + c];
+    const double b2 = 1. + (bb[0] * bb[0] + bb[1] * bb[1] + bb[2] * bb[2]);
+    const double bv = bb[0] * vp[0] + bb[1] * vp[1] + bb[2] * vp[2];
+    vph[0] = vp[0] + vp[1] * bb[2] - vp[2] * bb[1] + bb[0] * bv;
+    vph[1] = vp[1] + vp[2] * bb[0] - vp[0] * bb[2] + bb[1] * bv;
+    vph[2] = vp[2] + vp[0] * bb[1] - vp[1] * bb[0] + bb[2] * bv;
+    for (int c = 0; c < 3; ++c) vph[c] = vph[c] / b2;
+    for (int c = 0; c < 3; ++c) PART(s, 0, n, 4 + c) = 2. * vph[c] - pp[c];
+    for (int c = 0; c < 3; ++c) PT(s, n, 1 + c) = PART(s, 0, n, 1 + c);
+  }
+}
+
+/* set_env_density (grid_part_connect.f90:884-952): qden weights at x^n
+   (pt(1:ndim), made local in place) times wgh/gam (pt(7), 2D pt(5)) summed
+   into av(1) at nodes i-1..i+1. */
+static void ora_env_density(ora_sim* s, int64_t np) {
+  const agpu_params* p = &s->p;
+  for (int64_t n = 1; n <= np; ++n) {
+    double ax1[3], ay1[3], az1[3];
+    int i, j, k;
+    PT(s, n, 1) = p->dx_inv * (PT(s, n, 1) - p->xmn);
+    PT(s, n, 2) = p->dy_inv * (PT(s, n, 2) - p->ymn);
+    if (p->ndim == 2) {
+      const double wghp = PT(s, n, 5);
+      ora_qden_1d(PT(s, n, 1), ax1, &i);
+      ora_qden_1d(PT(s, n, 2), ay1, &j);
+      i = i - 1;
+      j = j - 1;
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        double dvol = ay1[j1] * wghp;
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = dvol * ax1[i1];
+          AV(s, i1 + i, j + j1, 1, 1) = AV(s, i1 + i, j + j1, 1, 1) + dvol1;
+        }
+      }
+      continue;
+    }
+    PT(s, n, 3) = p->dz_inv * (PT(s, n, 3) - p->zmn);
+    const double wghp = PT(s, n, 7);
+    ora_qden_1d(PT(s, n, 1), ax1, &i);
+    ora_qden_1d(PT(s, n, 2), ay1, &j);
+    ora_qden_1d(PT(s, n, 3), az1, &k);
+    i = i - 1;
+    j = j - 1;
+    k = k - 1;
+    for (int k1 = 0; k1 <= 2; ++k1)
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        double dvol = ay1[j1] * az1[k1] * wghp;
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = dvol * ax1[i1];
+          AV(s, i1 + i, j + j1, k + k1, 1) = AV(s, i1 + i, j + j1, k + k1, 1) + dvol1;
+        }
+      }
+  }
+}
+
+/* den_zyxbd (src/parallel/mpi_curr_interface.f90, called by env_den_collect,
+   env_evolve_in_time.f90:37-78), one rank: fold the first ghost layer of
+   av(1) into the second interior layer and copy it onto the edge node, z
+   then y then x; the ghosts keep their values. */
+static void ora_den_zyxbd(ora_sim* s) {
+  const int i1 = s->ix1, i2 = s->ix2, j1 = s->jy1, j2 = s->jy2, k1 = s->kz1, k2 = s->kz2;
+  if (s->p.ndim > 2 && s->p.ibz == 0) {
+    for (int iy = j1; iy <= j2; ++iy)
+      for (int ix = i1; ix <= i2; ++ix) {
+        AV(s, ix, iy, k1 + 1, 1) = AV(s, ix, iy, k1 + 1, 1) + AV(s, ix, iy, k1 - 1, 1);
+        AV(s, ix, iy, k1, 1) = AV(s, ix, iy, k1 + 1, 1);
+      }
+    for (int iy = j1; iy <= j2; ++iy)
+      for (int ix = i1; ix <= i2; ++ix) {
+        AV(s, ix, iy, k2 - 1, 1) = AV(s, ix, iy, k2 - 1, 1) + AV(s, ix, iy, k2 + 1, 1);
+        AV(s, ix, iy, k2, 1) = AV(s, ix, iy, k2 - 1, 1);
+      }
+  }
+  if (s->p.iby == 0 || s->p.iby == 1) {
+    for (int k = k1; k <= k2; ++k)
+      for (int ix = i1; ix <= i2; ++ix) {
+        AV(s, ix, j1 + 1, k, 1) = AV(s, ix, j1 + 1, k, 1) + AV(s, ix, j1 - 1, k, 1);
+        if (s->p.iby == 0) AV(s, ix, j1, k, 1) = AV(s, ix, j1 + 1, k, 1);
+        else AV(s, ix, j1 - 1, k, 1) = 0.0;
+      }
+  }
+  if (s->p.iby < 2) {
+    for (int k = k1; k <= k2; ++k)
+      for (int ix = i1; ix <= i2; ++ix) {
+        AV(s, ix, j2 - 1, k, 1) = AV(s, ix, j2 - 1, k, 1) + AV(s, ix, j2 + 1, k, 1);
+        AV(s, ix, j2, k, 1) = AV(s, ix, j2 - 1, k, 1);
+      }
+  }
+  if (s->p.ibx < 2) {
+    for (int k = k1; k <= k2; ++k)
+      for (int iy = j1; iy <= j2; ++iy) {
+        AV(s, i1 + 1, iy, k, 1) = AV(s, i1 + 1, iy, k, 1) + AV(s, i1 - 1, iy, k, 1);
+        AV(s, i1, iy, k, 1) = AV(s, i1 + 1, iy, k, 1);
+      }
+    for (int k = k1; k <= k2; ++k)
+      for (int iy = j1; iy <= j2; ++iy) {
+        AV(s, i2 - 1, iy, k, 1) = AV(s, i2 - 1, iy, k, 1) + AV(s, i2 + 1, iy, k, 1);
+        AV(s, i2, iy, k, 1) = AV(s, i2 - 1, iy, k, 1);
+      }
+  }
+}
+
+/* env_bds(env, 2, 2) (src/fields/grid_fields.f90:864-1067) on env(1:2):
+   x ghosts copy the edge node (COEFF_0, a one-term DOT_PRODUCT summed from
+   zero), then the y ghosts over the widened x range and the z ghosts over
+   the widened x, y ranges take the quadratic extrapolation
+   alpha (e1 - e2) - 2 e1 + 3 e0 (alpha = 1 on a uniform grid); ib = 1 is
+   the parity copy. */
+static void ora_env_bds(ora_sim* s) {
+  static const int xpar[2] = {-1, 1}, ypar[2] = {1, -1}, zpar[2] = {1, 1};
+  int i1 = s->ix1, i2 = s->ix2, j1 = s->jy1, j2 = s->jy2, k1 = s->kz1, k2 = s->kz2;
+  const int pl = 2, pr = 2;
+  for (int c = 1; c <= 2; ++c)
+    for (int k = k1; k <= k2; ++k)
+      for (int j = j1; j <= j2; ++j) {
+        for (int point = pl; point >= 1; --point) {
+          const int i = i1 - point;
+          ENV(s, i, j, k, c) = (s->p.ibx == 1) ? xpar[c - 1] * ENV(s, 2 * i1 - i, j, k, c) : 0.0 + 1.0 * ENV(s, i1, j, k, c);
+        }
+        for (int point = 1; point <= pr; ++point) {
+          const int i = i2 + point;
+          ENV(s, i, j, k, c) = (s->p.ibx == 1) ? xpar[c - 1] * ENV(s, 2 * i2 - i, j, k, c) : 0.0 + 1.0 * ENV(s, i2, j, k, c);
+        }
+      }
+  i1 = i1 - pl;
+  i2 = i2 + pr;
+  for (int c = 1; c <= 2; ++c)
+    for (int k = k1; k <= k2; ++k)
+      for (int j = j1 - pl; j <= j1 - 1; ++j)
+        for (int i = i1; i <= i2; ++i)
+          ENV(s, i, j, k, c) = (s->p.iby == 1) ? ypar[c - 1] * ENV(s, i, 2 * j1 - j, k, c)
+                                               : (ENV(s, i, j1 + 2, k, c) - ENV(s, i, j1 + 1, k, c)) -
+                                                     2 * ENV(s, i, j1 + 1, k, c) + 3 * ENV(s, i, j1, k, c);
+  j1 = j1 - pl;
+  for (int c = 1; c <= 2; ++c)
+    for (int k = k1; k <= k2; ++k)
+      for (int j = j2 + 1; j <= j2 + pr; ++j)
+        for (int i = i1; i <= i2; ++i)
+          ENV(s, i, j, k, c) = (s->p.iby == 1) ? ypar[c - 1] * ENV(s, i, 2 * j2 - j, k, c)
+                                               : (ENV(s, i, j2 - 2, k, c) - ENV(s, i, j2 - 1, k, c)) -
+                                                     2 * ENV(s, i, j2 - 1, k, c) + 3 * ENV(s, i, j2, k, c);
+  j2 = j2 + pr;
+  if (s->p.ndim < 3) return;
+  for (int c = 1; c <= 2; ++c)
+    for (int k = k1 - pl; k <= k1 - 1; ++k)
+      for (int j = j1; j <= j2; ++j)
+        for (int i = i1; i <= i2; ++i)
+          ENV(s, i, j, k, c) = (s->p.ibz == 1) ? zpar[c - 1] * ENV(s, i, j, 2 * k1 - k, c)
+                                               : (ENV(s, i, j, k1 + 2, c) - ENV(s, i, j, k1 + 1, c)) -
+                                                     2 * ENV(s, i, j, k1 + 1, c) + 3 * ENV(s, i, j, k1, c);
+  for (int c = 1; c <= 2; ++c)
+    for (int k = k2 + 1; k <= k2 + pr; ++k)
+      for (int j = j1; j <= j2; ++j)
+        for (int i = i1; i <= i2; ++i)
+          ENV(s, i, j, k, c) = (s->p.ibz == 1) ? zpar[c - 1] * ENV(s, i, j, 2 * k2 - k, c)
+                                               : (ENV(s, i, j, k2 - 2, c) - ENV(s, i, j, k2 - 1, c)) -
+                                                     2 * ENV(s, i, j, k2 - 1, c) + 3 * ENV(s, i, j, k2, c);
+}
+
+/* advance_lpf_envelope (src/dynamics/curr_and_fields_util.f90:262-299) with
+   ib = 2 -> env_maxw_solve (src/fields/grid_fields.f90:588-694), whose
+   potential_lapl (1356-1403) and pp_lapl (326-424) build
+   S(A) = [D^2 - omp^2 chi] A in av(1:2) and first_ader adds the centred
+   x-derivative term; then A^{n+1} from the second-order time scheme. */
+static void ora_advance_lpf_envelope(ora_sim* s) {
+  const agpu_params* p = &s->p;
+  const int ix1 = s->ix1, ix2 = s->ix2, jy1 = s->jy1, jy2 = s->jy2, kz1 = s->kz1, kz2 = s->kz2;
+  ora_env_bds(s);
+  for (int k = kz1; k <= kz2; ++k)
+    for (int j = jy1; j <= jy2; ++j)
+      for (int i = ix1; i <= ix2; ++i) {
+        AV(s, i, j, k, 1) = -p->ompe * AV(s, i, j, k, 3) * ENV(s, i, j, k, 1);
+        AV(s, i, j, k, 2) = -p->ompe * AV(s, i, j, k, 3) * ENV(s, i, j, k, 2);
+      }
+  const double om0 = s->ep.om0, dtl = p->dt;
+  const double dt2 = dtl * dtl;
+  const double kfact = om0 * dtl;
+  const double k2_fact = 1. / (1. + kfact * kfact);
+  const double dx1_inv = om0 * p->dx_inv;
+  double aph1 = 1., aph2 = 0.;
+  if (s->ep.der_ord == 3) {
+    aph1 = dx1_inv * s->ep.opt_der1;
+    aph2 = dx1_inv * 0.5 * (1. - s->ep.opt_der1);
+  }
+  /* potential_lapl: x part */
+  const double dx2 = p->dx_inv * p->dx_inv;
+  double cf1 = 1., cf2 = 0.;
+  if (s->ep.der_ord > 2) {
+    cf1 = 1. - 4. * s->ep.hord_der2;
+    cf2 = s->ep.hord_der2;
+  }
+  const double dx4_1 = cf1 * dx2, dx4_2 = cf2 * dx2;
+  for (int c = 1; c <= 2; ++c)
+    for (int k = kz1; k <= kz2; ++k)
+      for (int j = jy1; j <= jy2; ++j)
+        for (int i = ix1; i <= ix2; ++i)
+          AV(s, i, j, k, c) =
+              AV(s, i, j, k, c) + dx4_1 * (ENV(s, i + 1, j, k, c) + ENV(s, i - 1, j, k, c) - 2. * ENV(s, i, j, k, c));
+  if (s->ep.der_ord > 2)
+    for (int c = 1; c <= 2; ++c)
+      for (int k = kz1; k <= kz2; ++k)
+        for (int j = jy1; j <= jy2; ++j)
+          for (int i = ix1; i <= ix2; ++i)
+            AV(s, i, j, k, c) =
+                AV(s, i, j, k, c) + dx4_2 * (ENV(s, i + 2, j, k, c) + ENV(s, i - 2, j, k, c) - 2. * ENV(s, i, j, k, c));
+  /* pp_lapl (der_ord < 4: cf(1) = 1) */
+  const double dy2 = p->dy_inv * p->dy_inv, dz2 = p->dz_inv * p->dz_inv;
+  for (int c = 1; c <= 2; ++c)
+    for (int k = kz1; k <= kz2; ++k)
+      for (int j = jy1; j <= jy2; ++j)
+        for (int i = ix1; i <= ix2; ++i)
+          AV(s, i, j, k, c) = AV(s, i, j, k, c) + dy2 * ((ENV(s, i, j + 1, k, c) - ENV(s, i, j, k, c)) -
+                                                        (ENV(s, i, j, k, c) - ENV(s, i, j - 1, k, c)));
+  if (p->ndim == 3)
+    for (int c = 1; c <= 2; ++c)
+      for (int k = kz1; k <= kz2; ++k)
+        for (int j = jy1; j <= jy2; ++j)
+          for (int i = ix1; i <= ix2; ++i)
+            AV(s, i, j, k, c) = AV(s, i, j, k, c) + dz2 * ((ENV(s, i, j, k + 1, c) - ENV(s, i, j, k, c)) -
+                                                          (ENV(s, i, j, k, c) - ENV(s, i, j, k - 1, c)));
+  /* first_ader */
+  for (int k = kz1; k <= kz2; ++k)
+    for (int j = jy1; j <= jy2; ++j)
+      for (int i = ix1; i <= ix2; ++i) {
+        if (s->ep.der_ord < 3) {
+          AV(s, i, j, k, 1) = AV(s, i, j, k, 1) - dx1_inv * (ENV(s, i + 1, j, k, 2) - ENV(s, i - 1, j, k, 2));
+          AV(s, i, j, k, 2) = AV(s, i, j, k, 2) + dx1_inv * (ENV(s, i + 1, j, k, 1) - ENV(s, i - 1, j, k, 1));
+        } else {
+          AV(s, i, j, k, 1) = AV(s, i, j, k, 1) - aph1 * (ENV(s, i + 1, j, k, 2) - ENV(s, i - 1, j, k, 2)) -
+                              aph2 * (ENV(s, i + 2, j, k, 2) - ENV(s, i - 2, j, k, 2));
+          AV(s, i, j, k, 2) = AV(s, i, j, k, 2) + aph1 * (ENV(s, i + 1, j, k, 1) - ENV(s, i - 1, j, k, 1)) +
+                              aph2 * (ENV(s, i + 2, j, k, 1) - ENV(s, i - 2, j, k, 1));
+        }
+      }
+  for (int k = kz1; k <= kz2; ++k)
+    for (int j = jy1; j <= jy2; ++j)
+      for (int i = ix1; i <= ix2; ++i) {
+        AV(s, i, j, k, 1) = dt2 * AV(s, i, j, k, 1) + 2. * ENV(s, i, j, k, 1) - ENV(s, i, j, k, 3) + kfact * ENV(s, i, j, k, 4);
+        AV(s, i, j, k, 2) = dt2 * AV(s, i, j, k, 2) + 2. * ENV(s, i, j, k, 2) - ENV(s, i, j, k, 4) - kfact * ENV(s, i, j, k, 3);
+      }
+  for (int k = kz1; k <= kz2; ++k)
+    for (int j = jy1; j <= jy2; ++j)
+      for (int i = ix1; i <= ix2; ++i) {
+        ENV(s, i, j, k, 3) = ENV(s, i, j, k, 1);
+        ENV(s, i, j, k, 4) = ENV(s, i, j, k, 2);
+        ENV(s, i, j, k, 1) = k2_fact * (AV(s, i, j, k, 1) - kfact * AV(s, i, j, k, 2));
+        ENV(s, i, j, k, 2) = k2_fact * (AV(s, i, j, k, 2) + kfact * AV(s, i, j, k, 1));
+      }
+}
+
+/* env_fields_average (env_evolve_in_time.f90:103-127): av(1) =
+   |(A^{n+1} + A^n)/2|^2 / 2 = (1/8)((e1+e3)^2 + (e2+e4)^2), then env_grad. */
+static void ora_env_fields_average(ora_sim* s) {
+  const double frac = 1.0 / 8.;
+  for (int k = s->kz1; k <= s->kz2; ++k)
+    for (int j = s->jy1; j <= s->jy2; ++j)
+      for (int i = s->ix1; i <= s->ix2; ++i) {
+        const double a = ENV(s, i, j, k, 1) + ENV(s, i, j, k, 3);
+        const double b = ENV(s, i, j, k, 2) + ENV(s, i, j, k, 4);
+        AV(s, i, j, k, 1) = frac * (a * a + b * b);
+      }
+  ora_env_grad(s);
+}
+
+/* set_env_grad_interp (grid_part_connect.f90:760-882): qqh gather at x^n of
+   grad F (av(2:4)) and F (av(1)); exit pt(1:3) = grad F, pt(4) = F (2D:
+   pt(1:2), pt(3)). */
+static void ora_env_grad_interp(ora_sim* s, int64_t np) {
+  const agpu_params* p = &s->p;
+  for (int64_t n = 1; n <= np; ++n) {
+    double ax1[3], axh1[3], ay1[3], ayh1[3], az1[3], azh1[3];
+    int i, ih, j, jh, k, kh;
+    const double xp0 = p->dx_inv * (PART(s, 0, n, 1) - p->xmn);
+    const double xp1 = p->dy_inv * (PART(s, 0, n, 2) - p->ymn);
+    ora_qqh_1d(xp0, ax1, axh1, &i, &ih);
+    ora_qqh_1d(xp1, ay1, ayh1, &j, &jh);
+    if (p->ndim == 2) {
+      double ap[4] = {0, 0, 0, 0};
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = j + j1;
+        double dvol = ay1[j1];
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = dvol * axh1[i1];
+          ap[1] = ap[1] + dvol1 * AV(s, i1 + ih, j2, 1, 2);
+          ap[3] = ap[3] + ax1[i1] * dvol * AV(s, i1 + i, j2, 1, 1);
+        }
+      }
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = jh + j1;
+        double dvol = ayh1[j1];
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = dvol * ax1[i1];
+          ap[2] = ap[2] + dvol1 * AV(s, i + i1, j2, 1, 3);
+        }
+      }
+      for (int c = 1; c <= 3; ++c) PT(s, n, c) = ap[c];
+      continue;
+    }
+    const double xp2 = p->dz_inv * (PART(s, 0, n, 3) - p->zmn);
+    ora_qqh_1d(xp2, az1, azh1, &k, &kh);
+    double ap[5] = {0, 0, 0, 0, 0};
+    for (int k1 = 0; k1 <= 2; ++k1) {
+      int k2 = k + k1;
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = j + j1;
+        double dvol = ay1[j1] * az1[k1];
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = dvol * axh1[i1];
+          ap[1] = ap[1] + dvol1 * AV(s, i1 + ih, j2, k2, 2);
+          ap[4] = ap[4] + ax1[i1] * dvol * AV(s, i1 + i, j2, k2, 1);
+        }
+      }
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = jh + j1;
+        double dvol = ayh1[j1] * az1[k1];
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = dvol * ax1[i1];
+          ap[2] = ap[2] + dvol1 * AV(s, i + i1, j2, k2, 3);
+        }
+      }
+      k2 = kh + k1;
+      for (int j1 = 0; j1 <= 2; ++j1) {
+        int j2 = j + j1;
+        double dvol = ay1[j1] * azh1[k1];
+        for (int i1 = 0; i1 <= 2; ++i1) {
+          double dvol1 = dvol * ax1[i1];
+          ap[3] = ap[3] + dvol1 * AV(s, i + i1, j2, k2, 4);
+        }
+      }
+    }
+    for (int c = 1; c <= 4; ++c) PT(s, n, c) = ap[c];
+  }
+}
+
+/* lpf_env_positions (src/dynamics/boris_push.f90:225-295), vbeam = 0:
+   gamma^{n+1/2} with the ponderomotive correction, x^{n+1} = x^n + dt v;
+   exit pt(1:3) = dt v, pt(4:6) = x^n, pt(7) = wgh_cmp (iform < 2). */
+static void ora_env_positions(ora_sim* s, int64_t np) {
+  const double dt_lp = s->p.dt;
+  const int ch = s->ndv;
+  for (int64_t n = 1; n <= np; ++n) {
+    if (s->p.curr_ndim == 2) {
+      const double pp1 = PART(s, 0, n, 3), pp2 = PART(s, 0, n, 4);
+      double vp1 = PT(s, n, 1), vp2 = PT(s, n, 2);
+      const double gam2 = 1. + (pp1 * pp1 + pp2 * pp2) + PT(s, n, 3);
+      const double gam = sqrt(gam2);
+      const double gam3 = gam2 * gam;
+      const double b2 = 0.25 * (pp1 * vp1 + pp2 * vp2);
+      double gam_inv = 1. / gam;
+      gam_inv = gam_inv * (1. - dt_lp * b2 / gam3);
+      vp1 = dt_lp * gam_inv * pp1;
+      vp2 = dt_lp * gam_inv * pp2;
+      PT(s, n, 3) = PART(s, 0, n, 1);
+      PT(s, n, 4) = PART(s, 0, n, 2);
+      PT(s, n, 5) = dt_lp * gam_inv;
+      PART(s, 0, n, 1) = PART(s, 0, n, 1) + vp1;
+      PART(s, 0, n, 2) = PART(s, 0, n, 2) + vp2;
+      PT(s, n, 1) = vp1;
+      PT(s, n, 2) = vp2;
+      continue;
+    }
+    double pp[3], vp[3];
+    for (int c = 0; c < 3; ++c) pp[c] = PART(s, 0, n, 4 + c);
+    for (int c = 0; c < 3; ++c) vp[c] = PT(s, n, 1 + c);
+    const double gam2 = 1. + (pp[0] * pp[0] + pp[1] * pp[1] + pp[2] * pp[2]) + PT(s, n, 4);
+    const double gam = sqrt(gam2);
+    const double gam3 = gam2 * gam;
+    const double b2 = 0.25 * (pp[0] * vp[0] + pp[1] * vp[1] + pp[2] * vp[2]);
+    double gam_inv = 1. / sqrt(gam2);
+    gam_inv = gam_inv * (1. - dt_lp * b2 / gam3);
+    for (int c = 0; c < 3; ++c) vp[c] = dt_lp * gam_inv * pp[c];
+    for (int c = 0; c < 3; ++c) PT(s, n, 4 + c) = PART(s, 0, n, 1 + c);
+    PT(s, n, 7) = dt_lp * gam_inv;
+    for (int c = 0; c < 3; ++c) PART(s, 0, n, 1 + c) = PART(s, 0, n, 1 + c) + vp[c];
+    for (int c = 0; c < 3; ++c) PT(s, n, 1 + c) = vp[c];
+  }
+  if (s->p.iform < 2)
+    for (int64_t n = 1; n <= np; ++n) PT(s, n, ch) = PART(s, 0, n, ch);
+}
+
+int ora_env_run(ora_sim* s, int iter, double t, agpu_step_out* out) {
+  agpu_params* p = &s->p;
+  agpu_step_out dummy;
+  if (!out) out = &dummy;
+  memset(out, 0, sizeof(*out));
+  out->ion_field_max = -1.0;
+  if (!s->env) return AGPU_E_STATE;
+  const size_t c3 = (size_t)s->n1p * s->n2p * s->n3p;
+  memset(s->av, 0, sizeof(double) * c3 * (size_t)s->nav); /* jc(:,:,:,:) = 0.0 */
+  ora_env_amp_prepare(s);
+  int64_t np = s->np[0];
+  memset(s->ebfp, 0, sizeof(double) * (size_t)s->ebfp_cap * (size_t)s->ndv); /* ebfp(:,:) = 0.0 */
+  ora_env_acc(s, np);
+  ora_env_momenta(s, np);
+  memset(s->av, 0, sizeof(double) * c3); /* jc(:,:,:,1) = 0.0 */
+  ora_env_density(s, np);
+  ora_den_zyxbd(s);
+  memcpy(s->av + 2 * c3, s->av, sizeof(double) * c3); /* jc(:,:,:,3) = jc(:,:,:,1) */
+  ora_advance_lpf_envelope(s);
+  ora_env_fields_average(s);
+  ora_env_grad_interp(s, np);
+  ora_env_positions(s, np);
+  out->removed[0] += ora_cell_part_dist_step(s, 0);
+  np = s->np[0];
+  ora_zero_currents(s);
+  if (np > 0) ora_curr_accumulate(s, 0, np);
+  ora_curr_collect(s);
+  ora_advance_fields(s);
+  int rc = 0;
+  if (p->w_speed > 0.0 && p->w_sh > 0) {
+    if (t >= p->wi_time && t < p->wf_time) {
+      if (iter % p->w_sh == 0) rc = ora_window_xshift(s, p->w_sh, iter, out);
+    }
+  }
+  for (int ic = 0; ic < 4; ++ic) out->np[ic] = s->np[ic];
+  out->xmn = p->xmn;
+  out->error_bits = s->error_bits;
+  return rc;
 }

@@ -75,6 +75,12 @@ def load():
         "ora_init_lp_fields": (None, [P, P]),
         "ora_envar_species": (None, [P, C.c_int, C.c_double, D]),
         "ora_envar_fields": (None, [P, D]),
+        "ora_env_enable": (C.c_int, [P, P]),
+        "ora_set_envelope": (C.c_int, [P, D]),
+        "ora_get_envelope": (C.c_int, [P, D]),
+        "ora_get_env_source": (C.c_int, [P, D]),
+        "ora_init_envelope": (None, [P, P, C.c_int]),
+        "ora_env_run": (C.c_int, [P, C.c_int, C.c_double, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -143,6 +149,37 @@ class Oracle:
     def init_lp_fields(self, pulse):
         """init_lp_inc0_fields: pulse is an aladyn_b200.abi.AgpuLpPulse."""
         self.lib.ora_init_lp_fields(self.h, C.cast(C.pointer(pulse), C.c_void_p))
+
+    # ---- envelope cycle ------------------------------------------------
+    def env_enable(self, ep):
+        """Allocate env(n1p,n2p,n3p,4); ep is an aladyn_b200.abi.AgpuEnvParams."""
+        assert self.lib.ora_env_enable(self.h, C.cast(C.pointer(ep), C.c_void_p)) == 0
+
+    def init_envelope(self, pulse, plane_wave=False):
+        """init_(gprof_)envelope_field: adds the pulse's A^n, A^{n-1} to env."""
+        self.lib.ora_init_envelope(self.h, C.cast(C.pointer(pulse), C.c_void_p), 1 if plane_wave else 0)
+
+    def set_envelope(self, env):
+        a = np.asfortranarray(env, dtype=np.float64)
+        assert a.shape == (self.n1p, self.n2p, self.n3p, 4)
+        assert self.lib.ora_set_envelope(self.h, _dp(a)) == 0
+
+    def get_envelope(self):
+        a = np.zeros((self.n1p, self.n2p, self.n3p, 4), dtype=np.float64, order="F")
+        assert self.lib.ora_get_envelope(self.h, _dp(a)) == 0
+        return a
+
+    def get_env_source(self):
+        nav = 4 if self.n3p > 1 else 3
+        a = np.zeros((self.n1p, self.n2p, self.n3p, nav), dtype=np.float64, order="F")
+        assert self.lib.ora_get_env_source(self.h, _dp(a)) == 0
+        return a
+
+    def env_run(self, t, iteration):
+        from aladyn_b200.abi import AgpuStepOut
+        out = AgpuStepOut()
+        rc = self.lib.ora_env_run(self.h, iteration, t, C.byref(out))
+        return rc, out
 
     def get_fields(self):
         a = np.zeros(self.field_shape(), dtype=np.float64, order="F")

@@ -1,0 +1,313 @@
+"""The oracle's envelope cycle (env_run / env_lpf2_evolve,
+src/dynamics/env_evolve_in_time.f90:196-391) against an independent numpy
+restatement of its grid part (env_bds, potential_lapl + pp_lapl,
+env_maxw_solve, env_fields_average, env_grad; src/fields/grid_fields.f90,
+curr_and_fields_util.f90:262-299) and of the pulse set-up
+(init_gprof_envelope_field / init_envelope_field, init_grid_fields.f90:
+140-399), bit for bit where the arithmetic is the same; plus the physics the
+model must show: a vacuum pulse moves at c, the ponderomotive force pushes an
+electron away from the intensity peak, and the Esirkepov current of the
+envelope pusher conserves charge."""
+import math
+
+import numpy as np
+import pytest
+
+from aladyn_b200.abi import AgpuLpPulse
+from aladyn_b200.config import env_params
+from aladyn_b200.conservation import step_residual
+from aladyn_b200.sim import pack_slot
+from oracle.oracle import Oracle
+from tests.helpers import LAM0, grid_small, small_case
+
+
+def env_case(ndim, nx=64, ny=24, nz=16, der_ord=2, cap=4000, w_sh=10):
+    p = small_case(ndim, nx=nx, ny=ny, nz=nz, cap=cap, w_sh=w_sh)
+    g = grid_small(ndim, nx, ny, nz)
+    return p, g, env_params(g, LAM0, der_ord)
+
+
+def pulse(p, a0=1.0, g_prof=True, xc_frac=0.5, wx_frac=0.12, wy_frac=0.3):
+    """A pulse centred in the box: ee0 = a0, focus at the centre (tf = 0)."""
+    a = AgpuLpPulse()
+    lx = p.nx * p.dx
+    a.ee0 = a0
+    a.t_loc = 0.0
+    a.tf = 0.0
+    a.wx = wx_frac * lx
+    a.wy = wy_frac * p.ny * p.dy
+    a.xf0 = p.xmn + xc_frac * lx
+    a.om0 = 2.0 * math.pi / LAM0
+    a.ycent = 0.0
+    a.zcent = 0.0
+    a.g_prof = 1 if g_prof else 0
+    return a
+
+
+# ---- numpy restatement ------------------------------------------------------
+def numpy_init(p, a, plane_wave=False):
+    """init_(gprof_)envelope_field on a zero env."""
+    n1p, n2p, n3p = p.nx + 5, p.ny + 5, (p.nz + 5 if p.ndim == 3 else 1)
+    env = np.zeros((n1p, n2p, n3p, 4), order="F")
+    i = np.arange(3, p.nx + 3)
+    j = np.arange(3, p.ny + 3)
+    k = np.arange(3, p.nz + 3) if p.ndim == 3 else np.array([1])
+    X = (p.xmn + p.dx * (i - 3.0))[:, None, None] - a.xf0 + 0 * j[None, :, None] + 0 * k[None, None, :]
+    yy = (p.ymn + p.dy * (j - 3.0) - a.ycent) / a.wy
+    zz = ((p.zmn + p.dz * (k - 3.0) - a.zcent) / a.wy) if p.ndim == 3 else np.zeros(1)
+    r2 = (yy[:, None] * yy[:, None] + zz[None, :] * zz[None, :]) if p.ndim == 3 else yy[:, None] * yy[:, None]
+    r2 = np.broadcast_to(r2[None], X.shape)
+    t = a.t_loc - a.tf
+    tm = t - p.dt
+    zra = 0.5 * a.om0 * a.wy * a.wy
+    pih = 0.5 * math.acos(-1.0)
+    if a.g_prof:
+        phi1 = (X - t) / a.wx
+        phi0 = (X - tm) / a.wx
+        ampl1, ampl0 = np.exp(-phi1 * phi1), np.exp(-phi0 * phi0)
+    else:
+        if plane_wave or p.ndim < 3:
+            phi1 = math.pi * (X - t) / a.wx
+            phi0 = math.pi * (X - tm) / a.wx
+        else:
+            phi1 = math.pi * (t - X) / a.wx
+            phi0 = math.pi * (tm - X) / a.wx
+        phi1 = np.where(np.abs(phi1) > pih, pih, phi1)
+        phi0 = np.where(np.abs(phi0) > pih, pih, phi0)
+        ampl1, ampl0 = np.cos(phi1) * np.cos(phi1), np.cos(phi0) * np.cos(phi0)
+    if plane_wave:
+        phi = np.arctan(X) if a.g_prof else np.zeros_like(X)
+        ar, ai = a.ee0 * np.cos(phi), -a.ee0 * np.sin(phi)
+    else:
+        xx = X / zra
+        w2 = 1. / (1. + xx * xx)
+        phi = np.arctan(xx) - xx * r2 * w2
+        ws = np.sqrt(w2) if p.ndim == 3 else np.sqrt(np.sqrt(w2))
+        ar = a.ee0 * np.cos(phi) * ws * np.exp(-w2 * r2)
+        ai = -a.ee0 * np.sin(phi) * ws * np.exp(-w2 * r2)
+    ks = slice(2, p.nz + 2) if p.ndim == 3 else slice(0, 1)
+    sl = (slice(2, p.nx + 2), slice(2, p.ny + 2), ks)
+    env[sl + (0,)] = ampl1 * ar
+    env[sl + (1,)] = ampl1 * ai
+    env[sl + (2,)] = ampl0 * ar
+    env[sl + (3,)] = ampl0 * ai
+    return env
+
+
+def numpy_env_grad(p, av):
+    """env_grad on av(..., 0) (0-based component index), der_ord < 4."""
+    nx, ny, nz = p.nx, p.ny, p.nz
+    i1, i2, j1, j2 = 2, nx + 1, 2, ny + 1            # 0-based ix1..ix2, jy1..jy2
+    k1, k2 = (2, nz + 1) if p.ndim == 3 else (0, 0)
+    F = av[..., 0]
+    K = slice(k1, k2 + 1)
+    J = slice(j1, j2 + 1)
+    gx = av[..., 1]
+    gx[i1:i2, J, K] = p.dx_inv * (F[i1 + 1:i2 + 1, J, K] - F[i1:i2, J, K])
+    gx[i2, J, K] = p.dx_inv * (2. * F[i2 - 1, J, K] - 3. * F[i2 - 2, J, K] + F[i2 - 3, J, K])
+    I = slice(i1, i2 + 1)
+    gy = av[..., 2]
+    gy[I, j1:j2, K] = p.dy_inv * (F[I, j1 + 1:j2 + 1, K] - F[I, j1:j2, K])
+    gy[I, j2, K] = p.dy_inv * (2. * F[I, j2, K] - 3. * F[I, j2 - 1, K] + F[I, j2 - 2, K])
+    if p.ndim == 3:
+        F[I, J, k2 + 1] = 2. * F[I, J, k2] - F[I, J, k2 - 1]
+        F[I, J, k1 - 1] = 2. * F[I, J, k1] - F[I, J, k1 + 1]
+        gz = av[..., 3]
+        gz[I, J, k1:k2 + 1] = p.dz_inv * (F[I, J, k1 + 1:k2 + 2] - F[I, J, k1:k2 + 1])
+
+
+def numpy_vacuum_step(p, ep, env):
+    """One env_run of an empty box: env_bds, S(A) = D^2 A (no plasma: the
+    source -ompe * 0 * A), first_ader, the time combination and the update,
+    env_fields_average and env_grad.  Returns (env, av)."""
+    env = env.copy(order="F")
+    nx, ny, nz = p.nx, p.ny, p.nz
+    i1, i2, j1, j2 = 2, nx + 1, 2, ny + 1
+    k1, k2 = (2, nz + 1) if p.ndim == 3 else (0, 0)
+    E = env
+    # env_bds: x copies, then y and z quadratic extrapolation over widened ranges
+    for c in range(2):
+        for q in (1, 2):
+            E[i1 - q, j1:j2 + 1, k1:k2 + 1, c] = 0.0 + 1.0 * E[i1, j1:j2 + 1, k1:k2 + 1, c]
+            E[i2 + q, j1:j2 + 1, k1:k2 + 1, c] = 0.0 + 1.0 * E[i2, j1:j2 + 1, k1:k2 + 1, c]
+    I = slice(i1 - 2, i2 + 3)
+    for c in range(2):
+        lo = (E[I, j1 + 2, k1:k2 + 1, c] - E[I, j1 + 1, k1:k2 + 1, c]) - 2 * E[I, j1 + 1, k1:k2 + 1, c] + \
+            3 * E[I, j1, k1:k2 + 1, c]
+        hi = (E[I, j2 - 2, k1:k2 + 1, c] - E[I, j2 - 1, k1:k2 + 1, c]) - 2 * E[I, j2 - 1, k1:k2 + 1, c] + \
+            3 * E[I, j2, k1:k2 + 1, c]
+        for q in (1, 2):
+            E[I, j1 - q, k1:k2 + 1, c] = lo
+            E[I, j2 + q, k1:k2 + 1, c] = hi
+    if p.ndim == 3:
+        J = slice(j1 - 2, j2 + 3)
+        for c in range(2):
+            lo = (E[I, J, k1 + 2, c] - E[I, J, k1 + 1, c]) - 2 * E[I, J, k1 + 1, c] + 3 * E[I, J, k1, c]
+            hi = (E[I, J, k2 - 2, c] - E[I, J, k2 - 1, c]) - 2 * E[I, J, k2 - 1, c] + 3 * E[I, J, k2, c]
+            for q in (1, 2):
+                E[I, J, k1 - q, c] = lo
+                E[I, J, k2 + q, c] = hi
+    X, Y, Z = slice(i1, i2 + 1), slice(j1, j2 + 1), slice(k1, k2 + 1)
+
+    def sh(a, di=0, dj=0, dk=0):
+        return a[i1 + di:i2 + 1 + di, j1 + dj:j2 + 1 + dj, k1 + dk:k2 + 1 + dk]
+
+    dt = p.dt
+    dt2 = dt * dt
+    kfact = ep.om0 * dt
+    k2_fact = 1. / (1. + kfact * kfact)
+    dx1_inv = ep.om0 * p.dx_inv
+    dx2 = p.dx_inv * p.dx_inv
+    cf1, cf2 = (1. - 4. * ep.hord_der2, ep.hord_der2) if ep.der_ord > 2 else (1., 0.)
+    dx4_1, dx4_2 = cf1 * dx2, cf2 * dx2
+    dy2, dz2 = p.dy_inv * p.dy_inv, p.dz_inv * p.dz_inv
+    c = []
+    for q in range(2):
+        e = E[..., q]
+        cq = -p.ompe * np.zeros_like(sh(e)) * sh(e)
+        cq = cq + dx4_1 * (sh(e, 1) + sh(e, -1) - 2. * sh(e))
+        if ep.der_ord > 2:
+            cq = cq + dx4_2 * (sh(e, 2) + sh(e, -2) - 2. * sh(e))
+        cq = cq + dy2 * ((sh(e, 0, 1) - sh(e)) - (sh(e) - sh(e, 0, -1)))
+        if p.ndim == 3:
+            cq = cq + dz2 * ((sh(e, 0, 0, 1) - sh(e)) - (sh(e) - sh(e, 0, 0, -1)))
+        c.append(cq)
+    e1, e2, e3, e4 = (E[..., q] for q in range(4))
+    if ep.der_ord < 3:
+        c[0] = c[0] - dx1_inv * (sh(e2, 1) - sh(e2, -1))
+        c[1] = c[1] + dx1_inv * (sh(e1, 1) - sh(e1, -1))
+    else:
+        aph1 = dx1_inv * ep.opt_der1
+        aph2 = dx1_inv * 0.5 * (1. - ep.opt_der1)
+        c[0] = c[0] - aph1 * (sh(e2, 1) - sh(e2, -1)) - aph2 * (sh(e2, 2) - sh(e2, -2))
+        c[1] = c[1] + aph1 * (sh(e1, 1) - sh(e1, -1)) + aph2 * (sh(e1, 2) - sh(e1, -2))
+    c1 = dt2 * c[0] + 2. * sh(e1) - sh(e3) + kfact * sh(e4)
+    c2 = dt2 * c[1] + 2. * sh(e2) - sh(e4) - kfact * sh(e3)
+    old1, old2 = sh(e1).copy(), sh(e2).copy()
+    E[X, Y, Z, 2] = old1
+    E[X, Y, Z, 3] = old2
+    E[X, Y, Z, 0] = k2_fact * (c1 - kfact * c2)
+    E[X, Y, Z, 1] = k2_fact * (c2 + kfact * c1)
+    av = np.zeros(E.shape[:3] + (p.ndim + 1,), order="F")
+    s1, s2 = E[X, Y, Z, 0] + E[X, Y, Z, 2], E[X, Y, Z, 1] + E[X, Y, Z, 3]
+    av[X, Y, Z, 0] = (1.0 / 8.) * (s1 * s1 + s2 * s2)
+    numpy_env_grad(p, av)
+    return E, av
+
+
+# ---- tests ------------------------------------------------------------------
+@pytest.mark.parametrize("ndim", [2, 3])
+@pytest.mark.parametrize("g_prof,plane_wave", [(True, False), (False, False), (True, True), (False, True)])
+def test_init_envelope_matches_numpy(ndim, g_prof, plane_wave):
+    p, g, ep = env_case(ndim)
+    o = Oracle(p)
+    o.env_enable(ep)
+    a = pulse(p, g_prof=g_prof)
+    o.init_envelope(a, plane_wave)
+    got = o.get_envelope()
+    want = numpy_init(p, a, plane_wave)
+    assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+    assert np.abs(want).max() > 0.1
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+@pytest.mark.parametrize("der_ord", [2, 3])
+def test_vacuum_step_matches_numpy(ndim, der_ord):
+    """One step of an empty box: the oracle's env and source scratch equal
+    the numpy restatement bit for bit (same operations in the same order)."""
+    p, g, ep = env_case(ndim, der_ord=der_ord)
+    o = Oracle(p)
+    o.env_enable(ep)
+    env0 = numpy_init(p, pulse(p))
+    o.set_envelope(env0)
+    rc, _ = o.env_run(0.0, 1)
+    assert rc == 0
+    want_env, want_av = numpy_vacuum_step(p, ep, env0)
+    got_env = o.get_envelope()
+    assert np.array_equal(got_env, want_env)
+    assert np.array_equal(o.get_env_source(), want_av)
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_vacuum_pulse_moves_at_c(ndim):
+    """|A|^2 of a vacuum pulse: its centroid moves at the group velocity
+    (~c) and its integral stays within 3% over 60 steps (the peak of this
+    short pulse falls by dispersion and diffraction)."""
+    p, g, ep = env_case(ndim, nx=128, ny=48, nz=48, w_sh=0)
+    o = Oracle(p)
+    o.env_enable(ep)
+    o.set_envelope(numpy_init(p, pulse(p, xc_frac=0.3, wx_frac=0.06, wy_frac=0.25)))
+
+    def centroid():
+        e = o.get_envelope()
+        a2 = e[..., 0] ** 2 + e[..., 1] ** 2
+        x = p.xmn + p.dx * (np.arange(a2.shape[0]) - 2.0)
+        prof = a2.sum(axis=(1, 2))
+        return (prof * x).sum() / prof.sum(), prof.sum()
+
+    x0, m0 = centroid()
+    steps = 60
+    for it in range(1, steps + 1):
+        assert o.env_run(it * p.dt, it)[0] == 0
+    x1, m1 = centroid()
+    v = (x1 - x0) / (steps * p.dt)
+    assert abs(v - 1.0) < 0.03, v
+    assert abs(m1 / m0 - 1.0) < 0.03, (m0, m1)
+
+
+def _one_electron(p, x, y, z=0.0):
+    rec = np.zeros((1, 7 if p.ndim == 3 else 5), order="F")
+    rec[0, 0], rec[0, 1] = x, y
+    if p.ndim == 3:
+        rec[0, 2] = z
+    rec[0, -1] = pack_slot(-1, 1, 1.0)
+    return rec
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_ponderomotive_push(ndim):
+    """An electron at rest off axis in the rising edge of the pulse is
+    pushed forward (px > 0) and away from the axis (py > 0)."""
+    p, g, ep = env_case(ndim, nx=96, ny=32, nz=24, w_sh=0)
+    o = Oracle(p)
+    o.env_enable(ep)
+    a = pulse(p, a0=2.0, xc_frac=0.4, wx_frac=0.08, wy_frac=0.25)
+    o.set_envelope(numpy_init(p, a))
+    xe = a.xf0 + 0.6 * a.wx
+    o.set_species(0, _one_electron(p, xe, 0.5 * a.wy))
+    for it in range(1, 4):
+        assert o.env_run(it * p.dt, it)[0] == 0
+    rec = o.get_species(0)
+    assert rec.shape[0] == 1
+    pc = 3 if ndim == 3 else 2
+    assert rec[0, pc] > 0.0 and rec[0, pc + 1] > 0.0, rec
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_envelope_step_conserves_charge(ndim):
+    """The Esirkepov current of the envelope pusher satisfies the discrete
+    continuity equation to FP64 round-off (particles kept off the edges)."""
+    p, g, ep = env_case(ndim, nx=48, ny=24, nz=16, w_sh=0)
+    o = Oracle(p)
+    o.env_enable(ep)
+    a = pulse(p, a0=2.0, xc_frac=0.5, wx_frac=0.1, wy_frac=0.3)
+    o.set_envelope(numpy_init(p, a))
+    rng = np.random.default_rng(5)
+    n = 400
+    lo = np.array([p.xmn + 8 * p.dx, p.ymn + 6 * p.dy, (p.zmn + 6 * p.dz) if ndim == 3 else 0.0])
+    hi = np.array([p.xmn + (p.nx - 8) * p.dx, p.ymn + (p.ny - 6) * p.dy,
+                   (p.zmn + (p.nz - 6) * p.dz) if ndim == 3 else 0.0])
+    rec = np.zeros((n, 7 if ndim == 3 else 5), order="F")
+    for d in range(ndim):
+        rec[:, d] = rng.uniform(lo[d], hi[d], n)
+        rec[:, ndim + d] = rng.normal(0.0, 0.3, n)
+    rec[:, -1] = pack_slot(-1, 0, 0.25)
+    o.set_species(0, rec)
+    for it in range(1, 3):
+        assert o.env_run(it * p.dt, it)[0] == 0
+    part0 = o.get_species(0)
+    assert o.env_run(3 * p.dt, 3)[0] == 0
+    part1 = o.get_species(0)
+    res, rho, div = step_residual(p, part0, part1, o.get_currents(), margin=4)
+    assert div > 1e-3 * rho
+    assert res <= 1e-13 * rho, (res, rho)
