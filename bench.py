@@ -671,6 +671,61 @@ def extra_pwfa(torch, warmup, steps):
             "error_bits": int(o.error_bits)}
 
 
+def extra_pwfa_envelope(torch, warmup, steps):
+    """The reference's own PWFA route (Env_cycle: beam_inject, then env_run
+    every step; model_id = 4 with a0 = 0 as its PWFA example): FP64 form,
+    the 512x256x256 PWFA box and bunch of ``extra_pwfa``, der_ord 2, the
+    envelope solver running on a zero envelope, plasma electrons and bunch
+    in species 0 pushed by the envelope pusher."""
+    from aladyn_b200.abi import AGPU_FP64
+    from aladyn_b200.beam import Bunch, bunch_records
+    from aladyn_b200.config import Grid, env_params, make_params, plasma
+    from aladyn_b200.sim import PicDevice
+    nx, ny, nz, nb = 512, 256, 256, 20_000_000
+    g = Grid(3, nx, ny, nz, 5.0, 2.5, 2.5, 0.8)
+    ncell = nx * ny * nz
+    p = make_params(g, precision=AGPU_FP64, capacity=(int(ncell * 4 * 1.04) + nb + 4096, 0, 0, 0), w_sh=10)
+    lx = nx * p.dx
+    b = Bunch(nb_tot=nb, charge_pc=200.0, sxb=5.0, syb=3.0, gam=1957.0, epsy=1.0, epsz=1.0, dg=1.0,
+              xc=p.xmn + 0.6 * lx, seed=77)
+    rec = bunch_records(p, b, n0_ref=0.1)
+    dev = PicDevice(p)
+    dev.env_enable(env_params(g, 0.8, 2))
+    dev.set_plasma_source(plasma(0, 2, 2, 1, -1, 0.25, x_start=p.gxmin, x_end=1.0e7, y_min=p.gymin, y_max=p.gymax,
+                                 z_min=p.gzmin, z_max=p.gzmax, jitter=0.5, seed=20241206))
+    dev.load_plasma(0)
+    rc = dev.beam_inject(0, rec, b.gam)
+    if rc != 0:
+        raise RuntimeError(f"agpu_beam_inject returned {rc}")
+    n = dev.count(0)
+    it = 0
+    for _ in range(warmup):
+        it += 1
+        dev.env_run(it * p.dt, it)
+    dev.set_profiling(True)
+    dev.reset_timers()
+    s = torch.cuda.ExternalStream(dev.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    dev.synchronize()
+    e0.record(s)
+    pushes = 0
+    for _ in range(steps):
+        it += 1
+        o = dev.env_run(it * p.dt, it)
+        pushes += o.np[0] + o.removed[0] - o.injected[0]
+    e1.record(s)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    tm = dev.timers()
+    dev.close()
+    return {"grid": [nx, ny, nz], "bunch_macroparticles": nb, "particles": int(n), "form": "fp64",
+            "route": "agpu_env_run (env_lpf2_evolve + window), envelope solver on a zero envelope",
+            "pushes_per_s": pushes / (ms * 1e-3), "ms_per_step": ms / steps,
+            "particle_kernels_ms_per_step": tm.ms_push_deposit / steps, "yee_ms_per_step": tm.ms_yee / steps,
+            "warmup": warmup, "steps": steps, "error_bits": int(o.error_bits)}
+
+
 def extra_scan(torch, warmup, steps):
     r = scan_measure(torch, warmup, steps, 0)
     return {"instances": r["n"], "warmup": warmup, "steps": steps,
@@ -740,17 +795,19 @@ def extra_accuracy(torch, steps=1000):
             "electrons": {k: int(v[1]) for k, v in f.items()}}
 
 
-def extras(torch, warmup):
+def extras(torch, warmup, only=None):
     k = 5
-    return {
-        "c1_2d": _guard(extra_forms, "lwfa2d_1024x256_ppc4", torch, warmup, 20, True),
-        "c2_cubic": _guard(extra_forms, "lwfa3d_1024x256x256_ppc8_cubic", torch, warmup, k),
-        "c3_pwfa": _guard(extra_pwfa, torch, warmup, k),
-        "c4_ionization": _guard(extra_ionization, torch, warmup, k),
-        "scan": _guard(extra_scan, torch, warmup, 10),
-        "continuity_residual": _guard(extra_continuity, torch),
-        "accuracy_1000_steps": _guard(extra_accuracy, torch),
+    todo = {
+        "c1_2d": (extra_forms, "lwfa2d_1024x256_ppc4", torch, warmup, 20, True),
+        "c2_cubic": (extra_forms, "lwfa3d_1024x256x256_ppc8_cubic", torch, warmup, k),
+        "c3_pwfa": (extra_pwfa, torch, warmup, k),
+        "c3_pwfa_envelope": (extra_pwfa_envelope, torch, warmup, k),
+        "c4_ionization": (extra_ionization, torch, warmup, k),
+        "scan": (extra_scan, torch, warmup, 10),
+        "continuity_residual": (extra_continuity, torch),
+        "accuracy_1000_steps": (extra_accuracy, torch),
     }
+    return {name: _guard(*job) for name, job in todo.items() if only is None or name == only}
 
 
 def bench_scan(a, torch):
@@ -792,8 +849,14 @@ def main(argv=None):
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-clocks", action="store_true", help="skip nvidia-smi sampling (profiler runs)")
     ap.add_argument("--no-extras", action="store_true", help="only the headline workload")
+    ap.add_argument("--extra", default=None, help="run one of the extra measurements alone and print it")
     a = ap.parse_args(argv)
     a.warmup = max(a.warmup, 3)
+    if a.extra:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps({a.extra: extras(torch, a.warmup, only=a.extra)[a.extra]}), flush=True)
+        return 0
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
