@@ -88,6 +88,7 @@ struct agpu_handle {
   double* env_av = nullptr;
   double* env_den = nullptr;
   agpu_env_params ep{};
+  long long env_steps = 0;  // env_run calls so far (the record sort period)
   // window state (lp_window_xshift saved variables)
   double xlapse = 0.0;
   int wi1 = 0;
@@ -1810,6 +1811,19 @@ int agpu_env_run(agpu_handle* h, int32_t iter, double t, agpu_step_out* out) {
   const int ic = 0;
   if (int rc = drop_removed(h, ic)) return rc;
   CK(cudaMemsetAsync(h->d_cnt, 0, sizeof(Counters), h->st));
+  // Every `every` calls the records move in memory along the tile
+  // permutation (tile, row inside the tile, offset octant): a warp then
+  // covers consecutive x cells of one tile row, so its stencil loads share
+  // cache lines and its FP64 atomics mostly hit different addresses.  Not in
+  // the deterministic mode, whose serial sums follow the particle order.
+  const int every = h->sort_interval > 0 ? h->sort_interval : 8;
+  if (!h->deterministic && h->key[ic] && h->np[ic] > 0 && h->env_steps % every == 0) {
+    ph_begin(h, PH_SORT);
+    if (int rc = rebin(h, ic)) return rc;
+    if (int rc = reorder_records(h, ic)) return rc;
+    ph_end(h, PH_SORT);
+  }
+  h->env_steps++;
   EnvArgs a;
   a.g = g;
   a.ebf = h->ebf;

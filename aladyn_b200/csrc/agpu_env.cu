@@ -17,6 +17,13 @@
 #include "agpu_env.h"
 #include "agpu_fp64_dep.cuh"
 
+#ifndef AGPU_ENV_ACC_MINB
+#define AGPU_ENV_ACC_MINB 1
+#endif
+#ifndef AGPU_ENV_POS_MINB
+#define AGPU_ENV_POS_MINB 1
+#endif
+
 namespace agpu {
 namespace {
 
@@ -94,7 +101,7 @@ __device__ __forceinline__ bool in_stencil(int lo, int n) { return lo >= 1 && lo
 // den.  The reference runs the three as separate sweeps with ebfp as
 // scratch; per particle the arithmetic is identical.
 template <bool SERIAL>
-__global__ void __launch_bounds__(256) k_env_acc(EnvArgs a) {
+__global__ void __launch_bounds__(256, AGPU_ENV_ACC_MINB) k_env_acc(EnvArgs a) {
   const Geo g = a.g;
   const long long stride = SERIAL ? 1 : (long long)gridDim.x * blockDim.x;
   const long long first = SERIAL ? 0 : blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -469,7 +476,7 @@ __global__ void k_env_update(double* env, double* av, Geo g, double k2_fact, dou
 // deposit (grid_part_connect.f90:956-1334) of the particles that stay, from
 // x^n to x^{n+1} with the packed weight (iform < 2).
 template <bool SERIAL>
-__global__ void __launch_bounds__(256) k_env_pos(EnvArgs a) {
+__global__ void __launch_bounds__(256, AGPU_ENV_POS_MINB) k_env_pos(EnvArgs a) {
   const Geo g = a.g;
   const long long stride = SERIAL ? 1 : (long long)gridDim.x * blockDim.x;
   const long long first = SERIAL ? 0 : blockIdx.x * (long long)blockDim.x + threadIdx.x;

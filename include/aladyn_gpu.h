@@ -331,7 +331,10 @@ int agpu_get_env_source(agpu_handle* h, double* av, int32_t n1p, int32_t n2p, in
 int agpu_init_envelope(agpu_handle* h, const agpu_lp_pulse* pulse, int32_t plane_wave);
 /* One call of env_run (src/dynamics/env_evolve_in_time.f90:363-391):
  * env_lpf2_evolve (196-361) for species 0 and, when mod(iter, w_sh) == 0
- * inside [wi_time, wf_time), lp_window_xshift, which shifts env as well. */
+ * inside [wi_time, wf_time), lp_window_xshift, which shifts env as well.
+ * Outside the deterministic mode the records of species 0 are moved in
+ * memory along the tile order every agpu_set_sort_interval steps (every 8
+ * calls when it is 0), which changes their order, not their values. */
 int agpu_env_run(agpu_handle* h, int32_t iter, double t, agpu_step_out* out);
 
 /* ---- PWFA bunch set-up ------------------------------------------------- */
