@@ -17,13 +17,6 @@
 #include "agpu_env.h"
 #include "agpu_fp64_dep.cuh"
 
-#ifndef AGPU_ENV_ACC_MINB
-#define AGPU_ENV_ACC_MINB 1
-#endif
-#ifndef AGPU_ENV_POS_MINB
-#define AGPU_ENV_POS_MINB 1
-#endif
-
 namespace agpu {
 namespace {
 
@@ -93,6 +86,102 @@ __global__ void k_env_grad(double* av, Geo g, double dxi, double dyi, double dzi
 
 __device__ __forceinline__ bool in_stencil(int lo, int n) { return lo >= 1 && lo + 2 <= n; }
 
+// The atomic-mode Esirkepov deposit of one 3D move: the terms of
+// esirkepov3d (grid_part_connect.f90:1168-1334) with every window loop
+// unrolled over its five slots, so the window arrays stay in registers, and
+// where the old-plane and new-plane terms of a component land on the same
+// node (the particle keeps its z node for Jx and Jy, its y node for Jz) the
+// two terms are summed before one atomic add instead of two.  The sums then
+// round differently from the reference's two adds (the serial mode keeps
+// esirkepov3d); the atomic mode's sum order is not the reference's anyway.
+__device__ __forceinline__ bool esirkepov3d_sum(const Geo& g, double* jc, const double xn[3], const double xo[3],
+                                                float wght) {
+  double ax0[3], ay0[3], az0[3], ax1[3], ay1[3], az1[3];
+  double axh[5], ayh[5], azh[5], axh0[5], axh1[5], ayh0[5], ayh1[5];
+  double currx[5], curry[5], currz[5];
+  const int ii0 = qden64(xo[0], ax0), jj0 = qden64(xo[1], ay0), kk0 = qden64(xo[2], az0);
+  const int i = qden64(xn[0], ax1), j = qden64(xn[1], ay1), k = qden64(xn[2], az1);
+  if ((unsigned)(i - ii0 + 1) > 2u || (unsigned)(j - jj0 + 1) > 2u || (unsigned)(k - kk0 + 1) > 2u) return false;
+  const double w = (double)wght;
+  const int ih = i - ii0 + 1, jh = j - jj0 + 1, kh = k - kk0 + 1;
+  esirk_1d(ax0, ax1, ih, axh, currx);
+  esirk_1d(ay0, ay1, jh, ayh, curry);
+  esirk_1d(az0, az1, kh, azh, currz);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    currx[q] = w * currx[q];
+    curry[q] = w * curry[q];
+    currz[q] = w * currz[q];
+    axh0[q] = 0.5 * axh[q];
+    axh1[q] = axh[q];
+    ayh0[q] = 0.5 * ayh[q];
+    ayh1[q] = ayh[q];
+  }
+#pragma unroll
+  for (int q = 1; q <= 3; ++q) {
+    axh0[q] = axh0[q] + ax0[q - 1];
+    axh1[q] = axh1[q] + 0.5 * ax0[q - 1];
+    ayh0[q] = ayh0[q] + ay0[q - 1];
+    ayh1[q] = ayh1[q] + 0.5 * ay0[q - 1];
+  }
+  const int x0 = ih < 1 ? ih : 1, x1 = (ih + 2) > 3 ? ih + 2 : 3;
+  const int y0 = jh < 1 ? jh : 1, y1 = (jh + 2) > 3 ? jh + 2 : 3;
+  const int z0 = kh < 1 ? kh : 1, z1 = (kh + 2) > 3 ? kh + 2 : 3;
+  const long long sy = g.n1p, sz = (long long)g.n1p * g.n2p;
+  // slot (i1, j1, k1) of the window of component c sits at base + i1 + sy j1 + sz k1
+  const long long bx0 = goff(g, ii0 - 2, jj0 - 2, kk0 - 1), bx1 = goff(g, ii0 - 2, jj0 - 2, k - 1);
+  const long long bz0 = goff(g, ii0 - 2, jj0 - 1, kk0 - 2), bz1 = goff(g, ii0 - 2, j - 1, kk0 - 2);
+  const bool samek = (k == kk0), samej = (j == jj0);
+  double* jx = jc;
+  double* jy = jc + g.ncell;
+  double* jz = jc + 2 * g.ncell;
+#pragma unroll
+  for (int k1 = 0; k1 <= 2; ++k1)
+#pragma unroll
+    for (int j1 = 0; j1 < 5; ++j1) {
+      if (j1 < y0 || j1 > y1) continue;
+      const double dvol = ayh0[j1] * az0[k1], dvolh = ayh1[j1] * az1[k1];
+      const double cvol = curry[j1] * az0[k1], cvolh = curry[j1] * az1[k1];
+#pragma unroll
+      for (int i1 = 0; i1 < 5; ++i1) {
+        if (i1 < x0 || i1 > x1) continue;
+        const long long o0 = bx0 + i1 + sy * j1 + sz * k1, o1 = bx1 + i1 + sy * j1 + sz * k1;
+        const double ax = dvol * currx[i1], bx = dvolh * currx[i1];
+        const double ay = axh0[i1] * cvol, by = axh1[i1] * cvolh;
+        if (samek) {
+          atomicAdd(&jx[o0], ax + bx);
+          atomicAdd(&jy[o0], ay + by);
+        } else {
+          atomicAdd(&jx[o0], ax);
+          atomicAdd(&jx[o1], bx);
+          atomicAdd(&jy[o0], ay);
+          atomicAdd(&jy[o1], by);
+        }
+      }
+    }
+#pragma unroll
+  for (int k1 = 0; k1 < 5; ++k1) {
+    if (k1 < z0 || k1 > z1) continue;
+#pragma unroll
+    for (int j1 = 0; j1 <= 2; ++j1) {
+      const double dvol = ay0[j1] * currz[k1], dvolh = ay1[j1] * currz[k1];
+#pragma unroll
+      for (int i1 = 0; i1 < 5; ++i1) {
+        if (i1 < x0 || i1 > x1) continue;
+        const long long o0 = bz0 + i1 + sy * j1 + sz * k1, o1 = bz1 + i1 + sy * j1 + sz * k1;
+        const double az = axh0[i1] * dvol, bz = axh1[i1] * dvolh;
+        if (samej) {
+          atomicAdd(&jz[o0], az + bz);
+        } else {
+          atomicAdd(&jz[o0], az);
+          atomicAdd(&jz[o1], bz);
+        }
+      }
+    }
+  }
+  return true;
+}
+
 // set_env_acc (src/particles/grid_part_connect.f90:414-615) ->
 // lpf_env_momenta (src/dynamics/boris_push.f90:170-223) ->
 // set_env_density (grid_part_connect.f90:884-952), per particle: the qqh
@@ -100,8 +189,8 @@ __device__ __forceinline__ bool in_stencil(int lo, int n) { return lo >= 1 && lo
 // rotation p^{n-1/2} -> p^{n+1/2}, and the qden deposit of wgh/gam_new into
 // den.  The reference runs the three as separate sweeps with ebfp as
 // scratch; per particle the arithmetic is identical.
-template <bool SERIAL>
-__global__ void __launch_bounds__(256, AGPU_ENV_ACC_MINB) k_env_acc(EnvArgs a) {
+template <bool SERIAL, int NDIM>
+__global__ void __launch_bounds__(256) k_env_acc(EnvArgs a) {
   const Geo g = a.g;
   const long long stride = SERIAL ? 1 : (long long)gridDim.x * blockDim.x;
   const long long first = SERIAL ? 0 : blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -121,7 +210,7 @@ __global__ void __launch_bounds__(256, AGPU_ENV_ACC_MINB) k_env_acc(EnvArgs a) {
     const double yl = a.dy_inv * (a.y[n] - a.ymn);
     qqh64(xl, ax1, axh1, &i, &ih);
     qqh64(yl, ay1, ayh1, &j, &jh);
-    if (g.ndim == 2) {
+    if (NDIM == 2) {
       if (!in_stencil(i, g.n1p) || !in_stencil(ih, g.n1p) || !in_stencil(j, g.n2p) || !in_stencil(jh, g.n2p)) {
         raise_err(a.err, AGPU_EBIT_INDEX);
         continue;
@@ -475,8 +564,8 @@ __global__ void k_env_update(double* env, double* av, Geo g, double k2_fact, dou
 // cell_part_dist(.false.) (mpi_part_interface.f90:467-523) -> Esirkepov
 // deposit (grid_part_connect.f90:956-1334) of the particles that stay, from
 // x^n to x^{n+1} with the packed weight (iform < 2).
-template <bool SERIAL>
-__global__ void __launch_bounds__(256, AGPU_ENV_POS_MINB) k_env_pos(EnvArgs a) {
+template <bool SERIAL, int NDIM>
+__global__ void __launch_bounds__(256) k_env_pos(EnvArgs a) {
   const Geo g = a.g;
   const long long stride = SERIAL ? 1 : (long long)gridDim.x * blockDim.x;
   const long long first = SERIAL ? 0 : blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -493,7 +582,7 @@ __global__ void __launch_bounds__(256, AGPU_ENV_POS_MINB) k_env_pos(EnvArgs a) {
     qqh64(xl, ax1, axh1, &i, &ih);
     qqh64(yl, ay1, ayh1, &j, &jh);
     const float wght = (float)slot_charge(dbits(a.slot[n])) * slot_wgh(dbits(a.slot[n]));
-    if (g.ndim == 2) {
+    if (NDIM == 2) {
       if (!in_stencil(i, g.n1p) || !in_stencil(ih, g.n1p) || !in_stencil(j, g.n2p) || !in_stencil(jh, g.n2p)) {
         raise_err(a.err, AGPU_EBIT_INDEX);
         a.flag[n] = 1;
@@ -601,7 +690,8 @@ __global__ void __launch_bounds__(256, AGPU_ENV_POS_MINB) k_env_pos(EnvArgs a) {
     }
     const double xo[3] = {xl, yl, zl};
     const double xnl[3] = {a.dx_inv * (xn - a.xmn), a.dy_inv * (yn - a.ymn), a.dz_inv * (zn - a.zmn)};
-    if (!esirkepov3d<SERIAL>(g, a.jc, xnl, xo, wght)) raise_err(a.err, AGPU_EBIT_INDEX);
+    const bool dep_ok = SERIAL ? esirkepov3d<true>(g, a.jc, xnl, xo, wght) : esirkepov3d_sum(g, a.jc, xnl, xo, wght);
+    if (!dep_ok) raise_err(a.err, AGPU_EBIT_INDEX);
   }
 }
 
@@ -686,10 +776,14 @@ void env_amp_grad(const EnvArgs& a, cudaStream_t st, int sms) {
 
 void env_acc_momenta(const EnvArgs& a, cudaStream_t st, int sms, bool serial) {
   if (a.np <= 0) return;
-  if (serial)
-    k_env_acc<true><<<1, 1, 0, st>>>(a);
-  else
-    k_env_acc<false><<<grid_for(a.np, 256, sms, 8), 256, 0, st>>>(a);
+  const int nb = grid_for(a.np, 256, sms, 8);
+  if (a.g.ndim == 3) {
+    if (serial) k_env_acc<true, 3><<<1, 1, 0, st>>>(a);
+    else k_env_acc<false, 3><<<nb, 256, 0, st>>>(a);
+  } else {
+    if (serial) k_env_acc<true, 2><<<1, 1, 0, st>>>(a);
+    else k_env_acc<false, 2><<<nb, 256, 0, st>>>(a);
+  }
 }
 
 void env_den_collect(const EnvArgs& a, cudaStream_t st, int sms) {
@@ -740,10 +834,14 @@ void env_advance(const EnvArgs& a, cudaStream_t st, int sms) {
 
 void env_positions_deposit(const EnvArgs& a, cudaStream_t st, int sms, bool serial) {
   if (a.np <= 0) return;
-  if (serial)
-    k_env_pos<true><<<1, 1, 0, st>>>(a);
-  else
-    k_env_pos<false><<<grid_for(a.np, 256, sms, 8), 256, 0, st>>>(a);
+  const int nb = grid_for(a.np, 256, sms, 8);
+  if (a.g.ndim == 3) {
+    if (serial) k_env_pos<true, 3><<<1, 1, 0, st>>>(a);
+    else k_env_pos<false, 3><<<nb, 256, 0, st>>>(a);
+  } else {
+    if (serial) k_env_pos<true, 2><<<1, 1, 0, st>>>(a);
+    else k_env_pos<false, 2><<<nb, 256, 0, st>>>(a);
+  }
 }
 
 void env_init_pulse(const EnvPulseArgs& a, double* env, const Geo& g, cudaStream_t st, int sms) {

@@ -671,7 +671,7 @@ def extra_pwfa(torch, warmup, steps):
             "error_bits": int(o.error_bits)}
 
 
-def extra_pwfa_envelope(torch, warmup, steps):
+def extra_pwfa_envelope(torch, warmup, steps, nx=512, ny=256, nz=256, nb=20_000_000):
     """The reference's own PWFA route (Env_cycle: beam_inject, then env_run
     every step; model_id = 4 with a0 = 0 as its PWFA example): FP64 form,
     the 512x256x256 PWFA box and bunch of ``extra_pwfa``, der_ord 2, the
@@ -681,22 +681,22 @@ def extra_pwfa_envelope(torch, warmup, steps):
     from aladyn_b200.beam import Bunch, bunch_records
     from aladyn_b200.config import Grid, env_params, make_params, plasma
     from aladyn_b200.sim import PicDevice
-    nx, ny, nz, nb = 512, 256, 256, 20_000_000
     g = Grid(3, nx, ny, nz, 5.0, 2.5, 2.5, 0.8)
     ncell = nx * ny * nz
     p = make_params(g, precision=AGPU_FP64, capacity=(int(ncell * 4 * 1.04) + nb + 4096, 0, 0, 0), w_sh=10)
     lx = nx * p.dx
-    b = Bunch(nb_tot=nb, charge_pc=200.0, sxb=5.0, syb=3.0, gam=1957.0, epsy=1.0, epsz=1.0, dg=1.0,
+    b = Bunch(nb_tot=max(nb, 1), charge_pc=200.0, sxb=5.0, syb=3.0, gam=1957.0, epsy=1.0, epsz=1.0, dg=1.0,
               xc=p.xmn + 0.6 * lx, seed=77)
-    rec = bunch_records(p, b, n0_ref=0.1)
+    rec = bunch_records(p, b, n0_ref=0.1) if nb > 0 else None
     dev = PicDevice(p)
     dev.env_enable(env_params(g, 0.8, 2))
     dev.set_plasma_source(plasma(0, 2, 2, 1, -1, 0.25, x_start=p.gxmin, x_end=1.0e7, y_min=p.gymin, y_max=p.gymax,
                                  z_min=p.gzmin, z_max=p.gzmax, jitter=0.5, seed=20241206))
     dev.load_plasma(0)
-    rc = dev.beam_inject(0, rec, b.gam)
-    if rc != 0:
-        raise RuntimeError(f"agpu_beam_inject returned {rc}")
+    if rec is not None:
+        rc = dev.beam_inject(0, rec, b.gam)
+        if rc != 0:
+            raise RuntimeError(f"agpu_beam_inject returned {rc}")
     n = dev.count(0)
     it = 0
     for _ in range(warmup):
@@ -807,6 +807,12 @@ def extras(torch, warmup, only=None):
         "continuity_residual": (extra_continuity, torch),
         "accuracy_1000_steps": (extra_accuracy, torch),
     }
+    # small cases for profiler captures, run only when named
+    captures = {
+        "pwfa_envelope_192x96x96_plasma": (extra_pwfa_envelope, torch, warmup, 3, 192, 96, 96, 0),
+    }
+    if only in captures:
+        return {only: _guard(*captures[only])}
     return {name: _guard(*job) for name, job in todo.items() if only is None or name == only}
 
 
