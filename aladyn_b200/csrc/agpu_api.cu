@@ -2060,8 +2060,9 @@ int agpu_diag(agpu_handle* h, agpu_diag_out* out) {
   if (!h || !out) return AGPU_E_ARG;
   std::memset(out, 0, sizeof(*out));
   // removed records of a binned species stay stored until the next
-  // compaction: the particle sums run over the alive ones along the tile
-  // permutation instead of compacting (a full copy and a rebinning)
+  // compaction: the particle sums leave them out (by their binning key in the
+  // split form, in memory order; along the tile permutation in the FP64
+  // form) instead of compacting (a full copy and a rebinning)
   if (int rc = refresh_counts(h)) return rc;
   CK(cudaMemsetAsync(h->d_diag, 0, sizeof(double) * 64, h->st));
   double dvol = h->p.dx * h->p.dy * (h->p.ndim == 3 ? h->p.dz : 1.0);
@@ -2077,7 +2078,8 @@ int agpu_diag(agpu_handle* h, agpu_diag_out* out) {
     const long long n = along ? h->nalive[ic] : h->np[ic];
     nd_alive[ic] = n;
     if (h->fp32)
-      part_diag32(h->sp[ic].view(), n, h->p.ndim, perm, o, h->st, h->sms);
+      part_diag32(h->sp[ic].view(), along ? h->np[ic] : n, h->p.ndim, along ? h->key[ic] : nullptr, h->tg.nkeys, o,
+                  h->st, h->sms);
     else
       part_diag64(h->part[ic], h->cap[ic], n, h->p.ndim, perm, o, h->st, h->sms);
   }

@@ -585,41 +585,39 @@ __device__ __forceinline__ void diag_terms32(float px, float py, float pz, uint6
   a[3] += (double)(w * py);
   a[4] += (double)(w * pz);
 }
-__global__ void k_part_diag32(Part32View p, long long n, int nd, const int* perm, double* out) {
+// Records 0..n-1 in memory order, four at a time with 16-byte loads (the
+// arrays are allocation-aligned), the last n % 4 one by one; with a key
+// array, the records whose binning key is `dead` (removed at a box edge,
+// still stored until the next compaction) are left out.
+__global__ void k_part_diag32(Part32View p, long long n, int nd, const int* key, int dead, double* out) {
   double a[5] = {0, 0, 0, 0, 0};
-  if (perm) {
-    for (long long qq = blockIdx.x * (long long)blockDim.x + threadIdx.x; qq < n; qq += (long long)gridDim.x * blockDim.x) {
-      const long long q = perm[qq];
-      diag_terms32(p.px[q], p.py[q], (nd == 3) ? p.pz[q] : 0.f, p.slot[q], a);
-    }
-  } else {
-    // records 0..n-1 four at a time with 16-byte loads (the arrays are
-    // allocation-aligned), the last n % 4 one by one
-    const long long n4 = n >> 2;
-    const float4* px4 = reinterpret_cast<const float4*>(p.px);
-    const float4* py4 = reinterpret_cast<const float4*>(p.py);
-    const float4* pz4 = reinterpret_cast<const float4*>(p.pz);
-    const ulonglong2* sl2 = reinterpret_cast<const ulonglong2*>(p.slot);
-    for (long long g4 = blockIdx.x * (long long)blockDim.x + threadIdx.x; g4 < n4; g4 += (long long)gridDim.x * blockDim.x) {
-      const float4 x = px4[g4], y = py4[g4];
-      const float4 z = (nd == 3) ? pz4[g4] : make_float4(0.f, 0.f, 0.f, 0.f);
-      const ulonglong2 s0 = sl2[2 * g4], s1 = sl2[2 * g4 + 1];
-      diag_terms32(x.x, y.x, z.x, s0.x, a);
-      diag_terms32(x.y, y.y, z.y, s0.y, a);
-      diag_terms32(x.z, y.z, z.z, s1.x, a);
-      diag_terms32(x.w, y.w, z.w, s1.y, a);
-    }
-    const long long q = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (q < n) diag_terms32(p.px[q], p.py[q], (nd == 3) ? p.pz[q] : 0.f, p.slot[q], a);
+  const long long n4 = n >> 2;
+  const float4* px4 = reinterpret_cast<const float4*>(p.px);
+  const float4* py4 = reinterpret_cast<const float4*>(p.py);
+  const float4* pz4 = reinterpret_cast<const float4*>(p.pz);
+  const ulonglong2* sl2 = reinterpret_cast<const ulonglong2*>(p.slot);
+  const int4* key4 = reinterpret_cast<const int4*>(key);
+  for (long long g4 = blockIdx.x * (long long)blockDim.x + threadIdx.x; g4 < n4; g4 += (long long)gridDim.x * blockDim.x) {
+    const float4 x = px4[g4], y = py4[g4];
+    const float4 z = (nd == 3) ? pz4[g4] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const ulonglong2 s0 = sl2[2 * g4], s1 = sl2[2 * g4 + 1];
+    const int4 kk = key ? key4[g4] : make_int4(0, 0, 0, 0);
+    if (!key || kk.x != dead) diag_terms32(x.x, y.x, z.x, s0.x, a);
+    if (!key || kk.y != dead) diag_terms32(x.y, y.y, z.y, s0.y, a);
+    if (!key || kk.z != dead) diag_terms32(x.z, y.z, z.z, s1.x, a);
+    if (!key || kk.w != dead) diag_terms32(x.w, y.w, z.w, s1.y, a);
   }
+  const long long q = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q < n && (!key || key[q] != dead)) diag_terms32(p.px[q], p.py[q], (nd == 3) ? p.pz[q] : 0.f, p.slot[q], a);
   for (int c = 0; c < 5; ++c) {
     double v = warp_sum(a[c]);
     if ((threadIdx.x & 31) == 0) atomicAdd(&out[c], v);
   }
 }
-void part_diag32(const Part32View& p, long long n, int nd, const int* perm, double* out, cudaStream_t st, int sms) {
+void part_diag32(const Part32View& p, long long n, int nd, const int* key, int dead, double* out, cudaStream_t st,
+                 int sms) {
   if (n <= 0) return;
-  k_part_diag32<<<grid_for(perm ? n : (n + 3) / 4, 256, sms, 16), 256, 0, st>>>(p, n, nd, perm, out);
+  k_part_diag32<<<grid_for((n + 3) / 4, 256, sms, 16), 256, 0, st>>>(p, n, nd, key, dead, out);
 }
 
 // max of a non-negative FP64 array (ion |E|^2), for the lp_max refresh.

@@ -79,7 +79,9 @@ void field_diag32(const float* ebf, const Geo& g, double dvol, double* out_e, do
 // perm: null (records 0..n-1) or the alive records perm[0..n-1]
 void part_diag64(const double* part, long long ld, long long n, int nd, const int* perm, double* out, cudaStream_t st,
                  int sms);
-void part_diag32(const Part32View& p, long long n, int nd, const int* perm, double* out, cudaStream_t st, int sms);
+// key: null (every record) or the binning keys, records keyed `dead` skipped
+void part_diag32(const Part32View& p, long long n, int nd, const int* key, int dead, double* out, cudaStream_t st,
+                 int sms);
 // Envar reductions (agpu_envar.cu): per species into d_out[0..16+AGPU_NE)
 // (ek(1:7), ekmax, psig(1:3), nde(1:ne) at 16..), fields into d_out[0..13)
 void envar_species(const double* part, long long ld, const Part32View* sp, const int* perm, long long n, const Geo& g,
