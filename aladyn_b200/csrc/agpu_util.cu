@@ -488,8 +488,11 @@ __device__ __forceinline__ void atomic_max_nonneg(double* a, double v) {
 
 // One warp per interior x-row (j, k), the lanes along x: coalesced reads and
 // no per-cell index division.
-template <typename T>
-__global__ void k_field_diag(const T* ebf, Geo g, int nf, double dvol, double* out_e, double* out_max) {
+// NFC field components (3 in 2D, 6 in 3D) as a template argument, so the
+// component loops unroll and the per-lane sums stay in registers.
+template <typename T, int NFC>
+__global__ void k_field_diag(const T* ebf, Geo g, double dvol, double* out_e, double* out_max) {
+  constexpr int nf = NFC;
   const int nx = g.ix2 - g.ix1 + 1, ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
   const long long nrows = (long long)ny * nz;
   double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -502,8 +505,10 @@ __global__ void k_field_diag(const T* ebf, Geo g, int nf, double dvol, double* o
     const int j = g.jy1 + (int)(r % ny), k = g.kz1 + (int)(r / ny);
     const long long o0 = goff(g, g.ix1, j, k);
     if (sizeof(T) == 8) {
+#pragma unroll 4
       for (int i = lane; i < nx; i += 32) {
         const long long o = o0 + i;
+#pragma unroll
         for (int c = 0; c < nf; ++c) {
           double v = (double)ebf[g.ncell * c + o];
           acc[c] += v * v;
@@ -515,18 +520,22 @@ __global__ void k_field_diag(const T* ebf, Geo g, int nf, double dvol, double* o
       // words are FP32), the row partial added in FP64
       float rs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       float rm = 0.f;
+#pragma unroll 4
       for (int i = lane; i < nx; i += 32) {
         const long long o = o0 + i;
+#pragma unroll
         for (int c = 0; c < nf; ++c) {
           const float v = (float)ebf[g.ncell * c + o];
           rs[c] = fmaf(v, v, rs[c]);
           if (c < ne) rm = fmaxf(rm, fabsf(v));
         }
       }
+#pragma unroll
       for (int c = 0; c < nf; ++c) acc[c] += (double)rs[c];
       mx = fmax(mx, (double)rm);
     }
   }
+#pragma unroll
   for (int c = 0; c < nf; ++c) {
     double v = warp_sum(acc[c]);
     if ((threadIdx.x & 31) == 0) atomicAdd(&out_e[c], v * dvol);
@@ -536,11 +545,17 @@ __global__ void k_field_diag(const T* ebf, Geo g, int nf, double dvol, double* o
 }
 void field_diag64(const double* ebf, const Geo& g, double dvol, double* out_e, double* out_max, cudaStream_t st, int sms) {
   long long cells = (long long)(g.ix2 - g.ix1 + 1) * (g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1);
-  k_field_diag<double><<<grid_for(cells / 8, 256, sms, 16), 256, 0, st>>>(ebf, g, g.nf, dvol, out_e, out_max);
+  if (g.nf == 6)
+    k_field_diag<double, 6><<<grid_for(cells / 8, 256, sms, 16), 256, 0, st>>>(ebf, g, dvol, out_e, out_max);
+  else
+    k_field_diag<double, 3><<<grid_for(cells / 8, 256, sms, 16), 256, 0, st>>>(ebf, g, dvol, out_e, out_max);
 }
 void field_diag32(const float* ebf, const Geo& g, double dvol, double* out_e, double* out_max, cudaStream_t st, int sms) {
   long long cells = (long long)(g.ix2 - g.ix1 + 1) * (g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1);
-  k_field_diag<float><<<grid_for(cells / 8, 256, sms, 16), 256, 0, st>>>(ebf, g, g.nf, dvol, out_e, out_max);
+  if (g.nf == 6)
+    k_field_diag<float, 6><<<grid_for(cells / 8, 256, sms, 16), 256, 0, st>>>(ebf, g, dvol, out_e, out_max);
+  else
+    k_field_diag<float, 3><<<grid_for(cells / 8, 256, sms, 16), 256, 0, st>>>(ebf, g, dvol, out_e, out_max);
 }
 
 // out[0] = sum w (gamma-1), out[1] = sum charge*w, out[2..4] = sum w p over
