@@ -50,7 +50,7 @@ def make_params(grid: Grid, *, precision: int = AGPU_FP64, nsp: int = 1, nsp_run
                 w_sh: int = 10, w_speed: float = 1.0, wi_time: float = 0.0,
                 wf_time: float = 1.0e9, capacity=(0, 0, 0, 0), der_ord: int = 2,
                 mass_number=(1.0, 1.0, 1.0), ionz_lev: int = 0, n_mol_atoms=(1, 1, 1, 1),
-                seed: int = 12345, shape: int = 0) -> AgpuParams:
+                seed: int = 12345, shape: int = 0, iform: int = 0) -> AgpuParams:
     p = AgpuParams()
     ndim = grid.ndim
     p.ndim = ndim
@@ -59,7 +59,7 @@ def make_params(grid: Grid, *, precision: int = AGPU_FP64, nsp: int = 1, nsp_run
     p.nfield = 6 if ndim == 3 else 3
     p.curr_ndim = 3 if ndim == 3 else 2
     p.ibx = p.iby = p.ibz = 0
-    p.iform = 0
+    p.iform = iform  # 0, 1: charge-conserving Esirkepov deposit; 2: ncdef (FP64 form)
     p.precision = precision
     p.nsp = nsp
     p.nsp_run = nsp_run

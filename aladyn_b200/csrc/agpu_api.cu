@@ -173,9 +173,10 @@ YeeC yee_coef(const agpu_params& p) {
   c.se1 = p.se_coeff[0];
   c.se2 = p.se_coeff[1];
   c.ompe = p.ompe;
-  c.djc1 = p.djc[0];
-  c.djc2 = p.djc[1];
-  c.djc3 = p.djc[2];
+  // curr_mpi_collect scales the currents by djc only when iform < 2
+  c.djc1 = p.iform < 2 ? p.djc[0] : 1.0;
+  c.djc2 = p.iform < 2 ? p.djc[1] : 1.0;
+  c.djc3 = p.iform < 2 ? p.djc[2] : 1.0;
   return c;
 }
 
@@ -405,7 +406,7 @@ int compact_species(agpu_handle* h, int ic, bool window) {
 // FP64 form runs the per-particle kernels.
 bool tiled(const agpu_handle* h, int ic) {
   return !h->deterministic && ic < h->p.nsp_run && h->key[ic] != nullptr &&
-         (h->fp32 || h->p.shape == AGPU_SHAPE_QUADRATIC);
+         (h->fp32 || (h->p.shape == AGPU_SHAPE_QUADRATIC && h->p.iform < 2));
 }
 
 // Keys from the current positions, histogram, scan and permutation.
@@ -876,7 +877,9 @@ int agpu_create(const agpu_params* params, agpu_handle** out) {
   if (!(p.ndim == 2 || p.ndim == 3)) return AGPU_E_ARG;
   if (p.nx < 4 || p.ny < 4 || (p.ndim == 3 && p.nz < 4)) return AGPU_E_ARG;
   if (p.nfield != (p.ndim == 3 ? 6 : 3) || p.curr_ndim != (p.ndim == 3 ? 3 : 2)) return AGPU_E_ARG;
-  if (p.ibx != 0 || p.iby != 0 || p.ibz != 0 || p.iform < 0 || p.iform > 1) return AGPU_E_ARG;
+  if (p.ibx != 0 || p.iby != 0 || p.ibz != 0 || p.iform < 0 || p.iform > 2) return AGPU_E_ARG;
+  // iform = 2 (the non-conserving deposit) in the FP64 form, quadratic shapes
+  if (p.iform == 2 && (p.precision != AGPU_FP64 || p.shape != AGPU_SHAPE_QUADRATIC)) return AGPU_E_ARG;
   if (p.nsp < 1 || p.nsp > 4 || p.nsp_run < 1 || p.nsp_run > p.nsp) return AGPU_E_ARG;
   if (p.precision != AGPU_FP64 && p.precision != AGPU_FP32_SPLIT) return AGPU_E_ARG;
   if (p.shape != AGPU_SHAPE_QUADRATIC && p.shape != AGPU_SHAPE_CUBIC) return AGPU_E_ARG;
@@ -1615,6 +1618,7 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
       a.gzmax = p.gzmax;
       a.initial = initial_time ? 1 : 0;
       a.shape = p.shape;
+      a.iform = p.iform;
       a.removed = &h->d_cnt->removed;
       a.err = &h->d_cnt->err;
       push_deposit64(a, h->st, h->sms, h->deterministic);

@@ -624,6 +624,11 @@ __global__ void __launch_bounds__(256) k_env_pos(EnvArgs a) {
         atomicAdd(a.removed, 1ull);
         continue;
       }
+      if (a.iform == 2) {
+        ncdef2d<SERIAL>(g, a.jc, a.dx_inv * (xn - a.xmn), a.dy_inv * (yn - a.ymn), xl, yl, pp1, pp2, wght,
+                        dt_lp * gam_inv);
+        continue;
+      }
       if (!esirkepov2d<SERIAL>(g, a.jc, a.dx_inv * (xn - a.xmn), a.dy_inv * (yn - a.ymn), xl, yl, wght))
         raise_err(a.err, AGPU_EBIT_INDEX);
       continue;
@@ -690,6 +695,10 @@ __global__ void __launch_bounds__(256) k_env_pos(EnvArgs a) {
     }
     const double xo[3] = {xl, yl, zl};
     const double xnl[3] = {a.dx_inv * (xn - a.xmn), a.dy_inv * (yn - a.ymn), a.dz_inv * (zn - a.zmn)};
+    if (a.iform == 2) {
+      ncdef3d<SERIAL>(g, a.jc, xnl, xo, pp, wght, dt_lp * gam_inv);
+      continue;
+    }
     const bool dep_ok = SERIAL ? esirkepov3d<true>(g, a.jc, xnl, xo, wght) : esirkepov3d_sum(g, a.jc, xnl, xo, wght);
     if (!dep_ok) raise_err(a.err, AGPU_EBIT_INDEX);
   }

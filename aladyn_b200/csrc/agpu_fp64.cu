@@ -336,6 +336,10 @@ __global__ void __launch_bounds__(256) k64_push_dep_3d(PushArgs64 a) {
     }
     double xn[3] = {a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn), a.dz_inv * (znew - a.zmn)};
     float wght = (float)slot_charge(sl) * slot_wgh(sl);
+    if (SHAPE != AGPU_SHAPE_CUBIC && a.iform == 2) {
+      ncdef3d<SERIAL>(g, a.jc, xn, xo, pn, wght, dtg);
+      continue;
+    }
     const bool dep_ok = (SHAPE == AGPU_SHAPE_CUBIC) ? esirkepov_cubic64<SERIAL>(g, a.jc, xn, xo, wght, 3)
                                                    : esirkepov3d<SERIAL>(g, a.jc, xn, xo, wght);
     if (!dep_ok) raise_err(a.err, AGPU_EBIT_INDEX);
@@ -449,6 +453,10 @@ __global__ void __launch_bounds__(256) k64_push_dep_2d(PushArgs64 a) {
       continue;
     }
     float wght = (float)slot_charge(sl) * slot_wgh(sl);
+    if (SHAPE != AGPU_SHAPE_CUBIC && a.iform == 2) {
+      ncdef2d<SERIAL>(g, a.jc, a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn), xl, yl, pn1, pn2, wght, dtg);
+      continue;
+    }
     bool dep_ok;
     if (SHAPE == AGPU_SHAPE_CUBIC) {
       const double xn2[2] = {a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn)}, xo2[2] = {xl, yl};

@@ -231,4 +231,84 @@ __device__ __forceinline__ bool esirkepov3d(const Geo& g, double* jc, const doub
   return true;
 }
 
+// ============================================================================
+// iform = 2: the non-conserving deposit ncdef_2d_curr / ncdef_3d_curr
+// (grid_part_connect.f90:1338-1512): half the particle's q w dt v on the qlh
+// shapes at the old and at the new position (xn, xo local).  q w dt / gamma
+// as the reference forms it from the push's dt / gamma (ebfp(ch), kept when
+// iform = 2); p the momenta at t^{n+1/2}.
+// ============================================================================
+template <bool SERIAL>
+__device__ __forceinline__ void ncdef3d(const Geo& g, double* jc, const double xn[3], const double xo[3],
+                                        const double p[3], float wght, double dtg) {
+  double ax0[3], ay0[3], az0[3], axh0[2], ayh0[2], azh0[2];
+  double ax1[3], ay1[3], az1[3], axh1[2], ayh1[2], azh1[2];
+  const double gam_inv = (double)wght * dtg;
+  double vp[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) vp[c] = 0.5 * gam_inv * p[c];
+  const int ii0 = qlh64(xo[0], ax0, axh0), jj0 = qlh64(xo[1], ay0, ayh0), kk0 = qlh64(xo[2], az0, azh0);
+  const int i = qlh64(xn[0], ax1, axh1), j = qlh64(xn[1], ay1, ayh1), k = qlh64(xn[2], az1, azh1);
+  const int ih0 = ii0, jh0 = jj0, kh0 = kk0, ih = i, jh = j, kh = k;
+  double* jx = jc;
+  double* jy = jc + g.ncell;
+  double* jz = jc + 2 * g.ncell;
+  for (int k1 = 0; k1 <= 2; ++k1) {
+    for (int j1 = 0; j1 <= 2; ++j1) {
+      const double dvol = vp[0] * ay1[j1] * az1[k1];
+      for (int i1 = 0; i1 <= 1; ++i1) jadd<SERIAL>(&jx[goff(g, ih + i1, j + j1, k + k1)], dvol * axh1[i1]);
+    }
+    for (int j1 = 0; j1 <= 2; ++j1) {
+      const double dvol = vp[0] * ay0[j1] * az0[k1];
+      for (int i1 = 0; i1 <= 1; ++i1) jadd<SERIAL>(&jx[goff(g, ih0 + i1, jj0 + j1, kk0 + k1)], dvol * axh0[i1]);
+    }
+  }
+  for (int k1 = 0; k1 <= 2; ++k1) {
+    for (int j1 = 0; j1 <= 1; ++j1) {
+      const double dvol = vp[1] * ayh0[j1] * az0[k1];
+      for (int i1 = 0; i1 <= 2; ++i1) jadd<SERIAL>(&jy[goff(g, ii0 + i1, jh0 + j1, kk0 + k1)], dvol * ax0[i1]);
+    }
+    for (int j1 = 0; j1 <= 1; ++j1) {
+      const double dvol = vp[1] * ayh1[j1] * az1[k1];
+      for (int i1 = 0; i1 <= 2; ++i1) jadd<SERIAL>(&jy[goff(g, i + i1, jh + j1, k + k1)], dvol * ax1[i1]);
+    }
+  }
+  for (int k1 = 0; k1 <= 1; ++k1) {
+    for (int j1 = 0; j1 <= 2; ++j1) {
+      const double dvol = vp[2] * ay0[j1] * azh0[k1];
+      for (int i1 = 0; i1 <= 2; ++i1) jadd<SERIAL>(&jz[goff(g, ii0 + i1, jj0 + j1, kh0 + k1)], dvol * ax0[i1]);
+    }
+    for (int j1 = 0; j1 <= 2; ++j1) {
+      const double dvol = vp[2] * ay1[j1] * azh1[k1];
+      for (int i1 = 0; i1 <= 2; ++i1) jadd<SERIAL>(&jz[goff(g, i + i1, j + j1, kh + k1)], dvol * ax1[i1]);
+    }
+  }
+}
+
+template <bool SERIAL>
+__device__ __forceinline__ void ncdef2d(const Geo& g, double* jc, double xn, double yn, double xo, double yo, double p1,
+                                        double p2, float wght, double dtg) {
+  double ax0[3], ay0[3], axh0[2], ayh0[2], ax1[3], ay1[3], axh1[2], ayh1[2];
+  double vp1 = (double)wght * dtg * p1, vp2 = (double)wght * dtg * p2;
+  vp1 = 0.5 * vp1;
+  vp2 = 0.5 * vp2;
+  const int ii0 = qlh64(xo, ax0, axh0), jj0 = qlh64(yo, ay0, ayh0);
+  const int i = qlh64(xn, ax1, axh1), j = qlh64(yn, ay1, ayh1);
+  const int ih0 = ii0, jh0 = jj0, ih = i, jh = j;
+  double* jx = jc;
+  double* jy = jc + g.ncell;
+  for (int j1 = 0; j1 <= 2; ++j1) {
+    double dvol = vp1 * ay1[j1];
+    for (int i1 = 0; i1 <= 1; ++i1) jadd<SERIAL>(&jx[goff(g, ih + i1, j + j1, 1)], dvol * axh1[i1]);
+    dvol = vp1 * ay0[j1];
+    for (int i1 = 0; i1 <= 1; ++i1) jadd<SERIAL>(&jx[goff(g, ih0 + i1, jj0 + j1, 1)], dvol * axh0[i1]);
+  }
+  for (int j1 = 0; j1 <= 1; ++j1) {
+    double dvol = vp2 * ayh0[j1];
+    for (int i1 = 0; i1 <= 2; ++i1) jadd<SERIAL>(&jy[goff(g, ii0 + i1, jh0 + j1, 1)], dvol * ax0[i1]);
+    dvol = vp2 * ayh1[j1];
+    for (int i1 = 0; i1 <= 2; ++i1) jadd<SERIAL>(&jy[goff(g, i + i1, jh + j1, 1)], dvol * ax1[i1]);
+  }
+}
+
 }  // namespace agpu

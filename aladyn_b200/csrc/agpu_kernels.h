@@ -36,6 +36,7 @@ struct PushArgs64 {
   double gxmin, gxmax, gymin, gymax, gzmin, gzmax;
   int initial;
   int shape;  // AGPU_SHAPE_QUADRATIC or AGPU_SHAPE_CUBIC
+  int iform;  // 0, 1: Esirkepov; 2: the non-conserving ncdef deposit
   unsigned long long* removed;
   unsigned int* err;
 };

@@ -84,7 +84,9 @@ typedef struct agpu_params {
   int32_t nfield;          /* 3 in 2D (Ex,Ey,Bz), 6 in 3D (Ex,Ey,Ez,Bx,By,Bz)    */
   int32_t curr_ndim;       /* 2 in 2D, 3 in 3D                                    */
   int32_t ibx, iby, ibz;   /* boundary codes; 0 (open) is the supported value     */
-  int32_t iform;           /* 0 or 1: Esirkepov deposition                        */
+  int32_t iform;           /* 0, 1: Esirkepov deposition; 2: the non-conserving
+                              ncdef deposit (grid_part_connect.f90:1338-1512),
+                              FP64 form with quadratic shapes only             */
   int32_t precision;       /* AGPU_FP64 or AGPU_FP32_SPLIT                        */
   int32_t nsp;             /* species count, 1..4; species 0 are electrons        */
   int32_t nsp_run;         /* species that move (1 in the wake regime)            */

@@ -949,6 +949,88 @@ static void ora_esirkepov_cubic_3d_one(ora_sim* s, double* jc, const double xp1[
       }
 }
 
+/* iform = 2: ncdef_2d_curr / ncdef_3d_curr (grid_part_connect.f90:1338-1512):
+   half of q w dt v (dt / gamma = the push's ebfp(ch), kept when iform = 2) on
+   the qlh shapes at the old and at the new position. */
+static void ora_ncdef_3d_one(ora_sim* s, double* jc, const double xp1[3], const double xp0[3], const double pv[3],
+                             float wght, double dtg) {
+  double ax0[3], ay0[3], az0[3], axh0[2], ayh0[2], azh0[2];
+  double ax1[3], ay1[3], az1[3], axh1[2], ayh1[2], azh1[2];
+  int ii0, jj0, kk0, i, j, k;
+  const double gam_inv = (double)wght * dtg;
+  double vp[3];
+  for (int c = 0; c < 3; ++c) vp[c] = 0.5 * gam_inv * pv[c];
+  ora_qlh_1d(xp0[0], ax0, axh0, &ii0);
+  ora_qlh_1d(xp0[1], ay0, ayh0, &jj0);
+  ora_qlh_1d(xp0[2], az0, azh0, &kk0);
+  ora_qlh_1d(xp1[0], ax1, axh1, &i);
+  ora_qlh_1d(xp1[1], ay1, ayh1, &j);
+  ora_qlh_1d(xp1[2], az1, azh1, &k);
+  const size_t c3 = (size_t)s->n1p * s->n2p * s->n3p;
+  double* jx = jc;
+  double* jy = jc + c3;
+  double* jz = jc + 2 * c3;
+#define ORA_O(ii, jj, kk) (((size_t)(ii)-1) + (size_t)s->n1p * (((size_t)(jj)-1) + (size_t)s->n2p * ((size_t)(kk)-1)))
+  for (int k1 = 0; k1 <= 2; ++k1) {
+    for (int j1 = 0; j1 <= 2; ++j1) {
+      double dvol = vp[0] * ay1[j1] * az1[k1];
+      for (int i1 = 0; i1 <= 1; ++i1) jx[ORA_O(i + i1, j + j1, k + k1)] += dvol * axh1[i1];
+    }
+    for (int j1 = 0; j1 <= 2; ++j1) {
+      double dvol = vp[0] * ay0[j1] * az0[k1];
+      for (int i1 = 0; i1 <= 1; ++i1) jx[ORA_O(ii0 + i1, jj0 + j1, kk0 + k1)] += dvol * axh0[i1];
+    }
+  }
+  for (int k1 = 0; k1 <= 2; ++k1) {
+    for (int j1 = 0; j1 <= 1; ++j1) {
+      double dvol = vp[1] * ayh0[j1] * az0[k1];
+      for (int i1 = 0; i1 <= 2; ++i1) jy[ORA_O(ii0 + i1, jj0 + j1, kk0 + k1)] += dvol * ax0[i1];
+    }
+    for (int j1 = 0; j1 <= 1; ++j1) {
+      double dvol = vp[1] * ayh1[j1] * az1[k1];
+      for (int i1 = 0; i1 <= 2; ++i1) jy[ORA_O(i + i1, j + j1, k + k1)] += dvol * ax1[i1];
+    }
+  }
+  for (int k1 = 0; k1 <= 1; ++k1) {
+    for (int j1 = 0; j1 <= 2; ++j1) {
+      double dvol = vp[2] * ay0[j1] * azh0[k1];
+      for (int i1 = 0; i1 <= 2; ++i1) jz[ORA_O(ii0 + i1, jj0 + j1, kk0 + k1)] += dvol * ax0[i1];
+    }
+    for (int j1 = 0; j1 <= 2; ++j1) {
+      double dvol = vp[2] * ay1[j1] * azh1[k1];
+      for (int i1 = 0; i1 <= 2; ++i1) jz[ORA_O(i + i1, j + j1, k + k1)] += dvol * ax1[i1];
+    }
+  }
+}
+static void ora_ncdef_2d_one(ora_sim* s, double* jc, const double xp1[2], const double xp0[2], double p1, double p2,
+                             float wght, double dtg) {
+  double ax0[3], ay0[3], axh0[2], ayh0[2], ax1[3], ay1[3], axh1[2], ayh1[2];
+  int ii0, jj0, i, j;
+  double vp1 = (double)wght * dtg * p1, vp2 = (double)wght * dtg * p2;
+  vp1 = 0.5 * vp1;
+  vp2 = 0.5 * vp2;
+  ora_qlh_1d(xp0[0], ax0, axh0, &ii0);
+  ora_qlh_1d(xp0[1], ay0, ayh0, &jj0);
+  ora_qlh_1d(xp1[0], ax1, axh1, &i);
+  ora_qlh_1d(xp1[1], ay1, ayh1, &j);
+  const size_t c3 = (size_t)s->n1p * s->n2p * s->n3p;
+  double* jx = jc;
+  double* jy = jc + c3;
+  for (int j1 = 0; j1 <= 2; ++j1) {
+    double dvol = vp1 * ay1[j1];
+    for (int i1 = 0; i1 <= 1; ++i1) jx[ORA_O(i + i1, j + j1, 1)] += dvol * axh1[i1];
+    dvol = vp1 * ay0[j1];
+    for (int i1 = 0; i1 <= 1; ++i1) jx[ORA_O(ii0 + i1, jj0 + j1, 1)] += dvol * axh0[i1];
+  }
+  for (int j1 = 0; j1 <= 1; ++j1) {
+    double dvol = vp2 * ayh0[j1];
+    for (int i1 = 0; i1 <= 2; ++i1) jy[ORA_O(ii0 + i1, jj0 + j1, 1)] += dvol * ax0[i1];
+    dvol = vp2 * ayh1[j1];
+    for (int i1 = 0; i1 <= 2; ++i1) jy[ORA_O(i + i1, j + j1, 1)] += dvol * ax1[i1];
+  }
+#undef ORA_O
+}
+
 static void ora_curr_accumulate(ora_sim* s, int ic, int64_t np) {
   const agpu_params* p = &s->p;
   int nth = s->nthreads;
@@ -981,7 +1063,9 @@ static void ora_curr_accumulate(ora_sim* s, int ic, int64_t np) {
       if (p->ndim == 2) {
         double xp1[2] = {p->dx_inv * (PART(s, ic, n, 1) - p->xmn), p->dy_inv * (PART(s, ic, n, 2) - p->ymn)};
         double xp0[2] = {p->dx_inv * (PT(s, n, 3) - p->xmn), p->dy_inv * (PT(s, n, 4) - p->ymn)};
-        if (p->shape == AGPU_SHAPE_CUBIC)
+        if (p->iform == 2)
+          ora_ncdef_2d_one(s, jc, xp1, xp0, PART(s, ic, n, 3), PART(s, ic, n, 4), wght, PT(s, n, 5));
+        else if (p->shape == AGPU_SHAPE_CUBIC)
           ora_esirkepov_cubic_2d_one(s, jc, xp1, xp0, wght);
         else
           ora_esirkepov_2d_one(s, jc, xp1, xp0, wght);
@@ -990,7 +1074,10 @@ static void ora_curr_accumulate(ora_sim* s, int ic, int64_t np) {
                          p->dz_inv * (PART(s, ic, n, 3) - p->zmn)};
         double xp0[3] = {p->dx_inv * (PT(s, n, 4) - p->xmn), p->dy_inv * (PT(s, n, 5) - p->ymn),
                          p->dz_inv * (PT(s, n, 6) - p->zmn)};
-        if (p->shape == AGPU_SHAPE_CUBIC)
+        if (p->iform == 2) {
+          const double pv[3] = {PART(s, ic, n, 4), PART(s, ic, n, 5), PART(s, ic, n, 6)};
+          ora_ncdef_3d_one(s, jc, xp1, xp0, pv, wght, PT(s, n, 7));
+        } else if (p->shape == AGPU_SHAPE_CUBIC)
           ora_esirkepov_cubic_3d_one(s, jc, xp1, xp0, wght);
         else
           ora_esirkepov_3d_one(s, jc, xp1, xp0, wght);

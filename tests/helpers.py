@@ -78,12 +78,12 @@ def plasma_source(p, ic=0, npx=2, npy=2, npz=2, x_start_frac=0.25, jitter=0.6, s
 
 
 def small_case(ndim, precision=AGPU_FP64, nx=64, ny=32, nz=16, cap=200_000, w_sh=10, nsp=1,
-               ionz_lev=0, n_mol_atoms=(1, 1, 1, 1), seed=12345):
+               ionz_lev=0, n_mol_atoms=(1, 1, 1, 1), seed=12345, iform=0):
     g = grid_small(ndim, nx, ny, nz)
     p = make_params(g, precision=precision, nsp=nsp, nsp_run=1, w_sh=w_sh,
                     capacity=(cap, cap if nsp > 1 else 0, cap if nsp > 2 else 0, 0),
                     ionz_lev=ionz_lev, n_mol_atoms=n_mol_atoms, seed=seed,
-                    mass_number=(14.0, 1.0, 1.0))
+                    mass_number=(14.0, 1.0, 1.0), iform=iform)
     return p
 
 

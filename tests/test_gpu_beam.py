@@ -12,7 +12,8 @@ against the oracle and closed forms.
   rounding of the sum).
 * After the set-up, the standard cycle (gather, push, deposit, Yee) with the
   bunch and a plasma, deterministic FP64 form: particles bit-exact against
-  the oracle for 6 steps.
+  the oracle for 6 steps; the same for the reference's own PWFA route, the
+  envelope cycle (particles, fields and env bit-exact).
 * Linearity at the full PWFA size: fields(A u B) = fields(A) + fields(B).
 """
 import numpy as np
@@ -159,3 +160,40 @@ def test_beam_inject_linearity_full_pwfa_grid():
     fa, fb, fab = fields
     assert np.isfinite(fab).all()
     assert np.abs(fab - fa - fb).max() <= 1e-11 * np.abs(fab).max()
+
+
+def test_pwfa_envelope_route_after_setup_bitexact():
+    """The reference's own PWFA route (Env_cycle: beam_inject, then env_run
+    every step, a0 = 0) on a small grid: plasma + bunch in species 0, the
+    envelope cycle, FP64 deterministic mode: particles, fields and env
+    bit-exact against the oracle for 6 steps."""
+    from aladyn_b200.config import env_params
+    kw = dict(capacity=(400_000, 0, 0, 0), w_sh=4)
+    g = grid_pwfa(3, 48, 24, 24)
+    p = make_params(g, **kw)
+    dev, ora = PicDevice(p), Oracle(make_params(g, **kw))
+    ep = env_params(g, 0.8, 2)
+    dev.env_enable(ep)
+    ora.env_enable(ep)
+    src = plasma_source(p, ic=0, npx=1, npy=1, npz=1, x_start_frac=0.1, n_over_n0=1.0)
+    b = pwfa_bunch(p, nb=5000, sxb=1.5, syb=1.0)
+    rec = bunch_records(p, b, n0_ref=0.1)
+    zero = np.zeros(dev.field_shape(), order="F")
+    for s in (dev, ora):
+        s.set_fields(zero)
+        s.set_plasma_source(src)
+        s.load_plasma(0)
+    assert dev.beam_inject(0, rec, b.gam) == 0
+    assert ora.beam_inject(0, rec, b.gam) == 0
+    dev.set_fields(ora.get_fields())
+    dev.set_deterministic(True)
+    for it in range(1, 7):
+        t = it * p.dt
+        out = dev.env_run(t, it)
+        rc, oo = ora.env_run(t, it)
+        assert rc == 0 and out.error_bits == 0
+        assert out.np[0] == oo.np[0]
+    a, c = dev.get_species(0), ora.get_species(0)
+    assert np.array_equal(a.view(np.uint64), c.view(np.uint64))
+    assert np.array_equal(dev.get_fields(), ora.get_fields())
+    assert np.array_equal(dev.get_envelope(), ora.get_envelope())

@@ -23,8 +23,9 @@ from tests.test_envelope import env_case, numpy_init, pulse
 pytestmark = pytest.mark.gpu
 
 
-def _pair(ndim, der_ord=2, nx=64, ny=24, nz=16, w_sh=10):
+def _pair(ndim, der_ord=2, nx=64, ny=24, nz=16, w_sh=10, iform=0):
     p, g, ep = env_case(ndim, nx=nx, ny=ny, nz=nz, der_ord=der_ord, cap=200000, w_sh=w_sh)
+    p.iform = iform
     dev = PicDevice(p)
     ora = Oracle(p)
     dev.env_enable(ep)
@@ -90,6 +91,23 @@ def test_env_run_deterministic_bitexact(ndim, der_ord):
     assert np.array_equal(dev.get_currents(), ora.get_currents()), "currents differ"
     # the plasma has felt the pulse
     assert np.abs(a[:, ndim:2 * ndim]).max() > 1e-3
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_env_run_iform2_deterministic_bitexact(ndim):
+    """The envelope cycle with the iform = 2 deposit (lpf_env_positions keeps
+    dt / gamma for it): bit-exact over 12 steps with a window shift."""
+    p, dev, ora = _pair(ndim, iform=2)
+    dev.set_deterministic(True)
+    for it in range(1, 13):
+        out = dev.env_run(it * p.dt, it)
+        rc, oo = ora.env_run(it * p.dt, it)
+        assert rc == 0 and out.error_bits == 0 and out.np[0] == oo.np[0]
+    a, b = dev.get_species(0), ora.get_species(0)
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    assert np.array_equal(dev.get_currents(), ora.get_currents())
+    assert np.array_equal(dev.get_fields(), ora.get_fields())
+    assert np.array_equal(dev.get_envelope(), ora.get_envelope())
 
 
 @pytest.mark.parametrize("ndim", [2, 3])

@@ -205,3 +205,43 @@ def test_sort_interval_keeps_physics(ndim):
         res.append((d.get_fields(), d.count(0)))
     assert res[0][1] == res[1][1]
     assert _relmax(res[1][0], res[0][0]) <= 1e-5
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_fp64_iform2_deterministic_multistep_bitexact(ndim):
+    """iform = 2 (the non-conserving ncdef deposit, unscaled currents): the
+    deterministic FP64 form against the oracle over 24 steps with window
+    shifts: particles, currents and fields bit-exact."""
+    p, dev, ora = _pair(ndim, iform=2)
+    dev.set_deterministic(True)
+    t = 0.0
+    for it in range(24):
+        out = dev.lp_run(t, it, initial_time=(it == 0))
+        rc, oo = ora.lp_run(t, it, initial_time=(it == 0))
+        assert rc == 0 and out.error_bits == 0
+        assert out.np[0] == oo.np[0]
+        t += p.dt
+    a, b = dev.get_species(0), ora.get_species(0)
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    assert np.array_equal(dev.get_currents(), ora.get_currents())
+    assert np.array_equal(dev.get_fields(), ora.get_fields())
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_fp64_iform2_atomic_close(ndim):
+    """iform = 2 with atomic sums (the untiled kernels): particles bit-exact
+    after one step, currents and fields to 1e-12."""
+    p, dev, ora = _pair(ndim, iform=2)
+    out = dev.lp_run(0.0, 0, initial_time=True)
+    rc, oo = ora.lp_run(0.0, 0, initial_time=True)
+    assert rc == 0 and out.error_bits == 0 and out.np[0] == oo.np[0]
+    a, b = dev.get_species(0), ora.get_species(0)
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    assert _relmax(dev.get_currents(), ora.get_currents()) <= 1e-12
+    assert _relmax(dev.get_fields(), ora.get_fields()) <= 1e-12
+
+
+def test_iform2_rejected_outside_fp64_quadratic():
+    from aladyn_b200.abi import AgpuError
+    with pytest.raises(AgpuError):
+        PicDevice(small_case(2, precision=AGPU_FP32_SPLIT, iform=2))
