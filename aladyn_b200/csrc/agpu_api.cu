@@ -89,6 +89,10 @@ struct agpu_handle {
   double* env_den = nullptr;
   agpu_env_params ep{};
   long long env_steps = 0;  // env_run calls so far (the record sort period)
+  // comoving frame (w_speed < 0): the field advection's scratch
+  double* xadv_tmp = nullptr;
+  double* xadv_coef = nullptr;  // bet[0..nx+1], then w1[0..nx+1]
+  XAdv xadv{};
   // window state (lp_window_xshift saved variables)
   double xlapse = 0.0;
   int wi1 = 0;
@@ -164,8 +168,13 @@ int dmalloc(void** p, size_t bytes) {
   return 0;
 }
 
+// Comoving frame (w_speed < 0: vbeam = -w_speed, set_init_param.f90:239-245):
+// the x displacement dt * vbeam subtracted after every push, 0 otherwise.
+double comoving_vdt(const agpu_params& p) { return p.w_speed < 0.0 ? p.dt * (-p.w_speed) : 0.0; }
+
 YeeC yee_coef(const agpu_params& p) {
   YeeC c;
+  c.vbeam = p.w_speed < 0.0 ? -p.w_speed : 0.0;
   c.dx_inv = p.dx_inv;
   c.dy_inv = p.dy_inv;
   c.dz_inv = p.dz_inv;
@@ -241,6 +250,8 @@ int free_all(agpu_handle* h) {
   cudaFree(h->env);
   cudaFree(h->env_av);
   cudaFree(h->env_den);
+  cudaFree(h->xadv_tmp);
+  cudaFree(h->xadv_coef);
   for (int i = 0; i < 2 * PH_N; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
@@ -570,6 +581,7 @@ int tiled_push(agpu_handle* h, int ic, int initial_time, agpu_step_out* out) {
     a.gymax = p.gymax;
     a.gzmin = p.gzmin;
     a.gzmax = p.gzmax;
+    a.vdt = comoving_vdt(p);
     a.initial = initial_time ? 1 : 0;
     a.err = &h->d_cnt->err;
     tile_push64(a, h->st);
@@ -674,6 +686,71 @@ int window_xshift(agpu_handle* h, int witr, int init_iter, agpu_step_out* out) {
     }
   }
   return 0;
+}
+
+// comoving_coordinate (src/dynamics/window.f90:227-275) for the comoving
+// frame (vb = -w_speed): the box stays put, the plasma source's x range (and
+// so every lattice column not yet injected) moves by -vb w_nst dt, the
+// particles at or left of gxmin (or past gxmax) are dropped along x only and
+// the columns that entered the box are injected.
+int comoving_coordinate(agpu_handle* h, double vb, int w_nst, int loc_it, agpu_step_out* out) {
+  agpu_params& p = h->p;
+  if (loc_it == 0) return 0;
+  const double dt_step = p.dt;
+  double dt_tot = 0.0;
+  for (int i = 1; i <= w_nst; ++i) dt_tot = dt_tot + dt_step;
+  for (int ic = 0; ic < p.nsp; ++ic) {
+    if (!h->has_src[ic]) continue;
+    h->src[ic].x_start = h->src[ic].x_start - vb * dt_tot;
+    h->src[ic].x_end = h->src[ic].x_end - vb * dt_tot;
+  }
+  for (int ic = 0; ic < p.nsp; ++ic) {
+    if (h->np[ic] <= 0) continue;
+    long long before = h->np[ic];
+    int rc = compact_species(h, ic, true);
+    if (rc) return rc;
+    out->removed[ic] += before - h->np[ic];
+  }
+  for (int ic = 0; ic < p.nsp; ++ic) {
+    if (!h->has_src[ic]) continue;
+    const agpu_plasma& s = h->src[ic];
+    if (s.x_start <= p.xmax && s.x_end > p.xmax) {
+      long long i1 = 1 + h->nptx[ic];
+      long long i2 = lattice_columns_end(h, ic, i1, p.xmax, true);
+      h->nptx[ic] = i2;
+      if (i2 > i1) {
+        long long before = h->np[ic];
+        int rc = add_lattice_columns(h, ic, i1, i2);
+        if (rc) return rc;
+        out->injected[ic] += h->np[ic] - before;
+      }
+    }
+  }
+  return 0;
+}
+
+// field_xadvect launches of one Yee step in the comoving frame: four
+// boundary-ghost kernels, two per component in the explicit substeps, two
+// tridiagonal sweeps
+long long xadv_launches(const agpu_handle* h) { return h->xadv.tmp ? 6 + 2LL * h->g.nf : 0; }
+
+// lp_run (src/dynamics/pic_evolve_in_time.f90 callers): the moving window
+// (w_speed > 0) or the comoving frame's coordinate step (w_speed < 0), every
+// w_sh steps inside [wi_time, wf_time)
+int window_or_comoving(agpu_handle* h, int iter, double t, agpu_step_out* out) {
+  const agpu_params& p = h->p;
+  if (p.w_sh <= 0 || !(t >= p.wi_time && t < p.wf_time) || iter % p.w_sh != 0) return 0;
+  int rc = 0;
+  if (p.w_speed > 0.0) {
+    ph_begin(h, PH_WINDOW);
+    rc = window_xshift(h, p.w_sh, iter, out);
+    ph_end(h, PH_WINDOW);
+  } else if (p.w_speed < 0.0) {
+    ph_begin(h, PH_WINDOW);
+    rc = comoving_coordinate(h, -p.w_speed, p.w_sh, iter, out);
+    ph_end(h, PH_WINDOW);
+  }
+  return rc;
 }
 
 int upload_table(agpu_handle* h, int ic, const double* tab, int zmax) {
@@ -880,6 +957,8 @@ int agpu_create(const agpu_params* params, agpu_handle** out) {
   if (p.ibx != 0 || p.iby != 0 || p.ibz != 0 || p.iform < 0 || p.iform > 2) return AGPU_E_ARG;
   // iform = 2 (the non-conserving deposit) in the FP64 form, quadratic shapes
   if (p.iform == 2 && (p.precision != AGPU_FP64 || p.shape != AGPU_SHAPE_QUADRATIC)) return AGPU_E_ARG;
+  // the comoving frame (w_speed < 0) in the FP64 form
+  if (p.w_speed < 0.0 && p.precision != AGPU_FP64) return AGPU_E_ARG;
   if (p.nsp < 1 || p.nsp > 4 || p.nsp_run < 1 || p.nsp_run > p.nsp) return AGPU_E_ARG;
   if (p.precision != AGPU_FP64 && p.precision != AGPU_FP32_SPLIT) return AGPU_E_ARG;
   if (p.shape != AGPU_SHAPE_QUADRATIC && p.shape != AGPU_SHAPE_CUBIC) return AGPU_E_ARG;
@@ -971,6 +1050,38 @@ int agpu_create(const agpu_params* params, agpu_handle** out) {
     }
     if (cudaMallocHost((void**)&h->h_cnt, sizeof(Counters)) != cudaSuccess) rc |= AGPU_E_NOMEM;
     if (cudaMallocHost((void**)&h->scr.h_total, sizeof(long long)) != cudaSuccess) rc |= AGPU_E_NOMEM;
+  }
+  if (!rc && p.w_speed < 0.0) {
+    // comoving frame: the advection's buffer and the tridiagonal coefficients
+    // of trid_der1 for a = -aphx_exp, b = 1, c = aphx_exp, b1 = bn = 1,
+    // c1 = an = 0 (grid_fields.f90:37-77, 210-324), computed once
+    const int n = p.nx;
+    const double vbeam = -p.w_speed, dth = 0.5 * p.dt;
+    const double aphx = dth * p.dx_inv;
+    const double aphx_exp = 0.5 * (-vbeam) * aphx;
+    const double a = -aphx_exp, b = 1., c = -a, b1 = 1., c1 = 0.0, an = 0.0, bn = 1.;
+    std::vector<double> coef(2 * (size_t)(n + 2), 0.0);
+    double* bet = coef.data();
+    double* w1 = coef.data() + (n + 2);
+    w1[1] = 0.0;
+    bet[1] = b1;
+    w1[2] = c1 / bet[1];
+    bet[2] = b - a * w1[2];
+    for (int k = 3; k <= n - 1; ++k) {
+      w1[k] = c / bet[k - 1];
+      bet[k] = b - a * w1[k];
+    }
+    w1[n] = c / bet[n - 1];
+    bet[n] = bn - an * w1[n];
+    rc |= dmalloc((void**)&h->xadv_tmp, sizeof(double) * g.ncell);
+    rc |= dmalloc((void**)&h->xadv_coef, sizeof(double) * coef.size());
+    if (!rc && cudaMemcpy(h->xadv_coef, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      rc |= AGPU_E_CUDA;
+    h->xadv.tmp = h->xadv_tmp;
+    h->xadv.bet = h->xadv_coef;
+    h->xadv.w1 = h->xadv_coef + (n + 2);
+    h->xadv.a = a;
+    h->xadv.aphx_exp = aphx_exp;
   }
   if (!rc) {
     if (h->ebf) cudaMemsetAsync(h->ebf, 0, sizeof(double) * g.ncell * g.nf, h->st);
@@ -1292,7 +1403,7 @@ int agpu_step(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu
   if (!h) return AGPU_E_ARG;
   const agpu_params& p = h->p;
   bool plain = h->use_graph && h->defer && !initial_time && p.ionz_lev == 0 && !h->profiling && !h->deterministic;
-  if (plain && p.w_speed > 0.0 && p.w_sh > 0 && t >= p.wi_time && t < p.wf_time && iter % p.w_sh == 0) plain = false;
+  if (plain && p.w_speed != 0.0 && p.w_sh > 0 && t >= p.wi_time && t < p.wf_time && iter % p.w_sh == 0) plain = false;
   if (plain && sort_step(h, iter)) plain = false;
   for (int ic = 0; ic < p.nsp_run && plain; ++ic)
     if (h->np[ic] > 0 && !(h->binned[ic] && h->key[ic])) plain = false;
@@ -1616,6 +1727,7 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
       a.gymax = p.gymax;
       a.gzmin = p.gzmin;
       a.gzmax = p.gzmax;
+      a.vdt = comoving_vdt(p);
       a.initial = initial_time ? 1 : 0;
       a.shape = p.shape;
       a.iform = p.iform;
@@ -1643,7 +1755,8 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
   YeeC c = yee_coef(p);
   // the fused step writes a second field array (its tiles read halos of the
   // input); not inside step graphs, whose launches keep their pointers
-  const bool fused = h->fused_yee && !h->use_graph;
+  // (the comoving frame's advection substeps run only in the plain sweeps)
+  const bool fused = h->fused_yee && !h->use_graph && !h->xadv.tmp;
   if (h->fp32) {
     Dev32 d{h->g, h->ebf32, h->jhi, h->jlo};
     jfold32(d, h->st, h->sms);
@@ -1660,26 +1773,17 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
       yee64_fused(h->ebf, h->ebf_alt, h->jc, h->g, c, h->st);
       std::swap(h->ebf, h->ebf_alt);
     } else {
-      yee64(d, c, h->st, h->sms);
+      yee64(d, c, h->st, h->sms, h->xadv.tmp ? &h->xadv : nullptr);
     }
   }
   CK(cudaGetLastError());
   ph_end(h, PH_YEE);
   h->timers.launches_yee += 1;
   // current fold (x, y[, z] faces; hi and lo in the split form) + the Yee kernels
-  h->timers.launches_total += ((p.ndim == 3) ? 3 : 2) * (h->fp32 ? 2 : 1) + (fused ? 1 : 6);
+  h->timers.launches_total += ((p.ndim == 3) ? 3 : 2) * (h->fp32 ? 2 : 1) + (fused ? 1 : 6) + xadv_launches(h);
   h->timers.yee_cells += (long long)p.nx * p.ny * (p.ndim == 3 ? p.nz : 1);
-  // lp_run: moving window
-  if (p.w_speed > 0.0 && p.w_sh > 0) {
-    if (t >= p.wi_time && t < p.wf_time) {
-      if (iter % p.w_sh == 0) {
-        ph_begin(h, PH_WINDOW);
-        rc = window_xshift(h, p.w_sh, iter, out);
-        ph_end(h, PH_WINDOW);
-        if (rc) return rc;
-      }
-    }
-  }
+  // lp_run: moving window, or the comoving frame's coordinate shift
+  if (int rc_ = window_or_comoving(h, iter, t, out)) return rc_;
   if (!h->defer)
     if (int rc_ = read_counters(h)) return rc_;
   // deferred mode: the counts of the last synchronisation point
@@ -1869,6 +1973,8 @@ int agpu_env_run(agpu_handle* h, int32_t iter, double t, agpu_step_out* out) {
   a.gymax = p.gymax;
   a.gzmin = p.gzmin;
   a.gzmax = p.gzmax;
+  a.vdt = comoving_vdt(p);
+  a.xtmp = h->xadv_tmp;
   a.om0 = h->ep.om0;
   a.opt_der1 = h->ep.opt_der1;
   a.hord_der2 = h->ep.hord_der2;
@@ -1897,7 +2003,7 @@ int agpu_env_run(agpu_handle* h, int32_t iter, double t, agpu_step_out* out) {
   CK(cudaGetLastError());
   ph_end(h, PH_PUSH);
   h->timers.launches_push_deposit += 2;
-  h->timers.launches_total += 12 + (g.ndim == 3 ? 2 : 0);
+  h->timers.launches_total += 12 + (g.ndim == 3 ? 2 : 0) + (a.vdt > 0. ? 1 : 0);
   h->timers.pushes += a.np;
   if (int rc = read_counters(h)) return rc;
   int rc = 0;
@@ -1913,22 +2019,13 @@ int agpu_env_run(agpu_handle* h, int32_t iter, double t, agpu_step_out* out) {
   ph_begin(h, PH_YEE);
   Dev64 d{g, h->ebf, h->jc};
   jfold64(d, h->st, h->sms);
-  yee64(d, yee_coef(p), h->st, h->sms);
+  yee64(d, yee_coef(p), h->st, h->sms, h->xadv.tmp ? &h->xadv : nullptr);
   CK(cudaGetLastError());
   ph_end(h, PH_YEE);
   h->timers.launches_yee += 1;
-  h->timers.launches_total += ((p.ndim == 3) ? 3 : 2) + 6;
+  h->timers.launches_total += ((p.ndim == 3) ? 3 : 2) + 6 + xadv_launches(h);
   h->timers.yee_cells += (long long)p.nx * p.ny * (p.ndim == 3 ? p.nz : 1);
-  if (p.w_speed > 0.0 && p.w_sh > 0) {
-    if (t >= p.wi_time && t < p.wf_time) {
-      if (iter % p.w_sh == 0) {
-        ph_begin(h, PH_WINDOW);
-        rc = window_xshift(h, p.w_sh, iter, out);
-        ph_end(h, PH_WINDOW);
-        if (rc) return rc;
-      }
-    }
-  }
+  if ((rc = window_or_comoving(h, iter, t, out))) return rc;
   if (int rc_ = read_counters(h)) return rc_;
   for (int q = 0; q < 4; ++q) out->np[q] = h->binned[q] ? h->nalive[q] : h->np[q];
   out->xmn = p.xmn;

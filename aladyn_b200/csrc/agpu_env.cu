@@ -559,6 +559,96 @@ __global__ void k_env_update(double* env, double* av, Geo g, double k2_fact, dou
   }
 }
 
+// env_lpf_solve (src/fields/grid_fields.f90:696-858) with ib = 0, the
+// comoving frame's reduced envelope solver, in three passes.  Pass 1, per
+// node: the source -ompe chi A, the transverse Laplacian (pp_lapl) added,
+// and on the row j = jy1 alone the factor -dt (the reference's
+// `do j = jy1, jy1`).
+__global__ void k_env_lpf_src(const double* __restrict__ env, double* av, Geo g, double ompe, double dy2, double dz2,
+                              double dtl) {
+  const long long total = interior_count(g);
+  const long long nc = g.ncell, sy = g.n1p, sz = (long long)g.n1p * g.n2p;
+  GRID_LOOP(t, total) {
+    int i, j, k;
+    interior_node(g, t, i, j, k);
+    const long long o = goff(g, i, j, k);
+    const double a3 = av[2 * nc + o];
+    double c[2];
+    c[0] = -ompe * a3 * env[o];
+    c[1] = -ompe * a3 * env[nc + o];
+    for (int q = 0; q < 2; ++q) {
+      const double* e = env + q * nc;
+      c[q] = c[q] + dy2 * ((e[o + sy] - e[o]) - (e[o] - e[o - sy]));
+    }
+    if (g.ndim == 3)
+      for (int q = 0; q < 2; ++q) {
+        const double* e = env + q * nc;
+        c[q] = c[q] + dz2 * ((e[o + sz] - e[o]) - (e[o] - e[o - sz]));
+      }
+    if (j == g.jy1) {
+      c[0] = -dtl * c[0];
+      c[1] = -dtl * c[1];
+    }
+    av[o] = c[0];
+    av[nc + o] = c[1];
+  }
+}
+// Pass 2: first_der's centred x-derivative with the om0 rotation into
+// (t1, t2); the row's x ghosts of av(1:2), which the reference leaves as
+// they are, travel along so that pass 3 reads the same neighbours.
+__global__ void k_env_lpf_der1(const double* __restrict__ av, double* t1, double* t2, Geo g, double om0, double dx1_inv) {
+  const long long total = interior_count(g);
+  const long long nc = g.ncell;
+  GRID_LOOP(t, total) {
+    int i, j, k;
+    interior_node(g, t, i, j, k);
+    const long long o = goff(g, i, j, k);
+    const double* a1 = av;
+    const double* a2 = av + nc;
+    t1[o] = om0 * a2[o] + dx1_inv * (a1[o + 1] - a1[o - 1]);
+    t2[o] = -om0 * a1[o] + dx1_inv * (a2[o + 1] - a2[o - 1]);
+    if (i == g.ix1) {
+      t1[o - 1] = a1[o - 1];
+      t2[o - 1] = a2[o - 1];
+    }
+    if (i == g.ix2) {
+      t1[o + 1] = a1[o + 1];
+      t2[o + 1] = a2[o + 1];
+    }
+  }
+}
+// Pass 3: explicit_mat_inv's three-point inversion (u - dx2_norm D2 u) / om0^2,
+// then A^{n+1} = A^{n-1} + u, the shift A^{n-1} <- A^n, A^n <- A^{n+1}, and
+// env_fields_average's av(1) = (1/8)((A^{n+1} + A^n)^2) of the update.
+__global__ void k_env_lpf_inv(double* env, double* av, const double* __restrict__ t1, const double* __restrict__ t2, Geo g,
+                              double dx2_norm, double om2) {
+  const long long total = interior_count(g);
+  const long long nc = g.ncell;
+  const double frac = 1.0 / 8.;
+  GRID_LOOP(t, total) {
+    int i, j, k;
+    interior_node(g, t, i, j, k);
+    const long long o = goff(g, i, j, k);
+    double v[2];
+    const double* tq[2] = {t1, t2};
+    for (int q = 0; q < 2; ++q) {
+      const double* u = tq[q];
+      const double w = dx2_norm * (u[o + 1] - 2. * u[o] + u[o - 1]);
+      v[q] = (u[o] - w) / om2;
+    }
+    const double e1 = env[o], e2 = env[nc + o];
+    v[0] = v[0] + env[2 * nc + o];
+    v[1] = v[1] + env[3 * nc + o];
+    env[2 * nc + o] = e1;
+    env[3 * nc + o] = e2;
+    env[o] = v[0];
+    env[nc + o] = v[1];
+    av[nc + o] = v[1];
+    const double sa = v[0] + e1, sb = v[1] + e2;
+    av[o] = frac * (sa * sa + sb * sb);
+  }
+}
+
 // set_env_grad_interp (grid_part_connect.f90:760-882) -> lpf_env_positions
 // (src/dynamics/boris_push.f90:225-295, vbeam = 0) -> the box test of
 // cell_part_dist(.false.) (mpi_part_interface.f90:467-523) -> Esirkepov
@@ -615,7 +705,9 @@ __global__ void __launch_bounds__(256) k_env_pos(EnvArgs a) {
       double gam_inv = 1. / gam;
       gam_inv = gam_inv * (1. - dt_lp * b2 / gam3);
       const double vp1 = dt_lp * gam_inv * pp1, vp2 = dt_lp * gam_inv * pp2;
-      const double xn = x + vp1, yn = y + vp2;
+      double xn = x + vp1;
+      const double yn = y + vp2;
+      if (a.vdt > 0.) xn = xn - a.vdt;  // comoving frame (boris_push.f90:288-294)
       a.x[n] = xn;
       a.y[n] = yn;
       const bool keep = (xn > a.gxmin && xn <= a.gxmax) && (yn > a.gymin && yn <= a.gymax);
@@ -682,7 +774,9 @@ __global__ void __launch_bounds__(256) k_env_pos(EnvArgs a) {
     gam_inv = gam_inv * (1. - dt_lp * b2 / gam3);
     double vp[3];
     for (int c = 0; c < 3; ++c) vp[c] = dt_lp * gam_inv * pp[c];
-    const double xn = x + vp[0], yn = y + vp[1], zn = z + vp[2];
+    double xn = x + vp[0];
+    const double yn = y + vp[1], zn = z + vp[2];
+    if (a.vdt > 0.) xn = xn - a.vdt;  // comoving frame (boris_push.f90:288-294)
     a.x[n] = xn;
     a.y[n] = yn;
     a.z[n] = zn;
@@ -812,6 +906,18 @@ void env_advance(const EnvArgs& a, cudaStream_t st, int sms) {
   k_env_bds_x<<<grid_blocks(2 * ny * nz, sms), 256, 0, st>>>(a.env, g, a.ibx);
   k_env_bds_y<<<grid_blocks(2 * nxw * nz, sms), 256, 0, st>>>(a.env, g, a.iby);
   if (g.ndim == 3) k_env_bds_z<<<grid_blocks(2 * nxw * nyw, sms), 256, 0, st>>>(a.env, g, a.ibz);
+  const long long n = interior_count(g);
+  if (a.vdt > 0.) {
+    // comoving frame: env_lpf_solve with ib = 0 (curr_and_fields_util.f90:276, 292-293)
+    const double om0 = a.om0;
+    const double dx_norm = a.dx_inv / om0;
+    k_env_lpf_src<<<grid_blocks(n, sms), 256, 0, st>>>(a.env, a.av, g, a.ompe, a.dy_inv * a.dy_inv, a.dz_inv * a.dz_inv,
+                                                      a.dt);
+    k_env_lpf_der1<<<grid_blocks(n, sms), 256, 0, st>>>(a.av, a.den, a.xtmp, g, om0, 0.5 * a.dx_inv);
+    k_env_lpf_inv<<<grid_blocks(n, sms), 256, 0, st>>>(a.env, a.av, a.den, a.xtmp, g, dx_norm * dx_norm, om0 * om0);
+    k_env_grad<<<grid_blocks(n, sms), 256, 0, st>>>(a.av, g, a.dx_inv, a.dy_inv, a.dz_inv);
+    return;
+  }
   SolveC s;
   s.ompe = a.ompe;
   s.dt2 = a.dt * a.dt;
@@ -834,7 +940,6 @@ void env_advance(const EnvArgs& a, cudaStream_t st, int sms) {
   s.dx4_2 = cf2 * dx2;
   s.dy2 = a.dy_inv * a.dy_inv;
   s.dz2 = a.dz_inv * a.dz_inv;
-  const long long n = interior_count(g);
   k_env_solve<<<grid_blocks(n, sms), 256, 0, st>>>(a.env, a.av, g, s);
   const double k2_fact = 1. / (1. + s.kfact * s.kfact);
   k_env_update<<<grid_blocks(n, sms), 256, 0, st>>>(a.env, a.av, g, k2_fact, s.kfact);

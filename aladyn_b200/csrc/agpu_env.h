@@ -28,6 +28,10 @@ struct EnvArgs {
   double xmn, ymn, zmn, dx_inv, dy_inv, dz_inv;
   double dt, lfact, ompe;
   double gxmin, gxmax, gymin, gymax, gzmin, gzmax;
+  double vdt;  // comoving frame: dt * vbeam subtracted from x after the push (0: off)
+  // comoving frame: a second ncell scratch for the reduced envelope solver
+  // (den is the first; both free once den has been copied into av)
+  double* xtmp;
   double om0, opt_der1, hord_der2;
   int der_ord, ibx, iby, ibz, iform;
   unsigned long long* removed;
@@ -48,8 +52,8 @@ void env_amp_grad(const EnvArgs& a, cudaStream_t st, int sms);
 void env_acc_momenta(const EnvArgs& a, cudaStream_t st, int sms, bool serial);
 // den_zyxbd on den, then av(1) = av(3) = den
 void env_den_collect(const EnvArgs& a, cudaStream_t st, int sms);
-// env_bds + the source term + env_maxw_solve, then env_fields_average and
-// env_grad
+// env_bds + the source term + env_maxw_solve (env_lpf_solve with ib = 0 in
+// the comoving frame, a.vdt > 0), then env_fields_average and env_grad
 void env_advance(const EnvArgs& a, cudaStream_t st, int sms);
 // set_env_grad_interp + lpf_env_positions + the box test of
 // cell_part_dist(.false.) + the Esirkepov deposit of the kept particles

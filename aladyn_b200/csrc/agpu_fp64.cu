@@ -319,6 +319,7 @@ __global__ void __launch_bounds__(256) k64_push_dep_3d(PushArgs64 a) {
     double xnew = x + dtg * pn[0];
     double ynew = y + dtg * pn[1];
     double znew = z + dtg * pn[2];
+    if (a.vdt > 0.) xnew = xnew - a.vdt;  // comoving frame (boris_push.f90:161-166)
     a.px[n] = pn[0];
     a.py[n] = pn[1];
     a.pz[n] = pn[2];
@@ -441,6 +442,7 @@ __global__ void __launch_bounds__(256) k64_push_dep_2d(PushArgs64 a) {
     double dtg = a.dt / sqrt(gam2);
     double xnew = x + dtg * pn1;
     double ynew = y + dtg * pn2;
+    if (a.vdt > 0.) xnew = xnew - a.vdt;  // comoving frame (boris_push.f90:161-166)
     a.px[n] = pn1;
     a.py[n] = pn2;
     a.x[n] = xnew;
@@ -488,8 +490,8 @@ void push_deposit64(const PushArgs64& a, cudaStream_t st, int sms, bool serial) 
 
 void jfold64(const Dev64& d, cudaStream_t st, int sms) { jfold_t<double>(d.jc, d.g, st, sms); }
 
-void yee64(const Dev64& d, const YeeC& c, cudaStream_t st, int sms) {
-  yee_t<double>(d.ebf, d.jc, (const double*)nullptr, d.g, c, st, sms);
+void yee64(const Dev64& d, const YeeC& c, cudaStream_t st, int sms, const XAdv* xa) {
+  yee_t<double>(d.ebf, d.jc, (const double*)nullptr, d.g, c, st, sms, xa);
 }
 void yee64_fused(const double* fin, double* fout, const double* jc, const Geo& g, const YeeC& c, cudaStream_t st) {
   yee_fused_t<double>(fin, fout, jc, (const double*)nullptr, g, c, st);

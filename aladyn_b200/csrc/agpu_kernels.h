@@ -10,6 +10,18 @@
 namespace agpu {
 struct YeeC {
   double dx_inv, dy_inv, dz_inv, dt, se1, se2, ompe, djc1, djc2, djc3;
+  double vbeam;  // comoving frame: the x advection speed of the fields (0: off)
+};
+// Scratch of the comoving frame's field advection (field_xadvect,
+// src/fields/grid_fields.f90:210-324): a one-component buffer for the
+// explicit step and the coefficients of the implicit step's tridiagonal
+// solve (trid_der1, grid_fields.f90:37-77, with b1 = bn = 1, c1 = an = 0),
+// the same for every row: bet[k], w1[k], k = 1..nx, a = -aphx_exp.
+struct XAdv {
+  double* tmp;
+  const double* bet;
+  const double* w1;
+  double a, aphx_exp;
 };
 }  // namespace agpu
 
@@ -34,6 +46,7 @@ struct PushArgs64 {
   double xmn, ymn, zmn, dx_inv, dy_inv, dz_inv;
   double dt, dth, lfact;
   double gxmin, gxmax, gymin, gymax, gzmin, gzmax;
+  double vdt;  // comoving frame: dt * vbeam subtracted from x after the push (0: off)
   int initial;
   int shape;  // AGPU_SHAPE_QUADRATIC or AGPU_SHAPE_CUBIC
   int iform;  // 0, 1: Esirkepov; 2: the non-conserving ncdef deposit
@@ -60,7 +73,7 @@ struct IonArgs64 {
 void field_bd64(const Dev64& d, cudaStream_t st, int sms);
 void push_deposit64(const PushArgs64& a, cudaStream_t st, int sms, bool serial);
 void jfold64(const Dev64& d, cudaStream_t st, int sms);
-void yee64(const Dev64& d, const YeeC& c, cudaStream_t st, int sms);
+void yee64(const Dev64& d, const YeeC& c, cudaStream_t st, int sms, const XAdv* xa = nullptr);
 // the whole leapfrog step in one z-streaming kernel, fin -> fout (fout != fin)
 void yee64_fused(const double* fin, double* fout, const double* jc, const Geo& g, const YeeC& c, cudaStream_t st);
 __global__ void k64_ion_efield(IonArgs64 a);

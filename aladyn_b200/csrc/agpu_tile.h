@@ -48,6 +48,7 @@ struct TileArgs64 {
   double xmn, ymn, zmn, dx_inv, dy_inv, dz_inv;
   double dt, dth, lfact;
   double gxmin, gxmax, gymin, gymax, gzmin, gzmax;
+  double vdt;  // comoving frame: dt * vbeam subtracted from x after the push (0: off)
   int initial;
   unsigned int* err;
 };

@@ -264,6 +264,8 @@ __global__ void __launch_bounds__(256, 2) k64_tile(TileArgs64 a) {
       xnew = x + dtg * pn1;
       ynew = y + dtg * pn2;
     }
+    // comoving frame (boris_push.f90:161-166)
+    if (a.vdt > 0.) xnew = xnew - a.vdt;
     a.px[p] = pp[0];
     a.py[p] = pp[1];
     a.x[p] = xnew;

@@ -412,8 +412,80 @@ __global__ void __launch_bounds__(YEE_BX* YEE_BY) k_rotb_j_n(T* ebf, const T* jc
   E3[o] = ez - ompe * (djc3 * j3);
 }
 
+// ---- comoving frame: field_xadvect (src/fields/grid_fields.f90:210-324) ----
+
+// x ghosts: f(ix1-1) = f(ix1+1), f(ix2+1) = f(ix2), components ic1..ic2
 template <typename T>
-void yee_t(T* ebf, const T* jc, const T* jlo, const Geo& g, const YeeC& c, cudaStream_t st, int sms) {
+__global__ void k_xadv_ghost(T* ebf, Geo g, int ic1, int ic2) {
+  const int ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
+  const long long rows = (long long)ny * nz;
+  const long long total = rows * (ic2 - ic1 + 1);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int ic = ic1 + (int)(t / rows);
+    const long long r = t - (long long)(ic - ic1) * rows;
+    const int j = g.jy1 + (int)(r % ny), k = g.kz1 + (int)(r / ny);
+    T* row = ebf + g.ncell * (ic - 1) + goff(g, 1, j, k) - 1;  // row[i] = f(i)
+    row[g.ix1 - 1] = row[g.ix1 + 1];
+    row[g.ix2 + 1] = row[g.ix2];
+  }
+}
+// explicit step of one component into the row buffer, then back
+template <typename T>
+__global__ void k_xadv_explicit(const T* f, double* tmp, Geo g, double aphx_exp) {
+  const int i = g.ix1 + blockIdx.x * YEE_BX + threadIdx.x;
+  const int j = g.jy1 + blockIdx.y * YEE_BY + threadIdx.y;
+  if (i > g.ix2 || j > g.jy2) return;
+  const long long o = goff(g, i, j, g.ndim == 3 ? g.kz1 + (int)blockIdx.z : 1);
+  tmp[o] = f[o] - aphx_exp * (f[o + 1] - f[o - 1]);
+}
+template <typename T>
+__global__ void k_xadv_copy(T* f, const double* tmp, Geo g) {
+  const int i = g.ix1 + blockIdx.x * YEE_BX + threadIdx.x;
+  const int j = g.jy1 + blockIdx.y * YEE_BY + threadIdx.y;
+  if (i > g.ix2 || j > g.jy2) return;
+  const long long o = goff(g, i, j, g.ndim == 3 ? g.kz1 + (int)blockIdx.z : 1);
+  f[o] = tmp[o];
+}
+// implicit step: one thread per row (component ic1..ic2), the Thomas sweeps
+// in place in trid_der1's order
+template <typename T>
+__global__ void k_xadv_implicit(T* ebf, Geo g, int ic1, int ic2, XAdv x) {
+  const int ny = g.jy2 - g.jy1 + 1, nz = g.kz2 - g.kz1 + 1;
+  const long long rows = (long long)ny * nz;
+  const long long total = rows * (ic2 - ic1 + 1);
+  const int n = g.ix2 - g.ix1 + 1;
+  const double a = x.a, an = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int ic = ic1 + (int)(t / rows);
+    const long long r = t - (long long)(ic - ic1) * rows;
+    const int j = g.jy1 + (int)(r % ny), k = g.kz1 + (int)(r / ny);
+    T* u = ebf + g.ncell * (ic - 1) + goff(g, g.ix1, j, k) - 1;  // u[kk] = f(ix1 + kk - 1), kk = 1..n
+    u[1] = u[1] / x.bet[1];
+    for (int kk = 2; kk <= n - 1; ++kk) u[kk] = (u[kk] - a * u[kk - 1]) / x.bet[kk];
+    u[n] = (u[n] - an * u[n - 1]) / x.bet[n];
+    for (int kk = n - 1; kk >= 1; --kk) u[kk] = u[kk] - x.w1[kk + 1] * u[kk + 1];
+  }
+}
+template <typename T>
+void xadvect_t(T* ebf, const Geo& g, int ic1, int ic2, int isch, const XAdv& x, cudaStream_t st, int sms) {
+  const long long rows = (long long)(g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1) * (ic2 - ic1 + 1);
+  k_xadv_ghost<T><<<grid_for(rows, 256, sms), 256, 0, st>>>(ebf, g, ic1, ic2);
+  if (isch == 0) {
+    const dim3 blk(YEE_BX, YEE_BY, 1);
+    const dim3 grd((g.ix2 - g.ix1 + YEE_BX) / YEE_BX, (g.jy2 - g.jy1 + YEE_BY) / YEE_BY, g.ndim == 3 ? g.kz2 - g.kz1 + 1 : 1);
+    for (int ic = ic1; ic <= ic2; ++ic) {
+      k_xadv_explicit<T><<<grd, blk, 0, st>>>(ebf + g.ncell * (ic - 1), x.tmp, g, x.aphx_exp);
+      k_xadv_copy<T><<<grd, blk, 0, st>>>(ebf + g.ncell * (ic - 1), x.tmp, g);
+    }
+  } else {
+    k_xadv_implicit<T><<<(int)((rows + 127) / 128), 128, 0, st>>>(ebf, g, ic1, ic2, x);
+  }
+}
+
+// xa: the comoving frame's advection scratch (c.vbeam > 0), else null
+template <typename T>
+void yee_t(T* ebf, const T* jc, const T* jlo, const Geo& g, const YeeC& c, cudaStream_t st, int sms,
+           const XAdv* xa = nullptr) {
   long long faces = (long long)(g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1) + (long long)(g.ix2 - g.ix1 + 1) * (g.kz2 - g.kz1 + 1) +
                     (g.ndim == 3 ? (long long)(g.ix2 - g.ix1 + 1) * (g.jy2 - g.jy1 + 1) : 0);
   int gf = grid_for(faces, 256, sms);
@@ -421,12 +493,19 @@ void yee_t(T* ebf, const T* jc, const T* jlo, const Geo& g, const YeeC& c, cudaS
   const dim3 grd((g.ix2 - g.ix1 + YEE_BX) / YEE_BX, (g.jy2 - g.jy1 + YEE_BY) / YEE_BY,
                  g.ndim == 3 ? g.kz2 - g.kz1 + 1 : 1);
   double dt = c.dt, dth = 0.5 * dt;
+  // the comoving frame's advection substeps (curr_and_fields_util.f90:200-258)
+  const bool adv = xa && c.vbeam > 0.0;
+  const int nb1 = g.nc + 1, nb2 = g.nf, ne1 = 1, ne2 = g.nc;
   k_ef_bds<T><<<gf, 256, 0, st>>>(ebf, g, c, 0.0);
+  if (adv) xadvect_t<T>(ebf, g, nb1, nb2, 0, *xa, st, sms);
   if (g.ndim == 3) k_rote_n<T, 3><<<grd, blk, 0, st>>>(ebf, g, c, dth); else k_rote_n<T, 2><<<grd, blk, 0, st>>>(ebf, g, c, dth);
   k_bf_bds<T><<<gf, 256, 0, st>>>(ebf, g, c, dt);
+  if (adv) xadvect_t<T>(ebf, g, ne1, ne2, 0, *xa, st, sms);
   if (g.ndim == 3) k_rotb_j_n<T, 3><<<grd, blk, 0, st>>>(ebf, jc, jlo, g, c, dt); else k_rotb_j_n<T, 2><<<grd, blk, 0, st>>>(ebf, jc, jlo, g, c, dt);
+  if (adv) xadvect_t<T>(ebf, g, ne1, ne2, 2, *xa, st, sms);
   k_ef_bds<T><<<gf, 256, 0, st>>>(ebf, g, c, dt);
   if (g.ndim == 3) k_rote_n<T, 3><<<grd, blk, 0, st>>>(ebf, g, c, dth); else k_rote_n<T, 2><<<grd, blk, 0, st>>>(ebf, g, c, dth);
+  if (adv) xadvect_t<T>(ebf, g, nb1, nb2, 2, *xa, st, sms);
 }
 
 }  // namespace agpu

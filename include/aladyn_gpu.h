@@ -108,6 +108,13 @@ typedef struct agpu_params {
   double djc[3];           /* current normalisation (dx/2,dy/2) or (dx/3,..)      */
   double ompe;             /* 4 pi r_c n0 1e-3                                    */
   double lorentz_fact[4];  /* 1/mass per species                                  */
+  /* w_speed > 0: moving window (lp_window_xshift) every w_sh steps in
+   * [wi_time, wf_time).  w_speed < 0: comoving frame with vbeam = -w_speed
+   * (set_init_param.f90:239-245), FP64 form only: the pushers subtract
+   * dt vbeam from x, the Yee step adds the field_xadvect substeps
+   * (grid_fields.f90:210-324), the envelope uses env_lpf_solve with ib = 0
+   * and every w_sh steps comoving_coordinate (window.f90:227-275) moves the
+   * plasma source left by vbeam w_sh dt, drops x <= gxmin and injects.     */
   double w_speed, wi_time, wf_time;
   double reserved_d[4];
   uint64_t seed;           /* Philox key for ionization draws                     */
@@ -302,8 +309,9 @@ int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t l
  * the complex envelope A of its vector potential (env(:,:,:,1:2) = Re, Im of
  * A^n, env(:,:,:,3:4) = A^{n-1}) advanced by the explicit Maxwell envelope
  * solver, and species 0 feels the wake fields plus the ponderomotive force
- * of |A|^2/2.  FP64 form, one running species, fixed (non-comoving) frame,
- * der_ord 2 or 3, no ionization or second colour. */
+ * of |A|^2/2.  FP64 form, one running species, der_ord 2 or 3, no
+ * ionization or second colour; in the comoving frame (w_speed < 0) the
+ * reduced solver env_lpf_solve (ib = 0) replaces env_maxw_solve. */
 typedef struct agpu_env_params {
   double om0;              /* oml = 2 pi / lam0, the envelope's carrier frequency   */
   double opt_der1;         /* der_ord 3: (4 - nu^2)/3, else 1

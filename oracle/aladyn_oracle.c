@@ -540,6 +540,13 @@ static void ora_push(ora_sim* s, int ic, int64_t np) {
   }
   if (s->p.iform < 2)
     for (int64_t p = 1; p <= np; ++p) PT(s, p, ch) = PART(s, ic, p, ch);
+  /* comoving frame (vbeam = -w_speed > 0): x -= dt vbeam (boris_push.f90:161-166) */
+  const double vbeam = s->p.w_speed < 0.0 ? -s->p.w_speed : 0.0;
+  if (vbeam > 0.)
+    for (int64_t p = 1; p <= np; ++p) {
+      PART(s, ic, p, 1) = PART(s, ic, p, 1) - dt_lp * vbeam;
+      PT(s, p, 1) = PT(s, p, 1) - dt_lp * vbeam;
+    }
 }
 
 /* A9: cell_part_dist(.false.) single domain -> reset_all_part_dist
@@ -590,6 +597,11 @@ static void ora_esirkepov_2d_one(ora_sim* s, double* jc, const double xp1[2], co
   ora_qden_1d(xp0[1], ay0, &jj0);
   ora_qden_1d(xp1[0], ax1, &i);
   ora_qden_1d(xp1[1], ay1, &j);
+  /* a move of more than one node has no window slot: flagged, not deposited */
+  if ((unsigned)(i - ii0 + 1) > 2u || (unsigned)(j - jj0 + 1) > 2u) {
+    s->error_bits |= AGPU_EBIT_INDEX;
+    return;
+  }
   for (int q = 0; q < 5; ++q) axh[q] = 0.;
   int ih = i - ii0 + 1;
   for (int i1 = 0; i1 <= 2; ++i1) axh[ih + i1] = ax1[i1];
@@ -648,6 +660,11 @@ static void ora_esirkepov_3d_one(ora_sim* s, double* jc, const double xp1[3], co
   ora_qden_1d(xp1[0], ax1, &i);
   ora_qden_1d(xp1[1], ay1, &j);
   ora_qden_1d(xp1[2], az1, &k);
+  /* a move of more than one node has no window slot: flagged, not deposited */
+  if ((unsigned)(i - ii0 + 1) > 2u || (unsigned)(j - jj0 + 1) > 2u || (unsigned)(k - kk0 + 1) > 2u) {
+    s->error_bits |= AGPU_EBIT_INDEX;
+    return;
+  }
 
   for (int q = 0; q < 5; ++q) axh[q] = 0.;
   int ih = i - ii0 + 1;
@@ -1352,24 +1369,87 @@ static void ora_rotb(ora_sim* s, double dtf) {
   }
 }
 
+/* field_xadvect (src/fields/grid_fields.f90:210-324), one rank: the x
+   ghosts ix1-1 and ix2+1 copy ix1+1 and ix2, then along each row
+   i = ix1..ix2 either the explicit step f_i - aphx_exp (f_{i+1} - f_{i-1})
+   (isch 0) or the implicit one (isch 2), the tridiagonal solve of
+   aphx_exp (f'_{i+1} - f'_{i-1}) + f'_i = f_i by trid_der1
+   (grid_fields.f90:37-77) with b1 = bn = 1, c1 = an = 0;
+   aphx_exp = v_adv dth dx_inv / 2. */
+static void ora_field_xadvect(ora_sim* s, double dth, double v_adv, int ic1, int ic2, int isch) {
+  const double aphx = dth * s->p.dx_inv;
+  const double aphx_exp = 0.5 * v_adv * aphx;
+  const int i1 = s->ix1, n1p = s->ix2, n = n1p - i1 + 1;
+  for (int ic = ic1; ic <= ic2; ++ic)
+    for (int k = s->kz1; k <= s->kz2; ++k)
+      for (int j = s->jy1; j <= s->jy2; ++j) EBF(s, i1 - 1, j, k, ic) = EBF(s, i1 + 1, j, k, ic);
+  for (int ic = ic1; ic <= ic2; ++ic)
+    for (int k = s->kz1; k <= s->kz2; ++k)
+      for (int j = s->jy1; j <= s->jy2; ++j) EBF(s, n1p + 1, j, k, ic) = EBF(s, n1p, j, k, ic);
+  double* w0 = (double*)malloc(sizeof(double) * (size_t)(n + 2));
+  double* w1 = (double*)malloc(sizeof(double) * (size_t)(n + 2));
+  for (int ic = ic1; ic <= ic2; ++ic)
+    for (int k = s->kz1; k <= s->kz2; ++k)
+      for (int j = s->jy1; j <= s->jy2; ++j) {
+        if (isch == 0) {
+          for (int i = i1; i <= n1p; ++i)
+            w0[i - 2] = EBF(s, i, j, k, ic) - aphx_exp * (EBF(s, i + 1, j, k, ic) - EBF(s, i - 1, j, k, ic));
+        } else {
+          const double a = -aphx_exp, b = 1., c = -a, b1 = 1., c1 = 0.0, an = 0.0, bn = 1.;
+          for (int i = i1; i <= n1p; ++i) w0[i - 2] = EBF(s, i, j, k, ic);
+          w1[1] = 0.0;
+          double bet = b1;
+          w0[1] = w0[1] / bet;
+          int kk = 2;
+          w1[kk] = c1 / bet;
+          bet = b - a * w1[kk];
+          w0[kk] = (w0[kk] - a * w0[kk - 1]) / bet;
+          for (kk = 3; kk <= n - 1; ++kk) {
+            w1[kk] = c / bet;
+            bet = b - a * w1[kk];
+            w0[kk] = (w0[kk] - a * w0[kk - 1]) / bet;
+          }
+          kk = n;
+          w1[kk] = c / bet;
+          bet = bn - an * w1[kk];
+          w0[kk] = (w0[kk] - an * w0[kk - 1]) / bet;
+          for (kk = n - 1; kk >= 1; --kk) w0[kk] = w0[kk] - w1[kk + 1] * w0[kk + 1];
+        }
+        for (int i = i1; i <= n1p; ++i) EBF(s, i, j, k, ic) = w0[i - 2];
+      }
+  free(w0);
+  free(w1);
+}
+
 void ora_advance_fields(ora_sim* s) {
   double dt_lp = s->p.dt;
   double dth = 0.5 * dt_lp;
+  /* comoving frame (vbeam = -w_speed > 0): the advection substeps of
+     advance_lpf_fields (curr_and_fields_util.f90:200-258) */
+  const int comoving = s->p.w_speed < 0.0;
+  const double vbeam = comoving ? -s->p.w_speed : 0.0;
   ora_ef_bds(s, 0.0, 0);
+  if (comoving) ora_field_xadvect(s, dth, -vbeam, s->nc + 1, s->nf, 0);
   ora_rote(s, dth);
   ora_bf_bds(s, dt_lp, 0);
+  if (comoving) ora_field_xadvect(s, dth, -vbeam, 1, s->nc, 0);
   ora_rotb(s, dt_lp);
   for (int ik = 1; ik <= s->nc; ++ik)
     for (int k = s->kz1; k <= s->kz2; ++k)
       for (int j = s->jy1; j <= s->jy2; ++j)
         for (int i = s->ix1; i <= s->ix2; ++i)
           EBF(s, i, j, k, ik) = EBF(s, i, j, k, ik) - s->p.ompe * JC(s, i, j, k, ik);
+  if (comoving) ora_field_xadvect(s, dth, -vbeam, 1, s->nc, 2);
   ora_ef_bds(s, dt_lp, 0);
   ora_rote(s, dth);
+  if (comoving) ora_field_xadvect(s, dth, -vbeam, s->nc + 1, s->nf, 2);
 }
 
 /* Exposed for tests: field-only pieces. */
 void ora_field_bd(ora_sim* s) { ora_field_xyzbd(s, s->nf); }
+void ora_field_xadvect_once(ora_sim* s, double dth, double v_adv, int ic1, int ic2, int isch) {
+  ora_field_xadvect(s, dth, v_adv, ic1, ic2, isch);
+}
 void ora_set_currents(ora_sim* s, const double* jc) {
   memcpy(s->jc, jc, sizeof(double) * (size_t)s->n1p * s->n2p * s->n3p * s->nc);
 }
@@ -1539,6 +1619,38 @@ static int ora_window_xshift(ora_sim* s, int witr, int init_iter, agpu_step_out*
     }
   }
   /* pex1: inject when targ_in <= xmax < targ_end */
+  for (int ic = 0; ic < p->nsp; ++ic) {
+    if (!s->has_src[ic]) continue;
+    if (s->src[ic].x_start <= p->xmax && s->src[ic].x_end > p->xmax) {
+      int64_t a = ora_inject_species(s, ic, p->xmax);
+      if (a < 0) return AGPU_E_CAPACITY;
+      if (out) out->injected[ic] += a;
+    }
+  }
+  return 0;
+}
+
+/* comoving_coordinate (src/dynamics/window.f90:227-275), one rank: the
+   target and the not-yet-injected lattice columns move by -vb w_nst dt (the
+   plasma source's x range here), particles left of the box are dropped
+   (cell_part_dist(.true.)) and the columns that entered are injected. */
+static int ora_comoving_coordinate(ora_sim* s, double vb, int w_nst, int loc_it, agpu_step_out* out) {
+  agpu_params* p = &s->p;
+  if (loc_it == 0) return 0;
+  const double dt_step = p->dt;
+  double dt_tot = 0.0;
+  for (int i = 1; i <= w_nst; ++i) dt_tot = dt_tot + dt_step;
+  for (int ic = 0; ic < p->nsp; ++ic) {
+    if (!s->has_src[ic]) continue;
+    s->src[ic].x_start = s->src[ic].x_start - vb * dt_tot;
+    s->src[ic].x_end = s->src[ic].x_end - vb * dt_tot;
+  }
+  for (int ic = 0; ic < p->nsp; ++ic) {
+    if (s->np[ic] > 0) {
+      int64_t r = ora_reset_dist(s, ic, 1, p->gxmin, p->gxmax, 0);
+      if (out) out->removed[ic] += r;
+    }
+  }
   for (int ic = 0; ic < p->nsp; ++ic) {
     if (!s->has_src[ic]) continue;
     if (s->src[ic].x_start <= p->xmax && s->src[ic].x_end > p->xmax) {
@@ -1900,6 +2012,11 @@ int ora_step(ora_sim* s, int iter, double t, int initial_time, agpu_step_out* ou
   if (p->w_speed > 0.0 && p->w_sh > 0) {
     if (t >= p->wi_time && t < p->wf_time) {
       if (iter % p->w_sh == 0) rc = ora_window_xshift(s, p->w_sh, iter, out);
+    }
+  }
+  if (p->w_speed < 0.0 && p->w_sh > 0) { /* comoving = (w_speed < 0), vbeam = -w_speed */
+    if (t >= p->wi_time && t < p->wf_time) {
+      if (iter % p->w_sh == 0) rc = ora_comoving_coordinate(s, -p->w_speed, p->w_sh, iter, out);
     }
   }
   for (int ic = 0; ic < 4; ++ic) out->np[ic] = s->np[ic];
@@ -2920,6 +3037,71 @@ static void ora_env_bds(ora_sim* s) {
    potential_lapl (1356-1403) and pp_lapl (326-424) build
    S(A) = [D^2 - omp^2 chi] A in av(1:2) and first_ader adds the centred
    x-derivative term; then A^{n+1} from the second-order time scheme. */
+/* env_lpf_solve (src/fields/grid_fields.f90:696-858) with ib = 0, the
+   comoving frame's reduced envelope solver: the transverse Laplacian
+   (pp_lapl) added to the source, times -dt on the row j = jy1 only (the
+   reference's loop `do j = jy1, jy1`), the centred x-derivative of
+   first_der and the three-point inversion of explicit_mat_inv row by row,
+   then A^{n+1} = A^{n-1} + the result. */
+static void ora_env_lpf_solve(ora_sim* s) {
+  const agpu_params* p = &s->p;
+  const int ix1 = s->ix1, ix2 = s->ix2, jy1 = s->jy1, jy2 = s->jy2, kz1 = s->kz1, kz2 = s->kz2;
+  const double om0 = s->ep.om0, dtl = p->dt;
+  const double dhx = p->dx_inv;
+  const double om2 = om0 * om0;
+  const double dx1_inv = 0.5 * p->dx_inv;
+  const double dx_norm = dhx / om0;
+  const double dx2_norm = dx_norm * dx_norm;
+  const double dy2 = p->dy_inv * p->dy_inv, dz2 = p->dz_inv * p->dz_inv;
+  for (int c = 1; c <= 2; ++c)
+    for (int k = kz1; k <= kz2; ++k)
+      for (int j = jy1; j <= jy2; ++j)
+        for (int i = ix1; i <= ix2; ++i)
+          AV(s, i, j, k, c) = AV(s, i, j, k, c) + dy2 * ((ENV(s, i, j + 1, k, c) - ENV(s, i, j, k, c)) -
+                                                        (ENV(s, i, j, k, c) - ENV(s, i, j - 1, k, c)));
+  if (p->ndim == 3)
+    for (int c = 1; c <= 2; ++c)
+      for (int k = kz1; k <= kz2; ++k)
+        for (int j = jy1; j <= jy2; ++j)
+          for (int i = ix1; i <= ix2; ++i)
+            AV(s, i, j, k, c) = AV(s, i, j, k, c) + dz2 * ((ENV(s, i, j, k + 1, c) - ENV(s, i, j, k, c)) -
+                                                          (ENV(s, i, j, k, c) - ENV(s, i, j, k - 1, c)));
+  for (int c = 1; c <= 2; ++c)
+    for (int k = kz1; k <= kz2; ++k)
+      for (int i = ix1; i <= ix2; ++i) AV(s, i, jy1, k, c) = -dtl * AV(s, i, jy1, k, c);
+  const int n = ix2 - ix1 + 1;
+  double* w1 = (double*)malloc(sizeof(double) * (size_t)(n + 2));
+  double* w2 = (double*)malloc(sizeof(double) * (size_t)(n + 2));
+  for (int k = kz1; k <= kz2; ++k)
+    for (int j = jy1; j <= jy2; ++j) {
+      for (int i = ix1; i <= ix2; ++i) {
+        w1[i - 2] = om0 * AV(s, i, j, k, 2) + dx1_inv * (AV(s, i + 1, j, k, 1) - AV(s, i - 1, j, k, 1));
+        w2[i - 2] = -om0 * AV(s, i, j, k, 1) + dx1_inv * (AV(s, i + 1, j, k, 2) - AV(s, i - 1, j, k, 2));
+      }
+      for (int i = ix1; i <= ix2; ++i) {
+        AV(s, i, j, k, 1) = w1[i - 2];
+        AV(s, i, j, k, 2) = w2[i - 2];
+      }
+    }
+  for (int c = 1; c <= 2; ++c)
+    for (int k = kz1; k <= kz2; ++k)
+      for (int j = jy1; j <= jy2; ++j) {
+        for (int i = ix1; i <= ix2; ++i)
+          w1[i - 2] = dx2_norm * (AV(s, i + 1, j, k, c) - 2. * AV(s, i, j, k, c) + AV(s, i - 1, j, k, c));
+        for (int i = ix1; i <= ix2; ++i) AV(s, i, j, k, c) = (AV(s, i, j, k, c) - w1[i - 2]) / om2;
+      }
+  free(w1);
+  free(w2);
+  for (int c = 1; c <= 2; ++c)
+    for (int k = kz1; k <= kz2; ++k)
+      for (int j = jy1; j <= jy2; ++j)
+        for (int i = ix1; i <= ix2; ++i) {
+          AV(s, i, j, k, c) = AV(s, i, j, k, c) + ENV(s, i, j, k, c + 2);
+          ENV(s, i, j, k, c + 2) = ENV(s, i, j, k, c);
+          ENV(s, i, j, k, c) = AV(s, i, j, k, c);
+        }
+}
+
 static void ora_advance_lpf_envelope(ora_sim* s) {
   const agpu_params* p = &s->p;
   const int ix1 = s->ix1, ix2 = s->ix2, jy1 = s->jy1, jy2 = s->jy2, kz1 = s->kz1, kz2 = s->kz2;
@@ -2930,6 +3112,10 @@ static void ora_advance_lpf_envelope(ora_sim* s) {
         AV(s, i, j, k, 1) = -p->ompe * AV(s, i, j, k, 3) * ENV(s, i, j, k, 1);
         AV(s, i, j, k, 2) = -p->ompe * AV(s, i, j, k, 3) * ENV(s, i, j, k, 2);
       }
+  if (p->w_speed < 0.0) { /* comoving: ib = 0 (curr_and_fields_util.f90:276, 292-293) */
+    ora_env_lpf_solve(s);
+    return;
+  }
   const double om0 = s->ep.om0, dtl = p->dt;
   const double dt2 = dtl * dtl;
   const double kfact = om0 * dtl;
@@ -3134,6 +3320,13 @@ static void ora_env_positions(ora_sim* s, int64_t np) {
   }
   if (s->p.iform < 2)
     for (int64_t n = 1; n <= np; ++n) PT(s, n, ch) = PART(s, 0, n, ch);
+  /* comoving frame: x -= dt vbeam (boris_push.f90:288-294) */
+  const double vbeam = s->p.w_speed < 0.0 ? -s->p.w_speed : 0.0;
+  if (vbeam > 0.0)
+    for (int64_t n = 1; n <= np; ++n) {
+      PART(s, 0, n, 1) = PART(s, 0, n, 1) - dt_lp * vbeam;
+      PT(s, n, 1) = PT(s, n, 1) - dt_lp * vbeam;
+    }
 }
 
 int ora_env_run(ora_sim* s, int iter, double t, agpu_step_out* out) {
@@ -3168,6 +3361,11 @@ int ora_env_run(ora_sim* s, int iter, double t, agpu_step_out* out) {
   if (p->w_speed > 0.0 && p->w_sh > 0) {
     if (t >= p->wi_time && t < p->wf_time) {
       if (iter % p->w_sh == 0) rc = ora_window_xshift(s, p->w_sh, iter, out);
+    }
+  }
+  if (p->w_speed < 0.0 && p->w_sh > 0) { /* comoving = (w_speed < 0), vbeam = -w_speed */
+    if (t >= p->wi_time && t < p->wf_time) {
+      if (iter % p->w_sh == 0) rc = ora_comoving_coordinate(s, -p->w_speed, p->w_sh, iter, out);
     }
   }
   for (int ic = 0; ic < 4; ++ic) out->np[ic] = s->np[ic];

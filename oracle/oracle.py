@@ -51,6 +51,7 @@ def load():
         "ora_step": (C.c_int, [P, C.c_int, C.c_double, C.c_int, P]),
         "ora_field_bd": (None, [P]),
         "ora_advance_fields": (None, [P]),
+        "ora_field_xadvect_once": (None, [P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]),
         "ora_curr_fold": (None, [P]),
         "ora_zero_currents": (None, [P]),
         "ora_deposit_move": (None, [P, D, D, C.c_float]),
@@ -133,6 +134,11 @@ class Oracle:
         a = np.asfortranarray(ebf, dtype=np.float64)
         assert a.shape == self.field_shape()
         self.lib.ora_set_fields(self.h, _dp(a))
+
+    def field_xadvect(self, dth, v_adv, ic1, ic2, isch):
+        """One field_xadvect pass (the comoving frame's x advection) on
+        components ic1..ic2 (1-based); isch 0 explicit, 2 implicit."""
+        self.lib.ora_field_xadvect_once(self.h, dth, v_adv, ic1, ic2, isch)
 
     def envar_species(self, ic, pmass):
         """Envar's per-species reductions: (np, ek(1:7), ekmax, psig(1:3), nde(1:100))."""

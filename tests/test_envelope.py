@@ -116,15 +116,11 @@ def numpy_env_grad(p, av):
         gz[I, J, k1:k2 + 1] = p.dz_inv * (F[I, J, k1 + 1:k2 + 2] - F[I, J, k1:k2 + 1])
 
 
-def numpy_vacuum_step(p, ep, env):
-    """One env_run of an empty box: env_bds, S(A) = D^2 A (no plasma: the
-    source -ompe * 0 * A), first_ader, the time combination and the update,
-    env_fields_average and env_grad.  Returns (env, av)."""
-    env = env.copy(order="F")
+def numpy_env_bds(p, E):
+    """env_bds(env, 2, 2) on E(..., 0:2) in place (ib = 0)."""
     nx, ny, nz = p.nx, p.ny, p.nz
     i1, i2, j1, j2 = 2, nx + 1, 2, ny + 1
     k1, k2 = (2, nz + 1) if p.ndim == 3 else (0, 0)
-    E = env
     # env_bds: x copies, then y and z quadratic extrapolation over widened ranges
     for c in range(2):
         for q in (1, 2):
@@ -147,6 +143,17 @@ def numpy_vacuum_step(p, ep, env):
             for q in (1, 2):
                 E[I, J, k1 - q, c] = lo
                 E[I, J, k2 + q, c] = hi
+
+
+def numpy_vacuum_step(p, ep, env):
+    """One env_run of an empty box: env_bds, S(A) = D^2 A (no plasma: the
+    source -ompe * 0 * A), first_ader, the time combination and the update,
+    env_fields_average and env_grad.  Returns (env, av)."""
+    E = env.copy(order="F")
+    numpy_env_bds(p, E)
+    nx, ny, nz = p.nx, p.ny, p.nz
+    i1, i2, j1, j2 = 2, nx + 1, 2, ny + 1
+    k1, k2 = (2, nz + 1) if p.ndim == 3 else (0, 0)
     X, Y, Z = slice(i1, i2 + 1), slice(j1, j2 + 1), slice(k1, k2 + 1)
 
     def sh(a, di=0, dj=0, dk=0):
