@@ -35,6 +35,15 @@ AGPU_EBIT_IONZ_INDEX = 2
 AGPU_EBIT_NONFINITE = 4
 AGPU_EBIT_CAPACITY = 8
 
+# exchange points of a y slab's step (agpu_set_subdomain)
+AGPU_HALO_FIELDS = 1
+AGPU_HALO_PARTICLES = 2
+AGPU_HALO_CURRENTS = 3
+AGPU_HALO_E = 4
+AGPU_HALO_B = 5
+# int hook(void* user, agpu_handle* h, int32_t point, int32_t ic)
+HALO_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32)
+
 
 class AgpuParams(C.Structure):
     _fields_ = [
@@ -225,6 +234,12 @@ SIGNATURES = {
     "agpu_struct_sizes": (C.c_int, [C.POINTER(C.c_int64), C.c_int32]),
     "agpu_field_diag_noalloc": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                           C.c_double, _P, _P]),
+    "agpu_set_subdomain": (C.c_int, [_P, C.c_int32, C.c_int32, HALO_FN, _P]),
+    "agpu_halo_size": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
+    "agpu_halo_pack": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P]),
+    "agpu_halo_unpack": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int32]),
+    "agpu_halo_emigrants": (C.c_int, [_P, C.c_int32, C.c_int32, _P, C.c_int64, C.POINTER(C.c_int64)]),
+    "agpu_halo_immigrants": (C.c_int, [_P, C.c_int32, _P, C.c_int64, C.c_int64]),
 }
 
 _lib = None

@@ -89,6 +89,12 @@ struct agpu_handle {
   double* env_den = nullptr;
   agpu_env_params ep{};
   long long env_steps = 0;  // env_run calls so far (the record sort period)
+  // a slab of a y decomposition (agpu_set_subdomain): shared sides and the
+  // host's exchange hook
+  bool dd = false;
+  int dd_lo = 0, dd_hi = 0;
+  agpu_halo_fn halo_fn = nullptr;
+  void* halo_user = nullptr;
   // comoving frame (w_speed < 0): the field advection's scratch
   double* xadv_tmp = nullptr;
   double* xadv_coef = nullptr;  // bet[0..nx+1], then w1[0..nx+1]
@@ -323,9 +329,24 @@ long long lattice_columns_end(const agpu_handle* h, int ic, long long i1, double
 }
 
 int drop_removed(agpu_handle* h, int ic);
+int compact_species(agpu_handle* h, int ic, bool window);
 
 int add_lattice_columns(agpu_handle* h, int ic, long long i1, long long i2) {
-  long long n = (i2 - i1 + 1) * (long long)h->npty[ic] * h->nptz[ic];
+  // lattice rows j1r .. j1r+nrow-1: all of them, or for a y slab those whose
+  // jittered y, y_min + (j - 1/2 + u) dyl with |u| <= 1/2, can fall inside
+  // (gymin, gymax], plus one row of margin on each side
+  int j1r = 1, nrow = h->npty[ic];
+  if (h->dd) {
+    const double dyl = h->p.dy / (double)h->src[ic].npy;
+    const double y_min = h->src[ic].y_min;
+    long long lo = (long long)std::floor((h->p.gymin - y_min) / dyl);
+    long long hi = (long long)std::ceil((h->p.gymax - y_min) / dyl) + 1;
+    if (lo < 1) lo = 1;
+    if (hi > h->npty[ic]) hi = h->npty[ic];
+    j1r = (int)lo;
+    nrow = hi >= lo ? (int)(hi - lo + 1) : 0;
+  }
+  long long n = (i2 - i1 + 1) * (long long)nrow * h->nptz[ic];
   if (n <= 0) return 0;
   if (int rc = drop_removed(h, ic)) return rc;
   if (h->np[ic] + n > h->cap[ic]) {
@@ -336,7 +357,8 @@ int add_lattice_columns(agpu_handle* h, int ic, long long i1, long long i2) {
   LatticeArgs a;
   a.ndim = h->p.ndim;
   a.ic = ic;
-  a.npty = h->npty[ic];
+  a.npty = nrow;
+  a.j0 = j1r;
   a.nptz = h->nptz[ic];
   a.i1 = i1;
   a.i2 = i2;
@@ -358,6 +380,14 @@ int add_lattice_columns(agpu_handle* h, int ic, long long i1, long long i2) {
     lattice64(a, h->part[ic], h->cap[ic], h->np[ic], h->st, h->sms);
   CK(cudaGetLastError());
   h->timers.launches_total += 1;
+  if (h->dd) {
+    // a slab keeps the lattice particles of its own rows: the columns span
+    // the whole source, as in one box, and the rest is dropped here
+    h->np[ic] += n;
+    h->nalive[ic] = h->np[ic];
+    h->binned[ic] = false;
+    return compact_species(h, ic, false);
+  }
   h->np[ic] += n;
   h->nalive[ic] += n;
   h->binned[ic] = false;
@@ -416,7 +446,7 @@ int compact_species(agpu_handle* h, int ic, bool window) {
 // The FP64 tile kernel has the reference's quadratic shapes only; the cubic
 // FP64 form runs the per-particle kernels.
 bool tiled(const agpu_handle* h, int ic) {
-  return !h->deterministic && ic < h->p.nsp_run && h->key[ic] != nullptr &&
+  return !h->deterministic && !h->dd && ic < h->p.nsp_run && h->key[ic] != nullptr &&
          (h->fp32 || (h->p.shape == AGPU_SHAPE_QUADRATIC && h->p.iform < 2));
 }
 
@@ -1608,6 +1638,7 @@ int agpu_x_step_many(agpu_handle** hs, int32_t n, agpu_x_ws* w) {
 
 int agpu_set_step_graphs(agpu_handle* h, int32_t on) {
   if (!h) return AGPU_E_ARG;
+  if (on && h->dd) return AGPU_E_STATE;  // a slab's exchanges run between the kernels
   h->use_graph = on != 0;
   if (!h->use_graph && h->gexec) {
     cudaStreamSynchronize(h->st);
@@ -1616,6 +1647,13 @@ int agpu_set_step_graphs(agpu_handle* h, int32_t on) {
   }
   return 0;
 }
+
+// The host's exchange at one point of a y slab's step (no-op otherwise).
+static int halo_call(agpu_handle* h, int point, int ic) {
+  if (!h->dd || !h->halo_fn) return 0;
+  return h->halo_fn(h->halo_user, h, point, ic);
+}
+static int yee_halo(void* ctx, int point) { return halo_call((agpu_handle*)ctx, point, -1); }
 
 static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_time, agpu_step_out* out) {
   if (!h) return AGPU_E_ARG;
@@ -1640,6 +1678,7 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
   else field_bd64(Dev64{h->g, h->ebf, h->jc}, h->st, h->sms);
   CK(cudaGetLastError());
   h->timers.launches_total += (p.ndim == 3) ? 3 : 2;
+  if (int rc_ = halo_call(h, AGPU_HALO_FIELDS, -1)) return rc_;
   ph_end(h, PH_YEE);
   // ionization
   if (p.ionz_lev > 0) {
@@ -1657,7 +1696,11 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
   }
   for (int ic = 0; ic < p.nsp_run; ++ic) {
     long long np = h->np[ic];
-    if (np <= 0) continue;
+    if (np <= 0) {
+      // an empty slab still takes part in the particle exchange
+      if (int rc_ = halo_call(h, AGPU_HALO_PARTICLES, ic)) return rc_;
+      continue;
+    }
     if (tiled(h, ic)) {
       if (int rc_ = tiled_push(h, ic, initial_time, out)) return rc_;
       if (sort_step(h, iter))
@@ -1731,6 +1774,8 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
       a.initial = initial_time ? 1 : 0;
       a.shape = p.shape;
       a.iform = p.iform;
+      a.dd_ylo = h->dd_lo;
+      a.dd_yhi = h->dd_hi;
       a.removed = &h->d_cnt->removed;
       a.err = &h->d_cnt->err;
       push_deposit64(a, h->st, h->sms, h->deterministic);
@@ -1741,6 +1786,9 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
     h->timers.launches_total += 1;
     h->timers.pushes += np;
     if (int rc_ = read_counters(h)) return rc_;
+    // a y slab: the particles that crossed a shared side go to the
+    // neighbours (the host's hook), the ones that arrive are appended
+    if (int rc_ = halo_call(h, AGPU_HALO_PARTICLES, ic)) return rc_;
     if (h->h_cnt->removed > 0) {
       ph_begin(h, PH_SORT);
       long long before = h->np[ic];
@@ -1768,12 +1816,15 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
     }
   } else {
     Dev64 d{h->g, h->ebf, h->jc};
+    if (int rc_ = halo_call(h, AGPU_HALO_CURRENTS, -1)) return rc_;
     jfold64(d, h->st, h->sms);
     if (fused) {
       yee64_fused(h->ebf, h->ebf_alt, h->jc, h->g, c, h->st);
       std::swap(h->ebf, h->ebf_alt);
     } else {
-      yee64(d, c, h->st, h->sms, h->xadv.tmp ? &h->xadv : nullptr);
+      YeeHook hk{yee_halo, h, 0};
+      yee64(d, c, h->st, h->sms, h->xadv.tmp ? &h->xadv : nullptr, h->dd ? &hk : nullptr);
+      if (hk.rc) return hk.rc;
     }
   }
   CK(cudaGetLastError());
@@ -1791,6 +1842,97 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
   out->xmn = p.xmn;
   out->error_bits = h->error_bits;
   if (h->error_bits & AGPU_EBIT_CAPACITY) return AGPU_E_CAPACITY;
+  return 0;
+}
+
+// ---- domain decomposition in y ---------------------------------------------
+int agpu_set_subdomain(agpu_handle* h, int32_t lo_shared, int32_t hi_shared, agpu_halo_fn fn, void* user) {
+  if (!h) return AGPU_E_ARG;
+  const agpu_params& p = h->p;
+  const bool any = lo_shared || hi_shared;
+  if (any) {
+    // FP64 form, quadratic shapes, fixed frame, no envelope
+    if (h->fp32 || p.shape != AGPU_SHAPE_QUADRATIC || p.w_speed < 0.0 || h->env) return AGPU_E_ARG;
+    if (!fn) return AGPU_E_ARG;
+    if (p.ny < 3) return AGPU_E_ARG;  // the exchanges move up to 3 rows
+  }
+  if (int rc = agpu_synchronize(h)) return rc;
+  h->dd = any;
+  h->dd_lo = lo_shared ? 1 : 0;
+  h->dd_hi = hi_shared ? 1 : 0;
+  h->halo_fn = any ? fn : nullptr;
+  h->halo_user = any ? user : nullptr;
+  if (any) {
+    // the exchanges run between the kernels of a step: plain launches only
+    agpu_set_step_graphs(h, 0);
+    h->fused_yee = false;
+    for (int ic = 0; ic < 4; ++ic) h->binned[ic] = false;
+  }
+  return 0;
+}
+
+int agpu_halo_size(agpu_handle* h, int32_t ncomp, int32_t nrows, int64_t* n) {
+  if (!h || !n || ncomp < 0 || nrows < 0) return AGPU_E_ARG;
+  *n = (int64_t)ncomp * nrows * h->g.n1p * h->g.n3p;
+  return 0;
+}
+
+static int halo_args(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32_t j1, int32_t nrows, double** f) {
+  if (!h || h->fp32 || (what != 0 && what != 1)) return AGPU_E_ARG;
+  const int nmax = what == 0 ? h->g.nf : h->g.nc;
+  if (ic1 < 1 || ic2 < ic1 || ic2 > nmax || nrows < 0 || j1 < 1 || j1 + nrows - 1 > h->g.n2p) return AGPU_E_ARG;
+  *f = what == 0 ? h->ebf : h->jc;
+  return 0;
+}
+
+int agpu_halo_pack(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32_t j1, int32_t nrows, double* buf) {
+  double* f = nullptr;
+  if (int rc = halo_args(h, what, ic1, ic2, j1, nrows, &f)) return rc;
+  if (!buf) return AGPU_E_ARG;
+  halo_rows64(f, h->g, ic1 - 1, ic2 - ic1 + 1, j1, nrows, buf, 0, h->st, h->sms);
+  CK(cudaGetLastError());
+  h->timers.launches_total += 1;
+  return 0;
+}
+
+int agpu_halo_unpack(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32_t j1, int32_t nrows,
+                     const double* buf, int32_t mode) {
+  double* f = nullptr;
+  if (int rc = halo_args(h, what, ic1, ic2, j1, nrows, &f)) return rc;
+  if (mode < 0 || mode > 2 || (mode < 2 && !buf)) return AGPU_E_ARG;
+  halo_rows64(f, h->g, ic1 - 1, ic2 - ic1 + 1, j1, nrows, const_cast<double*>(buf), mode + 1, h->st, h->sms);
+  CK(cudaGetLastError());
+  h->timers.launches_total += 1;
+  return 0;
+}
+
+int agpu_halo_emigrants(agpu_handle* h, int32_t ic, int32_t side, double* buf, int64_t ld, int64_t* n) {
+  if (!h || h->fp32 || ic < 0 || ic >= h->p.nsp || (side != 0 && side != 1) || !n || ld < 0 || (ld > 0 && !buf))
+    return AGPU_E_ARG;
+  *n = 0;
+  if (h->np[ic] <= 0) return 0;
+  const agpu_params& p = h->p;
+  BoxBounds b{p.gxmin, p.gxmax, p.gymin, p.gymax, p.gzmin, p.gzmax, 1, p.ndim == 3 ? 1 : 0};
+  long long cnt = emigrants64(h->part[ic], h->cap[ic], h->np[ic], h->ndv, b, side, buf, ld, h->scr, h->st);
+  CK(cudaGetLastError());
+  h->timers.launches_total += 3;
+  *n = cnt;
+  return cnt > ld ? AGPU_E_CAPACITY : 0;
+}
+
+int agpu_halo_immigrants(agpu_handle* h, int32_t ic, const double* buf, int64_t ld, int64_t n) {
+  if (!h || h->fp32 || ic < 0 || ic >= h->p.nsp || n < 0 || (n > 0 && (!buf || ld < n))) return AGPU_E_ARG;
+  if (n == 0) return 0;
+  if (int rc = drop_removed(h, ic)) return rc;
+  if (h->np[ic] + n > h->cap[ic]) {
+    h->error_bits |= AGPU_EBIT_CAPACITY;
+    return AGPU_E_CAPACITY;
+  }
+  CK(cudaMemcpy2DAsync(h->part[ic] + h->np[ic], sizeof(double) * h->cap[ic], buf, sizeof(double) * ld, sizeof(double) * n,
+                       h->ndv, cudaMemcpyDeviceToDevice, h->st));
+  h->np[ic] += n;
+  h->nalive[ic] = h->np[ic];
+  h->binned[ic] = false;
   return 0;
 }
 
@@ -1834,6 +1976,7 @@ int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t l
 // ---- envelope cycle (Env_cycle, src/ALaDyn.F90:111-130) -------------------
 int agpu_env_enable(agpu_handle* h, const agpu_env_params* ep) {
   if (!h || !ep || h->fp32 || (ep->der_ord != 2 && ep->der_ord != 3) || !(ep->om0 > 0.0)) return AGPU_E_ARG;
+  if (h->dd) return AGPU_E_STATE;  // the envelope cycle runs on one box
   const Geo& g = h->g;
   if (g.ix2 - g.ix1 < 3 || g.jy2 - g.jy1 < 2 || (g.ndim == 3 && g.kz2 - g.kz1 < 2)) return AGPU_E_ARG;
   CK(cudaStreamSynchronize(h->st));
@@ -2289,6 +2432,7 @@ int agpu_set_sort_interval(agpu_handle* h, int32_t steps) {
 }
 int agpu_set_fused_yee(agpu_handle* h, int32_t on) {
   if (!h) return AGPU_E_ARG;
+  if (on && h->dd) return AGPU_E_STATE;
   h->fused_yee = on != 0;
   return 0;
 }

@@ -195,6 +195,19 @@ __device__ bool esirkepov_cubic64(const Geo& g, double* jc, const double* xn, co
 // per particle the arithmetic is identical, and a particle that leaves the
 // box is exactly one that the reference removes before its deposit.
 // ============================================================================
+
+// A slab of a y decomposition: a particle that left through a y side shared
+// with a neighbour but stays inside the x and z box moves to that neighbour
+// (part_prl_exchange).  The reference deposits it there, from its old
+// position in the neighbour's ghost rows; here the slab it leaves deposits
+// it into its own ghost rows, which the current exchange then adds to the
+// neighbour's rows: the same terms on the same nodes.
+__device__ __forceinline__ bool emigrant(const PushArgs64& a, double x, double y, double z) {
+  if (!((a.dd_ylo && y <= a.gymin) || (a.dd_yhi && y > a.gymax))) return false;
+  if (!(x > a.gxmin && x <= a.gxmax)) return false;
+  return a.g.ndim < 3 || (z > a.gzmin && z <= a.gzmax);
+}
+
 template <bool SERIAL, int SHAPE>
 __global__ void __launch_bounds__(256) k64_push_dep_3d(PushArgs64 a) {
   const Geo g = a.g;
@@ -333,7 +346,7 @@ __global__ void __launch_bounds__(256) k64_push_dep_3d(PushArgs64 a) {
     if (!keep) {
       a.flag[n] = 1;
       atomicAdd(a.removed, 1ull);
-      continue;
+      if (!emigrant(a, xnew, ynew, znew)) continue;
     }
     double xn[3] = {a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn), a.dz_inv * (znew - a.zmn)};
     float wght = (float)slot_charge(sl) * slot_wgh(sl);
@@ -452,7 +465,7 @@ __global__ void __launch_bounds__(256) k64_push_dep_2d(PushArgs64 a) {
     if (!keep) {
       a.flag[n] = 1;
       atomicAdd(a.removed, 1ull);
-      continue;
+      if (!emigrant(a, xnew, ynew, 0.)) continue;
     }
     float wght = (float)slot_charge(sl) * slot_wgh(sl);
     if (SHAPE != AGPU_SHAPE_CUBIC && a.iform == 2) {
@@ -490,8 +503,8 @@ void push_deposit64(const PushArgs64& a, cudaStream_t st, int sms, bool serial) 
 
 void jfold64(const Dev64& d, cudaStream_t st, int sms) { jfold_t<double>(d.jc, d.g, st, sms); }
 
-void yee64(const Dev64& d, const YeeC& c, cudaStream_t st, int sms, const XAdv* xa) {
-  yee_t<double>(d.ebf, d.jc, (const double*)nullptr, d.g, c, st, sms, xa);
+void yee64(const Dev64& d, const YeeC& c, cudaStream_t st, int sms, const XAdv* xa, YeeHook* hk) {
+  yee_t<double>(d.ebf, d.jc, (const double*)nullptr, d.g, c, st, sms, xa, hk);
 }
 void yee64_fused(const double* fin, double* fout, const double* jc, const Geo& g, const YeeC& c, cudaStream_t st) {
   yee_fused_t<double>(fin, fout, jc, (const double*)nullptr, g, c, st);

@@ -23,6 +23,14 @@ struct XAdv {
   const double* w1;
   double a, aphx_exp;
 };
+// A slab of a y decomposition: the host's exchange, called between the
+// Yee sweeps with the point (AGPU_HALO_E after each ef_bds, AGPU_HALO_B after
+// bf_bds); a non-zero return is kept in rc and the sweeps stop.
+struct YeeHook {
+  int (*fn)(void* ctx, int point);
+  void* ctx;
+  int rc;
+};
 }  // namespace agpu
 
 namespace agpu {
@@ -50,6 +58,9 @@ struct PushArgs64 {
   int initial;
   int shape;  // AGPU_SHAPE_QUADRATIC or AGPU_SHAPE_CUBIC
   int iform;  // 0, 1: Esirkepov; 2: the non-conserving ncdef deposit
+  // y sides shared with a neighbouring slab: a particle that leaves through
+  // one (and stays in the x and z box) still deposits its current here
+  int dd_ylo = 0, dd_yhi = 0;
   unsigned long long* removed;
   unsigned int* err;
 };
@@ -73,7 +84,7 @@ struct IonArgs64 {
 void field_bd64(const Dev64& d, cudaStream_t st, int sms);
 void push_deposit64(const PushArgs64& a, cudaStream_t st, int sms, bool serial);
 void jfold64(const Dev64& d, cudaStream_t st, int sms);
-void yee64(const Dev64& d, const YeeC& c, cudaStream_t st, int sms, const XAdv* xa = nullptr);
+void yee64(const Dev64& d, const YeeC& c, cudaStream_t st, int sms, const XAdv* xa = nullptr, YeeHook* hk = nullptr);
 // the whole leapfrog step in one z-streaming kernel, fin -> fout (fout != fin)
 void yee64_fused(const double* fin, double* fout, const double* jc, const Geo& g, const YeeC& c, cudaStream_t st);
 __global__ void k64_ion_efield(IonArgs64 a);

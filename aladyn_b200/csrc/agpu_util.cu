@@ -45,6 +45,60 @@ long long compact64(double* part, double* tmp, long long cap, long long np, int 
   return kept;
 }
 
+__global__ void k_halo_rows64(double* f, Geo g, int c0, int ncomp, int j1, int nrows, double* buf, int mode) {
+  const long long n1p = g.n1p, n3p = g.n3p;
+  const long long total = (long long)ncomp * n3p * nrows * n1p;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const long long i = t % n1p;
+    const long long r = (t / n1p) % nrows;
+    const long long k = (t / (n1p * nrows)) % n3p;
+    const long long c = t / (n1p * nrows * n3p);
+    double* v = f + g.ncell * (c0 + c) + i + n1p * ((j1 - 1 + r) + (long long)g.n2p * k);
+    if (mode == 0) buf[t] = *v;
+    else if (mode == 1) *v = buf[t];
+    else if (mode == 2) *v = *v + buf[t];
+    else *v = 0.0;
+  }
+}
+void halo_rows64(double* f, const Geo& g, int c0, int ncomp, int j1, int nrows, double* buf, int mode, cudaStream_t st,
+                 int sms) {
+  const long long total = (long long)ncomp * g.n3p * nrows * g.n1p;
+  if (total <= 0) return;
+  k_halo_rows64<<<grid_for(total, 256, sms, 8), 256, 0, st>>>(f, g, c0, ncomp, j1, nrows, buf, mode);
+}
+
+struct Emigrant64 {
+  const double *x, *y, *z;
+  BoxBounds b;
+  int side;
+  __device__ bool operator()(long long i) const {
+    const double a = x[i], c = y[i];
+    bool k = a > b.x0 && a <= b.x1;
+    if (b.use_z) {
+      const double d = z[i];
+      k = k && d > b.z0 && d <= b.z1;
+    }
+    return k && (side == 0 ? c <= b.y0 : c > b.y1);
+  }
+};
+struct MoveColsOut64 {
+  const double* src;
+  long long src_ld;
+  double* dst;
+  long long dst_ld;
+  int ndv;
+  __device__ void operator()(long long i, long long o) const {
+    if (o >= dst_ld) return;
+    for (int c = 0; c < ndv; ++c) dst[(long long)c * dst_ld + o] = src[(long long)c * src_ld + i];
+  }
+};
+long long emigrants64(const double* part, long long cap, long long np, int ndv, const BoxBounds& b, int side, double* out,
+                      long long ld, Scratch& s, cudaStream_t st) {
+  Emigrant64 pr{part, part + cap, part + 2 * cap, b, side};
+  MoveColsOut64 mv{part, cap, out, ld, ndv};
+  return select_run(pr, mv, np, s, st);
+}
+
 // Split form: x_loc = (ix - 3) + ox; keep 0 < x_loc <= nx along each axis,
 // evaluated exactly from the integer node and the offset in [-0.5, 0.5).
 struct InBox32 {
@@ -244,7 +298,7 @@ __global__ void k_lattice64(LatticeArgs a, double* part, long long ld, long long
   uint64_t sl = make_slot(a.charge, a.part_ind, a.wgh);
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
     long long ix = a.i1 + q % ncol;
-    int j = 1 + (int)((q / ncol) % a.npty);
+    int j = a.j0 + (int)((q / ncol) % a.npty);
     int k = 1 + (int)(q / (ncol * a.npty));
     double x, y, z;
     lattice_pos(a, ix, j, k, &x, &y, &z);
@@ -285,7 +339,7 @@ __global__ void k_lattice32(LatticeArgs a, Part32View p, long long n0, Geo g, do
   uint64_t sl = make_slot(a.charge, a.part_ind, a.wgh);
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
     long long ix = a.i1 + q % ncol;
-    int j = 1 + (int)((q / ncol) % a.npty);
+    int j = a.j0 + (int)((q / ncol) % a.npty);
     int k = 1 + (int)(q / (ncol * a.npty));
     double x, y, z;
     lattice_pos(a, ix, j, k, &x, &y, &z);

@@ -33,6 +33,7 @@ struct Part32View {
 
 struct LatticeArgs {
   int ndim, ic, npty, nptz;
+  int j0;  // first lattice row generated (1 for the whole source; a y slab's first row)
   long long i1, i2;
   int charge, part_ind;
   float wgh;
@@ -50,6 +51,17 @@ struct LaserArgs {
 
 long long compact64(double* part, double* tmp, long long cap, long long np, int ndv, const BoxBounds& b, Scratch& s,
                     cudaStream_t st);
+// A y slab's halo rows: copy rows j1 .. j1+nrows-1 of components
+// c0 .. c0+ncomp-1 (0-based) of f, every x and z node, to or from buf
+// ([component][z][row][x]); mode 0 pack (f -> buf), 1 write, 2 add, 3 zero.
+void halo_rows64(double* f, const Geo& g, int c0, int ncomp, int j1, int nrows, double* buf, int mode, cudaStream_t st,
+                 int sms);
+// Records of a slab that left through its low (side 0) or high (side 1)
+// y side and stayed in the x and z box b, in order, into out (leading
+// dimension ld; records beyond ld are counted, not written).  Returns the
+// count.
+long long emigrants64(const double* part, long long cap, long long np, int ndv, const BoxBounds& b, int side, double* out,
+                      long long ld, Scratch& s, cudaStream_t st);
 long long compact32(const Part32View& src, const Part32View& dst, long long np, int n1p, int n2p, int nx, int ny, int nz,
                     int use_y, int use_z, Scratch& s, cudaStream_t st);
 long long compact_flag64(const int* key, int dead, double* part, double* tmp, long long cap, long long np, int ndv, Scratch& s,

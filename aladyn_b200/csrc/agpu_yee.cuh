@@ -482,10 +482,11 @@ void xadvect_t(T* ebf, const Geo& g, int ic1, int ic2, int isch, const XAdv& x, 
   }
 }
 
-// xa: the comoving frame's advection scratch (c.vbeam > 0), else null
+// xa: the comoving frame's advection scratch (c.vbeam > 0), else null;
+// hk: a y slab's halo exchange after each boundary sweep, else null
 template <typename T>
 void yee_t(T* ebf, const T* jc, const T* jlo, const Geo& g, const YeeC& c, cudaStream_t st, int sms,
-           const XAdv* xa = nullptr) {
+           const XAdv* xa = nullptr, YeeHook* hk = nullptr) {
   long long faces = (long long)(g.jy2 - g.jy1 + 1) * (g.kz2 - g.kz1 + 1) + (long long)(g.ix2 - g.ix1 + 1) * (g.kz2 - g.kz1 + 1) +
                     (g.ndim == 3 ? (long long)(g.ix2 - g.ix1 + 1) * (g.jy2 - g.jy1 + 1) : 0);
   int gf = grid_for(faces, 256, sms);
@@ -496,14 +497,21 @@ void yee_t(T* ebf, const T* jc, const T* jlo, const Geo& g, const YeeC& c, cudaS
   // the comoving frame's advection substeps (curr_and_fields_util.f90:200-258)
   const bool adv = xa && c.vbeam > 0.0;
   const int nb1 = g.nc + 1, nb2 = g.nf, ne1 = 1, ne2 = g.nc;
+  auto halo = [&](int point) {
+    if (hk && !hk->rc) hk->rc = hk->fn(hk->ctx, point);
+    return hk && hk->rc;
+  };
   k_ef_bds<T><<<gf, 256, 0, st>>>(ebf, g, c, 0.0);
+  if (halo(AGPU_HALO_E)) return;
   if (adv) xadvect_t<T>(ebf, g, nb1, nb2, 0, *xa, st, sms);
   if (g.ndim == 3) k_rote_n<T, 3><<<grd, blk, 0, st>>>(ebf, g, c, dth); else k_rote_n<T, 2><<<grd, blk, 0, st>>>(ebf, g, c, dth);
   k_bf_bds<T><<<gf, 256, 0, st>>>(ebf, g, c, dt);
+  if (halo(AGPU_HALO_B)) return;
   if (adv) xadvect_t<T>(ebf, g, ne1, ne2, 0, *xa, st, sms);
   if (g.ndim == 3) k_rotb_j_n<T, 3><<<grd, blk, 0, st>>>(ebf, jc, jlo, g, c, dt); else k_rotb_j_n<T, 2><<<grd, blk, 0, st>>>(ebf, jc, jlo, g, c, dt);
   if (adv) xadvect_t<T>(ebf, g, ne1, ne2, 2, *xa, st, sms);
   k_ef_bds<T><<<gf, 256, 0, st>>>(ebf, g, c, dt);
+  if (halo(AGPU_HALO_E)) return;
   if (g.ndim == 3) k_rote_n<T, 3><<<grd, blk, 0, st>>>(ebf, g, c, dth); else k_rote_n<T, 2><<<grd, blk, 0, st>>>(ebf, g, c, dth);
   if (adv) xadvect_t<T>(ebf, g, nb1, nb2, 2, *xa, st, sms);
 }

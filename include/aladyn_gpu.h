@@ -507,6 +507,67 @@ int agpu_set_sort_interval(agpu_handle* h, int32_t steps);
  * binding can check its struct layouts against the library's. */
 int agpu_struct_sizes(int64_t* sizes, int32_t n);
 
+/* ---- domain decomposition in y ------------------------------------------ */
+/* One simulation split into slabs of rows along y, one handle per slab (one
+ * process per GPU, or several handles of one process): the reference's
+ * nprocy decomposition (src/parallel/parallel.F90:75-140) with npe_z = 1.
+ * Each handle is created with its slab's params: ny = the slab's interior
+ * rows, ymn = gymin = y of its first row, gymax = y after its last row (the
+ * loc_ygrid bounds), everything else global.  The exchanges the reference
+ * makes by MPI inside the step are handed to the caller's hook, which moves
+ * the packed rows between neighbours (NCCL, CUDA-aware MPI, device copies)
+ * with the pack/unpack calls below, ordered on the handle's stream:
+ *   AGPU_HALO_FIELDS    after field_xyzbd, before the gather: all nfield
+ *                       components (pfields_prepare, fill_ebfield_yzxbdsdata
+ *                       with 2 + 2 rows, curr_and_fields_util.f90:156-174);
+ *   AGPU_HALO_PARTICLES after the push of species ic: particles that crossed
+ *                       a shared side have deposited their current here and
+ *                       leave (part_prl_exchange, mpi_part_interface.f90:
+ *                       246-466); agpu_halo_emigrants / agpu_halo_immigrants;
+ *   AGPU_HALO_CURRENTS  after the deposit, before jc_xyzbd: ghost rows of jc
+ *                       summed into the neighbours' rows (fill_curr_yzxbdsdata,
+ *                       mpi_curr_interface.f90:51-159, 2 rows down, 3 up);
+ *   AGPU_HALO_E         in the Yee step after each ef_bds: E components
+ *                       (1 row up, 2 rows down, curr_and_fields_util.f90:
+ *                       186-193, 241-247);
+ *   AGPU_HALO_B         after bf_bds: B components (2 rows up, 1 row down,
+ *                       curr_and_fields_util.f90:209-215).
+ * Rows move whole: every x and z node of the array, ghosts included, so a
+ * slab sees its neighbour's boundary values exactly as one box would.  A
+ * non-zero return from the hook ends the step with that code.  Supported in
+ * the FP64 form with quadratic shapes and the fixed frame (no envelope);
+ * the slab handle uses the per-particle kernels, no step graphs and no
+ * fused Yee. */
+#define AGPU_HALO_FIELDS 1
+#define AGPU_HALO_PARTICLES 2
+#define AGPU_HALO_CURRENTS 3
+#define AGPU_HALO_E 4
+#define AGPU_HALO_B 5
+typedef int (*agpu_halo_fn)(void* user, agpu_handle* h, int32_t point, int32_t ic);
+/* lo_shared / hi_shared: the slab's low / high y side borders another slab
+ * (0: a physical boundary, handled as in one box). */
+int agpu_set_subdomain(agpu_handle* h, int32_t lo_shared, int32_t hi_shared, agpu_halo_fn fn, void* user);
+/* Elements of a block of nrows full rows of ncomp components:
+ * ncomp * nrows * n1p * n3p doubles, ordered [component][z][row][x]. */
+int agpu_halo_size(agpu_handle* h, int32_t ncomp, int32_t nrows, int64_t* n);
+/* Copy rows j1 .. j1+nrows-1 (1-based local rows, ghosts included) of
+ * components ic1..ic2 (1-based) of the fields (what = 0) or the currents
+ * (what = 1) into the device buffer buf, on the handle's stream. */
+int agpu_halo_pack(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32_t j1, int32_t nrows, double* buf);
+/* The reverse: mode 0 writes buf into the rows, 1 adds it, 2 zeroes the
+ * rows (buf unused). */
+int agpu_halo_unpack(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32_t j1, int32_t nrows,
+                     const double* buf, int32_t mode);
+/* Copy the records of species ic that left through the low (side 0) or
+ * high (side 1) y side and stayed inside the x and z box, in their order,
+ * into the device buffer buf (ndv columns of leading dimension ld); *n =
+ * their count (at most ld, else AGPU_E_CAPACITY).  Call it at
+ * AGPU_HALO_PARTICLES; the step drops them afterwards. */
+int agpu_halo_emigrants(agpu_handle* h, int32_t ic, int32_t side, double* buf, int64_t ld, int64_t* n);
+/* Append n records from a device buffer (ndv columns, leading dimension ld)
+ * to species ic. */
+int agpu_halo_immigrants(agpu_handle* h, int32_t ic, const double* buf, int64_t ld, int64_t n);
+
 #ifdef __cplusplus
 }
 #endif
