@@ -33,8 +33,12 @@ def _run(ndim, precision, steps=8):
 
 @pytest.mark.parametrize("ndim", [2, 3])
 @pytest.mark.parametrize("precision,tol", [(AGPU_FP64, 1e-12), (AGPU_FP32_SPLIT, 1e-6)])
-def test_diag_sums(ndim, precision, tol):
-    p, dev = _run(ndim, precision)
+@pytest.mark.parametrize("steps", [8, 11, 12])
+def test_diag_sums(ndim, precision, tol, steps):
+    """After 8 and 12 steps removed records of the last pushes are still
+    stored behind the alive ones; after 11 the last step shifted the window
+    (removal and injection after the push)."""
+    p, dev = _run(ndim, precision, steps)
     d = dev.diag()
     s = dev.get_species(0)
     f = dev.get_fields()
