@@ -77,3 +77,40 @@ def test_fp32_split_ionization_statistics():
     q32, _, _ = unpack_slot(dev.get_species(1)[:, -1])
     q64, _, _ = unpack_slot(ora.get_species(1)[:, -1])
     assert abs(int(q32.astype(np.int64).sum()) - int(q64.astype(np.int64).sum())) <= 0.03 * int(q64.sum())
+
+
+@pytest.mark.parametrize("dopant", [0.005, 0.01])
+def test_fp32_split_ionization_binomial_bound(dopant):
+    """The split form against the FP64 oracle on a larger box at the C4
+    workload's dopant fractions (0.5% and 1% of the electron density), with a
+    bound tied to the count: each ion's ionization is a Bernoulli draw, so a
+    total of n new electrons has a variance of at most n; the two runs draw
+    independently (their records are ordered differently), so
+    |n32 - n64| <= 5 sqrt(2 n64) unless the FP32 gather biases the rates."""
+    kw = dict(nx=96, ny=32, nz=24, cap=1_200_000, nsp=2, ionz_lev=1, n_mol_atoms=(1, 2, 1, 1))
+    p = small_case(3, precision=AGPU_FP32_SPLIT, **kw)
+    dev = PicDevice(p)
+    ora = Oracle(small_case(3, precision=AGPU_FP64, **kw), threads=8)
+    ebf = laser_fields(p, a0=A0)
+    n_e = 8.71
+    el = plasma_source(p, ic=0, npx=1, npy=1, npz=1, n_over_n0=n_e, x_start_frac=0.3)
+    ion = plasma_source(p, ic=1, npx=2, npy=1, npz=1, charge=0, wgh=dopant * n_e / 2, x_start_frac=0.3, seed=4242)
+    for s in (dev, ora):
+        s.set_fields(ebf)
+        s.set_plasma_source(el)
+        s.set_plasma_source(ion)
+        s.load_plasma(0)
+        s.load_plasma(1)
+    dev.set_ionization_species(1, 7, 0, 7, 1, LP_MAX)
+    ora.set_ionization_species(1, 7, 0, 1, LP_MAX)
+    t, n32, n64 = 0.0, 0, 0
+    for it in range(12):
+        out = dev.lp_run(t, it, initial_time=(it == 0))
+        rc, oo = ora.lp_run(t, it, initial_time=(it == 0))
+        assert rc == 0 and out.error_bits == 0
+        n32 += out.new_electrons
+        n64 += oo.new_electrons
+        t += p.dt
+    print(f"dopant {dopant}: new electrons FP32 {n32}, FP64 {n64}, bound {5 * np.sqrt(2 * n64):.0f}")
+    assert n64 > 5000
+    assert abs(n32 - n64) <= 5 * np.sqrt(2 * n64), (n32, n64)
