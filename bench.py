@@ -442,7 +442,7 @@ def make_reducers(torch, world: int, device: str):
     return barrier, (lambda x: red(x, dist.ReduceOp.MAX)), (lambda x: red(x, dist.ReduceOp.SUM))
 
 
-def scan_measure(torch, warmup, steps, threads=0, n=256):
+def scan_measure(torch, warmup, steps, threads=0, n=256, sort_interval=0):
     """Batched scan: the n instances advanced together (agpu_batch_run)
     against the same instances run one after the other through the
     single-instance path in its fastest form (deferred counts, each step
@@ -468,6 +468,7 @@ def scan_measure(torch, warmup, steps, threads=0, n=256):
     batch = PicBatch([c[0] for c in cases])
     for d, (p, las, src) in zip(batch.instances, cases):
         setup(d, las, src)
+        d.set_sort_interval(sort_interval)
     st = batch.run(warmup, threads)
     if st != [0] * n:
         raise RuntimeError(f"batched warm-up failed: {st}")
@@ -552,6 +553,29 @@ def extra_forms(name, torch, warmup, steps, graphs=False):
                     if tm.ms_yee else None,
                     "error_bits": r["err"]}
     out["fp32_over_fp64"] = out["fp32_split"]["pushes_per_s"] / out["fp64"]["pushes_per_s"]
+    return out
+
+
+def extra_c1(torch, warmup, steps):
+    """C1 (2D, 1024x256, 4 ppc): both forms on the fixed path (deferred
+    counts + step graphs), then the split form with the options the tuner
+    (aladyn_b200/autotune.py) picks for this workload: sort interval, fused
+    Yee, step graphs, each candidate timed on a fresh instance."""
+    from aladyn_b200.abi import AGPU_FP32_SPLIT
+    from aladyn_b200.autotune import Tuner, tune_single
+    name = "lwfa2d_1024x256_ppc4"
+    out = extra_forms(name, torch, warmup, steps, True)
+    p, _, _, ppc = make_workload(name, AGPU_FP32_SPLIT, 1.04)
+    np0 = [0]
+
+    def make():
+        d = load_device(name, AGPU_FP32_SPLIT)[0]
+        np0[0] = d.count(0)
+        return d
+
+    r = tune_single(torch, make, p, ppc, warmup, steps, tuner=Tuner(None))
+    out["fp32_split_tuned"] = dict(r.as_dict(), pushes_per_s=np0[0] / (r.ms_per_step * 1e-3),
+                                   note="particles at the start / tuned ms per step")
     return out
 
 
@@ -726,12 +750,37 @@ def extra_pwfa_envelope(torch, warmup, steps, nx=512, ny=256, nz=256, nb=20_000_
             "warmup": warmup, "steps": steps, "error_bits": int(o.error_bits)}
 
 
+def tune_scan(torch, n_tune=32, warmup=3, steps=5):
+    """The batch's worker threads and sort interval chosen by the tuner
+    (aladyn_b200/autotune.py) on the first n_tune instances of the scan."""
+    from aladyn_b200.abi import AGPU_FP32_SPLIT
+    from aladyn_b200.autotune import Tuner, tune_batch
+    from aladyn_b200.sim import PicBatch
+    cases = scan_instances(n_tune, AGPU_FP32_SPLIT)
+    for p, _, _ in cases:
+        p.capacity[0] = int(p.capacity[0] * 1.5)
+
+    def make():
+        b = PicBatch([c[0] for c in cases])
+        for d, (p, las, src) in zip(b.instances, cases):
+            d.init_laser(las)
+            d.set_plasma_source(src)
+            d.load_plasma(0)
+        return b
+
+    return tune_batch(torch, make, cases[0][0], 4, n_tune, warmup, steps, tuner=Tuner(None))
+
+
 def extra_scan(torch, warmup, steps):
-    r = scan_measure(torch, warmup, steps, 0)
+    tuned = tune_scan(torch)
+    r = scan_measure(torch, warmup, steps, int(tuned.best["threads"]), sort_interval=int(tuned.best["sort_interval"]))
     return {"instances": r["n"], "warmup": warmup, "steps": steps,
             "batched_instance_steps_per_s": r["value"], "sequential_instance_steps_per_s": r["sequential"],
             "batched_over_sequential": r["value"] / r["sequential"],
             "sequential_path": "agpu_step per instance, one after the other, deferred counts and step graphs",
+            "batched_options": tuned.best,
+            "tuning": dict(tuned.as_dict(), note="worker threads and sort interval measured on the first "
+                           "32 instances (5 steps each), the fastest applied to the 256-instance batch"),
             "batched_gpu_launches": int(r["launches_b"])}
 
 
@@ -798,7 +847,7 @@ def extra_accuracy(torch, steps=1000):
 def extras(torch, warmup, only=None):
     k = 5
     todo = {
-        "c1_2d": (extra_forms, "lwfa2d_1024x256_ppc4", torch, warmup, 20, True),
+        "c1_2d": (extra_c1, torch, warmup, 20),
         "c2_cubic": (extra_forms, "lwfa3d_1024x256x256_ppc8_cubic", torch, warmup, k),
         "c3_pwfa": (extra_pwfa, torch, warmup, k),
         "c3_pwfa_envelope": (extra_pwfa_envelope, torch, warmup, k),
