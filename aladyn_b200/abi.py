@@ -119,6 +119,19 @@ class AgpuEnvParams(C.Structure):
     ]
 
 
+class AgpuStretchAxis(C.Structure):
+    _fields_ = [
+        ("cnst", C.c_double), ("smin", C.c_double), ("smax", C.c_double), ("xs", C.c_double),
+        ("dl_inv", C.c_double), ("dli_inv", C.c_double), ("ratio", C.c_double), ("nl_stretch", C.c_double),
+        ("init_cell", C.c_double), ("n", C.c_int32), ("reserved", C.c_int32),
+        ("d1", C.POINTER(C.c_double)), ("d1h", C.POINTER(C.c_double)),
+    ]
+
+
+class AgpuStretch(C.Structure):
+    _fields_ = [("on", C.c_int32), ("reserved", C.c_int32), ("y", AgpuStretchAxis), ("z", AgpuStretchAxis)]
+
+
 AGPU_NE = 100
 
 
@@ -234,6 +247,7 @@ SIGNATURES = {
     "agpu_struct_sizes": (C.c_int, [C.POINTER(C.c_int64), C.c_int32]),
     "agpu_field_diag_noalloc": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                           C.c_double, _P, _P]),
+    "agpu_set_stretch": (C.c_int, [_P, C.POINTER(AgpuStretch)]),
     "agpu_set_subdomain": (C.c_int, [_P, C.c_int32, C.c_int32, HALO_FN, _P]),
     "agpu_halo_size": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
     "agpu_halo_pack": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P]),

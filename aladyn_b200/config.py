@@ -12,6 +12,7 @@ values are bit-identical to what the reference computes with
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 from dataclasses import dataclass
 
@@ -119,6 +120,96 @@ def make_params(grid: Grid, *, precision: int = AGPU_FP64, nsp: int = 1, nsp_run
     for i in range(4):
         p.capacity[i] = int(capacity[i])
     return p
+
+
+class StretchedGrid:
+    """The stretched transverse axes of set_grid (src/grid/set_grid_param.f90:
+    52-226) with str_flag 1 or 2 (set_init_param.f90:54-69): ny_stretch =
+    nint(ny/6) (1) or nint(ny/4) (2) cells at each end of y (and z in 3D,
+    nz_stretch = ny_stretch) follow y = s + L tan(xi) on a uniform xi grid of
+    step dxi = 0.4 pi / ny_stretch, L = dy / dxi.  Holds the node
+    coordinates y, yh (0 .. n+1), the metric factors d1 = cos^2(xi) and d1h
+    (the reference's dy1, dy1h, loc_yg(:, 3:4)) and the agpu_stretch struct
+    for the library and the oracle."""
+
+    def __init__(self, p: "AgpuParams", str_flag: int = 1):
+        import numpy as np
+
+        from .abi import AgpuStretch
+        if p.ndim < 2 or str_flag not in (1, 2):
+            raise ValueError("stretched grids need ndim >= 2 and str_flag 1 or 2")
+        size = float(np.float32(1.0) / np.float32(6.0))  # size_of_stretch_along_y = 1./6. (default real)
+        f = float(p.ny) * size if str_flag == 1 else float(p.ny) * 1.5 * size
+        self.n_stretch = int(math.floor(f + 0.5))  # nint
+        # aph = acos(-1.0)*0.4 in default real
+        self.aph = float(np.float32(np.arccos(np.float32(-1.0))) * np.float32(0.4))
+        self.st = AgpuStretch()
+        self.st.on = 1
+        self.y = self._axis(p.ny, p.dy, p.dy_inv, self.st.y)
+        if p.ndim == 3:
+            self.z = self._axis(p.nz, p.dz, p.dz_inv, self.st.z)
+        # loc_ygrid / loc_zgrid bounds: gmin = y(1), gmax = y(n+1)
+        p.ymn = p.gymin = self.y["y"][1]
+        p.gymax = self.y["y"][p.ny + 1]
+        if p.ndim == 3:
+            p.zmn = p.gzmin = self.z["y"][1]
+            p.gzmax = self.z["y"][p.nz + 1]
+        self.struct = self.st
+
+    def _axis(self, n, d, d_inv, ax):
+        import numpy as np
+        ys = self.n_stretch
+        y = [d * float(i - 1 - n // 2) for i in range(n + 2)]
+        yh = [v + 0.5 * d for v in y]
+        d1 = [1.0] * (n + 2)
+        d1h = [1.0] * (n + 2)
+        ns1 = n + 1 - ys
+        dli = self.aph / float(ys)
+        dli_inv = 1. / dli
+        l_s = d * dli_inv
+        ratio = dli * d_inv
+        smin, smax = y[ys + 1], y[ns1]
+        for i in range(0, ys + 1):
+            yy = dli * float(i - 1 - ys)
+            yyh = yy + 0.5 * dli
+            y[i] = smin + l_s * math.tan(yy)
+            yh[i] = smin + l_s * math.tan(yyh)
+            d1h[i] = math.cos(yyh) * math.cos(yyh)
+            d1[i] = math.cos(yy) * math.cos(yy)
+        for i in range(ns1, n + 2):
+            yy = dli * float(i - ns1)
+            yyh = yy + dli * 0.5
+            y[i] = smax + l_s * math.tan(yy)
+            yh[i] = smax + l_s * math.tan(yyh)
+            d1h[i] = math.cos(yyh) * math.cos(yyh)
+            d1[i] = math.cos(yy) * math.cos(yy)
+        out = {"y": np.array(y), "yh": np.array(yh), "d1": np.ascontiguousarray(d1, dtype=np.float64),
+               "d1h": np.ascontiguousarray(d1h, dtype=np.float64), "smin": smin, "smax": smax, "l_s": l_s,
+               "dli": dli}
+        # map2dy_part_sind's parameters (stretched_grid.f90:80-88)
+        ax.cnst = 1.0 * n * d / 2
+        ax.smin, ax.smax = smin, smax
+        ax.xs = ys * d
+        ax.dl_inv = d_inv
+        ax.dli_inv = dli_inv
+        ax.ratio = ratio
+        ax.nl_stretch = float(ys)
+        ax.init_cell = 0.0
+        ax.n = n
+        ax.d1 = out["d1"].ctypes.data_as(C.POINTER(C.c_double))
+        ax.d1h = out["d1h"].ctypes.data_as(C.POINTER(C.c_double))
+        return out
+
+    def map(self, axis: str, v: float) -> float:
+        """The particle map of the axis (the library's str_map), in Python."""
+        a = self.st.y if axis == "y" else self.st.z
+        def inv(yp):
+            return a.dli_inv * math.atan(a.ratio * (yp + a.cnst - a.xs)) + a.nl_stretch
+        if v <= a.smin:
+            return inv(v) - a.init_cell
+        if v >= a.smax:
+            return (a.n - inv(2 * 0.0 - v)) - a.init_cell
+        return (v + a.cnst) * a.dl_inv - a.init_cell
 
 
 def env_params(grid: Grid, lam0: float, der_ord: int = 2):

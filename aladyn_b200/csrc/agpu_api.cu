@@ -89,6 +89,13 @@ struct agpu_handle {
   double* env_den = nullptr;
   agpu_env_params ep{};
   long long env_steps = 0;  // env_run calls so far (the record sort period)
+  // stretched y and z (agpu_set_stretch): the particle maps and the metric
+  // factors loc_yg(:, 3), loc_yg(:, 4), loc_zg(:, 3), loc_zg(:, 4) on the device
+  bool str = false;
+  StrAxis sy{}, sz{};
+  double* d_metric = nullptr;  // my3, my4 (ny+2 each), then mz3, mz4 (nz+2 each)
+  std::vector<double> h_metric;  // the same on the host
+  double by3 = 1.0, ty4 = 1.0, bz3 = 1.0, tz4 = 1.0;
   // a slab of a y decomposition (agpu_set_subdomain): shared sides and the
   // host's exchange hook
   bool dd = false;
@@ -257,6 +264,7 @@ int free_all(agpu_handle* h) {
   cudaFree(h->env_av);
   cudaFree(h->env_den);
   cudaFree(h->xadv_tmp);
+  cudaFree(h->d_metric);
   cudaFree(h->xadv_coef);
   for (int i = 0; i < 2 * PH_N; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
@@ -446,7 +454,7 @@ int compact_species(agpu_handle* h, int ic, bool window) {
 // The FP64 tile kernel has the reference's quadratic shapes only; the cubic
 // FP64 form runs the per-particle kernels.
 bool tiled(const agpu_handle* h, int ic) {
-  return !h->deterministic && !h->dd && ic < h->p.nsp_run && h->key[ic] != nullptr &&
+  return !h->deterministic && !h->dd && !h->str && ic < h->p.nsp_run && h->key[ic] != nullptr &&
          (h->fp32 || (h->p.shape == AGPU_SHAPE_QUADRATIC && h->p.iform < 2));
 }
 
@@ -1201,6 +1209,31 @@ int agpu_get_currents(agpu_handle* h, double* jc, int32_t n1p, int32_t n2p, int3
       double* c = jc + (size_t)g.ncell * i;
       for (size_t q = 0; q < (size_t)g.ncell; ++q) c[q] = d * c[q];
     }
+  if (h->str) {
+    // the stretched metric on the interior (curr_and_fields_util.f90:120-150)
+    const int ny = h->p.ny;
+    const double* my3 = h->h_metric.data();
+    const double* my4 = my3 + (ny + 2);
+    const double* mz3 = my3 + 2 * (ny + 2);
+    const double* mz4 = mz3 + (h->p.ndim == 3 ? h->p.nz + 2 : 0);
+    auto at = [&](int c, int i, int j, int k) -> double& {
+      return jc[(size_t)g.ncell * c + (size_t)(i - 1) + (size_t)g.n1p * ((size_t)(j - 1) + (size_t)g.n2p * (k - 1))];
+    };
+    for (int k = g.kz1; k <= g.kz2; ++k)
+      for (int j = g.jy1; j <= g.jy2; ++j)
+        for (int i = g.ix1; i <= g.ix2; ++i) {
+          const double dery = my3[j - 2], derhy = my4[j - 2];
+          if (g.nc == 2) {
+            at(0, i, j, k) = dery * at(0, i, j, k);
+            at(1, i, j, k) = derhy * at(1, i, j, k);
+          } else {
+            const double derz = mz3[k - 2], derhz = mz4[k - 2];
+            at(0, i, j, k) = dery * derz * at(0, i, j, k);
+            at(1, i, j, k) = derhy * derz * at(1, i, j, k);
+            at(2, i, j, k) = dery * derhz * at(2, i, j, k);
+          }
+        }
+  }
   return 0;
 }
 
@@ -1288,6 +1321,7 @@ int agpu_set_plasma_source(agpu_handle* h, const agpu_plasma* src) {
   int ic = src->ic;
   if (ic < 0 || ic >= h->p.nsp || src->npx < 1 || src->npy < 1 || src->npz < 1) return AGPU_E_ARG;
   if (!(src->jitter >= 0.0 && src->jitter < 1.0)) return AGPU_E_ARG;
+  if (h->str) return AGPU_E_STATE;  // stretched targets come from the host
   h->src[ic] = *src;
   h->has_src[ic] = true;
   h->nptx[ic] = 0;
@@ -1638,7 +1672,7 @@ int agpu_x_step_many(agpu_handle** hs, int32_t n, agpu_x_ws* w) {
 
 int agpu_set_step_graphs(agpu_handle* h, int32_t on) {
   if (!h) return AGPU_E_ARG;
-  if (on && h->dd) return AGPU_E_STATE;  // a slab's exchanges run between the kernels
+  if (on && (h->dd || h->str)) return AGPU_E_STATE;  // a slab's exchanges run between the kernels
   h->use_graph = on != 0;
   if (!h->use_graph && h->gexec) {
     cudaStreamSynchronize(h->st);
@@ -1646,6 +1680,22 @@ int agpu_set_step_graphs(agpu_handle* h, int32_t on) {
     h->gexec = nullptr;
   }
   return 0;
+}
+
+// The stretched axes' metric in the Yee coefficients (no-op on a uniform grid).
+static void stretch_coef(const agpu_handle* h, YeeC& c) {
+  if (!h->str) return;
+  const int ny = h->p.ny, nz = h->p.ndim == 3 ? h->p.nz : 0;
+  c.my3 = h->d_metric;
+  c.my4 = h->d_metric + (ny + 2);
+  if (h->p.ndim == 3) {
+    c.mz3 = h->d_metric + 2 * (ny + 2);
+    c.mz4 = h->d_metric + 2 * (ny + 2) + (nz + 2);
+  }
+  c.by3 = h->by3;
+  c.ty4 = h->ty4;
+  c.bz3 = h->bz3;
+  c.tz4 = h->tz4;
 }
 
 // The host's exchange at one point of a y slab's step (no-op otherwise).
@@ -1776,6 +1826,9 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
       a.iform = p.iform;
       a.dd_ylo = h->dd_lo;
       a.dd_yhi = h->dd_hi;
+      a.str = h->str ? 1 : 0;
+      a.sy = h->sy;
+      a.sz = h->sz;
       a.removed = &h->d_cnt->removed;
       a.err = &h->d_cnt->err;
       push_deposit64(a, h->st, h->sms, h->deterministic);
@@ -1801,10 +1854,12 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
   // curr_mpi_collect -> jc_xyzbd (djc folded into the E update)
   ph_begin(h, PH_YEE);
   YeeC c = yee_coef(p);
+  stretch_coef(h, c);
   // the fused step writes a second field array (its tiles read halos of the
   // input); not inside step graphs, whose launches keep their pointers
-  // (the comoving frame's advection substeps run only in the plain sweeps)
-  const bool fused = h->fused_yee && !h->use_graph && !h->xadv.tmp;
+  // (the comoving frame's advection substeps and the stretched metric run
+  // only in the plain sweeps)
+  const bool fused = h->fused_yee && !h->use_graph && !h->xadv.tmp && !h->str;
   if (h->fp32) {
     Dev32 d{h->g, h->ebf32, h->jhi, h->jlo};
     jfold32(d, h->st, h->sms);
@@ -1845,6 +1900,68 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
   return 0;
 }
 
+// ---- stretched transverse grids ------------------------------------------------
+static StrAxis str_axis(const agpu_stretch_axis& a) {
+  StrAxis s;
+  s.cnst = a.cnst;
+  s.smin = a.smin;
+  s.smax = a.smax;
+  s.xs = a.xs;
+  s.dl_inv = a.dl_inv;
+  s.dli_inv = a.dli_inv;
+  s.ratio = a.ratio;
+  s.nl_stretch = a.nl_stretch;
+  s.init_cell = a.init_cell;
+  s.n = (double)a.n;
+  return s;
+}
+
+int agpu_set_stretch(agpu_handle* h, const agpu_stretch* st) {
+  if (!h || !st) return AGPU_E_ARG;
+  const agpu_params& p = h->p;
+  if (int rc = agpu_synchronize(h)) return rc;
+  if (!st->on) {
+    h->str = false;
+    return 0;
+  }
+  // FP64 form, quadratic shapes, the standard cycle; host-supplied records
+  if (h->fp32 || p.ndim < 2 || p.shape != AGPU_SHAPE_QUADRATIC || p.iform == 2 || p.ionz_lev > 0 || h->env || h->dd ||
+      p.w_speed < 0.0)
+    return AGPU_E_ARG;
+  for (int ic = 0; ic < 4; ++ic)
+    if (h->has_src[ic]) return AGPU_E_STATE;
+  if (st->y.n != p.ny || !st->y.d1 || !st->y.d1h) return AGPU_E_ARG;
+  if (p.ndim == 3 && (st->z.n != p.nz || !st->z.d1 || !st->z.d1h)) return AGPU_E_ARG;
+  const int ny = p.ny, nz = p.ndim == 3 ? p.nz : 0;
+  const size_t nm = 2 * (size_t)(ny + 2) + (p.ndim == 3 ? 2 * (size_t)(nz + 2) : 0);
+  if (!h->d_metric && dmalloc((void**)&h->d_metric, sizeof(double) * nm)) return AGPU_E_NOMEM;
+  h->h_metric.assign(nm, 1.0);
+  std::memcpy(h->h_metric.data(), st->y.d1, sizeof(double) * (ny + 2));
+  std::memcpy(h->h_metric.data() + (ny + 2), st->y.d1h, sizeof(double) * (ny + 2));
+  if (p.ndim == 3) {
+    std::memcpy(h->h_metric.data() + 2 * (ny + 2), st->z.d1, sizeof(double) * (nz + 2));
+    std::memcpy(h->h_metric.data() + 2 * (ny + 2) + (nz + 2), st->z.d1h, sizeof(double) * (nz + 2));
+  }
+  CK(cudaMemcpy(h->d_metric, st->y.d1, sizeof(double) * (ny + 2), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_metric + (ny + 2), st->y.d1h, sizeof(double) * (ny + 2), cudaMemcpyHostToDevice));
+  if (p.ndim == 3) {
+    CK(cudaMemcpy(h->d_metric + 2 * (ny + 2), st->z.d1, sizeof(double) * (nz + 2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_metric + 2 * (ny + 2) + (nz + 2), st->z.d1h, sizeof(double) * (nz + 2), cudaMemcpyHostToDevice));
+  }
+  h->sy = str_axis(st->y);
+  h->sz = p.ndim == 3 ? str_axis(st->z) : StrAxis{};
+  // the Mur faces: loc_yg(1, 3), loc_yg(ny, 4), loc_zg(1, 3), loc_zg(nz, 4)
+  h->by3 = st->y.d1[1];
+  h->ty4 = st->y.d1h[ny];
+  h->bz3 = p.ndim == 3 ? st->z.d1[1] : 1.0;
+  h->tz4 = p.ndim == 3 ? st->z.d1h[nz] : 1.0;
+  h->str = true;
+  h->fused_yee = false;
+  agpu_set_step_graphs(h, 0);
+  for (int ic = 0; ic < 4; ++ic) h->binned[ic] = false;
+  return 0;
+}
+
 // ---- domain decomposition in y ---------------------------------------------
 int agpu_set_subdomain(agpu_handle* h, int32_t lo_shared, int32_t hi_shared, agpu_halo_fn fn, void* user) {
   if (!h) return AGPU_E_ARG;
@@ -1852,7 +1969,7 @@ int agpu_set_subdomain(agpu_handle* h, int32_t lo_shared, int32_t hi_shared, agp
   const bool any = lo_shared || hi_shared;
   if (any) {
     // FP64 form, quadratic shapes, fixed frame, no envelope
-    if (h->fp32 || p.shape != AGPU_SHAPE_QUADRATIC || p.w_speed < 0.0 || h->env) return AGPU_E_ARG;
+    if (h->fp32 || p.shape != AGPU_SHAPE_QUADRATIC || p.w_speed < 0.0 || h->env || h->str) return AGPU_E_ARG;
     if (!fn) return AGPU_E_ARG;
     if (p.ny < 3) return AGPU_E_ARG;  // the exchanges move up to 3 rows
   }
@@ -1976,7 +2093,7 @@ int agpu_window_inject(agpu_handle* h, int32_t ic, const double* part, int64_t l
 // ---- envelope cycle (Env_cycle, src/ALaDyn.F90:111-130) -------------------
 int agpu_env_enable(agpu_handle* h, const agpu_env_params* ep) {
   if (!h || !ep || h->fp32 || (ep->der_ord != 2 && ep->der_ord != 3) || !(ep->om0 > 0.0)) return AGPU_E_ARG;
-  if (h->dd) return AGPU_E_STATE;  // the envelope cycle runs on one box
+  if (h->dd || h->str) return AGPU_E_STATE;  // the envelope cycle runs on one uniform box
   const Geo& g = h->g;
   if (g.ix2 - g.ix1 < 3 || g.jy2 - g.jy1 < 2 || (g.ndim == 3 && g.kz2 - g.kz1 < 2)) return AGPU_E_ARG;
   CK(cudaStreamSynchronize(h->st));
@@ -2432,7 +2549,7 @@ int agpu_set_sort_interval(agpu_handle* h, int32_t steps) {
 }
 int agpu_set_fused_yee(agpu_handle* h, int32_t on) {
   if (!h) return AGPU_E_ARG;
-  if (on && h->dd) return AGPU_E_STATE;
+  if (on && (h->dd || h->str)) return AGPU_E_STATE;
   h->fused_yee = on != 0;
   return 0;
 }

@@ -202,6 +202,15 @@ __device__ bool esirkepov_cubic64(const Geo& g, double* jc, const double* xn, co
 // position in the neighbour's ghost rows; here the slab it leaves deposits
 // it into its own ghost rows, which the current exchange then adds to the
 // neighbour's rows: the same terms on the same nodes.
+// set_local_*_positions (grid_part_lib.f90:458-519): y and z in cells, by
+// the stretched axes' map when the grid is stretched
+__device__ __forceinline__ double ly(const PushArgs64& a, double y) {
+  return a.str ? str_map(a.sy, y) : a.dy_inv * (y - a.ymn);
+}
+__device__ __forceinline__ double lz(const PushArgs64& a, double z) {
+  return a.str ? str_map(a.sz, z) : a.dz_inv * (z - a.zmn);
+}
+
 __device__ __forceinline__ bool emigrant(const PushArgs64& a, double x, double y, double z) {
   if (!((a.dd_ylo && y <= a.gymin) || (a.dd_yhi && y > a.gymax))) return false;
   if (!(x > a.gxmin && x <= a.gxmax)) return false;
@@ -220,7 +229,7 @@ __global__ void __launch_bounds__(256) k64_push_dep_3d(PushArgs64 a) {
     double pp[3] = {a.px[n], a.py[n], a.pz[n]};
     uint64_t sl = dbits(a.slot[n]);
     // set_local_3d_positions
-    double xo[3] = {a.dx_inv * (x - a.xmn), a.dy_inv * (y - a.ymn), a.dz_inv * (z - a.zmn)};
+    double xo[3] = {a.dx_inv * (x - a.xmn), ly(a, y), lz(a, z)};
     double ap[6] = {0, 0, 0, 0, 0, 0};
     if (SHAPE == AGPU_SHAPE_CUBIC) {
       if (!gather_cubic64(g, ex, xo, 3, ap)) {
@@ -348,7 +357,7 @@ __global__ void __launch_bounds__(256) k64_push_dep_3d(PushArgs64 a) {
       atomicAdd(a.removed, 1ull);
       if (!emigrant(a, xnew, ynew, znew)) continue;
     }
-    double xn[3] = {a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn), a.dz_inv * (znew - a.zmn)};
+    double xn[3] = {a.dx_inv * (xnew - a.xmn), ly(a, ynew), lz(a, znew)};
     float wght = (float)slot_charge(sl) * slot_wgh(sl);
     if (SHAPE != AGPU_SHAPE_CUBIC && a.iform == 2) {
       ncdef3d<SERIAL>(g, a.jc, xn, xo, pn, wght, dtg);
@@ -372,7 +381,7 @@ __global__ void __launch_bounds__(256) k64_push_dep_2d(PushArgs64 a) {
     double pp1 = a.px[n], pp2 = a.py[n];
     uint64_t sl = dbits(a.slot[n]);
     double xl = a.dx_inv * (x - a.xmn);
-    double yl = a.dy_inv * (y - a.ymn);
+    double yl = ly(a, y);
     double ap1 = 0., ap2 = 0., ap3 = 0.;
     if (SHAPE == AGPU_SHAPE_CUBIC) {
       double apc[6];
@@ -469,15 +478,15 @@ __global__ void __launch_bounds__(256) k64_push_dep_2d(PushArgs64 a) {
     }
     float wght = (float)slot_charge(sl) * slot_wgh(sl);
     if (SHAPE != AGPU_SHAPE_CUBIC && a.iform == 2) {
-      ncdef2d<SERIAL>(g, a.jc, a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn), xl, yl, pn1, pn2, wght, dtg);
+      ncdef2d<SERIAL>(g, a.jc, a.dx_inv * (xnew - a.xmn), ly(a, ynew), xl, yl, pn1, pn2, wght, dtg);
       continue;
     }
     bool dep_ok;
     if (SHAPE == AGPU_SHAPE_CUBIC) {
-      const double xn2[2] = {a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn)}, xo2[2] = {xl, yl};
+      const double xn2[2] = {a.dx_inv * (xnew - a.xmn), ly(a, ynew)}, xo2[2] = {xl, yl};
       dep_ok = esirkepov_cubic64<SERIAL>(g, a.jc, xn2, xo2, wght, 2);
     } else {
-      dep_ok = esirkepov2d<SERIAL>(g, a.jc, a.dx_inv * (xnew - a.xmn), a.dy_inv * (ynew - a.ymn), xl, yl, wght);
+      dep_ok = esirkepov2d<SERIAL>(g, a.jc, a.dx_inv * (xnew - a.xmn), ly(a, ynew), xl, yl, wght);
     }
     if (!dep_ok) raise_err(a.err, AGPU_EBIT_INDEX);
   }

@@ -11,7 +11,35 @@ namespace agpu {
 struct YeeC {
   double dx_inv, dy_inv, dz_inv, dt, se1, se2, ompe, djc1, djc2, djc3;
   double vbeam;  // comoving frame: the x advection speed of the fields (0: off)
+  // stretched y / z (null: uniform): loc_yg(jj, 3), loc_yg(jj, 4),
+  // loc_zg(kk, 3), loc_zg(kk, 4), jj = j - 2, kk = k - 2 (device arrays)
+  const double* my3 = nullptr;
+  const double* my4 = nullptr;
+  const double* mz3 = nullptr;
+  const double* mz4 = nullptr;
+  // the Mur faces' factors: loc_yg(1, 3) (bf_bds, y = ymin), loc_yg(ny, 4)
+  // (ef_bds, y = ymax), loc_zg(1, 3), loc_zg(nz, 4)
+  double by3 = 1.0, ty4 = 1.0, bz3 = 1.0, tz4 = 1.0;
 };
+
+// One stretched transverse axis (map2dy_part_sind / map2dz_part_sind,
+// src/grid/stretched_grid.f90:45-143): a particle coordinate in cells of the
+// uniform computational grid (node index - 1 of the integer nodes).
+struct StrAxis {
+  double cnst, smin, smax, xs, dl_inv, dli_inv, ratio, nl_stretch, init_cell, n;
+};
+AGPU_HD double str_inv(const StrAxis& s, double yp) {
+  // invert_stretched_grid: dli_inv atan(ratio (y + const - xs)) + nl_stretch
+  return s.dli_inv * atan(s.ratio * (yp + s.cnst - s.xs)) + s.nl_stretch;
+}
+AGPU_HD double str_map(const StrAxis& s, double yp) {
+  if (yp <= s.smin) return str_inv(s, yp) - s.init_cell;
+  if (yp >= s.smax) {
+    const double ym = 2 * 0.0 - yp;  // mirrored about the symmetry centre 0
+    return (s.n - str_inv(s, ym)) - s.init_cell;
+  }
+  return (yp + s.cnst) * s.dl_inv - s.init_cell;  // invert_uniform_grid
+}
 // Scratch of the comoving frame's field advection (field_xadvect,
 // src/fields/grid_fields.f90:210-324): a one-component buffer for the
 // explicit step and the coefficients of the implicit step's tridiagonal
@@ -61,6 +89,9 @@ struct PushArgs64 {
   // y sides shared with a neighbouring slab: a particle that leaves through
   // one (and stays in the x and z box) still deposits its current here
   int dd_ylo = 0, dd_yhi = 0;
+  // stretched y and z (str != 0): particle coordinates through str_map
+  int str = 0;
+  StrAxis sy{}, sz{};
   unsigned long long* removed;
   unsigned int* err;
 };

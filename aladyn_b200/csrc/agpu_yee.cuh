@@ -180,14 +180,14 @@ __device__ __forceinline__ void d_ef_bds(T* ebf, Geo g, YeeC c, double dtl, long
     } else if (t < nfx + nfy) {
       long long u = t - nfx;
       int i = g.ix1 + (int)(u % nx), k = g.kz1 + (int)(u / nx);
-      T aphy = (T)(1.0 * c.dy_inv * dtl);
+      T aphy = (T)(c.ty4 * c.dy_inv * dtl);  // loc_yg(ny, 4) dy_inv dt
       long long o = goff(g, i, g.jy2, k), o1 = o + g.n1p;
       E1[o1] = -(two * Bn[o] + (one - aphy) * E1[o]) / (one + aphy);
       if (nf > 3) E3[o1] = (two * B1[o] - (one - aphy) * E3[o]) / (one + aphy);
     } else {
       long long u = t - nfx - nfy;
       int i = g.ix1 + (int)(u % nx), j = g.jy1 + (int)(u / nx);
-      T aphz = (T)(1.0 * c.dz_inv * dtl);
+      T aphz = (T)(c.tz4 * c.dz_inv * dtl);  // loc_zg(nz, 4) dz_inv dt
       long long o = goff(g, i, j, g.kz2), o1 = o + (long long)g.n1p * g.n2p;
       E1[o1] = (two * B2[o] - (one - aphz) * E1[o]) / (one + aphz);
       E2[o1] = -(two * B1[o] + (one - aphz) * E2[o]) / (one + aphz);
@@ -221,7 +221,7 @@ __device__ __forceinline__ void d_bf_bds(T* ebf, Geo g, YeeC c, double dtl, long
     } else if (t < nfx + nfy) {
       long long u = t - nfx;
       int i = g.ix1 + (int)(u % nx), k = g.kz1 + (int)(u / nx);
-      T aphy = (T)(1.0 * c.dy_inv * dtl);
+      T aphy = (T)(c.by3 * c.dy_inv * dtl);  // loc_yg(1, 3) dy_inv dt
       long long o = goff(g, i, g.jy1, k), o1 = o - g.n1p;
       T v = two * E1[o] - (one - aphy) * Bn[o];
       Bn[o1] = v / (one + aphy);
@@ -232,7 +232,7 @@ __device__ __forceinline__ void d_bf_bds(T* ebf, Geo g, YeeC c, double dtl, long
     } else {
       long long u = t - nfx - nfy;
       int i = g.ix1 + (int)(u % nx), j = g.jy1 + (int)(u / nx);
-      T aphz = (T)(1.0 * c.dz_inv * dtl);
+      T aphz = (T)(c.bz3 * c.dz_inv * dtl);  // loc_zg(1, 3) dz_inv dt
       long long o = goff(g, i, j, g.kz1), o1 = o - (long long)g.n1p * g.n2p;
       T v = two * E2[o] - (one - aphz) * B1[o];
       B1[o1] = v / (one + aphz);
@@ -350,7 +350,10 @@ __global__ void __launch_bounds__(YEE_BX* YEE_BY) k_rote_n(T* ebf, Geo g, YeeC c
   if (i > g.ix2 || j > g.jy2) return;
   const double aphxd = dtf * c.dx_inv, aphyd = dtf * c.dy_inv, aphzd = dtf * c.dz_inv;
   const T aph1 = (T)(aphxd * c.se1), aph2 = (T)(aphxd * c.se2);
-  const T sdhy = (T)(1.0 * aphyd), sdhz = (T)(1.0 * aphzd);
+  // loc_yg(jj, 4) * aphy, loc_zg(kk, 4) * aphz (1 on a uniform axis)
+  const int kn = (NDIM == 3) ? g.kz1 + (int)blockIdx.z : 1;
+  const T sdhy = (T)((c.my4 ? c.my4[j - 2] : 1.0) * aphyd);
+  const T sdhz = (T)((c.mz4 && NDIM == 3 ? c.mz4[kn - 2] : 1.0) * aphzd);
   const T* __restrict__ E1 = ebf;
   const T* __restrict__ E2 = ebf + g.ncell;
   const T* __restrict__ E3 = ebf + 2 * g.ncell;
@@ -364,7 +367,7 @@ __global__ void __launch_bounds__(YEE_BX* YEE_BY) k_rote_n(T* ebf, Geo g, YeeC c
   T* __restrict__ Bx = ebf + 3 * g.ncell;
   T* __restrict__ By = ebf + 4 * g.ncell;
   T* __restrict__ Bz = ebf + 5 * g.ncell;
-  const long long o = goff(g, i, j, g.kz1 + (int)blockIdx.z);
+  const long long o = goff(g, i, j, kn);
   Bz[o] = Bz[o] - aph1 * (E2[o + 1] - E2[o]) + sdhy * (E1[o + sy] - E1[o]) - aph2 * (E2[o + 2] - E2[o - 1]);
   Bx[o] = Bx[o] - sdhy * (E3[o + sy] - E3[o]) + sdhz * (E2[o + sz] - E2[o]);
   By[o] = By[o] + aph1 * (E3[o + 1] - E3[o]) - sdhz * (E1[o + sz] - E1[o]) + aph2 * (E3[o + 2] - E3[o - 1]);
@@ -377,12 +380,15 @@ __global__ void __launch_bounds__(YEE_BX* YEE_BY) k_rotb_j_n(T* ebf, const T* jc
   if (i > g.ix2 || j > g.jy2) return;
   const double aphxd = dtf * c.dx_inv, aphyd = dtf * c.dy_inv, aphzd = dtf * c.dz_inv;
   const T aph1 = (T)(aphxd * c.se1), aph2 = (T)(aphxd * c.se2);
-  const T sdy = (T)(1.0 * aphyd), sdz = (T)(aphzd * 1.0);
+  // loc_yg(jj, 3) * aphy, aphz * loc_zg(kk, 3) (1 on a uniform axis)
+  const int kn = (NDIM == 3) ? g.kz1 + (int)blockIdx.z : 1;
+  const T sdy = (T)((c.my3 ? c.my3[j - 2] : 1.0) * aphyd);
+  const T sdz = (T)(aphzd * (c.mz3 && NDIM == 3 ? c.mz3[kn - 2] : 1.0));
   const T ompe = (T)c.ompe, djc1 = (T)c.djc1, djc2 = (T)c.djc2, djc3 = (T)c.djc3;
   T* __restrict__ E1 = ebf;
   T* __restrict__ E2 = ebf + g.ncell;
   const long long sy = g.n1p, sz = (long long)g.n1p * g.n2p;
-  const long long o = goff(g, i, j, NDIM == 3 ? g.kz1 + (int)blockIdx.z : 1);
+  const long long o = goff(g, i, j, kn);
   T j1 = jc[o], j2 = jc[o + g.ncell];
   if (jlo) {
     j1 = j1 + jlo[o];
@@ -392,6 +398,12 @@ __global__ void __launch_bounds__(YEE_BX* YEE_BY) k_rotb_j_n(T* ebf, const T* jc
     const T* Bz = ebf + 2 * g.ncell;
     T ex = E1[o] + sdy * (Bz[o] - Bz[o - sy]);
     T ey = E2[o] - aph1 * (Bz[o] - Bz[o - 1]) - aph2 * (Bz[o + 1] - Bz[o - 2]);
+    if (c.my3) {
+      // curr_mpi_collect on a stretched y: dery (djc jx), derhy (djc jy)
+      E1[o] = ex - ompe * ((T)c.my3[j - 2] * (djc1 * j1));
+      E2[o] = ey - ompe * ((T)c.my4[j - 2] * (djc2 * j2));
+      return;
+    }
     E1[o] = ex - ompe * (djc1 * j1);
     E2[o] = ey - ompe * (djc2 * j2);
     return;
@@ -407,6 +419,15 @@ __global__ void __launch_bounds__(YEE_BX* YEE_BY) k_rotb_j_n(T* ebf, const T* jc
   ex = ex - sdz * (By[o] - By[o - sz]);
   ey = ey + sdz * (Bx[o] - Bx[o - sz]);
   T ez = E3[o] + aph1 * (By[o] - By[o - 1]) - sdy * (Bx[o] - Bx[o - sy]) + aph2 * (By[o + 1] - By[o - 2]);
+  if (c.my3) {
+    // curr_mpi_collect on stretched y and z: dery derz, derhy derz, dery derhz
+    const T dery = (T)c.my3[j - 2], derhy = (T)c.my4[j - 2];
+    const T derz = (T)c.mz3[kn - 2], derhz = (T)c.mz4[kn - 2];
+    E1[o] = ex - ompe * ((dery * derz) * (djc1 * j1));
+    E2[o] = ey - ompe * ((derhy * derz) * (djc2 * j2));
+    E3[o] = ez - ompe * ((dery * derhz) * (djc3 * j3));
+    return;
+  }
   E1[o] = ex - ompe * (djc1 * j1);
   E2[o] = ey - ompe * (djc2 * j2);
   E3[o] = ez - ompe * (djc3 * j3);

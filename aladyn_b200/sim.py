@@ -182,6 +182,11 @@ class PicDevice:
     step = lp_run
 
     # -- envelope cycle (Env_cycle, src/ALaDyn.F90:111-130) -------------------
+    def set_stretch(self, st):
+        """A stretched grid (config.stretched_grid); st keeps its metric
+        arrays alive until the call returns (the library copies them)."""
+        check(self.lib.agpu_set_stretch(self.h, C.byref(st.struct)), "agpu_set_stretch")
+
     def env_enable(self, ep: "abi.AgpuEnvParams"):
         check(self.lib.agpu_env_enable(self.h, C.byref(ep)), "agpu_env_enable")
 

@@ -507,6 +507,40 @@ int agpu_set_sort_interval(agpu_handle* h, int32_t steps);
  * binding can check its struct layouts against the library's. */
 int agpu_struct_sizes(int64_t* sizes, int32_t n);
 
+/* ---- stretched transverse grids (str_flag 1, 2) --------------------------- */
+/* The reference's stretched y and z axes (src/grid/set_grid_param.f90:52-226,
+ * src/grid/stretched_grid.f90:45-160): ny_stretch cells at each end follow
+ * y = smin + L tan(xi) (and smax + ...), the rest stays uniform.  One axis:
+ * the particle-to-cell map of map2dy_part_sind / map2dz_part_sind and the
+ * metric factors loc_yg(0:n+1, 3) (d1, integer nodes) and loc_yg(0:n+1, 4)
+ * (d1h, half nodes) that scale the y (z) differences of rote / rotb, the Mur
+ * faces of ef_bds / bf_bds and the currents in curr_mpi_collect. */
+typedef struct agpu_stretch_axis {
+  double cnst;        /* n d / 2                                               */
+  double smin, smax;  /* ends of the uniform part                              */
+  double xs;          /* n_stretch d                                           */
+  double dl_inv;      /* 1 / d                                                 */
+  double dli_inv;     /* 1 / dxi, dxi = 0.4 pi / n_stretch                     */
+  double ratio;       /* dxi / d                                               */
+  double nl_stretch;  /* n_stretch                                             */
+  double init_cell;   /* loc_ygrid%min_cell (0 for one box)                    */
+  int32_t n;          /* interior cells along the axis                         */
+  int32_t reserved;
+  const double* d1;   /* host array d1[0 .. n+1]                               */
+  const double* d1h;  /* host array d1h[0 .. n+1]                              */
+} agpu_stretch_axis;
+typedef struct agpu_stretch {
+  int32_t on;         /* 1: y (and z in 3D) stretched, 0: uniform              */
+  int32_t reserved;
+  agpu_stretch_axis y, z;
+} agpu_stretch;
+/* FP64 form, quadratic shapes, standard cycle (no envelope, no ionization,
+ * no lattice plasma source: the reference loads stretched targets on the
+ * host, so the host supplies the records); the handle then uses the
+ * per-particle kernels.  The box bounds in agpu_params (ymn = gymin = y(1),
+ * gymax = y(ny+1), z alike) are the stretched grid's. */
+int agpu_set_stretch(agpu_handle* h, const agpu_stretch* s);
+
 /* ---- domain decomposition in y ------------------------------------------ */
 /* One simulation split into slabs of rows along y, one handle per slab (one
  * process per GPU, or several handles of one process): the reference's

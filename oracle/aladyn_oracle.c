@@ -64,6 +64,11 @@ typedef struct ora_sim {
   double* av;
   int nav;
   agpu_env_params ep;
+  /* stretched y and z (set_grid, stretched_grid.f90): the particle maps and
+     loc_yg(0:ny+1, 3:4), loc_zg(0:nz+1, 3:4) */
+  int str;
+  agpu_stretch_axis sy, sz;
+  double *ym3, *ym4, *zm3, *zm4;
 } ora_sim;
 
 /* ---- layout helpers (Fortran 1-based) ---------------------------------- */
@@ -158,7 +163,72 @@ void ora_destroy(ora_sim* s) {
   free(s->ebfp);
   free(s->env);
   free(s->av);
+  free(s->ym3);
+  free(s->ym4);
+  free(s->zm3);
+  free(s->zm4);
   free(s);
+}
+
+/* map2dy_part_sind / map2dz_part_sind (src/grid/stretched_grid.f90:45-143):
+   a stretched coordinate in cells of the uniform computational grid. */
+static double ora_str_inv(const agpu_stretch_axis* a, double yp) {
+  return a->dli_inv * atan(a->ratio * (yp + a->cnst - a->xs)) + a->nl_stretch;
+}
+static double ora_str_map(const agpu_stretch_axis* a, double yp) {
+  double yl;
+  if (yp <= a->smin) {
+    yl = ora_str_inv(a, yp) - a->init_cell;
+  } else if (yp >= a->smax) {
+    yp = 2 * 0.0 - yp;
+    yl = ora_str_inv(a, yp);
+    yl = (double)a->n - yl - a->init_cell;
+  } else {
+    yl = (yp + a->cnst) * a->dl_inv - a->init_cell;
+  }
+  return yl;
+}
+/* set_local_*_positions (grid_part_lib.f90:458-519) along y and z */
+static inline double ora_ly(const ora_sim* s, double y) {
+  return s->str ? ora_str_map(&s->sy, y) : s->p.dy_inv * (y - s->p.ymn);
+}
+static inline double ora_lz(const ora_sim* s, double z) {
+  return s->str ? ora_str_map(&s->sz, z) : s->p.dz_inv * (z - s->p.zmn);
+}
+/* metric factors loc_yg(jj, 3|4), loc_zg(kk, 3|4) (1 on a uniform grid) */
+static inline double ora_my(const ora_sim* s, int jj, int c) {
+  return s->str ? (c == 3 ? s->ym3[jj] : s->ym4[jj]) : 1.0;
+}
+static inline double ora_mz(const ora_sim* s, int kk, int c) {
+  return (s->str && s->p.ndim == 3) ? (c == 3 ? s->zm3[kk] : s->zm4[kk]) : 1.0;
+}
+
+int ora_set_stretch(ora_sim* s, const agpu_stretch* st) {
+  if (!st->on) {
+    s->str = 0;
+    return 0;
+  }
+  if (st->y.n != s->p.ny || (s->p.ndim == 3 && st->z.n != s->p.nz)) return AGPU_E_ARG;
+  const int ny = s->p.ny, nz = s->p.ndim == 3 ? s->p.nz : 0;
+  free(s->ym3);
+  free(s->ym4);
+  free(s->zm3);
+  free(s->zm4);
+  s->ym3 = (double*)malloc(sizeof(double) * (size_t)(ny + 2));
+  s->ym4 = (double*)malloc(sizeof(double) * (size_t)(ny + 2));
+  memcpy(s->ym3, st->y.d1, sizeof(double) * (size_t)(ny + 2));
+  memcpy(s->ym4, st->y.d1h, sizeof(double) * (size_t)(ny + 2));
+  s->zm3 = s->zm4 = NULL;
+  if (s->p.ndim == 3) {
+    s->zm3 = (double*)malloc(sizeof(double) * (size_t)(nz + 2));
+    s->zm4 = (double*)malloc(sizeof(double) * (size_t)(nz + 2));
+    memcpy(s->zm3, st->z.d1, sizeof(double) * (size_t)(nz + 2));
+    memcpy(s->zm4, st->z.d1h, sizeof(double) * (size_t)(nz + 2));
+  }
+  s->sy = st->y;
+  s->sz = st->z;
+  s->str = 1;
+  return 0;
 }
 
 void ora_set_threads(ora_sim* s, int n) { s->nthreads = n > 0 ? n : 1; }
@@ -329,7 +399,7 @@ static void ora_gather(ora_sim* s, int ic, int64_t np) {
     #pragma omp parallel for schedule(static) num_threads(s->nthreads) if (s->nthreads > 1)
     for (int64_t n = 1; n <= np; ++n) {
       double xl = p->dx_inv * (PART(s, ic, n, 1) - p->xmn);
-      double yl = p->dy_inv * (PART(s, ic, n, 2) - p->ymn);
+      double yl = ora_ly(s, PART(s, ic, n, 2));
       double ax1[3], axh[2], ay1[3], ayh[2];
       int i, j;
       ora_qlh_1d(xl, ax1, axh, &i);
@@ -368,8 +438,8 @@ static void ora_gather(ora_sim* s, int ic, int64_t np) {
   #pragma omp parallel for schedule(static) num_threads(s->nthreads) if (s->nthreads > 1)
   for (int64_t n = 1; n <= np; ++n) {
     double xl = p->dx_inv * (PART(s, ic, n, 1) - p->xmn);
-    double yl = p->dy_inv * (PART(s, ic, n, 2) - p->ymn);
-    double zl = p->dz_inv * (PART(s, ic, n, 3) - p->zmn);
+    double yl = ora_ly(s, PART(s, ic, n, 2));
+    double zl = ora_lz(s, PART(s, ic, n, 3));
     double ax1[3], axh[2], ay1[3], ayh[2], az1[3], azh[2];
     int i, j, k;
     ora_qlh_1d(xl, ax1, axh, &i);
@@ -1078,8 +1148,8 @@ static void ora_curr_accumulate(ora_sim* s, int ic, int64_t np) {
       ora_pack w = ora_unpack(PART(s, ic, n, s->ndv));
       float wght = (float)w.charge * w.wgh;
       if (p->ndim == 2) {
-        double xp1[2] = {p->dx_inv * (PART(s, ic, n, 1) - p->xmn), p->dy_inv * (PART(s, ic, n, 2) - p->ymn)};
-        double xp0[2] = {p->dx_inv * (PT(s, n, 3) - p->xmn), p->dy_inv * (PT(s, n, 4) - p->ymn)};
+        double xp1[2] = {p->dx_inv * (PART(s, ic, n, 1) - p->xmn), ora_ly(s, PART(s, ic, n, 2))};
+        double xp0[2] = {p->dx_inv * (PT(s, n, 3) - p->xmn), ora_ly(s, PT(s, n, 4))};
         if (p->iform == 2)
           ora_ncdef_2d_one(s, jc, xp1, xp0, PART(s, ic, n, 3), PART(s, ic, n, 4), wght, PT(s, n, 5));
         else if (p->shape == AGPU_SHAPE_CUBIC)
@@ -1087,10 +1157,9 @@ static void ora_curr_accumulate(ora_sim* s, int ic, int64_t np) {
         else
           ora_esirkepov_2d_one(s, jc, xp1, xp0, wght);
       } else {
-        double xp1[3] = {p->dx_inv * (PART(s, ic, n, 1) - p->xmn), p->dy_inv * (PART(s, ic, n, 2) - p->ymn),
-                         p->dz_inv * (PART(s, ic, n, 3) - p->zmn)};
-        double xp0[3] = {p->dx_inv * (PT(s, n, 4) - p->xmn), p->dy_inv * (PT(s, n, 5) - p->ymn),
-                         p->dz_inv * (PT(s, n, 6) - p->zmn)};
+        double xp1[3] = {p->dx_inv * (PART(s, ic, n, 1) - p->xmn), ora_ly(s, PART(s, ic, n, 2)),
+                         ora_lz(s, PART(s, ic, n, 3))};
+        double xp0[3] = {p->dx_inv * (PT(s, n, 4) - p->xmn), ora_ly(s, PT(s, n, 5)), ora_lz(s, PT(s, n, 6))};
         if (p->iform == 2) {
           const double pv[3] = {PART(s, ic, n, 4), PART(s, ic, n, 5), PART(s, ic, n, 6)};
           ora_ncdef_3d_one(s, jc, xp1, xp0, pv, wght, PT(s, n, 7));
@@ -1227,12 +1296,40 @@ static void ora_curr_collect(ora_sim* s) {
       for (size_t q = 0; q < comp; ++q) c[q] = d * c[q];
     }
   }
+  if (!s->str) return;
+  /* stretched grid (curr_and_fields_util.f90:120-150): dery, derhy (2D);
+     dery derz, derhy derz, dery derhz (3D) on the interior */
+  if (s->nc == 2) {
+    for (int k = s->kz1; k <= s->kz2; ++k)
+      for (int j = s->jy1; j <= s->jy2; ++j) {
+        const int jj = j - 2;
+        const double dery = s->ym3[jj], derhy = s->ym4[jj];
+        for (int i = s->ix1; i <= s->ix2; ++i) {
+          JC(s, i, j, k, 1) = dery * JC(s, i, j, k, 1);
+          JC(s, i, j, k, 2) = derhy * JC(s, i, j, k, 2);
+        }
+      }
+    return;
+  }
+  for (int k = s->kz1; k <= s->kz2; ++k) {
+    const int kk = k - 2;
+    const double derz = s->zm3[kk], derhz = s->zm4[kk];
+    for (int j = s->jy1; j <= s->jy2; ++j) {
+      const int jj = j - 2;
+      const double dery = s->ym3[jj], derhy = s->ym4[jj];
+      for (int i = s->ix1; i <= s->ix2; ++i) {
+        JC(s, i, j, k, 1) = dery * derz * JC(s, i, j, k, 1);
+        JC(s, i, j, k, 2) = derhy * derz * JC(s, i, j, k, 2);
+        JC(s, i, j, k, 3) = dery * derhz * JC(s, i, j, k, 3);
+      }
+    }
+  }
 }
 
 /* ======================================================================== */
 /* A14: advance_lpf_fields (curr_and_fields_util.f90:176-260) with ef_bds,   */
-/* bf_bds, rote, rotb (src/fields/grid_fields.f90:1069-1552); uniform grid   */
-/* so loc_xg/loc_yg/loc_zg stretch factors are 1.                            */
+/* bf_bds, rote, rotb (src/fields/grid_fields.f90:1069-1552); loc_xg is 1  */
+/* (x is never stretched), loc_yg/loc_zg are 1 unless the grid is stretched. */
 /* ======================================================================== */
 static void ora_ef_bds(ora_sim* s, double dtl, int imbd) {
   int nf = s->nf;
@@ -1250,7 +1347,7 @@ static void ora_ef_bds(ora_sim* s, double dtl, int imbd) {
   }
   if (s->p.ndim < 2) return;
   if (s->p.iby < 2 && imbd == 0) {
-    aphy = 1.0 * s->p.dy_inv * dtl;
+    aphy = ora_my(s, jy2 - 2, 4) * s->p.dy_inv * dtl;
     for (int k = s->kz1; k <= kz2; ++k)
       for (int i = s->ix1; i <= ix2; ++i)
         EBF(s, i, jy2 + 1, k, 1) = -(2. * EBF(s, i, jy2, k, nf) + (1. - aphy) * EBF(s, i, jy2, k, 1)) / (1. + aphy);
@@ -1261,7 +1358,7 @@ static void ora_ef_bds(ora_sim* s, double dtl, int imbd) {
   }
   if (s->p.ndim < 3) return;
   if (s->p.ibz < 2 && imbd == 0) {
-    aphz = 1.0 * s->p.dz_inv * dtl;
+    aphz = ora_mz(s, s->p.nz, 4) * s->p.dz_inv * dtl;
     for (int j = s->jy1; j <= jy2; ++j)
       for (int i = s->ix1; i <= ix2; ++i) {
         EBF(s, i, j, kz2 + 1, 1) = (2. * EBF(s, i, j, kz2, 5) - (1. - aphz) * EBF(s, i, j, kz2, 1)) / (1. + aphz);
@@ -1286,7 +1383,7 @@ static void ora_bf_bds(ora_sim* s, double dtl, int imbd) {
   }
   if (s->p.ndim < 2) return;
   if (s->p.iby < 2 && imbd == 0) {
-    aphy = 1.0 * s->p.dy_inv * dtl;
+    aphy = ora_my(s, 1, 3) * s->p.dy_inv * dtl;
     for (int k = s->kz1; k <= s->kz2; ++k)
       for (int i = s->ix1; i <= s->ix2; ++i) {
         EBF(s, i, jy1 - 1, k, nf) = 2. * EBF(s, i, jy1, k, 1) - (1. - aphy) * EBF(s, i, jy1, k, nf);
@@ -1301,7 +1398,7 @@ static void ora_bf_bds(ora_sim* s, double dtl, int imbd) {
   }
   if (s->p.ndim < 3) return;
   if (s->p.ibz < 2 && imbd == 0) {
-    aphz = 1.0 * s->p.dz_inv * dtl;
+    aphz = ora_mz(s, 1, 3) * s->p.dz_inv * dtl;
     for (int j = s->jy1; j <= s->jy2; ++j)
       for (int i = s->ix1; i <= s->ix2; ++i) {
         EBF(s, i, j, kz1 - 1, 4) = 2. * EBF(s, i, j, kz1, 2) - (1. - aphz) * EBF(s, i, j, kz1, 4);
@@ -1318,7 +1415,7 @@ static void ora_rote(ora_sim* s, double dtf) {
   double aph1 = aphx * s->p.se_coeff[0], aph2 = aphx * s->p.se_coeff[1];
   for (int k = s->kz1; k <= s->kz2; ++k)
     for (int j = s->jy1; j <= s->jy2; ++j) {
-      double sdhy = 1.0 * aphy;
+      double sdhy = ora_my(s, j - 2, 4) * aphy;
       for (int i = s->ix1; i <= s->ix2; ++i)
         EBF(s, i, j, k, nf) = EBF(s, i, j, k, nf) - aph1 * (EBF(s, i + 1, j, k, 2) - EBF(s, i, j, k, 2)) +
                               sdhy * (EBF(s, i, j + 1, k, 1) - EBF(s, i, j, k, 1)) -
@@ -1326,9 +1423,9 @@ static void ora_rote(ora_sim* s, double dtf) {
     }
   if (nf < 6) return;
   for (int k = s->kz1; k <= s->kz2; ++k) {
-    double sdhz = 1.0 * aphz;
+    double sdhz = ora_mz(s, k - 2, 4) * aphz;
     for (int j = s->jy1; j <= s->jy2; ++j) {
-      double sdhy = 1.0 * aphy;
+      double sdhy = ora_my(s, j - 2, 4) * aphy;
       for (int i = s->ix1; i <= s->ix2; ++i) {
         EBF(s, i, j, k, 4) = EBF(s, i, j, k, 4) - sdhy * (EBF(s, i, j + 1, k, 3) - EBF(s, i, j, k, 3)) +
                              sdhz * (EBF(s, i, j, k + 1, 2) - EBF(s, i, j, k, 2));
@@ -1346,7 +1443,7 @@ static void ora_rotb(ora_sim* s, double dtf) {
   double aph1 = aphx * s->p.se_coeff[0], aph2 = aphx * s->p.se_coeff[1];
   for (int k = s->kz1; k <= s->kz2; ++k)
     for (int j = s->jy1; j <= s->jy2; ++j) {
-      double sdy = 1.0 * aphy;
+      double sdy = ora_my(s, j - 2, 3) * aphy;
       for (int i = s->ix1; i <= s->ix2; ++i) {
         EBF(s, i, j, k, 1) = EBF(s, i, j, k, 1) + sdy * (EBF(s, i, j, k, nf) - EBF(s, i, j - 1, k, nf));
         EBF(s, i, j, k, 2) = EBF(s, i, j, k, 2) - aph1 * (EBF(s, i, j, k, nf) - EBF(s, i - 1, j, k, nf)) -
@@ -1355,9 +1452,9 @@ static void ora_rotb(ora_sim* s, double dtf) {
     }
   if (nf < 6) return;
   for (int k = s->kz1; k <= s->kz2; ++k) {
-    double sdz = aphz * 1.0;
+    double sdz = aphz * ora_mz(s, k - 2, 3);
     for (int j = s->jy1; j <= s->jy2; ++j) {
-      double sdy = aphy * 1.0;
+      double sdy = aphy * ora_my(s, j - 2, 3);
       for (int i = s->ix1; i <= s->ix2; ++i) {
         EBF(s, i, j, k, 1) = EBF(s, i, j, k, 1) - sdz * (EBF(s, i, j, k, 5) - EBF(s, i, j, k - 1, 5));
         EBF(s, i, j, k, 2) = EBF(s, i, j, k, 2) + sdz * (EBF(s, i, j, k, 4) - EBF(s, i, j, k - 1, 4));

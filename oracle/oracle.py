@@ -82,6 +82,7 @@ def load():
         "ora_get_env_source": (C.c_int, [P, D]),
         "ora_init_envelope": (None, [P, P, C.c_int]),
         "ora_env_run": (C.c_int, [P, C.c_int, C.c_double, P]),
+        "ora_set_stretch": (C.c_int, [P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -134,6 +135,11 @@ class Oracle:
         a = np.asfortranarray(ebf, dtype=np.float64)
         assert a.shape == self.field_shape()
         self.lib.ora_set_fields(self.h, _dp(a))
+
+    def set_stretch(self, st):
+        """A stretched grid (aladyn_b200.config.stretched_grid)."""
+        rc = self.lib.ora_set_stretch(self.h, C.cast(C.byref(st.struct), C.c_void_p))
+        assert rc == 0, rc
 
     def field_xadvect(self, dth, v_adv, ic1, ic2, isch):
         """One field_xadvect pass (the comoving frame's x advection) on
