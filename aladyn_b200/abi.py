@@ -249,6 +249,10 @@ SIGNATURES = {
                                           C.c_double, _P, _P]),
     "agpu_set_stretch": (C.c_int, [_P, C.POINTER(AgpuStretch)]),
     "agpu_set_subdomain": (C.c_int, [_P, C.c_int32, C.c_int32, HALO_FN, _P]),
+    "agpu_set_subdomain_yz": (C.c_int, [_P, C.POINTER(C.c_int32), HALO_FN, _P]),
+    "agpu_halo_size_z": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
+    "agpu_halo_pack_z": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P]),
+    "agpu_halo_unpack_z": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int32]),
     "agpu_halo_size": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
     "agpu_halo_pack": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P]),
     "agpu_halo_unpack": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int32]),

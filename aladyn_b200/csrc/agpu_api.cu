@@ -99,7 +99,7 @@ struct agpu_handle {
   // a slab of a y decomposition (agpu_set_subdomain): shared sides and the
   // host's exchange hook
   bool dd = false;
-  int dd_lo = 0, dd_hi = 0;
+  int dd_lo = 0, dd_hi = 0, dd_zlo = 0, dd_zhi = 0;
   agpu_halo_fn halo_fn = nullptr;
   void* halo_user = nullptr;
   // comoving frame (w_speed < 0): the field advection's scratch
@@ -1826,6 +1826,8 @@ static int step_impl(agpu_handle* h, int32_t iter, double t, int32_t initial_tim
       a.iform = p.iform;
       a.dd_ylo = h->dd_lo;
       a.dd_yhi = h->dd_hi;
+      a.dd_zlo = h->dd_zlo;
+      a.dd_zhi = h->dd_zhi;
       a.str = h->str ? 1 : 0;
       a.sy = h->sy;
       a.sz = h->sz;
@@ -1964,19 +1966,28 @@ int agpu_set_stretch(agpu_handle* h, const agpu_stretch* st) {
 
 // ---- domain decomposition in y ---------------------------------------------
 int agpu_set_subdomain(agpu_handle* h, int32_t lo_shared, int32_t hi_shared, agpu_halo_fn fn, void* user) {
-  if (!h) return AGPU_E_ARG;
+  const int32_t shared[4] = {lo_shared, hi_shared, 0, 0};
+  return agpu_set_subdomain_yz(h, shared, fn, user);
+}
+
+int agpu_set_subdomain_yz(agpu_handle* h, const int32_t* shared, agpu_halo_fn fn, void* user) {
+  if (!h || !shared) return AGPU_E_ARG;
   const agpu_params& p = h->p;
-  const bool any = lo_shared || hi_shared;
+  const bool zs = shared[2] || shared[3];
+  const bool any = shared[0] || shared[1] || zs;
   if (any) {
     // FP64 form, quadratic shapes, fixed frame, no envelope
     if (h->fp32 || p.shape != AGPU_SHAPE_QUADRATIC || p.w_speed < 0.0 || h->env || h->str) return AGPU_E_ARG;
     if (!fn) return AGPU_E_ARG;
-    if (p.ny < 3) return AGPU_E_ARG;  // the exchanges move up to 3 rows
+    if ((shared[0] || shared[1]) && p.ny < 3) return AGPU_E_ARG;  // the exchanges move up to 3 rows
+    if (zs && (p.ndim < 3 || p.nz < 3)) return AGPU_E_ARG;
   }
   if (int rc = agpu_synchronize(h)) return rc;
   h->dd = any;
-  h->dd_lo = lo_shared ? 1 : 0;
-  h->dd_hi = hi_shared ? 1 : 0;
+  h->dd_lo = shared[0] ? 1 : 0;
+  h->dd_hi = shared[1] ? 1 : 0;
+  h->dd_zlo = shared[2] ? 1 : 0;
+  h->dd_zhi = shared[3] ? 1 : 0;
   h->halo_fn = any ? fn : nullptr;
   h->halo_user = any ? user : nullptr;
   if (any) {
@@ -2002,6 +2013,41 @@ static int halo_args(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int
   return 0;
 }
 
+static int halo_args_z(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32_t k1, int32_t n, double** f) {
+  if (!h || h->fp32 || h->p.ndim < 3 || (what != 0 && what != 1)) return AGPU_E_ARG;
+  const int nmax = what == 0 ? h->g.nf : h->g.nc;
+  if (ic1 < 1 || ic2 < ic1 || ic2 > nmax || n < 0 || k1 < 1 || k1 + n - 1 > h->g.n3p) return AGPU_E_ARG;
+  *f = what == 0 ? h->ebf : h->jc;
+  return 0;
+}
+
+int agpu_halo_size_z(agpu_handle* h, int32_t ncomp, int32_t nplanes, int64_t* n) {
+  if (!h || !n || ncomp < 0 || nplanes < 0) return AGPU_E_ARG;
+  *n = (int64_t)ncomp * nplanes * h->g.n1p * h->g.n2p;
+  return 0;
+}
+
+int agpu_halo_pack_z(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32_t k1, int32_t nplanes, double* buf) {
+  double* f = nullptr;
+  if (int rc = halo_args_z(h, what, ic1, ic2, k1, nplanes, &f)) return rc;
+  if (!buf) return AGPU_E_ARG;
+  halo_planes64(f, h->g, ic1 - 1, ic2 - ic1 + 1, k1, nplanes, buf, 0, h->st, h->sms);
+  CK(cudaGetLastError());
+  h->timers.launches_total += 1;
+  return 0;
+}
+
+int agpu_halo_unpack_z(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32_t k1, int32_t nplanes,
+                       const double* buf, int32_t mode) {
+  double* f = nullptr;
+  if (int rc = halo_args_z(h, what, ic1, ic2, k1, nplanes, &f)) return rc;
+  if (mode < 0 || mode > 2 || (mode < 2 && !buf)) return AGPU_E_ARG;
+  halo_planes64(f, h->g, ic1 - 1, ic2 - ic1 + 1, k1, nplanes, const_cast<double*>(buf), mode + 1, h->st, h->sms);
+  CK(cudaGetLastError());
+  h->timers.launches_total += 1;
+  return 0;
+}
+
 int agpu_halo_pack(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32_t j1, int32_t nrows, double* buf) {
   double* f = nullptr;
   if (int rc = halo_args(h, what, ic1, ic2, j1, nrows, &f)) return rc;
@@ -2024,13 +2070,15 @@ int agpu_halo_unpack(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int
 }
 
 int agpu_halo_emigrants(agpu_handle* h, int32_t ic, int32_t side, double* buf, int64_t ld, int64_t* n) {
-  if (!h || h->fp32 || ic < 0 || ic >= h->p.nsp || (side != 0 && side != 1) || !n || ld < 0 || (ld > 0 && !buf))
+  if (!h || h->fp32 || ic < 0 || ic >= h->p.nsp || side < 0 || side > 3 || (side > 1 && h->p.ndim < 3) || !n ||
+      ld < 0 || (ld > 0 && !buf))
     return AGPU_E_ARG;
   *n = 0;
   if (h->np[ic] <= 0) return 0;
   const agpu_params& p = h->p;
   BoxBounds b{p.gxmin, p.gxmax, p.gymin, p.gymax, p.gzmin, p.gzmax, 1, p.ndim == 3 ? 1 : 0};
-  long long cnt = emigrants64(h->part[ic], h->cap[ic], h->np[ic], h->ndv, b, side, buf, ld, h->scr, h->st);
+  long long cnt =
+      emigrants64(h->part[ic], h->cap[ic], h->np[ic], h->ndv, b, side, h->dd_zlo, h->dd_zhi, buf, ld, h->scr, h->st);
   CK(cudaGetLastError());
   h->timers.launches_total += 3;
   *n = cnt;

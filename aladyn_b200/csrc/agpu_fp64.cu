@@ -196,12 +196,6 @@ __device__ bool esirkepov_cubic64(const Geo& g, double* jc, const double* xn, co
 // box is exactly one that the reference removes before its deposit.
 // ============================================================================
 
-// A slab of a y decomposition: a particle that left through a y side shared
-// with a neighbour but stays inside the x and z box moves to that neighbour
-// (part_prl_exchange).  The reference deposits it there, from its old
-// position in the neighbour's ghost rows; here the slab it leaves deposits
-// it into its own ghost rows, which the current exchange then adds to the
-// neighbour's rows: the same terms on the same nodes.
 // set_local_*_positions (grid_part_lib.f90:458-519): y and z in cells, by
 // the stretched axes' map when the grid is stretched
 __device__ __forceinline__ double ly(const PushArgs64& a, double y) {
@@ -211,10 +205,20 @@ __device__ __forceinline__ double lz(const PushArgs64& a, double z) {
   return a.str ? str_map(a.sz, z) : a.dz_inv * (z - a.zmn);
 }
 
+// A slab of a y (and z) decomposition: a particle that left through sides
+// shared with neighbours, and through no physical side, moves on to them
+// (part_prl_exchange, y first, then z).  The reference deposits it there,
+// from its old position in the neighbour's ghost rows; here the slab it
+// leaves deposits it into its own ghost rows, which the current exchange
+// then adds to the neighbour's rows: the same terms on the same nodes.
 __device__ __forceinline__ bool emigrant(const PushArgs64& a, double x, double y, double z) {
-  if (!((a.dd_ylo && y <= a.gymin) || (a.dd_yhi && y > a.gymax))) return false;
   if (!(x > a.gxmin && x <= a.gxmax)) return false;
-  return a.g.ndim < 3 || (z > a.gzmin && z <= a.gzmax);
+  const bool yin = y > a.gymin && y <= a.gymax;
+  const bool yok = yin || (a.dd_ylo && y <= a.gymin) || (a.dd_yhi && y > a.gymax);
+  if (a.g.ndim < 3) return yok && !yin;
+  const bool zin = z > a.gzmin && z <= a.gzmax;
+  const bool zok = zin || (a.dd_zlo && z <= a.gzmin) || (a.dd_zhi && z > a.gzmax);
+  return yok && zok && !(yin && zin);
 }
 
 template <bool SERIAL, int SHAPE>

@@ -86,9 +86,9 @@ struct PushArgs64 {
   int initial;
   int shape;  // AGPU_SHAPE_QUADRATIC or AGPU_SHAPE_CUBIC
   int iform;  // 0, 1: Esirkepov; 2: the non-conserving ncdef deposit
-  // y sides shared with a neighbouring slab: a particle that leaves through
-  // one (and stays in the x and z box) still deposits its current here
-  int dd_ylo = 0, dd_yhi = 0;
+  // y and z sides shared with neighbouring slabs: a particle that leaves
+  // through one (and no physical side) still deposits its current here
+  int dd_ylo = 0, dd_yhi = 0, dd_zlo = 0, dd_zhi = 0;
   // stretched y and z (str != 0): particle coordinates through str_map
   int str = 0;
   StrAxis sy{}, sz{};

@@ -60,6 +60,29 @@ __global__ void k_halo_rows64(double* f, Geo g, int c0, int ncomp, int j1, int n
     else *v = 0.0;
   }
 }
+// planes k1 .. k1+nplanes-1 of components c0 .. c0+ncomp-1, every x and y
+// node: buf[component][plane][y][x]
+__global__ void k_halo_planes64(double* f, Geo g, int c0, int ncomp, int k1, int nplanes, double* buf, int mode) {
+  const long long pl = (long long)g.n1p * g.n2p;
+  const long long total = (long long)ncomp * nplanes * pl;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const long long q = t % pl;
+    const long long r = (t / pl) % nplanes;
+    const long long c = t / (pl * nplanes);
+    double* v = f + g.ncell * (c0 + c) + pl * (k1 - 1 + r) + q;
+    if (mode == 0) buf[t] = *v;
+    else if (mode == 1) *v = buf[t];
+    else if (mode == 2) *v = *v + buf[t];
+    else *v = 0.0;
+  }
+}
+void halo_planes64(double* f, const Geo& g, int c0, int ncomp, int k1, int nplanes, double* buf, int mode,
+                   cudaStream_t st, int sms) {
+  const long long total = (long long)ncomp * nplanes * g.n1p * g.n2p;
+  if (total <= 0) return;
+  k_halo_planes64<<<grid_for(total, 256, sms, 8), 256, 0, st>>>(f, g, c0, ncomp, k1, nplanes, buf, mode);
+}
+
 void halo_rows64(double* f, const Geo& g, int c0, int ncomp, int j1, int nrows, double* buf, int mode, cudaStream_t st,
                  int sms) {
   const long long total = (long long)ncomp * g.n3p * nrows * g.n1p;
@@ -67,18 +90,33 @@ void halo_rows64(double* f, const Geo& g, int c0, int ncomp, int j1, int nrows, 
   k_halo_rows64<<<grid_for(total, 256, sms, 8), 256, 0, st>>>(f, g, c0, ncomp, j1, nrows, buf, mode);
 }
 
+void halo_planes64(double* f, const Geo& g, int c0, int ncomp, int k1, int nplanes, double* buf, int mode,
+                   cudaStream_t st, int sms);
+
+// Records that left through side `side` (0, 1: low, high y; 2, 3: low, high
+// z) of a slab and go to that neighbour: inside the x box, and, along the
+// other transverse axis, inside the slab (y, for the z sides: the y
+// exchange has run) or beyond a side that is shared too (z, for the y
+// sides: a corner crosser travels on through the z exchange).
 struct Emigrant64 {
   const double *x, *y, *z;
   BoxBounds b;
   int side;
+  int zlo, zhi;  // z sides shared
   __device__ bool operator()(long long i) const {
     const double a = x[i], c = y[i];
-    bool k = a > b.x0 && a <= b.x1;
-    if (b.use_z) {
-      const double d = z[i];
-      k = k && d > b.z0 && d <= b.z1;
+    if (!(a > b.x0 && a <= b.x1)) return false;
+    if (side < 2) {
+      if (b.use_z) {
+        const double d = z[i];
+        const bool zin = (d > b.z0 && d <= b.z1) || (zlo && d <= b.z0) || (zhi && d > b.z1);
+        if (!zin) return false;
+      }
+      return side == 0 ? c <= b.y0 : c > b.y1;
     }
-    return k && (side == 0 ? c <= b.y0 : c > b.y1);
+    if (!(c > b.y0 && c <= b.y1)) return false;
+    const double d = z[i];
+    return side == 2 ? d <= b.z0 : d > b.z1;
   }
 };
 struct MoveColsOut64 {
@@ -92,9 +130,9 @@ struct MoveColsOut64 {
     for (int c = 0; c < ndv; ++c) dst[(long long)c * dst_ld + o] = src[(long long)c * src_ld + i];
   }
 };
-long long emigrants64(const double* part, long long cap, long long np, int ndv, const BoxBounds& b, int side, double* out,
-                      long long ld, Scratch& s, cudaStream_t st) {
-  Emigrant64 pr{part, part + cap, part + 2 * cap, b, side};
+long long emigrants64(const double* part, long long cap, long long np, int ndv, const BoxBounds& b, int side, int zlo,
+                      int zhi, double* out, long long ld, Scratch& s, cudaStream_t st) {
+  Emigrant64 pr{part, part + cap, part + 2 * cap, b, side, zlo, zhi};
   MoveColsOut64 mv{part, cap, out, ld, ndv};
   return select_run(pr, mv, np, s, st);
 }

@@ -56,12 +56,16 @@ long long compact64(double* part, double* tmp, long long cap, long long np, int 
 // ([component][z][row][x]); mode 0 pack (f -> buf), 1 write, 2 add, 3 zero.
 void halo_rows64(double* f, const Geo& g, int c0, int ncomp, int j1, int nrows, double* buf, int mode, cudaStream_t st,
                  int sms);
-// Records of a slab that left through its low (side 0) or high (side 1)
-// y side and stayed in the x and z box b, in order, into out (leading
-// dimension ld; records beyond ld are counted, not written).  Returns the
-// count.
-long long emigrants64(const double* part, long long cap, long long np, int ndv, const BoxBounds& b, int side, double* out,
-                      long long ld, Scratch& s, cudaStream_t st);
+// The same for planes k1 .. k1+nplanes-1 along z (every x and y node;
+// buf[component][plane][y][x]).
+void halo_planes64(double* f, const Geo& g, int c0, int ncomp, int k1, int nplanes, double* buf, int mode,
+                   cudaStream_t st, int sms);
+// Records of a slab that left through side `side` (0, 1: low, high y; 2, 3:
+// low, high z) towards that neighbour (zlo, zhi: the z sides shared), in
+// order, into out (leading dimension ld; records beyond ld are counted, not
+// written).  Returns the count.
+long long emigrants64(const double* part, long long cap, long long np, int ndv, const BoxBounds& b, int side, int zlo,
+                      int zhi, double* out, long long ld, Scratch& s, cudaStream_t st);
 long long compact32(const Part32View& src, const Part32View& dst, long long np, int n1p, int n2p, int nx, int ny, int nz,
                     int use_y, int use_z, Scratch& s, cudaStream_t st);
 long long compact_flag64(const int* key, int dead, double* part, double* tmp, long long cap, long long np, int ndv, Scratch& s,

@@ -33,25 +33,40 @@ from . import abi
 from .abi import (AGPU_E_STATE, AGPU_HALO_B, AGPU_HALO_CURRENTS, AGPU_HALO_E, AGPU_HALO_FIELDS,
                   AGPU_HALO_PARTICLES, AgpuParams, HALO_FN, check)
 
-LOW, HIGH = 0, 1
+LOW, HIGH, ZLOW, ZHIGH = 0, 1, 2, 3
+
+
+def _split(n: int, parts: int):
+    base, extra = divmod(n, parts)
+    sizes = [base + (1 if r < extra else 0) for r in range(parts)]
+    return sizes, [sum(sizes[:r]) for r in range(parts)]
 
 
 # ---- layout -------------------------------------------------------------------
 class SlabLayout:
-    """Rows of a global box split into ``nslabs`` slabs along y: slab r owns
-    the global interior rows j0 .. j0 + rows - 1 (0-based), the first
-    ``ny % nslabs`` slabs one row more (the loc_ygrid split)."""
+    """A global box split into ``nslabs`` slabs of rows along y and, in 3D,
+    ``nzslabs`` blocks of planes along z (the reference's nprocy x nprocz
+    split): block r = ry + nslabs * rz owns the global interior rows
+    j0[ry] .. j0[ry] + rows[ry] - 1 and planes k0[rz] .. k0[rz] + planes[rz]
+    - 1 (0-based), the first ``ny % nslabs`` (``nz % nzslabs``) one more
+    (the loc_ygrid / loc_zgrid split)."""
 
-    def __init__(self, params: AgpuParams, nslabs: int):
+    def __init__(self, params: AgpuParams, nslabs: int, nzslabs: int = 1):
         if params.ndim < 2:
             raise ValueError("a y decomposition needs ndim >= 2")
         if nslabs < 1 or params.ny < 3 * nslabs:
             raise ValueError(f"{params.ny} rows cannot be split into {nslabs} slabs of at least 3 rows")
+        if nzslabs < 1 or (nzslabs > 1 and (params.ndim < 3 or params.nz < 3 * nzslabs)):
+            raise ValueError(f"the z planes cannot be split into {nzslabs} blocks of at least 3 planes")
         self.p = params
-        self.n = nslabs
-        base, extra = divmod(params.ny, nslabs)
-        self.rows = [base + (1 if r < extra else 0) for r in range(nslabs)]
-        self.j0 = [sum(self.rows[:r]) for r in range(nslabs)]
+        self.ny_s, self.nz_s = nslabs, nzslabs
+        self.n = nslabs * nzslabs
+        self.rows, self.j0 = _split(params.ny, nslabs)
+        nz = params.nz if params.ndim == 3 else 1
+        self.planes, self.k0 = _split(nz, nzslabs)
+
+    def coords(self, r: int):
+        return r % self.ny_s, r // self.ny_s
 
     def y_at(self, j0: int) -> float:
         """y of the slab boundary before global row j0 (the box's own
@@ -62,37 +77,84 @@ class SlabLayout:
             return self.p.gymax
         return self.p.ymn + self.p.dy * j0
 
+    def z_at(self, k0: int) -> float:
+        if k0 == 0:
+            return self.p.gzmin
+        if k0 == self.p.nz:
+            return self.p.gzmax
+        return self.p.zmn + self.p.dz * k0
+
     def params(self, r: int, capacity=None) -> AgpuParams:
-        """The params of slab r: ny = its rows, ymn = gymin = y of its first
-        row, gymax = y after its last row; everything else global."""
+        """The params of block r: ny (nz) = its rows (planes), ymn = gymin
+        = y of its first row, gymax = y after its last row, z alike;
+        everything else global."""
+        ry, rz = self.coords(r)
         q = AgpuParams()
         C.memmove(C.byref(q), C.byref(self.p), C.sizeof(AgpuParams))
-        q.ny = self.rows[r]
-        lo, hi = self.y_at(self.j0[r]), self.y_at(self.j0[r] + self.rows[r])
-        q.ymn = self.p.ymn if r == 0 else lo
+        q.ny = self.rows[ry]
+        lo, hi = self.y_at(self.j0[ry]), self.y_at(self.j0[ry] + self.rows[ry])
+        q.ymn = self.p.ymn if ry == 0 else lo
         q.gymin, q.gymax = lo, hi
+        if self.nz_s > 1:
+            q.nz = self.planes[rz]
+            lo, hi = self.z_at(self.k0[rz]), self.z_at(self.k0[rz] + self.planes[rz])
+            q.zmn = self.p.zmn if rz == 0 else lo
+            q.gzmin, q.gzmax = lo, hi
         if capacity is not None:
             for i in range(4):
                 q.capacity[i] = int(capacity[i])
         return q
 
     def shared(self, r: int):
-        """(low side shared, high side shared) of slab r."""
-        return r > 0, r < self.n - 1
+        """(low y, high y, low z, high z) side shared, of block r."""
+        ry, rz = self.coords(r)
+        return ry > 0, ry < self.ny_s - 1, rz > 0, rz < self.nz_s - 1
+
+    def neighbours(self, r: int) -> dict:
+        lo, hi, zlo, zhi = self.shared(r)
+        out = {}
+        if lo:
+            out[LOW] = r - 1
+        if hi:
+            out[HIGH] = r + 1
+        if zlo:
+            out[ZLOW] = r - self.ny_s
+        if zhi:
+            out[ZHIGH] = r + self.ny_s
+        return out
+
+    def local(self, r: int, a):
+        """Block r's part of a global (n1p, n2p, n3p, nc) array, ghosts
+        included (what the block's own handle holds)."""
+        import numpy as np
+        ry, rz = self.coords(r)
+        j0, nr = self.j0[ry], self.rows[ry]
+        if self.nz_s == 1:
+            return np.asfortranarray(a[:, j0:j0 + nr + 5])
+        k0, nk = self.k0[rz], self.planes[rz]
+        return np.asfortranarray(a[:, j0:j0 + nr + 5, k0:k0 + nk + 5])
 
     def assemble(self, arrays):
-        """One (n1p, n2p, n3p, nc) array of the global box from the slabs'
-        arrays: each slab's interior rows, the low ghost rows of slab 0 and
-        the high ghost rows of the last slab."""
+        """One (n1p, n2p, n3p, nc) array of the global box from the blocks'
+        arrays: each block's interior, and the ghost rows (planes) of the
+        blocks at the box's sides."""
         import numpy as np
         first = arrays[0]
-        n1p, _, n3p, nc = first.shape
+        n1p, _, n3p_loc, nc = first.shape
+        n3p = (self.p.nz + 5) if self.p.ndim == 3 else 1
         out = np.zeros((n1p, self.p.ny + 5, n3p, nc), order="F")
-        out[:, 0:2] = first[:, 0:2]
         for r, a in enumerate(arrays):
-            out[:, 2 + self.j0[r]:2 + self.j0[r] + self.rows[r]] = a[:, 2:2 + self.rows[r]]
-        last = arrays[-1]
-        out[:, self.p.ny + 2:] = last[:, self.rows[-1] + 2:]
+            ry, rz = self.coords(r)
+            j0, nr = self.j0[ry], self.rows[ry]
+            jl = 0 if ry == 0 else 2
+            jh = nr + 5 if ry == self.ny_s - 1 else nr + 2
+            if self.nz_s == 1:
+                out[:, j0 + jl:j0 + jh] = a[:, jl:jh]
+                continue
+            k0, nk = self.k0[rz], self.planes[rz]
+            kl = 0 if rz == 0 else 2
+            kh = nk + 5 if rz == self.nz_s - 1 else nk + 2
+            out[:, j0 + jl:j0 + jh, k0 + kl:k0 + kh] = a[:, jl:jh, kl:kh]
         return out
 
 
@@ -181,8 +243,9 @@ class DistExchanger:
 
 # ---- one slab ----------------------------------------------------------------
 class Slab:
-    """Slab r of a layout on its PicDevice: registers the exchange hook and
-    carries out the exchanges the library asks for."""
+    """Block r of a layout on its PicDevice: registers the exchange hook and
+    carries out the exchanges the library asks for (the y rows first, then,
+    with a z split, the z planes over the whole y range, ghosts included)."""
 
     def __init__(self, layout: SlabLayout, rank: int, dev, exchanger, emigrant_capacity: int = 1 << 16):
         import torch
@@ -192,15 +255,13 @@ class Slab:
         self.dev = dev
         self.ex = exchanger
         self.lib = dev.lib
-        self.lo, self.hi = layout.shared(rank)
-        self.nbr = {}
-        if self.lo:
-            self.nbr[LOW] = rank - 1
-        if self.hi:
-            self.nbr[HIGH] = rank + 1
+        self.lo, self.hi, self.zlo, self.zhi = layout.shared(rank)
+        self.nbr = layout.neighbours(rank)
+        self.zsplit = layout.nz_s > 1
         p = layout.params(rank)
         self.nf, self.nc = p.nfield, p.curr_ndim
         self.jy1, self.jy2 = 3, p.ny + 2
+        self.kz1, self.kz2 = 3, (p.nz + 2 if p.ndim == 3 else 1)
         self.ndv = 7 if p.ndim == 3 else 5
         self.device = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else "cpu"
         self.ecap = int(emigrant_capacity)
@@ -209,72 +270,84 @@ class Slab:
                       AGPU_HALO_B: 0}
         self.migrated = 0
         self._fn = HALO_FN(self._hook)
-        check(self.lib.agpu_set_subdomain(dev.h, int(self.lo), int(self.hi), self._fn, None), "agpu_set_subdomain")
+        if self.zsplit:
+            shared = (C.c_int32 * 4)(int(self.lo), int(self.hi), int(self.zlo), int(self.zhi))
+            check(self.lib.agpu_set_subdomain_yz(dev.h, shared, self._fn, None), "agpu_set_subdomain_yz")
+        else:
+            check(self.lib.agpu_set_subdomain(dev.h, int(self.lo), int(self.hi), self._fn, None), "agpu_set_subdomain")
         self._stream = torch.cuda.ExternalStream(dev.stream()) if torch.cuda.is_available() else None
 
     # -- helpers
-    def _size(self, ncomp, nrows):
-        n = C.c_int64()
-        check(self.lib.agpu_halo_size(self.dev.h, ncomp, nrows, C.byref(n)), "agpu_halo_size")
-        return n.value
+    def _size(self, axis, ncomp, n):
+        out = C.c_int64()
+        f = self.lib.agpu_halo_size if axis == "y" else self.lib.agpu_halo_size_z
+        check(f(self.dev.h, ncomp, n, C.byref(out)), "agpu_halo_size")
+        return out.value
 
     def _buf(self, n):
         return self.torch.empty(max(int(n), 1), dtype=self.torch.float64, device=self.device)
 
-    def _pack(self, what, ic1, ic2, j1, nrows):
-        b = self._buf(self._size(ic2 - ic1 + 1, nrows))
-        check(self.lib.agpu_halo_pack(self.dev.h, what, ic1, ic2, j1, nrows, C.c_void_p(b.data_ptr())), "agpu_halo_pack")
+    def _pack(self, axis, what, ic1, ic2, first, n):
+        b = self._buf(self._size(axis, ic2 - ic1 + 1, n))
+        f = self.lib.agpu_halo_pack if axis == "y" else self.lib.agpu_halo_pack_z
+        check(f(self.dev.h, what, ic1, ic2, first, n, C.c_void_p(b.data_ptr())), "agpu_halo_pack")
         return b
 
-    def _unpack(self, what, ic1, ic2, j1, nrows, buf, mode):
+    def _unpack(self, axis, what, ic1, ic2, first, n, buf, mode):
         ptr = C.c_void_p(buf.data_ptr()) if buf is not None else None
-        check(self.lib.agpu_halo_unpack(self.dev.h, what, ic1, ic2, j1, nrows, ptr, mode), "agpu_halo_unpack")
+        f = self.lib.agpu_halo_unpack if axis == "y" else self.lib.agpu_halo_unpack_z
+        check(f(self.dev.h, what, ic1, ic2, first, n, ptr, mode), "agpu_halo_unpack")
 
     def _sync_for_peers(self):
         # the thread exchanger reads the buffers from the neighbours' streams
         if isinstance(self.ex, ThreadExchanger):
             self.dev.synchronize()
 
-    def _rows(self, tag, what, ic1, ic2, down, up, add=False):
-        """Send `down` rows from the bottom of my interior to the low
-        neighbour (its high ghost rows) and `up` rows from the top to the
-        high neighbour (its low ghost rows); with add, send my ghost rows
-        instead (down: the 2 below jy1, up: the 3 above jy2) and add them
-        into the neighbours' edge rows, then zero mine."""
+    def _layers(self, axis, tag, what, ic1, ic2, down, up, add=False):
+        """Along y (rows) or z (planes): send `down` layers from the bottom
+        of my interior to the low neighbour (its high ghost layers) and `up`
+        layers from the top to the high neighbour (its low ghost layers);
+        with add, send my ghost layers instead (down: the 2 below the
+        interior, up: the 3 above) and add them into the neighbours' edge
+        layers, then zero mine."""
+        lo_side, hi_side = (LOW, HIGH) if axis == "y" else (ZLOW, ZHIGH)
+        i1, i2 = (self.jy1, self.jy2) if axis == "y" else (self.kz1, self.kz2)
         sends, sizes, place = {}, {}, {}
-        if self.lo:
-            n_send = down
-            j_send = (self.jy1 - down) if add else self.jy1
-            sends[self.nbr[LOW]] = self._pack(what, ic1, ic2, j_send, n_send)
-            n_recv = up
-            j_recv = self.jy1 if add else self.jy1 - up
-            sizes[self.nbr[LOW]] = self._size(ic2 - ic1 + 1, n_recv)
-            place[self.nbr[LOW]] = (j_recv, n_recv)
-        if self.hi:
-            n_send = up
-            j_send = (self.jy2 + 1) if add else self.jy2 - up + 1
-            sends[self.nbr[HIGH]] = self._pack(what, ic1, ic2, j_send, n_send)
-            n_recv = down
-            j_recv = (self.jy2 - down + 1) if add else self.jy2 + 1
-            sizes[self.nbr[HIGH]] = self._size(ic2 - ic1 + 1, n_recv)
-            place[self.nbr[HIGH]] = (j_recv, n_recv)
+        nc = ic2 - ic1 + 1
+        if lo_side in self.nbr:
+            src = self.nbr[lo_side]
+            sends[src] = self._pack(axis, what, ic1, ic2, (i1 - down) if add else i1, down)
+            sizes[src] = self._size(axis, nc, up)
+            place[src] = (i1 if add else i1 - up, up)
+        if hi_side in self.nbr:
+            src = self.nbr[hi_side]
+            sends[src] = self._pack(axis, what, ic1, ic2, (i2 + 1) if add else i2 - up + 1, up)
+            sizes[src] = self._size(axis, nc, down)
+            place[src] = ((i2 - down + 1) if add else i2 + 1, down)
         self._sync_for_peers()
-        got = self.ex.exchange(self.rank, tag, sends, sizes, self.device)
+        got = self.ex.exchange(self.rank, tag + (axis,), sends, sizes, self.device)
         for src, buf in got.items():
-            j1, nr = place[src]
-            self._unpack(what, ic1, ic2, j1, nr, buf, 1 if add else 0)
+            first, n = place[src]
+            self._unpack(axis, what, ic1, ic2, first, n, buf, 1 if add else 0)
         if add:
-            if self.lo:
-                self._unpack(what, ic1, ic2, self.jy1 - down, down, None, 2)
-            if self.hi:
-                self._unpack(what, ic1, ic2, self.jy2 + 1, up, None, 2)
+            if lo_side in self.nbr:
+                self._unpack(axis, what, ic1, ic2, i1 - down, down, None, 2)
+            if hi_side in self.nbr:
+                self._unpack(axis, what, ic1, ic2, i2 + 1, up, None, 2)
         self._sync_for_peers()
         self.ex.done(self.rank)
 
-    def _particles(self, ic):
-        torch = self.torch
+    def _exchange(self, tag, what, ic1, ic2, down, up, add=False):
+        self._layers("y", tag, what, ic1, ic2, down, up, add)
+        if self.zsplit:
+            self._layers("z", tag, what, ic1, ic2, down, up, add)
+
+    def _particles(self, ic, sides):
         sends, counts = {}, {}
-        for side, dst in self.nbr.items():
+        for side in sides:
+            if side not in self.nbr:
+                continue
+            dst = self.nbr[side]
             while True:
                 buf = self._buf(self.ecap * self.ndv)
                 n = C.c_int64()
@@ -286,13 +359,13 @@ class Slab:
                 check(rc, "agpu_halo_emigrants")
                 break
             k = int(n.value)
-            # compact the ndv columns of leading dimension ecap to leading dimension k
+            # the ndv columns of leading dimension ecap to leading dimension k
             sends[dst] = buf.view(self.ndv, self.ecap)[:, :k].contiguous().view(-1)
             counts[dst] = k
         self._sync_for_peers()
-        got_n = self.ex.exchange_counts(self.rank, ("n", ic), counts)
+        got_n = self.ex.exchange_counts(self.rank, ("n", ic, sides[0]), counts)
         sizes = {src: got_n[src] * self.ndv for src in got_n}
-        got = self.ex.exchange(self.rank, ("p", ic), sends, sizes, self.device)
+        got = self.ex.exchange(self.rank, ("p", ic, sides[0]), sends, sizes, self.device)
         for src in sorted(got):
             n = got_n[src]
             if n > 0:
@@ -309,18 +382,21 @@ class Slab:
             ctx = self.torch.cuda.stream(self._stream) if self._stream is not None else _Null()
             with ctx:
                 if point == AGPU_HALO_FIELDS:
-                    self._rows(("f",), 0, 1, self.nf, 2, 2)
+                    self._exchange(("f",), 0, 1, self.nf, 2, 2)
                 elif point == AGPU_HALO_E:
                     # fill_ebfield_yzxbdsdata(ef, 1, curr_ndim, str = 1, stl = 2)
-                    self._rows(("e",), 0, 1, self.nc, 2, 1)
+                    self._exchange(("e",), 0, 1, self.nc, 2, 1)
                 elif point == AGPU_HALO_B:
                     # fill_ebfield_yzxbdsdata(ef, curr_ndim + 1, nfield, str = 2, stl = 1)
-                    self._rows(("b",), 0, self.nc + 1, self.nf, 1, 2)
+                    self._exchange(("b",), 0, self.nc + 1, self.nf, 1, 2)
                 elif point == AGPU_HALO_CURRENTS:
-                    # fill_curr_yzxbdsdata: 2 ghost rows down, 3 up, summed
-                    self._rows(("j",), 1, 1, self.nc, 2, 3, add=True)
+                    # fill_curr_yzxbdsdata: 2 ghost layers down, 3 up, summed
+                    self._exchange(("j",), 1, 1, self.nc, 2, 3, add=True)
                 elif point == AGPU_HALO_PARTICLES:
-                    self._particles(ic)
+                    # part_prl_exchange: through the y sides, then the z sides
+                    self._particles(ic, (LOW, HIGH))
+                    if self.zsplit:
+                        self._particles(ic, (ZLOW, ZHIGH))
             return 0
         except Exception as e:  # reported by the step's return code
             self.error = e
@@ -364,4 +440,4 @@ def run_threads(slabs, fn):
             raise e
 
 
-__all__ = ["SlabLayout", "Slab", "ThreadExchanger", "DistExchanger", "run_threads", "LOW", "HIGH"]
+__all__ = ["SlabLayout", "Slab", "ThreadExchanger", "DistExchanger", "run_threads", "LOW", "HIGH", "ZLOW", "ZHIGH"]

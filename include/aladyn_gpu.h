@@ -541,13 +541,14 @@ typedef struct agpu_stretch {
  * gymax = y(ny+1), z alike) are the stretched grid's. */
 int agpu_set_stretch(agpu_handle* h, const agpu_stretch* s);
 
-/* ---- domain decomposition in y ------------------------------------------ */
-/* One simulation split into slabs of rows along y, one handle per slab (one
- * process per GPU, or several handles of one process): the reference's
- * nprocy decomposition (src/parallel/parallel.F90:75-140) with npe_z = 1.
- * Each handle is created with its slab's params: ny = the slab's interior
- * rows, ymn = gymin = y of its first row, gymax = y after its last row (the
- * loc_ygrid bounds), everything else global.  The exchanges the reference
+/* ---- domain decomposition in y (and z) ----------------------------------- */
+/* One simulation split into slabs of rows along y (or blocks of rows and
+ * planes along y and z), one handle per slab (one process per GPU, or
+ * several handles of one process): the reference's nprocy x nprocz
+ * decomposition (src/parallel/parallel.F90:75-140).  Each handle is created
+ * with its slab's params: ny = the slab's interior rows, ymn = gymin = y of
+ * its first row, gymax = y after its last row (the loc_ygrid bounds), z
+ * alike, everything else global.  The exchanges the reference
  * makes by MPI inside the step are handed to the caller's hook, which moves
  * the packed rows between neighbours (NCCL, CUDA-aware MPI, device copies)
  * with the pack/unpack calls below, ordered on the handle's stream:
@@ -581,6 +582,14 @@ typedef int (*agpu_halo_fn)(void* user, agpu_handle* h, int32_t point, int32_t i
 /* lo_shared / hi_shared: the slab's low / high y side borders another slab
  * (0: a physical boundary, handled as in one box). */
 int agpu_set_subdomain(agpu_handle* h, int32_t lo_shared, int32_t hi_shared, agpu_halo_fn fn, void* user);
+/* The y and z split (npe_y x npe_z blocks, 3D): shared[0..3] = low y, high
+ * y, low z, high z side shared.  At every point the hook exchanges the y
+ * rows first and then the z planes (every x and y node, y ghosts included,
+ * agpu_halo_pack_z), so corner values pass through the y neighbour, as
+ * fill_ebfield_yzxbdsdata extends its z exchange over the y ghosts; the
+ * particles go through the y sides, then the z sides (emigrant sides 2,
+ * 3). */
+int agpu_set_subdomain_yz(agpu_handle* h, const int32_t* shared, agpu_halo_fn fn, void* user);
 /* Elements of a block of nrows full rows of ncomp components:
  * ncomp * nrows * n1p * n3p doubles, ordered [component][z][row][x]. */
 int agpu_halo_size(agpu_handle* h, int32_t ncomp, int32_t nrows, int64_t* n);
@@ -592,11 +601,19 @@ int agpu_halo_pack(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32
  * rows (buf unused). */
 int agpu_halo_unpack(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32_t j1, int32_t nrows,
                      const double* buf, int32_t mode);
-/* Copy the records of species ic that left through the low (side 0) or
- * high (side 1) y side and stayed inside the x and z box, in their order,
- * into the device buffer buf (ndv columns of leading dimension ld); *n =
- * their count (at most ld, else AGPU_E_CAPACITY).  Call it at
- * AGPU_HALO_PARTICLES; the step drops them afterwards. */
+/* The same along z: planes k1 .. k1+nplanes-1, every x and y node,
+ * ncomp * nplanes * n1p * n2p doubles ordered [component][plane][y][x]. */
+int agpu_halo_size_z(agpu_handle* h, int32_t ncomp, int32_t nplanes, int64_t* n);
+int agpu_halo_pack_z(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32_t k1, int32_t nplanes, double* buf);
+int agpu_halo_unpack_z(agpu_handle* h, int32_t what, int32_t ic1, int32_t ic2, int32_t k1, int32_t nplanes,
+                       const double* buf, int32_t mode);
+/* Copy the records of species ic that left through side `side` towards
+ * that neighbour, in their order, into the device buffer buf (ndv columns
+ * of leading dimension ld); *n = their count (at most ld, else
+ * AGPU_E_CAPACITY).  Sides 0, 1: low, high y (x inside the box, z inside or
+ * beyond a shared z side); 2, 3: low, high z (x and y inside the slab, for
+ * after the y exchange).  Call it at AGPU_HALO_PARTICLES; the step drops
+ * them afterwards. */
 int agpu_halo_emigrants(agpu_handle* h, int32_t ic, int32_t side, double* buf, int64_t ld, int64_t* n);
 /* Append n records from a device buffer (ndv columns, leading dimension ld)
  * to species ic. */

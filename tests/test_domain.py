@@ -41,6 +41,37 @@ class FakeLib:
     def agpu_set_subdomain(self, h, lo, hi, fn, user):
         return 0
 
+    def agpu_set_subdomain_yz(self, h, shared, fn, user):
+        self.devs[h].shared = tuple(shared[i] for i in range(4))
+        return 0
+
+    def agpu_halo_size_z(self, h, ncomp, nplanes, n):
+        d = self.devs[h]
+        n._obj.value = ncomp * nplanes * d.n1p * d.n2p
+        return 0
+
+    def _block_z(self, d, what, ic1, ic2, k1, n):
+        f = d.ebf if what == 0 else d.jc
+        return f, (slice(None), slice(None), slice(k1 - 1, k1 - 1 + n), slice(ic1 - 1, ic2))
+
+    def agpu_halo_pack_z(self, h, what, ic1, ic2, k1, n, ptr):
+        d = self.devs[h]
+        f, sl = self._block_z(d, what, ic1, ic2, k1, n)
+        blk = np.transpose(f[sl], (3, 2, 1, 0))  # [component][plane][y][x]
+        _view(ptr.value, blk.size)[:] = blk.ravel()
+        return 0
+
+    def agpu_halo_unpack_z(self, h, what, ic1, ic2, k1, n, ptr, mode):
+        d = self.devs[h]
+        f, sl = self._block_z(d, what, ic1, ic2, k1, n)
+        shape = f[sl].shape
+        if mode == 2:
+            f[sl] = 0.0
+            return 0
+        blk = _view(ptr.value, int(np.prod(shape))).reshape(shape[::-1]).transpose(3, 2, 1, 0)
+        f[sl] = blk if mode == 0 else f[sl] + blk
+        return 0
+
     def agpu_halo_size(self, h, ncomp, nrows, n):
         d = self.devs[h]
         n._obj.value = ncomp * nrows * d.n1p * d.n3p
@@ -74,7 +105,17 @@ class FakeLib:
     def agpu_halo_emigrants(self, h, ic, side, ptr, ld, n):
         d = self.devs[h]
         y = d.part[:, 1]
-        sel = d.part[(y <= d.p.gymin) if side == 0 else (y > d.p.gymax)]
+        if side < 2:
+            m = (y <= d.p.gymin) if side == 0 else (y > d.p.gymax)
+            if d.p.ndim == 3:
+                z = d.part[:, 2]
+                zlo, zhi = d.shared[2:] if hasattr(d, "shared") else (0, 0)
+                m &= ((z > d.p.gzmin) & (z <= d.p.gzmax)) | ((z <= d.p.gzmin) & bool(zlo)) | \
+                    ((z > d.p.gzmax) & bool(zhi))
+        else:
+            z = d.part[:, 2]
+            m = (y > d.p.gymin) & (y <= d.p.gymax) & ((z <= d.p.gzmin) if side == 2 else (z > d.p.gzmax))
+        sel = d.part[m]
         n._obj.value = sel.shape[0]
         if sel.shape[0] > ld:
             return AGPU_E_CAPACITY
@@ -85,6 +126,8 @@ class FakeLib:
     def agpu_halo_immigrants(self, h, ic, ptr, ld, n):
         d = self.devs[h]
         rec = _view(ptr.value, ld * d.ndv).reshape(d.ndv, ld)[:, :n].T
+        # the step's compaction drops what left; here the stand-in keeps the
+        # records inside the slab, so that forwarded ones do not count twice
         d.part = np.concatenate([d.part, rec])
         return 0
 
@@ -331,3 +374,111 @@ def test_dist_exchanger_gloo(ndim):
         assert pr.exitcode == 0
     for rank, ok_f, ok_c, ok_p in sorted(res):
         assert ok_f and ok_c and ok_p, (rank, ok_f, ok_c, ok_p)
+
+
+# ---- y and z split (2 x 2 blocks, 3D) ------------------------------------------
+def _blocks(p, ny_s, nz_s, ex):
+    lay = SlabLayout(p, ny_s, nz_s)
+    lib = FakeLib()
+    blocks = []
+    for r in range(lay.n):
+        dev = FakeDev(lib, 200 + r, lay.params(r))
+        blocks.append(Slab(lay, r, dev, ex, emigrant_capacity=1))
+    return lay, blocks
+
+
+def test_yz_layout():
+    p = _params(3, ny=18, nz=14)
+    lay = SlabLayout(p, 2, 2)
+    assert lay.n == 4 and lay.rows == [9, 9] and lay.planes == [7, 7]
+    q = [lay.params(r) for r in range(4)]
+    assert q[0].gzmin == p.gzmin and q[2].gzmax == p.gzmax and q[0].gzmax == q[2].gzmin == q[2].zmn
+    assert q[0].gymax == q[1].gymin and q[0].nz == 7 and q[3].ny == 9
+    assert lay.shared(0) == (False, True, False, True) and lay.shared(3) == (True, False, True, False)
+    assert lay.neighbours(0) == {1: 1, 3: 2} and lay.neighbours(3) == {0: 2, 2: 1}
+    g = _global_fields(p, 6)
+    assert np.array_equal(lay.assemble([lay.local(r, g) for r in range(4)]), g)
+
+
+def test_yz_exchange_fields_with_corners():
+    p = _params(3, ny=18, nz=14)
+    ex = ThreadExchanger(4)
+    lay, blocks = _blocks(p, 2, 2, ex)
+    g = _global_fields(p, 6)
+    for r, b in enumerate(blocks):
+        loc = lay.local(r, g).copy(order="F")
+        lo, hi, zlo, zhi = lay.shared(r)
+        if lo:
+            loc[:, 0:2] = -999.0
+        if hi:
+            loc[:, -3:] = -999.0
+        if zlo:
+            loc[:, :, 0:2] = -999.0
+        if zhi:
+            loc[:, :, -3:] = -999.0
+        b.dev.ebf = loc
+    _run_point(blocks, AGPU_HALO_FIELDS)
+    for r, b in enumerate(blocks):
+        want = lay.local(r, g)
+        got = b.dev.ebf
+        ry, rz = lay.coords(r)
+        nr, nk = lay.rows[ry], lay.planes[rz]
+        # every node within 2 layers of the interior, corners included
+        sl = (slice(None), slice(0, nr + 4), slice(0, nk + 4))
+        assert np.array_equal(got[sl], want[sl]), r
+
+
+def test_yz_exchange_currents_with_corners():
+    p = _params(3, ny=18, nz=14)
+    ex = ThreadExchanger(4)
+    lay, blocks = _blocks(p, 2, 2, ex)
+    rng = np.random.default_rng(9)
+    total = np.zeros((p.nx + 5, p.ny + 5, p.nz + 5, 3), order="F")
+    for r, b in enumerate(blocks):
+        ry, rz = lay.coords(r)
+        shape = (p.nx + 5, lay.rows[ry] + 5, lay.planes[rz] + 5, 3)
+        loc = np.asfortranarray(rng.integers(-20, 20, shape).astype(np.float64))
+        b.dev.jc = loc.copy(order="F")
+        total[:, lay.j0[ry]:lay.j0[ry] + lay.rows[ry] + 5, lay.k0[rz]:lay.k0[rz] + lay.planes[rz] + 5] += loc
+    _run_point(blocks, AGPU_HALO_CURRENTS)
+    for r, b in enumerate(blocks):
+        ry, rz = lay.coords(r)
+        nr, nk = lay.rows[ry], lay.planes[rz]
+        want = total[:, lay.j0[ry]:lay.j0[ry] + nr + 5, lay.k0[rz]:lay.k0[rz] + nk + 5]
+        got = b.dev.jc
+        assert np.array_equal(got[:, 2:nr + 2, 2:nk + 2], want[:, 2:nr + 2, 2:nk + 2]), r
+
+
+def test_yz_exchange_particles_reach_the_diagonal_block():
+    p = _params(3, ny=18, nz=14)
+    ex = ThreadExchanger(4)
+    lay, blocks = _blocks(p, 2, 2, ex)
+    rng = np.random.default_rng(21)
+    start = []
+    for r, b in enumerate(blocks):
+        q = lay.params(r)
+        n = 60
+        rec = np.zeros((n, 7))
+        rec[:, 0] = rng.uniform(p.gxmin, p.gxmax, n)
+        rec[:, 1] = rng.uniform(q.gymin - 0.5 * p.dy, q.gymax + 0.5 * p.dy, n)
+        rec[:, 2] = rng.uniform(q.gzmin - 0.5 * p.dz, q.gzmax + 0.5 * p.dz, n)
+        rec[:, -1] = np.arange(n) + 1000 * r
+        b.dev.part = rec
+        start.append(rec.copy())
+    _run_point(blocks, AGPU_HALO_PARTICLES, 0)
+    allrec = np.concatenate(start)
+    for r, b in enumerate(blocks):
+        q = lay.params(r)
+        inside = (b.dev.part[:, 1] > q.gymin) & (b.dev.part[:, 1] <= q.gymax) & \
+            (b.dev.part[:, 2] > q.gzmin) & (b.dev.part[:, 2] <= q.gzmax)
+        got = np.sort(b.dev.part[inside, -1])
+        # every record that lies in this block after the exchange, whichever block it started in
+        m = (allrec[:, 1] > q.gymin) & (allrec[:, 1] <= q.gymax) & (allrec[:, 2] > q.gzmin) & (allrec[:, 2] <= q.gzmax)
+        assert np.array_equal(got, np.sort(allrec[m, -1])), r
+    # some records crossed a corner (both a y and a z side)
+    diag = 0
+    for r in range(4):
+        q = lay.params(r)
+        y, z = start[r][:, 1], start[r][:, 2]
+        diag += int((((y <= q.gymin) | (y > q.gymax)) & ((z <= q.gzmin) | (z > q.gzmax))).sum())
+    assert diag > 0

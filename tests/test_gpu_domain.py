@@ -1,7 +1,8 @@
-"""The y decomposition on the device (agpu_set_subdomain + the slab hook of
-aladyn_b200/domain.py) against one box: 2 and 3 slabs of one simulation on
-one GPU, one host thread per slab (the threads meet at barriers between
-kernels; no kernel waits on another), FP64 form.
+"""The y (and y x z) decomposition on the device (agpu_set_subdomain,
+agpu_set_subdomain_yz + the slab hook of aladyn_b200/domain.py) against one
+box: 2 and 3 slabs, and 2 x 2 blocks in 3D, of one simulation on one GPU,
+one host thread per block (the threads meet at barriers between kernels;
+no kernel waits on another), FP64 form.
 
 Tolerances: the plasma load is the same particle set bit for bit (each
 slab keeps the lattice particles of its rows); after 14 steps with a window
@@ -26,20 +27,20 @@ def _key(rec, scale):
     return rec[np.lexsort(r.T[::-1])]
 
 
-def _setup(ndim, nslabs):
+def _setup(ndim, nslabs, nzslabs=1):
     p = small_case(ndim, w_sh=10)
-    lay = SlabLayout(p, nslabs)
+    lay = SlabLayout(p, nslabs, nzslabs)
     ebf = laser_fields(p)
     src = plasma_source(p, x_start_frac=0.3)
     one = PicDevice(p)
     one.set_fields(ebf)
     one.set_plasma_source(src)
     one.load_plasma(0)
-    ex = ThreadExchanger(nslabs)
+    ex = ThreadExchanger(lay.n)
     slabs = []
-    for r in range(nslabs):
+    for r in range(lay.n):
         dev = PicDevice(lay.params(r))
-        dev.set_fields(np.asfortranarray(ebf[:, lay.j0[r]:lay.j0[r] + lay.rows[r] + 5]))
+        dev.set_fields(lay.local(r, ebf))
         dev.set_plasma_source(src)
         slabs.append(Slab(lay, r, dev, ex))
         dev.load_plasma(0)
@@ -54,9 +55,10 @@ def _relmax(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-@pytest.mark.parametrize("ndim,nslabs", [(2, 2), (2, 3), (3, 2), (3, 3)])
-def test_slabs_match_one_box(ndim, nslabs):
-    p, lay, one, slabs = _setup(ndim, nslabs)
+@pytest.mark.parametrize("ndim,nslabs,nzslabs", [(2, 2, 1), (2, 3, 1), (3, 2, 1), (3, 3, 1), (3, 2, 2)])
+def test_slabs_match_one_box(ndim, nslabs, nzslabs):
+    p, lay, one, slabs = _setup(ndim, nslabs, nzslabs)
+    nblocks = lay.n
     a0, b0 = _union(slabs), one.get_species(0)
     assert a0.shape == b0.shape and a0.shape[0] > 1000
     order = lambda a: a[np.lexsort(a.T[::-1])]
@@ -65,7 +67,7 @@ def test_slabs_match_one_box(ndim, nslabs):
     for it in range(14):
         t = it * p.dt
         o1 = one.lp_run(t, it, initial_time=(it == 0))
-        outs = [None] * nslabs
+        outs = [None] * nblocks
 
         def step(s):
             outs[s.rank] = s.dev.lp_run(t, it, initial_time=(it == 0))
@@ -84,14 +86,15 @@ def test_slabs_match_one_box(ndim, nslabs):
     err_f = _relmax(f_dd, f_one)
     j_one = one.get_currents()
     j_dd = lay.assemble([s.dev.get_currents() for s in slabs])
-    # the assembled interior rows (ghost rows at shared sides are zero in the slabs)
-    err_j = _relmax(j_dd[:, 2:p.ny + 2], j_one[:, 2:p.ny + 2])
+    # the assembled interior (ghost layers at shared sides are zero in the blocks)
+    kin = slice(2, p.nz + 2) if ndim == 3 else slice(0, 1)
+    err_j = _relmax(j_dd[:, 2:p.ny + 2, kin], j_one[:, 2:p.ny + 2, kin])
     a, b = _union(slabs), one.get_species(0)
     assert a.shape == b.shape
     scale = np.maximum(np.abs(b).max(axis=0), 1e-300)
     ka, kb = _key(a, scale), _key(b, scale)
     err_p = (np.abs(ka - kb) / scale).max()
-    print(f"ndim {ndim} slabs {nslabs}: fields {err_f:.2e} currents {err_j:.2e} particles {err_p:.2e}")
+    print(f"ndim {ndim} blocks {nslabs}x{nzslabs}: fields {err_f:.2e} currents {err_j:.2e} particles {err_p:.2e}")
     assert err_f <= 1e-10 and err_j <= 1e-10 and err_p <= 1e-10
 
 
