@@ -1,8 +1,10 @@
-"""Host logic of the y decomposition (aladyn_b200/domain.py) on CPU: the
-slab layout, and the row and particle exchanges of the slab hook driven
-through a stand-in for the library that keeps each slab's arrays in numpy
-(the same pack/unpack/emigrant/immigrant contract as agpu_halo_*), with the
-thread exchanger and with torch.distributed over gloo (world size 3).
+"""Host logic of the y and y x z decompositions (aladyn_b200/domain.py) on
+CPU: the block layout, and the row, plane and particle exchanges of the
+block hook driven through a stand-in for the library that keeps each
+block's arrays in numpy (the same pack/unpack/emigrant/immigrant contract
+as agpu_halo_*), with the thread exchanger and with torch.distributed over
+gloo (3 slabs; 2 x 2 blocks, where corner values and corner-crossing
+particles must reach the diagonal block).
 
 What the exchanges must give (the reference's fill_ebfield_yzxbdsdata,
 fill_curr_yzxbdsdata and part_prl_exchange): after FIELDS every slab's 2
@@ -482,3 +484,76 @@ def test_yz_exchange_particles_reach_the_diagonal_block():
         y, z = start[r][:, 1], start[r][:, 2]
         diag += int((((y <= q.gymin) | (y > q.gymax)) & ((z <= q.gzmin) | (z > q.gzmax))).sum())
     assert diag > 0
+
+
+def _gloo_yz_worker(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        p = _params(3, ny=18, nz=14)
+        lay = SlabLayout(p, 2, 2)
+        lib = FakeLib()
+        dev = FakeDev(lib, 300 + rank, lay.params(rank))
+        blk = Slab(lay, rank, dev, DistExchanger(), emigrant_capacity=2)
+        g = _global_fields(p, 6)
+        loc = lay.local(rank, g).copy(order="F")
+        lo, hi, zlo, zhi = lay.shared(rank)
+        if lo:
+            loc[:, 0:2] = -999.0
+        if hi:
+            loc[:, -3:] = -999.0
+        if zlo:
+            loc[:, :, 0:2] = -999.0
+        if zhi:
+            loc[:, :, -3:] = -999.0
+        dev.ebf = loc
+        assert blk._hook(None, dev.h, AGPU_HALO_FIELDS, -1) == 0, blk.error
+        ry, rz = lay.coords(rank)
+        nr, nk = lay.rows[ry], lay.planes[rz]
+        sl = (slice(None), slice(0, nr + 4), slice(0, nk + 4))
+        ok_f = np.array_equal(dev.ebf[sl], lay.local(rank, g)[sl])
+        # particles: every record that ends inside a block is there once
+        rng = np.random.default_rng(8)
+        recs = []
+        for r in range(world):
+            q = lay.params(r)
+            a = np.zeros((40, 7))
+            a[:, 0] = rng.uniform(p.gxmin, p.gxmax, 40)
+            a[:, 1] = rng.uniform(q.gymin - 0.5 * p.dy, q.gymax + 0.5 * p.dy, 40)
+            a[:, 2] = rng.uniform(q.gzmin - 0.5 * p.dz, q.gzmax + 0.5 * p.dz, 40)
+            a[:, -1] = np.arange(40) + 1000 * r
+            recs.append(a)
+        dev.part = recs[rank].copy()
+        assert blk._hook(None, dev.h, AGPU_HALO_PARTICLES, 0) == 0, blk.error
+        q = lay.params(rank)
+        inside = lambda a: (a[:, 1] > q.gymin) & (a[:, 1] <= q.gymax) & (a[:, 2] > q.gzmin) & (a[:, 2] <= q.gzmax)
+        allrec = np.concatenate(recs)
+        ok_p = np.array_equal(np.sort(dev.part[inside(dev.part), -1]), np.sort(allrec[inside(allrec), -1]))
+        out.put((rank, ok_f, ok_p))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_dist_exchanger_gloo_yz_blocks():
+    """2 x 2 blocks over torch.distributed (gloo, 4 ranks): field halos with
+    corners and particles reaching the diagonal block."""
+    import socket
+
+    import torch.multiprocessing as mp
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gloo_yz_worker, args=(r, 4, port, q)) for r in range(4)]
+    for pr in procs:
+        pr.start()
+    res = [q.get(timeout=180) for _ in range(4)]
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    for rank, ok_f, ok_p in sorted(res):
+        assert ok_f and ok_p, (rank, ok_f, ok_p)
