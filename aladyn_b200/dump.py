@@ -1,8 +1,10 @@
-"""Dump and restart in the reference's ``dumpRestart/`` file formats for one
-rank (``dump_data`` / ``restart``, src/start/pic_dump.f90:35-380, 382-795):
-a run of this library can be continued by the reference and a reference
-dump can be continued here (single domain, npe = 1; no envelope or fluid
-arrays, which this library does not evolve).
+"""Dump and restart in the reference's ``dumpRestart/`` file formats
+(``dump_data`` / ``restart``, src/start/pic_dump.f90:35-380, 382-795): a run
+of this library can be continued by the reference and a reference dump can
+be continued here, for one rank (``write_dump`` / ``read_dump``) or for the
+blocks of a y / z split (``write_dump_blocks`` / ``read_dump_blocks``, npe_y
+x npe_z ranks; no envelope or fluid arrays, which this library does not
+evolve on blocks).
 
 Files of a dump directory:
 
@@ -305,9 +307,18 @@ def capture(holder, params0, it: int, t: float, sources=()) -> DumpState:
             zpt.append(np.zeros(0))
             wghyz.append(np.zeros((0, 0)))
             continue
-        ypt.append(h.s.y_min + (np.arange(1, h.npty + 1) - 0.5) * h.dyl)
-        zpt.append(h.s.z_min + (np.arange(1, h.nptz + 1) - 0.5) * h.dzl if p.ndim == 3 else np.zeros(1))
-        wghyz.append(np.ones((h.npty, len(zpt[-1]))))
+        # the transverse lattice rows of this holder's box (loc_ypt: a block
+        # of a y / z split keeps the rows inside its own bounds)
+        yr = h.s.y_min + (np.arange(1, h.npty + 1) - 0.5) * h.dyl
+        yr = yr[(yr > p.gymin) & (yr <= p.gymax)]
+        if p.ndim == 3:
+            zr = h.s.z_min + (np.arange(1, h.nptz + 1) - 0.5) * h.dzl
+            zr = zr[(zr > p.gzmin) & (zr <= p.gzmax)]
+        else:
+            zr = np.zeros(1)
+        ypt.append(yr)
+        zpt.append(zr)
+        wghyz.append(np.ones((len(yr), len(zr))))
     return DumpState(it=it, t=t, ndim=p.ndim, nx=p.nx, fields=holder.get_fields(), species=species,
                      nptx=[int(v) for v in nptx[:nsp]], sptx_max=[int(v) for v in sptx_max[:nsp]], x0=x0,
                      xlapse=xlapse, ompe=p.ompe, targ_in=targ_in, targ_end=targ_end, xpt=xpt, wghpt=wghpt,
@@ -334,3 +345,174 @@ def restore(holder, st: DumpState) -> None:
         if s.shape[0] > 0:
             holder.set_species(ic, np.asfortranarray(s))
     holder.set_window_state(st.xlapse, list(st.nptx) + [0] * (4 - len(st.nptx)))
+
+
+# ---- several ranks: blocks of a y / z split ------------------------------------
+def _block_files(dirpath: str, stem: str, rz: int) -> str:
+    return os.path.join(dirpath, f"{stem}{rz:02d}.bin")
+
+
+def write_dump_blocks(dirpath: str, states, layout, xmax: float) -> None:
+    """Write the dumps of the blocks of a y / z split (``states[r]`` of block
+    r = ry + npe_y * rz, the reference's mype order) as ``dump_data`` writes
+    them with npe ranks (pic_dump.f90:84-377): ``Comm-data.bin`` from rank 0
+    with ``npt_arr(1:npe, 1:nsp)``, ``dist_npy(1:npe_y, 1:nsp)`` and
+    ``dist_npz(1:npe_z, 1:nsp)``; one ``EB-fieldsNN.bin`` and one
+    ``ParticlesNN.bin`` per z column NN, the column's ranks one after the
+    other in y order (each rank's whole local ebf, ghosts included, and its
+    species' records); ``Dist-wgyz.bin`` with every rank's transverse lattice
+    in mype order.  The reference places rank imody's fields at imody times
+    its own length, so the y rows (and z planes) must split evenly."""
+    ny_s, nz_s = layout.ny_s, layout.nz_s
+    npe = ny_s * nz_s
+    if len(states) != npe:
+        raise ValueError(f"{len(states)} states for {npe} blocks")
+    if len(set(layout.rows)) != 1 or len(set(layout.planes)) != 1:
+        raise ValueError("a dump of several ranks needs rows and planes split evenly (ny_loc = ny/npe_y)")
+    os.makedirs(dirpath, exist_ok=True)
+    st0 = states[0]
+    nsp = st0.nsp
+    n1p, n2p, n3p = st0.fields.shape[:3]
+    nd2 = 2 * st0.ndim
+    with_xpt = st0.targ_end > xmax
+    nptx_max = 0 if st0.xpt is None else st0.xpt.shape[0]
+    if with_xpt and st0.xpt is None:
+        raise ValueError("targ_end > xmax: the dump needs the xpt / wghpt table")
+    rdata = np.array([st0.t, st0.j0_norm, st0.ompe, st0.targ_in, st0.targ_end, st0.lp_in, st0.xp0_out, st0.xp1_out,
+                      st0.x0, st0.xlapse], dtype=np.float64)
+    ndata = np.array([st0.it, n1p, n2p, n3p, nptx_max, st0.nx + 2, 0, nd2, 0, 0], dtype=np.int32)
+    head = [rdata, ndata, np.asarray(st0.nptx, dtype=np.int32), np.asarray(st0.sptx_max, dtype=np.int32)]
+    npt_arr = np.array([[st.species[ic].shape[0] for ic in range(nsp)] for st in states], dtype=np.int32)
+    npty = np.array([[0 if st.ypt is None else len(st.ypt[ic]) for ic in range(nsp)] for st in states], dtype=np.int32)
+    nptz = np.array([[0 if st.zpt is None else len(st.zpt[ic]) for ic in range(nsp)] for st in states], dtype=np.int32)
+    dist_npy = np.array([npty[ry] for ry in range(ny_s)], dtype=np.int32)              # blocks (ry, 0)
+    dist_npz = np.array([nptz[ny_s * rz] for rz in range(nz_s)], dtype=np.int32)     # blocks (0, rz)
+    tail = [npt_arr.ravel(order="F"), dist_npy.ravel(order="F"), dist_npz.ravel(order="F")]
+    path = os.path.join(dirpath, COMM)
+    write_records(path, head)
+    if with_xpt:
+        blk = np.zeros(nsp * nptx_max, dtype=XPT_RECORD)
+        blk["n0"] = 16
+        blk["n1"] = 16
+        blk["x"] = np.asarray(st0.xpt, dtype=np.float64).T.ravel()
+        blk["w"] = np.asarray(st0.wghpt, dtype=np.float64).T.ravel()
+        with open(path, "ab") as f:
+            f.write(blk.tobytes())
+    with open(path, "ab") as f:
+        for r in tail:
+            b = np.ascontiguousarray(r).tobytes()
+            n = np.array([len(b)], dtype=np.int32).tobytes()
+            f.write(n + b + n)
+    with_part = int(npt_arr.sum()) > 0
+    for rz in range(nz_s):
+        with open(_block_files(dirpath, "EB-fields", rz), "wb") as f:
+            for ry in range(ny_s):
+                np.asfortranarray(states[ry + ny_s * rz].fields, dtype=np.float64).ravel(order="F").tofile(f)
+        if with_part:
+            with open(_block_files(dirpath, "Particles", rz), "wb") as f:
+                for ry in range(ny_s):
+                    for sp in states[ry + ny_s * rz].species:
+                        if sp.shape[0] > 0:
+                            np.asarray(sp, dtype=np.float64).ravel(order="F").tofile(f)
+    if nsp > 0:
+        with open(os.path.join(dirpath, DISTYZ), "wb") as f:
+            for r, st in enumerate(states):
+                for ic in range(nsp):
+                    if npty[r, ic] > 0:
+                        np.asarray(st.ypt[ic], dtype=np.float64).tofile(f)
+                for ic in range(nsp):
+                    if nptz[r, ic] > 0:
+                        np.asarray(st.zpt[ic], dtype=np.float64).tofile(f)
+                for ic in range(nsp):
+                    if nptz[r, ic] > 0 and npty[r, ic] > 0:
+                        np.asarray(st.wghyz[ic], dtype=np.float64).ravel(order="F").tofile(f)
+
+
+def read_dump_blocks(dirpath: str, layout):
+    """Read a dump of npe_y x npe_z ranks (``write_dump_blocks`` or the
+    reference's ``dump_data``) into one DumpState per block, in mype order."""
+    ny_s, nz_s = layout.ny_s, layout.nz_s
+    npe = ny_s * nz_s
+    path = os.path.join(dirpath, COMM)
+    with open(path, "rb") as f:
+        data = f.read()
+    head, pos = _records_at(data, 0, 4, path)
+    rdata = np.frombuffer(head[0], dtype=np.float64)
+    ndata = np.frombuffer(head[1], dtype=np.int32)
+    nptx = np.frombuffer(head[2], dtype=np.int32).astype(int).tolist()
+    sptx_max = np.frombuffer(head[3], dtype=np.int32).astype(int).tolist()
+    nsp = len(nptx)
+    it, n1p, n2p, n3p, nptx_max, nx2, _, nd2 = (int(v) for v in ndata[:8])
+    ndim = nd2 // 2
+    tail_bytes = (8 + 4 * npe * nsp) + (8 + 4 * ny_s * nsp) + (8 + 4 * nz_s * nsp)
+    xpt = wghpt = None
+    nblk = len(data) - pos - tail_bytes
+    if nblk > 0:
+        if nblk != nsp * nptx_max * XPT_RECORD.itemsize:
+            raise ValueError(f"{path}: {nblk} bytes of xpt records, expected {nsp * nptx_max} records")
+        blk = np.frombuffer(data, dtype=XPT_RECORD, count=nsp * nptx_max, offset=pos)
+        xpt = np.ascontiguousarray(blk["x"].reshape(nsp, nptx_max).T)
+        wghpt = np.ascontiguousarray(blk["w"].reshape(nsp, nptx_max).T)
+        pos += nblk
+    recs, pos = _records_at(data, pos, 3, path)
+    if pos != len(data):
+        raise ValueError(f"{path}: {len(data) - pos} bytes after the last record")
+    npt_arr = np.frombuffer(recs[0], dtype=np.int32).reshape((npe, nsp), order="F").astype(int)
+    dist_npy = np.frombuffer(recs[1], dtype=np.int32).reshape((ny_s, nsp), order="F").astype(int)
+    dist_npz = np.frombuffer(recs[2], dtype=np.int32).reshape((nz_s, nsp), order="F").astype(int)
+    ndv = nd2 + 1
+    ncell = n1p * n2p * n3p
+    fields, species = [None] * npe, [None] * npe
+    for rz in range(nz_s):
+        raw = np.fromfile(_block_files(dirpath, "EB-fields", rz), dtype=np.float64)
+        if raw.size % (ny_s * ncell):
+            raise ValueError(f"EB-fields{rz:02d}.bin: {raw.size} values for {ny_s} ranks of {ncell} cells")
+        nf = raw.size // (ny_s * ncell)
+        for ry in range(ny_s):
+            r = ry + ny_s * rz
+            fields[r] = raw[ry * ncell * nf:(ry + 1) * ncell * nf].reshape((n1p, n2p, n3p, nf), order="F").copy(
+                order="F")
+        ppath = _block_files(dirpath, "Particles", rz)
+        praw = np.fromfile(ppath, dtype=np.float64) if os.path.exists(ppath) else np.zeros(0)
+        off = 0
+        for ry in range(ny_s):
+            r = ry + ny_s * rz
+            species[r] = []
+            for ic in range(nsp):
+                n = int(npt_arr[r, ic])
+                species[r].append(praw[off:off + n * ndv].reshape((n, ndv), order="F").copy(order="F"))
+                off += n * ndv
+        if off != praw.size:
+            raise ValueError(f"Particles{rz:02d}.bin: {praw.size} values, expected {off}")
+    lat = [(None, None, None)] * npe
+    dpath = os.path.join(dirpath, DISTYZ)
+    if os.path.exists(dpath):
+        d = np.fromfile(dpath, dtype=np.float64)
+        off = 0
+        lat = []
+        for r in range(npe):
+            ry, rz = r % ny_s, r // ny_s
+            ny_r, nz_r = dist_npy[ry], dist_npz[rz]
+            ypt, zpt, wghyz = [], [], []
+            for ic in range(nsp):
+                ypt.append(d[off:off + ny_r[ic]].copy())
+                off += ny_r[ic]
+            for ic in range(nsp):
+                zpt.append(d[off:off + nz_r[ic]].copy())
+                off += nz_r[ic]
+            for ic in range(nsp):
+                n = ny_r[ic] * nz_r[ic] if (ny_r[ic] > 0 and nz_r[ic] > 0) else 0
+                wghyz.append(d[off:off + n].reshape((ny_r[ic], nz_r[ic]), order="F").copy())
+                off += n
+            lat.append((ypt, zpt, wghyz))
+        if off != d.size:
+            raise ValueError(f"{DISTYZ}: {d.size} values, expected {off}")
+    out = []
+    for r in range(npe):
+        out.append(DumpState(it=it, t=float(rdata[0]), ndim=ndim, nx=nx2 - 2, fields=fields[r], species=species[r],
+                             nptx=list(nptx), sptx_max=list(sptx_max), x0=float(rdata[8]), xlapse=float(rdata[9]),
+                             j0_norm=float(rdata[1]), ompe=float(rdata[2]), targ_in=float(rdata[3]),
+                             targ_end=float(rdata[4]), lp_in=float(rdata[5]), xp0_out=float(rdata[6]),
+                             xp1_out=float(rdata[7]), xpt=xpt, wghpt=wghpt, ypt=lat[r][0], zpt=lat[r][1],
+                             wghyz=lat[r][2]))
+    return out

@@ -152,3 +152,90 @@ def test_dump_before_target_enters_window(tmp_path):
     assert n > 0 and b.get_species(0).shape[0] == n
     assert np.array_equal(a.get_species(0).view(np.uint64), b.get_species(0).view(np.uint64))
     assert np.array_equal(a.get_fields().view(np.uint64), b.get_fields().view(np.uint64))
+
+
+# ---- dumps of several ranks (blocks of a y / z split) ---------------------------
+def _block_states(p, lay, seed=4):
+    from aladyn_b200.domain import SlabLayout  # noqa: F401  (layout type)
+    rng = np.random.default_rng(seed)
+    states = []
+    ndv = 7 if p.ndim == 3 else 5
+    nxpt = 30
+    xpt = np.cumsum(rng.uniform(0.1, 0.2, (nxpt, 2)), axis=0)
+    for r in range(lay.n):
+        q = lay.params(r)
+        n3p = q.nz + 5 if p.ndim == 3 else 1
+        fields = np.asfortranarray(rng.standard_normal((q.nx + 5, q.ny + 5, n3p, p.nfield)))
+        species = [np.asfortranarray(rng.standard_normal((int(rng.integers(0, 50)), ndv))) for _ in range(2)]
+        ny_r = 2 * q.ny
+        nz_r = 2 * q.nz if p.ndim == 3 else 1
+        ypt = [np.linspace(q.gymin, q.gymax, ny_r), np.zeros(0)]
+        zpt = [np.linspace(q.gzmin, q.gzmax, nz_r) if p.ndim == 3 else np.zeros(1), np.zeros(0)]
+        wghyz = [rng.uniform(0.5, 1.5, (ny_r, nz_r)), np.zeros((0, 0))]
+        states.append(dump.DumpState(it=17, t=3.25, ndim=p.ndim, nx=p.nx, fields=fields, species=species,
+                                     nptx=[11, 0], sptx_max=[30, 0], x0=1.5, xlapse=1.4, ompe=p.ompe, targ_in=0.5,
+                                     targ_end=1e3, xpt=xpt, wghpt=np.ones_like(xpt), ypt=ypt, zpt=zpt, wghyz=wghyz))
+    return states
+
+
+def _same_state(a, b):
+    assert np.array_equal(a.fields, b.fields)
+    assert len(a.species) == len(b.species)
+    for x, y in zip(a.species, b.species):
+        assert np.array_equal(x, y)
+    for u, v in zip(a.ypt + a.zpt + a.wghyz, b.ypt + b.zpt + b.wghyz):
+        assert np.array_equal(u, v)
+    assert np.array_equal(a.xpt, b.xpt) and (a.it, a.t, a.x0, a.xlapse) == (b.it, b.t, b.x0, b.xlapse)
+    assert list(a.nptx) == list(b.nptx) and list(a.sptx_max) == list(b.sptx_max)
+
+
+@pytest.mark.parametrize("ndim,ny_s,nz_s", [(2, 2, 1), (3, 2, 2), (3, 1, 2)])
+def test_block_dump_round_trip(ndim, ny_s, nz_s, tmp_path):
+    """dump_data with npe_y x npe_z ranks: one EB-fields / Particles file per
+    z column with the column's ranks in y order, Dist-wgyz in mype order,
+    npt_arr(1:npe, 1:nsp) and dist_npy / dist_npz in Comm-data."""
+    from aladyn_b200.domain import SlabLayout
+    p = small_case(ndim, nx=16, ny=12, nz=8)
+    lay = SlabLayout(p, ny_s, nz_s)
+    states = _block_states(p, lay)
+    d = str(tmp_path / "dump")
+    dump.write_dump_blocks(d, states, lay, xmax=p.xmax)
+    assert sorted(os.listdir(d)) == sorted(["Comm-data.bin", "Dist-wgyz.bin"] +
+                                           [f"EB-fields{rz:02d}.bin" for rz in range(nz_s)] +
+                                           [f"Particles{rz:02d}.bin" for rz in range(nz_s)])
+    # rank imody of a column at imody times its length
+    raw = np.fromfile(os.path.join(d, "EB-fields00.bin"))
+    n = states[0].fields.size
+    assert raw.size == ny_s * n and np.array_equal(raw[n:2 * n] if ny_s > 1 else raw[:n],
+                                                   states[1 if ny_s > 1 else 0].fields.ravel(order="F"))
+    back = dump.read_dump_blocks(d, lay)
+    assert len(back) == lay.n
+    for a, b in zip(states, back):
+        _same_state(a, b)
+    # the last three records of Comm-data: npt_arr(npe, nsp), dist_npy(npe_y, nsp), dist_npz(npe_z, nsp)
+    data = open(os.path.join(d, "Comm-data.bin"), "rb").read()
+    sizes = [4 * lay.n * 2, 4 * ny_s * 2, 4 * nz_s * 2]
+    pos = len(data) - sum(s + 8 for s in sizes)
+    npt = np.frombuffer(data[pos + 4:pos + 4 + sizes[0]], dtype=np.int32).reshape((lay.n, 2), order="F")
+    assert npt.tolist() == [[st.species[ic].shape[0] for ic in range(2)] for st in states]
+
+
+def test_block_dump_of_one_rank_is_the_single_rank_dump(tmp_path):
+    from aladyn_b200.domain import SlabLayout
+    p = small_case(3, nx=16, ny=12, nz=8)
+    lay = SlabLayout(p, 1, 1)
+    st = _block_states(p, lay)[0]
+    a, b = str(tmp_path / "a"), str(tmp_path / "b")
+    dump.write_dump(a, st, xmax=p.xmax)
+    dump.write_dump_blocks(b, [st], lay, xmax=p.xmax)
+    assert sorted(os.listdir(a)) == sorted(os.listdir(b))
+    for name in os.listdir(a):
+        assert open(os.path.join(a, name), "rb").read() == open(os.path.join(b, name), "rb").read(), name
+
+
+def test_block_dump_needs_an_even_split(tmp_path):
+    from aladyn_b200.domain import SlabLayout
+    p = small_case(2, nx=16, ny=13)
+    lay = SlabLayout(p, 2)
+    with pytest.raises(ValueError):
+        dump.write_dump_blocks(str(tmp_path / "d"), _block_states(p, lay), lay, xmax=p.xmax)
