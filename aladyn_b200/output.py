@@ -1,6 +1,8 @@
-"""Field and particle output files in the reference's formats for one rank
-(npe = 1): fields_out and part_pdata_out (src/IO/pic_out.f90:615-752,
-1356-1500), written from any state holder's arrays (the device's
+"""Field and particle output files in the reference's formats: fields_out
+and part_pdata_out (src/IO/pic_out.f90:615-752, 1356-1500) for one rank and,
+``fields_out_blocks`` / ``part_pdata_out_blocks``, for the ranks of a y / z
+split (every rank's part in mype order), written from any state holder's
+arrays (the device's
 ``PicDevice.get_fields`` / ``get_species`` or the oracle's), so that the
 reference's post-processing reads a run of this library.
 
@@ -128,40 +130,43 @@ def fields_out(dirpath: str, p, fields: np.ndarray, f_ind: int, f_var: int, iout
     return fname
 
 
-def part_pdata_out(dirpath: str, p, part: np.ndarray, pid: int, iout: int, timenow: float = 0.0,
-                   xmin_out: float = -1e30, xmax_out: float = 1e30, ymax_out: float = 1e30, jmp: int = 1,
-                   run: dict | None = None, xmn: float | None = None) -> str:
-    """Species pid (1-based) records part(np, ndv) as part_pdata_out writes
-    them.  Returns the file stem."""
-    run = run or {}
+def _pdata(p, part: np.ndarray, jmp: int, xmin_out: float, xmax_out: float, ymax_out: float) -> np.ndarray:
+    """The output records (float32: phase space, weight, charge) of records
+    p = 1, 1 + jmp, ... inside the output box."""
     ndim = int(p.ndim)
     nd2 = 2 * ndim
-    ndv = nd2 + 2
-    x0 = p.xmn if xmn is None else xmn
-    folder = os.path.join(dirpath, "%04d" % iout)
-    os.makedirs(folder, exist_ok=True)
     sel = part[::jmp]
     keep = (np.abs(sel[:, 1]) <= ymax_out)
     if ndim == 3:
         keep &= np.abs(sel[:, 2]) <= ymax_out
     keep &= (sel[:, 0] >= xmin_out) & (sel[:, 0] <= xmax_out)
     sel = sel[keep]
-    ip = sel.shape[0]
     charge, _, wgh = unpack_slot(sel[:, nd2])
-    pdata = np.empty((ip, ndv), dtype=np.float32)
+    pdata = np.empty((sel.shape[0], nd2 + 2), dtype=np.float32)
     pdata[:, :nd2] = sel[:, :nd2].astype(np.float32)
     pdata[:, nd2] = wgh
     pdata[:, nd2 + 1] = charge.astype(np.float32)
+    return pdata
+
+
+def _part_pars(p, pid, timenow, x0, xmin_out, xmax_out, ymax_out, jmp, run, npe, loc):
+    ndim = int(p.ndim)
+    ndv = 2 * ndim + 2
     nx, ny, nz = int(p.nx), int(p.ny), int(p.nz) if ndim == 3 else 1
     real_par = np.array([timenow, x0, x0 + nx * p.dx, p.gymin, p.gymax, p.gzmin, p.gzmax, run.get("w0_x", 0.0),
                          run.get("w0_y", 0.0), run.get("a0", 0.0), run.get("lam0", 0.0), ELECTRON_MASS,
                          run.get("n0_ref", 0.0), run.get("np_per_cell", 0.0), run.get("j0_norm", 0.0),
                          1.0 / p.lorentz_fact[pid - 1], xmin_out, xmax_out, ymax_out, run.get("gam_min", 0.0)],
                         dtype=np.float32)
-    int_par = np.array([1, nx, ny, nz, run.get("model_id", 1), run.get("dmodel_id", 1), int(p.nsp),
+    int_par = np.array([npe, nx, ny, nz, run.get("model_id", 1), run.get("dmodel_id", 1), int(p.nsp),
                         int(p.curr_ndim), run.get("mp_per_cell", 0), run.get("ion_min", 0), run.get("lpf_ord", 2),
-                        run.get("der_ord", 2), int(p.iform), ndv, 4, endian(), nx, ny, nz, jmp], dtype=np.int32)
-    fname = "%s%02d" % (PART_FILES[pid - 1], iout)
+                        run.get("der_ord", 2), int(p.iform), ndv, 4, endian(), loc[0], loc[1], loc[2], jmp],
+                       dtype=np.int32)
+    return real_par, int_par
+
+
+def _write_part(folder, fname, real_par, int_par, pdatas):
+    ip = sum(d.shape[0] for d in pdatas)
     with open(os.path.join(folder, fname + ".dat"), "w") as f:
         f.write("  Real parameters\n")
         for q in range(PAR_DIM):
@@ -171,9 +176,106 @@ def part_pdata_out(dirpath: str, p, part: np.ndarray, pid: int, iout: int, timen
             f.write(IPAR[q] + f"{int(int_par[q]):8d}\n")
         f.write("  Number of particles in the output box\n")
         f.write(f"{ip:20d}\n")
+    # each rank at mype + ndv * (records of the ranks before it), 4-byte
+    # units: its count, then its records
     with open(os.path.join(folder, fname + ".bin"), "wb") as f:
-        f.write(np.array([ip], dtype=np.int32).tobytes())
-        f.write(pdata.tobytes())
+        for d in pdatas:
+            f.write(np.array([d.shape[0]], dtype=np.int32).tobytes())
+            f.write(d.tobytes())
+
+
+def part_pdata_out(dirpath: str, p, part: np.ndarray, pid: int, iout: int, timenow: float = 0.0,
+                   xmin_out: float = -1e30, xmax_out: float = 1e30, ymax_out: float = 1e30, jmp: int = 1,
+                   run: dict | None = None, xmn: float | None = None) -> str:
+    """Species pid (1-based) records part(np, ndv) as part_pdata_out writes
+    them.  Returns the file stem."""
+    run = run or {}
+    x0 = p.xmn if xmn is None else xmn
+    folder = os.path.join(dirpath, "%04d" % iout)
+    os.makedirs(folder, exist_ok=True)
+    pdata = _pdata(p, part, jmp, xmin_out, xmax_out, ymax_out)
+    nz = int(p.nz) if p.ndim == 3 else 1
+    real_par, int_par = _part_pars(p, pid, timenow, x0, xmin_out, xmax_out, ymax_out, jmp, run, 1,
+                                   (int(p.nx), int(p.ny), nz))
+    fname = "%s%02d" % (PART_FILES[pid - 1], iout)
+    _write_part(folder, fname, real_par, int_par, [pdata])
+    return fname
+
+
+def part_pdata_out_blocks(dirpath: str, layout, parts, pid: int, iout: int, timenow: float = 0.0,
+                          xmin_out: float = -1e30, xmax_out: float = 1e30, ymax_out: float = 1e30, jmp: int = 1,
+                          run: dict | None = None, xmn: float | None = None) -> str:
+    """part_pdata_out of a run split into blocks (``parts[r]`` of block r,
+    mype order): one file, each rank's count and records one after the
+    other; npe and the first rank's local sizes in the parameters."""
+    run = run or {}
+    p = layout.p
+    x0 = p.xmn if xmn is None else xmn
+    folder = os.path.join(dirpath, "%04d" % iout)
+    os.makedirs(folder, exist_ok=True)
+    pdatas = [_pdata(layout.params(r), parts[r], jmp, xmin_out, xmax_out, ymax_out) for r in range(layout.n)]
+    q0 = layout.params(0)
+    real_par, int_par = _part_pars(p, pid, timenow, x0, xmin_out, xmax_out, ymax_out, jmp, run, layout.n,
+                                   (int(q0.nx), int(q0.ny), int(q0.nz) if p.ndim == 3 else 1))
+    fname = "%s%02d" % (PART_FILES[pid - 1], iout)
+    _write_part(folder, fname, real_par, int_par, pdatas)
+    return fname
+
+
+def fields_out_blocks(dirpath: str, layout, fields, f_ind: int, f_var: int, iout: int, tnow: float = 0.0,
+                      jump: int = 1, run: dict | None = None, xmn: float | None = None) -> str:
+    """fields_out of a run split into blocks (``fields[r]``, the local
+    ebf of block r, mype order): rank 0 writes the parameters, then each
+    rank's gr_dim and its interior sampled every ``jump`` node from its own
+    first node, in mype order, then the global grid coordinates; int_par
+    starts with npe_y, npe_z, npe_x and the summed sample counts."""
+    run = run or {}
+    p = layout.p
+    ndim = int(p.ndim)
+    nx, ny, nz = int(p.nx), int(p.ny), int(p.nz) if ndim == 3 else 1
+    x0 = p.xmn if xmn is None else xmn
+    folder = os.path.join(dirpath, "%04d" % iout)
+    os.makedirs(folder, exist_ok=True)
+    name = FIELD_NAMES.get(f_var) or ("Bzfout" if p.nfield == 3 else "Ezfout")
+    fname = "%s%02d" % (name, iout)
+    blocks = []
+    for r in range(layout.n):
+        q = layout.params(r)
+        qny, qnz = int(q.ny), int(q.nz) if ndim == 3 else 1
+        f = fields[r]
+        sub = f[2:nx + 2:jump, 2:qny + 2:jump, 2:qnz + 2:jump if ndim == 3 else 1, f_ind - 1] if ndim == 3 \
+            else f[2:nx + 2:jump, 2:qny + 2:jump, 0:1, f_ind - 1]
+        gr = np.array([_nsample(nx, jump), _nsample(qny, jump), _nsample(qnz, jump) if ndim == 3 else 1],
+                      dtype=np.int32)
+        blocks.append((gr, np.asarray(sub, dtype=np.float32).ravel(order="F")))
+    nyh = [_nsample(layout.rows[ry], jump) for ry in range(layout.ny_s)]
+    nzh = [_nsample(layout.planes[rz], jump) for rz in range(layout.nz_s)] if ndim == 3 else [1]
+    int_par = np.array([layout.ny_s, layout.nz_s, 1, _nsample(nx, jump), sum(nyh), max(layout.rows),
+                        sum(nzh), max(layout.planes) if ndim == 3 else 1, jump, int(p.iby), int(p.iform),
+                        run.get("model_id", 1), run.get("dmodel_id", 1), int(p.nsp), int(p.curr_ndim),
+                        run.get("mp_per_cell", 0), run.get("lpf_ord", 2), run.get("der_ord", 2), 2, endian()],
+                       dtype=np.int32)
+    real_par = np.array([tnow, x0, x0 + nx * p.dx, p.gymin, p.gymax, p.gzmin, p.gzmax, run.get("w0_x", 0.0),
+                         run.get("w0_y", 0.0), run.get("n_over_nc", 0.0), run.get("a0", 0.0), run.get("lam0", 0.0),
+                         ELECTRON_MASS, p.ompe, run.get("targ_in", 0.0), run.get("targ_end", 0.0),
+                         run.get("gam0", 0.0), run.get("nb_over_np", 0.0), run.get("b_charge", 0.0),
+                         run.get("vbeam", 0.0)], dtype=np.float32)
+    with open(os.path.join(folder, fname + ".dat"), "w") as f:
+        f.write("  Integer parameters\n")
+        for r in range(0, PAR_DIM, 4):
+            f.write("".join(f"{int(v):14d}" for v in int_par[r:r + 4]) + "\n")
+        f.write("  Real parameters\n")
+        for r in range(0, PAR_DIM, 4):
+            f.write("".join(fortran_e(v, 14, 5) for v in real_par[r:r + 4]) + "\n")
+    xg = (x0 + p.dx * np.arange(0, nx, jump)).astype(np.float32)
+    yg = (p.dy * (np.arange(1, ny + 1, jump) - 1 - ny // 2)).astype(np.float32)
+    zg = (p.dz * (np.arange(1, nz + 1, jump) - 1 - nz // 2)).astype(np.float32) if ndim == 3 else \
+        np.zeros(1, dtype=np.float32)
+    recs = [np.array([PAR_DIM], dtype=np.int32), int_par, real_par]
+    for gr, w in blocks:
+        recs += [gr, w]
+    with open(os.path.join(folder, fname + ".bin"), "wb") as f:
+        _records(f, recs + [xg, yg, zg])
     return fname
 
 
