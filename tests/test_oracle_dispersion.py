@@ -82,19 +82,23 @@ def _predicted(p, ey0):
     return float((spec * vg).sum() / spec.sum())
 
 
-def _measure(ndim, der_ord, nx, ntr, steps, length, w0):
+def _measure(ndim, der_ord, nx, ntr, steps, length, w0, w_sh=0, shifts=None):
     g = Grid(ndim, nx, ntr, ntr, k0=10.0, yx_rat=4.0, zx_rat=4.0, cfl=0.8)
-    p = make_params(g, w_sh=0, capacity=(16, 0, 0, 0), der_ord=der_ord)
+    p = make_params(g, w_sh=w_sh, capacity=(16, 0, 0, 0), der_ord=der_ord)
     ebf, x = _pulse(p, p.xmn + 0.25 * nx * p.dx, length, w0)
     o = Oracle(p)
     o.set_fields(ebf)
     c0 = _centroid(p, o.get_fields(), x)
     t = 0.0
     for it in range(steps):
-        rc, _ = o.lp_run(t, it)
+        rc, out = o.lp_run(t, it)
         assert rc == 0
+        if shifts is not None:
+            shifts.append(out.nshx)
         t += p.dt
-    v = (_centroid(p, o.get_fields(), x) - c0) / (steps * p.dt)
+    # lab-frame positions: the window's origin moved by the shifts
+    lab = x + (o.xmn() - p.xmn)
+    v = (_centroid(p, o.get_fields(), lab) - c0) / (steps * p.dt)
     return v, _predicted(p, ebf[2:nx + 2, 2:ntr + 2, _ks(p), 1])
 
 
@@ -112,3 +116,21 @@ def test_pulse_moves_at_the_schemes_group_velocity(ndim):
         slow[der_ord] = 1.0 - vp
     assert slow[2] > 0.03
     assert slow[3] < slow[2] / 5
+
+
+def test_group_velocity_in_the_moving_window():
+    """The same 2D pulse inside the moving window (w_sh 10, w_speed 1):
+    every shift moves the fields by whole cells and the origin with them,
+    so the lab-frame centroid still moves at the group velocity, and the
+    window has advanced by the rounded lapse nint(dx_inv * w_speed * dt *
+    w_sh * shifts) cells (lp_window_xshift, src/dynamics/window.f90:
+    276-347), while the pulse (slower than c) slid back in the window."""
+    shifts = []
+    v, vp = _measure(2, 2, **CASES[2], w_sh=10, shifts=shifts)
+    # a shift at every iteration 10, 20, ... 390 of the 400
+    nsh = [n for n in shifts if n > 0]
+    assert [i for i, n in enumerate(shifts) if n > 0] == list(range(10, 400, 10))
+    g = Grid(2, 640, 64, 64, k0=10.0, yx_rat=4.0, zx_rat=4.0, cfl=0.8)
+    p = make_params(g, w_sh=10, capacity=(16, 0, 0, 0))
+    assert sum(nsh) == round(p.dx_inv * p.dt * 10 * len(nsh))
+    assert abs(v - vp) <= 0.01 * (1.0 - vp), (v, vp)
