@@ -59,3 +59,37 @@ def test_charge_density_partition_of_unity():
     q, _, w = unpack_slot(part[:, -1])
     total = float(np.sum(q.astype(np.float32) * w.astype(np.float32), dtype=np.float64))
     assert abs(rho.sum() - total) <= 1e-12 * abs(total)
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_total_current_is_the_charge_weighted_displacement(ndim):
+    """The first moment of the qden shapes is the particle's position, so
+    the Esirkepov current of a step, summed over the grid, is exactly
+    sum_p w_p (x1_p - x0_p) per axis, w = real(charge * wgh, sp): the raw
+    sum of a component is (ndim) w dx_inv displacement (the transverse
+    shape factors of each term sum to ndim), and djc = dx / ndim scales it
+    back (grid_part_connect.f90:979-1059, 1168-1334; set_init_param.f90:
+    92-103)."""
+    from aladyn_b200.sim import unpack_slot
+    p, src, ebf = conservation_case(ndim)
+    o = Oracle(p)
+    o.set_fields(ebf)
+    o.set_plasma_source(src)
+    o.load_plasma(0)
+    t = 0.0
+    for it in range(4):
+        o.lp_run(t, it, initial_time=(it == 0))
+        t += p.dt
+    part0 = o.get_species(0)
+    o.lp_run(t, 4)
+    part1 = o.get_species(0)
+    assert part1.shape[0] == part0.shape[0] > 0
+    q, _, wgh = unpack_slot(part1[:, -1])
+    w = (q.astype(np.float32) * wgh.astype(np.float32)).astype(np.float64)
+    jc = o.get_currents()
+    for a in range(ndim):
+        moved = w * (part1[:, a] - part0[:, a])
+        total = float(np.sum(jc[..., a]))
+        scale = float(np.sum(np.abs(moved)))
+        assert scale > 0
+        assert abs(total - float(np.sum(moved))) <= 1e-13 * scale, (a, total, np.sum(moved), scale)
