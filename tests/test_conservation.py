@@ -61,17 +61,24 @@ def test_charge_density_partition_of_unity():
     assert abs(rho.sum() - total) <= 1e-12 * abs(total)
 
 
+@pytest.mark.parametrize("edge", [6.0, 0.6])
 @pytest.mark.parametrize("ndim", [2, 3])
-def test_total_current_is_the_charge_weighted_displacement(ndim):
+def test_total_current_is_the_charge_weighted_displacement(ndim, edge):
     """The first moment of the qden shapes is the particle's position, so
     the Esirkepov current of a step, summed over the grid, is exactly
     sum_p w_p (x1_p - x0_p) per axis, w = real(charge * wgh, sp): the raw
     sum of a component is (ndim) w dx_inv displacement (the transverse
     shape factors of each term sum to ndim), and djc = dx / ndim scales it
     back (grid_part_connect.f90:979-1059, 1168-1334; set_init_param.f90:
-    92-103)."""
+    92-103).  With the plasma 0.6 cells from the transverse edges the
+    particles deposit into the ghost layers, and the sum holds through the
+    fold of those layers into the boundary cells (jc_xyzbd,
+    mpi_curr_interface.f90:551-643)."""
     from aladyn_b200.sim import unpack_slot
     p, src, ebf = conservation_case(ndim)
+    src.y_min, src.y_max = p.gymin + edge * p.dy, p.gymax - edge * p.dy
+    if ndim == 3:
+        src.z_min, src.z_max = p.gzmin + edge * p.dz, p.gzmax - edge * p.dz
     o = Oracle(p)
     o.set_fields(ebf)
     o.set_plasma_source(src)
