@@ -61,9 +61,10 @@ def test_charge_density_partition_of_unity():
     assert abs(rho.sum() - total) <= 1e-12 * abs(total)
 
 
+@pytest.mark.parametrize("shape", [0, 1])
 @pytest.mark.parametrize("edge", [6.0, 0.6])
 @pytest.mark.parametrize("ndim", [2, 3])
-def test_total_current_is_the_charge_weighted_displacement(ndim, edge):
+def test_total_current_is_the_charge_weighted_displacement(ndim, edge, shape):
     """The first moment of the qden shapes is the particle's position, so
     the Esirkepov current of a step, summed over the grid, is exactly
     sum_p w_p (x1_p - x0_p) per axis, w = real(charge * wgh, sp): the raw
@@ -73,9 +74,11 @@ def test_total_current_is_the_charge_weighted_displacement(ndim, edge):
     92-103).  With the plasma 0.6 cells from the transverse edges the
     particles deposit into the ghost layers, and the sum holds through the
     fold of those layers into the boundary cells (jc_xyzbd,
-    mpi_curr_interface.f90:551-643)."""
+    mpi_curr_interface.f90:551-643).  The cubic extension's 4-point shapes
+    (shape 1) have the same first moment and obey the same identity."""
     from aladyn_b200.sim import unpack_slot
     p, src, ebf = conservation_case(ndim)
+    p.shape = shape
     src.y_min, src.y_max = p.gymin + edge * p.dy, p.gymax - edge * p.dy
     if ndim == 3:
         src.z_min, src.z_max = p.gzmin + edge * p.dz, p.gzmax - edge * p.dz

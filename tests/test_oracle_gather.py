@@ -14,7 +14,9 @@ at right angles to the one B component that is set, the implicit
 midpoint rotation gives d = s x b with d = p^{n+1/2} - p^{n-1/2},
 s = (p^{n+1/2} + p^{n-1/2}) / gamma(p^n), b = (dt / 2) q B / m, so
 b = -(s x d) / |s|^2 along that component.  A half-cell error in any
-component's stagger would show as slope * dx / 2."""
+component's stagger would show as slope * dx / 2.  The cubic extension
+(shape 1: cubic integer-node, quadratic half-node weights) has the same
+first moments and gathers linear fields exactly too."""
 import math
 
 import numpy as np
@@ -71,19 +73,21 @@ def _expected(p, coef, rec):
     return coef[0] + coef[1] * x[0] + coef[2] * x[1] + (coef[3] * x[2] if p.ndim == 3 else 0.0)
 
 
+@pytest.mark.parametrize("shape", [0, 1])
 @pytest.mark.parametrize("ndim", [2, 3])
-def test_linear_electric_field_is_gathered_exactly(ndim):
+def test_linear_electric_field_is_gathered_exactly(ndim, shape):
     p = small_case(ndim, nx=48, ny=32, nz=32, cap=4096, w_sh=0)
+    p.shape = shape
     rng = np.random.default_rng(11)
     rec = _particles(p, 2000, rng, 0.0)
     o = Oracle(p)
-    shape = o.field_shape()
-    f = np.zeros(shape, order="F")
+    fshape = o.field_shape()
+    f = np.zeros(fshape, order="F")
     coefs = {}
     stag = STAGGER3 if ndim == 3 else STAGGER2
     for c in range(ndim):
         coefs[c] = rng.uniform(-0.4, 0.4, 4)
-        f[..., c] = _linear(p, c, stag[c], coefs[c], shape)
+        f[..., c] = _linear(p, c, stag[c], coefs[c], fshape)
     _, out = _one_step(p, f, rec)
     for c in range(ndim):
         got = -out[:, ndim + c] / p.dt  # p^{n+1/2} = dt q E / m, q = -1, m = 1
@@ -91,9 +95,11 @@ def test_linear_electric_field_is_gathered_exactly(ndim):
         assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max(), c
 
 
+@pytest.mark.parametrize("shape", [0, 1])
 @pytest.mark.parametrize("ndim,comp", [(2, 2), (3, 3), (3, 4), (3, 5)])
-def test_linear_magnetic_field_is_gathered_exactly(ndim, comp):
+def test_linear_magnetic_field_is_gathered_exactly(ndim, comp, shape):
     p = small_case(ndim, nx=48, ny=32, nz=32, cap=4096, w_sh=0)
+    p.shape = shape
     rng = np.random.default_rng(17 + comp)
     axis = comp - 3 if ndim == 3 else 2  # the field's direction (x, y, z)
     n = 2000
@@ -101,11 +107,11 @@ def test_linear_magnetic_field_is_gathered_exactly(ndim, comp):
     mom[:, axis] = 0.0
     rec = _particles(p, n, rng, mom[:, :ndim])
     o = Oracle(p)
-    shape = o.field_shape()
-    f = np.zeros(shape, order="F")
+    fshape = o.field_shape()
+    f = np.zeros(fshape, order="F")
     coef = np.array([3.0, *rng.uniform(-0.6, 0.6, 3)])
     stag = STAGGER3 if ndim == 3 else STAGGER2
-    f[..., comp] = _linear(p, comp, stag[comp], coef, shape)
+    f[..., comp] = _linear(p, comp, stag[comp], coef, fshape)
     _, out = _one_step(p, f, rec)
     p0 = np.zeros((n, 3))
     p1 = np.zeros((n, 3))
