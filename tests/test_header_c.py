@@ -2,7 +2,9 @@
 strict C99 and as C++11 (the extern "C" guard), and a C program that takes
 the address of every declared entry point links against libaladyn_gpu.so
 (each declared name resolves in the library at link time) and runs the
-host-only calls (struct sizes, error strings) without a device."""
+host-only calls (struct sizes, error strings) without a device; every
+struct member's offset as a C compiler lays it out equals the ctypes
+mirror's."""
 import ctypes as C
 import os
 import shutil
@@ -59,3 +61,39 @@ def test_header_compiles_and_links_from_c(tmp_path):
     structs = (AgpuParams, AgpuPlasma, AgpuLaser, AgpuStepOut, AgpuDiagOut, AgpuTimers)
     assert [int(v) for v in out[:6]] == [C.sizeof(c) for c in structs]
     assert int(out[6]) == len(names)
+
+
+STRUCTS = {
+    "agpu_params": "AgpuParams", "agpu_plasma": "AgpuPlasma", "agpu_laser": "AgpuLaser",
+    "agpu_lp_pulse": "AgpuLpPulse", "agpu_step_out": "AgpuStepOut", "agpu_diag_out": "AgpuDiagOut",
+    "agpu_timers": "AgpuTimers", "agpu_env_params": "AgpuEnvParams", "agpu_envar_out": "AgpuEnvarOut",
+    "agpu_envar_fields_out": "AgpuEnvarFieldsOut", "agpu_stretch_axis": "AgpuStretchAxis",
+    "agpu_stretch": "AgpuStretch",
+}
+
+
+@pytest.mark.skipif(CC is None, reason="needs gcc")
+def test_every_struct_field_offset_matches_the_ctypes_mirror(tmp_path):
+    """offsetof and sizeof of every member of every struct the header
+    declares, as a C compiler lays them out, equal the ctypes mirror's
+    (same member names: a renamed or reordered member fails to compile or
+    to match)."""
+    lines, want = [], []
+    for cname, pyname in STRUCTS.items():
+        cls = getattr(abi, pyname)
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        want.append(C.sizeof(cls))
+        for fname, _ in cls._fields_:
+            if fname.startswith("reserved"):
+                continue
+            lines.append(f'  printf("%zu\\n", offsetof({cname}, {fname}));')
+            want.append(getattr(cls, fname).offset)
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stddef.h>\n#include <stdio.h>\n#include \"aladyn_gpu.h\"\nint main(void) {\n"
+                   + "\n".join(lines) + "\n  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run([CC, "-std=c99", "-Wall", "-Werror", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)],
+                   check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got == want
+    assert len(want) > 100
