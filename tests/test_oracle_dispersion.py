@@ -134,3 +134,31 @@ def test_group_velocity_in_the_moving_window():
     p = make_params(g, w_sh=10, capacity=(16, 0, 0, 0))
     assert sum(nsh) == round(p.dx_inv * p.dt * 10 * len(nsh))
     assert abs(v - vp) <= 0.01 * (1.0 - vp), (v, vp)
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_open_boundary_absorbs_the_outgoing_pulse(ndim):
+    """The open x boundary (the Mur-type ef_bds / bf_bds faces, src/fields/
+    grid_fields.f90:1069-1354) lets a pulse leave: once the pulse has run
+    out through the right face, under 0.5 % of its field energy is left in
+    the box (measured 0.05 % in 2D, 0.14 % in 3D; a reflecting face would
+    keep all of it)."""
+    nx, ntr = (400, 64) if ndim == 2 else (200, 40)
+    g = Grid(ndim, nx, ntr, ntr, k0=10.0, yx_rat=4.0, zx_rat=4.0, cfl=0.8)
+    p = make_params(g, w_sh=0, capacity=(16, 0, 0, 0))
+    lx = nx * p.dx
+    ebf, _ = _pulse(p, p.xmn + 0.6 * lx, 0.12 * lx, 0.25 * ntr * p.dy)
+    o = Oracle(p)
+    o.set_fields(ebf)
+    ks = _ks(p)
+
+    def energy(f):
+        return float((f[2:nx + 2, 2:ntr + 2, ks, :] ** 2).sum())
+
+    e0 = energy(o.get_fields())
+    t = 0.0
+    for it in range(int(0.75 * lx / p.dt)):
+        rc, _ = o.lp_run(t, it)
+        assert rc == 0
+        t += p.dt
+    assert energy(o.get_fields()) < 5e-3 * e0
